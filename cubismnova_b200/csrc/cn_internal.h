@@ -1,0 +1,228 @@
+// cn_internal.h -- shared host/device definitions of the C-ABI library.
+#pragma once
+
+#include "cubismnova_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace cn {
+
+// Largest BC vector per block field.  The reference allows any length; more
+// than this many BCs on one block is rejected with CN_ERR_TOO_MANY_BC.
+constexpr int kMaxBcPerBlock = 16;
+
+// One BC of a block field as stored on the device (16 bytes).
+struct DevBC {
+    int32_t meta; // dir | side << 2 | kind << 3
+    int32_t pad;
+    double value;
+};
+
+__host__ __device__ inline int bc_dir(int32_t m) { return m & 3; }
+__host__ __device__ inline int bc_side(int32_t m) { return (m >> 2) & 1; }
+__host__ __device__ inline int bc_kind(int32_t m) { return (m >> 3) & 7; }
+
+// Per (component, block) summary of the BC vector: bits [2d, 2d+1] hold the
+// neighbour skipped in direction d (0: none/periodic, 1: -1 side, 2: +1 side),
+// i.e. Block/FieldLab.h:207-214 with the last BC per direction winning.
+// Bit 6 is set if the block has any BC at all.
+constexpr uint8_t kHasBc = 0x40;
+
+// Device view of the BC tables of one component.
+struct BcView {
+    const int32_t *off;  // nblocks+1 offsets (CSR)
+    const DevBC *ent;    // entries
+    const uint8_t *mode; // nblocks summaries
+};
+
+struct HostBC {
+    int dir, side, kind;
+    double value;
+};
+
+} // namespace cn
+
+struct cn_grid {
+    int nb[3];
+    int n[3];
+    int ncomp;
+    cn_dtype dtype;
+    double begin[3], end[3], h[3];
+    size_t esize;
+    int64_t block_stride; // elements
+    int64_t comp_stride;  // elements
+    int nblocks;
+    int device;
+    void *d_data;
+    // BC vectors [comp][block]
+    std::vector<std::vector<std::vector<cn::HostBC>>> bcs;
+    bool bc_dirty;
+    // device BC tables, component c at c*(nblocks+1) / c*nblocks
+    int32_t *d_bc_off;
+    cn::DevBC *d_bc_ent;
+    uint8_t *d_bc_mode;
+    size_t bc_ent_cap;
+    int *d_err; // device error word
+};
+
+namespace cn {
+
+// thread-local error message handling
+cn_status fail(cn_status s, const std::string &msg);
+cn_status ok();
+cn_status cuda_fail(cudaError_t e, const char *what);
+
+#define CN_CUDA_TRY(call)                                                      \
+    do {                                                                       \
+        cudaError_t e__ = (call);                                              \
+        if (e__ != cudaSuccess)                                                \
+            return ::cn::cuda_fail(e__, #call);                                \
+    } while (0)
+
+cn_status check_stencil(const cn_stencil *s);
+// Checks stencil validity and that the ghost width fits into a block.
+cn_status check_lab(const cn_grid *g, const cn_stencil *s);
+// Uploads the BC tables if they changed.
+cn_status sync_bc(cn_grid *g, cudaStream_t stream);
+BcView bc_view(const cn_grid *g, int comp);
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Geometry of a lab for one stencil on one grid.
+struct LabGeom {
+    int n[3];  // cells per block
+    int nb[3]; // blocks per dimension
+    int lo[3]; // -begin
+    int hi[3]; // end - 1
+    int tensorial;
+    int valid_bc[3]; // BC/Base.h:73-78 per direction
+    int64_t bstride;
+};
+
+inline LabGeom make_geom(const cn_grid *g, const cn_stencil *s)
+{
+    LabGeom L;
+    for (int d = 0; d < 3; ++d) {
+        L.n[d] = g->n[d];
+        L.nb[d] = g->nb[d];
+        L.lo[d] = -s->begin[d];
+        L.hi[d] = s->end[d] - 1;
+        L.valid_bc[d] = !(s->begin[d] == 0 || s->end[d] == 1);
+    }
+    L.tensorial = s->tensorial ? 1 : 0;
+    L.bstride = g->block_stride;
+    return L;
+}
+
+// ---------------------------------------------------------------------------
+// Device: value of lab cell q of block `block` after FieldLab::loadData.
+//
+// The reference fills a lab in passes (inner copy, 26 neighbour copies, then
+// each BC of the vector in order, later BCs overwriting earlier ones).  Here
+// every lab cell is resolved on its own: the last BC (highest index k) whose
+// slab covers q decides; Dirichlet yields its value, Absorbing and Symmetry
+// redirect to a source cell whose value is taken *as it was before BC k ran*,
+// i.e. resolved again among BCs 0..k-1.  Each redirect makes the cell inner
+// along the BC's direction (ghost width <= block size), so the chain has at
+// most 3 links.  With no covering BC the cell holds its loaded value: inner
+// data, or the periodic neighbour unless that neighbour was skipped
+// (Block/FieldLabLoader.h:196-205).  Returns false if the reference leaves
+// the cell undefined.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabGeom &L,
+                                          const BcView &bc, int block, int bx, int by,
+                                          int bz, int q0, int q1, int q2, bool apply_bc,
+                                          T &out)
+{
+    int q[3] = {q0, q1, q2};
+    T signs[3];
+    int nsign = 0;
+    // skip flags hold even when the BCs themselves are not applied
+    const uint8_t mode = bc.mode[block];
+    if (apply_bc && (mode & kHasBc)) {
+        const int k0 = bc.off[block];
+        int kmax = bc.off[block + 1] - k0;
+        const DevBC *e = bc.ent + k0;
+        for (int link = 0; link < 4; ++link) {
+            int found = -1;
+            int32_t meta = 0;
+            for (int k = kmax - 1; k >= 0; --k) {
+                const int32_t m = e[k].meta;
+                const int kind = bc_kind(m);
+                if (kind == CN_BC_BASE)
+                    continue;
+                const int d = bc_dir(m);
+                if (!L.valid_bc[d])
+                    continue;
+                const bool in_slab = bc_side(m) == 0 ? (q[d] < 0) : (q[d] >= L.n[d]);
+                if (!in_slab)
+                    continue;
+                if (!L.tensorial) {
+                    bool inner_other = true;
+#pragma unroll
+                    for (int o = 0; o < 3; ++o)
+                        if (o != d && (q[o] < 0 || q[o] >= L.n[o]))
+                            inner_other = false;
+                    if (!inner_other)
+                        continue;
+                }
+                found = k;
+                meta = m;
+                break;
+            }
+            if (found < 0)
+                break;
+            const int d = bc_dir(meta);
+            const int kind = bc_kind(meta);
+            if (kind == CN_BC_DIRICHLET) {
+                T v = static_cast<T>(e[found].value);
+                for (int i = nsign - 1; i >= 0; --i)
+                    v = signs[i] * v;
+                out = v;
+                return true;
+            } else if (kind == CN_BC_ABSORBING) {
+                q[d] = bc_side(meta) == 0 ? 0 : L.n[d] - 1;
+            } else { // symmetry
+                q[d] = (bc_side(meta) == 0 ? -1 : 2 * L.n[d] - 1) - q[d];
+                if (nsign < 3)
+                    signs[nsign++] = static_cast<T>(e[found].value);
+            }
+            kmax = found;
+        }
+    }
+    // loaded value
+    const int r0 = q[0] < 0 ? -1 : (q[0] >= L.n[0] ? 1 : 0);
+    const int r1 = q[1] < 0 ? -1 : (q[1] >= L.n[1] ? 1 : 0);
+    const int r2 = q[2] < 0 ? -1 : (q[2] >= L.n[2] ? 1 : 0);
+    int src_block = block;
+    if (r0 | r1 | r2) {
+        if (!L.tensorial && (r0 != 0) + (r1 != 0) + (r2 != 0) > 1)
+            return false;
+        // skipped neighbour: Block/FieldLab.h:207-214 + FieldLabLoader.h:197-201
+        const int s0 = mode & 3, s1 = (mode >> 2) & 3, s2 = (mode >> 4) & 3;
+        if ((r0 != 0 && s0 == (r0 < 0 ? 1 : 2)) || (r1 != 0 && s1 == (r1 < 0 ? 1 : 2)) ||
+            (r2 != 0 && s2 == (r2 < 0 ? 1 : 2)))
+            return false;
+        int nbx = bx + r0, nby = by + r1, nbz = bz + r2;
+        nbx = nbx < 0 ? nbx + L.nb[0] : (nbx >= L.nb[0] ? nbx - L.nb[0] : nbx);
+        nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
+        nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
+        src_block = nbx + L.nb[0] * (nby + L.nb[1] * nbz);
+        q[0] -= r0 * L.n[0];
+        q[1] -= r1 * L.n[1];
+        q[2] -= r2 * L.n[2];
+    }
+    T v = comp[(int64_t)src_block * L.bstride + q[0] +
+               (int64_t)L.n[0] * (q[1] + (int64_t)L.n[1] * q[2])];
+    for (int i = nsign - 1; i >= 0; --i)
+        v = signs[i] * v;
+    out = v;
+    return true;
+}
+
+} // namespace cn

@@ -1,0 +1,402 @@
+// fd.cu -- K1: lab fill fused with the 2nd-order finite-difference stencils
+// (7-point Laplacian, central gradient, divergence) and the ddx kernel ABI.
+//
+// Design (one CTA per z-slab tile of one block, N0 x N1 x TZ cells):
+//   * the tile's inner cells are one contiguous range of the block (x-fastest
+//     block storage), so a single 1-D TMA bulk copy (cp.async.bulk, mbarrier
+//     completion, bounded wait) stages them into shared memory;
+//   * while that copy is in flight the threads gather the six one-cell faces
+//     of the tile with cn::lab_value (periodic neighbours, BC chain), i.e. the
+//     lab of a stencil (-1,2) non-tensorial (Block/FieldLab.h:180-224);
+//   * each thread then evaluates the stencil from shared memory and writes
+//     coalesced rows of the output blocks.
+// Arithmetic uses __d*_rn / __f*_rn intrinsics so nothing is contracted into
+// an FMA: results are bit-identical to the reference loops compiled without
+// contraction (Kernel/Laplacian/Laplacian.cpp:123-130,
+// Kernel/Divergence/nova/nova.cpp:113-126, ISPC .../ddxGold.cpp:9-33).
+#include "cn_internal.h"
+#include "cn_tma.cuh"
+
+namespace cn {
+
+template <typename T> struct Arith;
+template <> struct Arith<double> {
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+};
+template <> struct Arith<float> {
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+};
+
+enum FdOp { kLap = 0, kGrad = 1, kLapGrad = 2, kDiv = 3 };
+
+template <typename T> struct FdParams {
+    const T *in[3];  // input component bases (kDiv: 3 components)
+    BcView bc[3];
+    LabGeom L;
+    T *lap;          // kLap / kLapGrad / kDiv output component base
+    T *grad;         // kGrad / kLapGrad: first of 3 components
+    int64_t out_cstride;
+    T ih[3], ih2[3];
+    int TZ;
+    int use_bulk;
+    int *err;
+};
+
+// Shared-memory tile of one component: inner cells + the six faces.
+template <typename T> struct Tile {
+    T *in, *xlo, *xhi, *ylo, *yhi, *zlo, *zhi;
+};
+
+template <typename T>
+__device__ __forceinline__ size_t tile_elems(int N0, int N1, int TZ)
+{
+    return (size_t)N0 * N1 * TZ + 2 * ((size_t)N1 * TZ + (size_t)N0 * TZ + (size_t)N0 * N1);
+}
+
+template <typename T>
+__device__ __forceinline__ Tile<T> carve(T *base, int N0, int N1, int TZ)
+{
+    Tile<T> t;
+    t.in = base;
+    t.xlo = t.in + (size_t)N0 * N1 * TZ;
+    t.xhi = t.xlo + (size_t)N1 * TZ;
+    t.ylo = t.xhi + (size_t)N1 * TZ;
+    t.yhi = t.ylo + (size_t)N0 * TZ;
+    t.zlo = t.yhi + (size_t)N0 * TZ;
+    t.zhi = t.zlo + (size_t)N0 * N1;
+    return t;
+}
+
+// Gathers the faces selected by mask (bit 0: x, 1: y, 2: z) of the tile that
+// starts at z0.  Undefined lab cells (never read by these stencils unless the
+// BC set-up leaves a face undefined) are set to zero.
+template <typename T>
+__device__ __forceinline__ void gather_faces(const T *comp, const LabGeom &L, const BcView &bc,
+                                             int block, int bx, int by, int bz, int z0, int TZ,
+                                             const Tile<T> &t, unsigned mask)
+{
+    const int N0 = L.n[0], N1 = L.n[1];
+    const int nth = blockDim.x;
+    if (mask & 1u) {
+        const int m = N1 * TZ;
+        for (int i = threadIdx.x; i < 2 * m; i += nth) {
+            const int side = i / m, r = i - side * m;
+            const int y = r % N1, z = r / N1;
+            T v;
+            if (!lab_value<T>(comp, L, bc, block, bx, by, bz, side ? N0 : -1, y, z0 + z, true, v))
+                v = T(0);
+            (side ? t.xhi : t.xlo)[r] = v;
+        }
+    }
+    if (mask & 2u) {
+        const int m = N0 * TZ;
+        for (int i = threadIdx.x; i < 2 * m; i += nth) {
+            const int side = i / m, r = i - side * m;
+            const int x = r % N0, z = r / N0;
+            T v;
+            if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, side ? N1 : -1, z0 + z, true, v))
+                v = T(0);
+            (side ? t.yhi : t.ylo)[r] = v;
+        }
+    }
+    if (mask & 4u) {
+        const int m = N0 * N1;
+        for (int i = threadIdx.x; i < 2 * m; i += nth) {
+            const int side = i / m, r = i - side * m;
+            const int x = r % N0, y = r / N0;
+            T v;
+            if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, side ? z0 + TZ : z0 - 1, true, v))
+                v = T(0);
+            (side ? t.zhi : t.zlo)[r] = v;
+        }
+    }
+}
+
+template <typename T, int OP>
+__global__ void __launch_bounds__(256) fd_kernel(FdParams<T> p)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
+    T *base = reinterpret_cast<T *>(smem_raw + 128);
+    const LabGeom &L = p.L;
+    const int N0 = L.n[0], N1 = L.n[1], N2 = L.n[2];
+    const int TZ = p.TZ;
+    const int tiles_per_block = N2 / TZ;
+    const int block = blockIdx.x / tiles_per_block;
+    const int z0 = (blockIdx.x - block * tiles_per_block) * TZ;
+    const int bx = block % L.nb[0];
+    const int by = (block / L.nb[0]) % L.nb[1];
+    const int bz = block / (L.nb[0] * L.nb[1]);
+    constexpr int NC = (OP == kDiv) ? 3 : 1;
+    const size_t te = tile_elems<T>(N0, N1, TZ);
+    Tile<T> tl[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        tl[c] = carve<T>(base + c * te, N0, N1, TZ);
+    const uint32_t in_bytes = (uint32_t)((size_t)N0 * N1 * TZ * sizeof(T));
+    const int64_t in_off = (int64_t)block * L.bstride + (int64_t)z0 * N0 * N1;
+
+    if (p.use_bulk) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(bar, in_bytes * NC);
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                bulk_g2s(tl[c].in, p.in[c] + in_off, in_bytes, bar);
+        }
+    } else {
+        const int m = N0 * N1 * TZ;
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            for (int i = threadIdx.x; i < m; i += blockDim.x)
+                tl[c].in[i] = p.in[c][in_off + i];
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const unsigned mask = (OP == kDiv) ? (1u << c) : 7u;
+        gather_faces<T>(p.in[c], L, p.bc[c], block, bx, by, bz, z0, TZ, tl[c], mask);
+    }
+    if (p.use_bulk) {
+        if (!mbar_wait_bounded(bar, 0)) {
+            atomicExch(p.err, kDevErrTimeout);
+        }
+    }
+    __syncthreads();
+
+    using A = Arith<T>;
+    const int m = N0 * N1 * TZ;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int x = i % N0;
+        const int y = (i / N0) % N1;
+        const int z = i / (N0 * N1);
+        const int64_t o = in_off + i;
+        if (OP == kDiv) {
+            const Tile<T> &a = tl[0], &b = tl[1], &c = tl[2];
+            const T axp = x + 1 < N0 ? a.in[i + 1] : a.xhi[y + N1 * z];
+            const T axm = x > 0 ? a.in[i - 1] : a.xlo[y + N1 * z];
+            const T byp = y + 1 < N1 ? b.in[i + N0] : b.yhi[x + N0 * z];
+            const T bym = y > 0 ? b.in[i - N0] : b.ylo[x + N0 * z];
+            const T czp = z + 1 < TZ ? c.in[i + N0 * N1] : c.zhi[x + N0 * y];
+            const T czm = z > 0 ? c.in[i - N0 * N1] : c.zlo[x + N0 * y];
+            const T t0 = A::mul(A::sub(axp, axm), p.ih[0]);
+            const T t1 = A::mul(A::sub(byp, bym), p.ih[1]);
+            const T t2 = A::mul(A::sub(czp, czm), p.ih[2]);
+            p.lap[o] = A::mul(T(0.5), A::add(A::add(t0, t1), t2));
+        } else {
+            const Tile<T> &a = tl[0];
+            const T c0 = a.in[i];
+            const T xp = x + 1 < N0 ? a.in[i + 1] : a.xhi[y + N1 * z];
+            const T xm = x > 0 ? a.in[i - 1] : a.xlo[y + N1 * z];
+            const T yp = y + 1 < N1 ? a.in[i + N0] : a.yhi[x + N0 * z];
+            const T ym = y > 0 ? a.in[i - N0] : a.ylo[x + N0 * z];
+            const T zp = z + 1 < TZ ? a.in[i + N0 * N1] : a.zhi[x + N0 * y];
+            const T zm = z > 0 ? a.in[i - N0 * N1] : a.zlo[x + N0 * y];
+            if (OP == kLap || OP == kLapGrad) {
+                const T c2 = A::mul(T(2), c0);
+                const T ddx = A::mul(p.ih2[0], A::add(A::sub(xp, c2), xm));
+                const T ddy = A::mul(p.ih2[1], A::add(A::sub(yp, c2), ym));
+                const T ddz = A::mul(p.ih2[2], A::add(A::sub(zp, c2), zm));
+                p.lap[o] = A::add(A::add(ddx, ddy), ddz);
+            }
+            if (OP == kGrad || OP == kLapGrad) {
+                p.grad[o] = A::mul(T(0.5), A::mul(A::sub(xp, xm), p.ih[0]));
+                p.grad[o + p.out_cstride] = A::mul(T(0.5), A::mul(A::sub(yp, ym), p.ih[1]));
+                p.grad[o + 2 * p.out_cstride] = A::mul(T(0.5), A::mul(A::sub(zp, zm), p.ih[2]));
+            }
+        }
+    }
+}
+
+static size_t fd_smem_bytes(int N0, int N1, int TZ, size_t es, int nc)
+{
+    const size_t te = (size_t)N0 * N1 * TZ + 2 * ((size_t)N1 * TZ + (size_t)N0 * TZ + (size_t)N0 * N1);
+    return 128 + te * es * nc;
+}
+
+// Largest z-slab height (a divisor of N2) whose tile fits the budget.
+static int pick_tz(int N0, int N1, int N2, size_t es, int nc, size_t budget)
+{
+    for (int tz = N2; tz >= 1; --tz) {
+        if (N2 % tz) continue;
+        if (fd_smem_bytes(N0, N1, tz, es, nc) <= budget) return tz;
+    }
+    return 0;
+}
+
+static cn_status check_out(const cn_grid *in, const cn_grid *out, int out_comp, int ncomp_out)
+{
+    if (!out) return fail(CN_ERR_INVALID_ARGUMENT, "output grid is NULL");
+    if (out->nblocks != in->nblocks || out->n[0] != in->n[0] || out->n[1] != in->n[1] ||
+        out->n[2] != in->n[2] || out->dtype != in->dtype)
+        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
+    if (out_comp < 0 || out_comp + ncomp_out > out->ncomp)
+        return fail(CN_ERR_INVALID_ARGUMENT, "output component out of range");
+    return CN_OK;
+}
+
+template <typename T, int OP>
+static cn_status launch_fd(cn_grid *u, int comp, cn_grid *o1, int c1, cn_grid *o2, int c2,
+                           cudaStream_t st)
+{
+    cn_stencil s = {{-1, -1, -1}, {2, 2, 2}, 0};
+    cn_status stt = check_lab(u, &s);
+    if (stt != CN_OK) return stt;
+    stt = sync_bc(u, st);
+    if (stt != CN_OK) return stt;
+    FdParams<T> p = {};
+    p.L = make_geom(u, &s);
+    const int NC = OP == kDiv ? 3 : 1;
+    for (int c = 0; c < NC; ++c) {
+        p.in[c] = reinterpret_cast<const T *>(u->d_data) + (size_t)(comp + c) * u->comp_stride;
+        p.bc[c] = bc_view(u, comp + c);
+    }
+    if (o1) p.lap = reinterpret_cast<T *>(o1->d_data) + (size_t)c1 * o1->comp_stride;
+    if (o2) {
+        p.grad = reinterpret_cast<T *>(o2->d_data) + (size_t)c2 * o2->comp_stride;
+        p.out_cstride = o2->comp_stride;
+    }
+    for (int d = 0; d < 3; ++d) {
+        p.ih[d] = (T)(1. / u->h[d]);
+        p.ih2[d] = (T)(1. / (u->h[d] * u->h[d]));
+    }
+    const int N0 = u->n[0], N1 = u->n[1], N2 = u->n[2];
+    const int tz = pick_tz(N0, N1, N2, sizeof(T), NC, 100 * 1024);
+    if (tz == 0) return fail(CN_ERR_UNSUPPORTED, "block too large for the fused stencil tile");
+    p.TZ = tz;
+    const size_t tile_bytes = (size_t)N0 * N1 * tz * sizeof(T);
+    p.use_bulk = (tile_bytes % 16 == 0) && ((u->block_stride * sizeof(T)) % 16 == 0);
+    p.err = u->d_err;
+    const size_t smem = fd_smem_bytes(N0, N1, tz, sizeof(T), NC);
+    CN_CUDA_TRY(cudaFuncSetAttribute(fd_kernel<T, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    const int64_t ctas = (int64_t)u->nblocks * (N2 / tz);
+    fd_kernel<T, OP><<<(unsigned)ctas, 256, smem, st>>>(p);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+template <int OP>
+static cn_status dispatch_fd(cn_grid *u, int comp, int ncin, cn_grid *o1, int c1, cn_grid *o2,
+                             int c2, void *stream)
+{
+    if (!u) return fail(CN_ERR_INVALID_ARGUMENT, "input grid is NULL");
+    if (comp < 0 || comp + ncin > u->ncomp)
+        return fail(CN_ERR_INVALID_ARGUMENT, "input component out of range");
+    cn_status s;
+    if (o1 && (s = check_out(u, o1, c1, 1)) != CN_OK) return s;
+    if (o2 && (s = check_out(u, o2, c2, 3)) != CN_OK) return s;
+    cudaStream_t st = as_stream(stream);
+    if (u->dtype == CN_FLOAT64) return launch_fd<double, OP>(u, comp, o1, c1, o2, c2, st);
+    if (u->dtype == CN_FLOAT32) return launch_fd<float, OP>(u, comp, o1, c1, o2, c2, st);
+    return fail(CN_ERR_UNSUPPORTED, "finite-difference stencils need FLOAT32 or FLOAT64 grids");
+}
+
+// ---------------------------------------------------------------- ddx ABI
+template <typename T>
+__global__ void __launch_bounds__(256)
+    ddx_kernel(int nx, int ny, int nz, const T *__restrict__ src, int xps, int xyps,
+               T *__restrict__ dst, int xpd, int xypd, T fac)
+{
+    using A = Arith<T>;
+    const int64_t total = (int64_t)nx * ny * nz;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx);
+        const int y = (int)((i / nx) % ny);
+        const int z = (int)(i / ((int64_t)nx * ny));
+        const T *s = src + x + (int64_t)xps * y + (int64_t)xyps * z;
+        T acc = A::add(s[-1], s[1]);
+        acc = A::add(acc, s[-xps]);
+        acc = A::add(acc, s[xps]);
+        acc = A::add(acc, s[-xyps]);
+        acc = A::add(acc, s[xyps]);
+        acc = A::sub(acc, A::mul(T(6), s[0]));
+        dst[x + (int64_t)xpd * y + (int64_t)xypd * z] = A::mul(fac, acc);
+    }
+}
+
+template <typename T>
+static cn_status launch_ddx(int nx, int ny, int nz, const T *src, int xps, int xyps, T *dst,
+                            int xpd, int xypd, T fac, cudaStream_t st)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !src || !dst)
+        return fail(CN_ERR_INVALID_ARGUMENT, "ddx: bad extent or pointer");
+    const int64_t total = (int64_t)nx * ny * nz;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    ddx_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(nx, ny, nz, src, xps, xyps, dst, xpd, xypd, fac);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+} // namespace cn
+
+using namespace cn;
+
+extern "C" {
+
+cn_status cn_laplacian(cn_grid *u, int comp, cn_grid *out, int out_comp, void *stream)
+{
+    if (!out) return fail(CN_ERR_INVALID_ARGUMENT, "output grid is NULL");
+    return dispatch_fd<kLap>(u, comp, 1, out, out_comp, nullptr, 0, stream);
+}
+
+cn_status cn_gradient(cn_grid *u, int comp, cn_grid *out, int out_comp, void *stream)
+{
+    if (!out) return fail(CN_ERR_INVALID_ARGUMENT, "output grid is NULL");
+    return dispatch_fd<kGrad>(u, comp, 1, nullptr, 0, out, out_comp, stream);
+}
+
+cn_status cn_lap_grad(cn_grid *u, int comp, cn_grid *lap, int lap_comp, cn_grid *grad,
+                      int grad_comp, void *stream)
+{
+    if (!lap || !grad) return fail(CN_ERR_INVALID_ARGUMENT, "output grid is NULL");
+    return dispatch_fd<kLapGrad>(u, comp, 1, lap, lap_comp, grad, grad_comp, stream);
+}
+
+cn_status cn_divergence(cn_grid *v, int comp, cn_grid *out, int out_comp, void *stream)
+{
+    if (!out) return fail(CN_ERR_INVALID_ARGUMENT, "output grid is NULL");
+    return dispatch_fd<kDiv>(v, comp, 3, out, out_comp, nullptr, 0, stream);
+}
+
+void cn_ddx_f64(int Nx, int Ny, int Nz, const double *src, int xps, int xyps, double *dst,
+                int xpd, int xypd, double factor)
+{
+    // ddxGold.cpp:49: fac = 1.0 / (factor * factor)
+    (void)launch_ddx<double>(Nx, Ny, Nz, src, xps, xyps, dst, xpd, xypd,
+                             1.0 / (factor * factor), nullptr);
+}
+
+void cn_ddx_f32(int Nx, int Ny, int Nz, const float *src, int xps, int xyps, float *dst,
+                int xpd, int xypd, float factor)
+{
+    // computed in double, stored as float, as `const Real fac = 1.0 / (f*f)`
+    const float fac = (float)(1.0 / (double)(factor * factor));
+    (void)launch_ddx<float>(Nx, Ny, Nz, src, xps, xyps, dst, xpd, xypd, fac, nullptr);
+}
+
+cn_status cn_ddx_async(cn_dtype dtype, int Nx, int Ny, int Nz, const void *src, int xps,
+                       int xyps, void *dst, int xpd, int xypd, double factor, void *stream)
+{
+    cudaStream_t st = as_stream(stream);
+    if (dtype == CN_FLOAT64)
+        return launch_ddx<double>(Nx, Ny, Nz, (const double *)src, xps, xyps, (double *)dst, xpd,
+                                  xypd, 1.0 / (factor * factor), st);
+    if (dtype == CN_FLOAT32) {
+        const float f = (float)factor;
+        return launch_ddx<float>(Nx, Ny, Nz, (const float *)src, xps, xyps, (float *)dst, xpd,
+                                 xypd, (float)(1.0 / (double)(f * f)), st);
+    }
+    return fail(CN_ERR_UNSUPPORTED, "ddx: dtype must be FLOAT32 or FLOAT64");
+}
+
+} // extern "C"

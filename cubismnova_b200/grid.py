@@ -1,0 +1,246 @@
+"""Grid::Cartesian on one GPU (include/Cubism/Grid/Cartesian.h).
+
+All blocks of all components stay resident in HBM in the reference layout
+(component-major, block-major, x fastest, 32-byte padded blocks), so a host
+array in the reference's SoA order uploads with one copy and
+``Cartesian.loadLab`` becomes an on-device gather.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .core import IndexRange
+
+_DT = {np.dtype(np.float32): _lib.CN_FLOAT32, np.dtype(np.float64): _lib.CN_FLOAT64,
+       np.dtype(np.int32): _lib.CN_INT32}
+
+
+def _stream_handle(stream):
+    """cudaStream_t of a torch stream (or the current torch stream)."""
+    if stream is None:
+        import torch
+        if torch.cuda.is_available():
+            return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+class BCVector:
+    """The BC vector of one block field (Block/Field.h:73-74, 437-442).
+
+    ``push_back`` appends on the device table as well; order is preserved
+    and matters exactly as in the reference."""
+
+    def __init__(self, grid, comp, block):
+        self._g, self._c, self._b = grid, comp, block
+
+    def _list(self):
+        return self._g._bcs[self._c].setdefault(self._b, [])
+
+    def push_back(self, bc):
+        info = bc.getBoundaryInfo()
+        _lib.check(_lib.lib().cn_bc_push(self._g._h, self._c, self._b, info.dir, info.side,
+                                         bc.kind, C.c_double(bc.value)))
+        self._list().append(bc)
+
+    append = push_back
+
+    def clear(self):
+        _lib.check(_lib.lib().cn_bc_clear(self._g._h, self._c, self._b))
+        self._list().clear()
+
+    def __len__(self):
+        return len(self._list())
+
+    def __iter__(self):
+        return iter(list(self._list()))
+
+    def __getitem__(self, i):
+        return self._list()[i]
+
+
+class FieldState:
+    """Cartesian::FieldState (Grid/Cartesian.h:78-85) without the mesh pointer."""
+
+    def __init__(self, block_index):
+        self.block_index = block_index
+
+
+class BlockField:
+    """Non-owning view of one scalar block field (component ``comp``)."""
+
+    def __init__(self, grid, flat, comp):
+        self._g, self.flat, self.comp = grid, flat, comp
+        nb = grid.getSize()
+        self._state = FieldState((flat % nb[0], (flat // nb[0]) % nb[1], flat // (nb[0] * nb[1])))
+
+    def getState(self):
+        return self._state
+
+    def getIndexRange(self):
+        return IndexRange(self._g.getBlockCells())
+
+    def getBC(self):
+        return BCVector(self._g, self.comp, self.flat)
+
+    @property
+    def grid(self):
+        return self._g
+
+
+class TensorBlock:
+    """Rank-1 block (component access ``[c]``), FieldContainer-like."""
+
+    def __init__(self, grid, flat):
+        self._g, self.flat = grid, flat
+
+    def __getitem__(self, c):
+        if not 0 <= c < self._g.ncomp:
+            raise IndexError("component out of range")
+        return BlockField(self._g, self.flat, c)
+
+    def getState(self):
+        return BlockField(self._g, self.flat, 0).getState()
+
+    def getIndexRange(self):
+        return IndexRange(self._g.getBlockCells())
+
+
+class Cartesian:
+    """Grid::Cartesian(nblocks, block_cells, begin, end) with ``ncomp`` components."""
+
+    def __init__(self, nblocks, block_cells, begin=(0.0, 0.0, 0.0), end=(1.0, 1.0, 1.0),
+                 ncomp: int = 1, dtype=np.float64):
+        nb = tuple(int(v) for v in (nblocks if hasattr(nblocks, "__len__") else (nblocks,) * 3))
+        bc = tuple(int(v) for v in (block_cells if hasattr(block_cells, "__len__") else (block_cells,) * 3))
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in _DT:
+            raise ValueError("dtype must be float32, float64 or int32")
+        self.ncomp = int(ncomp)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().cn_grid_create(_lib.ivec3(nb), _lib.ivec3(bc), self.ncomp,
+                                             _DT[self.dtype], _lib.dvec3(begin), _lib.dvec3(end),
+                                             C.byref(h)))
+        self._h = h
+        self._nb, self._n = nb, bc
+        self._bcs = [dict() for _ in range(self.ncomp)]
+        bs, cs, tb = C.c_int64(), C.c_int64(), C.c_size_t()
+        _lib.check(_lib.lib().cn_grid_layout(h, C.byref(bs), C.byref(cs), C.byref(tb)))
+        self.block_stride, self.comp_stride, self.total_bytes = bs.value, cs.value, tb.value
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().cn_grid_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- topology (Grid/Cartesian.h:230-274)
+    def size(self):
+        return self._nb[0] * self._nb[1] * self._nb[2]
+
+    def getSize(self):
+        return self._nb
+
+    def getBlockCells(self):
+        return self._n
+
+    def getCellSize(self):
+        h = (C.c_double * 3)()
+        _lib.check(_lib.lib().cn_grid_cell_size(self._h, h))
+        return tuple(h)
+
+    def flat_index(self, p):
+        if isinstance(p, (int, np.integer)):
+            if not 0 <= int(p) < self.size():
+                raise IndexError("block index out of range")
+            return int(p)
+        x, y, z = (int(v) for v in p)
+        return x + self._nb[0] * (y + self._nb[1] * z)
+
+    def __getitem__(self, p):
+        flat = self.flat_index(p)
+        if self.ncomp == 1:
+            return BlockField(self, flat, 0)
+        return TensorBlock(self, flat)
+
+    def __iter__(self):
+        for i in range(self.size()):
+            yield self[i]
+
+    def field(self, block, comp=0):
+        return BlockField(self, self.flat_index(block), comp)
+
+    # -- data movement
+    def device_ptr(self, comp=0):
+        p = C.c_void_p()
+        _lib.check(_lib.lib().cn_grid_data(self._h, comp, C.byref(p)))
+        return p.value
+
+    def tensor(self, comp=0):
+        """torch view of one component's device storage: (nblocks, block_stride)."""
+        import torch
+        ptr = self.device_ptr(comp)
+        dt = {np.dtype(np.float32): "<f4", np.dtype(np.float64): "<f8", np.dtype(np.int32): "<i4"}[self.dtype]
+
+        class _CAI:
+            __cuda_array_interface__ = {"shape": (self.size(), self.block_stride), "typestr": dt,
+                                        "data": (ptr, False), "version": 3, "strides": None}
+        return torch.as_tensor(_CAI(), device="cuda")
+
+    def upload(self, host, comp=0, stream=None):
+        a = np.ascontiguousarray(host, dtype=self.dtype).reshape(-1)
+        if a.size != self.comp_stride:
+            raise ValueError(f"expected {self.comp_stride} elements, got {a.size}")
+        _lib.check(_lib.lib().cn_grid_upload(self._h, comp, a.ctypes.data_as(C.c_void_p),
+                                             a.nbytes, None if stream is None else _stream_handle(stream)))
+        if stream is not None:
+            self._keep = a
+
+    def download(self, comp=0):
+        a = np.empty(self.comp_stride, dtype=self.dtype)
+        _lib.check(_lib.lib().cn_grid_download(self._h, comp, a.ctypes.data_as(C.c_void_p),
+                                               a.nbytes, None))
+        return a
+
+    def blocks_view(self, flat_array):
+        """(nblocks, nz, ny, nx) view of a component array in grid layout."""
+        n = self._n
+        cells = n[0] * n[1] * n[2]
+        return flat_array.reshape(self.size(), self.block_stride)[:, :cells].reshape(
+            self.size(), n[2], n[1], n[0])
+
+    def copy_from(self, other, stream=None):
+        """Cartesian::operator= (Grid/Cartesian.h:160-169)."""
+        _lib.check(_lib.lib().cn_grid_copy(self._h, other._h, _stream_handle(stream)))
+
+    # -- boundary conditions
+    def push_boundary_bc(self, bc_factory, dir, side, comp=0):
+        """Push ``bc_factory(dir, side)`` onto every block touching face (dir, side)."""
+        for f in self:
+            fld = f if self.ncomp == 1 else f[comp]
+            bi = fld.getState().block_index
+            if (side == 0 and bi[dir] == 0) or (side == 1 and bi[dir] == self._nb[dir] - 1):
+                fld.getBC().push_back(bc_factory(dir, side))
+
+    def sync_bcs(self, stream=None):
+        _lib.check(_lib.lib().cn_bc_sync(self._h, _stream_handle(stream)))
+
+    # -- lab loading (Grid/Cartesian.h:412-427)
+    def loadLab(self, field, lab, c=0, d=0):
+        comp = field.comp if isinstance(field, BlockField) else int(c)
+        lab.loadData(field.getState().block_index, self, comp=comp)

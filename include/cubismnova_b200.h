@@ -1,0 +1,176 @@
+/*
+ * cubismnova_b200.h -- C ABI of the B200-native CubismNova lab/stencil path.
+ *
+ * The reference (CubismNova 0.6.0) is a header-only C++ template library with
+ * no FFI of its own.  The entry points below are the seams a replacement slots
+ * behind; each one names the reference interface it replaces (file:line
+ * within the CubismNova source tree).
+ *
+ * Conventions
+ *   - All functions return cn_status (0 == CN_OK); no C++ exception crosses
+ *     this boundary.  cn_last_error_string() holds the message of the last
+ *     failure on the calling thread, using the reference's own strings where
+ *     the reference throws.
+ *   - The library owns device memory of a grid; callers own host buffers.
+ *   - "stream" is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Every call with a stream argument is stream-ordered and
+ *     returns without waiting for the device unless stated otherwise.
+ *   - Grid data layout on the device is the reference layout
+ *     (Grid/Cartesian.h:490-529, Grid/BlockFieldAssembler.h:189-194):
+ *     component-major, then block-major in x-fastest block order, each block
+ *     block_cells[0]*block_cells[1]*block_cells[2] cells x-fastest, blocks
+ *     block_stride elements apart (cells*sizeof rounded up to 32 bytes).
+ *     A host array in the reference's SoA order uploads with one copy.
+ *   - Only cell-centred fields are supported.
+ */
+#ifndef CUBISMNOVA_B200_H
+#define CUBISMNOVA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CN_ABI_VERSION 1
+
+typedef enum cn_status {
+    CN_OK = 0,
+    CN_ERR_INVALID_ARGUMENT = 1,
+    CN_ERR_STENCIL_BEGIN = 2,    /* "Stencil: begin_ must be <= 0" (Core/Stencil.h:101-102) */
+    CN_ERR_STENCIL_END = 3,      /* "Stencil: end_ must be > 0" (Core/Stencil.h:104-105) */
+    CN_ERR_STENCIL_COMPONENT = 4,/* a single component violates begin<=0 / end>0 */
+    CN_ERR_NOT_ALLOCATED = 5,    /* "FieldLab: can not load lab data when not allocated first" (Block/FieldLab.h:189-190) */
+    CN_ERR_NO_FIELD = 6,         /* "FieldLab: no field loaded" (Block/FieldLab.h:417-419) */
+    CN_ERR_SIZE_MISMATCH = 7,    /* "Cartesian: Can not assign two grids of unequal size." (Grid/Cartesian.h:162-164) */
+    CN_ERR_STENCIL_TOO_WIDE = 8, /* ghost width larger than the block in some dimension */
+    CN_ERR_CUDA = 9,             /* a CUDA runtime call failed */
+    CN_ERR_OUT_OF_MEMORY = 10,
+    CN_ERR_DEVICE = 11,          /* a kernel reported an error word */
+    CN_ERR_UNSUPPORTED = 12,
+    CN_ERR_TOO_MANY_BC = 13
+} cn_status;
+
+typedef enum cn_dtype { CN_FLOAT32 = 0, CN_FLOAT64 = 1, CN_INT32 = 2 } cn_dtype;
+
+/* BC::Base (periodic no-op) / BC::Dirichlet / BC::Absorbing / BC::Symmetry
+ * (BC/Base.h:39-79, BC/Dirichlet.h:38, BC/Absorbing.h:35, BC/Symmetry.h:43) */
+typedef enum cn_bc_kind {
+    CN_BC_BASE = 0,
+    CN_BC_DIRICHLET = 1,
+    CN_BC_ABSORBING = 2,
+    CN_BC_SYMMETRY = 3
+} cn_bc_kind;
+
+/* Core::Stencil(begin, end, tensorial) (Core/Stencil.h:44-67): begin <= 0
+ * inclusive, end > 0 exclusive; tensorial labs include edge/corner ghosts. */
+typedef struct cn_stencil {
+    int begin[3];
+    int end[3];
+    int tensorial;
+} cn_stencil;
+
+typedef struct cn_grid cn_grid;
+
+/* ---------------------------------------------------------------- errors */
+const char *cn_status_string(cn_status s);
+/* Message of the last failed call on this thread ("" if none). */
+const char *cn_last_error_string(void);
+int cn_abi_version(void);
+
+/* Validates a stencil exactly like Core::Stencil::check_
+ * (Core/Stencil.h:99-107), then rejects single-component violations. */
+cn_status cn_stencil_check(const cn_stencil *s);
+
+/* ------------------------------------------------------------------ grid */
+/* Grid::Cartesian(nblocks, block_cells, begin, end) (Grid/Cartesian.h:132-143)
+ * with ncomp scalar components (rank-0: 1, rank-1 vector: 3, Euler state: 5).
+ * Allocates the device storage on the current CUDA device. */
+cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int ncomp,
+                         cn_dtype dtype, const double begin[3], const double end[3],
+                         cn_grid **out);
+cn_status cn_grid_destroy(cn_grid *g);
+/* Layout in elements: block stride, component stride; total bytes. */
+cn_status cn_grid_layout(const cn_grid *g, int64_t *block_stride, int64_t *comp_stride,
+                         size_t *total_bytes);
+/* Mesh::StructuredUniform cell size h = (end-begin)/cells
+ * (Mesh/StructuredUniform.h:61, :333-336). */
+cn_status cn_grid_cell_size(const cn_grid *g, double h[3]);
+/* Device pointer of one component (component-major SoA). */
+cn_status cn_grid_data(cn_grid *g, int comp, void **device_ptr);
+/* Host <-> device copy of one component, reference SoA order; nbytes must be
+ * comp_stride*sizeof(dtype).  Blocking unless the host memory is pinned. */
+cn_status cn_grid_upload(cn_grid *g, int comp, const void *host, size_t nbytes, void *stream);
+cn_status cn_grid_download(const cn_grid *g, int comp, void *host, size_t nbytes, void *stream);
+/* Cartesian::operator= (Grid/Cartesian.h:160-169): copy all block data. */
+cn_status cn_grid_copy(cn_grid *dst, const cn_grid *src, void *stream);
+
+/* -------------------------------------------------------------------- BC */
+/* field.getBC().push_back(new BC::Kind(dir, side, value))
+ * (Block/Field.h:437-442) for block `block` (flat x-fastest index) of
+ * component comp.  value = Dirichlet value or Symmetry sign; ignored
+ * otherwise.  Order matters exactly as in the reference vector. */
+cn_status cn_bc_push(cn_grid *g, int comp, int block, int dir, int side, cn_bc_kind kind,
+                     double value);
+/* Push the same BC to every block touching domain face (dir, side); the
+ * usual way the reference's drivers attach BCs to a Cartesian grid. */
+cn_status cn_bc_push_boundary(cn_grid *g, int comp, int dir, int side, cn_bc_kind kind,
+                              double value);
+/* Clear the BC vector of one block (block >= 0) or of all blocks (-1). */
+cn_status cn_bc_clear(cn_grid *g, int comp, int block);
+cn_status cn_bc_count(const cn_grid *g, int comp, int block, int *count);
+/* Upload the BC tables now (otherwise done by the next kernel call); call it
+ * before capturing kernels of this grid into a CUDA graph. */
+cn_status cn_bc_sync(cn_grid *g, void *stream);
+
+/* ------------------------------------------------------------------- lab */
+/* Extent of the dense active lab range of one block for stencil s:
+ * block_cells - begin + end - 1 (Block/FieldLab.h:199-202). */
+cn_status cn_lab_extent(const cn_grid *g, const cn_stencil *s, int extent[3]);
+/* Cartesian::loadLab / FieldLab::loadData (Grid/Cartesian.h:412-427,
+ * Block/FieldLab.h:180-224) for blocks [block_begin, block_begin+count):
+ * lab i is written to d_labs + i*prod(extent) elements, x fastest, lab cell
+ * q (q_d in [begin_d, block_cells_d+end_d-1)) at offset
+ * (q0-b0) + E0*((q1-b1) + E1*(q2-b2)).  Cells the reference leaves undefined
+ * (corners of a non-tensorial lab, a skipped neighbour no valid BC covers)
+ * are not written.  apply_bc = 0 skips the BCs (loadData(..., false)). */
+cn_status cn_lab_fill(cn_grid *g, int comp, const cn_stencil *s, int block_begin,
+                      int block_count, int apply_bc, void *d_labs, void *stream);
+
+/* ------------------------------------------------------- fused stencils */
+/* Each call fills the lab of every block (stencil (-1,2) non-tensorial, BCs
+ * of the input component applied) and applies the stencil in the same
+ * kernel, writing the output grid (same geometry and dtype, FLOAT64).
+ *
+ * 7-point Laplacian, grouping of Kernel/Laplacian/Laplacian.cpp:123-130:
+ *   out = ihx2*((u[+x] - 2u) + u[-x]) + ihy2*(...) + ihz2*(...), no FMA. */
+cn_status cn_laplacian(cn_grid *u, int comp, cn_grid *out, int out_comp, void *stream);
+/* Central gradient, out_comp..out_comp+2 = 0.5*((u[+d]-u[-d]) * ih_d)
+ * (Kernel/Divergence/nova/nova.cpp:113-126 per-direction terms), no FMA. */
+cn_status cn_gradient(cn_grid *u, int comp, cn_grid *out, int out_comp, void *stream);
+/* Laplacian and gradient from one lab load (one kernel). */
+cn_status cn_lap_grad(cn_grid *u, int comp, cn_grid *lap, int lap_comp, cn_grid *grad,
+                      int grad_comp, void *stream);
+/* Divergence of components comp..comp+2 of v (nova.cpp:113-126):
+ *   out = 0.5*((((v0[+x]-v0[-x])*ihx) + ((v1[+y]-v1[-y])*ihy)) + ((v2[+z]-v2[-z])*ihz)). */
+cn_status cn_divergence(cn_grid *v, int comp, cn_grid *out, int out_comp, void *stream);
+
+/* The kernel ABI of the reference's ISPC benchmark
+ * (test/sandbox/Benchmarks/ISPC/BaseBenchmark.h:27-37) on DEVICE pointers:
+ * dst = fac*(sum of 6 neighbours - 6*src), fac = 1/(factor*factor),
+ * summation order of ISPC/CFD_2ndOrder/DDX/ddxGold.cpp:9-33, no FMA.
+ * src points at the first inner element of a pitched lab.  Runs on the
+ * legacy default stream and returns after launch. */
+void cn_ddx_f64(int Nx, int Ny, int Nz, const double *src, int x_pitch_src, int xy_pitch_src,
+                double *dst, int x_pitch_dst, int xy_pitch_dst, double factor);
+void cn_ddx_f32(int Nx, int Ny, int Nz, const float *src, int x_pitch_src, int xy_pitch_src,
+                float *dst, int x_pitch_dst, int xy_pitch_dst, float factor);
+cn_status cn_ddx_async(cn_dtype dtype, int Nx, int Ny, int Nz, const void *src, int x_pitch_src,
+                       int xy_pitch_src, void *dst, int x_pitch_dst, int xy_pitch_dst,
+                       double factor, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUBISMNOVA_B200_H */

@@ -1,0 +1,188 @@
+"""CPU oracle for the lab-fill / stencil hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker.  The product
+package ``cubismnova_b200`` never imports it.
+
+Two libraries sit behind it:
+
+* ``liboracle.so`` -- the plain-C restatement (``cn_oracle.c`` and friends),
+  built from this directory by ``make``;
+* ``_ref/libcnref.so`` -- the reference's own header-only C++ code
+  (``Block/FieldLab.h``, ``BC/*.h``, ``Grid/Cartesian.h``) instantiated by
+  ``ref_shim.cpp``; present only where it was built from the reference
+  sources.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+BC_BASE, BC_DIRICHLET, BC_ABSORBING, BC_SYMMETRY = 0, 1, 2, 3
+
+
+class OrBC(C.Structure):
+    _fields_ = [("dir", C.c_int32), ("side", C.c_int32), ("kind", C.c_int32),
+                ("pad", C.c_int32), ("value", C.c_double)]
+
+
+class OrGeom(C.Structure):
+    _fields_ = [("nb", C.c_int32 * 3), ("n", C.c_int32 * 3), ("lo", C.c_int32 * 3),
+                ("hi", C.c_int32 * 3), ("tensorial", C.c_int32),
+                ("block_stride", C.c_int64)]
+
+
+_lib = None
+_ref = None
+
+
+def build(quiet: bool = True) -> None:
+    """Run ``make`` in this directory (oracle + reference shim if possible)."""
+    out = subprocess.run(["make", "-C", _HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = C.CDLL(path)
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libcnref.so"))
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        path = os.path.join(_HERE, "_ref", "libcnref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError("reference shim not built: " + path)
+        _ref = C.CDLL(path)
+        _ref.ref_c1_sweep_f64.restype = C.c_double
+    return _ref
+
+
+def block_stride(n, dtype) -> int:
+    """Elements between blocks: cells*sizeof rounded up to 32 B
+    (Grid/Cartesian.h:490-513)."""
+    itemsize = np.dtype(dtype).itemsize
+    cells = int(n[0]) * int(n[1]) * int(n[2])
+    nbytes = (cells * itemsize + 31) // 32 * 32
+    return nbytes // itemsize
+
+
+def make_geom(nb, n, lo, hi, tensorial, stride) -> OrGeom:
+    g = OrGeom()
+    for d in range(3):
+        g.nb[d], g.n[d], g.lo[d], g.hi[d] = int(nb[d]), int(n[d]), int(lo[d]), int(hi[d])
+    g.tensorial = 1 if tensorial else 0
+    g.block_stride = int(stride)
+    return g
+
+
+def bc_arrays(nblocks: int, bclists):
+    """CSR (offsets, entries) from a dict block -> list of (dir, side, kind, value)."""
+    off = np.zeros(nblocks + 1, dtype=np.int32)
+    ents = []
+    for b in range(nblocks):
+        lst = bclists.get(b, []) if bclists else []
+        off[b + 1] = off[b] + len(lst)
+        for (d, s, k, v) in lst:
+            e = OrBC()
+            e.dir, e.side, e.kind, e.value = int(d), int(s), int(k), float(v)
+            ents.append(e)
+    arr = (OrBC * max(1, len(ents)))(*ents) if ents else (OrBC * 1)()
+    return off, arr
+
+
+_SUFFIX = {np.dtype(np.float64): "f64", np.dtype(np.float32): "f32",
+           np.dtype(np.int32): "i32"}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def lab_fill(comp, nb, n, lo, hi, tensorial, bclists, block, use_ref=False,
+             lab_init=None):
+    """Lab of one block: returns (lab[Lz,Ly,Lx], defined[Lz,Ly,Lx] bool)."""
+    comp = np.ascontiguousarray(comp)
+    sfx = _SUFFIX[comp.dtype]
+    stride = block_stride(n, comp.dtype)
+    g = make_geom(nb, n, lo, hi, tensorial, stride)
+    nblocks = int(np.prod(nb))
+    off, ents = bc_arrays(nblocks, bclists)
+    L = [int(n[d]) + int(lo[d]) + int(hi[d]) for d in range(3)]
+    lab = np.zeros((L[2], L[1], L[0]), dtype=comp.dtype) if lab_init is None \
+        else np.array(lab_init, dtype=comp.dtype, copy=True)
+    w = np.zeros((L[2], L[1], L[0]), dtype=np.uint8)
+    f = getattr(ref() if use_ref else lib(), ("ref_" if use_ref else "or_") + "lab_fill_" + sfx)
+    rc = f(C.byref(g), _ptr(comp), _ptr(off), ents, C.c_int(block), _ptr(lab), _ptr(w))
+    if rc != 0:
+        raise ValueError("lab fill rejected the geometry")
+    return lab, w.astype(bool)
+
+
+def laplacian_f64(comp, nb, n, bclists, ih2):
+    comp = np.ascontiguousarray(comp, dtype=np.float64)
+    stride = block_stride(n, np.float64)
+    g = make_geom(nb, n, (1, 1, 1), (1, 1, 1), False, stride)
+    off, ents = bc_arrays(int(np.prod(nb)), bclists)
+    out = np.zeros_like(comp)
+    ih2a = (C.c_double * 3)(*[float(v) for v in ih2])
+    rc = lib().or_laplacian_f64(C.byref(g), _ptr(comp), _ptr(off), ents, ih2a, _ptr(out))
+    if rc:
+        raise ValueError("or_laplacian_f64 failed")
+    return out
+
+
+def gradient_f64(comp, nb, n, bclists, ih):
+    comp = np.ascontiguousarray(comp, dtype=np.float64)
+    stride = block_stride(n, np.float64)
+    g = make_geom(nb, n, (1, 1, 1), (1, 1, 1), False, stride)
+    off, ents = bc_arrays(int(np.prod(nb)), bclists)
+    out = np.zeros((3,) + comp.shape, dtype=np.float64)
+    iha = (C.c_double * 3)(*[float(v) for v in ih])
+    rc = lib().or_gradient_f64(C.byref(g), _ptr(comp), _ptr(off), ents, iha, _ptr(out),
+                               C.c_int64(comp.size))
+    if rc:
+        raise ValueError("or_gradient_f64 failed")
+    return out
+
+
+def ddx(src, pitches, extent, factor, dst_pitches):
+    """ddx gold kernel on a pitched array; src is the full lab, offset given."""
+    raise NotImplementedError
+
+
+def ref_c1_sweep(comp, nb, n, ih2, ih, threads=0, nblocks=0, reps=1,
+                 want_lap=True, want_grad=True):
+    """Reference FieldLab + Laplacian/gradient loops with OpenMP; returns
+    (seconds per sweep, lap, grad)."""
+    comp = np.ascontiguousarray(comp, dtype=np.float64)
+    stride = block_stride(n, np.float64)
+    lap = np.zeros_like(comp) if want_lap else None
+    grad = np.zeros((3,) + comp.shape, dtype=np.float64) if want_grad else None
+    nba = (C.c_int * 3)(*[int(v) for v in nb])
+    na = (C.c_int * 3)(*[int(v) for v in n])
+    t = ref().ref_c1_sweep_f64(
+        nba, na, _ptr(comp), C.c_int64(stride),
+        _ptr(lap) if lap is not None else None,
+        _ptr(grad) if grad is not None else None, C.c_int64(comp.size),
+        (C.c_double * 3)(*ih2), (C.c_double * 3)(*ih),
+        C.c_int(threads if threads > 0 else (os.cpu_count() or 1)),
+        C.c_int(nblocks), C.c_int(reps))
+    return t, lap, grad
