@@ -12,5 +12,7 @@ from . import bc as BC
 from . import grid as Grid
 from . import block as Block
 from . import ops
+from . import euler
+from . import workloads
 
-__all__ = ["Core", "BC", "Grid", "Block", "ops", "CnError", "build"]
+__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "CnError", "build"]

@@ -1,0 +1,506 @@
+// euler.cu -- K2: lab fill fused with WENO5-JS + Rusanov + flux divergence for
+// the 3-D compressible Euler equations, and the fused SSP-RK3 stage update.
+//
+// One CTA owns an 8x8x8 tile of one block.  It stages the tile and its
+// cross-shaped 3-cell halo (the lab of a stencil (-3,4) non-tensorial,
+// Block/FieldLab.h:180-224) of all five conserved variables into shared memory
+// as primitives (rho, u, v, w, p): halo cells inside the block are plain
+// loads, cells outside are resolved by cn::lab_value (periodic neighbour,
+// skip rule and BC chain of each component's BC vector).  Then, per
+// direction, every face flux of the tile is computed exactly once (one thread
+// per face: 2 x 5 WENO5 reconstructions + Rusanov), stored in shared memory,
+// and differenced into per-cell accumulators held in registers.  The epilogue
+// applies the SSP-RK3 (Shu & Osher 1988) convex combination and optionally
+// accumulates FP64 conservation sums per CTA (reduced in a fixed order by a
+// second kernel, so the sums are deterministic).
+//
+// Shared memory per CTA: 5 x 1664 primitives + 5 x 576 face fluxes.
+#include "cn_internal.h"
+#include "cn_tma.cuh"
+#include "euler_math.cuh"
+
+#include <cstring>
+#include <mutex>
+
+namespace cn {
+namespace euler {
+
+constexpr int TB = 8;                 // tile edge
+constexpr int G = 3;                  // ghost width
+constexpr int XW = TB + 2 * G;        // 14
+constexpr int NXB = XW * TB * TB;     // core + x halos: 896
+constexpr int NYH = TB * 2 * G * TB;  // y halos: 384
+constexpr int NZH = 2 * G * TB * TB;  // z halos: 384
+constexpr int SV = NXB + NYH + NZH;   // cells per variable: 1664
+constexpr int NCELL = TB * TB * TB;   // 512
+constexpr int NFACE = (TB + 1) * TB * TB; // 576
+constexpr int NT = 192;               // threads per CTA (576 = 3 * 192)
+constexpr int CPT = (NCELL + NT - 1) / NT; // cells per thread: 3
+
+template <typename T> struct StageParams {
+    const T *U[5];   // state whose lab is loaded (component bases)
+    const T *Un[5];  // U^n (stages 2 and 3)
+    T *out[5];
+    BcView bc[5];
+    LabGeom L;
+    T ih[3];
+    T dt;
+    T gamma, gm1, igm1;
+    int stage;       // 0: out = L(U); 1..3: SSP-RK3 stage
+    double *partials; // per-CTA FP64 sums of the 5 outputs (may be null)
+    int *err;
+};
+
+// shared-memory index of tile-local cell (x, y, z), coordinates in [-3, 11)
+// on the cross: core/x-halo box, then y halos, then z halos
+__device__ __forceinline__ int sidx(int x, int y, int z)
+{
+    const bool in_y = (unsigned)y < (unsigned)TB;
+    const bool in_z = (unsigned)z < (unsigned)TB;
+    const int ixb = (z * TB + y) * XW + (x + G);
+    const int jy = y < 0 ? y + G : y - TB + G;
+    const int iyh = NXB + (z * 2 * G + jy) * TB + x;
+    const int kz = z < 0 ? z + G : z - TB + G;
+    const int izh = NXB + NYH + (kz * TB + y) * TB + x;
+    return (in_y && in_z) ? ixb : (in_z ? iyh : izh);
+}
+
+template <typename T>
+__device__ __forceinline__ void decode_cross(int i, int &x, int &y, int &z)
+{
+    if (i < NXB) {
+        x = i % XW - G;
+        y = (i / XW) % TB;
+        z = i / (XW * TB);
+    } else if (i < NXB + NYH) {
+        const int r = i - NXB;
+        x = r % TB;
+        const int jy = (r / TB) % (2 * G);
+        z = r / (TB * 2 * G);
+        y = jy < G ? jy - G : jy - G + TB;
+    } else {
+        const int r = i - NXB - NYH;
+        x = r % TB;
+        y = (r / TB) % TB;
+        const int kz = r / (TB * TB);
+        z = kz < G ? kz - G : kz - G + TB;
+    }
+}
+
+// Face fluxes of direction D for the whole tile (one thread per face, each
+// face once), then flux differences into the per-cell accumulators.
+template <typename T, int D>
+__device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F, T (&acc)[CPT][5],
+                                      T gamma, T igm1, T ihd)
+{
+    for (int f = threadIdx.x; f < NFACE; f += NT) {
+        int x, y, z;
+        if (D == 0) {
+            x = f % (TB + 1);
+            y = (f / (TB + 1)) % TB;
+            z = f / ((TB + 1) * TB);
+        } else if (D == 1) {
+            x = f % TB;
+            y = (f / TB) % (TB + 1);
+            z = f / (TB * (TB + 1));
+        } else {
+            x = f % TB;
+            y = (f / TB) % TB;
+            z = f / (TB * TB);
+        }
+        // cells i-2 .. i+3 around the face between cell i = (x,y,z)-e_D and (x,y,z)
+        int idx[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int o = k - 3;
+            idx[k] = D == 0 ? sidx(x + o, y, z) : (D == 1 ? sidx(x, y + o, z) : sidx(x, y, z + o));
+        }
+        T WL[5], WR[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const T *Wc = W + c * SV;
+            const T v0 = Wc[idx[0]], v1 = Wc[idx[1]], v2 = Wc[idx[2]];
+            const T v3 = Wc[idx[3]], v4 = Wc[idx[4]], v5 = Wc[idx[5]];
+            WL[c] = weno5<T>(v0, v1, v2, v3, v4);
+            WR[c] = weno5<T>(v5, v4, v3, v2, v1);
+        }
+        T Fl[5];
+        rusanov<T>(WL, WR, D, gamma, igm1, Fl);
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            F[c * NFACE + f] = Fl[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int cidx = threadIdx.x + k * NT;
+        if (cidx < NCELL) {
+            const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
+            const int flo = D == 0 ? x + (TB + 1) * (y + TB * z)
+                                   : (D == 1 ? x + TB * (y + (TB + 1) * z) : x + TB * (y + TB * z));
+            constexpr int step = D == 0 ? 1 : (D == 1 ? TB : TB * TB);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                const T df = F[c * NFACE + flo + step] - F[c * NFACE + flo];
+                acc[k][c] = D == 0 ? df * ihd : dfma(df, ihd, acc[k][c]);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT, 2) stage_kernel(StageParams<T> p)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T *W = reinterpret_cast<T *>(smem_raw);       // [5][SV]
+    T *F = W + 5 * SV;                            // [5][NFACE]
+    __shared__ double red[NT / 32][5];
+
+    const LabGeom &L = p.L;
+    const int N0 = L.n[0], N1 = L.n[1], N2 = L.n[2];
+    const int tx = N0 / TB, ty = N1 / TB, tz = N2 / TB;
+    const int tiles = tx * ty * tz;
+    const int block = blockIdx.x / tiles;
+    int t = blockIdx.x - block * tiles;
+    const int x0 = (t % tx) * TB;
+    t /= tx;
+    const int y0 = (t % ty) * TB;
+    const int z0 = (t / ty) * TB;
+    const int bx = block % L.nb[0];
+    const int by = (block / L.nb[0]) % L.nb[1];
+    const int bz = block / (L.nb[0] * L.nb[1]);
+    const int64_t boff = (int64_t)block * L.bstride;
+
+    // ---- stage the lab cross as primitives
+    for (int i = threadIdx.x; i < SV; i += NT) {
+        int x, y, z;
+        decode_cross<T>(i, x, y, z);
+        const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
+        T u[5];
+        if ((unsigned)gx < (unsigned)N0 && (unsigned)gy < (unsigned)N1 &&
+            (unsigned)gz < (unsigned)N2) {
+            const int64_t o = boff + gx + (int64_t)N0 * (gy + (int64_t)N1 * gz);
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                u[c] = p.U[c][o];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                if (!lab_value<T>(p.U[c], L, p.bc[c], block, bx, by, bz, gx, gy, gz, true, u[c]))
+                    u[c] = T(0);
+            }
+        }
+        T w[5];
+        to_primitive<T>(u[0], u[1], u[2], u[3], u[4], p.gm1, w);
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            W[c * SV + i] = w[c];
+    }
+    __syncthreads();
+
+    T acc[CPT][5];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k)
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            acc[k][c] = T(0);
+
+    sweep<T, 0>(W, F, acc, p.gamma, p.igm1, p.ih[0]);
+    sweep<T, 1>(W, F, acc, p.gamma, p.igm1, p.ih[1]);
+    sweep<T, 2>(W, F, acc, p.gamma, p.igm1, p.ih[2]);
+
+    // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows
+    double sums[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int cidx = threadIdx.x + k * NT;
+        if (cidx < NCELL) {
+            const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
+            const int64_t o = boff + (x0 + x) + (int64_t)N0 * ((y0 + y) + (int64_t)N1 * (z0 + z));
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                const T rhs = -acc[k][c];
+                T v;
+                if (p.stage == 0) {
+                    v = rhs;
+                } else {
+                    const T us = p.U[c][o];
+                    const T tt = dfma(p.dt, rhs, us);
+                    if (p.stage == 1) {
+                        v = tt;
+                    } else if (p.stage == 2) {
+                        v = dfma(T(0.75), p.Un[c][o], T(0.25) * tt);
+                    } else {
+                        v = dfma(T(1.0 / 3.0), p.Un[c][o], T(2.0 / 3.0) * tt);
+                    }
+                }
+                p.out[c][o] = v;
+                sums[c] += (double)v;
+            }
+        }
+    }
+    if (p.partials) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            double s = sums[c];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+                s += __shfl_down_sync(0xffffffffu, s, off);
+            if (lane == 0)
+                red[warp][c] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x < 5) {
+            double s = 0;
+            for (int w = 0; w < NT / 32; ++w)
+                s += red[w][threadIdx.x];
+            p.partials[(int64_t)blockIdx.x * 5 + threadIdx.x] = s;
+        }
+    }
+}
+
+// Fixed-order reduction of per-CTA partials: out[c] = sum_i partials[i][c].
+__global__ void __launch_bounds__(256) reduce_partials(const double *partials, int n, double *out)
+{
+    __shared__ double sh[256];
+    for (int c = 0; c < 5; ++c) {
+        double s = 0;
+        for (int i = threadIdx.x; i < n; i += 256)
+            s += partials[(int64_t)i * 5 + c];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w)
+                sh[threadIdx.x] += sh[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            out[c] = sh[0];
+        __syncthreads();
+    }
+}
+
+// Max over cells of |u_d| + c for each direction (for the CFL time step).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    max_speed_kernel(const T *r, const T *m0, const T *m1, const T *m2, const T *E, int64_t nb,
+                     int64_t cells, int64_t bstride, T gamma, T gm1, unsigned long long *out)
+{
+    double mx[3] = {0, 0, 0};
+    const int64_t total = nb * cells;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i / cells, c = i - b * cells;
+        const int64_t o = b * bstride + c;
+        T w[5];
+        to_primitive<T>(r[o], m0[o], m1[o], m2[o], E[o], gm1, w);
+        const double cs = sqrt((double)gamma * (double)w[4] / (double)w[0]);
+        for (int d = 0; d < 3; ++d)
+            mx[d] = fmax(mx[d], fabs((double)w[1 + d]) + cs);
+    }
+    for (int d = 0; d < 3; ++d) {
+        double v = mx[d];
+        for (int off = 16; off > 0; off >>= 1)
+            v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+        if ((threadIdx.x & 31) == 0)
+            atomicMax(out + d, (unsigned long long)__double_as_longlong(v)); // v >= 0: order-preserving
+    }
+}
+
+} // namespace euler
+
+using namespace euler;
+
+static cn_status check_euler(const cn_grid *g, int comp0)
+{
+    if (!g) return fail(CN_ERR_INVALID_ARGUMENT, "grid is NULL");
+    if (comp0 < 0 || comp0 + 5 > g->ncomp)
+        return fail(CN_ERR_INVALID_ARGUMENT, "Euler state needs 5 components");
+    if (g->dtype != CN_FLOAT64 && g->dtype != CN_FLOAT32)
+        return fail(CN_ERR_UNSUPPORTED, "Euler kernels need FLOAT32 or FLOAT64 grids");
+    for (int d = 0; d < 3; ++d)
+        if (g->n[d] % TB != 0 || g->n[d] < G)
+            return fail(CN_ERR_UNSUPPORTED, "Euler kernels need block cells divisible by 8");
+    return CN_OK;
+}
+
+static bool same_shape(const cn_grid *a, const cn_grid *b)
+{
+    return a->nblocks == b->nblocks && a->n[0] == b->n[0] && a->n[1] == b->n[1] &&
+           a->n[2] == b->n[2] && a->dtype == b->dtype && a->block_stride == b->block_stride;
+}
+
+template <typename T>
+static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, int cn_,
+                              cn_grid *out, int co, int stage, double dt, double gamma,
+                              double *partials, cudaStream_t st)
+{
+    cn_stencil s = {{-G, -G, -G}, {G + 1, G + 1, G + 1}, 0};
+    cn_status r = check_lab(Us, &s);
+    if (r != CN_OK) return r;
+    r = sync_bc(bcsrc, st);
+    if (r != CN_OK) return r;
+    StageParams<T> p = {};
+    p.L = make_geom(Us, &s);
+    for (int c = 0; c < 5; ++c) {
+        p.U[c] = reinterpret_cast<const T *>(Us->d_data) + (size_t)(cs + c) * Us->comp_stride;
+        p.Un[c] = Un ? reinterpret_cast<const T *>(Un->d_data) + (size_t)(cn_ + c) * Un->comp_stride
+                     : nullptr;
+        p.out[c] = reinterpret_cast<T *>(out->d_data) + (size_t)(co + c) * out->comp_stride;
+        p.bc[c] = bc_view(bcsrc, cs + c);
+    }
+    for (int d = 0; d < 3; ++d) p.ih[d] = (T)(1.0 / Us->h[d]);
+    p.dt = (T)dt;
+    p.gamma = (T)gamma;
+    p.gm1 = (T)(gamma - 1.0);
+    p.igm1 = (T)(1.0 / (gamma - 1.0));
+    p.stage = stage;
+    p.partials = partials;
+    p.err = Us->d_err;
+    const size_t smem = (size_t)(5 * SV + 5 * NFACE) * sizeof(T);
+    CN_CUDA_TRY(cudaFuncSetAttribute(stage_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t ctas = (int64_t)Us->nblocks * (Us->n[0] / TB) * (Us->n[1] / TB) * (Us->n[2] / TB);
+    stage_kernel<T><<<(unsigned)ctas, NT, smem, st>>>(p);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+static int64_t stage_ctas(const cn_grid *g)
+{
+    return (int64_t)g->nblocks * (g->n[0] / TB) * (g->n[1] / TB) * (g->n[2] / TB);
+}
+
+static cn_status run_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, int cn_, cn_grid *out,
+                           int co, int stage, double dt, double gamma, double *partials,
+                           cudaStream_t st)
+{
+    if (Us->dtype == CN_FLOAT64)
+        return launch_stage<double>(bcsrc, Us, cs, Un, cn_, out, co, stage, dt, gamma, partials, st);
+    return launch_stage<float>(bcsrc, Us, cs, Un, cn_, out, co, stage, dt, gamma, partials, st);
+}
+
+} // namespace cn
+
+using namespace cn;
+
+// Scratch of the conservation sums and the wave-speed maximum: per-CTA
+// partials and the 5 totals, one set per device, grown on demand.
+struct SumScratch {
+    double *partials = nullptr;
+    double *totals = nullptr;
+    int64_t cap = 0;
+};
+static SumScratch g_sum[64];
+static std::mutex g_sum_mu;
+
+static cn_status ensure_sum_scratch(int64_t nctas, SumScratch **out)
+{
+    int dev = 0;
+    CN_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(CN_ERR_UNSUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_sum_mu);
+    SumScratch &sc = g_sum[dev];
+    if (!sc.totals) CN_CUDA_TRY(cudaMalloc(&sc.totals, 5 * sizeof(double)));
+    if (nctas > sc.cap) {
+        if (sc.partials) cudaFree(sc.partials);
+        sc.partials = nullptr;
+        sc.cap = 0;
+        CN_CUDA_TRY(cudaMalloc(&sc.partials, (size_t)nctas * 5 * sizeof(double)));
+        sc.cap = nctas;
+    }
+    *out = &sc;
+    return CN_OK;
+}
+
+extern "C" {
+
+cn_status cn_euler_rhs(cn_grid *U, int comp0, double gamma, cn_grid *rhs, int rhs_comp0, void *stream)
+{
+    cn_status s = check_euler(U, comp0);
+    if (s != CN_OK) return s;
+    if (!rhs || !same_shape(U, rhs) || rhs_comp0 < 0 || rhs_comp0 + 5 > rhs->ncomp)
+        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
+    return run_stage(U, U, comp0, nullptr, 0, rhs, rhs_comp0, 0, 0.0, gamma, nullptr, as_stream(stream));
+}
+
+cn_status cn_euler_rk3_stage(cn_grid *bcsrc, cn_grid *Us, cn_grid *Un, cn_grid *out, int stage,
+                             double dt, double gamma, double *sums_out, void *stream)
+{
+    if (stage < 1 || stage > 3) return fail(CN_ERR_INVALID_ARGUMENT, "stage must be 1, 2 or 3");
+    cn_status s = check_euler(Us, 0);
+    if (s != CN_OK) return s;
+    if (!bcsrc || !out || !same_shape(Us, out) || !same_shape(Us, bcsrc) || bcsrc->ncomp < 5 ||
+        out->ncomp < 5 || (stage > 1 && (!Un || !same_shape(Us, Un) || Un->ncomp < 5)))
+        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
+    cudaStream_t st = as_stream(stream);
+    double *partials = nullptr;
+    SumScratch *sc = nullptr;
+    if (sums_out) {
+        s = ensure_sum_scratch(stage_ctas(Us), &sc);
+        if (s != CN_OK) return s;
+        partials = sc->partials;
+    }
+    s = run_stage(bcsrc, Us, 0, stage > 1 ? Un : nullptr, 0, out, 0, stage, dt, gamma, partials, st);
+    if (s != CN_OK) return s;
+    if (sums_out) {
+        const double vol = Us->h[0] * Us->h[1] * Us->h[2];
+        reduce_partials<<<1, 256, 0, st>>>(sc->partials, (int)stage_ctas(Us), sc->totals);
+        CN_CUDA_TRY(cudaGetLastError());
+        double t[5];
+        CN_CUDA_TRY(cudaMemcpyAsync(t, sc->totals, sizeof(t), cudaMemcpyDeviceToHost, st));
+        CN_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int c = 0; c < 5; ++c) sums_out[c] = t[c] * vol;
+    }
+    return CN_OK;
+}
+
+cn_status cn_euler_rk3_step(cn_grid *U, cn_grid *work1, cn_grid *work2, double dt, double gamma,
+                            double *sums_out, void *stream)
+{
+    cn_status s;
+    if ((s = cn_euler_rk3_stage(U, U, nullptr, work1, 1, dt, gamma, nullptr, stream)) != CN_OK) return s;
+    if ((s = cn_euler_rk3_stage(U, work1, U, work2, 2, dt, gamma, nullptr, stream)) != CN_OK) return s;
+    // stage 3 writes U^{n+1} over U^n: each cell reads its own U^n before writing
+    return cn_euler_rk3_stage(U, work2, U, U, 3, dt, gamma, sums_out, stream);
+}
+
+cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stream)
+{
+    cn_status s = check_euler(U, 0);
+    if (s != CN_OK) return s;
+    if (!out) return fail(CN_ERR_INVALID_ARGUMENT, "out is NULL");
+    cudaStream_t st = as_stream(stream);
+    SumScratch *sc = nullptr;
+    s = ensure_sum_scratch(1, &sc);
+    if (s != CN_OK) return s;
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(sc->totals);
+    CN_CUDA_TRY(cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), st));
+    const int64_t cells = (int64_t)U->n[0] * U->n[1] * U->n[2];
+    if (U->dtype == CN_FLOAT64) {
+        const double *b = reinterpret_cast<const double *>(U->d_data);
+        max_speed_kernel<double><<<148 * 8, 256, 0, st>>>(b, b + U->comp_stride, b + 2 * U->comp_stride,
+                                                          b + 3 * U->comp_stride, b + 4 * U->comp_stride,
+                                                          U->nblocks, cells, U->block_stride, gamma,
+                                                          gamma - 1.0, d);
+    } else {
+        const float *b = reinterpret_cast<const float *>(U->d_data);
+        max_speed_kernel<float><<<148 * 8, 256, 0, st>>>(b, b + U->comp_stride, b + 2 * U->comp_stride,
+                                                         b + 3 * U->comp_stride, b + 4 * U->comp_stride,
+                                                         U->nblocks, cells, U->block_stride, (float)gamma,
+                                                         (float)(gamma - 1.0), d);
+    }
+    CN_CUDA_TRY(cudaGetLastError());
+    unsigned long long h[3];
+    CN_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CN_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int k = 0; k < 3; ++k) {
+        double v;
+        memcpy(&v, &h[k], sizeof(v));
+        out[k] = v;
+    }
+    return CN_OK;
+}
+
+} // extern "C"

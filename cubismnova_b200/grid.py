@@ -231,11 +231,13 @@ class Cartesian:
     # -- boundary conditions
     def push_boundary_bc(self, bc_factory, dir, side, comp=0):
         """Push ``bc_factory(dir, side)`` onto every block touching face (dir, side)."""
-        for f in self:
-            fld = f if self.ncomp == 1 else f[comp]
-            bi = fld.getState().block_index
-            if (side == 0 and bi[dir] == 0) or (side == 1 and bi[dir] == self._nb[dir] - 1):
-                fld.getBC().push_back(bc_factory(dir, side))
+        bc = bc_factory(dir, side)
+        _lib.check(_lib.lib().cn_bc_push_boundary(self._h, comp, dir, side, bc.kind, C.c_double(bc.value)))
+        nb = self._nb
+        for flat in range(self.size()):
+            bi = (flat % nb[0], (flat // nb[0]) % nb[1], flat // (nb[0] * nb[1]))
+            if (side == 0 and bi[dir] == 0) or (side == 1 and bi[dir] == nb[dir] - 1):
+                self._bcs[comp].setdefault(flat, []).append(bc)
 
     def sync_bcs(self, stream=None):
         _lib.check(_lib.lib().cn_bc_sync(self._h, _stream_handle(stream)))

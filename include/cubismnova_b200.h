@@ -170,6 +170,30 @@ cn_status cn_ddx_async(cn_dtype dtype, int Nx, int Ny, int Nz, const void *src, 
                        int xy_pitch_src, void *dst, int x_pitch_dst, int xy_pitch_dst,
                        double factor, void *stream);
 
+/* ------------------------------------------------- compressible Euler */
+/* The reference promises WENO reconstruction operators (README.rst:28-31)
+ * without code; these entry points implement the published method on the
+ * lab of stencil (-3,4) non-tensorial, per-component BC vectors applied.
+ * State: 5 components (rho, rho*u, rho*v, rho*w, E) of one grid, gamma-law
+ * gas; WENO5-JS (eps 1e-6, linear weights 1/10, 6/10, 3/10) on primitive
+ * variables, Rusanov flux, RHS = -sum_d (F_{i+1/2} - F_{i-1/2}) / h_d.
+ * Block cells must be multiples of 8; FLOAT64 or FLOAT32 grids. */
+cn_status cn_euler_rhs(cn_grid *U, int comp0, double gamma, cn_grid *rhs, int rhs_comp0,
+                       void *stream);
+/* One SSP-RK3 stage (Shu & Osher), BCs taken from bcsrc's BC vectors:
+ *   stage 1: out = Us + dt L(Us)
+ *   stage 2: out = 3/4 Un + 1/4 (Us + dt L(Us))
+ *   stage 3: out = 1/3 Un + 2/3 (Us + dt L(Us))    (out may alias Un)
+ * If sums_out is not NULL the FP64 sums of the 5 outputs times the cell
+ * volume are returned (the call then waits for the stream). */
+cn_status cn_euler_rk3_stage(cn_grid *bcsrc, cn_grid *Us, cn_grid *Un, cn_grid *out, int stage,
+                             double dt, double gamma, double *sums_out, void *stream);
+/* U <- U^{n+1}: three stages through work1, work2 (same shape as U). */
+cn_status cn_euler_rk3_step(cn_grid *U, cn_grid *work1, cn_grid *work2, double dt, double gamma,
+                            double *sums_out, void *stream);
+/* max over cells of |u_d| + c per direction (waits for the stream). */
+cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -186,3 +186,36 @@ def ref_c1_sweep(comp, nb, n, ih2, ih, threads=0, nblocks=0, reps=1,
         C.c_int(threads if threads > 0 else (os.cpu_count() or 1)),
         C.c_int(nblocks), C.c_int(reps))
     return t, lap, grad
+
+
+def euler_stage(Us, Un, nb, n, bclists, stage, dt, gamma, h, threads=0):
+    """Euler RHS (stage 0) or SSP-RK3 stage on (5, comp_stride) arrays.
+    bclists: list of 5 dicts block -> [(dir, side, kind, value)]."""
+    Us = np.ascontiguousarray(Us)
+    dt_ = Us.dtype
+    sfx = {np.dtype(np.float64): "f64", np.dtype(np.float32): "f32"}[dt_]
+    stride = block_stride(n, dt_)
+    g = make_geom(nb, n, (3, 3, 3), (3, 3, 3), False, stride)
+    nblocks = int(np.prod(nb))
+    offs, ents = [], []
+    for c in range(5):
+        o, e = bc_arrays(nblocks, (bclists[c] if bclists else {}))
+        offs.append(o)
+        ents.append(e)
+    off_ptrs = (C.c_void_p * 5)(*[o.ctypes.data for o in offs])
+    ent_ptrs = (C.c_void_p * 5)(*[C.addressof(e) for e in ents])
+    out = np.array(Un, copy=True) if (Un is not None and stage == 3) else np.zeros_like(Us)
+    Unp = _ptr(np.ascontiguousarray(Un)) if Un is not None else None
+    f = getattr(lib(), "or_euler_stage_" + sfx)
+    rc = f(C.byref(g), _ptr(Us), Unp, _ptr(out), C.c_int64(Us.shape[-1]), off_ptrs, ent_ptrs,
+           C.c_int(stage), C.c_double(dt), C.c_double(gamma), (C.c_double * 3)(*h),
+           C.c_int(threads if threads > 0 else (os.cpu_count() or 1)))
+    if rc:
+        raise ValueError("or_euler_stage failed")
+    return out
+
+
+def euler_rk3_step(U, nb, n, bclists, dt, gamma, h, threads=0):
+    U1 = euler_stage(U, None, nb, n, bclists, 1, dt, gamma, h, threads)
+    U2 = euler_stage(U1, U, nb, n, bclists, 2, dt, gamma, h, threads)
+    return euler_stage(U2, U, nb, n, bclists, 3, dt, gamma, h, threads)

@@ -81,6 +81,18 @@ void or_ddx_f64(int nx, int ny, int nz, const double *src, int xps, int xyps,
 void or_ddx_f32(int nx, int ny, int nz, const float *src, int xps, int xyps,
                 float *dst, int xpd, int xypd, float factor);
 
+/* Compressible Euler (5 conserved components cstride elements apart, grid
+ * layout), lab stencil (-3,4) non-tensorial with per-component BC vectors
+ * bc_off[c]/bcs[c]: stage 0 writes the RHS L(Us) to out; stages 1..3 the
+ * SSP-RK3 stages  out = Us + dt L | 3/4 Un + 1/4 (Us + dt L) |
+ * 1/3 Un + 2/3 (Us + dt L).  out may alias Un but not Us. */
+int or_euler_stage_f64(const or_geom *g, const double *Us, const double *Un, double *out,
+                       int64_t cstride, const int32_t *const *bc_off, const or_bc *const *bcs,
+                       int stage, double dt, double gamma, const double h[3], int nthreads);
+int or_euler_stage_f32(const or_geom *g, const float *Us, const float *Un, float *out,
+                       int64_t cstride, const int32_t *const *bc_off, const or_bc *const *bcs,
+                       int stage, double dt, double gamma, const double h[3], int nthreads);
+
 #ifdef __cplusplus
 }
 #endif
