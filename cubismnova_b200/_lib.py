@@ -70,6 +70,7 @@ _SIGS = {
     "cn_ddx_f64": (None, [_I, _I, _I, _P, _I, _I, _P, _I, _I, _D]),
     "cn_ddx_f32": (None, [_I, _I, _I, _P, _I, _I, _P, _I, _I, C.c_float]),
     "cn_ddx_async": (_I, [_I, _I, _I, _I, _P, _I, _I, _P, _I, _I, _D, _P]),
+    "cn_calib_fma_peak": (_I, [_I, C.POINTER(C.c_double)]),
 }
 
 
@@ -131,3 +132,10 @@ def stencil_struct(begin, end, tensorial) -> CnStencil:
         s.end[d] = int(end[d])
     s.tensorial = 1 if tensorial else 0
     return s
+
+
+def fma_peak_tflops(dtype: int) -> float:
+    """Measured FMA throughput of the current device (CN_FLOAT64 / CN_FLOAT32)."""
+    v = C.c_double()
+    check(lib().cn_calib_fma_peak(dtype, C.byref(v)))
+    return v.value

@@ -133,17 +133,17 @@ inline LabGeom make_geom(const cn_grid *g, const cn_stencil *s)
 // (Block/FieldLabLoader.h:196-205).  Returns false if the reference leaves
 // the cell undefined.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ int pick3(int d, int a, int b, int c) { return d == 0 ? a : (d == 1 ? b : c); }
+
 template <typename T>
 __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabGeom &L,
-                                          const BcView &bc, int block, int bx, int by,
-                                          int bz, int q0, int q1, int q2, bool apply_bc,
-                                          T &out)
+                                          const BcView &bc, int block, int bx, int by, int bz,
+                                          int q0, int q1, int q2, bool apply_bc, T &out)
 {
-    int q[3] = {q0, q1, q2};
-    T signs[3];
-    int nsign = 0;
     // skip flags hold even when the BCs themselves are not applied
     const uint8_t mode = bc.mode[block];
+    T s0 = T(1), s1 = T(1), s2 = T(1); // symmetry signs of the chain, outermost first
+    int nsign = 0;
     if (apply_bc && (mode & kHasBc)) {
         const int k0 = bc.off[block];
         int kmax = bc.off[block + 1] - k0;
@@ -153,22 +153,20 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
             int32_t meta = 0;
             for (int k = kmax - 1; k >= 0; --k) {
                 const int32_t m = e[k].meta;
-                const int kind = bc_kind(m);
-                if (kind == CN_BC_BASE)
+                if (bc_kind(m) == CN_BC_BASE)
                     continue;
                 const int d = bc_dir(m);
-                if (!L.valid_bc[d])
+                if (!pick3(d, L.valid_bc[0], L.valid_bc[1], L.valid_bc[2]))
                     continue;
-                const bool in_slab = bc_side(m) == 0 ? (q[d] < 0) : (q[d] >= L.n[d]);
-                if (!in_slab)
+                const int qd = pick3(d, q0, q1, q2);
+                const int nd = pick3(d, L.n[0], L.n[1], L.n[2]);
+                if (!(bc_side(m) == 0 ? (qd < 0) : (qd >= nd)))
                     continue;
                 if (!L.tensorial) {
-                    bool inner_other = true;
-#pragma unroll
-                    for (int o = 0; o < 3; ++o)
-                        if (o != d && (q[o] < 0 || q[o] >= L.n[o]))
-                            inner_other = false;
-                    if (!inner_other)
+                    const bool in0 = d == 0 || ((unsigned)q0 < (unsigned)L.n[0]);
+                    const bool in1 = d == 1 || ((unsigned)q1 < (unsigned)L.n[1]);
+                    const bool in2 = d == 2 || ((unsigned)q2 < (unsigned)L.n[2]);
+                    if (!(in0 && in1 && in2))
                         continue;
                 }
                 found = k;
@@ -179,48 +177,59 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
                 break;
             const int d = bc_dir(meta);
             const int kind = bc_kind(meta);
+            const int nd = pick3(d, L.n[0], L.n[1], L.n[2]);
             if (kind == CN_BC_DIRICHLET) {
                 T v = static_cast<T>(e[found].value);
-                for (int i = nsign - 1; i >= 0; --i)
-                    v = signs[i] * v;
+                // apply the chain's signs innermost first
+                if (nsign > 2) v = s2 * v;
+                if (nsign > 1) v = s1 * v;
+                if (nsign > 0) v = s0 * v;
                 out = v;
                 return true;
-            } else if (kind == CN_BC_ABSORBING) {
-                q[d] = bc_side(meta) == 0 ? 0 : L.n[d] - 1;
-            } else { // symmetry
-                q[d] = (bc_side(meta) == 0 ? -1 : 2 * L.n[d] - 1) - q[d];
-                if (nsign < 3)
-                    signs[nsign++] = static_cast<T>(e[found].value);
             }
+            int qd = pick3(d, q0, q1, q2);
+            if (kind == CN_BC_ABSORBING) {
+                qd = bc_side(meta) == 0 ? 0 : nd - 1;
+            } else { // symmetry: r = roffset - q
+                qd = (bc_side(meta) == 0 ? -1 : 2 * nd - 1) - qd;
+                const T sg = static_cast<T>(e[found].value);
+                if (nsign == 0) s0 = sg;
+                else if (nsign == 1) s1 = sg;
+                else s2 = sg;
+                ++nsign;
+            }
+            if (d == 0) q0 = qd;
+            else if (d == 1) q1 = qd;
+            else q2 = qd;
             kmax = found;
         }
     }
     // loaded value
-    const int r0 = q[0] < 0 ? -1 : (q[0] >= L.n[0] ? 1 : 0);
-    const int r1 = q[1] < 0 ? -1 : (q[1] >= L.n[1] ? 1 : 0);
-    const int r2 = q[2] < 0 ? -1 : (q[2] >= L.n[2] ? 1 : 0);
+    const int r0 = q0 < 0 ? -1 : (q0 >= L.n[0] ? 1 : 0);
+    const int r1 = q1 < 0 ? -1 : (q1 >= L.n[1] ? 1 : 0);
+    const int r2 = q2 < 0 ? -1 : (q2 >= L.n[2] ? 1 : 0);
     int src_block = block;
     if (r0 | r1 | r2) {
         if (!L.tensorial && (r0 != 0) + (r1 != 0) + (r2 != 0) > 1)
             return false;
         // skipped neighbour: Block/FieldLab.h:207-214 + FieldLabLoader.h:197-201
-        const int s0 = mode & 3, s1 = (mode >> 2) & 3, s2 = (mode >> 4) & 3;
-        if ((r0 != 0 && s0 == (r0 < 0 ? 1 : 2)) || (r1 != 0 && s1 == (r1 < 0 ? 1 : 2)) ||
-            (r2 != 0 && s2 == (r2 < 0 ? 1 : 2)))
+        const int c0 = mode & 3, c1 = (mode >> 2) & 3, c2 = (mode >> 4) & 3;
+        if ((r0 != 0 && c0 == (r0 < 0 ? 1 : 2)) || (r1 != 0 && c1 == (r1 < 0 ? 1 : 2)) ||
+            (r2 != 0 && c2 == (r2 < 0 ? 1 : 2)))
             return false;
         int nbx = bx + r0, nby = by + r1, nbz = bz + r2;
         nbx = nbx < 0 ? nbx + L.nb[0] : (nbx >= L.nb[0] ? nbx - L.nb[0] : nbx);
         nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
         nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
         src_block = nbx + L.nb[0] * (nby + L.nb[1] * nbz);
-        q[0] -= r0 * L.n[0];
-        q[1] -= r1 * L.n[1];
-        q[2] -= r2 * L.n[2];
+        q0 -= r0 * L.n[0];
+        q1 -= r1 * L.n[1];
+        q2 -= r2 * L.n[2];
     }
-    T v = comp[(int64_t)src_block * L.bstride + q[0] +
-               (int64_t)L.n[0] * (q[1] + (int64_t)L.n[1] * q[2])];
-    for (int i = nsign - 1; i >= 0; --i)
-        v = signs[i] * v;
+    T v = comp[(int64_t)src_block * L.bstride + q0 + (int64_t)L.n[0] * (q1 + (int64_t)L.n[1] * q2)];
+    if (nsign > 2) v = s2 * v;
+    if (nsign > 1) v = s1 * v;
+    if (nsign > 0) v = s0 * v;
     out = v;
     return true;
 }

@@ -194,6 +194,44 @@ cn_status cn_euler_rk3_step(cn_grid *U, cn_grid *work1, cn_grid *work2, double d
 /* max over cells of |u_d| + c per direction (waits for the stream). */
 cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stream);
 
+/* ------------------------------------------------- pointwise field ops */
+/* The optimised hooks that Block/FieldOperator.h:149-227 declares (under
+ * CUBISM_OPTIMIZED_FIELD_OP) and never defines, with the reference's exact
+ * names and signatures:  dst[i] = src0[i] OP src1[i]  (...2_T),
+ * dst[i] = src0[i] OP src1  (...1_T),  fieldRcp: dst[i] = src1 * (1/src0[i])
+ * (FieldOperator.h:16-30).  Device or managed pointers run in place, host
+ * pointers are staged through device memory; each call returns once dst
+ * holds the result. */
+void fieldAdd2_double(const double *src0, const double *src1, double *dst, const size_t n);
+void fieldSub2_double(const double *src0, const double *src1, double *dst, const size_t n);
+void fieldMul2_double(const double *src0, const double *src1, double *dst, const size_t n);
+void fieldDiv2_double(const double *src0, const double *src1, double *dst, const size_t n);
+void fieldAdd2_float(const float *src0, const float *src1, float *dst, const size_t n);
+void fieldSub2_float(const float *src0, const float *src1, float *dst, const size_t n);
+void fieldMul2_float(const float *src0, const float *src1, float *dst, const size_t n);
+void fieldDiv2_float(const float *src0, const float *src1, float *dst, const size_t n);
+void fieldAdd1_double(const double *src0, const double src1, double *dst, const size_t n);
+void fieldSub1_double(const double *src0, const double src1, double *dst, const size_t n);
+void fieldMul1_double(const double *src0, const double src1, double *dst, const size_t n);
+void fieldDiv1_double(const double *src0, const double src1, double *dst, const size_t n);
+void fieldAdd1_float(const float *src0, const float src1, float *dst, const size_t n);
+void fieldSub1_float(const float *src0, const float src1, float *dst, const size_t n);
+void fieldMul1_float(const float *src0, const float src1, float *dst, const size_t n);
+void fieldDiv1_float(const float *src0, const float src1, float *dst, const size_t n);
+void fieldRcp_double(const double *src0, const double src1, double *dst, const size_t n);
+void fieldRcp_float(const float *src0, const float src1, float *dst, const size_t n);
+/* Stream-ordered form on device pointers: op 0..4 = add, sub, mul, div, rcp;
+ * src1 == NULL selects the scalar form (rcp always uses the scalar). */
+cn_status cn_field_op(int op, cn_dtype dtype, const void *src0, const void *src1, double scalar,
+                      void *dst, size_t n, void *stream);
+
+/* --------------------------------------------------------- calibration */
+/* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the current device
+ * for FLOAT64 or FLOAT32: the roofline denominator of the ALU-bound Euler
+ * kernels.  No reference counterpart (the reference has no device code).
+ * Synchronous; takes a few milliseconds. */
+cn_status cn_calib_fma_peak(cn_dtype dtype, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

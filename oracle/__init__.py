@@ -219,3 +219,29 @@ def euler_rk3_step(U, nb, n, bclists, dt, gamma, h, threads=0):
     U1 = euler_stage(U, None, nb, n, bclists, 1, dt, gamma, h, threads)
     U2 = euler_stage(U1, U, nb, n, bclists, 2, dt, gamma, h, threads)
     return euler_stage(U2, U, nb, n, bclists, 3, dt, gamma, h, threads)
+
+
+def ref_euler_stage(Us, Un, nb, n, bclists, stage, dt, gamma, h, threads=0, blocks=None, reps=1):
+    """The Euler stage with labs loaded by the reference FieldLab (oracle/_ref).
+    Returns (seconds for the sampled blocks, out)."""
+    Us = np.ascontiguousarray(Us, dtype=np.float64)
+    stride = block_stride(n, np.float64)
+    nblocks = int(np.prod(nb))
+    offs, ents = [], []
+    for c in range(5):
+        o, e = bc_arrays(nblocks, (bclists[c] if bclists else {}))
+        offs.append(o)
+        ents.append(e)
+    off_ptrs = (C.c_void_p * 5)(*[o.ctypes.data for o in offs])
+    ent_ptrs = (C.c_void_p * 5)(*[C.addressof(e) for e in ents])
+    out = np.array(Un, copy=True) if (Un is not None and stage == 3) else np.zeros_like(Us)
+    b0, cnt = (0, nblocks) if blocks is None else blocks
+    f = ref().ref_euler_stage_f64
+    f.restype = C.c_double
+    t = f((C.c_int * 3)(*nb), (C.c_int * 3)(*n), _ptr(Us),
+          _ptr(np.ascontiguousarray(Un)) if Un is not None else None, _ptr(out),
+          C.c_int64(stride), C.c_int64(Us.shape[-1]), off_ptrs, ent_ptrs, C.c_int(stage),
+          C.c_double(dt), C.c_double(gamma), (C.c_double * 3)(*h),
+          C.c_int(threads if threads > 0 else (os.cpu_count() or 1)), C.c_int(b0), C.c_int(cnt),
+          C.c_int(reps))
+    return t, out

@@ -23,82 +23,9 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define DEFINE_EULER(SUF, T, FMA, SQRT, FABS, FMAX)                            \
-    static T weno5_##SUF(T v0, T v1, T v2, T v3, T v4)                         \
-    {                                                                          \
-        const T c1312 = (T)(13.0 / 12.0), quarter = (T)0.25, eps = (T)1e-6;    \
-        const T d0 = (T)0.1, d1 = (T)0.6, d2 = (T)0.3, six = (T)6;             \
-        const T a0 = FMA((T)-2, v1, v0) + v2;                                  \
-        const T b0 = FMA((T)3, v2, FMA((T)-4, v1, v0));                        \
-        const T a1 = FMA((T)-2, v2, v1) + v3;                                  \
-        const T b1 = v1 - v3;                                                  \
-        const T a2 = FMA((T)-2, v3, v2) + v4;                                  \
-        const T b2 = FMA((T)3, v2, FMA((T)-4, v3, v4));                        \
-        const T s0 = eps + FMA(c1312 * a0, a0, quarter * (b0 * b0));           \
-        const T s1 = eps + FMA(c1312 * a1, a1, quarter * (b1 * b1));           \
-        const T s2 = eps + FMA(c1312 * a2, a2, quarter * (b2 * b2));           \
-        const T t0 = s0 * s0, t1 = s1 * s1, t2 = s2 * s2;                      \
-        const T w0 = d0 * (t1 * t2);                                           \
-        const T w1 = d1 * (t0 * t2);                                           \
-        const T w2 = d2 * (t0 * t1);                                           \
-        const T n0 = FMA((T)2, v0, FMA((T)-7, v1, (T)11 * v2));                \
-        const T n1 = FMA((T)5, v2, FMA((T)2, v3, -v1));                        \
-        const T n2 = FMA((T)2, v2, FMA((T)5, v3, -v4));                        \
-        const T num = FMA(w0, n0, FMA(w1, n1, w2 * n2));                       \
-        const T den = six * ((w0 + w1) + w2);                                  \
-        return num / den;                                                      \
-    }                                                                          \
-                                                                               \
-    static void rusanov_##SUF(const T *WL, const T *WR, int d, T gamma,        \
-                              T igm1, T *F)                                    \
-    {                                                                          \
-        const T half = (T)0.5;                                                 \
-        const T rl = WL[0], rr = WR[0];                                        \
-        const T unl = WL[1 + d], unr = WR[1 + d];                              \
-        const T pl = WL[4], pr = WR[4];                                        \
-        const T mul0 = rl * WL[1], mul1 = rl * WL[2], mul2 = rl * WL[3];       \
-        const T mur0 = rr * WR[1], mur1 = rr * WR[2], mur2 = rr * WR[3];       \
-        const T kel = FMA(WL[1], WL[1], FMA(WL[2], WL[2], WL[3] * WL[3]));     \
-        const T ker = FMA(WR[1], WR[1], FMA(WR[2], WR[2], WR[3] * WR[3]));     \
-        const T El = FMA(half * rl, kel, pl * igm1);                           \
-        const T Er = FMA(half * rr, ker, pr * igm1);                           \
-        const T cl = SQRT((gamma * pl) / rl);                                  \
-        const T cr = SQRT((gamma * pr) / rr);                                  \
-        const T a = FMAX(FABS(unl) + cl, FABS(unr) + cr);                      \
-        const T fl0 = rl * unl, fr0 = rr * unr;                                \
-        T fl1 = mul0 * unl, fr1 = mur0 * unr;                                  \
-        T fl2 = mul1 * unl, fr2 = mur1 * unr;                                  \
-        T fl3 = mul2 * unl, fr3 = mur2 * unr;                                  \
-        if (d == 0) {                                                          \
-            fl1 = fl1 + pl;                                                    \
-            fr1 = fr1 + pr;                                                    \
-        } else if (d == 1) {                                                   \
-            fl2 = fl2 + pl;                                                    \
-            fr2 = fr2 + pr;                                                    \
-        } else {                                                               \
-            fl3 = fl3 + pl;                                                    \
-            fr3 = fr3 + pr;                                                    \
-        }                                                                      \
-        const T fl4 = (El + pl) * unl, fr4 = (Er + pr) * unr;                  \
-        F[0] = half * FMA(-a, rr - rl, fl0 + fr0);                             \
-        F[1] = half * FMA(-a, mur0 - mul0, fl1 + fr1);                         \
-        F[2] = half * FMA(-a, mur1 - mul1, fl2 + fr2);                         \
-        F[3] = half * FMA(-a, mur2 - mul2, fl3 + fr3);                         \
-        F[4] = half * FMA(-a, Er - El, fl4 + fr4);                             \
-    }                                                                          \
-                                                                               \
-    static void prim_##SUF(T r, T m0, T m1, T m2, T E, T gm1, T *W)            \
-    {                                                                          \
-        const T inv = (T)1 / r;                                                \
-        const T u = m0 * inv, v = m1 * inv, w = m2 * inv;                      \
-        const T ke = (T)0.5 * FMA(m0, u, FMA(m1, v, m2 * w));                  \
-        W[0] = r;                                                              \
-        W[1] = u;                                                              \
-        W[2] = v;                                                              \
-        W[3] = w;                                                              \
-        W[4] = gm1 * (E - ke);                                                 \
-    }                                                                          \
-                                                                               \
+#include "cn_euler_math.h"
+
+#define DEFINE_EULER(SUF, T, FMA)                                             \
     /* One block: RHS (stage 0) or SSP-RK3 stage of all its cells.  Us, Un,    \
      * out are 5 component bases (comp_stride apart). */                       \
     static int block_##SUF(const or_geom *g, const T *Us, const T *Un, T *out,  \
@@ -236,5 +163,5 @@
         return err;                                                            \
     }
 
-DEFINE_EULER(f64, double, fma, sqrt, fabs, fmax)
-DEFINE_EULER(f32, float, fmaf, sqrtf, fabsf, fmaxf)
+DEFINE_EULER(f64, double, fma)
+DEFINE_EULER(f32, float, fmaf)

@@ -14,6 +14,7 @@
 #include "Cubism/Mesh/StructuredUniform.h"
 
 #include "cn_oracle.h"
+#include "cn_euler_math.h"
 
 #include <chrono>
 #include <cstdint>
@@ -168,6 +169,114 @@ void c1Blocks(typename RefGrid<T>::G &u, T *lap, T *grad, int64_t stride,
         }
     }
 }
+
+// Euler RHS / SSP-RK3 stage on labs loaded by the reference FieldLab (one lab
+// per component, stencil (-3,4) non-tensorial, per-component BC vectors), the
+// face loops of cn_euler.c.  Runs blocks [b0, b0+cnt) on nthreads threads.
+template <typename T>
+static double eulerStage(const int nb[3], const int n[3], const T *Us, const T *Un, T *out,
+                         int64_t stride, int64_t cstride, const int32_t *const *bc_off,
+                         const or_bc *const *bcs, int stage, double dt, double gamma,
+                         const double h[3], int nthreads, int b0, int cnt, int reps);
+
+template <>
+double eulerStage<double>(const int nb[3], const int n[3], const double *Us, const double *Un,
+                          double *out, int64_t stride, int64_t cstride,
+                          const int32_t *const *bc_off, const or_bc *const *bcs, int stage,
+                          double dt, double gamma, const double h[3], int nthreads, int b0,
+                          int cnt, int reps)
+{
+    using T = double;
+    using R = RefGrid<T>;
+    std::vector<std::unique_ptr<R>> g;
+    for (int c = 0; c < 5; ++c) {
+        g.emplace_back(new R(nb, n, Us + c * cstride, stride));
+        g.back()->attach(bc_off ? bc_off[c] : nullptr, bcs ? bcs[c] : nullptr);
+    }
+    const T ih[3] = {(T)(1.0 / h[0]), (T)(1.0 / h[1]), (T)(1.0 / h[2])};
+    const T gm1 = (T)(gamma - 1.0), igm1 = (T)(1.0 / (gamma - 1.0)), gam = (T)gamma, dtt = (T)dt;
+    const int N0 = n[0], N1 = n[1], N2 = n[2];
+    double best = 1e300;
+    for (int rep = 0; rep < (reps < 1 ? 1 : reps); ++rep) {
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel num_threads(nthreads)
+        {
+            typename R::Lab lab[5];
+            const typename R::S s(-3, 4, false);
+            for (int c = 0; c < 5; ++c) lab[c].allocate(s, (*g[0]->grid)[0].getIndexRange());
+            const int L0 = N0 + 6, L1 = N1 + 6, L2 = N2 + 6;
+            const size_t le = (size_t)L0 * L1 * L2;
+            std::vector<T> prim(5 * le), flux(5 * (size_t)(N0 + 1) * (N1 + 1) * (N2 + 1)),
+                acc(5 * (size_t)N0 * N1 * N2);
+#pragma omp for schedule(dynamic, 1)
+            for (int b = b0; b < b0 + cnt; ++b) {
+                for (int c = 0; c < 5; ++c) g[c]->grid->loadLab((*g[c]->grid)[(size_t)b], lab[c]);
+                for (int z = -3; z < N2 + 3; ++z)
+                    for (int y = -3; y < N1 + 3; ++y)
+                        for (int x = -3; x < N0 + 3; ++x) {
+                            const int nout = (x < 0 || x >= N0) + (y < 0 || y >= N1) + (z < 0 || z >= N2);
+                            if (nout > 1) continue; // corners of a non-tensorial lab
+                            T W[5];
+                            prim_f64(lab[0](x, y, z), lab[1](x, y, z), lab[2](x, y, z), lab[3](x, y, z),
+                                     lab[4](x, y, z), gm1, W);
+                            const size_t li = (x + 3) + (size_t)L0 * ((y + 3) + (size_t)L1 * (z + 3));
+                            for (int c = 0; c < 5; ++c) prim[c * le + li] = W[c];
+                        }
+                const size_t cells = (size_t)N0 * N1 * N2;
+                for (int d = 0; d < 3; ++d) {
+                    const int E0 = N0 + (d == 0), E1 = N1 + (d == 1), E2 = N2 + (d == 2);
+                    const size_t nf = (size_t)E0 * E1 * E2;
+                    const ptrdiff_t st = d == 0 ? 1 : (d == 1 ? L0 : (ptrdiff_t)L0 * L1);
+                    for (int z = 0; z < E2; ++z)
+                        for (int y = 0; y < E1; ++y)
+                            for (int x = 0; x < E0; ++x) {
+                                const ptrdiff_t li = (x + 3) + (ptrdiff_t)L0 * ((y + 3) + (ptrdiff_t)L1 * (z + 3));
+                                T WL[5], WR[5], F[5];
+                                for (int c = 0; c < 5; ++c) {
+                                    const T *P = prim.data() + c * le + li;
+                                    const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st];
+                                    const T v3 = P[0], v4 = P[st], v5 = P[2 * st];
+                                    WL[c] = weno5_f64(v0, v1, v2, v3, v4);
+                                    WR[c] = weno5_f64(v5, v4, v3, v2, v1);
+                                }
+                                rusanov_f64(WL, WR, d, gam, igm1, F);
+                                const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
+                                for (int c = 0; c < 5; ++c) flux[c * nf + fi] = F[c];
+                            }
+                    const size_t fst = d == 0 ? 1 : (d == 1 ? (size_t)E0 : (size_t)E0 * E1);
+                    for (int z = 0; z < N2; ++z)
+                        for (int y = 0; y < N1; ++y)
+                            for (int x = 0; x < N0; ++x) {
+                                const size_t ci = x + (size_t)N0 * (y + (size_t)N1 * z);
+                                const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
+                                for (int c = 0; c < 5; ++c) {
+                                    const T df = flux[c * nf + fi + fst] - flux[c * nf + fi];
+                                    acc[c * cells + ci] = d == 0 ? df * ih[d] : std::fma(df, ih[d], acc[c * cells + ci]);
+                                }
+                            }
+                }
+                const int64_t boff = (int64_t)b * stride;
+                for (size_t ci = 0; ci < cells; ++ci)
+                    for (int c = 0; c < 5; ++c) {
+                        const T rhs = -acc[c * cells + ci];
+                        const int64_t o = c * cstride + boff + (int64_t)ci;
+                        T v;
+                        if (stage == 0) v = rhs;
+                        else {
+                            const T tt = std::fma(dtt, rhs, Us[o]);
+                            if (stage == 1) v = tt;
+                            else if (stage == 2) v = std::fma((T)0.75, Un[o], (T)0.25 * tt);
+                            else v = std::fma((T)(1.0 / 3.0), Un[o], (T)(2.0 / 3.0) * tt);
+                        }
+                        out[o] = v;
+                    }
+            }
+        }
+        const double dts = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        best = dts < best ? dts : best;
+    }
+    return best;
+}
 } // namespace
 
 extern "C" {
@@ -209,6 +318,18 @@ double ref_c1_sweep_f64(const int nb[3], const int n[3], const double *comp,
         best = dt < best ? dt : best;
     }
     return best;
+}
+
+// Euler RHS (stage 0) / SSP-RK3 stage (1..3) of blocks [b0, b0+cnt) on the
+// reference FieldLab; returns the best seconds over reps.
+double ref_euler_stage_f64(const int nb[3], const int n[3], const double *Us, const double *Un,
+                           double *out, int64_t stride, int64_t cstride,
+                           const int32_t *const *bc_off, const or_bc *const *bcs, int stage,
+                           double dt, double gamma, const double h[3], int nthreads, int b0,
+                           int cnt, int reps)
+{
+    return eulerStage<double>(nb, n, Us, Un, out, stride, cstride, bc_off, bcs, stage, dt, gamma, h,
+                              nthreads, b0, cnt, reps);
 }
 
 int ref_max_threads(void)

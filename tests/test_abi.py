@@ -15,7 +15,7 @@ def declared_functions():
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        names += re.findall(r"\b(cn_[a-z0-9_]+)\s*\(", src)
+        names += re.findall(r"\b(cn_[a-z0-9_]+|field[A-Za-z0-9_]+)\s*\(", src)
     return sorted(set(names))
 
 

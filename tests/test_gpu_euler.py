@@ -86,10 +86,14 @@ def test_fp32_vs_fp64_error(cn):
         cn.euler.rk3_step(U32, w[2], w[3], dt)
     torch.cuda.synchronize()
     a, b = _host(U64), _host(U32).astype(np.float64)
+    # errors relative to the magnitude of the state (rho ~ 1, E ~ 2.5): FP32
+    # round-off accumulated over 5 RK3 steps
+    scale = max(np.max(np.abs(a[0])), np.max(np.abs(a[4])))
     for c in range(5):
-        scale = np.max(np.abs(a[c]))
+        l1 = np.mean(np.abs(a[c] - b[c])) / scale
         linf = np.max(np.abs(a[c] - b[c])) / scale
-        assert linf < 1e-5, (c, linf)
+        print(f"var {c}: L1 {l1:.3e}  Linf {linf:.3e} (relative to max |state|)")
+        assert linf < 1e-6 and l1 < 1e-7, (c, l1, linf)
 
 
 def test_uniform_state_full_size_is_steady(cn):

@@ -153,3 +153,59 @@ def test_cartesian_exact_function(oracle_lib):
         bi = (b % nb[0], (b // nb[0]) % nb[1], b // (nb[0] * nb[1]))
         lab, _ = oracle_lib.lab_fill(comp, nb, n, (2,) * 3, (2,) * 3, True, {}, b)
         LC.check_exact_function(LC.Lab(lab, n, (2,) * 3, (2,) * 3), bi, h, f, 8 * eps)
+
+
+def _euler_host_state(nb, n, seed=3):
+    import oracle as O
+    stride = O.block_stride(n, np.float64)
+    nbk = int(np.prod(nb))
+    rng = np.random.default_rng(seed)
+    U = np.zeros((5, nbk * stride))
+    rho = 1.0 + 0.3 * rng.random(nbk * stride)
+    vel = (rng.random((3, nbk * stride)) * 2 - 1) * 0.1
+    U[0] = rho
+    U[1:4] = rho * vel
+    U[4] = 2.5 + 0.5 * rho * (vel ** 2).sum(0)
+    return U
+
+
+def _c2_bclists(nb):
+    ff = (1.0, 0.0, 0.0, 0.0, 2.5)
+    out = []
+    for c in range(5):
+        d = {}
+        for b in range(int(np.prod(nb))):
+            bi = (b % nb[0], (b // nb[0]) % nb[1], b // (nb[0] * nb[1]))
+            lst = []
+            if bi[1] == 0: lst.append((1, 0, 2, 0.0))
+            if bi[1] == nb[1] - 1: lst.append((1, 1, 2, 0.0))
+            if bi[2] == 0: lst.append((2, 0, 1, ff[c]))
+            if bi[2] == nb[2] - 1: lst.append((2, 1, 1, ff[c]))
+            if lst: d[b] = lst
+        out.append(d)
+    return out
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("stage", [0, 1, 2, 3])
+def test_euler_oracle_lab_matches_reference_fieldlab(oracle_lib, stage):
+    """The Euler oracle on its restated lab equals the same math on labs
+    loaded by the reference's own FieldLab + BCs (mixed C2-style BCs)."""
+    nb, n = (2, 3, 2), (8, 8, 8)
+    U = _euler_host_state(nb, n)
+    Un = _euler_host_state(nb, n, seed=4)
+    bcl = _c2_bclists(nb)
+    h = (1 / 16, 1 / 24, 1 / 16)
+    want = oracle_lib.euler_stage(U, Un if stage > 1 else None, nb, n, bcl, stage, 1e-3, 1.4, h)
+    _, got = oracle_lib.ref_euler_stage(U, Un if stage > 1 else None, nb, n, bcl, stage, 1e-3, 1.4, h)
+    assert np.array_equal(got, want)
+
+
+def test_euler_oracle_constant_state_is_steady(oracle_lib):
+    nb, n = (2, 2, 2), (8, 8, 8)
+    import oracle as O
+    stride = O.block_stride(n, np.float64)
+    U = np.zeros((5, 8 * stride))
+    U[0], U[4] = 1.0, 2.5
+    out = oracle_lib.euler_stage(U, None, nb, n, _c2_bclists(nb), 0, 0.0, 1.4, (1 / 16,) * 3)
+    assert not out.any()
