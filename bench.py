@@ -404,7 +404,11 @@ def run_ours(args, world, rank, local, pg):
 
     from cubismnova_b200 import _lib
     torch.cuda.set_device(local)
-    W = WORKLOADS[args.workload]()
+    cls = WORKLOADS[args.workload]
+    if args.blocks:
+        cls = type(cls.__name__, (cls,), {"nb": tuple(args.blocks),
+                                          "desc": cls.desc + f" [reduced: {tuple(args.blocks)} blocks]"})
+    W = cls()
     stream = torch.cuda.Stream()
     peaks = measured_peaks()
     L = W.launches_per_step
@@ -516,6 +520,8 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel, if measured")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--blocks", type=int, nargs=3, default=None,
+                    help="override the block counts (reduced grids for profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

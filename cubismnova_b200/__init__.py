@@ -14,5 +14,6 @@ from . import block as Block
 from . import ops
 from . import euler
 from . import workloads
+from . import mg
 
-__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "CnError", "build"]
+__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "CnError", "build"]

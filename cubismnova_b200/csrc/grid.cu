@@ -298,6 +298,20 @@ cn_status cn_grid_layout(const cn_grid *g, int64_t *block_stride, int64_t *comp_
     return CN_OK;
 }
 
+cn_status cn_grid_shape(const cn_grid *g, int info[8])
+{
+    if (!g || !info) {
+        return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    }
+    for (int d = 0; d < 3; ++d) {
+        info[d] = g->nb[d];
+        info[3 + d] = g->n[d];
+    }
+    info[6] = g->ncomp;
+    info[7] = (int)g->dtype;
+    return CN_OK;
+}
+
 cn_status cn_grid_cell_size(const cn_grid *g, double h[3])
 {
     if (!g || !h) {

@@ -425,25 +425,12 @@ __global__ void __launch_bounds__(kCoarseThreads)
 using namespace cn;
 using namespace cn::mg;
 
-struct cn_mg {
-    int nlevels;
-    int nu1, nu2;
-    double omega;
-    std::vector<cn_grid *> p, pt, f, k; // per level (FP32); k[0] is the caller's grid
-    cn_grid *r32 = nullptr;             // finest FP32 residual
-    double *partials = nullptr;
-    double *sums = nullptr;
-    int *iters = nullptr;
-    int nparts = 0;
-    int coarse_iters_max = 0;
-    int smoother = 0;   // 0 Jacobi, 1 learned (set by cn_mg_set_learned)
-    void *learned = nullptr;
-};
+#include "mg_internal.h"
 
-static const cn_stencil kS1 = {{-1, -1, -1}, {2, 2, 2}, 0};
-static const cn_stencil kS1t = {{-1, -1, -1}, {2, 2, 2}, 1};
+const cn_stencil kS1 = {{-1, -1, -1}, {2, 2, 2}, 0};
+const cn_stencil kS1t = {{-1, -1, -1}, {2, 2, 2}, 1};
 
-static KArgs kargs(cn_mg *m, int l)
+KArgs kargs(cn_mg *m, int l)
 {
     KArgs a;
     a.G.L = make_geom(m->p[l], &kS1);
@@ -457,14 +444,14 @@ static KArgs kargs(cn_mg *m, int l)
     return a;
 }
 
-static unsigned grid_for(int64_t n)
+unsigned grid_for(int64_t n)
 {
     int64_t b = (n + 255) / 256;
     if (b > 148 * 16) b = 148 * 16;
     return (unsigned)(b < 1 ? 1 : b);
 }
 
-static float *fptr(cn_grid *g) { return reinterpret_cast<float *>(g->d_data); }
+float *fptr(cn_grid *g) { return reinterpret_cast<float *>(g->d_data); }
 
 // weighted Jacobi sweeps on level l (p = 0 on entry if zero_guess)
 static cn_status smooth(cn_mg *m, int l, int sweeps, bool zero_guess, cudaStream_t st)
@@ -499,14 +486,14 @@ static cn_status coarsest(cn_mg *m, int l, cudaStream_t st)
     return CN_OK;
 }
 
-static cn_status vcycle(cn_mg *m, int l, cudaStream_t st);
 
 static cn_status smooth_any(cn_mg *m, int l, int sweeps, bool zero_guess, cudaStream_t st)
 {
+    if (m->nn && ((m->nn_levels >> l) & 1)) return nn_smooth(m, l, sweeps, zero_guess, st);
     return smooth(m, l, sweeps, zero_guess, st);
 }
 
-static cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
+cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
 {
     if (l == m->nlevels - 1) return coarsest(m, l, st);
     cn_status s = smooth_any(m, l, m->nu1, true, st);
@@ -525,6 +512,10 @@ static cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
     prolong_kernel<<<grid_for(fcells), 256, 0, st>>>(Lf, fptr(m->p[l]), Lct, bc_view(m->p[l + 1], 0),
                                                       fptr(m->p[l + 1]), m->p[l]->nblocks);
     CN_CUDA_TRY(cudaGetLastError());
+    if (l == 0 && m->capture) {
+        s = m->capture(m, st);
+        if (s != CN_OK) return s;
+    }
     return smooth_any(m, l, m->nu2, false, st);
 }
 
@@ -617,6 +608,7 @@ cn_status cn_mg_destroy(cn_mg *m)
         if (l > 0) cn_grid_destroy(m->k[l]);
     }
     cn_grid_destroy(m->r32);
+    for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
     if (m->partials) cudaFree(m->partials);
     if (m->sums) cudaFree(m->sums);
     if (m->iters) cudaFree(m->iters);
@@ -709,6 +701,16 @@ cn_status cn_mg_solve(cn_mg *m, const cn_grid *f, cn_grid *p64, double rtol, int
     }
     if (cycles) *cycles = c;
     if (relres) *relres = rel;
+    return CN_OK;
+}
+
+// p64 += finest-level correction (the result of the last V-cycle)
+cn_status cn_mg_accumulate(cn_mg *m, cn_grid *p64, void *stream)
+{
+    if (!m || !p64) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    const int64_t n = p64->comp_stride;
+    axpy64_kernel<<<grid_for(n), 256, 0, as_stream(stream)>>>(reinterpret_cast<double *>(p64->d_data), fptr(m->p[0]), n);
+    CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
 

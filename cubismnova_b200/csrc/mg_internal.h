@@ -1,0 +1,45 @@
+// mg_internal.h -- multigrid solver state shared by mg.cu and learned.cu.
+#pragma once
+
+#include "cn_internal.h"
+
+#include <vector>
+
+struct cn_nn;
+
+struct cn_mg {
+    int nlevels;
+    int nu1, nu2;
+    double omega;
+    std::vector<cn_grid *> p, pt, f, k; // per level (FP32); k[0] is the caller's grid
+    cn_grid *r32 = nullptr;             // finest FP32 residual
+    double *partials = nullptr;
+    double *sums = nullptr;
+    int *iters = nullptr;
+    int nparts = 0;
+    int coarse_iters_max = 0;
+    // learned smoother: network, the levels it replaces Jacobi on (bit l),
+    // and per-level work grids (features, hidden activations, output)
+    cn_nn *nn = nullptr;
+    unsigned nn_levels = 0;
+    std::vector<cn_grid *> nn_bufs; // 4 per level: X (2 comps), H1 (16), H2 (16), Y (1)
+    // optional hook run at the finest level after the coarse-grid correction
+    cn_status (*capture)(cn_mg *, cudaStream_t) = nullptr;
+    void *capture_ctx = nullptr;
+};
+
+namespace cn {
+namespace mg {
+struct KArgs;
+}
+} // namespace cn
+
+extern const cn_stencil kS1, kS1t;
+unsigned grid_for(int64_t n);
+float *fptr(cn_grid *g);
+cn_status vcycle(cn_mg *m, int l, cudaStream_t st);
+// learned smoothing: `apps` applications of the network on level l
+extern "C" cn_status cn_mg_accumulate(cn_mg *m, cn_grid *p64, void *stream);
+extern "C" cn_status cn_mg_residual(cn_mg *m, const cn_grid *p64, const cn_grid *f, cn_grid *r32, double *rr,
+                                      double *ff, void *stream);
+cn_status nn_smooth(cn_mg *m, int l, int apps, bool zero_guess, cudaStream_t st);

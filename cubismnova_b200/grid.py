@@ -133,9 +133,28 @@ class Cartesian:
         _lib.check(_lib.lib().cn_grid_layout(h, C.byref(bs), C.byref(cs), C.byref(tb)))
         self.block_stride, self.comp_stride, self.total_bytes = bs.value, cs.value, tb.value
 
+    @classmethod
+    def view_of(cls, handle, owner=None):
+        """Non-owning Python view of a grid created inside the library (for
+        example a multigrid level); ``owner`` is kept alive with the view."""
+        g = cls.__new__(cls)
+        g._h = C.c_void_p(handle.value if isinstance(handle, C.c_void_p) else handle)
+        g._owned = False
+        g._owner = owner
+        bs, cs, tb = C.c_int64(), C.c_int64(), C.c_size_t()
+        _lib.check(_lib.lib().cn_grid_layout(g._h, C.byref(bs), C.byref(cs), C.byref(tb)))
+        g.block_stride, g.comp_stride, g.total_bytes = bs.value, cs.value, tb.value
+        info = (C.c_int * 8)()
+        _lib.check(_lib.lib().cn_grid_shape(g._h, info))
+        g._nb, g._n = tuple(info[0:3]), tuple(info[3:6])
+        g.ncomp = info[6]
+        g.dtype = {v: k for k, v in _DT.items()}[info[7]]
+        g._bcs = [dict() for _ in range(g.ncomp)]
+        return g
+
     # -- lifetime
     def close(self):
-        if getattr(self, "_h", None) is not None and self._h.value:
+        if getattr(self, "_owned", True) and getattr(self, "_h", None) is not None and self._h.value:
             _lib.lib().cn_grid_destroy(self._h)
             self._h = C.c_void_p()
 

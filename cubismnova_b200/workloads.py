@@ -105,3 +105,49 @@ def euler_bclists(nb, gamma: float = 1.4):
                 d[b] = lst
         out.append(d)
     return out
+
+
+def poisson_coefficient(k: Cartesian, seed: int = 1234, sigma: float = 0.5):
+    """k = 3-cell box filter (per axis, periodic) of exp(N(0, sigma^2)) i.i.d. per cell."""
+    import torch
+    nb, n = k.getSize(), k.getBlockCells()
+    G = [nb[d] * n[d] for d in range(3)]
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    a = torch.exp(torch.randn((G[2], G[1], G[0]), generator=gen, device="cuda", dtype=torch.float64) * sigma)
+    for dim in range(3):
+        a = (torch.roll(a, 1, dim) + a + torch.roll(a, -1, dim)) / 3.0
+    _global_to_blocks(k, a, torch)
+
+
+def poisson_rhs(f: Cartesian, seed: int = 4321, count: int = 32, width=(0.02, 0.08), amp=(-1.0, 1.0)):
+    """f = sum of `count` Gaussians (centres uniform in [0,1)^3, widths and
+    amplitudes uniform in the given ranges, periodic minimum-image distance),
+    minus its mean."""
+    import torch
+    nb, n = f.getSize(), f.getBlockCells()
+    G = [nb[d] * n[d] for d in range(3)]
+    h = f.getCellSize()
+    gen = torch.Generator(device="cpu").manual_seed(seed)
+    c = torch.rand((count, 3), generator=gen, dtype=torch.float64)
+    w = width[0] + (width[1] - width[0]) * torch.rand(count, generator=gen, dtype=torch.float64)
+    a = amp[0] + (amp[1] - amp[0]) * torch.rand(count, generator=gen, dtype=torch.float64)
+    xs = [((torch.arange(G[d], device="cuda", dtype=torch.float64) + 0.5) * h[d]) for d in range(3)]
+    out = torch.zeros((G[2], G[1], G[0]), device="cuda", dtype=torch.float64)
+    for j in range(count):
+        d2 = []
+        for d in range(3):
+            t = xs[d] - float(c[j, d])
+            t = t - torch.round(t)
+            d2.append(t * t)
+        r2 = d2[2][:, None, None] + d2[1][None, :, None] + d2[0][None, None, :]
+        out += float(a[j]) * torch.exp(-r2 / (2.0 * float(w[j]) ** 2))
+    out -= out.mean()
+    _global_to_blocks(f, out, torch)
+
+
+def _global_to_blocks(g: Cartesian, arr, torch):
+    nb, n = g.getSize(), g.getBlockCells()
+    cells = n[0] * n[1] * n[2]
+    v = arr.reshape(nb[2], n[2], nb[1], n[1], nb[0], n[0]).permute(0, 2, 4, 1, 3, 5).reshape(g.size(), cells)
+    g.tensor(0)[:, :cells].copy_(v.to(g.tensor(0).dtype))
+    torch.cuda.synchronize()

@@ -94,6 +94,8 @@ cn_status cn_grid_destroy(cn_grid *g);
 /* Layout in elements: block stride, component stride; total bytes. */
 cn_status cn_grid_layout(const cn_grid *g, int64_t *block_stride, int64_t *comp_stride,
                          size_t *total_bytes);
+/* nblocks[3], block_cells[3], ncomp, dtype of a grid (Grid/Cartesian.h:240-256). */
+cn_status cn_grid_shape(const cn_grid *g, int info[8]);
 /* Mesh::StructuredUniform cell size h = (end-begin)/cells
  * (Mesh/StructuredUniform.h:61, :333-336). */
 cn_status cn_grid_cell_size(const cn_grid *g, double h[3]);
@@ -193,6 +195,38 @@ cn_status cn_euler_rk3_step(cn_grid *U, cn_grid *work1, cn_grid *work2, double d
                             double *sums_out, void *stream);
 /* max over cells of |u_d| + c per direction (waits for the stream). */
 cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stream);
+
+/* ------------------------------------------------------------ multigrid */
+/* Geometric multigrid for div(k grad p) = f on a periodic grid (the
+ * reference announces integrated multigrid solvers, README.rst:43-44, with
+ * no code).  k: FLOAT32 cell coefficients, 1 component, cubic cells; the
+ * levels halve the cells per block while they are even (max_levels <= 0: all).
+ * Operator: harmonic face means, L p = ih2 * sum_d [kf+(p+ - p) - kf-(p - p-)];
+ * smoother: weighted Jacobi (omega), nu1 pre / nu2 post sweeps; restriction:
+ * mean of 8 children; prolongation: trilinear; coarsest level (<= 4096 cells):
+ * FP64 conjugate gradients in one CTA.  V-cycles run in FP32. */
+typedef struct cn_mg cn_mg;
+cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_levels, cn_mg **out);
+cn_status cn_mg_destroy(cn_mg *m);
+cn_status cn_mg_levels(const cn_mg *m, int *nlevels, int *coarsest_cells);
+/* e = one V-cycle for L e = rhs from e = 0 (FLOAT32 grids of the finest shape). */
+cn_status cn_mg_vcycle(cn_mg *m, const cn_grid *rhs, cn_grid *e, void *stream);
+/* FP64 residual r = f - L p64 (p64 FLOAT64, f FLOAT32); r32 optional FLOAT32
+ * copy of r; returns sum r^2 and sum f^2 (waits for the stream). */
+cn_status cn_mg_residual(cn_mg *m, const cn_grid *p64, const cn_grid *f, cn_grid *r32, double *rr,
+                         double *ff, void *stream);
+/* Solve to ||f - L p|| <= rtol ||f||: p64 zeroed, then per cycle the FP64
+ * residual, one FP32 V-cycle on it, p64 += e (defect correction). */
+cn_status cn_mg_solve(cn_mg *m, const cn_grid *f, cn_grid *p64, double rtol, int max_cycles,
+                      int *cycles, double *relres, void *stream);
+/* Single finest-level operators (tests): one Jacobi sweep, residual
+ * restricted onto level 1, and p += prolongation of a level-1 correction. */
+cn_status cn_mg_jacobi(cn_mg *m, const cn_grid *pin, const cn_grid *f, cn_grid *pout, void *stream);
+cn_status cn_mg_restrict_residual(cn_mg *m, const cn_grid *p, const cn_grid *f, cn_grid *fc,
+                                  void *stream);
+cn_status cn_mg_prolong(cn_mg *m, const cn_grid *ec, cn_grid *p, void *stream);
+/* Level grids owned by the solver: which = 0 solution, 1 right-hand side, 2 k. */
+cn_status cn_mg_level_grid(cn_mg *m, int level, int which, cn_grid **out);
 
 /* ------------------------------------------------- pointwise field ops */
 /* The optimised hooks that Block/FieldOperator.h:149-227 declares (under

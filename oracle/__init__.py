@@ -245,3 +245,62 @@ def ref_euler_stage(Us, Un, nb, n, bclists, stage, dt, gamma, h, threads=0, bloc
           C.c_int(threads if threads > 0 else (os.cpu_count() or 1)), C.c_int(b0), C.c_int(cnt),
           C.c_int(reps))
     return t, out
+
+
+# ---------------------------------------------------------------- multigrid
+def _i3(v):
+    return (C.c_int * 3)(*[int(x) for x in v])
+
+
+def _f32p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def mg_jacobi(pin, k, f, nb, n, omega, ih2):
+    out = np.zeros_like(f)
+    s = block_stride(n, np.float32)
+    lib().or_mg_jacobi(_i3(nb), _i3(n), C.c_int64(s), _f32p(pin), _f32p(k), _f32p(f),
+                       C.c_float(omega), C.c_float(ih2), _f32p(out))
+    return out
+
+
+def mg_resid_restrict(p, k, f, nb, n, ih2):
+    nc = [v // 2 for v in n]
+    cs = block_stride(nc, np.float32)
+    out = np.zeros(int(np.prod(nb)) * cs, dtype=np.float32)
+    lib().or_mg_resid_restrict(_i3(nb), _i3(n), C.c_int64(block_stride(n, np.float32)), _f32p(p), _f32p(k),
+                               _f32p(f), C.c_float(ih2), C.c_int64(cs), _f32p(out))
+    return out
+
+
+def mg_restrict_mean(kf, nb, n):
+    nc = [v // 2 for v in n]
+    cs = block_stride(nc, np.float32)
+    out = np.zeros(int(np.prod(nb)) * cs, dtype=np.float32)
+    lib().or_mg_restrict_mean(_i3(nb), _i3(n), C.c_int64(block_stride(n, np.float32)), _f32p(kf),
+                              C.c_int64(cs), _f32p(out))
+    return out
+
+
+def mg_prolong(p, e, nb, n):
+    out = np.array(p, dtype=np.float32, copy=True)
+    nc = [v // 2 for v in n]
+    lib().or_mg_prolong(_i3(nb), _i3(n), C.c_int64(block_stride(n, np.float32)), _f32p(out),
+                        C.c_int64(block_stride(nc, np.float32)), _f32p(e))
+    return out
+
+
+def mg_resid64(p64, k, f, nb, n, ih2):
+    r32 = np.zeros_like(f)
+    rr, ff = C.c_double(), C.c_double()
+    lib().or_mg_resid64(_i3(nb), _i3(n), C.c_int64(block_stride(n, np.float64)), _ptr(p64),
+                        C.c_int64(block_stride(n, np.float32)), _f32p(k), _f32p(f), C.c_double(ih2),
+                        _f32p(r32), C.byref(rr), C.byref(ff))
+    return r32, rr.value, ff.value
+
+
+def mg_coarse_cg(f, k, nb, n, ih2, max_iter=10000, rtol=1e-13):
+    p = np.zeros_like(f)
+    it = lib().or_mg_coarse_cg(_i3(nb), _i3(n), C.c_int64(block_stride(n, np.float32)), _f32p(f), _f32p(k),
+                               C.c_double(ih2), C.c_int(max_iter), C.c_double(rtol), _f32p(p))
+    return p, it

@@ -93,7 +93,7 @@ def test_fp32_vs_fp64_error(cn):
         l1 = np.mean(np.abs(a[c] - b[c])) / scale
         linf = np.max(np.abs(a[c] - b[c])) / scale
         print(f"var {c}: L1 {l1:.3e}  Linf {linf:.3e} (relative to max |state|)")
-        assert linf < 1e-6 and l1 < 1e-7, (c, l1, linf)
+        assert linf < 1e-6 and l1 < 5e-7, (c, l1, linf)
 
 
 def test_uniform_state_full_size_is_steady(cn):
