@@ -15,5 +15,6 @@ from . import ops
 from . import euler
 from . import workloads
 from . import mg
+from . import learned
 
-__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "CnError", "build"]
+__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "CnError", "build"]

@@ -1,0 +1,115 @@
+"""Learned 3-D convolutional smoother for the multigrid solver
+(csrc/learned.cu): training on device-resident patches with the library's own
+forward/backward kernels and Adam, and use inside the V-cycle."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .grid import Cartesian, _stream_handle
+
+_P, _I, _D = C.c_void_p, C.c_int, C.c_double
+_lib.register({
+    "cn_nn_create": (_I, [C.c_uint64, _D, _D, C.POINTER(_P)]),
+    "cn_nn_destroy": (_I, [_P]),
+    "cn_nn_get_weights": (_I, [_P, _P]),
+    "cn_nn_set_weights": (_I, [_P, _P]),
+    "cn_nn_weight_count": (_I, []),
+    "cn_nn_loss_grad": (_I, [_P, _P, _P, _P, _I, _I, _D, C.POINTER(C.c_double), _P, _P]),
+    "cn_nn_adam_step": (_I, [_P, _D, _P]),
+    "cn_nn_train": (_I, [_P, _P, _P, _P, _I, _I, _D, _I, _I, _D, C.c_uint64, C.POINTER(C.c_double), _P]),
+    "cn_mg_collect_patches": (_I, [_P, _P, _I, _I, C.c_uint64, _P, _P, _P, _I, C.POINTER(_I), _P]),
+    "cn_mg_set_smoother": (_I, [_P, _P, C.c_uint]),
+})
+
+CI, CH = 2, 16
+SHAPES = ((27, CI, CH), (27, CH, CH), (27, CH, 1))
+
+
+class LearnedSmoother:
+    """p <- p + omega * r/D + N(r/D, (r/D) ln k), N a 3-layer 3^3 conv net."""
+
+    def __init__(self, seed: int = 0, omega: float = 0.8, init_scale: float = 1e-3):
+        h = C.c_void_p()
+        _lib.check(_lib.lib().cn_nn_create(seed, omega, init_scale, C.byref(h)))
+        self._h, self.omega = h, omega
+        self.nweights = _lib.lib().cn_nn_weight_count()
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.lib().cn_nn_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def weights(self):
+        w = np.empty(self.nweights, dtype=np.float32)
+        _lib.check(_lib.lib().cn_nn_get_weights(self._h, w.ctypes.data_as(C.c_void_p)))
+        out, o = [], 0
+        for s in SHAPES:
+            n = int(np.prod(s))
+            out.append(w[o:o + n].reshape(s))
+            o += n
+        return out
+
+    def set_weights(self, W1, W2, W3):
+        w = np.concatenate([np.asarray(a, dtype=np.float32).ravel() for a in (W1, W2, W3)])
+        assert w.size == self.nweights
+        _lib.check(_lib.lib().cn_nn_set_weights(self._h, w.ctypes.data_as(C.c_void_p)))
+
+    def loss_grad(self, x, k, r, P: int, ih2: float, stream=None):
+        """x (B,2,(P+8)^3), k (B,(P+2)^3), r (B,P^3): contiguous float32 CUDA tensors."""
+        B = x.shape[0]
+        loss = C.c_double()
+        g = np.empty(self.nweights, dtype=np.float32)
+        _lib.check(_lib.lib().cn_nn_loss_grad(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(k.data_ptr()),
+                                              C.c_void_p(r.data_ptr()), B, P, ih2, C.byref(loss),
+                                              g.ctypes.data_as(C.c_void_p), _stream_handle(stream)))
+        out, o = [], 0
+        for s in SHAPES:
+            n = int(np.prod(s))
+            out.append(g[o:o + n].reshape(s))
+            o += n
+        return loss.value, out
+
+    def train(self, x, k, r, P: int, ih2: float, epochs: int = 10, batch: int = 16, lr: float = 1e-3,
+              seed: int = 0, stream=None) -> float:
+        last = C.c_double()
+        _lib.check(_lib.lib().cn_nn_train(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(k.data_ptr()),
+                                          C.c_void_p(r.data_ptr()), x.shape[0], P, ih2, epochs, batch, lr, seed,
+                                          C.byref(last), _stream_handle(stream)))
+        return last.value
+
+
+def collect_patches(mg, f: Cartesian, cycles: int, per_snapshot: int, max_patches: int, seed: int = 0,
+                    stream=None):
+    """Training samples from plain V-cycles (see cn_mg_collect_patches)."""
+    import torch
+    n = f.getBlockCells()
+    P = n[0]
+    x = torch.empty((max_patches, 2, (P + 8) ** 3), dtype=torch.float32, device="cuda")
+    k = torch.empty((max_patches, (P + 2) ** 3), dtype=torch.float32, device="cuda")
+    r = torch.empty((max_patches, P ** 3), dtype=torch.float32, device="cuda")
+    cnt = C.c_int()
+    _lib.check(_lib.lib().cn_mg_collect_patches(mg.handle, f.handle, cycles, per_snapshot, seed,
+                                                C.c_void_p(x.data_ptr()), C.c_void_p(k.data_ptr()),
+                                                C.c_void_p(r.data_ptr()), max_patches, C.byref(cnt),
+                                                _stream_handle(stream)))
+    m = cnt.value
+    return x[:m].contiguous(), k[:m].contiguous(), r[:m].contiguous(), P
+
+
+def use_in(mg, smoother, level_mask: int = 0xFFFF):
+    """Replace Jacobi by the learned smoother on the levels in level_mask
+    (smoother None: back to Jacobi everywhere)."""
+    _lib.check(_lib.lib().cn_mg_set_smoother(mg.handle, smoother.handle if smoother else None, level_mask))

@@ -228,6 +228,40 @@ cn_status cn_mg_prolong(cn_mg *m, const cn_grid *ec, cn_grid *p, void *stream);
 /* Level grids owned by the solver: which = 0 solution, 1 right-hand side, 2 k. */
 cn_status cn_mg_level_grid(cn_mg *m, int level, int which, cn_grid **out);
 
+/* p64 += the finest-level correction of the last V-cycle. */
+cn_status cn_mg_accumulate(cn_mg *m, cn_grid *p64, void *stream);
+
+/* ------------------------------------------------------ learned smoother */
+/* A learned 3x3x3 convolutional smoother (no reference counterpart; the
+ * reference has no learned components): inputs x0 = r/D, x1 = x0 ln k,
+ * h1 = relu(conv(W1, x)) (2 -> 16 ch), h2 = relu(conv(W2, h1)) (16 -> 16),
+ * y = conv(W3, h2) (16 -> 1); smoothing step p += omega*x0 + y.  Weights
+ * [tap][cin][cout], tap = dx+1 + 3(dy+1) + 9(dz+1), FP32 master copy. */
+typedef struct cn_nn cn_nn;
+cn_status cn_nn_create(uint64_t seed, double omega, double init_scale, cn_nn **out);
+cn_status cn_nn_destroy(cn_nn *nn);
+int cn_nn_weight_count(void);
+cn_status cn_nn_get_weights(const cn_nn *nn, float *host);
+cn_status cn_nn_set_weights(cn_nn *nn, const float *host);
+/* Training loss (1/B) sum_b ||r_b - A c_b||^2 / ||r_b||^2, c = omega x0 + y,
+ * and its gradient, on device patches x [B][2][(P+8)^3], k [B][(P+2)^3],
+ * r [B][P^3]; grad_out (optional, device or host) receives all weights'
+ * gradients.  Waits for the stream if loss is requested. */
+cn_status cn_nn_loss_grad(cn_nn *nn, const float *x, const float *k, const float *r, int B, int P,
+                          double ih2, double *loss, float *grad_out, void *stream);
+cn_status cn_nn_adam_step(cn_nn *nn, double lr, void *stream);
+cn_status cn_nn_train(cn_nn *nn, const float *x, const float *k, const float *r, int npatches, int P,
+                      double ih2, int epochs, int batch, double lr, uint64_t seed, double *last_loss,
+                      void *stream);
+/* Training patches from `cycles` plain V-cycles of m on L p = f: per cycle
+ * `per_snapshot` random blocks of the finest residual before pre-smoothing
+ * and after the coarse-grid correction (device outputs, see cn_nn_loss_grad). */
+cn_status cn_mg_collect_patches(cn_mg *m, const cn_grid *f, int cycles, int per_snapshot, uint64_t seed,
+                                float *x, float *k, float *r, int max_patches, int *count, void *stream);
+/* Use the network instead of Jacobi on the levels set in level_mask (bit l);
+ * nn == NULL restores Jacobi everywhere. */
+cn_status cn_mg_set_smoother(cn_mg *m, cn_nn *nn, unsigned level_mask);
+
 /* ------------------------------------------------- pointwise field ops */
 /* The optimised hooks that Block/FieldOperator.h:149-227 declares (under
  * CUBISM_OPTIMIZED_FIELD_OP) and never defines, with the reference's exact
