@@ -251,7 +251,7 @@ cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int nco
     g->nblocks = (int)nbl;
     g->comp_stride = g->block_stride * nbl;
     g->bcs.assign(ncomp, std::vector<std::vector<HostBC>>(nbl));
-    g->bc_dirty = true;
+    g->bc_dirty = false; // the device tables are initialised empty below
     cudaError_t e = cudaGetDevice(&g->device);
     if (e != cudaSuccess) {
         delete g;
@@ -264,6 +264,13 @@ cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int nco
     if (e == cudaSuccess) e = cudaMalloc(&g->d_bc_mode, (size_t)ncomp * nbl);
     if (e == cudaSuccess) e = cudaMalloc(&g->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(g->d_err, 0, sizeof(int));
+    // valid empty BC tables from the start: every kernel may read them, even
+    // on a grid whose BCs were never pushed or synchronised
+    if (e == cudaSuccess) e = cudaMemset(g->d_bc_off, 0, sizeof(int32_t) * ncomp * (nbl + 1));
+    if (e == cudaSuccess) e = cudaMemset(g->d_bc_mode, 0, (size_t)ncomp * nbl);
+    if (e == cudaSuccess) e = cudaMalloc(&g->d_bc_ent, sizeof(cn::DevBC));
+    if (e == cudaSuccess) e = cudaMemset(g->d_bc_ent, 0, sizeof(cn::DevBC));
+    if (e == cudaSuccess) g->bc_ent_cap = 1;
     if (e != cudaSuccess) {
         cn_grid_destroy(g);
         return cuda_fail(e, "cn_grid_create allocation");

@@ -281,12 +281,15 @@ __global__ void __launch_bounds__(256) sum_pairs_kernel(const double *partials, 
     }
 }
 
-// p64 += e
-__global__ void __launch_bounds__(256) axpy64_kernel(double *p64, const float *e, int64_t n)
+// p64 += e (block layouts with their own strides)
+__global__ void __launch_bounds__(256) axpy64_kernel(double *p64, int64_t s64, const float *e, int64_t s32,
+                                                     int64_t cells, int nblocks)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x)
-        p64[i] += (double)e[i];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cells * nblocks;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i / cells, c = i - b * cells;
+        p64[b * s64 + c] += (double)e[b * s32 + c];
+    }
 }
 
 // Coarsest level: CG in FP64 on -L x = -f, one CTA, cells <= 4096, periodic
@@ -688,12 +691,11 @@ cn_status cn_mg_solve(cn_mg *m, const cn_grid *f, cn_grid *p64, double rtol, int
     const double fn = std::sqrt(ff);
     double rel = fn > 0 ? std::sqrt(rr) / fn : 0.0;
     int c = 0;
-    const int64_t n = p64->comp_stride;
     while (c < max_cycles && rel > rtol) {
         s = vcycle(m, 0, st);
         if (s != CN_OK) return s;
-        axpy64_kernel<<<grid_for(n), 256, 0, st>>>(reinterpret_cast<double *>(p64->d_data), fptr(m->p[0]), n);
-        CN_CUDA_TRY(cudaGetLastError());
+        s = cn_mg_accumulate(m, p64, stream);
+        if (s != CN_OK) return s;
         s = cn_mg_residual(m, p64, f, m->f[0], &rr, nullptr, stream);
         if (s != CN_OK) return s;
         rel = std::sqrt(rr) / fn;
@@ -708,8 +710,13 @@ cn_status cn_mg_solve(cn_mg *m, const cn_grid *f, cn_grid *p64, double rtol, int
 cn_status cn_mg_accumulate(cn_mg *m, cn_grid *p64, void *stream)
 {
     if (!m || !p64) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
-    const int64_t n = p64->comp_stride;
-    axpy64_kernel<<<grid_for(n), 256, 0, as_stream(stream)>>>(reinterpret_cast<double *>(p64->d_data), fptr(m->p[0]), n);
+    const cn_grid *g = m->p[0];
+    if (p64->dtype != CN_FLOAT64 || p64->nblocks != g->nblocks || p64->n[0] != g->n[0] || p64->n[1] != g->n[1] ||
+        p64->n[2] != g->n[2])
+        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
+    const int64_t cells = (int64_t)g->n[0] * g->n[1] * g->n[2];
+    axpy64_kernel<<<grid_for(cells * g->nblocks), 256, 0, as_stream(stream)>>>(
+        reinterpret_cast<double *>(p64->d_data), p64->block_stride, fptr(m->p[0]), g->block_stride, cells, g->nblocks);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }

@@ -7,10 +7,17 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
+def _end(nb, n):
+    """Domain extent giving cubic cells (h = 1 / max cells)."""
+    g = max(nb[d] * n[d] for d in range(3))
+    return tuple(nb[d] * n[d] / g for d in range(3))
+
+
 def _setup(cn, nb, n, seed=1):
-    k = cn.Grid.Cartesian(nb, n, dtype=np.float32)
+    e = _end(nb, n)
+    k = cn.Grid.Cartesian(nb, n, end=e, dtype=np.float32)
     cn.workloads.poisson_coefficient(k, seed=seed)
-    f = cn.Grid.Cartesian(nb, n, dtype=np.float32)
+    f = cn.Grid.Cartesian(nb, n, end=e, dtype=np.float32)
     cn.workloads.poisson_rhs(f, seed=seed + 1)
     return k, f
 
@@ -20,12 +27,12 @@ def test_jacobi_and_restriction_match_oracle(cn, oracle_lib):
     nb, n = (2, 3, 2), (8, 8, 8)
     k, f = _setup(cn, nb, n)
     m = cn.mg.Multigrid(k, omega=0.8)
-    p = cn.Grid.Cartesian(nb, n, dtype=np.float32)
+    p = cn.Grid.Cartesian(nb, n, end=_end(nb, n), dtype=np.float32)
     rng = np.random.default_rng(2)
     ph = np.zeros(p.comp_stride, dtype=np.float32)
     p.blocks_view(ph)[:] = rng.standard_normal(p.blocks_view(ph).shape)
     p.upload(ph)
-    out = cn.Grid.Cartesian(nb, n, dtype=np.float32)
+    out = cn.Grid.Cartesian(nb, n, end=_end(nb, n), dtype=np.float32)
     m.jacobi(p, f, out)
     torch.cuda.synchronize()
     kh, fh = k.download(), f.download()
