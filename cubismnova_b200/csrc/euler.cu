@@ -1,20 +1,22 @@
 // euler.cu -- K2: lab fill fused with WENO5-JS + Rusanov + flux divergence for
 // the 3-D compressible Euler equations, and the fused SSP-RK3 stage update.
 //
-// One CTA owns an 8x8x8 tile of one block.  It stages the tile and its
-// cross-shaped 3-cell halo (the lab of a stencil (-3,4) non-tensorial,
-// Block/FieldLab.h:180-224) of all five conserved variables into shared memory
-// as primitives (rho, u, v, w, p): halo cells inside the block are plain
-// loads, cells outside are resolved by cn::lab_value (periodic neighbour,
-// skip rule and BC chain of each component's BC vector).  Then, per
-// direction, every face flux of the tile is computed exactly once (one thread
-// per face: 2 x 5 WENO5 reconstructions + Rusanov), stored in shared memory,
-// and differenced into per-cell accumulators held in registers.  The epilogue
+// One CTA owns an 8x8x8 tile of one block.  It stages the tile's cells of all
+// five conserved variables into shared memory as primitives (rho, u, v, w, p)
+// and, before the sweep of each direction, that direction's two 3-cell halo
+// slabs (together the lab of a stencil (-3,4) non-tensorial,
+// Block/FieldLab.h:180-224): halo cells inside the block are plain loads,
+// cells outside are resolved by cn::lab_value (periodic neighbour, skip rule
+// and BC chain of each component's BC vector).  Per direction every face flux
+// of the tile is computed exactly once (one thread per face: 2 x 5 WENO5
+// reconstructions + Rusanov), stored in shared memory, and differenced into
+// per-cell accumulators held in registers.  The epilogue
 // applies the SSP-RK3 (Shu & Osher 1988) convex combination and optionally
 // accumulates FP64 conservation sums per CTA (reduced in a fixed order by a
 // second kernel, so the sums are deterministic).
 //
-// Shared memory per CTA: 5 x 1664 primitives + 5 x 576 face fluxes.
+// Shared memory per CTA: 5 x 896 primitives (the tile plus one direction's
+// halo slabs, restaged before each sweep) + 5 x 576 face fluxes.
 #include "cn_internal.h"
 #include "cn_tma.cuh"
 #include "euler_math.cuh"
@@ -27,11 +29,9 @@ namespace euler {
 
 constexpr int TB = 8;                 // tile edge
 constexpr int G = 3;                  // ghost width
-constexpr int XW = TB + 2 * G;        // 14
-constexpr int NXB = XW * TB * TB;     // core + x halos: 896
-constexpr int NYH = TB * 2 * G * TB;  // y halos: 384
-constexpr int NZH = 2 * G * TB * TB;  // z halos: 384
-constexpr int SV = NXB + NYH + NZH;   // cells per variable: 1664
+constexpr int NCORE = TB * TB * TB;   // tile cells: 512
+constexpr int NHALO = 2 * G * TB * TB; // one direction's halo slabs: 384
+constexpr int SV = NCORE + NHALO;     // staged cells per variable: 896
 constexpr int NCELL = TB * TB * TB;   // 512
 constexpr int NFACE = (TB + 1) * TB * TB; // 576
 constexpr int NT = 192;               // threads per CTA (576 = 3 * 192)
@@ -51,39 +51,38 @@ template <typename T> struct StageParams {
     int *err;
 };
 
-// shared-memory index of tile-local cell (x, y, z), coordinates in [-3, 11)
-// on the cross: core/x-halo box, then y halos, then z halos
-__device__ __forceinline__ int sidx(int x, int y, int z)
+// Shared-memory index of tile-local cell (x, y, z) while direction D is being
+// swept: the core cells, then the two 3-cell halo slabs of direction D (only
+// one direction's halo is staged at a time; the slot is reloaded per sweep).
+template <int D> __device__ __forceinline__ int sidx(int x, int y, int z)
 {
-    const bool in_y = (unsigned)y < (unsigned)TB;
-    const bool in_z = (unsigned)z < (unsigned)TB;
-    const int ixb = (z * TB + y) * XW + (x + G);
-    const int jy = y < 0 ? y + G : y - TB + G;
-    const int iyh = NXB + (z * 2 * G + jy) * TB + x;
-    const int kz = z < 0 ? z + G : z - TB + G;
-    const int izh = NXB + NYH + (kz * TB + y) * TB + x;
-    return (in_y && in_z) ? ixb : (in_z ? iyh : izh);
+    const int c = D == 0 ? x : (D == 1 ? y : z);
+    if ((unsigned)c < (unsigned)TB) return x + TB * (y + TB * z);
+    const int h = c < 0 ? c + G : c - TB + G; // 0..5
+    if (D == 0) return NCORE + (z * TB + y) * (2 * G) + h;
+    if (D == 1) return NCORE + (z * (2 * G) + h) * TB + x;
+    return NCORE + (h * TB + y) * TB + x;
 }
 
-template <typename T>
-__device__ __forceinline__ void decode_cross(int i, int &x, int &y, int &z)
+// tile-local coordinates of halo slot i of direction D
+template <int D> __device__ __forceinline__ void halo_cell(int i, int &x, int &y, int &z)
 {
-    if (i < NXB) {
-        x = i % XW - G;
-        y = (i / XW) % TB;
-        z = i / (XW * TB);
-    } else if (i < NXB + NYH) {
-        const int r = i - NXB;
-        x = r % TB;
-        const int jy = (r / TB) % (2 * G);
-        z = r / (TB * 2 * G);
-        y = jy < G ? jy - G : jy - G + TB;
+    int h;
+    if (D == 0) {
+        h = i % (2 * G);
+        y = (i / (2 * G)) % TB;
+        z = i / (2 * G * TB);
+        x = h < G ? h - G : h - G + TB;
+    } else if (D == 1) {
+        x = i % TB;
+        h = (i / TB) % (2 * G);
+        z = i / (TB * 2 * G);
+        y = h < G ? h - G : h - G + TB;
     } else {
-        const int r = i - NXB - NYH;
-        x = r % TB;
-        y = (r / TB) % TB;
-        const int kz = r / (TB * TB);
-        z = kz < G ? kz - G : kz - G + TB;
+        x = i % TB;
+        y = (i / TB) % TB;
+        h = i / (TB * TB);
+        z = h < G ? h - G : h - G + TB;
     }
 }
 
@@ -113,7 +112,7 @@ __device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const int o = k - 3;
-            idx[k] = D == 0 ? sidx(x + o, y, z) : (D == 1 ? sidx(x, y + o, z) : sidx(x, y, z + o));
+            idx[k] = D == 0 ? sidx<0>(x + o, y, z) : (D == 1 ? sidx<1>(x, y + o, z) : sidx<2>(x, y, z + o));
         }
         T WL[5], WR[5];
 #pragma unroll
@@ -121,8 +120,7 @@ __device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F
             const T *Wc = W + c * SV;
             const T v0 = Wc[idx[0]], v1 = Wc[idx[1]], v2 = Wc[idx[2]];
             const T v3 = Wc[idx[3]], v4 = Wc[idx[4]], v5 = Wc[idx[5]];
-            WL[c] = weno5<T>(v0, v1, v2, v3, v4);
-            WR[c] = weno5<T>(v5, v4, v3, v2, v1);
+            weno5_pair(v0, v1, v2, v3, v4, v5, WL[c], WR[c]);
         }
         T Fl[5];
         rusanov<T>(WL, WR, D, gamma, igm1, Fl);
@@ -149,8 +147,42 @@ __device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F
     __syncthreads();
 }
 
+// Loads the two 3-cell halo slabs of direction D into the halo slot:
+// cells inside the block are plain loads, cells outside are resolved by
+// cn::lab_value (periodic neighbour, skip rule, BC chain per component).
+template <typename T, int D>
+__device__ __forceinline__ void stage_halo(const StageParams<T> &p, T *W, int block, int bx, int by, int bz, int x0,
+                                           int y0, int z0, int64_t boff)
+{
+    const LabGeom &L = p.L;
+    const int N0 = L.n[0], N1 = L.n[1], N2 = L.n[2];
+    for (int i = threadIdx.x; i < NHALO; i += NT) {
+        int x, y, z;
+        halo_cell<D>(i, x, y, z);
+        const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
+        T u[5];
+        if ((unsigned)gx < (unsigned)N0 && (unsigned)gy < (unsigned)N1 && (unsigned)gz < (unsigned)N2) {
+            const int64_t o = boff + gx + (int64_t)N0 * (gy + (int64_t)N1 * gz);
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                u[c] = p.U[c][o];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                if (!lab_value<T>(p.U[c], L, p.bc[c], block, bx, by, bz, gx, gy, gz, true, u[c]))
+                    u[c] = T(0);
+            }
+        }
+        T w[5];
+        to_primitive<T>(u[0], u[1], u[2], u[3], u[4], p.gm1, w);
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            W[c * SV + NCORE + i] = w[c];
+    }
+}
+
 template <typename T>
-__global__ void __launch_bounds__(NT, 2) stage_kernel(StageParams<T> p)
+__global__ void __launch_bounds__(NT, 3) stage_kernel(StageParams<T> p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *W = reinterpret_cast<T *>(smem_raw);       // [5][SV]
@@ -172,31 +204,17 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(StageParams<T> p)
     const int bz = block / (L.nb[0] * L.nb[1]);
     const int64_t boff = (int64_t)block * L.bstride;
 
-    // ---- stage the lab cross as primitives
-    for (int i = threadIdx.x; i < SV; i += NT) {
-        int x, y, z;
-        decode_cross<T>(i, x, y, z);
-        const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
-        T u[5];
-        if ((unsigned)gx < (unsigned)N0 && (unsigned)gy < (unsigned)N1 &&
-            (unsigned)gz < (unsigned)N2) {
-            const int64_t o = boff + gx + (int64_t)N0 * (gy + (int64_t)N1 * gz);
-#pragma unroll
-            for (int c = 0; c < 5; ++c)
-                u[c] = p.U[c][o];
-        } else {
-#pragma unroll
-            for (int c = 0; c < 5; ++c) {
-                if (!lab_value<T>(p.U[c], L, p.bc[c], block, bx, by, bz, gx, gy, gz, true, u[c]))
-                    u[c] = T(0);
-            }
-        }
+    // ---- stage the tile's cells as primitives (the halo slot follows per sweep)
+    for (int i = threadIdx.x; i < NCORE; i += NT) {
+        const int x = i % TB, y = (i / TB) % TB, z = i / (TB * TB);
+        const int64_t o = boff + (x0 + x) + (int64_t)N0 * ((y0 + y) + (int64_t)N1 * (z0 + z));
         T w[5];
-        to_primitive<T>(u[0], u[1], u[2], u[3], u[4], p.gm1, w);
+        to_primitive<T>(p.U[0][o], p.U[1][o], p.U[2][o], p.U[3][o], p.U[4][o], p.gm1, w);
 #pragma unroll
         for (int c = 0; c < 5; ++c)
             W[c * SV + i] = w[c];
     }
+    stage_halo<T, 0>(p, W, block, bx, by, bz, x0, y0, z0, boff);
     __syncthreads();
 
     T acc[CPT][5];
@@ -207,7 +225,11 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(StageParams<T> p)
             acc[k][c] = T(0);
 
     sweep<T, 0>(W, F, acc, p.gamma, p.igm1, p.ih[0]);
+    stage_halo<T, 1>(p, W, block, bx, by, bz, x0, y0, z0, boff);
+    __syncthreads();
     sweep<T, 1>(W, F, acc, p.gamma, p.igm1, p.ih[1]);
+    stage_halo<T, 2>(p, W, block, bx, by, bz, x0, y0, z0, boff);
+    __syncthreads();
     sweep<T, 2>(W, F, acc, p.gamma, p.igm1, p.ih[2]);
 
     // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows

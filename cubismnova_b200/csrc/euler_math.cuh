@@ -41,10 +41,10 @@ __device__ __forceinline__ float dabs(float a) { return fabsf(a); }
 __device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float dmax(float a, float b) { return fmaxf(a, b); }
 
-// Left-biased WENO5-JS value at i+1/2 from v0..v4 = v[i-2..i+2].
-// 1 division, 14 FMA, 12 other flops (see flop count in euler.cu).
+// Left-biased WENO5-JS reconstruction at i+1/2 from v0..v4 = v[i-2..i+2],
+// returned as numerator and denominator: value = num / den.
 template <typename T>
-__device__ __forceinline__ T weno5(T v0, T v1, T v2, T v3, T v4)
+__device__ __forceinline__ void weno5_nd(T v0, T v1, T v2, T v3, T v4, T &num, T &den)
 {
     using C = K<T>;
     // smoothness indicators
@@ -65,9 +65,34 @@ __device__ __forceinline__ T weno5(T v0, T v1, T v2, T v3, T v4)
     const T n0 = dfma(T(2), v0, dfma(T(-7), v1, T(11) * v2)); // 2v0 - 7v1 + 11v2
     const T n1 = dfma(T(5), v2, dfma(T(2), v3, -v1));         // -v1 + 5v2 + 2v3
     const T n2 = dfma(T(2), v2, dfma(T(5), v3, -v4));         // 2v2 + 5v3 - v4
-    const T num = dfma(w0, n0, dfma(w1, n1, w2 * n2));
-    const T den = C::six * ((w0 + w1) + w2);
-    return num / den;
+    num = dfma(w0, n0, dfma(w1, n1, w2 * n2));
+    den = C::six * ((w0 + w1) + w2);
+}
+
+// Left and right states at the face between v2 and v3 from v0..v5 =
+// v[i-2..i+3].  FP64 shares one division between the two:
+//   inv = 1/(denL*denR), vL = (numL*denR)*inv, vR = (numR*denL)*inv
+// (den >= 6e-25 since eps = 1e-6, so the product cannot underflow in FP64);
+// FP32 divides twice, as the product could leave the FP32 range.
+__device__ __forceinline__ void weno5_pair(double v0, double v1, double v2, double v3, double v4, double v5,
+                                           double &vl, double &vr)
+{
+    double nl, dl, nr, dr;
+    weno5_nd<double>(v0, v1, v2, v3, v4, nl, dl);
+    weno5_nd<double>(v5, v4, v3, v2, v1, nr, dr);
+    const double inv = 1.0 / (dl * dr);
+    vl = (nl * dr) * inv;
+    vr = (nr * dl) * inv;
+}
+
+__device__ __forceinline__ void weno5_pair(float v0, float v1, float v2, float v3, float v4, float v5, float &vl,
+                                           float &vr)
+{
+    float nl, dl, nr, dr;
+    weno5_nd<float>(v0, v1, v2, v3, v4, nl, dl);
+    weno5_nd<float>(v5, v4, v3, v2, v1, nr, dr);
+    vl = nl / dl;
+    vr = nr / dr;
 }
 
 // Rusanov flux through a face with normal direction `d` (0,1,2) from the

@@ -72,8 +72,7 @@
                             const T *P = prim + c * le + li;                   \
                             const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st]; \
                             const T v3 = P[0], v4 = P[st], v5 = P[2 * st];     \
-                            WL[c] = weno5_##SUF(v0, v1, v2, v3, v4);           \
-                            WR[c] = weno5_##SUF(v5, v4, v3, v2, v1);           \
+                            weno5_pair_##SUF(v0, v1, v2, v3, v4, v5, &WL[c], &WR[c]); \
                         }                                                      \
                         rusanov_##SUF(WL, WR, d, gamma, igm1, F);              \
                         const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z); \

@@ -12,8 +12,8 @@
 
 #include <math.h>
 
-#define DEFINE_EULER_MATH(SUF, T, FMA, SQRT, FABS, FMAX)                            \
-    static inline T weno5_##SUF(T v0, T v1, T v2, T v3, T v4)                         \
+#define DEFINE_EULER_MATH(SUF, T, FMA, SQRT, FABS, FMAX, SHARED_DIV)                            \
+    static inline void weno5_nd_##SUF(T v0, T v1, T v2, T v3, T v4, T *num, T *den) \
     {                                                                          \
         const T c1312 = (T)(13.0 / 12.0), quarter = (T)0.25, eps = (T)1e-6;    \
         const T d0 = (T)0.1, d1 = (T)0.6, d2 = (T)0.3, six = (T)6;             \
@@ -33,9 +33,27 @@
         const T n0 = FMA((T)2, v0, FMA((T)-7, v1, (T)11 * v2));                \
         const T n1 = FMA((T)5, v2, FMA((T)2, v3, -v1));                        \
         const T n2 = FMA((T)2, v2, FMA((T)5, v3, -v4));                        \
-        const T num = FMA(w0, n0, FMA(w1, n1, w2 * n2));                       \
-        const T den = six * ((w0 + w1) + w2);                                  \
-        return num / den;                                                      \
+        *num = FMA(w0, n0, FMA(w1, n1, w2 * n2));                              \
+        *den = six * ((w0 + w1) + w2);                                         \
+    }                                                                          \
+                                                                               \
+    /* left and right states at the face between v2 and v3 (v0..v5 =         \
+     * v[i-2..i+3]); SHARED_DIV: one division for both, as the device's FP64  \
+     * path does, else one division each (FP32) */                            \
+    static inline void weno5_pair_##SUF(T v0, T v1, T v2, T v3, T v4, T v5,    \
+                                        T *vl, T *vr)                          \
+    {                                                                          \
+        T nl, dl, nr, dr;                                                      \
+        weno5_nd_##SUF(v0, v1, v2, v3, v4, &nl, &dl);                          \
+        weno5_nd_##SUF(v5, v4, v3, v2, v1, &nr, &dr);                          \
+        if (SHARED_DIV) {                                                      \
+            const T inv = (T)1 / (dl * dr);                                    \
+            *vl = (nl * dr) * inv;                                             \
+            *vr = (nr * dl) * inv;                                             \
+        } else {                                                               \
+            *vl = nl / dl;                                                     \
+            *vr = nr / dr;                                                     \
+        }                                                                      \
     }                                                                          \
                                                                                \
     static inline void rusanov_##SUF(const T *WL, const T *WR, int d, T gamma,        \
@@ -88,7 +106,7 @@
         W[4] = gm1 * (E - ke);                                                 \
     }                                                                          \
 
-DEFINE_EULER_MATH(f64, double, fma, sqrt, fabs, fmax)
-DEFINE_EULER_MATH(f32, float, fmaf, sqrtf, fabsf, fmaxf)
+DEFINE_EULER_MATH(f64, double, fma, sqrt, fabs, fmax, 1)
+DEFINE_EULER_MATH(f32, float, fmaf, sqrtf, fabsf, fmaxf, 0)
 
 #endif

@@ -236,8 +236,7 @@ double eulerStage<double>(const int nb[3], const int n[3], const double *Us, con
                                     const T *P = prim.data() + c * le + li;
                                     const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st];
                                     const T v3 = P[0], v4 = P[st], v5 = P[2 * st];
-                                    WL[c] = weno5_f64(v0, v1, v2, v3, v4);
-                                    WR[c] = weno5_f64(v5, v4, v3, v2, v1);
+                                    weno5_pair_f64(v0, v1, v2, v3, v4, v5, &WL[c], &WR[c]);
                                 }
                                 rusanov_f64(WL, WR, d, gam, igm1, F);
                                 const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
