@@ -11,6 +11,8 @@ descriptions; FP64 unless stated):
          stage update; BCs x periodic, y absorbing, z Dirichlet (far field).
          Metric counts cell-updates per RK stage.
   c4     the same Euler step at 1024^3 cells (32^3 blocks of 32^3), FP32.
+  c3     two-level AMR layout, 2136 blocks of 8^3/16^3/32^3 cells, FP64 Euler,
+         one CUDA graph (3 persistent launches) per SSP-RK3 step.
   c1     128^3 cells = 8^3 blocks of 16^3, one scalar, lab (-1,2) + 7-point
          Laplacian + central gradient fused (one kernel per step).
 
@@ -394,7 +396,104 @@ class C4(Euler):
     bytes_per_cell_step = (80 + 120 + 120) // 2
 
 
-WORKLOADS = {"c1": C1, "c2": C2, "c4": C4}
+class C3:
+    """Batched two-level AMR step: 2136 blocks of 8^3/16^3/32^3 cells (seeded
+    octree, 652 on the refined level), level-interface ghosts by trilinear
+    prolongation and conservative restriction, FP64 Euler; each SSP-RK3 step
+    is one CUDA graph of three persistent launches over the tile work list,
+    schedule chosen by the autotuner."""
+    name = "c3"
+    desc = ("AMR Euler SSP-RK3 step, 2136 blocks of {8,16,32}^3 cells on 2 levels (18.3 M cells), FP64, "
+            "interface ghosts by trilinear prolongation / conservative restriction, one CUDA graph per step "
+            "(3 persistent launches), autotuned schedule")
+    dtype = "f64"
+    stages = 3
+    launches_per_step = 3
+    bytes_per_cell_step = 320
+    nb, n = ("amr", "amr")
+
+    def __init__(self):
+        import torch
+
+        import cubismnova_b200 as cn
+        self.cn, self.torch = cn, torch
+        l, c, o, F = cn.workloads.amr_layout()
+        self.U = cn.amr.AmrGrid(l, c, o, F)
+        self.w1, self.w2 = self.U.like(), self.U.like()
+        cn.workloads.euler_pulse_amr(self.U)
+        self.cells = self.U.total_cells
+        self.updates_per_step = self.cells * self.stages
+        self.flops_per_cell_stage = EULER_FLOPS_PER_CELL_STAGE
+        self.nb, self.n = (len(l),), (int(F),)
+        # CFL on the fine level (h = 1/F), sound speed of the pulse state < 1.3
+        self.dt = 0.3 / (3 * 1.3 * F)
+        order, ctas, ms = cn.amr.autotune(self.U, self.w1, self.w2, self.dt, reps=2)
+        self.schedule = dict(order=["block order", "largest blocks first", "Morton"][order], ctas=ctas,
+                             ms_per_step=round(ms, 3))
+        cn.workloads.euler_pulse_amr(self.U)
+        self.stream = torch.cuda.Stream()
+        cn.amr.rk3_step(self.U, self.w1, self.w2, self.dt, stream=self.stream)  # eager once before capture
+        self.stream.synchronize()
+        cn.workloads.euler_pulse_amr(self.U)
+        self.graph = cn.amr.Graph.capture(
+            lambda: cn.amr.rk3_step(self.U, self.w1, self.w2, self.dt, stream=self.stream), self.stream)
+        self.h_state = None
+        self.desc = self.desc + f"; schedule {self.schedule}"
+
+    def needs_flush(self):
+        return False
+
+    def step(self, stream, events=None):
+        if events is not None:
+            events[0].record(stream)
+        self.graph.launch(stream)
+        if events is not None:
+            for e in events[1:]:
+                e.record(stream)
+
+    def e2e_step(self, stream):
+        torch = self.torch
+        if self.h_state is None:
+            self.h_state = torch.empty((5, self.U.comp_stride), dtype=torch.float64).pin_memory()
+            for k in range(5):
+                self.h_state[k].copy_(self.U.tensor(k))
+        with torch.cuda.stream(stream):
+            for k in range(5):
+                self.U.tensor(k).copy_(self.h_state[k], non_blocking=True)
+            self.graph.launch(stream)
+            for k in range(5):
+                self.h_state[k].copy_(self.U.tensor(k), non_blocking=True)
+        nbytes = 5 * self.U.comp_stride * 8
+        return nbytes, nbytes
+
+    @classmethod
+    def cpu_sample_static(cls, threads, reps=1):
+        """The C oracle (no reference AMR code exists) on the small two-level
+        layout (99 blocks, 104 k cells), one RK3 stage, 1 thread."""
+        import oracle as O
+
+        from cubismnova_b200 import workloads as WL
+        l, c, o, F = WL.amr_small_layout()
+        blk, tot = O.amr_blocks(l, c, o, F)
+        rng = np.random.default_rng(0)
+        U = np.zeros((5, tot))
+        U[0] = 1 + 0.1 * rng.random(tot)
+        U[4] = 2.5
+        best = 1e300
+        for _ in range(max(1, reps)):
+            t0 = time.perf_counter()
+            O.amr_stage(U, U, blk, F, 2, 1e-4, 1.4)
+            best = min(best, time.perf_counter() - t0)
+        return dict(value=tot / best / 1e9, unit="Gcell-updates/s", cores=1, kind="port",
+                    sample=f"one SSP-RK3 stage of the C oracle on the small two-level layout ({len(l)} blocks, "
+                           f"{tot} cells), 1 thread, best of {max(1, reps)}",
+                    seconds_per_sweep=best)
+
+    def cpu_sample(self, threads):
+        return self.cpu_sample_static(threads)
+
+
+WORKLOADS = {"c1": C1, "c2": C2, "c3": C3, "c4": C4}
 DEFAULT_WORKLOAD = "c2"
 
 

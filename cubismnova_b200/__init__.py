@@ -16,5 +16,6 @@ from . import euler
 from . import workloads
 from . import mg
 from . import learned
+from . import amr
 
-__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "CnError", "build"]
+__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "amr", "CnError", "build"]

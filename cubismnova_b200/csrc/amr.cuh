@@ -1,0 +1,93 @@
+// amr.cuh -- ghost cells of blocks on two refinement levels (ratio 2).
+//
+// A layout is a set of cubic blocks tiling a periodic box; each block has a
+// level (0 coarse, 1 fine; cell size 2 or 1 in level-1 units), n^3 cells and
+// an origin in level-1 cell units (multiples of 8).  A lookup grid with one
+// entry per 8^3 level-1 cells maps a position to the block that covers it.
+// A ghost cell of block b takes its value from the block s covering it:
+//   same level   copy of the cell;
+//   s coarser    trilinear prolongation from s (cell-centred weights 3/4, 1/4
+//                per direction, x then y then z), the stencil's neighbour
+//                index clamped to s's cells;
+//   s finer      conservative restriction: mean of the 8 fine cells,
+//                ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)), child c = dx|dy<<1|dz<<2.
+// The reference describes level interfaces only in notes
+// (test/sandbox/doc/notes/01_notes.md:192-196); this is the standard
+// block-structured AMR ghost fill.
+#pragma once
+
+#include <cstdint>
+
+namespace cn {
+namespace amr {
+
+struct BlockDev {
+    int level;  // 0 or 1
+    int n;      // cells per dimension
+    int ox, oy, oz; // origin in level-1 cell units
+    int pad;
+    int64_t off; // element offset of the block in each component
+    double ih;   // 1 / h
+};
+
+struct Geom {
+    const BlockDev *blk;
+    const int32_t *lookup; // lres^3 block ids
+    int L1;                // domain extent in level-1 cells (periodic)
+    int lres;              // L1 / 8
+};
+
+__device__ __forceinline__ int wrap(int x, int L) { return x < 0 ? x + L : (x >= L ? x - L : x); }
+__device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+template <typename T>
+__device__ __forceinline__ T cell(const T *comp, const BlockDev &B, int x, int y, int z)
+{
+    return comp[B.off + x + (int64_t)B.n * (y + (int64_t)B.n * z)];
+}
+
+// value of lab cell q (tile coordinates of block b, possibly outside it)
+template <typename T>
+__device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, int qy, int qz)
+{
+    const BlockDev B = A.blk[b];
+    if ((unsigned)qx < (unsigned)B.n && (unsigned)qy < (unsigned)B.n && (unsigned)qz < (unsigned)B.n)
+        return cell<T>(comp, B, qx, qy, qz);
+    const int cs = B.level == 0 ? 2 : 1;
+    const int X = wrap(B.ox + qx * cs, A.L1), Y = wrap(B.oy + qy * cs, A.L1), Z = wrap(B.oz + qz * cs, A.L1);
+    const int s = A.lookup[(X >> 3) + A.lres * ((Y >> 3) + A.lres * (Z >> 3))];
+    const BlockDev S = A.blk[s];
+    const int fx = X - S.ox, fy = Y - S.oy, fz = Z - S.oz; // level-1 units inside S
+    if (S.level == B.level) {
+        const int css = S.level == 0 ? 2 : 1;
+        return cell<T>(comp, S, fx / css, fy / css, fz / css);
+    }
+    if (S.level < B.level) {
+        // fine ghost cell inside a coarse block: trilinear prolongation
+        const int px = fx >> 1, py = fy >> 1, pz = fz >> 1;
+        const int qx1 = clampi(px + ((fx & 1) ? 1 : -1), 0, S.n - 1);
+        const int qy1 = clampi(py + ((fy & 1) ? 1 : -1), 0, S.n - 1);
+        const int qz1 = clampi(pz + ((fz & 1) ? 1 : -1), 0, S.n - 1);
+        const T e000 = cell<T>(comp, S, px, py, pz), e100 = cell<T>(comp, S, qx1, py, pz);
+        const T e010 = cell<T>(comp, S, px, qy1, pz), e110 = cell<T>(comp, S, qx1, qy1, pz);
+        const T e001 = cell<T>(comp, S, px, py, qz1), e101 = cell<T>(comp, S, qx1, py, qz1);
+        const T e011 = cell<T>(comp, S, px, qy1, qz1), e111 = cell<T>(comp, S, qx1, qy1, qz1);
+        const T a = T(0.75), c = T(0.25);
+        const T a0 = a * e000 + c * e100;
+        const T a1 = a * e010 + c * e110;
+        const T a2 = a * e001 + c * e101;
+        const T a3 = a * e011 + c * e111;
+        const T b0 = a * a0 + c * a1;
+        const T b1 = a * a2 + c * a3;
+        return a * b0 + c * b1;
+    }
+    // coarse ghost cell over a fine block: mean of its 8 children
+    T v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        v[k] = cell<T>(comp, S, fx + (k & 1), fy + ((k >> 1) & 1), fz + (k >> 2));
+    return (((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]))) * T(0.125);
+}
+
+} // namespace amr
+} // namespace cn

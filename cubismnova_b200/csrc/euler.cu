@@ -20,6 +20,7 @@
 #include "cn_internal.h"
 #include "cn_tma.cuh"
 #include "euler_math.cuh"
+#include "euler_stage.cuh"
 
 #include <cstring>
 #include <mutex>
@@ -27,260 +28,14 @@
 namespace cn {
 namespace euler {
 
-constexpr int TB = 8;                 // tile edge
-constexpr int G = 3;                  // ghost width
-constexpr int NCORE = TB * TB * TB;   // tile cells: 512
-constexpr int NHALO = 2 * G * TB * TB; // one direction's halo slabs: 384
-constexpr int SV = NCORE + NHALO;     // staged cells per variable: 896
-constexpr int NCELL = TB * TB * TB;   // 512
-constexpr int NFACE = (TB + 1) * TB * TB; // 576
-constexpr int NT = 192;               // threads per CTA (576 = 3 * 192)
-constexpr int CPT = (NCELL + NT - 1) / NT; // cells per thread: 3
-
-template <typename T> struct StageParams {
-    const T *U[5];   // state whose lab is loaded (component bases)
-    const T *Un[5];  // U^n (stages 2 and 3)
-    T *out[5];
-    BcView bc[5];
-    LabGeom L;
-    T ih[3];
-    T dt;
-    T gamma, gm1, igm1;
-    int stage;       // 0: out = L(U); 1..3: SSP-RK3 stage
-    double *partials; // per-CTA FP64 sums of the 5 outputs (may be null)
-    int *err;
-};
-
-// Shared-memory index of tile-local cell (x, y, z) while direction D is being
-// swept: the core cells, then the two 3-cell halo slabs of direction D (only
-// one direction's halo is staged at a time; the slot is reloaded per sweep).
-template <int D> __device__ __forceinline__ int sidx(int x, int y, int z)
-{
-    const int c = D == 0 ? x : (D == 1 ? y : z);
-    if ((unsigned)c < (unsigned)TB) return x + TB * (y + TB * z);
-    const int h = c < 0 ? c + G : c - TB + G; // 0..5
-    if (D == 0) return NCORE + (z * TB + y) * (2 * G) + h;
-    if (D == 1) return NCORE + (z * (2 * G) + h) * TB + x;
-    return NCORE + (h * TB + y) * TB + x;
-}
-
-// tile-local coordinates of halo slot i of direction D
-template <int D> __device__ __forceinline__ void halo_cell(int i, int &x, int &y, int &z)
-{
-    int h;
-    if (D == 0) {
-        h = i % (2 * G);
-        y = (i / (2 * G)) % TB;
-        z = i / (2 * G * TB);
-        x = h < G ? h - G : h - G + TB;
-    } else if (D == 1) {
-        x = i % TB;
-        h = (i / TB) % (2 * G);
-        z = i / (TB * 2 * G);
-        y = h < G ? h - G : h - G + TB;
-    } else {
-        x = i % TB;
-        y = (i / TB) % TB;
-        h = i / (TB * TB);
-        z = h < G ? h - G : h - G + TB;
-    }
-}
-
-// Face fluxes of direction D for the whole tile (one thread per face, each
-// face once), then flux differences into the per-cell accumulators.
-template <typename T, int D>
-__device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F, T (&acc)[CPT][5],
-                                      T gamma, T igm1, T ihd)
-{
-    for (int f = threadIdx.x; f < NFACE; f += NT) {
-        int x, y, z;
-        if (D == 0) {
-            x = f % (TB + 1);
-            y = (f / (TB + 1)) % TB;
-            z = f / ((TB + 1) * TB);
-        } else if (D == 1) {
-            x = f % TB;
-            y = (f / TB) % (TB + 1);
-            z = f / (TB * (TB + 1));
-        } else {
-            x = f % TB;
-            y = (f / TB) % TB;
-            z = f / (TB * TB);
-        }
-        // cells i-2 .. i+3 around the face between cell i = (x,y,z)-e_D and (x,y,z)
-        int idx[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const int o = k - 3;
-            idx[k] = D == 0 ? sidx<0>(x + o, y, z) : (D == 1 ? sidx<1>(x, y + o, z) : sidx<2>(x, y, z + o));
-        }
-        T WL[5], WR[5];
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            const T *Wc = W + c * SV;
-            const T v0 = Wc[idx[0]], v1 = Wc[idx[1]], v2 = Wc[idx[2]];
-            const T v3 = Wc[idx[3]], v4 = Wc[idx[4]], v5 = Wc[idx[5]];
-            weno5_pair(v0, v1, v2, v3, v4, v5, WL[c], WR[c]);
-        }
-        T Fl[5];
-        rusanov<T>(WL, WR, D, gamma, igm1, Fl);
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            F[c * NFACE + f] = Fl[c];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const int cidx = threadIdx.x + k * NT;
-        if (cidx < NCELL) {
-            const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
-            const int flo = D == 0 ? x + (TB + 1) * (y + TB * z)
-                                   : (D == 1 ? x + TB * (y + (TB + 1) * z) : x + TB * (y + TB * z));
-            constexpr int step = D == 0 ? 1 : (D == 1 ? TB : TB * TB);
-#pragma unroll
-            for (int c = 0; c < 5; ++c) {
-                const T df = F[c * NFACE + flo + step] - F[c * NFACE + flo];
-                acc[k][c] = D == 0 ? df * ihd : dfma(df, ihd, acc[k][c]);
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// Loads the two 3-cell halo slabs of direction D into the halo slot:
-// cells inside the block are plain loads, cells outside are resolved by
-// cn::lab_value (periodic neighbour, skip rule, BC chain per component).
-template <typename T, int D>
-__device__ __forceinline__ void stage_halo(const StageParams<T> &p, T *W, int block, int bx, int by, int bz, int x0,
-                                           int y0, int z0, int64_t boff)
-{
-    const LabGeom &L = p.L;
-    const int N0 = L.n[0], N1 = L.n[1], N2 = L.n[2];
-    for (int i = threadIdx.x; i < NHALO; i += NT) {
-        int x, y, z;
-        halo_cell<D>(i, x, y, z);
-        const int gx = x0 + x, gy = y0 + y, gz = z0 + z;
-        T u[5];
-        if ((unsigned)gx < (unsigned)N0 && (unsigned)gy < (unsigned)N1 && (unsigned)gz < (unsigned)N2) {
-            const int64_t o = boff + gx + (int64_t)N0 * (gy + (int64_t)N1 * gz);
-#pragma unroll
-            for (int c = 0; c < 5; ++c)
-                u[c] = p.U[c][o];
-        } else {
-#pragma unroll
-            for (int c = 0; c < 5; ++c) {
-                if (!lab_value<T>(p.U[c], L, p.bc[c], block, bx, by, bz, gx, gy, gz, true, u[c]))
-                    u[c] = T(0);
-            }
-        }
-        T w[5];
-        to_primitive<T>(u[0], u[1], u[2], u[3], u[4], p.gm1, w);
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            W[c * SV + NCORE + i] = w[c];
-    }
-}
-
 template <typename T>
-__global__ void __launch_bounds__(NT, 3) stage_kernel(StageParams<T> p)
+__global__ void __launch_bounds__(NT, 3) stage_kernel(StageParams<T> p, CartSrc src)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T *W = reinterpret_cast<T *>(smem_raw);       // [5][SV]
-    T *F = W + 5 * SV;                            // [5][NFACE]
+    T *W = reinterpret_cast<T *>(smem_raw); // [5][Stg<T>::SV]
+    T *F = W + 5 * Stg<T>::SV;              // [5][NFACE]
     __shared__ double red[NT / 32][5];
-
-    const LabGeom &L = p.L;
-    const int N0 = L.n[0], N1 = L.n[1], N2 = L.n[2];
-    const int tx = N0 / TB, ty = N1 / TB, tz = N2 / TB;
-    const int tiles = tx * ty * tz;
-    const int block = blockIdx.x / tiles;
-    int t = blockIdx.x - block * tiles;
-    const int x0 = (t % tx) * TB;
-    t /= tx;
-    const int y0 = (t % ty) * TB;
-    const int z0 = (t / ty) * TB;
-    const int bx = block % L.nb[0];
-    const int by = (block / L.nb[0]) % L.nb[1];
-    const int bz = block / (L.nb[0] * L.nb[1]);
-    const int64_t boff = (int64_t)block * L.bstride;
-
-    // ---- stage the tile's cells as primitives (the halo slot follows per sweep)
-    for (int i = threadIdx.x; i < NCORE; i += NT) {
-        const int x = i % TB, y = (i / TB) % TB, z = i / (TB * TB);
-        const int64_t o = boff + (x0 + x) + (int64_t)N0 * ((y0 + y) + (int64_t)N1 * (z0 + z));
-        T w[5];
-        to_primitive<T>(p.U[0][o], p.U[1][o], p.U[2][o], p.U[3][o], p.U[4][o], p.gm1, w);
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            W[c * SV + i] = w[c];
-    }
-    stage_halo<T, 0>(p, W, block, bx, by, bz, x0, y0, z0, boff);
-    __syncthreads();
-
-    T acc[CPT][5];
-#pragma unroll
-    for (int k = 0; k < CPT; ++k)
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            acc[k][c] = T(0);
-
-    sweep<T, 0>(W, F, acc, p.gamma, p.igm1, p.ih[0]);
-    stage_halo<T, 1>(p, W, block, bx, by, bz, x0, y0, z0, boff);
-    __syncthreads();
-    sweep<T, 1>(W, F, acc, p.gamma, p.igm1, p.ih[1]);
-    stage_halo<T, 2>(p, W, block, bx, by, bz, x0, y0, z0, boff);
-    __syncthreads();
-    sweep<T, 2>(W, F, acc, p.gamma, p.igm1, p.ih[2]);
-
-    // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows
-    double sums[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const int cidx = threadIdx.x + k * NT;
-        if (cidx < NCELL) {
-            const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
-            const int64_t o = boff + (x0 + x) + (int64_t)N0 * ((y0 + y) + (int64_t)N1 * (z0 + z));
-#pragma unroll
-            for (int c = 0; c < 5; ++c) {
-                const T rhs = -acc[k][c];
-                T v;
-                if (p.stage == 0) {
-                    v = rhs;
-                } else {
-                    const T us = p.U[c][o];
-                    const T tt = dfma(p.dt, rhs, us);
-                    if (p.stage == 1) {
-                        v = tt;
-                    } else if (p.stage == 2) {
-                        v = dfma(T(0.75), p.Un[c][o], T(0.25) * tt);
-                    } else {
-                        v = dfma(T(1.0 / 3.0), p.Un[c][o], T(2.0 / 3.0) * tt);
-                    }
-                }
-                p.out[c][o] = v;
-                sums[c] += (double)v;
-            }
-        }
-    }
-    if (p.partials) {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            double s = sums[c];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1)
-                s += __shfl_down_sync(0xffffffffu, s, off);
-            if (lane == 0)
-                red[warp][c] = s;
-        }
-        __syncthreads();
-        if (threadIdx.x < 5) {
-            double s = 0;
-            for (int w = 0; w < NT / 32; ++w)
-                s += red[w][threadIdx.x];
-            p.partials[(int64_t)blockIdx.x * 5 + threadIdx.x] = s;
-        }
-    }
+    stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, F, red);
 }
 
 // Fixed-order reduction of per-CTA partials: out[c] = sum_i partials[i][c].
@@ -365,15 +120,16 @@ static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, 
     r = sync_bc(bcsrc, st);
     if (r != CN_OK) return r;
     StageParams<T> p = {};
-    p.L = make_geom(Us, &s);
+    CartSrc src;
+    src.L = make_geom(Us, &s);
     for (int c = 0; c < 5; ++c) {
         p.U[c] = reinterpret_cast<const T *>(Us->d_data) + (size_t)(cs + c) * Us->comp_stride;
         p.Un[c] = Un ? reinterpret_cast<const T *>(Un->d_data) + (size_t)(cn_ + c) * Un->comp_stride
                      : nullptr;
         p.out[c] = reinterpret_cast<T *>(out->d_data) + (size_t)(co + c) * out->comp_stride;
-        p.bc[c] = bc_view(bcsrc, cs + c);
+        src.bc[c] = bc_view(bcsrc, cs + c);
     }
-    for (int d = 0; d < 3; ++d) p.ih[d] = (T)(1.0 / Us->h[d]);
+    for (int d = 0; d < 3; ++d) src.ih[d] = 1.0 / Us->h[d];
     p.dt = (T)dt;
     p.gamma = (T)gamma;
     p.gm1 = (T)(gamma - 1.0);
@@ -381,10 +137,15 @@ static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, 
     p.stage = stage;
     p.partials = partials;
     p.err = Us->d_err;
-    const size_t smem = (size_t)(5 * SV + 5 * NFACE) * sizeof(T);
-    CN_CUDA_TRY(cudaFuncSetAttribute(stage_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = (size_t)(5 * Stg<T>::SV + 5 * NFACE) * sizeof(T);
+    // set once (outside any graph capture: the first call is an eager one)
+    static bool attr_done = false;
+    if (!attr_done) {
+        CN_CUDA_TRY(cudaFuncSetAttribute(stage_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_done = true;
+    }
     const int64_t ctas = (int64_t)Us->nblocks * (Us->n[0] / TB) * (Us->n[1] / TB) * (Us->n[2] / TB);
-    stage_kernel<T><<<(unsigned)ctas, NT, smem, st>>>(p);
+    stage_kernel<T><<<(unsigned)ctas, NT, smem, st>>>(p, src);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }

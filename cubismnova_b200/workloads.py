@@ -151,3 +151,109 @@ def _global_to_blocks(g: Cartesian, arr, torch):
     v = arr.reshape(nb[2], n[2], nb[1], n[1], nb[0], n[0]).permute(0, 2, 4, 1, 3, 5).reshape(g.size(), cells)
     g.tensor(0)[:, :cells].copy_(v.to(g.tensor(0).dtype))
     torch.cuda.synchronize()
+
+
+def amr_layout(seed: int = 1, roots: int = 8, keep_root: float = 0.9, keep16: float = 0.8,
+               split16_in: float = 0.5, split32_in: float = 0.3, radius: float = 0.15,
+               centre=(0.5, 0.5, 0.5)):
+    """Two-level block layout of the periodic unit box by seeded octree splitting.
+
+    The box is cut into roots^3 cubes of edge 1/roots; with F = 64 * roots
+    level-1 cells across the box, a cube of edge F/roots/2^k (level-1 cells)
+    becomes one block.  Outside a sphere (radius, centre) blocks are level 0
+    (cell = 2 level-1 cells): a root stays one 32^3 block with probability
+    keep_root, else its 16^3 children stay with probability keep16, else they
+    split into 8^3 blocks.  Inside the sphere blocks are level 1: 1/16-edge
+    cubes stay 32^3 blocks unless split (split16_in), 1/32-edge cubes stay
+    16^3 unless split (split32_in) into 8^3 blocks.  The defaults give 2045
+    blocks (55 % 8^3, 21 % 16^3, 24 % 32^3, 651 on level 1, 18.3 M cells).
+    Returns (levels, cells, origins, F)."""
+    rng = np.random.default_rng(seed)
+    F = 64 * roots
+    levels, cells, origins = [], [], []
+    c = np.array(centre)
+
+    def inside(o, s):
+        d = (np.array(o) + s / 2) / F - c
+        d -= np.round(d)
+        return np.linalg.norm(d) < radius
+
+    def leaf(level, n, o):
+        levels.append(level)
+        cells.append(n)
+        origins.append(o)
+
+    def rec(o, s):  # s: edge in level-1 cells
+        l1 = inside(o, s)
+        if s == 64:
+            if not l1 and rng.random() < keep_root:
+                return leaf(0, 32, o)
+        elif s == 32:
+            if l1:
+                if rng.random() > split16_in:
+                    return leaf(1, 32, o)
+            elif rng.random() < keep16:
+                return leaf(0, 16, o)
+        elif s == 16:
+            if not l1:
+                return leaf(0, 8, o)
+            if rng.random() > split32_in:
+                return leaf(1, 16, o)
+        else:
+            return leaf(1, 8, o)
+        h = s // 2
+        for k in range(8):
+            rec((o[0] + (k & 1) * h, o[1] + ((k >> 1) & 1) * h, o[2] + (k >> 2) * h), h)
+
+    for k in range(roots):
+        for j in range(roots):
+            for i in range(roots):
+                rec((64 * i, 64 * j, 64 * k), 64)
+    return np.array(levels), np.array(cells), np.array(origins), F
+
+
+def amr_small_layout(seed: int = 3):
+    """A small two-level layout (box of 64 level-1 cells) with every kind of
+    interface, for parity tests: 2^3 roots of edge 32 become a level-0 16^3
+    block, or level-0 8^3 / level-1 16^3 children, or level-1 8^3 blocks."""
+    rng = np.random.default_rng(seed)
+    levels, cells, origins = [], [], []
+    for k in range(2):
+        for j in range(2):
+            for i in range(2):
+                o = (32 * i, 32 * j, 32 * k)
+                r = rng.random()
+                if r < 0.3:
+                    levels.append(0), cells.append(16), origins.append(o)
+                    continue
+                for c in range(8):
+                    oc = (o[0] + (c & 1) * 16, o[1] + ((c >> 1) & 1) * 16, o[2] + (c >> 2) * 16)
+                    r2 = rng.random()
+                    if r2 < 0.4:
+                        levels.append(0), cells.append(8), origins.append(oc)
+                    elif r2 < 0.7:
+                        levels.append(1), cells.append(16), origins.append(oc)
+                    else:
+                        for g in range(8):
+                            og = (oc[0] + (g & 1) * 8, oc[1] + ((g >> 1) & 1) * 8, oc[2] + (g >> 2) * 8)
+                            levels.append(1), cells.append(8), origins.append(og)
+    return np.array(levels), np.array(cells), np.array(origins), 64
+
+
+def euler_pulse_amr(U, seed: int = 1234, amp: float = 0.5, sigma: float = 0.1, noise: float = 1e-2,
+                    gamma: float = 1.4, centre=(0.5, 0.5, 0.5)):
+    """The Euler pulse state on an AMR layout (periodic minimum-image distance)."""
+    import torch
+    x, y, z = U.cell_centres()
+    d = [x - centre[0], y - centre[1], z - centre[2]]
+    r2 = sum((t - torch.round(t)) ** 2 for t in d)
+    rho = 1.0 + amp * torch.exp(-r2 / (2 * sigma * sigma))
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    vel = [(torch.rand(rho.shape, generator=gen, device="cuda", dtype=torch.float64) * 2 - 1) * noise
+           for _ in range(3)]
+    ke = 0.5 * rho * (vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)
+    U.tensor(0).copy_(rho.to(U.tensor(0).dtype))
+    for k in range(3):
+        U.tensor(1 + k).copy_((rho * vel[k]).to(U.tensor(0).dtype))
+    U.tensor(4).copy_((1.0 / (gamma - 1.0) + ke).to(U.tensor(0).dtype))
+    torch.cuda.synchronize()

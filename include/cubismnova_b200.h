@@ -262,6 +262,48 @@ cn_status cn_mg_collect_patches(cn_mg *m, const cn_grid *f, int cycles, int per_
  * nn == NULL restores Jacobi everywhere. */
 cn_status cn_mg_set_smoother(cn_mg *m, cn_nn *nn, unsigned level_mask);
 
+/* ----------------------------------------------------- AMR block layouts */
+/* Cubic blocks of uneven sizes on two refinement levels (ratio 2) tiling a
+ * periodic unit box (the reference sketches level interfaces only in its notes,
+ * test/sandbox/doc/notes/01_notes.md:192-196).  Block b: level[b] in {0, 1}
+ * (cell size 2 or 1 level-1 units), cells[b] (a multiple of 8) per dimension,
+ * origin[3b..3b+2] in level-1 units (multiples of 8); fine_extent = the box
+ * in level-1 cells.  Data: ncomp components, blocks contiguous in block order.
+ * Ghost cells: same level copy; coarse source: trilinear prolongation (3/4,
+ * 1/4 weights, stencil clamped to the source block); fine source: mean of the
+ * 8 children (conservative restriction). */
+typedef struct cn_amr cn_amr;
+cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const int *origin, int fine_extent,
+                        int ncomp, cn_dtype dtype, cn_amr **out);
+cn_status cn_amr_destroy(cn_amr *a);
+cn_status cn_amr_info(const cn_amr *a, int64_t *total_cells, int64_t *comp_stride, int *nitems);
+cn_status cn_amr_block_offset(const cn_amr *a, int block, int64_t *offset);
+cn_status cn_amr_data(cn_amr *a, int comp, void **device_ptr);
+/* Dense lab (n+2*ghost)^3 of one block, face ghosts only (corners untouched). */
+cn_status cn_amr_lab_fill(cn_amr *a, int comp, int ghost, int block, void *d_lab, void *stream);
+/* Euler (5 components, periodic box) on the layout: stage 0 = RHS, 1..3 =
+ * SSP-RK3 stages as cn_euler_rk3_stage; one persistent launch per stage over
+ * the 8^3-tile work list of Us. */
+cn_status cn_amr_rk3_stage(cn_amr *Us, cn_amr *Un, cn_amr *out, int stage, double dt, double gamma,
+                           void *stream);
+cn_status cn_amr_rk3_step(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, void *stream);
+/* Work-list order (0 block order, 1 largest blocks first, 2 Morton order of
+ * tiles) and persistent grid (0: one CTA per tile). */
+cn_status cn_amr_set_schedule(cn_amr *a, int order, int ctas);
+/* Times all schedules over `reps` steps (advancing U) and keeps the fastest. */
+cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, int reps,
+                          int *order_out, int *ctas_out, double *ms_out, void *stream);
+
+/* ----------------------------------------------------------- CUDA graphs */
+/* Capture the calls issued on `stream` between begin and end into a graph
+ * (thread-local capture).  Run each captured call once eagerly first, and
+ * synchronise BC tables (cn_bc_sync) before capturing. */
+typedef struct cn_graph cn_graph;
+cn_status cn_graph_begin(void *stream);
+cn_status cn_graph_end(void *stream, cn_graph **out);
+cn_status cn_graph_launch(cn_graph *g, void *stream);
+cn_status cn_graph_destroy(cn_graph *g);
+
 /* ------------------------------------------------- pointwise field ops */
 /* The optimised hooks that Block/FieldOperator.h:149-227 declares (under
  * CUBISM_OPTIMIZED_FIELD_OP) and never defines, with the reference's exact

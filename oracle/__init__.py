@@ -304,3 +304,44 @@ def mg_coarse_cg(f, k, nb, n, ih2, max_iter=10000, rtol=1e-13):
     it = lib().or_mg_coarse_cg(_i3(nb), _i3(n), C.c_int64(block_stride(n, np.float32)), _f32p(f), _f32p(k),
                                C.c_double(ih2), C.c_int(max_iter), C.c_double(rtol), _f32p(p))
     return p, it
+
+
+# ---------------------------------------------------------------------- AMR
+AMR_BLOCK = np.dtype([("level", "<i4"), ("n", "<i4"), ("ox", "<i4"), ("oy", "<i4"), ("oz", "<i4"),
+                      ("pad", "<i4"), ("off", "<i8"), ("ih", "<f8")])
+
+
+def amr_blocks(levels, cells, origins, L1):
+    """Oracle block table (offsets: blocks contiguous in block order)."""
+    nb = len(levels)
+    blk = np.zeros(nb, dtype=AMR_BLOCK)
+    off = 0
+    for b in range(nb):
+        cs = 2 if levels[b] == 0 else 1
+        blk[b] = (levels[b], cells[b], origins[b][0], origins[b][1], origins[b][2], 0, off, L1 / cs)
+        off += cells[b] ** 3
+    return blk, off
+
+
+def amr_lab(comp, blk, L1, b, g):
+    n = int(blk[b]["n"])
+    E = n + 2 * g
+    lab = np.zeros((E, E, E))
+    w = np.zeros((E, E, E), dtype=np.uint8)
+    rc = lib().or_amr_lab_f64(blk.ctypes.data_as(C.c_void_p), C.c_int(len(blk)), C.c_int(L1),
+                              _ptr(np.ascontiguousarray(comp, dtype=np.float64)), C.c_int(b), C.c_int(g),
+                              _ptr(lab), _ptr(w))
+    if rc:
+        raise ValueError("or_amr_lab_f64 failed")
+    return lab, w.astype(bool)
+
+
+def amr_stage(Us, Un, blk, L1, stage, dt, gamma):
+    Us = np.ascontiguousarray(Us, dtype=np.float64)
+    out = np.array(Un, copy=True) if (Un is not None and stage == 3) else np.zeros_like(Us)
+    rc = lib().or_amr_stage_f64(blk.ctypes.data_as(C.c_void_p), C.c_int(len(blk)), C.c_int(L1), _ptr(Us),
+                                _ptr(np.ascontiguousarray(Un)) if Un is not None else None, _ptr(out),
+                                C.c_int64(Us.shape[-1]), C.c_int(stage), C.c_double(dt), C.c_double(gamma))
+    if rc:
+        raise ValueError("or_amr_stage_f64 failed")
+    return out
