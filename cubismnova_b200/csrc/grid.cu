@@ -204,6 +204,27 @@ const char *cn_last_error_string(void) { return g_last_error.c_str(); }
 
 int cn_abi_version(void) { return CN_ABI_VERSION; }
 
+cn_status cn_device_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    CN_CUDA_TRY(cudaMalloc(ptr, bytes));
+    return CN_OK;
+}
+
+cn_status cn_device_free(void *ptr)
+{
+    if (ptr) CN_CUDA_TRY(cudaFree(ptr));
+    return CN_OK;
+}
+
+cn_status cn_memcpy(void *dst, const void *src, size_t bytes, void *stream)
+{
+    if (!dst || !src) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    CN_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, as_stream(stream)));
+    if (!stream) CN_CUDA_TRY(cudaStreamSynchronize(nullptr));
+    return CN_OK;
+}
+
 cn_status cn_stencil_check(const cn_stencil *s) { return check_stencil(s); }
 
 cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int ncomp,

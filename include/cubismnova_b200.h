@@ -73,6 +73,14 @@ typedef struct cn_stencil {
 
 typedef struct cn_grid cn_grid;
 
+/* ------------------------------------------------------- device memory */
+/* Plain device buffers for callers without the CUDA runtime headers (the C++
+ * facade's lab storage).  cn_memcpy copies in any direction (stream NULL:
+ * returns when done). */
+cn_status cn_device_alloc(size_t bytes, void **ptr);
+cn_status cn_device_free(void *ptr);
+cn_status cn_memcpy(void *dst, const void *src, size_t bytes, void *stream);
+
 /* ---------------------------------------------------------------- errors */
 const char *cn_status_string(cn_status s);
 /* Message of the last failed call on this thread ("" if none). */

@@ -1,0 +1,347 @@
+// cubismnova_b200.hpp -- C++ facade of the C ABI with the reference's names.
+//
+// Header-only: a reference user includes this instead of Cubism/Grid/Cartesian.h,
+// Cubism/Block/FieldLab.h, Cubism/BC/*.h and Cubism/Core/Stencil.h and links
+// libcubismnova_b200.so.  Class and method names, argument meaning and the
+// exception messages follow CubismNova; the data lives on the GPU:
+//
+//   Grid::Cartesian<T>     Grid/Cartesian.h:50-550 (device SoA, same layout)
+//   Grid::BlockField<T>    the block field views of Grid/Cartesian.h:334-373
+//                          with getBC() (Block/Field.h:437-442)
+//   Block::FieldLab<T>     Block/FieldLab.h:30-492 (allocate, loadData,
+//                          active ranges, getActiveField, footprint)
+//   BC::Base/Dirichlet/Absorbing/Symmetry   BC/*.h
+//   Core::Stencil          Core/Stencil.h:21-108
+//   Ops::laplacian/gradient/lapGrad/divergence   the benchmark stencils
+//
+// Errors raise std::runtime_error with the reference's message where the
+// reference throws (Core/Stencil.h:101-106, Block/FieldLab.h:189-190,
+// :417-419, Grid/Cartesian.h:162-164).
+#pragma once
+
+#include "cubismnova_b200.h"
+
+#include <array>
+#include <cstddef>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace cubism_b200 {
+
+inline void check(cn_status s)
+{
+    if (s != CN_OK) {
+        const char *m = cn_last_error_string();
+        throw std::runtime_error((m && *m) ? std::string(m) : std::string(cn_status_string(s)));
+    }
+}
+
+template <typename T> struct DType;
+template <> struct DType<double> { static constexpr cn_dtype value = CN_FLOAT64; };
+template <> struct DType<float> { static constexpr cn_dtype value = CN_FLOAT32; };
+template <> struct DType<int> { static constexpr cn_dtype value = CN_INT32; };
+
+using MultiIndex = std::array<int, 3>;
+
+namespace Core {
+/// Core::Stencil(begin, end, tensorial): begin <= 0 inclusive, end > 0 exclusive.
+class Stencil {
+public:
+    Stencil() : Stencil(0, 1, false) {}
+    Stencil(int b, int e, bool tensorial = false) : Stencil(MultiIndex{b, b, b}, MultiIndex{e, e, e}, tensorial) {}
+    Stencil(const MultiIndex &b, const MultiIndex &e, bool tensorial = false)
+    {
+        for (int d = 0; d < 3; ++d) {
+            s_.begin[d] = b[d];
+            s_.end[d] = e[d];
+        }
+        s_.tensorial = tensorial ? 1 : 0;
+        check(cn_stencil_check(&s_));
+    }
+    MultiIndex getBegin() const { return {s_.begin[0], s_.begin[1], s_.begin[2]}; }
+    MultiIndex getEnd() const { return {s_.end[0], s_.end[1], s_.end[2]}; }
+    bool isTensorial() const { return s_.tensorial != 0; }
+    const cn_stencil *raw() const { return &s_; }
+
+private:
+    cn_stencil s_;
+};
+
+/// The subset of Core::IndexRange used by the lab API (begin inclusive, end exclusive).
+struct IndexRange {
+    MultiIndex begin{0, 0, 0}, end{0, 0, 0};
+    MultiIndex getBegin() const { return begin; }
+    MultiIndex getEnd() const { return end; }
+    MultiIndex getExtent() const { return {end[0] - begin[0], end[1] - begin[1], end[2] - begin[2]}; }
+    size_t size() const
+    {
+        const MultiIndex e = getExtent();
+        return (size_t)e[0] * e[1] * e[2];
+    }
+};
+} // namespace Core
+
+namespace BC {
+/// BC::Base (periodic no-op) and the three concrete BCs (BC/Base.h:39-79).
+struct Base {
+    Base(size_t dir, size_t side) : dir(dir), side(side) {}
+    virtual ~Base() = default;
+    virtual cn_bc_kind kind() const { return CN_BC_BASE; }
+    virtual double value() const { return 0.0; }
+    virtual std::string name() const { return "Base"; }
+    size_t dir, side;
+};
+struct Dirichlet : Base {
+    Dirichlet(size_t dir, size_t side, double v) : Base(dir, side), v(v) {}
+    cn_bc_kind kind() const override { return CN_BC_DIRICHLET; }
+    double value() const override { return v; }
+    std::string name() const override { return "Dirichlet"; }
+    double &getValue() { return v; }
+    double v;
+};
+struct Absorbing : Base {
+    using Base::Base;
+    cn_bc_kind kind() const override { return CN_BC_ABSORBING; }
+    std::string name() const override { return "Zeroth-Order Absorbing"; }
+};
+struct Symmetry : Base {
+    Symmetry(size_t dir, size_t side, double sign = 1) : Base(dir, side), sign(sign) {}
+    cn_bc_kind kind() const override { return CN_BC_SYMMETRY; }
+    double value() const override { return sign; }
+    std::string name() const override { return "Symmetry"; }
+    double sign;
+};
+} // namespace BC
+
+namespace Grid {
+
+template <typename T> class Cartesian;
+
+/// The BC vector of one block field: push_back mirrors
+/// field.getBC().push_back(new BC::X(...)); the grid keeps the BC objects.
+template <typename T> class BCVector {
+public:
+    BCVector(Cartesian<T> *g, int comp, int block) : g_(g), comp_(comp), block_(block) {}
+    void push_back(BC::Base *bc);
+    void clear();
+    size_t size() const;
+
+private:
+    Cartesian<T> *g_;
+    int comp_, block_;
+};
+
+/// A block field view (component comp of block `flat`).
+template <typename T> class BlockField {
+public:
+    BlockField(Cartesian<T> *g, int flat, int comp) : g_(g), flat_(flat), comp_(comp) {}
+    struct State {
+        MultiIndex block_index;
+    };
+    State getState() const;
+    Core::IndexRange getIndexRange() const;
+    BCVector<T> getBC() { return BCVector<T>(g_, comp_, flat_); }
+    int flat() const { return flat_; }
+    int comp() const { return comp_; }
+    Cartesian<T> &grid() const { return *g_; }
+
+private:
+    Cartesian<T> *g_;
+    int flat_, comp_;
+};
+
+/// Grid::Cartesian(nblocks, block_cells, begin, end) with ncomp components on the GPU.
+template <typename T> class Cartesian {
+public:
+    Cartesian(const MultiIndex &nblocks, const MultiIndex &block_cells,
+              const std::array<double, 3> &begin = {0, 0, 0}, const std::array<double, 3> &end = {1, 1, 1},
+              int ncomp = 1)
+        : nb_(nblocks), n_(block_cells), ncomp_(ncomp)
+    {
+        check(cn_grid_create(nblocks.data(), block_cells.data(), ncomp, DType<T>::value, begin.data(), end.data(),
+                             &g_));
+        check(cn_grid_layout(g_, &bstride_, &cstride_, nullptr));
+    }
+    Cartesian(const Cartesian &) = delete;
+    Cartesian &operator=(const Cartesian &) = delete;
+    ~Cartesian() { cn_grid_destroy(g_); }
+
+    /// Cartesian::operator= (Grid/Cartesian.h:160-169): copy the block data.
+    void assign(const Cartesian &c, void *stream = nullptr) { check(cn_grid_copy(g_, c.g_, stream)); }
+
+    size_t size() const { return (size_t)nb_[0] * nb_[1] * nb_[2]; }
+    MultiIndex getSize() const { return nb_; }
+    MultiIndex getBlockCells() const { return n_; }
+    std::array<double, 3> getCellSize() const
+    {
+        std::array<double, 3> h;
+        check(cn_grid_cell_size(g_, h.data()));
+        return h;
+    }
+    int flatIndex(const MultiIndex &p) const { return p[0] + nb_[0] * (p[1] + nb_[1] * p[2]); }
+    BlockField<T> operator[](const MultiIndex &p) { return BlockField<T>(this, flatIndex(p), 0); }
+    BlockField<T> operator[](size_t i) { return BlockField<T>(this, (int)i, 0); }
+    BlockField<T> field(size_t i, int comp) { return BlockField<T>(this, (int)i, comp); }
+
+    int64_t blockStride() const { return bstride_; }
+    int64_t componentStride() const { return cstride_; }
+    T *deviceData(int comp = 0)
+    {
+        void *p = nullptr;
+        check(cn_grid_data(g_, comp, &p));
+        return static_cast<T *>(p);
+    }
+    /// Host array in the reference SoA order (componentStride() elements).
+    void upload(const T *host, int comp = 0, void *stream = nullptr)
+    {
+        check(cn_grid_upload(g_, comp, host, sizeof(T) * (size_t)cstride_, stream));
+    }
+    void download(T *host, int comp = 0, void *stream = nullptr) const
+    {
+        check(cn_grid_download(g_, comp, host, sizeof(T) * (size_t)cstride_, stream));
+    }
+    void syncBCs(void *stream = nullptr) { check(cn_bc_sync(g_, stream)); }
+    cn_grid *raw() { return g_; }
+    const cn_grid *raw() const { return g_; }
+    std::vector<std::unique_ptr<BC::Base>> &ownedBCs() { return owned_; }
+
+private:
+    cn_grid *g_ = nullptr;
+    MultiIndex nb_, n_;
+    int ncomp_;
+    int64_t bstride_ = 0, cstride_ = 0;
+    std::vector<std::unique_ptr<BC::Base>> owned_;
+};
+
+template <typename T> void BCVector<T>::push_back(BC::Base *bc)
+{
+    check(cn_bc_push(g_->raw(), comp_, block_, (int)bc->dir, (int)bc->side, bc->kind(), bc->value()));
+    g_->ownedBCs().emplace_back(bc);
+}
+template <typename T> void BCVector<T>::clear() { check(cn_bc_clear(g_->raw(), comp_, block_)); }
+template <typename T> size_t BCVector<T>::size() const
+{
+    int c = 0;
+    check(cn_bc_count(g_->raw(), comp_, block_, &c));
+    return (size_t)c;
+}
+
+template <typename T> typename BlockField<T>::State BlockField<T>::getState() const
+{
+    const MultiIndex nb = g_->getSize();
+    return State{{flat_ % nb[0], (flat_ / nb[0]) % nb[1], flat_ / (nb[0] * nb[1])}};
+}
+template <typename T> Core::IndexRange BlockField<T>::getIndexRange() const
+{
+    Core::IndexRange r;
+    r.end = g_->getBlockCells();
+    return r;
+}
+
+} // namespace Grid
+
+namespace Block {
+/// Block::FieldLab on the device: a dense (active lab range) device buffer.
+template <typename T> class FieldLab {
+public:
+    FieldLab() = default;
+    FieldLab(const FieldLab &) = delete;
+    FieldLab &operator=(const FieldLab &) = delete;
+    ~FieldLab() { release_(); }
+
+    /// Block/FieldLab.h:104-165: the buffer is (re)allocated for the largest lab
+    /// this stencil and range need; a smaller later request reuses it.
+    void allocate(const Core::Stencil &s, const Core::IndexRange &max_range, bool force = false)
+    {
+        s_ = s;
+        const MultiIndex e = max_range.getExtent();
+        size_t need = 1;
+        for (int d = 0; d < 3; ++d) need *= (size_t)(e[d] + 2 - s.getBegin()[d] + s.getEnd()[d] - 1);
+        if (force || need > cap_) {
+            release_();
+            if (cudaMallocWrapper_(need)) throw std::runtime_error("FieldLab: device allocation failed");
+            cap_ = need;
+        }
+        max_ = max_range;
+        allocated_ = true;
+    }
+    bool isAllocated() const { return allocated_; }
+
+    /// Cartesian::loadLab / FieldLab::loadData (Grid/Cartesian.h:412-427,
+    /// Block/FieldLab.h:180-224) for block field `f`.
+    void loadData(Grid::BlockField<T> f, bool apply_bc = true, void *stream = nullptr)
+    {
+        if (!allocated_) throw std::runtime_error("FieldLab: can not load lab data when not allocated first");
+        check(cn_lab_fill(f.grid().raw(), f.comp(), s_.raw(), f.flat(), 1, apply_bc ? 1 : 0, buf_, stream));
+        field_ = f.flat();
+        range_.end = f.grid().getBlockCells();
+    }
+    const Core::Stencil &getActiveStencil() const { return s_; }
+    Core::IndexRange getActiveRange() const { return range_; }
+    Core::IndexRange getActiveLabRange() const
+    {
+        Core::IndexRange r;
+        r.begin = s_.getBegin();
+        for (int d = 0; d < 3; ++d) r.end[d] = range_.end[d] + s_.getEnd()[d] - 1;
+        return r;
+    }
+    int getActiveField() const
+    {
+        if (field_ < 0) throw std::runtime_error("FieldLab: no field loaded");
+        return field_;
+    }
+    Core::IndexRange getMaximumRange() const { return max_; }
+    /// device pointer of the lab (active lab range, x fastest)
+    T *deviceData() { return static_cast<T *>(buf_); }
+
+private:
+    Core::Stencil s_;
+    Core::IndexRange range_, max_;
+    void *buf_ = nullptr;
+    size_t cap_ = 0;
+    bool allocated_ = false;
+    int field_ = -1;
+    int cudaMallocWrapper_(size_t n);
+    void release_();
+};
+} // namespace Block
+
+namespace Ops {
+template <typename T>
+inline void laplacian(Grid::Cartesian<T> &u, Grid::Cartesian<T> &out, int comp = 0, int out_comp = 0,
+                      void *stream = nullptr)
+{
+    check(cn_laplacian(u.raw(), comp, out.raw(), out_comp, stream));
+}
+template <typename T>
+inline void gradient(Grid::Cartesian<T> &u, Grid::Cartesian<T> &out, int comp = 0, int out_comp = 0,
+                     void *stream = nullptr)
+{
+    check(cn_gradient(u.raw(), comp, out.raw(), out_comp, stream));
+}
+template <typename T>
+inline void lapGrad(Grid::Cartesian<T> &u, Grid::Cartesian<T> &lap, Grid::Cartesian<T> &grad, void *stream = nullptr)
+{
+    check(cn_lap_grad(u.raw(), 0, lap.raw(), 0, grad.raw(), 0, stream));
+}
+template <typename T>
+inline void divergence(Grid::Cartesian<T> &v, Grid::Cartesian<T> &out, void *stream = nullptr)
+{
+    check(cn_divergence(v.raw(), 0, out.raw(), 0, stream));
+}
+} // namespace Ops
+
+} // namespace cubism_b200
+
+template <typename T> int cubism_b200::Block::FieldLab<T>::cudaMallocWrapper_(size_t n)
+{
+    return cn_device_alloc(n * sizeof(T), &buf_) == CN_OK ? 0 : 1;
+}
+template <typename T> void cubism_b200::Block::FieldLab<T>::release_()
+{
+    if (buf_) cn_device_free(buf_);
+    buf_ = nullptr;
+    cap_ = 0;
+}

@@ -1,0 +1,111 @@
+// The reference's BC and FieldLab unit-test assertions, through the C++ facade
+// on the GPU (test/UnitTests/BC/DirichletTest.cpp, AbsorbingTest.cpp,
+// SymmetryTest.cpp, Block/FieldLabTest.cpp:223-291).  Exit status 0 = pass.
+#include "cubismnova_b200.hpp"
+
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+using namespace cubism_b200;
+
+static int failures = 0;
+#define EXPECT(c)                                                                  \
+    do {                                                                           \
+        if (!(c)) {                                                                \
+            std::printf("FAILED %s:%d: %s\n", __FILE__, __LINE__, #c);             \
+            ++failures;                                                            \
+        }                                                                          \
+    } while (0)
+
+struct HostLab {
+    std::vector<int> v;
+    int lo, n;
+    int E() const { return n + 2 * lo; }
+    int operator()(int x, int y, int z) const { return v[(x + lo) + E() * ((y + lo) + E() * (z + lo))]; }
+};
+
+static HostLab load(Grid::Cartesian<int> &g, Block::FieldLab<int> &lab)
+{
+    lab.loadData(g[0]);
+    HostLab h;
+    h.lo = 3;
+    h.n = 16;
+    h.v.resize((size_t)h.E() * h.E() * h.E());
+    check(cn_memcpy(h.v.data(), lab.deviceData(), sizeof(int) * h.v.size(), nullptr));
+    return h;
+}
+
+int main()
+{
+    // FieldAndLab fixture: 16^3 iota int field, stencil (-3,4)
+    Grid::Cartesian<int> g({1, 1, 1}, {16, 16, 16});
+    std::vector<int> host(g.componentStride());
+    for (size_t i = 0; i < host.size(); ++i) host[i] = (int)i;
+    g.upload(host.data());
+    Block::FieldLab<int> lab;
+    try {
+        lab.getActiveField();
+        EXPECT(false);
+    } catch (const std::runtime_error &e) {
+        EXPECT(std::string(e.what()) == "FieldLab: no field loaded");
+    }
+    try {
+        lab.loadData(g[0]);
+        EXPECT(false);
+    } catch (const std::runtime_error &e) {
+        EXPECT(std::string(e.what()) == "FieldLab: can not load lab data when not allocated first");
+    }
+    try {
+        Core::Stencil s(1, 4);
+        EXPECT(false);
+    } catch (const std::runtime_error &e) {
+        EXPECT(std::string(e.what()) == "Stencil: begin_ must be <= 0");
+    }
+    const Core::Stencil s(-3, 4);
+    lab.allocate(s, g[0].getIndexRange());
+    // Dirichlet on all six faces (DirichletTest.cpp:38-66)
+    for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) g[0].getBC().push_back(new BC::Dirichlet(d, side, 10 + 2 * d + side));
+    HostLab h = load(g, lab);
+    for (int d = 0; d < 3; ++d)
+        for (int a = 0; a < 16; ++a)
+            for (int b = 0; b < 16; ++b)
+                for (int k = 1; k <= 3; ++k) {
+                    int lo[3] = {a, b, 0}, hi[3] = {a, b, 0};
+                    // the two in-plane coordinates, then the normal one
+                    int q0[3], q1[3];
+                    for (int m = 0, j = 0; m < 3; ++m) {
+                        if (m == d) continue;
+                        q0[m] = q1[m] = (j++ == 0) ? a : b;
+                    }
+                    q0[d] = -k;
+                    q1[d] = 15 + k;
+                    (void)lo;
+                    (void)hi;
+                    EXPECT(h(q0[0], q0[1], q0[2]) == 10 + 2 * d);
+                    EXPECT(h(q1[0], q1[1], q1[2]) == 11 + 2 * d);
+                }
+    // Absorbing and Symmetry (AbsorbingTest.cpp, SymmetryTest.cpp)
+    g[0].getBC().clear();
+    g[0].getBC().push_back(new BC::Absorbing(1, 0));
+    g[0].getBC().push_back(new BC::Symmetry(1, 1, -1));
+    h = load(g, lab);
+    for (int z = 0; z < 16; ++z)
+        for (int x = 0; x < 16; ++x)
+            for (int k = 1; k <= 3; ++k) {
+                EXPECT(h(x, -k, z) == h(x, 0, z));
+                EXPECT(h(x, 15 + k, z) == -h(x, 16 - k, z));
+            }
+    // interior untouched and periodic x ghosts (FieldLabTest.cpp:53-79)
+    for (int z = 0; z < 16; ++z)
+        for (int y = 0; y < 16; ++y) {
+            EXPECT(h(-1, y, z) == h(15, y, z));
+            EXPECT(h(16, y, z) == h(0, y, z));
+            for (int x = 0; x < 16; ++x) EXPECT(h(x, y, z) == host[x + 16 * (y + 16 * z)]);
+        }
+    EXPECT(lab.getActiveLabRange().getBegin()[0] == -3 && lab.getActiveLabRange().getEnd()[2] == 19);
+    EXPECT(lab.getActiveField() == 0);
+    std::printf("%s (%d failures)\n", failures ? "FAIL" : "PASS", failures);
+    return failures ? 1 : 0;
+}

@@ -88,3 +88,14 @@ def test_product_does_not_import_oracle():
         assert not re.search(r"^\s*(import|from)\s+oracle\b", src, flags=re.M), p
     for p in glob.glob(os.path.join(ROOT, "cubismnova_b200", "csrc", "*")):
         assert "cn_oracle" not in open(p).read(), p
+
+
+def test_cpp_facade_compiles():
+    """The C++ facade compiles with the host compiler (no GPU needed)."""
+    import subprocess
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                            os.path.join(ROOT, "tests", "cpp", "facade_test.cpp")],
+                           capture_output=True, text=True, cwd=d)
+        assert r.returncode == 0, r.stderr
