@@ -103,7 +103,9 @@ __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int 
 {
     using C = K<T>;
     const T rl = WL[0], rr = WR[0];
-    const T unl = WL[1 + d], unr = WR[1 + d];
+    // normal velocities (selects, not an index: d is a runtime value)
+    const T unl = d == 0 ? WL[1] : (d == 1 ? WL[2] : WL[3]);
+    const T unr = d == 0 ? WR[1] : (d == 1 ? WR[2] : WR[3]);
     const T pl = WL[4], pr = WR[4];
     // conservative states
     const T mul0 = rl * WL[1], mul1 = rl * WL[2], mul2 = rl * WL[3];

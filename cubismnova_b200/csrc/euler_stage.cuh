@@ -86,22 +86,19 @@ struct CartSrc {
     }
 };
 
-// Shared-memory index of tile-local cell (x, y, z) while direction D is being
-// swept: the core cells, then the two 3-cell halo slabs of direction D (only
-// one direction's halo is staged at a time; the slot is reloaded per sweep).
-template <int D, bool ALL> __device__ __forceinline__ int sidx(int x, int y, int z)
-{
-    const int c = D == 0 ? x : (D == 1 ? y : z);
-    if ((unsigned)c < (unsigned)TB) return x + TB * (y + TB * z);
-    const int h = c < 0 ? c + G : c - TB + G; // 0..5
-    const int base = NCORE + (ALL ? D * NHALO : 0);
-    if (D == 0) return base + (z * TB + y) * (2 * G) + h;
-    if (D == 1) return base + (z * (2 * G) + h) * TB + x;
-    return base + (h * TB + y) * TB + x;
-}
+// Shared-memory layout per variable: the tile's 512 core cells x-fastest,
+// then the halo slot(s).  The halo slot of direction D holds the two 3-cell
+// slabs of that direction, slab coordinate h = 0..5 (cells -3..-1 and 8..10
+// along D) with the same stride along D as the core (1, 8, 64):
+//   D = 0: (z*8 + y)*6 + h,   D = 1: (z*6 + h)*8 + x,   D = 2: (h*8 + y)*8 + x.
+// FP64 keeps one slot and restages it before each sweep; FP32 keeps all three.
+//
+// The direction is a runtime (warp-uniform) value: one copy of the face code
+// serves all three sweeps, which keeps the kernel's hot code small enough for
+// the instruction caches.
 
 // tile-local coordinates of halo slot i of direction D
-template <int D> __device__ __forceinline__ void halo_cell(int i, int &x, int &y, int &z)
+__device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z)
 {
     int h;
     if (D == 0) {
@@ -124,32 +121,41 @@ template <int D> __device__ __forceinline__ void halo_cell(int i, int &x, int &y
 
 // Face fluxes of direction D for the whole tile (one thread per face, each
 // face once), then flux differences into the per-cell accumulators.
-template <typename T, int D>
-__device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F, T (&acc)[CPT][5],
+template <typename T>
+__device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restrict__ F, T (&acc)[CPT][5],
                                       T gamma, T igm1, T ihd)
 {
+    constexpr bool ALL = Stg<T>::all;
+    const int cs = D == 0 ? 1 : (D == 1 ? TB : TB * TB); // stride along D (core and halo slot)
+    const int hslot = NCORE + (ALL ? D * NHALO : 0);
     for (int f = threadIdx.x; f < NFACE; f += NT) {
-        int x, y, z;
+        // (x, y, z): the cell on the high side of face f; a: its coordinate along D
+        int x, y, z, a;
         if (D == 0) {
             x = f % (TB + 1);
             y = (f / (TB + 1)) % TB;
             z = f / ((TB + 1) * TB);
+            a = x;
         } else if (D == 1) {
             x = f % TB;
             y = (f / TB) % (TB + 1);
             z = f / (TB * (TB + 1));
+            a = y;
         } else {
             x = f % TB;
             y = (f / TB) % TB;
             z = f / (TB * TB);
+            a = z;
         }
-        // cells i-2 .. i+3 around the face between cell i = (x,y,z)-e_D and (x,y,z)
+        // row bases: core cell with coordinate 0 along D, halo slab cell h = 0
+        const int cbase = x + TB * (y + TB * z) - a * cs;
+        const int hbase = hslot + (D == 0 ? (z * TB + y) * (2 * G) : (D == 1 ? z * (2 * G * TB) + x : y * TB + x));
+        // cells a-3 .. a+2 along D
         int idx[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const int o = k - 3;
-            constexpr bool ALL = Stg<T>::all;
-            idx[k] = D == 0 ? sidx<0, ALL>(x + o, y, z) : (D == 1 ? sidx<1, ALL>(x, y + o, z) : sidx<2, ALL>(x, y, z + o));
+            const int q = a + k - 3;
+            idx[k] = (unsigned)q < (unsigned)TB ? cbase + q * cs : hbase + (q < 0 ? q + G : q - TB + G) * cs;
         }
         T WL[5], WR[5];
 #pragma unroll
@@ -173,10 +179,9 @@ __device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F
             const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
             const int flo = D == 0 ? x + (TB + 1) * (y + TB * z)
                                    : (D == 1 ? x + TB * (y + (TB + 1) * z) : x + TB * (y + TB * z));
-            constexpr int step = D == 0 ? 1 : (D == 1 ? TB : TB * TB);
 #pragma unroll
             for (int c = 0; c < 5; ++c) {
-                const T df = F[c * NFACE + flo + step] - F[c * NFACE + flo];
+                const T df = F[c * NFACE + flo + cs] - F[c * NFACE + flo];
                 acc[k][c] = D == 0 ? df * ihd : dfma(df, ihd, acc[k][c]);
             }
         }
@@ -185,14 +190,19 @@ __device__ __forceinline__ void sweep(const T *__restrict__ W, T *__restrict__ F
 }
 
 // Loads the two 3-cell halo slabs of direction D into the halo slot:
-// cells inside the block are plain loads, cells outside are resolved by
-// cn::lab_value (periodic neighbour, skip rule, BC chain per component).
-template <typename T, int D, typename Src>
-__device__ __forceinline__ void stage_halo(const StageParams<T> &p, const Src &src, const TileInfo<T> &t, T *W)
+// cells inside the block are plain loads, cells outside are resolved by the
+// source policy (for the Cartesian grid cn::lab_value: periodic neighbour,
+// skip rule, BC chain per component).  The out-of-block path resolves one
+// component at a time into the slot and converts in place, so its code
+// exists once.
+template <typename T, typename Src>
+__device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const Src &src, const TileInfo<T> &t,
+                                           T *W)
 {
+    T *slot = W + NCORE + (Stg<T>::all ? D * NHALO : 0);
     for (int i = threadIdx.x; i < NHALO; i += NT) {
         int x, y, z;
-        halo_cell<D>(i, x, y, z);
+        halo_cell(D, i, x, y, z);
         const int gx = t.x0 + x, gy = t.y0 + y, gz = t.z0 + z;
         T u[5];
         if ((unsigned)gx < (unsigned)t.N0 && (unsigned)gy < (unsigned)t.N1 && (unsigned)gz < (unsigned)t.N2) {
@@ -201,15 +211,18 @@ __device__ __forceinline__ void stage_halo(const StageParams<T> &p, const Src &s
             for (int c = 0; c < 5; ++c)
                 u[c] = p.U[c][o];
         } else {
+#pragma unroll 1
+            for (int c = 0; c < 5; ++c)
+                slot[c * Stg<T>::SV + i] = src.halo(p.U[c], c, t, gx, gy, gz);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                u[c] = src.halo(p.U[c], c, t, gx, gy, gz);
+                u[c] = slot[c * Stg<T>::SV + i];
         }
         T w[5];
         to_primitive<T>(u[0], u[1], u[2], u[3], u[4], p.gm1, w);
 #pragma unroll
         for (int c = 0; c < 5; ++c)
-            W[c * Stg<T>::SV + NCORE + (Stg<T>::all ? D * NHALO : 0) + i] = w[c];
+            slot[c * Stg<T>::SV + i] = w[c];
     }
 }
 
@@ -232,10 +245,12 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
         for (int c = 0; c < 5; ++c)
             W[c * Stg<T>::SV + i] = w[c];
     }
-    stage_halo<T, 0>(p, src, t, W);
     if (Stg<T>::all) {
-        stage_halo<T, 1>(p, src, t, W);
-        stage_halo<T, 2>(p, src, t, W);
+#pragma unroll 1
+        for (int D = 0; D < 3; ++D)
+            stage_halo<T>(D, p, src, t, W);
+    } else {
+        stage_halo<T>(0, p, src, t, W);
     }
     __syncthreads();
 
@@ -246,17 +261,15 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
         for (int c = 0; c < 5; ++c)
             acc[k][c] = T(0);
 
-    sweep<T, 0>(W, F, acc, p.gamma, p.igm1, t.ih[0]);
-    if (!Stg<T>::all) {
-        stage_halo<T, 1>(p, src, t, W);
-        __syncthreads();
+#pragma unroll 1
+    for (int D = 0; D < 3; ++D) {
+        if (!Stg<T>::all && D > 0) {
+            stage_halo<T>(D, p, src, t, W);
+            __syncthreads();
+        }
+        const T ihd = D == 0 ? t.ih[0] : (D == 1 ? t.ih[1] : t.ih[2]);
+        sweep<T>(D, W, F, acc, p.gamma, p.igm1, ihd);
     }
-    sweep<T, 1>(W, F, acc, p.gamma, p.igm1, t.ih[1]);
-    if (!Stg<T>::all) {
-        stage_halo<T, 2>(p, src, t, W);
-        __syncthreads();
-    }
-    sweep<T, 2>(W, F, acc, p.gamma, p.igm1, t.ih[2]);
 
     // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows
     double sums[5] = {0, 0, 0, 0, 0};

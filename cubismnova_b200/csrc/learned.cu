@@ -1,7 +1,8 @@
 // learned.cu -- a learned 3-D convolutional smoother for the multigrid solver.
 //
 // Network (no biases, so it is positively homogeneous in the residual):
-//   x  = (x0, x1),  x0 = r / D  (the Jacobi-scaled residual),  x1 = x0 * ln k
+//   x  = (x0, x1),  x0 = (L p - f) / D = -r / D  (the Jacobi correction of
+//        L p = f, whose diagonal is -D),  x1 = x0 * ln k
 //   h1 = relu(conv3(W1, x))   2 -> 16 channels, 3x3x3 taps
 //   h2 = relu(conv3(W2, h1)) 16 -> 16
 //   y  = conv3(W3, h2)       16 -> 1
@@ -347,7 +348,8 @@ __global__ void __launch_bounds__(128) conv_grid(GridIO g, const float *__restri
 namespace cn {
 namespace nn {
 
-// x0 = r / D, x1 = x0 ln k with r = f - L p (p == NULL: p = 0), and r itself.
+// x0 = (L p - f) / D = -r / D (the Jacobi correction; L has diagonal -D),
+// x1 = x0 ln k, with r = f - L p (p == NULL: p = 0), and r itself.
 __global__ void __launch_bounds__(256) features_grid(const float *p, const float *k, const float *f, LabGeom L, BcView pbc,
                                                      BcView kbc, int nblocks, float ih2, float *x0, float *x1, float *rout)
 {
@@ -372,8 +374,9 @@ __global__ void __launch_bounds__(256) features_grid(const float *p, const float
         }
         const float Lp = ih2 * ((fl[0] + fl[1]) + fl[2]);
         const float D = ih2 * ((s[0] + s[1]) + s[2]);
-        const float r = __ldg(f + o) - Lp;
-        const float a = r / D;
+        const float fc = __ldg(f + o);
+        const float r = fc - Lp;
+        const float a = (Lp - fc) / D;
         x0[o] = a;
         x1[o] = a * logf(kc);
         if (rout) rout[o] = r;

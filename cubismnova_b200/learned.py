@@ -29,7 +29,8 @@ SHAPES = ((27, CI, CH), (27, CH, CH), (27, CH, 1))
 
 
 class LearnedSmoother:
-    """p <- p + omega * r/D + N(r/D, (r/D) ln k), N a 3-layer 3^3 conv net."""
+    """p <- p + omega * x0 + N(x0, x0 ln k) with x0 = -r/D the Jacobi correction
+    (r = f - L p, D = -diag L), N a 3-layer 3^3 conv net."""
 
     def __init__(self, seed: int = 0, omega: float = 0.8, init_scale: float = 1e-3):
         h = C.c_void_p()

@@ -241,7 +241,8 @@ cn_status cn_mg_accumulate(cn_mg *m, cn_grid *p64, void *stream);
 
 /* ------------------------------------------------------ learned smoother */
 /* A learned 3x3x3 convolutional smoother (no reference counterpart; the
- * reference has no learned components): inputs x0 = r/D, x1 = x0 ln k,
+ * reference has no learned components): inputs x0 = -r/D (the Jacobi
+ * correction, r = f - L p, D = -diag L), x1 = x0 ln k,
  * h1 = relu(conv(W1, x)) (2 -> 16 ch), h2 = relu(conv(W2, h1)) (16 -> 16),
  * y = conv(W3, h2) (16 -> 1); smoothing step p += omega*x0 + y.  Weights
  * [tap][cin][cout], tap = dx+1 + 3(dy+1) + 9(dz+1), FP32 master copy. */
