@@ -287,3 +287,81 @@ cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stre
 }
 
 } // extern "C"
+
+// --------------------------------------------------------------------------
+// SSP-RK3 stage with conservation sums and no device allocation.
+//
+// cn_euler_rk3_stage grows its per-CTA partials with cudaMalloc on first use
+// and whenever a larger grid arrives.  Some callers cannot allow that: a
+// solver that captures its time step into a CUDA graph (a cudaMalloc during
+// capture is not a stream operation and breaks the capture), a host that runs
+// with a fixed device-memory budget reserved up front, or one that must not
+// synchronise the device mid-run the way a first-time cudaMalloc/cudaFree may.
+// This variant takes its scratch from a fixed file-scope device array instead,
+// so a call never allocates; the price is a hard limit on the grid size.
+//
+// Size: one 5-double partial per 8^3 tile plus the 5 totals, for at most
+// kStaticSumTiles tiles (16.8M cells, e.g. 256^3), 1.25 MiB per device.
+// Nothing in the array needs to start at zero: every call writes each
+// partial it later reads (one per tile of the grid) and then the totals.
+// The array is one per device and the calls share it, so two calls that
+// overlap on the same device (two streams, or two host threads) race on it
+// and may return each other's sums; callers serialise them.
+// Set-up: the first call on a device, with that device current, looks up the
+// array's device address with cudaGetSymbolAddress and keeps it; that first
+// call should be made before any stream capture begins.
+// --------------------------------------------------------------------------
+static constexpr int64_t kStaticSumTiles = 32768;
+static __device__ __align__(256) double g_static_sums[kStaticSumTiles * 5 + 5];
+static double *g_static_sums_ptr[64];
+static std::mutex g_static_sums_mu;
+
+static cn_status static_sum_scratch(double **out)
+{
+    int dev = 0;
+    CN_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(CN_ERR_UNSUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_static_sums_mu);
+    if (!g_static_sums_ptr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_sums);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_sums)");
+        if (!p) return fail(CN_ERR_CUDA, "cudaGetSymbolAddress returned a null address");
+        g_static_sums_ptr[dev] = static_cast<double *>(p);
+    }
+    *out = g_static_sums_ptr[dev];
+    return CN_OK;
+}
+
+extern "C" cn_status cn_euler_rk3_stage_noalloc(cn_grid *bcsrc, cn_grid *Us, cn_grid *Un, cn_grid *out,
+                                                int stage, double dt, double gamma, double *sums_out,
+                                                void *stream)
+{
+    if (stage < 1 || stage > 3) return fail(CN_ERR_INVALID_ARGUMENT, "stage must be 1, 2 or 3");
+    if (!sums_out) return fail(CN_ERR_INVALID_ARGUMENT, "sums_out is NULL");
+    cn_status s = check_euler(Us, 0);
+    if (s != CN_OK) return s;
+    if (!bcsrc || !out || !same_shape(Us, out) || !same_shape(Us, bcsrc) || bcsrc->ncomp < 5 ||
+        out->ncomp < 5 || (stage > 1 && (!Un || !same_shape(Us, Un) || Un->ncomp < 5)))
+        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
+    const int64_t tiles = stage_ctas(Us);
+    if (tiles > kStaticSumTiles)
+        return fail(CN_ERR_UNSUPPORTED,
+                    "cn_euler_rk3_stage_noalloc: grid has more than 32768 8^3 tiles (16.8M cells), "
+                    "the size of its fixed scratch");
+    double *scratch = nullptr;
+    s = static_sum_scratch(&scratch);
+    if (s != CN_OK) return s;
+    double *partials = scratch, *totals = scratch + kStaticSumTiles * 5;
+    cudaStream_t st = as_stream(stream);
+    s = run_stage(bcsrc, Us, 0, stage > 1 ? Un : nullptr, 0, out, 0, stage, dt, gamma, partials, st);
+    if (s != CN_OK) return s;
+    reduce_partials<<<1, 256, 0, st>>>(partials, (int)tiles, totals);
+    CN_CUDA_TRY(cudaGetLastError());
+    double t[5];
+    CN_CUDA_TRY(cudaMemcpyAsync(t, totals, sizeof(t), cudaMemcpyDeviceToHost, st));
+    CN_CUDA_TRY(cudaStreamSynchronize(st));
+    const double vol = Us->h[0] * Us->h[1] * Us->h[2];
+    for (int c = 0; c < 5; ++c) sums_out[c] = t[c] * vol;
+    return CN_OK;
+}
