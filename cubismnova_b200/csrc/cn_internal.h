@@ -234,4 +234,48 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
     return true;
 }
 
+// Lab value through the full BC chain (out of line: only blocks with BCs or
+// skip flags take it, so its code exists once per kernel; kernels calling it
+// pass L and bc from __grid_constant__ parameters or device memory).
+template <typename T>
+__device__ __noinline__ T lab_fetch_slow(const T *comp, const LabGeom &L, const BcView &bc, int block, int x, int y,
+                                    int z)
+{
+    const int bx = block % L.nb[0];
+    const int by = (block / L.nb[0]) % L.nb[1];
+    const int bz = block / (L.nb[0] * L.nb[1]);
+    T v;
+    if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, z, true, v))
+        v = T(0);
+    return v;
+}
+
+// Value of component comp at cell (x,y,z) of `block` (may lie outside it): in-block cells and the periodic neighbours of blocks without BCs
+// or skip flags (lab mode byte 0, what cn::lab_value resolves to for them)
+// are plain loads; the rest go through the lab.
+template <typename T>
+__device__ __forceinline__ T lab_fetch(const T *comp, const LabGeom &L, const BcView &bc, int block,
+                                   int x, int y, int z)
+{
+    if ((unsigned)x < (unsigned)L.n[0] && (unsigned)y < (unsigned)L.n[1] &&
+        (unsigned)z < (unsigned)L.n[2])
+        return __ldg(comp + (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z));
+    if (__ldg(bc.mode + block) != 0)
+        return lab_fetch_slow<T>(comp, L, bc, block, x, y, z);
+    const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0);
+    const int r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0);
+    const int r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+    if (!L.tensorial && (r0 != 0) + (r1 != 0) + (r2 != 0) > 1)
+        return T(0); // outside a non-tensorial lab: undefined, read as 0
+    int nbx = block % L.nb[0] + r0, nby = (block / L.nb[0]) % L.nb[1] + r1, nbz = block / (L.nb[0] * L.nb[1]) + r2;
+    nbx = nbx < 0 ? nbx + L.nb[0] : (nbx >= L.nb[0] ? nbx - L.nb[0] : nbx);
+    nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
+    nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
+    const int src = nbx + L.nb[0] * (nby + L.nb[1] * nbz);
+    x -= r0 * L.n[0];
+    y -= r1 * L.n[1];
+    z -= r2 * L.n[2];
+    return __ldg(comp + (int64_t)src * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z));
+}
+
 } // namespace cn

@@ -24,6 +24,7 @@
 // (periodic block neighbours and BCs), so the network sees exactly the
 // neighbourhood a FieldLab would give it.
 #include "cn_internal.h"
+#include "learned_tc.h"
 #include "mg_internal.h"
 
 #include <algorithm>
@@ -285,12 +286,7 @@ __global__ void adam_kernel(float *p, const float *g, float *m, float *v, int n,
 template <typename T>
 __device__ __forceinline__ T gfetch(const T *comp, const LabGeom &L, const BcView &bc, int block, int x, int y, int z)
 {
-    if ((unsigned)x < (unsigned)L.n[0] && (unsigned)y < (unsigned)L.n[1] && (unsigned)z < (unsigned)L.n[2])
-        return __ldg(comp + (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z));
-    const int bx = block % L.nb[0], by = (block / L.nb[0]) % L.nb[1], bz = block / (L.nb[0] * L.nb[1]);
-    T v;
-    if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, z, true, v)) v = T(0);
-    return v;
+    return lab_fetch<T>(comp, L, bc, block, x, y, z);
 }
 
 struct GridIO {
@@ -304,7 +300,7 @@ struct GridIO {
 };
 
 template <int Cin, int Cout, bool RELU>
-__global__ void __launch_bounds__(128) conv_grid(GridIO g, const float *__restrict__ W)
+__global__ void __launch_bounds__(128) conv_grid(const __grid_constant__ GridIO g, const float *__restrict__ W)
 {
     extern __shared__ float sw[];
     for (int i = threadIdx.x; i < 27 * Cin * Cout; i += blockDim.x) sw[i] = W[i];
@@ -350,8 +346,10 @@ namespace nn {
 
 // x0 = (L p - f) / D = -r / D (the Jacobi correction; L has diagonal -D),
 // x1 = x0 ln k, with r = f - L p (p == NULL: p = 0), and r itself.
-__global__ void __launch_bounds__(256) features_grid(const float *p, const float *k, const float *f, LabGeom L, BcView pbc,
-                                                     BcView kbc, int nblocks, float ih2, float *x0, float *x1, float *rout)
+__global__ void __launch_bounds__(256) features_grid(const float *p, const float *k, const float *f,
+                                                     const __grid_constant__ LabGeom L,
+                                                     const __grid_constant__ BcView pbc,
+                                                     const __grid_constant__ BcView kbc, int nblocks, float ih2, float *x0, float *x1, float *rout)
 {
     const int64_t cells = (int64_t)L.n[0] * L.n[1] * L.n[2];
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < cells * nblocks; t += (int64_t)gridDim.x * blockDim.x) {
@@ -392,7 +390,8 @@ __global__ void __launch_bounds__(256) smooth_update(float *p, const float *x0, 
 }
 
 // Patch extraction around block b: out[c][X][Y][Z] for X,Y,Z in [-h, n+h).
-__global__ void __launch_bounds__(256) extract_patch(const float *comp, LabGeom L, BcView bc, const int *blocks, int np,
+__global__ void __launch_bounds__(256) extract_patch(const float *comp, const __grid_constant__ LabGeom L,
+                                                     const __grid_constant__ BcView bc, const int *blocks, int np,
                                                      int halo, float *out, int64_t out_stride)
 {
     const int E = L.n[0] + 2 * halo;
@@ -430,6 +429,10 @@ struct cn_nn {
     float *h1 = nullptr, *h2 = nullptr, *y = nullptr, *c = nullptr, *res = nullptr, *gc = nullptr, *gh2 = nullptr,
           *gh1 = nullptr;
     double *sums = nullptr;
+    // grid inference: 1 = BF16 tensor cores (tcgen05) where the block shape
+    // allows, 0 = FP32 CUDA cores; packed BF16 weights of the three layers
+    int inference = 1;
+    uint16_t *wpack = nullptr;
 };
 
 static constexpr int NW1 = 27 * CI * CH, NW2 = 27 * CH * CH, NW3 = 27 * CH;
@@ -518,6 +521,13 @@ cn_status cn_nn_create(uint64_t seed, double omega, double init_scale, cn_nn **o
     return CN_OK;
 }
 
+cn_status cn_nn_set_inference(cn_nn *nn, int mode)
+{
+    if (!nn || mode < 0 || mode > 1) return fail(CN_ERR_INVALID_ARGUMENT, "cn_nn_set_inference: bad argument");
+    nn->inference = mode;
+    return CN_OK;
+}
+
 cn_status cn_nn_destroy(cn_nn *nn)
 {
     if (!nn) return CN_OK;
@@ -525,6 +535,7 @@ cn_status cn_nn_destroy(cn_nn *nn)
     for (float *b : bufs)
         if (b) cudaFree(b);
     if (nn->sums) cudaFree(nn->sums);
+    if (nn->wpack) cudaFree(nn->wpack);
     delete nn;
     return CN_OK;
 }
@@ -696,10 +707,42 @@ static cn_status features(cn_mg *m, int l, const float *p, const float *f, float
     return CN_OK;
 }
 
+// Tensor-core inference: features (FP32) -> three tcgen05 convolution
+// layers, the last fused with the update of p.
+static cn_status nn_smooth_tc(cn_mg *m, int l, int apps, bool zero_guess, cudaStream_t st)
+{
+    cn_grid *P = m->p[l], *X = m->nn_bufs[4 * l];
+    if ((int)m->nn_act.size() < 2 * m->nlevels) m->nn_act.resize(2 * m->nlevels, nullptr);
+    const size_t abytes = (size_t)P->nblocks * P->n[0] * P->n[1] * P->n[2] * 16 * sizeof(uint16_t);
+    for (int i = 0; i < 2; ++i)
+        if (!m->nn_act[2 * l + i]) CN_CUDA_TRY(cudaMalloc(&m->nn_act[2 * l + i], abytes));
+    cn_nn *nn = m->nn;
+    if (!nn->wpack) CN_CUDA_TRY(cudaMalloc(&nn->wpack, 3 * nntc::kPackedWeightBytes));
+    uint16_t *w1 = nn->wpack, *w2 = w1 + nntc::kPackedWeightBytes / 2, *w3 = w2 + nntc::kPackedWeightBytes / 2;
+    cn_status s;
+    if ((s = nntc::pack_weights(nn->w, CI, CH, w1, st)) != CN_OK) return s;
+    if ((s = nntc::pack_weights(nn->w + NW1, CH, CH, w2, st)) != CN_OK) return s;
+    if ((s = nntc::pack_weights(nn->w + NW1 + NW2, CH, 1, w3, st)) != CN_OK) return s;
+    uint16_t *h1 = static_cast<uint16_t *>(m->nn_act[2 * l]), *h2 = static_cast<uint16_t *>(m->nn_act[2 * l + 1]);
+    const float *x = reinterpret_cast<const float *>(X->d_data);
+    for (int a = 0; a < apps; ++a) {
+        const bool zg = zero_guess && a == 0;
+        if ((s = features(m, l, zg ? nullptr : fptr(P), fptr(m->f[l]), nullptr, st)) != CN_OK) return s;
+        if ((s = nntc::conv_features(x, X->comp_stride, X->block_stride, P->nb, P->n, w1, h1, P->d_err, st)) != CN_OK)
+            return s;
+        if ((s = nntc::conv_hidden(h1, P->nb, P->n, w2, 1, h2, P->d_err, st)) != CN_OK) return s;
+        if ((s = nntc::conv_update(h2, P->nb, P->n, w3, x, X->block_stride, fptr(P), P->block_stride,
+                                   (float)nn->omega, zg ? 1 : 0, P->d_err, st)) != CN_OK)
+            return s;
+    }
+    return CN_OK;
+}
+
 cn_status nn_smooth(cn_mg *m, int l, int apps, bool zero_guess, cudaStream_t st)
 {
     cn_status s = level_bufs(m, l);
     if (s != CN_OK) return s;
+    if (m->nn->inference == 1 && nntc::supported(m->p[l]->n) && apps > 0) return nn_smooth_tc(m, l, apps, zero_guess, st);
     cn_grid *X = m->nn_bufs[4 * l], *H1 = m->nn_bufs[4 * l + 1], *H2 = m->nn_bufs[4 * l + 2], *Y = m->nn_bufs[4 * l + 3];
     const LabGeom Lt = make_geom(m->p[l], &kS1t);
     const float *W1 = m->nn->w, *W2 = m->nn->w + NW1, *W3 = m->nn->w + NW1 + NW2;

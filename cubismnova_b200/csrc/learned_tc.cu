@@ -1,0 +1,343 @@
+// learned_tc.cu -- the learned smoother's 3x3x3 convolutions on the tensor
+// cores (tcgen05, sm_100a): BF16 activations and weights, FP32 accumulation
+// in tensor memory.
+//
+// Implicit GEMM without an im2col buffer.  A CTA owns a brick of 16x16x4
+// output cells of one block and stages the 18x18x6 input region (brick plus
+// a one-cell halo) in shared memory, one row of 16 BF16 channels per region
+// cell, rows in region order r = i + 18 (j + 18 k).  An output cell sits at
+// row R0 + m with m = x + 18 y + 324 z, and its input at tap (dx, dy, dz) at
+// row R0 + m + dx + 18 dy + 324 dz: for every tap the A operand of an
+// M = 128 tile is the same run of 128 rows, shifted.  So one M-tile is 27
+// MMAs (M = 128, N = 16, K = 16 channels, one per tap) accumulating into the
+// same TMEM columns; the A descriptor's start address moves by the tap's row
+// offset.  Rows m whose (x, y) fall outside the brick (x or y in 16..17) are
+// computed and dropped.  The brick spans m in [0, 1258): 10 M-tiles.
+//
+// Shared-memory operand layout (unswizzled, K-major): A is two planes (K
+// chunks of channels 0-7 and 8-15) of SROWS rows x 16 bytes; core matrices
+// are 8 consecutive rows of one plane (SBO = 128 B between 8-row groups,
+// LBO = one plane between the two K chunks), so a shift by any number of
+// rows is again a valid operand.  B (weights of one tap, N = 16 output
+// channels x K = 16 input channels) uses the same form: planes of 16 rows.
+//
+// Layers: 2 -> 16 (input channels padded with zeros to 16), 16 -> 16, and
+// 16 -> 1 (output channels padded to N = 16); ReLU after the first two.  The
+// first layer reads the FP32 features (x0, x1) of the grid; hidden
+// activations are channels-last BF16, 32 bytes per cell; the last layer
+// applies the smoothing update p += omega x0 + y in its epilogue.
+// Neighbour cells outside the block are the periodic neighbours of the block
+// grid (the activation grids carry no BCs), corners and edges included.
+//
+// One thread issues the MMAs and commits them to an mbarrier; all threads
+// wait on it with a bounded poll (on timeout the CTA records an error word,
+// skips its epilogue, frees its TMEM and exits).
+#include "cn_internal.h"
+#include "cn_tc.cuh"
+#include "cn_tma.cuh"
+#include "learned_tc.h"
+
+#include <cuda_bf16.h>
+
+namespace cn {
+namespace nntc {
+
+constexpr int BX = 16, BY = 16, BZ = 4;              // brick of output cells
+constexpr int RX = BX + 2, RY = BY + 2, RZ = BZ + 2; // input region 18 x 18 x 6
+constexpr int RCELLS = RX * RY * RZ;                 // 1944
+constexpr int R0 = 1 + RX + RX * RY;                 // row of output cell (0,0,0): 343
+constexpr int MSPAN = (BX - 1) + RX * (BY - 1) + RX * RY * (BZ - 1) + 1; // 1258
+constexpr int MT = (MSPAN + 127) / 128;              // 10 M-tiles
+// highest row read: R0 + 128 MT - 1 + R0 (tap offsets lie in [-R0, R0])
+constexpr int SROWS = ((2 * R0 + 128 * MT + 7) / 8) * 8; // 1968
+constexpr int NTHREADS = 256;
+constexpr int TMEM_COLS = 256;                       // >= 16 * MT
+constexpr uint32_t PLANE = SROWS * 16;               // bytes of one K plane of A
+constexpr uint32_t WTAP = 512;                       // bytes of one tap's B (2 planes x 16 rows x 16 B)
+constexpr size_t SMEM = 2 * (size_t)PLANE + 27 * WTAP + 16;
+constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 16);
+static_assert(RCELLS <= SROWS, "region must fit the A rows");
+static_assert(16 * MT <= TMEM_COLS, "accumulators must fit the TMEM allocation");
+
+struct Params {
+    // input: mode 0 reads FP32 components x0 (comp 0) and x1 (comp 1) of a
+    // block grid; modes 1, 2 read channels-last BF16 activations
+    const float *x;        // features, component-major (comp stride xcs)
+    int64_t xcs;
+    int64_t xbs;           // block stride (elements) of the feature grid
+    const uint16_t *act;   // [nblocks][cells][16] BF16
+    const uint16_t *w;     // [27][2][16][8] BF16 B tiles of this layer
+    // output: mode 0, 1 write BF16 activations (ReLU); mode 2 updates p
+    uint16_t *out;
+    float *p;              // mode 2: p (FP32 grid, block stride pbs)
+    int64_t pbs;
+    float omega;
+    int zero_guess;        // mode 2: p starts from zero
+    int relu;
+    int nb[3], n[3];
+    int bricks[3];         // bricks per block along x, y, z
+    int *err;
+};
+
+__device__ __forceinline__ uint16_t bf16_bits(float v)
+{
+    return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+
+// block-local cell (x, y, z), one cell outside allowed, of block b -> (block, cell)
+__device__ __forceinline__ void wrap_cell(const Params &P, int b, int x, int y, int z, int &ob, int &oc)
+{
+    int bx = b % P.nb[0], by = (b / P.nb[0]) % P.nb[1], bz = b / (P.nb[0] * P.nb[1]);
+    if (x < 0) { x += P.n[0]; bx = bx == 0 ? P.nb[0] - 1 : bx - 1; }
+    else if (x >= P.n[0]) { x -= P.n[0]; bx = bx == P.nb[0] - 1 ? 0 : bx + 1; }
+    if (y < 0) { y += P.n[1]; by = by == 0 ? P.nb[1] - 1 : by - 1; }
+    else if (y >= P.n[1]) { y -= P.n[1]; by = by == P.nb[1] - 1 ? 0 : by + 1; }
+    if (z < 0) { z += P.n[2]; bz = bz == 0 ? P.nb[2] - 1 : bz - 1; }
+    else if (z >= P.n[2]) { z -= P.n[2]; bz = bz == P.nb[2] - 1 ? 0 : bz + 1; }
+    ob = bx + P.nb[0] * (by + P.nb[1] * bz);
+    oc = x + P.n[0] * (y + P.n[1] * z);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NTHREADS) conv3_tc_kernel(const __grid_constant__ Params P)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *A = smem;                       // [2][SROWS][16 B]
+    unsigned char *Bw = smem + 2 * PLANE;          // [27][2][16][16 B]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Bw + 27 * WTAP);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
+
+    const int bricks = P.bricks[0] * P.bricks[1] * P.bricks[2];
+    const int block = blockIdx.x / bricks;
+    int br = blockIdx.x - block * bricks;
+    const int ox = (br % P.bricks[0]) * BX;
+    br /= P.bricks[0];
+    const int oy = (br % P.bricks[1]) * BY;
+    const int oz = (br / P.bricks[1]) * BZ;
+    const int cells = P.n[0] * P.n[1] * P.n[2];
+
+    // ---- TMEM and barrier set-up (warp 0 allocates)
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    if (threadIdx.x < 32) {
+        tc::tmem_alloc(slot, TMEM_COLS);
+        tc::tmem_relinquish();
+    }
+
+    // ---- weights: 27 taps x 512 B as 16-byte chunks
+    for (int i = threadIdx.x; i < 27 * 32; i += NTHREADS)
+        reinterpret_cast<uint4 *>(Bw)[i] = __ldg(reinterpret_cast<const uint4 *>(P.w) + i);
+
+    // ---- input region: row u = region cell, two 16-byte chunks (K planes)
+    for (int t = threadIdx.x; t < 2 * SROWS; t += NTHREADS) {
+        const int u = t >> 1, kc = t & 1;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (u < RCELLS) {
+            const int i = u % RX, j = (u / RX) % RY, k = u / (RX * RY);
+            const int x = ox + i - 1, y = oy + j - 1, z = oz + k - 1;
+            int sb = block, sc;
+            if ((unsigned)x < (unsigned)P.n[0] && (unsigned)y < (unsigned)P.n[1] && (unsigned)z < (unsigned)P.n[2])
+                sc = x + P.n[0] * (y + P.n[1] * z);
+            else
+                wrap_cell(P, block, x, y, z, sb, sc);
+            if (MODE == 0) {
+                if (kc == 0) {
+                    const int64_t o = (int64_t)sb * P.xbs + sc;
+                    const float a = __ldg(P.x + o), b = __ldg(P.x + P.xcs + o);
+                    v.x = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
+                }
+            } else {
+                v = __ldg(reinterpret_cast<const uint4 *>(P.act + ((int64_t)sb * cells + sc) * 16) + kc);
+            }
+        }
+        *reinterpret_cast<uint4 *>(A + kc * PLANE + u * 16) = v;
+    }
+    fence_proxy_async_smem(); // generic-proxy smem writes -> visible to the tensor cores
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *slot;
+
+    // ---- MMAs: 10 M-tiles x 27 taps, one issuing thread
+    if (threadIdx.x == 0) {
+        const uint32_t a0 = smem_u32(A), b0 = smem_u32(Bw);
+#pragma unroll 1
+        for (int t = 0; t < MT; ++t) {
+#pragma unroll 1
+            for (int q = 0; q < 27; ++q) {
+                const int off = (q % 3 - 1) + RX * ((q / 3) % 3 - 1) + RX * RY * (q / 9 - 1);
+                const uint32_t row = (uint32_t)(R0 + 128 * t + off);
+                tc::mma_bf16(tbase + 16u * t, tc::smem_desc(a0 + row * 16u, PLANE, 128u),
+                             tc::smem_desc(b0 + q * WTAP, 256u, 128u), IDESC, q > 0 ? 1u : 0u);
+            }
+        }
+        tc::mma_commit(bar);
+    }
+    const int ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0);
+    tc::fence_after_sync();
+
+    // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 of the tiles t = w / 4, w / 4 + 2, ...
+    if (ok) {
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const uint32_t lane_base = (uint32_t)(32 * (w & 3)) << 16;
+#pragma unroll 1
+        for (int t = w >> 2; t < MT; t += 2) {
+            float v[16];
+            tc::tmem_ld16(tbase + lane_base + 16u * t, v);
+            const int m = 128 * t + 32 * (w & 3) + lane;
+            const int z = m / (RX * RY), rem = m - z * (RX * RY);
+            const int y = rem / RX, x = rem - y * RX;
+            if (x >= BX || y >= BY || z >= BZ)
+                continue;
+            const int c = (ox + x) + P.n[0] * ((oy + y) + P.n[1] * (oz + z));
+            if (MODE == 2) {
+                const int64_t o = (int64_t)block * P.pbs + c;
+                const float x0 = __ldg(P.x + (int64_t)block * P.xbs + c);
+                const float pv = P.zero_guess ? 0.f : P.p[o];
+                P.p[o] = pv + (P.omega * x0 + v[0]);
+            } else {
+                uint32_t h[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    float a = v[2 * j], b = v[2 * j + 1];
+                    if (P.relu) {
+                        a = fmaxf(a, 0.f);
+                        b = fmaxf(b, 0.f);
+                    }
+                    h[j] = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(P.out + ((int64_t)block * cells + c) * 16);
+                dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+            }
+        }
+    } else if (threadIdx.x == 0 && P.err) {
+        atomicExch(P.err, kDevErrTimeout);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32)
+        tc::tmem_dealloc(tbase, TMEM_COLS);
+}
+
+// FP32 weights [27][cin][cout] -> BF16 B tiles [27][kc][co][8] (B[co][ci] = W[tap][ci][co])
+__global__ void pack_weights_kernel(const float *W, int cin, int cout, uint16_t *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x; // [27][2][16][8]
+    if (i >= 27 * 256)
+        return;
+    const int tap = i / 256, r = i % 256;
+    const int kc = r / 128, co = (r / 8) % 16, e = r % 8;
+    const int ci = kc * 8 + e;
+    const float v = (ci < cin && co < cout) ? W[(tap * cin + ci) * cout + co] : 0.f;
+    out[i] = bf16_bits(v);
+}
+
+static bool attr_set[3];
+
+template <int MODE>
+static cn_status launch(const Params &P, int nblocks, cudaStream_t st)
+{
+    if (!attr_set[MODE]) {
+        CN_CUDA_TRY(cudaFuncSetAttribute(conv3_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM));
+        attr_set[MODE] = true;
+    }
+    const int64_t ctas = (int64_t)nblocks * P.bricks[0] * P.bricks[1] * P.bricks[2];
+    conv3_tc_kernel<MODE><<<(unsigned)ctas, NTHREADS, SMEM, st>>>(P);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+bool supported(const int n[3])
+{
+    return n[0] % BX == 0 && n[1] % BY == 0 && n[2] % BZ == 0;
+}
+
+cn_status pack_weights(const float *W, int cin, int cout, uint16_t *out, cudaStream_t st)
+{
+    pack_weights_kernel<<<(27 * 256 + 255) / 256, 256, 0, st>>>(W, cin, cout, out);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+static Params base_params(const int nb[3], const int n[3], int *err)
+{
+    Params P = {};
+    for (int d = 0; d < 3; ++d) {
+        P.nb[d] = nb[d];
+        P.n[d] = n[d];
+    }
+    P.bricks[0] = n[0] / BX;
+    P.bricks[1] = n[1] / BY;
+    P.bricks[2] = n[2] / BZ;
+    P.err = err;
+    return P;
+}
+
+cn_status conv_features(const float *x, int64_t xcs, int64_t xbs, const int nb[3], const int n[3],
+                        const uint16_t *w, uint16_t *out, int *err, cudaStream_t st)
+{
+    Params P = base_params(nb, n, err);
+    P.x = x;
+    P.xcs = xcs;
+    P.xbs = xbs;
+    P.w = w;
+    P.out = out;
+    P.relu = 1;
+    return launch<0>(P, nb[0] * nb[1] * nb[2], st);
+}
+
+cn_status conv_hidden(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, int relu,
+                      uint16_t *out, int *err, cudaStream_t st)
+{
+    Params P = base_params(nb, n, err);
+    P.act = act;
+    P.w = w;
+    P.out = out;
+    P.relu = relu;
+    return launch<1>(P, nb[0] * nb[1] * nb[2], st);
+}
+
+cn_status conv_update(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, const float *x0,
+                      int64_t xbs, float *p, int64_t pbs, float omega, int zero_guess, int *err, cudaStream_t st)
+{
+    Params P = base_params(nb, n, err);
+    P.act = act;
+    P.w = w;
+    P.x = x0;
+    P.xbs = xbs;
+    P.p = p;
+    P.pbs = pbs;
+    P.omega = omega;
+    P.zero_guess = zero_guess;
+    return launch<2>(P, nb[0] * nb[1] * nb[2], st);
+}
+
+} // namespace nntc
+} // namespace cn
+
+using namespace cn;
+
+extern "C" cn_status cn_conv3_bf16(const void *in, void *out, const int nblocks[3], const int block_cells[3],
+                                   const float *weights, int relu, void *stream)
+{
+    if (!in || !out || !nblocks || !block_cells || !weights)
+        return fail(CN_ERR_INVALID_ARGUMENT, "cn_conv3_bf16: NULL argument");
+    for (int d = 0; d < 3; ++d)
+        if (nblocks[d] < 1 || block_cells[d] < 1)
+            return fail(CN_ERR_INVALID_ARGUMENT, "cn_conv3_bf16: bad grid shape");
+    if (!nntc::supported(block_cells))
+        return fail(CN_ERR_UNSUPPORTED, "cn_conv3_bf16: block cells must be multiples of (16, 16, 4)");
+    cudaStream_t st = as_stream(stream);
+    uint16_t *w = nullptr;
+    CN_CUDA_TRY(cudaMallocAsync(&w, 27 * nntc::WTAP, st));
+    cn_status s = nntc::pack_weights(weights, 16, 16, w, st);
+    if (s == CN_OK)
+        s = nntc::conv_hidden(static_cast<const uint16_t *>(in), nblocks, block_cells, w, relu,
+                              static_cast<uint16_t *>(out), nullptr, st);
+    cudaFreeAsync(w, st);
+    return s;
+}

@@ -1,0 +1,30 @@
+// learned_tc.h -- tensor-core (tcgen05) convolution layers of the learned
+// smoother, used by learned.cu for grid inference (see learned_tc.cu).
+#pragma once
+
+#include "cn_internal.h"
+
+#include <cstdint>
+
+namespace cn {
+namespace nntc {
+
+// bytes of one layer's packed BF16 weights ([27][2][16][8])
+constexpr size_t kPackedWeightBytes = 27 * 512;
+
+// block cells must be multiples of the 16 x 16 x 4 brick
+bool supported(const int n[3]);
+// FP32 [27][cin][cout] -> packed BF16 B tiles (cin, cout <= 16, zero padded)
+cn_status pack_weights(const float *W, int cin, int cout, uint16_t *out, cudaStream_t st);
+// layer 1: FP32 features x0 = x[0..], x1 = x[xcs..] (block stride xbs) -> ReLU -> BF16 activations
+cn_status conv_features(const float *x, int64_t xcs, int64_t xbs, const int nb[3], const int n[3],
+                        const uint16_t *w, uint16_t *out, int *err, cudaStream_t st);
+// hidden layer: BF16 activations -> (ReLU) -> BF16 activations
+cn_status conv_hidden(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, int relu,
+                      uint16_t *out, int *err, cudaStream_t st);
+// last layer (output channel 0) fused with p = (zero_guess ? 0 : p) + (omega x0 + y)
+cn_status conv_update(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, const float *x0,
+                      int64_t xbs, float *p, int64_t pbs, float omega, int zero_guess, int *err, cudaStream_t st);
+
+} // namespace nntc
+} // namespace cn

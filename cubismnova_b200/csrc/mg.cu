@@ -32,33 +32,31 @@ struct Geo {
     int nblocks;
 };
 
+// Cell t of a level in block order (32-bit arithmetic: cn_mg_create checks
+// that the finest level has fewer than 2^31 cells).
 __device__ __forceinline__ void cell_of(int64_t t, const LabGeom &L, int &block, int &x, int &y,
                                         int &z)
 {
-    const int64_t cells = (int64_t)L.n[0] * L.n[1] * L.n[2];
-    block = (int)(t / cells);
-    int64_t c = t - (int64_t)block * cells;
-    x = (int)(c % L.n[0]);
-    c /= L.n[0];
-    y = (int)(c % L.n[1]);
-    z = (int)(c / L.n[1]);
+    const unsigned n0 = (unsigned)L.n[0], n1 = (unsigned)L.n[1];
+    const unsigned cells = n0 * n1 * (unsigned)L.n[2];
+    const unsigned tt = (unsigned)t;
+    const unsigned b = tt / cells;
+    const unsigned c = tt - b * cells;
+    const unsigned yz = c / n0;
+    const unsigned zz = yz / n1;
+    block = (int)b;
+    x = (int)(c - yz * n0);
+    y = (int)(yz - zz * n1);
+    z = (int)zz;
 }
 
-// value of component comp at cell (x,y,z) of `block` (may lie one cell outside)
+// neighbour values: cn::lab_fetch (plain loads inside the block and for
+// periodic neighbours of blocks without BCs, the lab otherwise)
 template <typename T>
-__device__ __forceinline__ T fetch(const T *comp, const LabGeom &L, const BcView &bc, int block,
-                                   int x, int y, int z)
+__device__ __forceinline__ T fetch(const T *comp, const LabGeom &L, const BcView &bc, int block, int x, int y,
+                                   int z)
 {
-    if ((unsigned)x < (unsigned)L.n[0] && (unsigned)y < (unsigned)L.n[1] &&
-        (unsigned)z < (unsigned)L.n[2])
-        return __ldg(comp + (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z));
-    const int bx = block % L.nb[0];
-    const int by = (block / L.nb[0]) % L.nb[1];
-    const int bz = block / (L.nb[0] * L.nb[1]);
-    T v;
-    if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, z, true, v))
-        v = T(0);
-    return v;
+    return lab_fetch<T>(comp, L, bc, block, x, y, z);
 }
 
 template <typename T> __device__ __forceinline__ T harm(T a, T b)
@@ -67,28 +65,69 @@ template <typename T> __device__ __forceinline__ T harm(T a, T b)
     return (t + t) / (a + b);
 }
 
-// L p and the diagonal D at one cell; TP is the solution type (float in the
-// V-cycle, double in the outer residual), k is always FP32 storage.
+// The 13 values of the 7-point operator at one cell: v[0] = p, v[1] = k,
+// then per direction d: p(+e_d), p(-e_d), k(+e_d), k(-e_d); p == NULL reads
+// as zero.  Cells interior to their block take plain loads.
 template <typename TP>
-__device__ __forceinline__ void op7(const TP *p, const float *k, const Geo &G, const BcView &kbc,
-                                    int block, int x, int y, int z, TP ih2, TP &Lp, TP &D, TP &pc)
+__device__ __forceinline__ void load7(const TP *p, const float *k, const Geo &G, const BcView &kbc, int block,
+                                      int x, int y, int z, TP (&v)[14])
 {
     const LabGeom &L = G.L, &Lk = G.Lk;
-    pc = fetch<TP>(p, L, G.bc, block, x, y, z);
-    const TP kc = (TP)fetch<float>(k, Lk, kbc, block, x, y, z);
+    if (x > 0 && y > 0 && z > 0 && x < L.n[0] - 1 && y < L.n[1] - 1 && z < L.n[2] - 1) {
+        const int64_t cell = x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
+        const TP *pb = p ? p + (int64_t)block * L.bstride + cell : nullptr;
+        const float *kb = k + (int64_t)block * Lk.bstride + cell;
+        const int64_t st[3] = {1, L.n[0], (int64_t)L.n[0] * L.n[1]};
+        v[0] = pb ? __ldg(pb) : TP(0);
+        v[1] = (TP)__ldg(kb);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            v[2 + 4 * d] = pb ? __ldg(pb + st[d]) : TP(0);
+            v[3 + 4 * d] = pb ? __ldg(pb - st[d]) : TP(0);
+            v[4 + 4 * d] = (TP)__ldg(kb + st[d]);
+            v[5 + 4 * d] = (TP)__ldg(kb - st[d]);
+        }
+    } else {
+        v[0] = p ? fetch<TP>(p, L, G.bc, block, x, y, z) : TP(0);
+        v[1] = (TP)fetch<float>(k, Lk, kbc, block, x, y, z);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int ox = d == 0, oy = d == 1, oz = d == 2;
+            v[2 + 4 * d] = p ? fetch<TP>(p, L, G.bc, block, x + ox, y + oy, z + oz) : TP(0);
+            v[3 + 4 * d] = p ? fetch<TP>(p, L, G.bc, block, x - ox, y - oy, z - oz) : TP(0);
+            v[4 + 4 * d] = (TP)fetch<float>(k, Lk, kbc, block, x + ox, y + oy, z + oz);
+            v[5 + 4 * d] = (TP)fetch<float>(k, Lk, kbc, block, x - ox, y - oy, z - oz);
+        }
+    }
+}
+
+// L p and the diagonal D at one cell from its 13 values; TP is the solution
+// type (float in the V-cycle, double in the outer residual), k is FP32.
+template <typename TP>
+__device__ __forceinline__ void op7_math(const TP (&v)[14], TP ih2, TP &Lp, TP &D, TP &pc)
+{
+    pc = v[0];
+    const TP kc = v[1];
     TP f[3], s[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const int ox = d == 0, oy = d == 1, oz = d == 2;
-        const TP pp = fetch<TP>(p, L, G.bc, block, x + ox, y + oy, z + oz);
-        const TP pm = fetch<TP>(p, L, G.bc, block, x - ox, y - oy, z - oz);
-        const TP kp = harm<TP>(kc, (TP)fetch<float>(k, Lk, kbc, block, x + ox, y + oy, z + oz));
-        const TP km = harm<TP>((TP)fetch<float>(k, Lk, kbc, block, x - ox, y - oy, z - oz), kc);
+        const TP pp = v[2 + 4 * d], pm = v[3 + 4 * d];
+        const TP kp = harm<TP>(kc, v[4 + 4 * d]);
+        const TP km = harm<TP>(v[5 + 4 * d], kc);
         f[d] = kp * (pp - pc) - km * (pc - pm);
         s[d] = kp + km;
     }
     Lp = ih2 * ((f[0] + f[1]) + f[2]);
     D = ih2 * ((s[0] + s[1]) + s[2]);
+}
+
+template <typename TP>
+__device__ __forceinline__ void op7(const TP *p, const float *k, const Geo &G, const BcView &kbc,
+                                    int block, int x, int y, int z, TP ih2, TP &Lp, TP &D, TP &pc)
+{
+    TP v[14];
+    load7<TP>(p, k, G, kbc, block, x, y, z, v);
+    op7_math<TP>(v, ih2, Lp, D, pc);
 }
 
 struct KArgs {
@@ -100,8 +139,8 @@ struct KArgs {
 };
 
 // weighted Jacobi sweep: pout = pin + omega (L pin - f) / D  (pin == NULL: zero guess)
-__global__ void __launch_bounds__(256) jacobi_kernel(KArgs a, const float *pin, const float *f,
-                                                     float *pout, float omega)
+__global__ void __launch_bounds__(256) jacobi_kernel(const __grid_constant__ KArgs a, const float *pin,
+                                                     const float *f, float *pout, float omega)
 {
     const LabGeom &L = a.G.L;
     const int64_t total = (int64_t)a.G.nblocks * L.n[0] * L.n[1] * L.n[2];
@@ -111,35 +150,17 @@ __global__ void __launch_bounds__(256) jacobi_kernel(KArgs a, const float *pin, 
         cell_of(t, L, block, x, y, z);
         const int64_t o = (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
         const float fc = __ldg(f + o);
-        float out;
-        if (pin) {
-            float Lp, D, pc;
-            op7<float>(pin, a.k, a.G, a.kbc, block, x, y, z, a.ih2, Lp, D, pc);
-            out = pc + omega * ((Lp - fc) / D);
-        } else {
-            // L 0 = 0: only the diagonal is needed
-            float Lp, D, pc;
-            (void)Lp;
-            (void)pc;
-            const float kc = fetch<float>(a.k, L, a.kbc, block, x, y, z);
-            float s[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const int ox = d == 0, oy = d == 1, oz = d == 2;
-                const float kp = harm<float>(kc, fetch<float>(a.k, L, a.kbc, block, x + ox, y + oy, z + oz));
-                const float km = harm<float>(fetch<float>(a.k, L, a.kbc, block, x - ox, y - oy, z - oz), kc);
-                s[d] = kp + km;
-            }
-            D = a.ih2 * ((s[0] + s[1]) + s[2]);
-            out = 0.0f + omega * ((0.0f - fc) / D);
-        }
-        pout[o] = out;
+        float Lp, D, pc;
+        op7<float>(pin, a.k, a.G, a.kbc, block, x, y, z, a.ih2, Lp, D, pc);
+        // zero guess (pin == NULL): L 0 = 0, only the diagonal is used
+        pout[o] = pin ? pc + omega * ((Lp - fc) / D) : 0.0f + omega * ((0.0f - fc) / D);
     }
 }
 
 // residual of the fine level restricted onto the coarse right-hand side:
 // one thread per coarse cell, fc = (sum of its 8 children's f - L p) / 8
-__global__ void __launch_bounds__(256) resid_restrict_kernel(KArgs a, const float *p, const float *f,
+__global__ void __launch_bounds__(256) resid_restrict_kernel(const __grid_constant__ KArgs a, const float *p,
+                                                             const float *f,
                                                              LabGeom Lc, float *fc)
 {
     const LabGeom &L = a.G.L;
@@ -183,8 +204,10 @@ __global__ void __launch_bounds__(256) restrict_mean_kernel(LabGeom L, const flo
 }
 
 // p_fine += trilinear interpolation of the coarse correction e
-__global__ void __launch_bounds__(256) prolong_kernel(LabGeom L, float *p, LabGeom Lct, BcView cbc,
-                                                      const float *e, int nblocks)
+__global__ void __launch_bounds__(256) prolong_kernel(const __grid_constant__ LabGeom L, float *p,
+                                                      const __grid_constant__ LabGeom Lct,
+                                                      const __grid_constant__ BcView cbc, const float *e,
+                                                      int nblocks)
 {
     const int64_t total = (int64_t)nblocks * L.n[0] * L.n[1] * L.n[2];
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
@@ -193,29 +216,45 @@ __global__ void __launch_bounds__(256) prolong_kernel(LabGeom L, float *p, LabGe
         cell_of(t, L, block, x, y, z);
         const int X = x >> 1, Y = y >> 1, Z = z >> 1;
         const int sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1, sz = (z & 1) ? 1 : -1;
-        const float e000 = fetch<float>(e, Lct, cbc, block, X, Y, Z);
-        const float e100 = fetch<float>(e, Lct, cbc, block, X + sx, Y, Z);
-        const float e010 = fetch<float>(e, Lct, cbc, block, X, Y + sy, Z);
-        const float e110 = fetch<float>(e, Lct, cbc, block, X + sx, Y + sy, Z);
-        const float e001 = fetch<float>(e, Lct, cbc, block, X, Y, Z + sz);
-        const float e101 = fetch<float>(e, Lct, cbc, block, X + sx, Y, Z + sz);
-        const float e011 = fetch<float>(e, Lct, cbc, block, X, Y + sy, Z + sz);
-        const float e111 = fetch<float>(e, Lct, cbc, block, X + sx, Y + sy, Z + sz);
-        const float a0 = 0.75f * e000 + 0.25f * e100;
-        const float a1 = 0.75f * e010 + 0.25f * e110;
-        const float a2 = 0.75f * e001 + 0.25f * e101;
-        const float a3 = 0.75f * e011 + 0.25f * e111;
+        float v[8];
+        if ((unsigned)(X + sx) < (unsigned)Lct.n[0] && (unsigned)(Y + sy) < (unsigned)Lct.n[1] &&
+            (unsigned)(Z + sz) < (unsigned)Lct.n[2]) {
+            const float *eb = e + (int64_t)block * Lct.bstride + X + (int64_t)Lct.n[0] * (Y + (int64_t)Lct.n[1] * Z);
+            const int64_t ox = sx, oy = (int64_t)sy * Lct.n[0], oz = (int64_t)sz * Lct.n[0] * Lct.n[1];
+            v[0] = __ldg(eb);
+            v[1] = __ldg(eb + ox);
+            v[2] = __ldg(eb + oy);
+            v[3] = __ldg(eb + ox + oy);
+            v[4] = __ldg(eb + oz);
+            v[5] = __ldg(eb + ox + oz);
+            v[6] = __ldg(eb + oy + oz);
+            v[7] = __ldg(eb + ox + oy + oz);
+        } else {
+            v[0] = fetch<float>(e, Lct, cbc, block, X, Y, Z);
+            v[1] = fetch<float>(e, Lct, cbc, block, X + sx, Y, Z);
+            v[2] = fetch<float>(e, Lct, cbc, block, X, Y + sy, Z);
+            v[3] = fetch<float>(e, Lct, cbc, block, X + sx, Y + sy, Z);
+            v[4] = fetch<float>(e, Lct, cbc, block, X, Y, Z + sz);
+            v[5] = fetch<float>(e, Lct, cbc, block, X + sx, Y, Z + sz);
+            v[6] = fetch<float>(e, Lct, cbc, block, X, Y + sy, Z + sz);
+            v[7] = fetch<float>(e, Lct, cbc, block, X + sx, Y + sy, Z + sz);
+        }
+        const float a0 = 0.75f * v[0] + 0.25f * v[1];
+        const float a1 = 0.75f * v[2] + 0.25f * v[3];
+        const float a2 = 0.75f * v[4] + 0.25f * v[5];
+        const float a3 = 0.75f * v[6] + 0.25f * v[7];
         const float b0 = 0.75f * a0 + 0.25f * a1;
         const float b1 = 0.75f * a2 + 0.25f * a3;
-        const float v = 0.75f * b0 + 0.25f * b1;
+        const float val = 0.75f * b0 + 0.25f * b1;
         const int64_t o = (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
-        p[o] = p[o] + v;
+        p[o] = p[o] + val;
     }
 }
 
 // FP64 residual of the outer iteration: r = f - L p64 (p64 += e first if e),
 // r32 = (float) r, per-CTA FP64 partial sums of r^2 (and f^2).
-__global__ void __launch_bounds__(256) resid64_kernel(KArgs a, const double *p64, const float *f,
+__global__ void __launch_bounds__(256) resid64_kernel(const __grid_constant__ KArgs a, const double *p64,
+                                                      const float *f,
                                                       float *r32, double *partials)
 {
     __shared__ double sh[2][8];
@@ -534,6 +573,8 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
         return fail(CN_ERR_UNSUPPORTED, "cn_mg_create: cubic cells are required");
     if (nu1 < 0 || nu2 < 0 || omega <= 0 || omega >= 2)
         return fail(CN_ERR_INVALID_ARGUMENT, "cn_mg_create: bad smoothing parameters");
+    if ((int64_t)k->nblocks * k->n[0] * k->n[1] * k->n[2] >= ((int64_t)1 << 31))
+        return fail(CN_ERR_UNSUPPORTED, "cn_mg_create: at most 2^31 - 1 cells");
     cn_mg *m = new cn_mg();
     m->nu1 = nu1;
     m->nu2 = nu2;
@@ -612,6 +653,8 @@ cn_status cn_mg_destroy(cn_mg *m)
     }
     cn_grid_destroy(m->r32);
     for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
+    for (void *a : m->nn_act)
+        if (a) cudaFree(a);
     if (m->partials) cudaFree(m->partials);
     if (m->sums) cudaFree(m->sums);
     if (m->iters) cudaFree(m->iters);

@@ -23,6 +23,7 @@ struct cn_mg {
     cn_nn *nn = nullptr;
     unsigned nn_levels = 0;
     std::vector<cn_grid *> nn_bufs; // 4 per level: X (2 comps), H1 (16), H2 (16), Y (1)
+    std::vector<void *> nn_act;     // 2 per level: BF16 channels-last activations (tensor-core path)
     // optional hook run at the finest level after the coarse-grid correction
     cn_status (*capture)(cn_mg *, cudaStream_t) = nullptr;
     void *capture_ctx = nullptr;

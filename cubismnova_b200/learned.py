@@ -22,6 +22,8 @@ _lib.register({
     "cn_nn_train": (_I, [_P, _P, _P, _P, _I, _I, _D, _I, _I, _D, C.c_uint64, C.POINTER(C.c_double), _P]),
     "cn_mg_collect_patches": (_I, [_P, _P, _I, _I, C.c_uint64, _P, _P, _P, _I, C.POINTER(_I), _P]),
     "cn_mg_set_smoother": (_I, [_P, _P, C.c_uint]),
+    "cn_nn_set_inference": (_I, [_P, _I]),
+    "cn_conv3_bf16": (_I, [_P, _P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P, _I, _P]),
 })
 
 CI, CH = 2, 16
@@ -62,6 +64,11 @@ class LearnedSmoother:
             out.append(w[o:o + n].reshape(s))
             o += n
         return out
+
+    def set_inference(self, mode: str):
+        """Grid inference on "tensor" cores (BF16 activations and weights,
+        tcgen05, FP32 accumulation; the default) or "fp32" CUDA cores."""
+        _lib.check(_lib.lib().cn_nn_set_inference(self._h, {"fp32": 0, "tensor": 1}[mode]))
 
     def set_weights(self, W1, W2, W3):
         w = np.concatenate([np.asarray(a, dtype=np.float32).ravel() for a in (W1, W2, W3)])
@@ -108,6 +115,19 @@ def collect_patches(mg, f: Cartesian, cycles: int, per_snapshot: int, max_patche
                                                 _stream_handle(stream)))
     m = cnt.value
     return x[:m].contiguous(), k[:m].contiguous(), r[:m].contiguous(), P
+
+
+def conv3_bf16(x, nblocks, block_cells, weights, relu: bool = False, stream=None):
+    """One 16 -> 16 channel 3x3x3 convolution on the tensor cores
+    (cn_conv3_bf16): x is a CUDA tensor [nblocks*cells, 16] of bfloat16 in
+    grid order, weights a CUDA float32 tensor [27, 16, 16]; returns a new
+    bfloat16 tensor of x's shape."""
+    import torch
+    out = torch.empty_like(x)
+    _lib.check(_lib.lib().cn_conv3_bf16(C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()), _lib.ivec3(nblocks),
+                                        _lib.ivec3(block_cells), C.c_void_p(weights.data_ptr()), 1 if relu else 0,
+                                        _stream_handle(stream)))
+    return out
 
 
 def use_in(mg, smoother, level_mask: int = 0xFFFF):

@@ -279,6 +279,17 @@ cn_status cn_mg_collect_patches(cn_mg *m, const cn_grid *f, int cycles, int per_
 /* Use the network instead of Jacobi on the levels set in level_mask (bit l);
  * nn == NULL restores Jacobi everywhere. */
 cn_status cn_mg_set_smoother(cn_mg *m, cn_nn *nn, unsigned level_mask);
+/* Grid inference precision: 1 (default) = BF16 activations and weights on
+ * the tensor cores (tcgen05, FP32 accumulation) on levels whose block cells
+ * are multiples of (16, 16, 4), else FP32; 0 = FP32 on the CUDA cores. */
+cn_status cn_nn_set_inference(cn_nn *nn, int mode);
+/* One 3x3x3 convolution, 16 -> 16 channels, on the tensor cores: in and out
+ * are device arrays [nblocks][cells][16] of BF16 (channels last, blocks and
+ * cells in grid order), neighbours across blocks periodic; weights FP32
+ * device [27][16][16] ([tap][cin][cout], rounded to BF16); optional ReLU.
+ * Block cells must be multiples of (16, 16, 4). */
+cn_status cn_conv3_bf16(const void *in, void *out, const int nblocks[3], const int block_cells[3],
+                        const float *weights, int relu, void *stream);
 
 /* ----------------------------------------------------- AMR block layouts */
 /* Cubic blocks of uneven sizes on two refinement levels (ratio 2) tiling a

@@ -306,6 +306,52 @@ def mg_coarse_cg(f, k, nb, n, ih2, max_iter=10000, rtol=1e-13):
     return p, it
 
 
+def _blocks(a, nb, n, dtype):
+    """(nblocks, cells) view of a block-strided component."""
+    nblk, cells = int(np.prod(nb)), int(np.prod(n))
+    return a.reshape(nblk, block_stride(n, dtype))[:, :cells]
+
+
+def mg_solve(k, f, nb, n, h, nu1=2, nu2=2, omega=0.8, rtol=1e-8, max_cycles=100):
+    """The device solver's algorithm on the CPU: FP32 V-cycles (levels halve
+    the block cells while even; weighted Jacobi, nu1 from a zero guess / nu2;
+    fused residual restriction; trilinear prolongation; CG on the coarsest
+    level) inside an FP64 defect correction p64 += V(r32), from p64 = 0 until
+    ||r|| <= rtol ||f||.  Returns (p64, cycles, relres)."""
+    ks, ns = [k], [list(n)]
+    while all(v % 2 == 0 for v in ns[-1]):
+        ks.append(mg_restrict_mean(ks[-1], nb, ns[-1]))
+        ns.append([v // 2 for v in ns[-1]])
+    ih2 = [1.0 / (h * 2 ** l) ** 2 for l in range(len(ns))]
+
+    def vcycle(l, fl):
+        if l == len(ns) - 1:
+            return mg_coarse_cg(fl, ks[l], nb, ns[l], ih2[l])[0]
+        p = None
+        for _ in range(nu1):
+            p = mg_jacobi(p, ks[l], fl, nb, ns[l], omega, ih2[l])
+        if p is None:
+            p = np.zeros_like(fl)
+        fc = mg_resid_restrict(p, ks[l], fl, nb, ns[l], ih2[l])
+        p = mg_prolong(p, vcycle(l + 1, fc), nb, ns[l])
+        for _ in range(nu2):
+            p = mg_jacobi(p, ks[l], fl, nb, ns[l], omega, ih2[l])
+        return p
+
+    p64 = np.zeros(int(np.prod(nb)) * block_stride(n, np.float64))
+    r32, rr, ff = mg_resid64(p64, k, f, nb, n, ih2[0])
+    fn = np.sqrt(ff)
+    rel = np.sqrt(rr) / fn if fn > 0 else 0.0
+    cycles = 0
+    while cycles < max_cycles and rel > rtol:
+        e = vcycle(0, r32)
+        _blocks(p64, nb, n, np.float64)[:] += _blocks(e, nb, n, np.float32).astype(np.float64)
+        r32, rr, _ = mg_resid64(p64, k, f, nb, n, ih2[0])
+        rel = np.sqrt(rr) / fn
+        cycles += 1
+    return p64, cycles, rel
+
+
 # ---------------------------------------------------------------------- AMR
 AMR_BLOCK = np.dtype([("level", "<i4"), ("n", "<i4"), ("ox", "<i4"), ("oy", "<i4"), ("oz", "<i4"),
                       ("pad", "<i4"), ("off", "<i8"), ("ih", "<f8")])

@@ -139,3 +139,24 @@ def test_manufactured_solution_second_order(cn):
         gv = got.view(p64.size(), -1)[:, :cells].reshape(4, 4, 4, n[2], n[1], n[0]).permute(0, 3, 1, 4, 2, 5).reshape(N, N, N)
         errs.append(float((gv - u).abs().max()))
     assert errs[1] < errs[0] / 3.0, errs
+
+
+def test_solve_matches_oracle_solve(cn, oracle_lib):
+    """The whole solve (V(2,2) cycles in FP64 defect correction) against the
+    oracle's composition of the same operators: the same cycle count (the
+    coarsest CG differs in summation order only) and the same solution up to
+    the periodic constant, within 1e-5 of its range."""
+    import torch
+    nb, n = (2, 2, 2), (16, 16, 16)
+    k, f = _setup(cn, nb, n)
+    m = cn.mg.Multigrid(k, nu1=2, nu2=2, omega=0.8)
+    p64 = cn.Grid.Cartesian(nb, n, dtype=np.float64)
+    cycles, rel = m.solve(f, p64, rtol=1e-8, max_cycles=60)
+    torch.cuda.synchronize()
+    want, wc, wrel = oracle_lib.mg_solve(k.download(), f.download(), nb, n, k.getCellSize()[0], rtol=1e-8,
+                                         max_cycles=60)
+    assert abs(cycles - wc) <= 1 and rel <= 1e-8 and wrel <= 1e-8
+    got = p64.blocks_view(p64.download())
+    ref = p64.blocks_view(want)
+    got, ref = got - got.mean(), ref - ref.mean()
+    assert np.max(np.abs(got - ref)) <= 1e-5 * np.ptp(ref)

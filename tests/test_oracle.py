@@ -209,3 +209,46 @@ def test_euler_oracle_constant_state_is_steady(oracle_lib):
     U[0], U[4] = 1.0, 2.5
     out = oracle_lib.euler_stage(U, None, nb, n, _c2_bclists(nb), 0, 0.0, 1.4, (1 / 16,) * 3)
     assert not out.any()
+
+
+def _to_global(a, nb, n, dtype, oracle_lib):
+    s = oracle_lib.block_stride(n, dtype)
+    cells = int(np.prod(n))
+    v = a.reshape(-1, s)[:, :cells].reshape(nb[2], nb[1], nb[0], n[2], n[1], n[0])
+    return v.transpose(0, 3, 1, 4, 2, 5).reshape(nb[2] * n[2], nb[1] * n[1], nb[0] * n[0])
+
+
+def test_mg_oracle_solve_satisfies_the_discrete_equation(oracle_lib):
+    """The oracle's multigrid solve reaches 1e-8 and its answer satisfies an
+    independent numpy statement of div(k grad p) = f (harmonic face means,
+    periodic) to that tolerance."""
+    nb, n = (2, 2, 2), (8, 8, 8)
+    G = nb[0] * n[0]
+    rng = np.random.default_rng(3)
+    s = oracle_lib.block_stride(n, np.float32)
+    N = int(np.prod(nb)) * s
+    kg = np.exp(0.3 * rng.standard_normal((G, G, G)))
+    for ax in range(3):
+        kg = (np.roll(kg, 1, ax) + kg + np.roll(kg, -1, ax)) / 3.0
+    fg = rng.standard_normal((G, G, G))
+    fg -= fg.mean()
+
+    def to_blocks(g):
+        v = g.reshape(nb[2], n[2], nb[1], n[1], nb[0], n[0]).transpose(0, 2, 4, 1, 3, 5).reshape(-1, int(np.prod(n)))
+        out = np.zeros((v.shape[0], s), dtype=np.float32)
+        out[:, :v.shape[1]] = v
+        return out.reshape(N)
+    k, f = to_blocks(kg), to_blocks(fg)
+    h = 1.0 / G
+    p64, cycles, rel = oracle_lib.mg_solve(k, f, nb, n, h, rtol=1e-8, max_cycles=40)
+    assert rel <= 1e-8 and cycles < 40
+    p = _to_global(p64, nb, n, np.float64, oracle_lib)
+    k32 = _to_global(k, nb, n, np.float32, oracle_lib).astype(np.float64)
+    f32 = _to_global(f, nb, n, np.float32, oracle_lib).astype(np.float64)
+    Lp = np.zeros_like(p)
+    for ax in range(3):
+        kp, km = np.roll(k32, -1, ax), np.roll(k32, 1, ax)
+        hp, hm = 2 * k32 * kp / (k32 + kp), 2 * km * k32 / (km + k32)
+        Lp += hp * (np.roll(p, -1, ax) - p) - hm * (p - np.roll(p, 1, ax))
+    Lp /= h * h
+    assert np.linalg.norm(f32 - Lp) <= 2e-8 * np.linalg.norm(f32)
