@@ -112,7 +112,9 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- dist helpers
-def dist_setup(args):
+def dist_setup(args, backend=None):
+    """One process per GPU under torchrun (RANK / LOCAL_RANK / WORLD_SIZE);
+    NCCL unless `backend` says otherwise (the CPU tests use gloo)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -122,8 +124,10 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = backend or "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -134,10 +138,12 @@ def barrier(pg):
 
 
 def max_over_ranks(pg, value: float) -> float:
+    """Largest value over the ranks (device times: the job's time is the slowest rank's)."""
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 

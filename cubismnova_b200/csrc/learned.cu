@@ -25,7 +25,10 @@
 // neighbourhood a FieldLab would give it.
 #include "cn_internal.h"
 #include "learned_tc.h"
+#include "mg_tile.cuh"
 #include "mg_internal.h"
+
+#include <cuda_bf16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -345,39 +348,60 @@ namespace cn {
 namespace nn {
 
 // x0 = (L p - f) / D = -r / D (the Jacobi correction; L has diagonal -D),
-// x1 = x0 ln k, with r = f - L p (p == NULL: p = 0), and r itself.
-__global__ void __launch_bounds__(256) features_grid(const float *p, const float *k, const float *f,
-                                                     const __grid_constant__ LabGeom L,
-                                                     const __grid_constant__ BcView pbc,
-                                                     const __grid_constant__ BcView kbc, int nblocks, float ih2, float *x0, float *x1, float *rout)
+// x1 = x0 ln k, with r = f - L p (p == NULL: p = 0), and r itself; with
+// `packed`, also the BF16 channels-last input of the tensor-core layers,
+// (x0, x1, 0, ..., 0) per cell.  One CTA per tile of a block: p and k with a
+// one-cell halo staged in shared memory (mg_tile.cuh).
+struct FeatArgs {
+    LabGeom L;
+    BcView pbc, kbc;
+    const float *p, *k, *f;
+    const float *coef; // level coefficients of the multigrid (component stride ccs)
+    int64_t ccs;
+    float ih2;
+    float *x0, *x1, *rout;
+    uint16_t *packed;
+};
+
+__global__ void __launch_bounds__(mg::kTileThreads, mg::kTileMinCtas) features_tile(const __grid_constant__ FeatArgs A,
+                                                                  const __grid_constant__ mg::Tile T)
 {
-    const int64_t cells = (int64_t)L.n[0] * L.n[1] * L.n[2];
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < cells * nblocks; t += (int64_t)gridDim.x * blockDim.x) {
-        const int block = (int)(t / cells);
-        const int64_t c = t - block * cells;
-        const int x = (int)(c % L.n[0]), y = (int)((c / L.n[0]) % L.n[1]), z = (int)(c / ((int64_t)L.n[0] * L.n[1]));
-        const int64_t o = (int64_t)block * L.bstride + c;
-        const float kc = __ldg(k + o);
-        const float pc = p ? __ldg(p + o) : 0.f;
-        float fl[3], s[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const int ox = d == 0, oy = d == 1, oz = d == 2;
-            const float kp = harmf(kc, gfetch<float>(k, L, kbc, block, x + ox, y + oy, z + oz));
-            const float km = harmf(gfetch<float>(k, L, kbc, block, x - ox, y - oy, z - oz), kc);
-            const float pp = p ? gfetch<float>(p, L, pbc, block, x + ox, y + oy, z + oz) : 0.f;
-            const float pm = p ? gfetch<float>(p, L, pbc, block, x - ox, y - oy, z - oz) : 0.f;
-            fl[d] = kp * (pp - pc) - km * (pc - pm);
-            s[d] = kp + km;
-        }
-        const float Lp = ih2 * ((fl[0] + fl[1]) + fl[2]);
-        const float D = ih2 * ((s[0] + s[1]) + s[2]);
-        const float fc = __ldg(f + o);
+    __shared__ float sp[mg::kRegionMax];
+    __shared__ int snb[27];
+    const LabGeom &L = A.L;
+    const mg::TilePos q = mg::tile_pos(T);
+    mg::neighbour_blocks(L.nb, q.block, snb);
+    __syncthreads();
+    if (A.p)
+        mg::stage_region<float>(A.p, L, A.pbc, q, false, snb, sp);
+    else
+        for (int u = threadIdx.x; u < q.ex * q.ey * q.ez; u += mg::kTileThreads) sp[u] = 0.f;
+    mg::cp_async_wait_all();
+    __syncthreads();
+    const int cells = T.t[0] * T.t[1] * T.t[2];
+    const int64_t bcells = (int64_t)L.n[0] * L.n[1] * L.n[2];
+    const int st[3] = {1, q.ex, q.ex * q.ey};
+    for (int c = threadIdx.x; c < cells; c += mg::kTileThreads) {
+        int x, y, z;
+        mg::tile_cell(T, c, x, y, z);
+        const int64_t lc = (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
+        const int64_t o = (int64_t)q.block * L.bstride + lc;
+        float Lp, D, pc;
+        mg::op7_coef<float>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, A.coef, A.ccs, o, A.ih2, Lp, D, pc);
+        const float fc = __ldg(A.f + o);
         const float r = fc - Lp;
         const float a = (Lp - fc) / D;
-        x0[o] = a;
-        x1[o] = a * logf(kc);
-        if (rout) rout[o] = r;
+        const float b = a * logf(__ldg(A.k + o));
+        A.x0[o] = a;
+        A.x1[o] = b;
+        if (A.rout) A.rout[o] = r;
+        if (A.packed) {
+            const uint32_t w0 = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
+                                ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+            uint4 *dst = reinterpret_cast<uint4 *>(A.packed + ((int64_t)q.block * bcells + lc) * 16);
+            dst[0] = make_uint4(w0, 0u, 0u, 0u);
+            dst[1] = make_uint4(0u, 0u, 0u, 0u);
+        }
     }
 }
 
@@ -694,15 +718,26 @@ static cn_status conv_on_grid(cn_grid *in, cn_grid *out, const float *W, const L
     return CN_OK;
 }
 
-static cn_status features(cn_mg *m, int l, const float *p, const float *f, float *rout, cudaStream_t st)
+static cn_status features(cn_mg *m, int l, const float *p, const float *f, float *rout, cudaStream_t st,
+                          uint16_t *packed = nullptr)
 {
     cn_grid *X = m->nn_bufs[4 * l];
-    const LabGeom L = make_geom(m->p[l], &kS1);
-    const int64_t n = (int64_t)m->p[l]->nblocks * L.n[0] * L.n[1] * L.n[2];
-    float *x0 = reinterpret_cast<float *>(X->d_data);
-    features_grid<<<nblk(n), 256, 0, st>>>(p, fptr(m->k[l]), f, L, bc_view(m->p[l], 0), bc_view(m->k[l], 0),
-                                            m->p[l]->nblocks, (float)(1.0 / (m->p[l]->h[0] * m->p[l]->h[0])), x0,
-                                            x0 + X->comp_stride, rout);
+    FeatArgs A;
+    A.L = make_geom(m->p[l], &kS1);
+    A.pbc = bc_view(m->p[l], 0);
+    A.kbc = bc_view(m->k[l], 0);
+    A.p = p;
+    A.k = fptr(m->k[l]);
+    A.f = f;
+    A.coef = reinterpret_cast<const float *>(m->coef[l]->d_data);
+    A.ccs = m->coef[l]->comp_stride;
+    A.ih2 = (float)(1.0 / (m->p[l]->h[0] * m->p[l]->h[0]));
+    A.x0 = reinterpret_cast<float *>(X->d_data);
+    A.x1 = A.x0 + X->comp_stride;
+    A.rout = rout;
+    A.packed = packed;
+    const mg::Tile T = mg::tile_of(m->p[l]->n);
+    features_tile<<<(unsigned)(m->p[l]->nblocks * T.count), mg::kTileThreads, 0, st>>>(A, T);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
@@ -727,9 +762,9 @@ static cn_status nn_smooth_tc(cn_mg *m, int l, int apps, bool zero_guess, cudaSt
     const float *x = reinterpret_cast<const float *>(X->d_data);
     for (int a = 0; a < apps; ++a) {
         const bool zg = zero_guess && a == 0;
-        if ((s = features(m, l, zg ? nullptr : fptr(P), fptr(m->f[l]), nullptr, st)) != CN_OK) return s;
-        if ((s = nntc::conv_features(x, X->comp_stride, X->block_stride, P->nb, P->n, w1, h1, P->d_err, st)) != CN_OK)
-            return s;
+        // features -> packed BF16 in h2 -> layer 1 -> h1 -> layer 2 -> h2 -> layer 3 + update
+        if ((s = features(m, l, zg ? nullptr : fptr(P), fptr(m->f[l]), nullptr, st, h2)) != CN_OK) return s;
+        if ((s = nntc::conv_hidden(h2, P->nb, P->n, w1, 1, h1, P->d_err, st)) != CN_OK) return s;
         if ((s = nntc::conv_hidden(h1, P->nb, P->n, w2, 1, h2, P->d_err, st)) != CN_OK) return s;
         if ((s = nntc::conv_update(h2, P->nb, P->n, w3, x, X->block_stride, fptr(P), P->block_stride,
                                    (float)nn->omega, zg ? 1 : 0, P->d_err, st)) != CN_OK)

@@ -22,20 +22,21 @@
 // channels x K = 16 input channels) uses the same form: planes of 16 rows.
 //
 // Layers: 2 -> 16 (input channels padded with zeros to 16), 16 -> 16, and
-// 16 -> 1 (output channels padded to N = 16); ReLU after the first two.  The
-// first layer reads the FP32 features (x0, x1) of the grid; hidden
-// activations are channels-last BF16, 32 bytes per cell; the last layer
-// applies the smoothing update p += omega x0 + y in its epilogue.
+// 16 -> 1 (output channels padded to N = 16); ReLU after the first two.  All
+// inputs are channels-last BF16, 32 bytes per cell (the features kernel
+// writes (x0, x1, 0, ..., 0)), staged with asynchronous 16-byte copies; the
+// last layer applies the smoothing update p += omega x0 + y in its epilogue.
 // Neighbour cells outside the block are the periodic neighbours of the block
 // grid (the activation grids carry no BCs), corners and edges included.
 //
-// One thread issues the MMAs and commits them to an mbarrier; all threads
-// wait on it with a bounded poll (on timeout the CTA records an error word,
-// skips its epilogue, frees its TMEM and exits).
+// One thread issues the MMAs, commits them to an mbarrier and polls it
+// (bounded; on timeout the CTA records an error word, skips its epilogue,
+// frees its TMEM and exits) while the other threads wait at the CTA barrier.
 #include "cn_internal.h"
 #include "cn_tc.cuh"
 #include "cn_tma.cuh"
 #include "learned_tc.h"
+#include "mg_tile.cuh"
 
 #include <cuda_bf16.h>
 
@@ -54,20 +55,17 @@ constexpr int NTHREADS = 256;
 constexpr int TMEM_COLS = 256;                       // >= 16 * MT
 constexpr uint32_t PLANE = SROWS * 16;               // bytes of one K plane of A
 constexpr uint32_t WTAP = 512;                       // bytes of one tap's B (2 planes x 16 rows x 16 B)
-constexpr size_t SMEM = 2 * (size_t)PLANE + 27 * WTAP + 16;
+constexpr size_t SMEM = 2 * (size_t)PLANE + 27 * WTAP + 16 + 28 * 4;
 constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 16);
 static_assert(RCELLS <= SROWS, "region must fit the A rows");
 static_assert(16 * MT <= TMEM_COLS, "accumulators must fit the TMEM allocation");
 
 struct Params {
-    // input: mode 0 reads FP32 components x0 (comp 0) and x1 (comp 1) of a
-    // block grid; modes 1, 2 read channels-last BF16 activations
-    const float *x;        // features, component-major (comp stride xcs)
-    int64_t xcs;
-    int64_t xbs;           // block stride (elements) of the feature grid
-    const uint16_t *act;   // [nblocks][cells][16] BF16
+    const uint16_t *act;   // input activations [nblocks][cells][16] BF16
+    const float *x;        // mode 2: x0 of the features grid (block stride xbs)
+    int64_t xbs;
     const uint16_t *w;     // [27][2][16][8] BF16 B tiles of this layer
-    // output: mode 0, 1 write BF16 activations (ReLU); mode 2 updates p
+    // output: mode 1 writes BF16 activations (optional ReLU); mode 2 updates p
     uint16_t *out;
     float *p;              // mode 2: p (FP32 grid, block stride pbs)
     int64_t pbs;
@@ -84,20 +82,6 @@ __device__ __forceinline__ uint16_t bf16_bits(float v)
     return __bfloat16_as_ushort(__float2bfloat16_rn(v));
 }
 
-// block-local cell (x, y, z), one cell outside allowed, of block b -> (block, cell)
-__device__ __forceinline__ void wrap_cell(const Params &P, int b, int x, int y, int z, int &ob, int &oc)
-{
-    int bx = b % P.nb[0], by = (b / P.nb[0]) % P.nb[1], bz = b / (P.nb[0] * P.nb[1]);
-    if (x < 0) { x += P.n[0]; bx = bx == 0 ? P.nb[0] - 1 : bx - 1; }
-    else if (x >= P.n[0]) { x -= P.n[0]; bx = bx == P.nb[0] - 1 ? 0 : bx + 1; }
-    if (y < 0) { y += P.n[1]; by = by == 0 ? P.nb[1] - 1 : by - 1; }
-    else if (y >= P.n[1]) { y -= P.n[1]; by = by == P.nb[1] - 1 ? 0 : by + 1; }
-    if (z < 0) { z += P.n[2]; bz = bz == 0 ? P.nb[2] - 1 : bz - 1; }
-    else if (z >= P.n[2]) { z -= P.n[2]; bz = bz == P.nb[2] - 1 ? 0 : bz + 1; }
-    ob = bx + P.nb[0] * (by + P.nb[1] * bz);
-    oc = x + P.n[0] * (y + P.n[1] * z);
-}
-
 template <int MODE>
 __global__ void __launch_bounds__(NTHREADS) conv3_tc_kernel(const __grid_constant__ Params P)
 {
@@ -106,6 +90,8 @@ __global__ void __launch_bounds__(NTHREADS) conv3_tc_kernel(const __grid_constan
     unsigned char *Bw = smem + 2 * PLANE;          // [27][2][16][16 B]
     uint64_t *bar = reinterpret_cast<uint64_t *>(Bw + 27 * WTAP);
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
+    int *snb = reinterpret_cast<int *>(slot + 1);   // 27 periodic neighbour blocks
+    int *okf = snb + 27;                            // MMA completion flag
 
     const int bricks = P.bricks[0] * P.bricks[1] * P.bricks[2];
     const int block = blockIdx.x / bricks;
@@ -125,57 +111,59 @@ __global__ void __launch_bounds__(NTHREADS) conv3_tc_kernel(const __grid_constan
         tc::tmem_alloc(slot, TMEM_COLS);
         tc::tmem_relinquish();
     }
+    mg::neighbour_blocks(P.nb, block, snb);
+    __syncthreads();
 
     // ---- weights: 27 taps x 512 B as 16-byte chunks
     for (int i = threadIdx.x; i < 27 * 32; i += NTHREADS)
         reinterpret_cast<uint4 *>(Bw)[i] = __ldg(reinterpret_cast<const uint4 *>(P.w) + i);
 
-    // ---- input region: row u = region cell, two 16-byte chunks (K planes)
+    // ---- input region: row u = region cell, two 16-byte chunks (K planes),
+    // asynchronous 16-byte copies (many in flight per thread); rows past the
+    // region are zero
     for (int t = threadIdx.x; t < 2 * SROWS; t += NTHREADS) {
         const int u = t >> 1, kc = t & 1;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        unsigned char *dst = A + kc * PLANE + u * 16;
         if (u < RCELLS) {
             const int i = u % RX, j = (u / RX) % RY, k = u / (RX * RY);
             const int x = ox + i - 1, y = oy + j - 1, z = oz + k - 1;
-            int sb = block, sc;
-            if ((unsigned)x < (unsigned)P.n[0] && (unsigned)y < (unsigned)P.n[1] && (unsigned)z < (unsigned)P.n[2])
-                sc = x + P.n[0] * (y + P.n[1] * z);
-            else
-                wrap_cell(P, block, x, y, z, sb, sc);
-            if (MODE == 0) {
-                if (kc == 0) {
-                    const int64_t o = (int64_t)sb * P.xbs + sc;
-                    const float a = __ldg(P.x + o), b = __ldg(P.x + P.xcs + o);
-                    v.x = (uint32_t)bf16_bits(a) | ((uint32_t)bf16_bits(b) << 16);
-                }
-            } else {
-                v = __ldg(reinterpret_cast<const uint4 *>(P.act + ((int64_t)sb * cells + sc) * 16) + kc);
-            }
+            const int r0 = x < 0 ? -1 : (x >= P.n[0] ? 1 : 0), r1 = y < 0 ? -1 : (y >= P.n[1] ? 1 : 0),
+                      r2 = z < 0 ? -1 : (z >= P.n[2] ? 1 : 0);
+            const int sb = snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+            const int sc = (x - r0 * P.n[0]) + P.n[0] * ((y - r1 * P.n[1]) + P.n[1] * (z - r2 * P.n[2]));
+            const uint16_t *src = P.act + ((int64_t)sb * cells + sc) * 16 + kc * 8;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+        } else {
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(0u, 0u, 0u, 0u);
         }
-        *reinterpret_cast<uint4 *>(A + kc * PLANE + u * 16) = v;
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     fence_proxy_async_smem(); // generic-proxy smem writes -> visible to the tensor cores
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tbase = *slot;
 
-    // ---- MMAs: 10 M-tiles x 27 taps, one issuing thread
+    // ---- MMAs: 10 M-tiles x 27 taps, issued by one thread, which then
+    // polls the completion barrier (bounded) while the others wait at the
+    // CTA barrier.  Descriptor start addresses advance in 16-byte units.
     if (threadIdx.x == 0) {
-        const uint32_t a0 = smem_u32(A), b0 = smem_u32(Bw);
+        const uint64_t da = tc::smem_desc(smem_u32(A), PLANE, 128u);
+        const uint64_t db = tc::smem_desc(smem_u32(Bw), 256u, 128u);
 #pragma unroll 1
         for (int t = 0; t < MT; ++t) {
-#pragma unroll 1
+#pragma unroll
             for (int q = 0; q < 27; ++q) {
                 const int off = (q % 3 - 1) + RX * ((q / 3) % 3 - 1) + RX * RY * (q / 9 - 1);
-                const uint32_t row = (uint32_t)(R0 + 128 * t + off);
-                tc::mma_bf16(tbase + 16u * t, tc::smem_desc(a0 + row * 16u, PLANE, 128u),
-                             tc::smem_desc(b0 + q * WTAP, 256u, 128u), IDESC, q > 0 ? 1u : 0u);
+                tc::mma_bf16(tbase + 16u * t, da + (uint64_t)(R0 + 128 * t + off), db + (uint64_t)(q * (WTAP / 16)),
+                             IDESC, q > 0 ? 1u : 0u);
             }
         }
         tc::mma_commit(bar);
+        *okf = mbar_wait_bounded(bar, 0) ? 1 : 0;
     }
-    const int ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0);
+    __syncthreads();
+    const int ok = *okf;
     tc::fence_after_sync();
 
     // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 of the tiles t = w / 4, w / 4 + 2, ...
@@ -235,7 +223,7 @@ __global__ void pack_weights_kernel(const float *W, int cin, int cout, uint16_t 
     out[i] = bf16_bits(v);
 }
 
-static bool attr_set[3];
+static bool attr_set[3]; // per mode (1: hidden layer, 2: last layer + update)
 
 template <int MODE>
 static cn_status launch(const Params &P, int nblocks, cudaStream_t st)
@@ -275,19 +263,6 @@ static Params base_params(const int nb[3], const int n[3], int *err)
     P.bricks[2] = n[2] / BZ;
     P.err = err;
     return P;
-}
-
-cn_status conv_features(const float *x, int64_t xcs, int64_t xbs, const int nb[3], const int n[3],
-                        const uint16_t *w, uint16_t *out, int *err, cudaStream_t st)
-{
-    Params P = base_params(nb, n, err);
-    P.x = x;
-    P.xcs = xcs;
-    P.xbs = xbs;
-    P.w = w;
-    P.out = out;
-    P.relu = 1;
-    return launch<0>(P, nb[0] * nb[1] * nb[2], st);
 }
 
 cn_status conv_hidden(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, int relu,

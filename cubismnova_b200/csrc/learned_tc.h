@@ -16,10 +16,7 @@ constexpr size_t kPackedWeightBytes = 27 * 512;
 bool supported(const int n[3]);
 // FP32 [27][cin][cout] -> packed BF16 B tiles (cin, cout <= 16, zero padded)
 cn_status pack_weights(const float *W, int cin, int cout, uint16_t *out, cudaStream_t st);
-// layer 1: FP32 features x0 = x[0..], x1 = x[xcs..] (block stride xbs) -> ReLU -> BF16 activations
-cn_status conv_features(const float *x, int64_t xcs, int64_t xbs, const int nb[3], const int n[3],
-                        const uint16_t *w, uint16_t *out, int *err, cudaStream_t st);
-// hidden layer: BF16 activations -> (ReLU) -> BF16 activations
+// hidden layer (also the first, on the packed features): BF16 activations -> (ReLU) -> BF16 activations
 cn_status conv_hidden(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, int relu,
                       uint16_t *out, int *err, cudaStream_t st);
 // last layer (output channel 0) fused with p = (zero_guess ? 0 : p) + (omega x0 + y)

@@ -17,6 +17,7 @@
 // the same lab resolution as every other stencil (periodic block wrap, and the
 // grid's BCs if any); halo cells inside a block are plain cached loads.
 #include "cn_internal.h"
+#include "mg_tile.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -59,127 +60,127 @@ __device__ __forceinline__ T fetch(const T *comp, const LabGeom &L, const BcView
     return lab_fetch<T>(comp, L, bc, block, x, y, z);
 }
 
-template <typename T> __device__ __forceinline__ T harm(T a, T b)
-{
-    const T t = a * b;
-    return (t + t) / (a + b);
-}
-
-// The 13 values of the 7-point operator at one cell: v[0] = p, v[1] = k,
-// then per direction d: p(+e_d), p(-e_d), k(+e_d), k(-e_d); p == NULL reads
-// as zero.  Cells interior to their block take plain loads.
-template <typename TP>
-__device__ __forceinline__ void load7(const TP *p, const float *k, const Geo &G, const BcView &kbc, int block,
-                                      int x, int y, int z, TP (&v)[14])
-{
-    const LabGeom &L = G.L, &Lk = G.Lk;
-    if (x > 0 && y > 0 && z > 0 && x < L.n[0] - 1 && y < L.n[1] - 1 && z < L.n[2] - 1) {
-        const int64_t cell = x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
-        const TP *pb = p ? p + (int64_t)block * L.bstride + cell : nullptr;
-        const float *kb = k + (int64_t)block * Lk.bstride + cell;
-        const int64_t st[3] = {1, L.n[0], (int64_t)L.n[0] * L.n[1]};
-        v[0] = pb ? __ldg(pb) : TP(0);
-        v[1] = (TP)__ldg(kb);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            v[2 + 4 * d] = pb ? __ldg(pb + st[d]) : TP(0);
-            v[3 + 4 * d] = pb ? __ldg(pb - st[d]) : TP(0);
-            v[4 + 4 * d] = (TP)__ldg(kb + st[d]);
-            v[5 + 4 * d] = (TP)__ldg(kb - st[d]);
-        }
-    } else {
-        v[0] = p ? fetch<TP>(p, L, G.bc, block, x, y, z) : TP(0);
-        v[1] = (TP)fetch<float>(k, Lk, kbc, block, x, y, z);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const int ox = d == 0, oy = d == 1, oz = d == 2;
-            v[2 + 4 * d] = p ? fetch<TP>(p, L, G.bc, block, x + ox, y + oy, z + oz) : TP(0);
-            v[3 + 4 * d] = p ? fetch<TP>(p, L, G.bc, block, x - ox, y - oy, z - oz) : TP(0);
-            v[4 + 4 * d] = (TP)fetch<float>(k, Lk, kbc, block, x + ox, y + oy, z + oz);
-            v[5 + 4 * d] = (TP)fetch<float>(k, Lk, kbc, block, x - ox, y - oy, z - oz);
-        }
-    }
-}
-
-// L p and the diagonal D at one cell from its 13 values; TP is the solution
-// type (float in the V-cycle, double in the outer residual), k is FP32.
-template <typename TP>
-__device__ __forceinline__ void op7_math(const TP (&v)[14], TP ih2, TP &Lp, TP &D, TP &pc)
-{
-    pc = v[0];
-    const TP kc = v[1];
-    TP f[3], s[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const TP pp = v[2 + 4 * d], pm = v[3 + 4 * d];
-        const TP kp = harm<TP>(kc, v[4 + 4 * d]);
-        const TP km = harm<TP>(v[5 + 4 * d], kc);
-        f[d] = kp * (pp - pc) - km * (pc - pm);
-        s[d] = kp + km;
-    }
-    Lp = ih2 * ((f[0] + f[1]) + f[2]);
-    D = ih2 * ((s[0] + s[1]) + s[2]);
-}
-
-template <typename TP>
-__device__ __forceinline__ void op7(const TP *p, const float *k, const Geo &G, const BcView &kbc,
-                                    int block, int x, int y, int z, TP ih2, TP &Lp, TP &D, TP &pc)
-{
-    TP v[14];
-    load7<TP>(p, k, G, kbc, block, x, y, z, v);
-    op7_math<TP>(v, ih2, Lp, D, pc);
-}
-
 struct KArgs {
     Geo G;
     BcView kbc;
     const float *k;
+    const float *coef; // level coefficients (7 components, component stride ccs)
+    int64_t ccs;
     float ih2;
     double ih2d;
 };
 
-// weighted Jacobi sweep: pout = pin + omega (L pin - f) / D  (pin == NULL: zero guess)
-__global__ void __launch_bounds__(256) jacobi_kernel(const __grid_constant__ KArgs a, const float *pin,
-                                                     const float *f, float *pout, float omega)
+// Coefficients of one level (see op7_coef): k staged per tile with its
+// one-cell halo, then per cell the same operations as op7_math.
+__global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const __grid_constant__ KArgs a,
+                                                            const __grid_constant__ Tile T, float *coef)
 {
+    __shared__ float sk[kRegionMax];
+    __shared__ int snb[27];
     const LabGeom &L = a.G.L;
-    const int64_t total = (int64_t)a.G.nblocks * L.n[0] * L.n[1] * L.n[2];
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        int block, x, y, z;
-        cell_of(t, L, block, x, y, z);
-        const int64_t o = (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
+    const TilePos q = tile_pos(T);
+    neighbour_blocks(L.nb, q.block, snb);
+    __syncthreads();
+    stage_region<float>(a.k, a.G.Lk, a.kbc, q, false, snb, sk);
+    cp_async_wait_all();
+    __syncthreads();
+    const int cells = T.t[0] * T.t[1] * T.t[2];
+    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
+        int x, y, z;
+        tile_cell(T, c, x, y, z);
+        const int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
+        const int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1));
+        const int st[3] = {1, q.ex, q.ex * q.ey};
+        const float kc = sk[u];
+        float sd[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float kp = harm<float>(kc, sk[u + st[d]]);
+            const float km = harm<float>(sk[u - st[d]], kc);
+            coef[d * a.ccs + o] = kp;
+            coef[(3 + d) * a.ccs + o] = km;
+            sd[d] = kp + km;
+        }
+        coef[6 * a.ccs + o] = a.ih2 * ((sd[0] + sd[1]) + sd[2]);
+    }
+}
+
+// weighted Jacobi sweep: pout = pin + omega (L pin - f) / D  (pin == NULL: zero guess)
+__global__ void __launch_bounds__(kTileThreads, kTileMinCtas) jacobi_kernel(const __grid_constant__ KArgs a,
+                                                              const __grid_constant__ Tile T, const float *pin,
+                                                              const float *f, float *pout, float omega)
+{
+    __shared__ float sp[kRegionMax];
+    __shared__ int snb[27];
+    const LabGeom &L = a.G.L;
+    const TilePos q = tile_pos(T);
+    if (pin) {
+        neighbour_blocks(L.nb, q.block, snb);
+        __syncthreads();
+        stage_region<float>(pin, L, a.G.bc, q, false, snb, sp);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    const int cells = T.t[0] * T.t[1] * T.t[2];
+    const int st[3] = {1, q.ex, q.ex * q.ey};
+    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
+        int x, y, z;
+        tile_cell(T, c, x, y, z);
+        const int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
         const float fc = __ldg(f + o);
-        float Lp, D, pc;
-        op7<float>(pin, a.k, a.G, a.kbc, block, x, y, z, a.ih2, Lp, D, pc);
-        // zero guess (pin == NULL): L 0 = 0, only the diagonal is used
-        pout[o] = pin ? pc + omega * ((Lp - fc) / D) : 0.0f + omega * ((0.0f - fc) / D);
+        if (pin) {
+            float Lp, D, pc;
+            op7_coef<float>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
+            pout[o] = pc + omega * ((Lp - fc) / D);
+        } else {
+            // zero guess: L 0 = 0, only the diagonal is used
+            const float D = __ldg(a.coef + 6 * a.ccs + o);
+            pout[o] = 0.0f + omega * ((0.0f - fc) / D);
+        }
     }
 }
 
 // residual of the fine level restricted onto the coarse right-hand side:
-// one thread per coarse cell, fc = (sum of its 8 children's f - L p) / 8
-__global__ void __launch_bounds__(256) resid_restrict_kernel(const __grid_constant__ KArgs a, const float *p,
-                                                             const float *f,
-                                                             LabGeom Lc, float *fc)
+// fc = (sum of its 8 children's f - L p) / 8, children summed in the order
+// ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), child c = dx | dy<<1 | dz<<2
+__global__ void __launch_bounds__(kTileThreads, kTileMinCtas) resid_restrict_kernel(const __grid_constant__ KArgs a,
+                                                                      const __grid_constant__ Tile T,
+                                                                      const float *p, const float *f,
+                                                                      const __grid_constant__ LabGeom Lc, float *fc)
 {
+    __shared__ float sp[kRegionMax];
+    __shared__ float sr[32 * 8 * 4];
+    __shared__ int snb[27];
     const LabGeom &L = a.G.L;
-    const int64_t total = (int64_t)a.G.nblocks * Lc.n[0] * Lc.n[1] * Lc.n[2];
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        int block, X, Y, Z;
-        cell_of(t, Lc, block, X, Y, Z);
+    const TilePos q = tile_pos(T);
+    neighbour_blocks(L.nb, q.block, snb);
+    __syncthreads();
+    stage_region<float>(p, L, a.G.bc, q, false, snb, sp);
+    cp_async_wait_all();
+    __syncthreads();
+    const int cells = T.t[0] * T.t[1] * T.t[2];
+    const int st[3] = {1, q.ex, q.ex * q.ey};
+    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
+        int x, y, z;
+        tile_cell(T, c, x, y, z);
+        const int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
+        float Lp, D, pc;
+        op7_coef<float>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
+        sr[c] = __ldg(f + o) - Lp;
+    }
+    __syncthreads();
+    const int hx = T.t[0] / 2, hy = T.t[1] / 2, hz = T.t[2] / 2;
+    for (int c = threadIdx.x; c < hx * hy * hz; c += kTileThreads) {
+        const int X = c % hx, Y = (c / hx) % hy, Z = c / (hx * hy);
         float r[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int x = 2 * X + (c & 1), y = 2 * Y + ((c >> 1) & 1), z = 2 * Z + (c >> 2);
-            const int64_t o = (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
-            float Lp, D, pc;
-            op7<float>(p, a.k, a.G, a.kbc, block, x, y, z, a.ih2, Lp, D, pc);
-            r[c] = __ldg(f + o) - Lp;
+        for (int ch = 0; ch < 8; ++ch) {
+            const int x = 2 * X + (ch & 1), y = 2 * Y + ((ch >> 1) & 1), z = 2 * Z + (ch >> 2);
+            r[ch] = sr[x + T.t[0] * (y + T.t[1] * z)];
         }
         const float s = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-        fc[(int64_t)block * Lc.bstride + X + (int64_t)Lc.n[0] * (Y + (int64_t)Lc.n[1] * Z)] = s * 0.125f;
+        const int gx = q.x0 / 2 + X, gy = q.y0 / 2 + Y, gz = q.z0 / 2 + Z;
+        fc[(int64_t)q.block * Lc.bstride + gx + (int64_t)Lc.n[0] * (gy + (int64_t)Lc.n[1] * gz)] = s * 0.125f;
     }
 }
 
@@ -203,72 +204,78 @@ __global__ void __launch_bounds__(256) restrict_mean_kernel(LabGeom L, const flo
     }
 }
 
-// p_fine += trilinear interpolation of the coarse correction e
-__global__ void __launch_bounds__(256) prolong_kernel(const __grid_constant__ LabGeom L, float *p,
-                                                      const __grid_constant__ LabGeom Lct,
-                                                      const __grid_constant__ BcView cbc, const float *e,
-                                                      int nblocks)
+// p_fine += trilinear interpolation of the coarse correction e: the fine
+// tile's coarse cells plus a one-cell halo (edges and corners included) are
+// staged, then each fine cell combines its 8 coarse values.
+__global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(const __grid_constant__ LabGeom L,
+                                                               const __grid_constant__ Tile T, float *p,
+                                                               const __grid_constant__ LabGeom Lct,
+                                                               const __grid_constant__ BcView cbc, const float *e)
 {
-    const int64_t total = (int64_t)nblocks * L.n[0] * L.n[1] * L.n[2];
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        int block, x, y, z;
-        cell_of(t, L, block, x, y, z);
+    __shared__ float se[(16 + 2) * (4 + 2) * (2 + 2)];
+    __shared__ int snb[27];
+    const TilePos qf = tile_pos(T);
+    neighbour_blocks(Lct.nb, qf.block, snb);
+    __syncthreads();
+    TilePos qc = qf;
+    qc.x0 = qf.x0 / 2;
+    qc.y0 = qf.y0 / 2;
+    qc.z0 = qf.z0 / 2;
+    qc.ex = T.t[0] / 2 + 2;
+    qc.ey = T.t[1] / 2 + 2;
+    qc.ez = T.t[2] / 2 + 2;
+    stage_region<float>(e, Lct, cbc, qc, true, snb, se);
+    cp_async_wait_all();
+    __syncthreads();
+    const int cells = T.t[0] * T.t[1] * T.t[2];
+    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
+        int x, y, z;
+        tile_cell(T, c, x, y, z);
         const int X = x >> 1, Y = y >> 1, Z = z >> 1;
         const int sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1, sz = (z & 1) ? 1 : -1;
-        float v[8];
-        if ((unsigned)(X + sx) < (unsigned)Lct.n[0] && (unsigned)(Y + sy) < (unsigned)Lct.n[1] &&
-            (unsigned)(Z + sz) < (unsigned)Lct.n[2]) {
-            const float *eb = e + (int64_t)block * Lct.bstride + X + (int64_t)Lct.n[0] * (Y + (int64_t)Lct.n[1] * Z);
-            const int64_t ox = sx, oy = (int64_t)sy * Lct.n[0], oz = (int64_t)sz * Lct.n[0] * Lct.n[1];
-            v[0] = __ldg(eb);
-            v[1] = __ldg(eb + ox);
-            v[2] = __ldg(eb + oy);
-            v[3] = __ldg(eb + ox + oy);
-            v[4] = __ldg(eb + oz);
-            v[5] = __ldg(eb + ox + oz);
-            v[6] = __ldg(eb + oy + oz);
-            v[7] = __ldg(eb + ox + oy + oz);
-        } else {
-            v[0] = fetch<float>(e, Lct, cbc, block, X, Y, Z);
-            v[1] = fetch<float>(e, Lct, cbc, block, X + sx, Y, Z);
-            v[2] = fetch<float>(e, Lct, cbc, block, X, Y + sy, Z);
-            v[3] = fetch<float>(e, Lct, cbc, block, X + sx, Y + sy, Z);
-            v[4] = fetch<float>(e, Lct, cbc, block, X, Y, Z + sz);
-            v[5] = fetch<float>(e, Lct, cbc, block, X + sx, Y, Z + sz);
-            v[6] = fetch<float>(e, Lct, cbc, block, X, Y + sy, Z + sz);
-            v[7] = fetch<float>(e, Lct, cbc, block, X + sx, Y + sy, Z + sz);
-        }
-        const float a0 = 0.75f * v[0] + 0.25f * v[1];
-        const float a1 = 0.75f * v[2] + 0.25f * v[3];
-        const float a2 = 0.75f * v[4] + 0.25f * v[5];
-        const float a3 = 0.75f * v[6] + 0.25f * v[7];
+        const int u = (X + 1) + qc.ex * ((Y + 1) + qc.ey * (Z + 1));
+        const int ox = sx, oy = sy * qc.ex, oz = sz * qc.ex * qc.ey;
+        const float v0 = se[u], v1 = se[u + ox], v2 = se[u + oy], v3 = se[u + ox + oy];
+        const float v4 = se[u + oz], v5 = se[u + ox + oz], v6 = se[u + oy + oz], v7 = se[u + ox + oy + oz];
+        const float a0 = 0.75f * v0 + 0.25f * v1;
+        const float a1 = 0.75f * v2 + 0.25f * v3;
+        const float a2 = 0.75f * v4 + 0.25f * v5;
+        const float a3 = 0.75f * v6 + 0.25f * v7;
         const float b0 = 0.75f * a0 + 0.25f * a1;
         const float b1 = 0.75f * a2 + 0.25f * a3;
         const float val = 0.75f * b0 + 0.25f * b1;
-        const int64_t o = (int64_t)block * L.bstride + x + (int64_t)L.n[0] * (y + (int64_t)L.n[1] * z);
+        const int64_t o = (int64_t)qf.block * L.bstride + (qf.x0 + x) + (int64_t)L.n[0] * ((qf.y0 + y) + (int64_t)L.n[1] * (qf.z0 + z));
         p[o] = p[o] + val;
     }
 }
 
 // FP64 residual of the outer iteration: r = f - L p64 (p64 += e first if e),
 // r32 = (float) r, per-CTA FP64 partial sums of r^2 (and f^2).
-__global__ void __launch_bounds__(256) resid64_kernel(const __grid_constant__ KArgs a, const double *p64,
-                                                      const float *f,
-                                                      float *r32, double *partials)
+__global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_constant__ KArgs a,
+                                                               const __grid_constant__ Tile T, const double *p64,
+                                                               const float *f, float *r32, double *partials)
 {
-    __shared__ double sh[2][8];
-    const LabGeom &L = a.G.L;
-    const int64_t total = (int64_t)a.G.nblocks * L.n[0] * L.n[1] * L.n[2];
+    __shared__ double sp[kRegionMax];
+    __shared__ float sk[kRegionMax];
+    __shared__ double sh[2][kTileThreads / 32];
+    __shared__ int snb[27];
+    const LabGeom &L = a.G.L, &Lk = a.G.Lk;
+    const TilePos q = tile_pos(T);
+    neighbour_blocks(L.nb, q.block, snb);
+    __syncthreads();
+    stage_region<double>(p64, L, a.G.bc, q, false, snb, sp);
+    stage_region<float>(a.k, Lk, a.kbc, q, false, snb, sk);
+    cp_async_wait_all();
+    __syncthreads();
     double rr = 0, ff = 0;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        int block, x, y, z;
-        cell_of(t, L, block, x, y, z);
-        const LabGeom &Lk = a.G.Lk;
-        const int64_t o = (int64_t)block * Lk.bstride + x + (int64_t)Lk.n[0] * (y + (int64_t)Lk.n[1] * z);
-        double Lp, D, pc;
-        op7<double>(p64, a.k, a.G, a.kbc, block, x, y, z, a.ih2d, Lp, D, pc);
+    const int cells = T.t[0] * T.t[1] * T.t[2];
+    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
+        int x, y, z;
+        tile_cell(T, c, x, y, z);
+        const int64_t o = (int64_t)q.block * Lk.bstride + (q.x0 + x) + (int64_t)Lk.n[0] * ((q.y0 + y) + (int64_t)Lk.n[1] * (q.z0 + z));
+        double v[14], Lp, D, pc;
+        region7<double>(sp, sk, q, x, y, z, v);
+        op7_math<double>(v, a.ih2d, Lp, D, pc);
         const double fc = (double)__ldg(f + o);
         const double r = fc - Lp;
         if (r32) r32[o] = (float)r;
@@ -287,7 +294,7 @@ __global__ void __launch_bounds__(256) resid64_kernel(const __grid_constant__ KA
     __syncthreads();
     if (threadIdx.x == 0) {
         double s0 = 0, s1 = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+        for (int i = 0; i < kTileThreads / 32; ++i) {
             s0 += sh[0][i];
             s1 += sh[1][i];
         }
@@ -481,6 +488,8 @@ KArgs kargs(cn_mg *m, int l)
     a.G.nblocks = m->p[l]->nblocks;
     a.kbc = bc_view(m->k[l], 0);
     a.k = reinterpret_cast<const float *>(m->k[l]->d_data);
+    a.coef = (int)m->coef.size() > l && m->coef[l] ? reinterpret_cast<const float *>(m->coef[l]->d_data) : nullptr;
+    a.ccs = (int)m->coef.size() > l && m->coef[l] ? m->coef[l]->comp_stride : 0;
     a.ih2d = 1.0 / (m->p[l]->h[0] * m->p[l]->h[0]);
     a.ih2 = (float)a.ih2d;
     return a;
@@ -499,13 +508,13 @@ float *fptr(cn_grid *g) { return reinterpret_cast<float *>(g->d_data); }
 static cn_status smooth(cn_mg *m, int l, int sweeps, bool zero_guess, cudaStream_t st)
 {
     KArgs a = kargs(m, l);
-    const int64_t cells = (int64_t)m->p[l]->nblocks * m->p[l]->n[0] * m->p[l]->n[1] * m->p[l]->n[2];
+    const Tile T = tile_of(m->p[l]->n);
     for (int s = 0; s < sweeps; ++s) {
         const bool zg = zero_guess && s == 0;
         // ping-pong so that the result of the last sweep lands in p
         float *src = fptr(m->p[l]), *dst = fptr(m->pt[l]);
-        jacobi_kernel<<<grid_for(cells), 256, 0, st>>>(a, zg ? nullptr : src, fptr(m->f[l]), dst,
-                                                        (float)m->omega);
+        jacobi_kernel<<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads, 0, st>>>(
+            a, T, zg ? nullptr : src, fptr(m->f[l]), dst, (float)m->omega);
         CN_CUDA_TRY(cudaGetLastError());
         std::swap(m->p[l], m->pt[l]);
     }
@@ -542,17 +551,16 @@ cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
     if (s != CN_OK) return s;
     KArgs a = kargs(m, l);
     const LabGeom Lc = make_geom(m->p[l + 1], &kS1);
-    const int64_t ccells = (int64_t)m->p[l + 1]->nblocks * Lc.n[0] * Lc.n[1] * Lc.n[2];
-    resid_restrict_kernel<<<grid_for(ccells), 256, 0, st>>>(a, fptr(m->p[l]), fptr(m->f[l]), Lc,
-                                                             fptr(m->f[l + 1]));
+    const Tile T = tile_of(m->p[l]->n);
+    resid_restrict_kernel<<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads, 0, st>>>(
+        a, T, fptr(m->p[l]), fptr(m->f[l]), Lc, fptr(m->f[l + 1]));
     CN_CUDA_TRY(cudaGetLastError());
     s = vcycle(m, l + 1, st);
     if (s != CN_OK) return s;
     const LabGeom Lf = make_geom(m->p[l], &kS1);
     const LabGeom Lct = make_geom(m->p[l + 1], &kS1t);
-    const int64_t fcells = (int64_t)m->p[l]->nblocks * Lf.n[0] * Lf.n[1] * Lf.n[2];
-    prolong_kernel<<<grid_for(fcells), 256, 0, st>>>(Lf, fptr(m->p[l]), Lct, bc_view(m->p[l + 1], 0),
-                                                      fptr(m->p[l + 1]), m->p[l]->nblocks);
+    prolong_kernel<<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads, 0, st>>>(
+        Lf, T, fptr(m->p[l]), Lct, bc_view(m->p[l + 1], 0), fptr(m->p[l + 1]));
     CN_CUDA_TRY(cudaGetLastError());
     if (l == 0 && m->capture) {
         s = m->capture(m, st);
@@ -612,8 +620,7 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
         for (int d = 0; d < 3; ++d) cells[d] /= 2;
     }
     if (s == CN_OK) s = cn_grid_create(k->nb, k->n, 1, CN_FLOAT32, b0, e0, &m->r32);
-    const int64_t fine = (int64_t)k->nblocks * k->n[0] * k->n[1] * k->n[2];
-    m->nparts = (int)grid_for(fine);
+    m->nparts = k->nblocks * tile_of(k->n).count;
     if (s == CN_OK && cudaMalloc(&m->partials, sizeof(double) * 2 * m->nparts) != cudaSuccess)
         s = fail(CN_ERR_OUT_OF_MEMORY, "cn_mg_create: partials");
     if (s == CN_OK && cudaMalloc(&m->sums, sizeof(double) * 2) != cudaSuccess)
@@ -632,6 +639,21 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
     }
     if (s == CN_OK) s = sync_bc(m->p[0], nullptr);
     if (s == CN_OK) s = sync_bc(k, nullptr);
+    // operator coefficients of every level (k is fixed from here on)
+    for (int l = 0; l < levels && s == CN_OK; ++l) {
+        cn_grid *c = nullptr;
+        s = cn_grid_create(k->nb, m->p[l]->n, 7, CN_FLOAT32, b0, e0, &c);
+        m->coef.push_back(c);
+        if (s != CN_OK) break;
+        if (c->block_stride != m->p[l]->block_stride) {
+            s = fail(CN_ERR_UNSUPPORTED, "cn_mg_create: coefficient layout");
+            break;
+        }
+        const KArgs a = kargs(m, l);
+        const Tile T = tile_of(m->p[l]->n);
+        coef_kernel<<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads>>>(a, T, fptr(c));
+        if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
+    }
     if (s == CN_OK && cudaDeviceSynchronize() != cudaSuccess) s = fail(CN_ERR_CUDA, "cn_mg_create");
     if (s != CN_OK) {
         extern cn_status cn_mg_destroy(cn_mg *);
@@ -652,6 +674,7 @@ cn_status cn_mg_destroy(cn_mg *m)
         if (l > 0) cn_grid_destroy(m->k[l]);
     }
     cn_grid_destroy(m->r32);
+    for (cn_grid *g : m->coef) cn_grid_destroy(g);
     for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
     for (void *a : m->nn_act)
         if (a) cudaFree(a);
@@ -706,9 +729,9 @@ cn_status cn_mg_residual(cn_mg *m, const cn_grid *p64, const cn_grid *f, cn_grid
     KArgs a = kargs(m, 0);
     a.G.L.bstride = p64->block_stride;
     a.G.bc = bc_view(p64, 0);
-    resid64_kernel<<<m->nparts, 256, 0, st>>>(a, reinterpret_cast<const double *>(p64->d_data),
-                                               reinterpret_cast<const float *>(f->d_data),
-                                               r32 ? fptr(r32) : nullptr, m->partials);
+    resid64_kernel<<<m->nparts, kTileThreads, 0, st>>>(a, tile_of(p64->n), reinterpret_cast<const double *>(p64->d_data),
+                                                        reinterpret_cast<const float *>(f->d_data),
+                                                        r32 ? fptr(r32) : nullptr, m->partials);
     CN_CUDA_TRY(cudaGetLastError());
     sum_pairs_kernel<<<1, 256, 0, st>>>(m->partials, m->nparts, m->sums);
     CN_CUDA_TRY(cudaGetLastError());
@@ -770,9 +793,9 @@ cn_status cn_mg_jacobi(cn_mg *m, const cn_grid *pin, const cn_grid *f, cn_grid *
 {
     if (!m || !pin || !f || !pout) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
     KArgs a = kargs(m, 0);
-    const int64_t cells = (int64_t)pin->nblocks * pin->n[0] * pin->n[1] * pin->n[2];
-    jacobi_kernel<<<grid_for(cells), 256, 0, as_stream(stream)>>>(
-        a, reinterpret_cast<const float *>(pin->d_data), reinterpret_cast<const float *>(f->d_data),
+    const Tile T = tile_of(pin->n);
+    jacobi_kernel<<<(unsigned)(pin->nblocks * T.count), kTileThreads, 0, as_stream(stream)>>>(
+        a, T, reinterpret_cast<const float *>(pin->d_data), reinterpret_cast<const float *>(f->d_data),
         fptr(pout), (float)m->omega);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
@@ -783,9 +806,9 @@ cn_status cn_mg_restrict_residual(cn_mg *m, const cn_grid *p, const cn_grid *f, 
     if (!m || !p || !f || !fc || m->nlevels < 2) return fail(CN_ERR_INVALID_ARGUMENT, "bad argument");
     KArgs a = kargs(m, 0);
     const LabGeom Lc = make_geom(fc, &kS1);
-    const int64_t cc = (int64_t)fc->nblocks * Lc.n[0] * Lc.n[1] * Lc.n[2];
-    resid_restrict_kernel<<<grid_for(cc), 256, 0, as_stream(stream)>>>(
-        a, reinterpret_cast<const float *>(p->d_data), reinterpret_cast<const float *>(f->d_data), Lc, fptr(fc));
+    const Tile T = tile_of(p->n);
+    resid_restrict_kernel<<<(unsigned)(p->nblocks * T.count), kTileThreads, 0, as_stream(stream)>>>(
+        a, T, reinterpret_cast<const float *>(p->d_data), reinterpret_cast<const float *>(f->d_data), Lc, fptr(fc));
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
@@ -796,10 +819,9 @@ cn_status cn_mg_prolong(cn_mg *m, const cn_grid *ec, cn_grid *p, void *stream)
     cn_status s = sync_bc(const_cast<cn_grid *>(ec), as_stream(stream));
     if (s != CN_OK) return s;
     const LabGeom Lf = make_geom(p, &kS1), Lct = make_geom(ec, &kS1t);
-    const int64_t fc = (int64_t)p->nblocks * Lf.n[0] * Lf.n[1] * Lf.n[2];
-    prolong_kernel<<<grid_for(fc), 256, 0, as_stream(stream)>>>(Lf, fptr(p), Lct, bc_view(ec, 0),
-                                                                 reinterpret_cast<const float *>(ec->d_data),
-                                                                 p->nblocks);
+    const Tile T = tile_of(p->n);
+    prolong_kernel<<<(unsigned)(p->nblocks * T.count), kTileThreads, 0, as_stream(stream)>>>(
+        Lf, T, fptr(p), Lct, bc_view(ec, 0), reinterpret_cast<const float *>(ec->d_data));
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }

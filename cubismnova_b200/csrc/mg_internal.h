@@ -12,6 +12,7 @@ struct cn_mg {
     int nu1, nu2;
     double omega;
     std::vector<cn_grid *> p, pt, f, k; // per level (FP32); k[0] is the caller's grid
+    std::vector<cn_grid *> coef;        // per level (FP32, 7 comps): k+ faces x,y,z, k- faces x,y,z, D
     cn_grid *r32 = nullptr;             // finest FP32 residual
     double *partials = nullptr;
     double *sums = nullptr;

@@ -1,0 +1,217 @@
+// mg_tile.cuh -- tiles of a block for the level operators of the multigrid
+// solver and the learned smoother's features: tile geometry, asynchronous
+// staging of a tile plus its one-cell halo into shared memory, and the
+// variable-coefficient 7-point operator evaluated from the staged region.
+#pragma once
+
+#include "cn_internal.h"
+#include "cn_tma.cuh"
+
+namespace cn {
+namespace mg {
+
+template <typename T> __device__ __forceinline__ T harm(T a, T b)
+{
+    const T t = a * b;
+    return (t + t) / (a + b);
+}
+
+// L p and the diagonal D at one cell from its 13 values; TP is the solution
+// type (float in the V-cycle, double in the outer residual), k is FP32.
+template <typename TP>
+__device__ __forceinline__ void op7_math(const TP (&v)[14], TP ih2, TP &Lp, TP &D, TP &pc)
+{
+    pc = v[0];
+    const TP kc = v[1];
+    TP f[3], s[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const TP pp = v[2 + 4 * d], pm = v[3 + 4 * d];
+        const TP kp = harm<TP>(kc, v[4 + 4 * d]);
+        const TP km = harm<TP>(v[5 + 4 * d], kc);
+        f[d] = kp * (pp - pc) - km * (pc - pm);
+        s[d] = kp + km;
+    }
+    Lp = ih2 * ((f[0] + f[1]) + f[2]);
+    D = ih2 * ((s[0] + s[1]) + s[2]);
+}
+
+// Operator coefficients of a level, precomputed once from k (they depend on
+// k only): per cell the harmonic face means kp_d = harm(k, k(+e_d)) and
+// km_d = harm(k(-e_d), k) (neighbours through the lab) and the diagonal
+// D = ih2 ((s0 + s1) + s2), s_d = kp_d + km_d: components 0-2 kp, 3-5 km,
+// 6 D of an FP32 grid laid out like p.  Evaluated with the same operations
+// as op7_math, so L p and D come out bit for bit the same.
+template <typename TP>
+__device__ __forceinline__ void op7_coef(const TP *sp, int u, const int (&st)[3], const float *coef, int64_t ccs,
+                                         int64_t o, TP ih2, TP &Lp, TP &D, TP &pc)
+{
+    pc = sp[u];
+    TP f[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const TP kp = (TP)__ldg(coef + d * ccs + o), km = (TP)__ldg(coef + (3 + d) * ccs + o);
+        f[d] = kp * (sp[u + st[d]] - pc) - km * (pc - sp[u - st[d]]);
+    }
+    Lp = ih2 * ((f[0] + f[1]) + f[2]);
+    D = (TP)__ldg(coef + 6 * ccs + o);
+}
+
+// ---------------------------------------------------------------- tiles
+// The level operators work on tiles of one block: up to 32 x 8 x 4 cells
+// (extents: the largest divisors of the block's cells within those caps,
+// even when the block's extent is even, so fine tiles hold whole coarse
+// cells).  A CTA stages its tile plus a one-cell halo of p and k into shared
+// memory (halo cells outside the block through cn::lab_fetch: periodic
+// neighbour or the BC chain), then every thread evaluates its cells from
+// shared memory with the same operation order as the per-cell form.
+struct Tile {
+    int t[3];      // tile extent (cells)
+    int per[3];    // tiles per block along x, y, z
+    int count;     // tiles per block
+    int sh[2];     // log2 of t[0], t[1] when powers of two, else -1
+};
+
+constexpr int kTileCap[3] = {32, 8, 4};
+constexpr int kRegionMax = (32 + 2) * (8 + 2) * (4 + 2); // 2040
+constexpr int kTileThreads = 256;
+constexpr int kTileMinCtas = 4; // resident CTAs per SM the tile kernels are compiled for (<= 64 registers)
+
+inline int tile_extent(int n, int cap)
+{
+    for (int t = n < cap ? n : cap; t >= 1; --t)
+        if (n % t == 0 && (n % 2 != 0 || t % 2 == 0 || t == 1))
+            return t;
+    return 1;
+}
+
+inline Tile tile_of(const int n[3])
+{
+    Tile T;
+    T.count = 1;
+    for (int d = 0; d < 3; ++d) {
+        T.t[d] = tile_extent(n[d], kTileCap[d]);
+        T.per[d] = n[d] / T.t[d];
+        T.count *= T.per[d];
+    }
+    for (int d = 0; d < 2; ++d) {
+        T.sh[d] = -1;
+        for (int b = 0; b < 31; ++b)
+            if (T.t[d] == (1 << b)) T.sh[d] = b;
+    }
+    return T;
+}
+
+// tile-local cell c -> (x, y, z)
+__device__ __forceinline__ void tile_cell(const Tile &T, int c, int &x, int &y, int &z)
+{
+    if (T.sh[0] >= 0 && T.sh[1] >= 0) {
+        x = c & (T.t[0] - 1);
+        y = (c >> T.sh[0]) & (T.t[1] - 1);
+        z = c >> (T.sh[0] + T.sh[1]);
+    } else {
+        x = c % T.t[0];
+        y = (c / T.t[0]) % T.t[1];
+        z = c / (T.t[0] * T.t[1]);
+    }
+}
+
+struct TilePos {
+    int block, x0, y0, z0;
+    int ex, ey, ez; // staged region extents (tile + 2)
+};
+
+__device__ __forceinline__ TilePos tile_pos(const Tile &T)
+{
+    TilePos q;
+    q.block = blockIdx.x / T.count;
+    int r = blockIdx.x - q.block * T.count;
+    q.x0 = (r % T.per[0]) * T.t[0];
+    r /= T.per[0];
+    q.y0 = (r % T.per[1]) * T.t[1];
+    q.z0 = (r / T.per[1]) * T.t[2];
+    q.ex = T.t[0] + 2;
+    q.ey = T.t[1] + 2;
+    q.ez = T.t[2] + 2;
+    return q;
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The 27 periodic neighbour blocks of block b (itself included), index
+// (r0+1) + 3 (r1+1) + 9 (r2+1) for the offsets r in {-1, 0, 1}^3, written to
+// shared memory by the first 27 threads; a barrier must follow.
+__device__ __forceinline__ void neighbour_blocks(const int nb[3], int b, int *snb)
+{
+    if (threadIdx.x < 27) {
+        const int t = threadIdx.x;
+        int bx = b % nb[0] + t % 3 - 1, by = (b / nb[0]) % nb[1] + (t / 3) % 3 - 1, bz = b / (nb[0] * nb[1]) + t / 9 - 1;
+        bx = bx < 0 ? bx + nb[0] : (bx >= nb[0] ? bx - nb[0] : bx);
+        by = by < 0 ? by + nb[1] : (by >= nb[1] ? by - nb[1] : by);
+        bz = bz < 0 ? bz + nb[2] : (bz >= nb[2] ? bz - nb[2] : bz);
+        snb[t] = bx + nb[0] * (by + nb[1] * bz);
+    }
+}
+
+// Stage one field over the region, one warp per region row.  Cells inside
+// the block, and outside it in blocks without BCs or skip flags (the
+// periodic neighbour, from the table snb of neighbour_blocks), are
+// asynchronous 4- or 8-byte copies, many in flight per thread; cells of
+// blocks with BCs resolve through the lab (cn::lab_fetch_slow).  Edge and
+// corner cells of the region are zero unless tensorial (the 7-point operator
+// does not read them).  The caller waits with cp_async_wait_all() and a
+// barrier.
+template <typename T>
+__device__ __forceinline__ void stage_region(const T *comp, const LabGeom &L, const BcView &bc, const TilePos &q,
+                                             bool tensorial, const int *snb, T *s)
+{
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte cells");
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rows = q.ey * q.ez;
+    const bool plain = __ldg(bc.mode + q.block) == 0;
+    for (int r = warp; r < rows; r += kTileThreads / 32) {
+        const int j = r % q.ey, k = r / q.ey;
+        const int y = q.y0 + j - 1, z = q.z0 + k - 1;
+        const int r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0), r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+        const int yl = y - r1 * L.n[1], zl = z - r2 * L.n[2];
+        for (int i = lane; i < q.ex; i += 32) {
+            const int x = q.x0 + i - 1;
+            const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0);
+            const int outside = (r0 != 0) + (r1 != 0) + (r2 != 0);
+            T *dst = s + i + q.ex * r;
+            if (!tensorial && outside > 1) {
+                *dst = T(0);
+            } else if (outside == 0 || plain) {
+                const int sb = outside == 0 ? q.block : snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+                const T *src = comp + (int64_t)sb * L.bstride + (x - r0 * L.n[0]) +
+                               (int64_t)L.n[0] * (yl + (int64_t)L.n[1] * zl);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+                             "n"((int)sizeof(T))
+                             : "memory");
+            } else {
+                *dst = lab_fetch_slow<T>(comp, L, bc, q.block, x, y, z);
+            }
+        }
+    }
+}
+
+// the 13 operator values of tile cell (x, y, z) from the staged region
+template <typename TP>
+__device__ __forceinline__ void region7(const TP *sp, const float *sk, const TilePos &q, int x, int y, int z,
+                                        TP (&v)[14])
+{
+    const int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1));
+    const int st[3] = {1, q.ex, q.ex * q.ey};
+    v[0] = sp[u];
+    v[1] = (TP)sk[u];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        v[2 + 4 * d] = sp[u + st[d]];
+        v[3 + 4 * d] = sp[u - st[d]];
+        v[4 + 4 * d] = (TP)sk[u + st[d]];
+        v[5 + 4 * d] = (TP)sk[u - st[d]];
+    }
+}
+
+} // namespace mg
+} // namespace cn
