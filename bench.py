@@ -245,7 +245,9 @@ class C1:
                     seconds_per_sweep=t)
 
     def cpu_sample(self, threads):
-        return self.cpu_sample_static(threads)
+        """About 10 s of host work: the full sweep, repeated."""
+        t1 = self.cpu_sample_static(threads, reps=1)["seconds_per_sweep"]
+        return self.cpu_sample_static(threads, reps=int(min(2000, max(1, 10.0 / t1))))
 
 
 # FP64/FP32 operations per cell and RK stage of the Euler kernel, each face
@@ -356,12 +358,13 @@ class Euler:
         return 5 * nbytes, 5 * nbytes
 
     @classmethod
-    def cpu_sample_static(cls, threads, reps=2):
+    def cpu_sample_static(cls, threads, reps=2, nb=None):
         """One SSP-RK3 stage (stage 2: lab + WENO + Rusanov + update reading U^n)
-        over a 4^3-block sample grid of the same block size and BC pattern, on
-        the reference FieldLab (oracle/_ref) or, without it, the C oracle."""
+        over a sample grid of the same block size and BC pattern (default 4^3
+        blocks), best of `reps`, on the reference FieldLab (oracle/_ref) or,
+        without it, the C oracle."""
         import oracle as O
-        nb, n = cls.sample_nb, cls.n
+        nb, n = tuple(nb or cls.sample_nb), cls.n
         stride = O.block_stride(n, np.float64)
         U = euler_host_state(nb, n, stride)
         bcl = euler_bclists_host(nb)
@@ -385,7 +388,10 @@ class Euler:
                     seconds_per_sweep=t)
 
     def cpu_sample(self, threads):
-        return self.cpu_sample_static(threads)
+        """About 10 s of host work: the stage on 8x8x4 blocks, repeated."""
+        nb = (8, 8, 4)
+        t1 = self.cpu_sample_static(threads, reps=1, nb=nb)["seconds_per_sweep"]
+        return self.cpu_sample_static(threads, reps=int(min(100, max(1, 10.0 / t1))), nb=nb)
 
 
 class C2(Euler):
@@ -551,6 +557,7 @@ class C5:
     dtype = "f32"
     metric = unit = "Gcell/s solved to 1e-8"
     launches_per_step = 1  # the events bracket the whole solve
+    with_learned = True
     roofline_scope = ("whole solve (all kernels and the per-cycle host check of the residual norm) against "
                       "its compulsory HBM bytes")
     rtol = 1e-8
@@ -582,7 +589,7 @@ class C5:
         ncl = [self.cells // 8 ** l for l in range(L)]
         per_cycle = 81 * sum(ncl[:-1]) + 12 * ncl[-1] + 40 * ncl[0]
         self.bytes_per_cell_step = (28 * self.cells + self.cycles * per_cycle) / self.cells
-        self.learned = self._learned()
+        self.learned = self._learned() if self.with_learned else None
         self.desc = self.desc + f"; {L} levels, {self.cycles} cycles (relres {self.relres:.2e})"
         self.h_f = self.h_p = None
 
@@ -670,6 +677,8 @@ def run_ours(args, world, rank, local, pg):
     from cubismnova_b200 import _lib
     torch.cuda.set_device(local)
     cls = WORKLOADS[args.workload]
+    if getattr(args, "no_learned", False) and hasattr(cls, "with_learned"):
+        cls = type(cls.__name__, (cls,), {"with_learned": False})
     if args.blocks:
         cls = type(cls.__name__, (cls,), {"nb": tuple(args.blocks),
                                           "desc": cls.desc + f" [reduced: {tuple(args.blocks)} blocks]"})
@@ -793,6 +802,8 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel, if measured")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="c5: skip training and timing the learned smoother")
     ap.add_argument("--blocks", type=int, nargs=3, default=None,
                     help="override the block counts (reduced grids for profiling runs)")
     args = ap.parse_args()

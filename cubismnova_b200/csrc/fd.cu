@@ -72,24 +72,43 @@ __device__ __forceinline__ Tile<T> carve(T *base, int N0, int N1, int TZ)
 }
 
 // Gathers the faces selected by mask (bit 0: x, 1: y, 2: z) of the tile that
-// starts at z0.  Undefined lab cells (never read by these stencils unless the
-// BC set-up leaves a face undefined) are set to zero.
+// starts at z0.  Blocks without BCs or skip flags (lab mode byte 0) read the
+// periodic neighbour blocks from the table snb (index (r0+1) + 3 (r1+1) +
+// 9 (r2+1)) with plain loads; the others resolve every face cell with
+// cn::lab_value.  Undefined lab cells (never read by these stencils unless
+// the BC set-up leaves a face undefined) are set to zero.
+template <typename T>
+__device__ __forceinline__ T face_value(const T *comp, const LabGeom &L, const BcView &bc, bool plain,
+                                        const int *snb, int block, int bx, int by, int bz, int x, int y, int z)
+{
+    if (plain) {
+        const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0), r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0),
+                  r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+        const int sb = snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+        return __ldg(comp + (int64_t)sb * L.bstride + (x - r0 * L.n[0]) +
+                     (int64_t)L.n[0] * ((y - r1 * L.n[1]) + (int64_t)L.n[1] * (z - r2 * L.n[2])));
+    }
+    T v;
+    if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, z, true, v))
+        v = T(0);
+    return v;
+}
+
 template <typename T>
 __device__ __forceinline__ void gather_faces(const T *comp, const LabGeom &L, const BcView &bc,
                                              int block, int bx, int by, int bz, int z0, int TZ,
-                                             const Tile<T> &t, unsigned mask)
+                                             const Tile<T> &t, unsigned mask, const int *snb)
 {
     const int N0 = L.n[0], N1 = L.n[1];
     const int nth = blockDim.x;
+    const bool plain = __ldg(bc.mode + block) == 0;
     if (mask & 1u) {
         const int m = N1 * TZ;
         for (int i = threadIdx.x; i < 2 * m; i += nth) {
             const int side = i / m, r = i - side * m;
             const int y = r % N1, z = r / N1;
-            T v;
-            if (!lab_value<T>(comp, L, bc, block, bx, by, bz, side ? N0 : -1, y, z0 + z, true, v))
-                v = T(0);
-            (side ? t.xhi : t.xlo)[r] = v;
+            (side ? t.xhi : t.xlo)[r] =
+                face_value<T>(comp, L, bc, plain, snb, block, bx, by, bz, side ? N0 : -1, y, z0 + z);
         }
     }
     if (mask & 2u) {
@@ -97,10 +116,8 @@ __device__ __forceinline__ void gather_faces(const T *comp, const LabGeom &L, co
         for (int i = threadIdx.x; i < 2 * m; i += nth) {
             const int side = i / m, r = i - side * m;
             const int x = r % N0, z = r / N0;
-            T v;
-            if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, side ? N1 : -1, z0 + z, true, v))
-                v = T(0);
-            (side ? t.yhi : t.ylo)[r] = v;
+            (side ? t.yhi : t.ylo)[r] =
+                face_value<T>(comp, L, bc, plain, snb, block, bx, by, bz, x, side ? N1 : -1, z0 + z);
         }
     }
     if (mask & 4u) {
@@ -108,10 +125,12 @@ __device__ __forceinline__ void gather_faces(const T *comp, const LabGeom &L, co
         for (int i = threadIdx.x; i < 2 * m; i += nth) {
             const int side = i / m, r = i - side * m;
             const int x = r % N0, y = r / N0;
-            T v;
-            if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, side ? z0 + TZ : z0 - 1, true, v))
-                v = T(0);
-            (side ? t.zhi : t.zlo)[r] = v;
+            const int z = side ? z0 + TZ : z0 - 1;
+            // z faces inside the block (interior tiles) are plain loads
+            (side ? t.zhi : t.zlo)[r] =
+                (unsigned)z < (unsigned)L.n[2]
+                    ? __ldg(comp + (int64_t)block * L.bstride + x + (int64_t)N0 * (y + (int64_t)N1 * z))
+                    : face_value<T>(comp, L, bc, plain, snb, block, bx, by, bz, x, y, z);
         }
     }
 }
@@ -131,6 +150,15 @@ __global__ void __launch_bounds__(256) fd_kernel(FdParams<T> p)
     const int bx = block % L.nb[0];
     const int by = (block / L.nb[0]) % L.nb[1];
     const int bz = block / (L.nb[0] * L.nb[1]);
+    __shared__ int snb[27]; // periodic neighbour blocks
+    if (threadIdx.x < 27) {
+        const int t = threadIdx.x;
+        int nx = bx + t % 3 - 1, ny = by + (t / 3) % 3 - 1, nz = bz + t / 9 - 1;
+        nx = nx < 0 ? nx + L.nb[0] : (nx >= L.nb[0] ? nx - L.nb[0] : nx);
+        ny = ny < 0 ? ny + L.nb[1] : (ny >= L.nb[1] ? ny - L.nb[1] : ny);
+        nz = nz < 0 ? nz + L.nb[2] : (nz >= L.nb[2] ? nz - L.nb[2] : nz);
+        snb[t] = nx + L.nb[0] * (ny + L.nb[1] * nz);
+    }
     constexpr int NC = (OP == kDiv) ? 3 : 1;
     const size_t te = tile_elems<T>(N0, N1, TZ);
     Tile<T> tl[NC];
@@ -158,11 +186,12 @@ __global__ void __launch_bounds__(256) fd_kernel(FdParams<T> p)
         for (int c = 0; c < NC; ++c)
             for (int i = threadIdx.x; i < m; i += blockDim.x)
                 tl[c].in[i] = p.in[c][in_off + i];
+        __syncthreads(); // snb
     }
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const unsigned mask = (OP == kDiv) ? (1u << c) : 7u;
-        gather_faces<T>(p.in[c], L, p.bc[c], block, bx, by, bz, z0, TZ, tl[c], mask);
+        gather_faces<T>(p.in[c], L, p.bc[c], block, bx, by, bz, z0, TZ, tl[c], mask, snb);
     }
     if (p.use_bulk) {
         if (!mbar_wait_bounded(bar, 0)) {
@@ -221,12 +250,16 @@ static size_t fd_smem_bytes(int N0, int N1, int TZ, size_t es, int nc)
     return 128 + te * es * nc;
 }
 
-// Largest z-slab height (a divisor of N2) whose tile fits the budget.
+// z-slab height: the largest divisor of N2 whose tile fits the budget and
+// holds at most 2048 cells (more, smaller CTAs balance the SMs and overlap
+// the staging of one tile with the stencil of another); at least 1.
 static int pick_tz(int N0, int N1, int N2, size_t es, int nc, size_t budget)
 {
     for (int tz = N2; tz >= 1; --tz) {
         if (N2 % tz) continue;
-        if (fd_smem_bytes(N0, N1, tz, es, nc) <= budget) return tz;
+        if (fd_smem_bytes(N0, N1, tz, es, nc) > budget) continue;
+        if (tz > 1 && (size_t)N0 * N1 * tz > 2048) continue;
+        return tz;
     }
     return 0;
 }
