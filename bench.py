@@ -506,7 +506,9 @@ class C3:
                     seconds_per_sweep=best)
 
     def cpu_sample(self, threads):
-        return self.cpu_sample_static(threads)
+        """About 10 s of host work: the stage repeated."""
+        t1 = self.cpu_sample_static(threads, reps=1)["seconds_per_sweep"]
+        return self.cpu_sample_static(threads, reps=int(min(500, max(1, 10.0 / t1))))
 
 
 def poisson_host(nb, n, seed=1234, sigma=0.5, count=32):

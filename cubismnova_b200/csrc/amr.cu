@@ -31,8 +31,10 @@ struct Src {
         t.ih[0] = t.ih[1] = t.ih[2] = (T)B.ih;
         t.bx = t.by = t.bz = 0;
     }
+    template <typename T> __device__ __forceinline__ void prepare(const euler::TileInfo<T> &, int *) const {}
     template <typename T>
-    __device__ __forceinline__ T halo(const T *comp, int, const euler::TileInfo<T> &t, int gx, int gy, int gz) const
+    __device__ __forceinline__ T halo(const T *comp, int, const euler::TileInfo<T> &t, int gx, int gy, int gz,
+                                      const int *) const
     {
         return value<T>(comp, A, t.block, gx, gy, gz);
     }
@@ -45,9 +47,10 @@ __global__ void __launch_bounds__(euler::NT, 3) stage_kernel(euler::StageParams<
     T *W = reinterpret_cast<T *>(smem_raw);
     T *F = W + 5 * euler::Stg<T>::SV;
     __shared__ double red[euler::NT / 32][5];
+    __shared__ int snb[28];
     // persistent: each CTA walks the work list with a grid stride
     for (int item = blockIdx.x; item < nitems; item += gridDim.x)
-        euler::stage_tile<T>(p, src, item, item, W, F, red);
+        euler::stage_tile<T>(p, src, item, item, W, F, red, snb);
 }
 
 // dense lab of one block: (n+2g)^3, face ghosts only (non-tensorial)

@@ -77,9 +77,43 @@ struct CartSrc {
         t.by = (t.block / L.nb[0]) % L.nb[1];
         t.bz = t.block / (L.nb[0] * L.nb[1]);
     }
+    // Per tile, in shared memory (a barrier must follow): snb[0..26] the 27
+    // periodic neighbour blocks of the tile's block (index (r0+1) + 3 (r1+1) +
+    // 9 (r2+1)), snb[27] the mask of the components whose block carries
+    // neither BCs nor skip flags (lab mode byte 0).
     template <typename T>
-    __device__ __forceinline__ T halo(const T *comp, int c, const TileInfo<T> &t, int gx, int gy, int gz) const
+    __device__ __forceinline__ void prepare(const TileInfo<T> &t, int *snb) const
     {
+        if (threadIdx.x < 27) {
+            const int q = threadIdx.x;
+            int nx = t.bx + q % 3 - 1, ny = t.by + (q / 3) % 3 - 1, nz = t.bz + q / 9 - 1;
+            nx = nx < 0 ? nx + L.nb[0] : (nx >= L.nb[0] ? nx - L.nb[0] : nx);
+            ny = ny < 0 ? ny + L.nb[1] : (ny >= L.nb[1] ? ny - L.nb[1] : ny);
+            nz = nz < 0 ? nz + L.nb[2] : (nz >= L.nb[2] ? nz - L.nb[2] : nz);
+            snb[q] = nx + L.nb[0] * (ny + L.nb[1] * nz);
+        }
+        if (threadIdx.x == 32) {
+            unsigned plain = 0;
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                plain |= (__ldg(bc[c].mode + t.block) == 0 ? 1u : 0u) << c;
+            snb[27] = (int)plain;
+        }
+    }
+    // A halo cell outside the tile's block: for a plain component the
+    // periodic neighbour (what cn::lab_value gives for mode 0), else the lab.
+    template <typename T>
+    __device__ __forceinline__ T halo(const T *comp, int c, const TileInfo<T> &t, int gx, int gy, int gz,
+                                      const int *snb) const
+    {
+        if (((unsigned)snb[27] >> c) & 1u) {
+            const int r0 = gx < 0 ? -1 : (gx >= L.n[0] ? 1 : 0), r1 = gy < 0 ? -1 : (gy >= L.n[1] ? 1 : 0),
+                      r2 = gz < 0 ? -1 : (gz >= L.n[2] ? 1 : 0);
+            // the halo of a face sweep leaves the block along one direction only
+            const int sb = snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+            return comp[(int64_t)sb * L.bstride + (gx - r0 * L.n[0]) +
+                        (int64_t)L.n[0] * ((gy - r1 * L.n[1]) + (int64_t)L.n[1] * (gz - r2 * L.n[2]))];
+        }
         T v;
         if (!lab_value<T>(comp, L, bc[c], t.block, t.bx, t.by, t.bz, gx, gy, gz, true, v)) v = T(0);
         return v;
@@ -197,7 +231,7 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
 // exists once.
 template <typename T, typename Src>
 __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const Src &src, const TileInfo<T> &t,
-                                           T *W)
+                                           T *W, const int *snb)
 {
     T *slot = W + NCORE + (Stg<T>::all ? D * NHALO : 0);
     for (int i = threadIdx.x; i < NHALO; i += NT) {
@@ -213,7 +247,7 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
         } else {
 #pragma unroll 1
             for (int c = 0; c < 5; ++c)
-                slot[c * Stg<T>::SV + i] = src.halo(p.U[c], c, t, gx, gy, gz);
+                slot[c * Stg<T>::SV + i] = src.halo(p.U[c], c, t, gx, gy, gz, snb);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
                 u[c] = slot[c * Stg<T>::SV + i];
@@ -231,10 +265,12 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
 // W [5][Stg<T>::SV], F [5][NFACE] and red [NT/32][5] in shared memory.
 template <typename T, typename Src>
 __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &src, int item, int slot, T *W, T *F,
-                                           double (*red)[5])
+                                           double (*red)[5], int *snb)
 {
     TileInfo<T> t;
     src.template tile<T>(item, t);
+    src.template prepare<T>(t, snb);
+    __syncthreads(); // snb
     // ---- stage the tile's cells as primitives (the halo slot follows per sweep)
     for (int i = threadIdx.x; i < NCORE; i += NT) {
         const int x = i % TB, y = (i / TB) % TB, z = i / (TB * TB);
@@ -248,9 +284,9 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
     if (Stg<T>::all) {
 #pragma unroll 1
         for (int D = 0; D < 3; ++D)
-            stage_halo<T>(D, p, src, t, W);
+            stage_halo<T>(D, p, src, t, W, snb);
     } else {
-        stage_halo<T>(0, p, src, t, W);
+        stage_halo<T>(0, p, src, t, W, snb);
     }
     __syncthreads();
 
@@ -264,7 +300,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
 #pragma unroll 1
     for (int D = 0; D < 3; ++D) {
         if (!Stg<T>::all && D > 0) {
-            stage_halo<T>(D, p, src, t, W);
+            stage_halo<T>(D, p, src, t, W, snb);
             __syncthreads();
         }
         const T ihd = D == 0 ? t.ih[0] : (D == 1 ? t.ih[1] : t.ih[2]);
