@@ -49,6 +49,8 @@ _SIGS = {
     "cn_abi_version": (_I, []),
     "cn_stencil_check": (_I, [_ST]),
     "cn_grid_create": (_I, [_I3, _I3, _I, _I, _D3, _D3, C.POINTER(_P)]),
+    "cn_grid_create_entity": (_I, [_I3, _I3, _I, _I, _I, _D3, _D3, C.POINTER(_P)]),
+    "cn_grid_entity": (_I, [_P, C.POINTER(_I), _I3]),
     "cn_grid_destroy": (_I, [_P]),
     "cn_grid_layout": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_size_t)]),
     "cn_grid_cell_size": (_I, [_P, _D3]),

@@ -57,7 +57,7 @@ class FieldLab:
         if not self._alloc:
             raise RuntimeError("FieldLab: can not load lab data when not allocated first")
         flat = grid.flat_index(fid)
-        ext = grid.getBlockCells()
+        ext = grid.getBlockExtent()
         if any(e > m for e, m in zip(ext, self._max_range.getExtent())):
             raise RuntimeError("FieldLab: block larger than the allocated maximum range")
         torch = self._torch

@@ -48,7 +48,9 @@ struct HostBC {
 
 struct cn_grid {
     int nb[3];
-    int n[3];
+    int n[3];      // block extent in entities: cells, or cells + 1 for nodes / along a face direction
+    int cells[3];  // block cells (the mesh)
+    int entity;    // cn_entity
     int ncomp;
     cn_dtype dtype;
     double begin[3], end[3], h[3];

@@ -231,6 +231,16 @@ cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int nco
                          cn_dtype dtype, const double begin[3], const double end[3],
                          cn_grid **out)
 {
+    return cn_grid_create_entity(nblocks, block_cells, ncomp, dtype, CN_ENTITY_CELL, begin, end, out);
+}
+
+// Grid/Cartesian.h:490-513: a block holds cells^3 cell values, (cells+1)^3
+// node values, or, per face direction, (cells+1)^3 slots ("slightly more than
+// needed") of which the face field's index range (cells + 1 along its
+// direction) uses the first ones.
+cn_status cn_grid_create_entity(const int nblocks[3], const int block_cells[3], int ncomp, cn_dtype dtype,
+                                cn_entity entity, const double begin[3], const double end[3], cn_grid **out)
+{
     if (!out || !nblocks || !block_cells) {
         return fail(CN_ERR_INVALID_ARGUMENT, "cn_grid_create: NULL argument");
     }
@@ -239,14 +249,17 @@ cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int nco
     if (es == 0 || ncomp < 1) {
         return fail(CN_ERR_INVALID_ARGUMENT, "cn_grid_create: bad dtype or ncomp");
     }
+    if (entity < CN_ENTITY_CELL || entity > CN_ENTITY_FACE_Z) {
+        return fail(CN_ERR_INVALID_ARGUMENT, "cn_grid_create: bad entity type");
+    }
     int64_t nbl = 1;
-    int64_t cells = 1;
+    int64_t cells = 1; // storage elements per block
     for (int d = 0; d < 3; ++d) {
         if (nblocks[d] < 1 || block_cells[d] < 1 || block_cells[d] > 1024) {
             return fail(CN_ERR_INVALID_ARGUMENT, "cn_grid_create: block counts and cells must be >= 1");
         }
         nbl *= nblocks[d];
-        cells *= block_cells[d];
+        cells *= block_cells[d] + (entity == CN_ENTITY_CELL ? 0 : 1);
     }
     if (nbl > (1 << 30)) {
         return fail(CN_ERR_INVALID_ARGUMENT, "cn_grid_create: too many blocks");
@@ -255,9 +268,11 @@ cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int nco
     if (!g) {
         return fail(CN_ERR_OUT_OF_MEMORY, "cn_grid_create: host allocation failed");
     }
+    g->entity = entity;
     for (int d = 0; d < 3; ++d) {
         g->nb[d] = nblocks[d];
-        g->n[d] = block_cells[d];
+        g->cells[d] = block_cells[d];
+        g->n[d] = block_cells[d] + ((entity == CN_ENTITY_NODE || entity == CN_ENTITY_FACE_X + d) ? 1 : 0);
         g->begin[d] = begin ? begin[d] : 0.0;
         g->end[d] = end ? end[d] : 1.0;
         // Mesh/StructuredUniform.h:61: extent / cells
@@ -337,6 +352,15 @@ cn_status cn_grid_shape(const cn_grid *g, int info[8])
     }
     info[6] = g->ncomp;
     info[7] = (int)g->dtype;
+    return CN_OK;
+}
+
+cn_status cn_grid_entity(const cn_grid *g, int *entity, int block_cells[3])
+{
+    if (!g) return fail(CN_ERR_INVALID_ARGUMENT, "grid is NULL");
+    if (entity) *entity = g->entity;
+    if (block_cells)
+        for (int d = 0; d < 3; ++d) block_cells[d] = g->cells[d];
     return CN_OK;
 }
 

@@ -70,10 +70,14 @@ struct KArgs {
     double ih2d;
 };
 
-// Coefficients of one level (see op7_coef): k staged per tile with its
-// one-cell halo, then per cell the same operations as op7_math.
+// Coefficients of one level (see op7_coef) in precision TC (float for the
+// V-cycle, double for the outer FP64 residual): k staged per tile with its
+// one-cell halo, then per cell the operations of op7_math in TC.
+template <typename TC>
 __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const __grid_constant__ KArgs a,
-                                                            const __grid_constant__ Tile T, float *coef)
+                                                                          const __grid_constant__ Tile T,
+                                                                          const __grid_constant__ LabGeom Lo,
+                                                                          TC ih2, TC *coef, int64_t ccs)
 {
     __shared__ float sk[kRegionMax];
     __shared__ int snb[27];
@@ -84,24 +88,23 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const 
     stage_region<float>(a.k, a.G.Lk, a.kbc, q, false, snb, sk);
     cp_async_wait_all();
     __syncthreads();
-    const int cells = T.t[0] * T.t[1] * T.t[2];
-    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
-        int x, y, z;
-        tile_cell(T, c, x, y, z);
-        const int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
+    int x, y, z0, zl;
+    if (!column_run(T, x, y, z0, zl)) return;
+    const int st[3] = {1, q.ex, q.ex * q.ey};
+    for (int z = z0; z < z0 + zl; ++z) {
+        const int64_t o = (int64_t)q.block * Lo.bstride + (q.x0 + x) + (int64_t)Lo.n[0] * ((q.y0 + y) + (int64_t)Lo.n[1] * (q.z0 + z));
         const int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1));
-        const int st[3] = {1, q.ex, q.ex * q.ey};
-        const float kc = sk[u];
-        float sd[3];
+        const TC kc = (TC)sk[u];
+        TC sd[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            const float kp = harm<float>(kc, sk[u + st[d]]);
-            const float km = harm<float>(sk[u - st[d]], kc);
-            coef[d * a.ccs + o] = kp;
-            coef[(3 + d) * a.ccs + o] = km;
+            const TC kp = harm<TC>(kc, (TC)sk[u + st[d]]);
+            const TC km = harm<TC>((TC)sk[u - st[d]], kc);
+            coef[d * ccs + o] = kp;
+            coef[(3 + d) * ccs + o] = km;
             sd[d] = kp + km;
         }
-        coef[6 * a.ccs + o] = a.ih2 * ((sd[0] + sd[1]) + sd[2]);
+        coef[6 * ccs + o] = ih2 * ((sd[0] + sd[1]) + sd[2]);
     }
 }
 
@@ -121,16 +124,17 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) jacobi_kernel(cons
         cp_async_wait_all();
         __syncthreads();
     }
-    const int cells = T.t[0] * T.t[1] * T.t[2];
+    int x, y, z0, zl;
+    if (!column_run(T, x, y, z0, zl)) return;
     const int st[3] = {1, q.ex, q.ex * q.ey};
-    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
-        int x, y, z;
-        tile_cell(T, c, x, y, z);
-        const int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
+    const int64_t oz = (int64_t)L.n[0] * L.n[1];
+    int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z0));
+    int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z0 + 1));
+    for (int k = 0; k < zl; ++k, o += oz, u += st[2]) {
         const float fc = __ldg(f + o);
         if (pin) {
             float Lp, D, pc;
-            op7_coef<float>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
+            op7_coef<float, float>(sp, u, st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
             pout[o] = pc + omega * ((Lp - fc) / D);
         } else {
             // zero guess: L 0 = 0, only the diagonal is used
@@ -158,15 +162,20 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) resid_restrict_ker
     stage_region<float>(p, L, a.G.bc, q, false, snb, sp);
     cp_async_wait_all();
     __syncthreads();
-    const int cells = T.t[0] * T.t[1] * T.t[2];
-    const int st[3] = {1, q.ex, q.ex * q.ey};
-    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
-        int x, y, z;
-        tile_cell(T, c, x, y, z);
-        const int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
-        float Lp, D, pc;
-        op7_coef<float>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
-        sr[c] = __ldg(f + o) - Lp;
+    {
+        int x, y, z0, zl;
+        if (column_run(T, x, y, z0, zl)) {
+            const int st[3] = {1, q.ex, q.ex * q.ey};
+            const int64_t oz = (int64_t)L.n[0] * L.n[1];
+            int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z0));
+            int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z0 + 1));
+            int c = x + T.t[0] * (y + T.t[1] * z0);
+            for (int k = 0; k < zl; ++k, o += oz, u += st[2], c += T.t[0] * T.t[1]) {
+                float Lp, D, pc;
+                op7_coef<float, float>(sp, u, st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
+                sr[c] = __ldg(f + o) - Lp;
+            }
+        }
     }
     __syncthreads();
     const int hx = T.t[0] / 2, hy = T.t[1] / 2, hz = T.t[2] / 2;
@@ -253,10 +262,10 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(con
 // r32 = (float) r, per-CTA FP64 partial sums of r^2 (and f^2).
 __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_constant__ KArgs a,
                                                                const __grid_constant__ Tile T, const double *p64,
-                                                               const float *f, float *r32, double *partials)
+                                                               const float *f, float *r32, double *partials,
+                                                               const double *coef64, int64_t c64s)
 {
     __shared__ double sp[kRegionMax];
-    __shared__ float sk[kRegionMax];
     __shared__ double sh[2][kTileThreads / 32];
     __shared__ int snb[27];
     const LabGeom &L = a.G.L, &Lk = a.G.Lk;
@@ -264,23 +273,25 @@ __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_c
     neighbour_blocks(L.nb, q.block, snb);
     __syncthreads();
     stage_region<double>(p64, L, a.G.bc, q, false, snb, sp);
-    stage_region<float>(a.k, Lk, a.kbc, q, false, snb, sk);
     cp_async_wait_all();
     __syncthreads();
     double rr = 0, ff = 0;
-    const int cells = T.t[0] * T.t[1] * T.t[2];
-    for (int c = threadIdx.x; c < cells; c += kTileThreads) {
-        int x, y, z;
-        tile_cell(T, c, x, y, z);
-        const int64_t o = (int64_t)q.block * Lk.bstride + (q.x0 + x) + (int64_t)Lk.n[0] * ((q.y0 + y) + (int64_t)Lk.n[1] * (q.z0 + z));
-        double v[14], Lp, D, pc;
-        region7<double>(sp, sk, q, x, y, z, v);
-        op7_math<double>(v, a.ih2d, Lp, D, pc);
-        const double fc = (double)__ldg(f + o);
-        const double r = fc - Lp;
-        if (r32) r32[o] = (float)r;
-        rr += r * r;
-        ff += fc * fc;
+    int x, y, z0, zl;
+    if (column_run(T, x, y, z0, zl)) {
+        const int st[3] = {1, q.ex, q.ex * q.ey};
+        for (int z = z0; z < z0 + zl; ++z) {
+            const int64_t cell = (q.x0 + x) + (int64_t)Lk.n[0] * ((q.y0 + y) + (int64_t)Lk.n[1] * (q.z0 + z));
+            const int64_t o = (int64_t)q.block * Lk.bstride + cell;   // FP32 fields (f, r32)
+            const int64_t o64 = (int64_t)q.block * L.bstride + cell;  // FP64 fields (coefficients)
+            double Lp, D, pc;
+            op7_coef<double, double>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, coef64, c64s, o64, a.ih2d, Lp,
+                             D, pc);
+            const double fc = (double)__ldg(f + o);
+            const double r = fc - Lp;
+            if (r32) r32[o] = (float)r;
+            rr += r * r;
+            ff += fc * fc;
+        }
     }
     for (int off = 16; off > 0; off >>= 1) {
         rr += __shfl_down_sync(0xffffffffu, rr, off);
@@ -651,7 +662,18 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
         }
         const KArgs a = kargs(m, l);
         const Tile T = tile_of(m->p[l]->n);
-        coef_kernel<<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads>>>(a, T, fptr(c));
+        coef_kernel<float><<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads>>>(a, T, a.G.L, a.ih2, fptr(c),
+                                                                                      c->comp_stride);
+        if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
+    }
+    // FP64 coefficients of the finest level for the outer residual
+    if (s == CN_OK) s = cn_grid_create(k->nb, k->n, 7, CN_FLOAT64, b0, e0, &m->coef64);
+    if (s == CN_OK) {
+        const KArgs a = kargs(m, 0);
+        const Tile T = tile_of(k->n);
+        const LabGeom L64 = make_geom(m->coef64, &kS1);
+        coef_kernel<double><<<(unsigned)(k->nblocks * T.count), kTileThreads>>>(
+            a, T, L64, a.ih2d, reinterpret_cast<double *>(m->coef64->d_data), m->coef64->comp_stride);
         if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
     }
     if (s == CN_OK && cudaDeviceSynchronize() != cudaSuccess) s = fail(CN_ERR_CUDA, "cn_mg_create");
@@ -675,6 +697,7 @@ cn_status cn_mg_destroy(cn_mg *m)
     }
     cn_grid_destroy(m->r32);
     for (cn_grid *g : m->coef) cn_grid_destroy(g);
+    cn_grid_destroy(m->coef64);
     for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
     for (void *a : m->nn_act)
         if (a) cudaFree(a);
@@ -729,9 +752,12 @@ cn_status cn_mg_residual(cn_mg *m, const cn_grid *p64, const cn_grid *f, cn_grid
     KArgs a = kargs(m, 0);
     a.G.L.bstride = p64->block_stride;
     a.G.bc = bc_view(p64, 0);
-    resid64_kernel<<<m->nparts, kTileThreads, 0, st>>>(a, tile_of(p64->n), reinterpret_cast<const double *>(p64->d_data),
-                                                        reinterpret_cast<const float *>(f->d_data),
-                                                        r32 ? fptr(r32) : nullptr, m->partials);
+    if (p64->block_stride != m->coef64->block_stride)
+        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
+    resid64_kernel<<<m->nparts, kTileThreads, 0, st>>>(
+        a, tile_of(p64->n), reinterpret_cast<const double *>(p64->d_data), reinterpret_cast<const float *>(f->d_data),
+        r32 ? fptr(r32) : nullptr, m->partials, reinterpret_cast<const double *>(m->coef64->d_data),
+        m->coef64->comp_stride);
     CN_CUDA_TRY(cudaGetLastError());
     sum_pairs_kernel<<<1, 256, 0, st>>>(m->partials, m->nparts, m->sums);
     CN_CUDA_TRY(cudaGetLastError());

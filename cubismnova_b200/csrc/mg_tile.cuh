@@ -42,8 +42,8 @@ __device__ __forceinline__ void op7_math(const TP (&v)[14], TP ih2, TP &Lp, TP &
 // D = ih2 ((s0 + s1) + s2), s_d = kp_d + km_d: components 0-2 kp, 3-5 km,
 // 6 D of an FP32 grid laid out like p.  Evaluated with the same operations
 // as op7_math, so L p and D come out bit for bit the same.
-template <typename TP>
-__device__ __forceinline__ void op7_coef(const TP *sp, int u, const int (&st)[3], const float *coef, int64_t ccs,
+template <typename TP, typename TC>
+__device__ __forceinline__ void op7_coef(const TP *sp, int u, const int (&st)[3], const TC *coef, int64_t ccs,
                                          int64_t o, TP ih2, TP &Lp, TP &D, TP &pc)
 {
     pc = sp[u];
@@ -70,6 +70,7 @@ struct Tile {
     int per[3];    // tiles per block along x, y, z
     int count;     // tiles per block
     int sh[2];     // log2 of t[0], t[1] when powers of two, else -1
+    int zs;        // z groups: threads take (x, y) columns, split into zs runs along z
 };
 
 constexpr int kTileCap[3] = {32, 8, 4};
@@ -99,7 +100,33 @@ inline Tile tile_of(const int n[3])
         for (int b = 0; b < 31; ++b)
             if (T.t[d] == (1 << b)) T.sh[d] = b;
     }
+    const int cols = T.t[0] * T.t[1];
+    T.zs = 1;
+    for (int g = T.t[2]; g >= 1; --g)
+        if (T.t[2] % g == 0 && g * cols <= kTileThreads) {
+            T.zs = g;
+            break;
+        }
     return T;
+}
+
+// This thread's run of cells: column (x, y) of the tile and z0 .. z0+zl-1;
+// false for threads without work (more threads than columns x z groups).
+__device__ __forceinline__ bool column_run(const Tile &T, int &x, int &y, int &z0, int &zl)
+{
+    const int cols = T.t[0] * T.t[1];
+    const int g = threadIdx.x / cols, col = threadIdx.x - g * cols;
+    if (g >= T.zs) return false;
+    if (T.sh[0] >= 0) {
+        x = col & (T.t[0] - 1);
+        y = col >> T.sh[0];
+    } else {
+        x = col % T.t[0];
+        y = col / T.t[0];
+    }
+    zl = T.t[2] / T.zs;
+    z0 = g * zl;
+    return true;
 }
 
 // tile-local cell c -> (x, y, z)

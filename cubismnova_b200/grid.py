@@ -16,6 +16,8 @@ from .core import IndexRange
 
 _DT = {np.dtype(np.float32): _lib.CN_FLOAT32, np.dtype(np.float64): _lib.CN_FLOAT64,
        np.dtype(np.int32): _lib.CN_INT32}
+# Cubism::EntityType of the values (cn_entity)
+ENTITIES = {"cell": 0, "node": 1, "face_x": 2, "face_y": 3, "face_z": 4}
 
 
 def _stream_handle(stream):
@@ -83,7 +85,7 @@ class BlockField:
         return self._state
 
     def getIndexRange(self):
-        return IndexRange(self._g.getBlockCells())
+        return IndexRange(self._g.getBlockExtent())
 
     def getBC(self):
         return BCVector(self._g, self.comp, self.flat)
@@ -108,14 +110,19 @@ class TensorBlock:
         return BlockField(self._g, self.flat, 0).getState()
 
     def getIndexRange(self):
-        return IndexRange(self._g.getBlockCells())
+        return IndexRange(self._g.getBlockExtent())
 
 
 class Cartesian:
-    """Grid::Cartesian(nblocks, block_cells, begin, end) with ``ncomp`` components."""
+    """Grid::Cartesian(nblocks, block_cells, begin, end) with ``ncomp`` components.
+
+    ``entity`` is the Cubism::EntityType of the values: "cell" (default),
+    "node", or one direction of a face container ("face_x", "face_y",
+    "face_z"); ``getBlockCells`` is the mesh, ``getBlockExtent`` the values
+    per block (cells + 1 for nodes and along the face direction)."""
 
     def __init__(self, nblocks, block_cells, begin=(0.0, 0.0, 0.0), end=(1.0, 1.0, 1.0),
-                 ncomp: int = 1, dtype=np.float64):
+                 ncomp: int = 1, dtype=np.float64, entity: str = "cell"):
         nb = tuple(int(v) for v in (nblocks if hasattr(nblocks, "__len__") else (nblocks,) * 3))
         bc = tuple(int(v) for v in (block_cells if hasattr(block_cells, "__len__") else (block_cells,) * 3))
         self.dtype = np.dtype(dtype)
@@ -123,11 +130,14 @@ class Cartesian:
             raise ValueError("dtype must be float32, float64 or int32")
         self.ncomp = int(ncomp)
         h = C.c_void_p()
-        _lib.check(_lib.lib().cn_grid_create(_lib.ivec3(nb), _lib.ivec3(bc), self.ncomp,
-                                             _DT[self.dtype], _lib.dvec3(begin), _lib.dvec3(end),
-                                             C.byref(h)))
+        self.entity = entity
+        _lib.check(_lib.lib().cn_grid_create_entity(_lib.ivec3(nb), _lib.ivec3(bc), self.ncomp, _DT[self.dtype],
+                                                    ENTITIES[entity], _lib.dvec3(begin), _lib.dvec3(end),
+                                                    C.byref(h)))
         self._h = h
-        self._nb, self._n = nb, bc
+        info = (C.c_int * 8)()
+        _lib.check(_lib.lib().cn_grid_shape(h, info))
+        self._nb, self._n, self._cells = nb, tuple(info[3:6]), bc
         self._bcs = [dict() for _ in range(self.ncomp)]
         bs, cs, tb = C.c_int64(), C.c_int64(), C.c_size_t()
         _lib.check(_lib.lib().cn_grid_layout(h, C.byref(bs), C.byref(cs), C.byref(tb)))
@@ -147,6 +157,10 @@ class Cartesian:
         info = (C.c_int * 8)()
         _lib.check(_lib.lib().cn_grid_shape(g._h, info))
         g._nb, g._n = tuple(info[0:3]), tuple(info[3:6])
+        ent, cells = C.c_int(), (C.c_int * 3)()
+        _lib.check(_lib.lib().cn_grid_entity(g._h, C.byref(ent), cells))
+        g.entity = {v: k for k, v in ENTITIES.items()}[ent.value]
+        g._cells = tuple(cells)
         g.ncomp = info[6]
         g.dtype = {v: k for k, v in _DT.items()}[info[7]]
         g._bcs = [dict() for _ in range(g.ncomp)]
@@ -176,6 +190,12 @@ class Cartesian:
         return self._nb
 
     def getBlockCells(self):
+        """Cells per block of the mesh (Grid/Cartesian.h:240-256)."""
+        return self._cells
+
+    def getBlockExtent(self):
+        """Values per block and direction: the block field's index-range
+        extent (cells, or cells + 1 for nodes / along a face direction)."""
         return self._n
 
     def getCellSize(self):

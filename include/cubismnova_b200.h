@@ -54,6 +54,18 @@ typedef enum cn_status {
 
 typedef enum cn_dtype { CN_FLOAT32 = 0, CN_FLOAT64 = 1, CN_INT32 = 2 } cn_dtype;
 
+/* Cubism::EntityType (Common.h) of a grid's values: cell centres, nodes
+ * (cells + 1 per block and direction), or the faces normal to x, y or z
+ * (cells + 1 along that direction).  A reference FaceContainer grid is three
+ * face grids, one per direction. */
+typedef enum cn_entity {
+    CN_ENTITY_CELL = 0,
+    CN_ENTITY_NODE = 1,
+    CN_ENTITY_FACE_X = 2,
+    CN_ENTITY_FACE_Y = 3,
+    CN_ENTITY_FACE_Z = 4
+} cn_entity;
+
 /* BC::Base (periodic no-op) / BC::Dirichlet / BC::Absorbing / BC::Symmetry
  * (BC/Base.h:39-79, BC/Dirichlet.h:38, BC/Absorbing.h:35, BC/Symmetry.h:43) */
 typedef enum cn_bc_kind {
@@ -98,6 +110,14 @@ cn_status cn_stencil_check(const cn_stencil *s);
 cn_status cn_grid_create(const int nblocks[3], const int block_cells[3], int ncomp,
                          cn_dtype dtype, const double begin[3], const double end[3],
                          cn_grid **out);
+/* The same for node and face entities (Grid/Cartesian.h:490-513): the block
+ * extent is block_cells (+1 for nodes, +1 along the face direction); every
+ * lab, BC and stencil entry point works on that extent (FieldLab.h:104-224
+ * with the entity's index range), the cell size h stays (end-begin)/cells. */
+cn_status cn_grid_create_entity(const int nblocks[3], const int block_cells[3], int ncomp, cn_dtype dtype,
+                                cn_entity entity, const double begin[3], const double end[3], cn_grid **out);
+/* Entity type and block cells of a grid (its block extent is cn_grid_shape's). */
+cn_status cn_grid_entity(const cn_grid *g, int *entity, int block_cells[3]);
 cn_status cn_grid_destroy(cn_grid *g);
 /* Layout in elements: block stride, component stride; total bytes. */
 cn_status cn_grid_layout(const cn_grid *g, int64_t *block_stride, int64_t *comp_stride,

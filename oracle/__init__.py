@@ -116,12 +116,22 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def entity_stride(cells, entity, dtype) -> int:
+    """Block stride of a node (entity 1) or face (2..4) grid: (cells + 1)^3
+    slots rounded to 32 bytes (Grid/Cartesian.h:490-513); cells for entity 0."""
+    ext = [int(c) + (0 if entity == 0 else 1) for c in cells]
+    return block_stride(ext, dtype)
+
+
 def lab_fill(comp, nb, n, lo, hi, tensorial, bclists, block, use_ref=False,
-             lab_init=None):
-    """Lab of one block: returns (lab[Lz,Ly,Lx], defined[Lz,Ly,Lx] bool)."""
+             lab_init=None, stride=None, entity=0):
+    """Lab of one block: returns (lab[Lz,Ly,Lx], defined[Lz,Ly,Lx] bool).
+    `n` is the block's index-range extent; `stride` the block stride (default:
+    the cell layout of `n`); `entity` (cn_entity numbering) selects the
+    reference's node / face grid for use_ref (the C oracle is extent-generic)."""
     comp = np.ascontiguousarray(comp)
     sfx = _SUFFIX[comp.dtype]
-    stride = block_stride(n, comp.dtype)
+    stride = block_stride(n, comp.dtype) if stride is None else int(stride)
     g = make_geom(nb, n, lo, hi, tensorial, stride)
     nblocks = int(np.prod(nb))
     off, ents = bc_arrays(nblocks, bclists)
@@ -129,8 +139,14 @@ def lab_fill(comp, nb, n, lo, hi, tensorial, bclists, block, use_ref=False,
     lab = np.zeros((L[2], L[1], L[0]), dtype=comp.dtype) if lab_init is None \
         else np.array(lab_init, dtype=comp.dtype, copy=True)
     w = np.zeros((L[2], L[1], L[0]), dtype=np.uint8)
-    f = getattr(ref() if use_ref else lib(), ("ref_" if use_ref else "or_") + "lab_fill_" + sfx)
-    rc = f(C.byref(g), _ptr(comp), _ptr(off), ents, C.c_int(block), _ptr(lab), _ptr(w))
+    if use_ref and entity != 0:
+        if comp.dtype != np.float64:
+            raise ValueError("node/face reference labs are built for float64")
+        rc = ref().ref_lab_fill_entity_f64(C.byref(g), C.c_int(entity), _ptr(comp), _ptr(off), ents, C.c_int(block),
+                                           _ptr(lab), _ptr(w))
+    else:
+        f = getattr(ref() if use_ref else lib(), ("ref_" if use_ref else "or_") + "lab_fill_" + sfx)
+        rc = f(C.byref(g), _ptr(comp), _ptr(off), ents, C.c_int(block), _ptr(lab), _ptr(w))
     if rc != 0:
         raise ValueError("lab fill rejected the geometry")
     return lab, w.astype(bool)

@@ -276,6 +276,78 @@ double eulerStage<double>(const int nb[3], const int n[3], const double *Us, con
     }
     return best;
 }
+// Lab of one block of a node grid or of one direction of a face container
+// grid (Grid::Cartesian<T, Mesh, EntityType::Node|Face, 0>): g->n is the
+// field's index-range extent, g->block_stride the storage stride.
+template <typename T, EntityType E>
+int labFillEntity(const or_geom *g, int face_dir, const T *comp, const int32_t *bc_off, const or_bc *bcs,
+                  int block, T *lab_out, uint8_t *written)
+{
+    using G = Grid::Cartesian<T, Mesh, E, 0>;
+    using F = typename G::BaseType::FieldType; // the scalar (face) field
+    using Lab = Block::FieldLab<F>;
+    using S = typename Lab::StencilType;
+    int cells[3];
+    for (int d = 0; d < 3; ++d)
+        cells[d] = g->n[d] - ((E == EntityType::Node || d == face_dir) ? 1 : 0);
+    G grid(MIndex{g->nb[0], g->nb[1], g->nb[2]}, MIndex{cells[0], cells[1], cells[2]});
+    auto field = [&](size_t i) -> F & {
+        if constexpr (E == EntityType::Face) {
+            return grid[i][(size_t)face_dir];
+        } else {
+            return grid[i];
+        }
+    };
+    const size_t ext = (size_t)g->n[0] * g->n[1] * g->n[2];
+    for (size_t i = 0; i < grid.size(); ++i)
+        std::memcpy(field(i).getData(), comp + i * g->block_stride, ext * sizeof(T));
+    std::vector<std::unique_ptr<BC::Base<Lab>>> owned;
+    if (bc_off) {
+        for (size_t i = 0; i < grid.size(); ++i) {
+            auto &v = field(i).getBC();
+            for (int k = bc_off[i]; k < bc_off[i + 1]; ++k) {
+                const or_bc &b = bcs[k];
+                BC::Base<Lab> *pb = nullptr;
+                if (b.kind == OR_BC_DIRICHLET) pb = new BC::Dirichlet<Lab>(b.dir, b.side, (T)b.value);
+                else if (b.kind == OR_BC_ABSORBING) pb = new BC::Absorbing<Lab>(b.dir, b.side);
+                else if (b.kind == OR_BC_SYMMETRY) pb = new BC::Symmetry<Lab>(b.dir, b.side, (T)b.value);
+                else pb = new BC::Base<Lab>(b.dir, b.side);
+                owned.emplace_back(pb);
+                v.push_back(pb);
+            }
+        }
+    }
+    Lab lab;
+    const S s(MIndex{-g->lo[0], -g->lo[1], -g->lo[2]}, MIndex{g->hi[0] + 1, g->hi[1] + 1, g->hi[2] + 1},
+              g->tensorial != 0);
+    lab.allocate(s, field(0).getIndexRange());
+    const int L[3] = {g->n[0] + g->lo[0] + g->hi[0], g->n[1] + g->lo[1] + g->hi[1], g->n[2] + g->lo[2] + g->hi[2]};
+    const size_t le = (size_t)L[0] * L[1] * L[2];
+    std::vector<T> pass[2];
+    const T poison[2] = {(T)-12345, (T)54321};
+    for (int p = 0; p < 2; ++p) {
+        T *mem = reinterpret_cast<T *>(lab.getBlockPtr());
+        const size_t nmem = lab.getBlockBytes() / sizeof(T);
+        for (size_t i = 0; i < nmem; ++i) mem[i] = poison[p];
+        // Cartesian::loadLab (Grid/Cartesian.h:412-427) without its extent
+        // assert, which calls FaceContainer::getIndexRange() with no face
+        // index and does not compile for face containers
+        auto idx = grid.getIndexFunctor((size_t)0, (size_t)(face_dir < 0 ? 0 : face_dir));
+        lab.loadData(field((size_t)block).getState().block_index, idx);
+        pass[p].resize(le);
+        for (int z = 0; z < L[2]; ++z)
+            for (int y = 0; y < L[1]; ++y)
+                for (int x = 0; x < L[0]; ++x)
+                    pass[p][x + (size_t)L[0] * (y + (size_t)L[1] * z)] = lab(x - g->lo[0], y - g->lo[1], z - g->lo[2]);
+    }
+    for (size_t i = 0; i < le; ++i) {
+        const bool same = std::memcmp(&pass[0][i], &pass[1][i], sizeof(T)) == 0;
+        written[i] = same ? 1 : 0;
+        if (same) lab_out[i] = pass[0][i];
+    }
+    return 0;
+}
+
 } // namespace
 
 extern "C" {
@@ -294,6 +366,16 @@ int ref_lab_fill_i32(const or_geom *g, const int32_t *comp, const int32_t *bc_of
                      const or_bc *bcs, int block, int32_t *lab, uint8_t *written)
 {
     return labFill<int32_t>(g, comp, bc_off, bcs, block, lab, written);
+}
+// entity: 1 node, 2..4 faces normal to x, y, z (cn_entity numbering)
+int ref_lab_fill_entity_f64(const or_geom *g, int entity, const double *comp, const int32_t *bc_off,
+                            const or_bc *bcs, int block, double *lab, uint8_t *written)
+{
+    if (entity == 1)
+        return labFillEntity<double, EntityType::Node>(g, -1, comp, bc_off, bcs, block, lab, written);
+    if (entity >= 2 && entity <= 4)
+        return labFillEntity<double, EntityType::Face>(g, entity - 2, comp, bc_off, bcs, block, lab, written);
+    return 1;
 }
 
 // Periodic grid (no BCs): Laplacian into lap and/or gradient into grad

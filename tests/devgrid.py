@@ -22,7 +22,7 @@ def lab_fill_all(cn, g, lo, hi, tens, comp=0, blocks=None, apply_bc=True):
     (labs[nblk, Lz, Ly, Lx], written[nblk, Lz, Ly, Lx])."""
     import torch
     from cubismnova_b200 import _lib
-    n = g.getBlockCells()
+    n = g.getBlockExtent()
     L = [n[d] + lo[d] + hi[d] for d in range(3)]
     st = _lib.stencil_struct([-v for v in lo], [v + 1 for v in hi], tens)
     b0, cnt = (0, g.size()) if blocks is None else blocks

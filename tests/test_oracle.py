@@ -252,3 +252,59 @@ def test_mg_oracle_solve_satisfies_the_discrete_equation(oracle_lib):
         Lp += hp * (np.roll(p, -1, ax) - p) - hm * (p - np.roll(p, 1, ax))
     Lp /= h * h
     assert np.linalg.norm(f32 - Lp) <= 2e-8 * np.linalg.norm(f32)
+
+
+ENTITY_N = {1: lambda c: [v + 1 for v in c], 2: lambda c: [c[0] + 1, c[1], c[2]],
+            3: lambda c: [c[0], c[1] + 1, c[2]], 4: lambda c: [c[0], c[1], c[2] + 1]}
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("entity", [1, 2, 3, 4], ids=["node", "face_x", "face_y", "face_z"])
+def test_oracle_vs_reference_node_face(oracle_lib, entity):
+    """Node grids and the three face fields of a FaceContainer grid
+    (Grid::Cartesian<T, Mesh, EntityType::Node|Face>): the extent-generic C
+    oracle against the reference's FieldLab on those fields, with randomised
+    geometries, stencils and BC vectors."""
+    O = oracle_lib
+    rng = np.random.default_rng(100 + entity)
+    for trial in range(40):
+        nb = rng.integers(1, 4, size=3)
+        cells = [int(v) for v in rng.integers(2, 6, size=3)]
+        n = ENTITY_N[entity](cells)
+        lo = [int(rng.integers(0, cells[d] + 1)) for d in range(3)]
+        hi = [int(rng.integers(0, cells[d] + 1)) for d in range(3)]
+        tens = bool(rng.integers(0, 2))
+        nblocks = int(np.prod(nb))
+        stride = O.entity_stride(cells, entity, np.float64)
+        comp = rng.standard_normal(nblocks * stride) * 100
+        bcl = {b: [(int(rng.integers(0, 3)), int(rng.integers(0, 2)), int(rng.integers(0, 4)),
+                    float(rng.integers(-3, 4))) for _ in range(int(rng.integers(0, 5)))]
+               for b in range(nblocks)}
+        for block in range(nblocks):
+            a, wa = O.lab_fill(comp, nb, n, lo, hi, tens, bcl, block, stride=stride)
+            r, wr = O.lab_fill(comp, nb, n, lo, hi, tens, bcl, block, use_ref=True, stride=stride, entity=entity)
+            assert np.all(wa <= wr)
+            assert np.array_equal(a[wa], r[wa])
+
+
+@pytest.mark.parametrize("entity", [1, 2], ids=["node", "face_x"])
+@pytest.mark.parametrize("tens", [False, True])
+def test_node_face_periodic_identities(oracle_lib, entity, tens):
+    """FieldLabTest.cpp:56-100 for Node and Face fields (there in 2-D): one
+    periodic block, stencil (-2, 3); ghosts equal the values one extent away."""
+    O = oracle_lib
+    cells = [16, 16, 16]
+    n = ENTITY_N[entity](cells)
+    stride = O.entity_stride(cells, entity, np.float64)
+    comp = np.zeros(stride)
+    comp[: int(np.prod(n))] = np.arange(int(np.prod(n)), dtype=np.float64)
+    lab, w = O.lab_fill(comp, (1, 1, 1), n, (2, 2, 2), (2, 2, 2), tens, {}, 0, stride=stride)
+    f = comp[: int(np.prod(n))].reshape(n[2], n[1], n[0])
+    L = LC.Lab(lab, n, (2, 2, 2), (2, 2, 2))
+    W = LC.Lab(w, n, (2, 2, 2), (2, 2, 2))
+    for z in range(-2, n[2] + 2):
+        for y in range(-2, n[1] + 2):
+            for x in range(-2, n[0] + 2):
+                if not W[(x, y, z)]:
+                    continue
+                assert L[(x, y, z)] == f[z % n[2], y % n[1], x % n[0]]
