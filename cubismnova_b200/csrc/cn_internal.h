@@ -96,14 +96,24 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 
 // Geometry of a lab for one stencil on one grid.
 struct LabGeom {
-    int n[3];  // cells per block
+    int n[3];  // largest block extent (cells, +1 for nodes / along a face direction)
     int nb[3]; // blocks per dimension
     int lo[3]; // -begin
     int hi[3]; // end - 1
     int tensorial;
     int valid_bc[3]; // BC/Base.h:73-78 per direction
     int64_t bstride;
+    // 1 where only the last block along the dimension has extent n and the
+    // others n - 1 (node fields: every dimension; face fields: their
+    // direction; Grid/BlockFieldAssembler.h:124-135); 0 for cell fields
+    int grow[3];
 };
+
+// extent along d of the block with coordinate bc along d
+__host__ __device__ __forceinline__ int block_extent(const LabGeom &L, int d, int bc)
+{
+    return L.n[d] - ((L.grow[d] && bc != L.nb[d] - 1) ? 1 : 0);
+}
 
 inline LabGeom make_geom(const cn_grid *g, const cn_stencil *s)
 {
@@ -117,6 +127,8 @@ inline LabGeom make_geom(const cn_grid *g, const cn_stencil *s)
     }
     L.tensorial = s->tensorial ? 1 : 0;
     L.bstride = g->block_stride;
+    for (int d = 0; d < 3; ++d)
+        L.grow[d] = (g->entity == CN_ENTITY_NODE || g->entity == CN_ENTITY_FACE_X + d) ? 1 : 0;
     return L;
 }
 
@@ -137,11 +149,21 @@ inline LabGeom make_geom(const cn_grid *g, const cn_stencil *s)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int pick3(int d, int a, int b, int c) { return d == 0 ? a : (d == 1 ? b : c); }
 
-template <typename T>
+// GROW: the grid may hold node / face fields (per-block extents); cell grids
+// (every fused stencil kernel) compile without that logic.
+template <typename T, bool GROW = false>
 __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabGeom &L,
                                           const BcView &bc, int block, int bx, int by, int bz,
                                           int q0, int q1, int q2, bool apply_bc, T &out)
 {
+    // this block's extents (node / face fields: the last block along a grown
+    // dimension holds one more entity); cells past its lab range are not part
+    // of its lab
+    const int e0 = GROW ? block_extent(L, 0, bx) : L.n[0];
+    const int e1 = GROW ? block_extent(L, 1, by) : L.n[1];
+    const int e2 = GROW ? block_extent(L, 2, bz) : L.n[2];
+    if (GROW && (q0 >= e0 + L.hi[0] || q1 >= e1 + L.hi[1] || q2 >= e2 + L.hi[2]))
+        return false;
     // skip flags hold even when the BCs themselves are not applied
     const uint8_t mode = bc.mode[block];
     T s0 = T(1), s1 = T(1), s2 = T(1); // symmetry signs of the chain, outermost first
@@ -161,13 +183,13 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
                 if (!pick3(d, L.valid_bc[0], L.valid_bc[1], L.valid_bc[2]))
                     continue;
                 const int qd = pick3(d, q0, q1, q2);
-                const int nd = pick3(d, L.n[0], L.n[1], L.n[2]);
+                const int nd = pick3(d, e0, e1, e2);
                 if (!(bc_side(m) == 0 ? (qd < 0) : (qd >= nd)))
                     continue;
                 if (!L.tensorial) {
-                    const bool in0 = d == 0 || ((unsigned)q0 < (unsigned)L.n[0]);
-                    const bool in1 = d == 1 || ((unsigned)q1 < (unsigned)L.n[1]);
-                    const bool in2 = d == 2 || ((unsigned)q2 < (unsigned)L.n[2]);
+                    const bool in0 = d == 0 || ((unsigned)q0 < (unsigned)e0);
+                    const bool in1 = d == 1 || ((unsigned)q1 < (unsigned)e1);
+                    const bool in2 = d == 2 || ((unsigned)q2 < (unsigned)e2);
                     if (!(in0 && in1 && in2))
                         continue;
                 }
@@ -179,7 +201,7 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
                 break;
             const int d = bc_dir(meta);
             const int kind = bc_kind(meta);
-            const int nd = pick3(d, L.n[0], L.n[1], L.n[2]);
+            const int nd = pick3(d, e0, e1, e2);
             if (kind == CN_BC_DIRICHLET) {
                 T v = static_cast<T>(e[found].value);
                 // apply the chain's signs innermost first
@@ -207,10 +229,11 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
         }
     }
     // loaded value
-    const int r0 = q0 < 0 ? -1 : (q0 >= L.n[0] ? 1 : 0);
-    const int r1 = q1 < 0 ? -1 : (q1 >= L.n[1] ? 1 : 0);
-    const int r2 = q2 < 0 ? -1 : (q2 >= L.n[2] ? 1 : 0);
+    const int r0 = q0 < 0 ? -1 : (q0 >= e0 ? 1 : 0);
+    const int r1 = q1 < 0 ? -1 : (q1 >= e1 ? 1 : 0);
+    const int r2 = q2 < 0 ? -1 : (q2 >= e2 ? 1 : 0);
     int src_block = block;
+    int s0e = e0, s1e = e1; // extents (x, y) of the source block
     if (r0 | r1 | r2) {
         if (!L.tensorial && (r0 != 0) + (r1 != 0) + (r2 != 0) > 1)
             return false;
@@ -224,11 +247,18 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
         nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
         nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
         src_block = nbx + L.nb[0] * (nby + L.nb[1] * nbz);
-        q0 -= r0 * L.n[0];
-        q1 -= r1 * L.n[1];
-        q2 -= r2 * L.n[2];
+        // a lower neighbour is read from its end (its own extent), an upper
+        // one from its start (FieldLabLoader.h:212-214, 230-240)
+        const int ne0 = GROW ? block_extent(L, 0, nbx) : L.n[0];
+        const int ne1 = GROW ? block_extent(L, 1, nby) : L.n[1];
+        const int ne2 = GROW ? block_extent(L, 2, nbz) : L.n[2];
+        q0 += r0 < 0 ? ne0 : -r0 * e0;
+        q1 += r1 < 0 ? ne1 : -r1 * e1;
+        q2 += r2 < 0 ? ne2 : -r2 * e2;
+        s0e = ne0;
+        s1e = ne1;
     }
-    T v = comp[(int64_t)src_block * L.bstride + q0 + (int64_t)L.n[0] * (q1 + (int64_t)L.n[1] * q2)];
+    T v = comp[(int64_t)src_block * L.bstride + q0 + (int64_t)s0e * (q1 + (int64_t)s1e * q2)];
     if (nsign > 2) v = s2 * v;
     if (nsign > 1) v = s1 * v;
     if (nsign > 0) v = s0 * v;
@@ -252,7 +282,8 @@ __device__ __noinline__ T lab_fetch_slow(const T *comp, const LabGeom &L, const 
     return v;
 }
 
-// Value of component comp at cell (x,y,z) of `block` (may lie outside it): in-block cells and the periodic neighbours of blocks without BCs
+// Value of component comp at cell (x,y,z) of `block` (may lie outside it);
+// cell-centred grids (every block has extent L.n): in-block cells and the periodic neighbours of blocks without BCs
 // or skip flags (lab mode byte 0, what cn::lab_value resolves to for them)
 // are plain loads; the rest go through the lab.
 template <typename T>

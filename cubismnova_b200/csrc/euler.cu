@@ -98,6 +98,8 @@ static cn_status check_euler(const cn_grid *g, int comp0)
         return fail(CN_ERR_INVALID_ARGUMENT, "Euler state needs 5 components");
     if (g->dtype != CN_FLOAT64 && g->dtype != CN_FLOAT32)
         return fail(CN_ERR_UNSUPPORTED, "Euler kernels need FLOAT32 or FLOAT64 grids");
+    if (g->entity != CN_ENTITY_CELL)
+        return fail(CN_ERR_UNSUPPORTED, "Euler kernels need cell-centred grids");
     for (int d = 0; d < 3; ++d)
         if (g->n[d] % TB != 0 || g->n[d] < G)
             return fail(CN_ERR_UNSUPPORTED, "Euler kernels need block cells divisible by 8");

@@ -321,6 +321,8 @@ static cn_status dispatch_fd(cn_grid *u, int comp, int ncin, cn_grid *o1, int c1
                              int c2, void *stream)
 {
     if (!u) return fail(CN_ERR_INVALID_ARGUMENT, "input grid is NULL");
+    if (u->entity != CN_ENTITY_CELL)
+        return fail(CN_ERR_UNSUPPORTED, "finite-difference stencils need cell-centred grids");
     if (comp < 0 || comp + ncin > u->ncomp)
         return fail(CN_ERR_INVALID_ARGUMENT, "input component out of range");
     cn_status s;

@@ -10,7 +10,7 @@
 
 namespace cn {
 
-template <typename T>
+template <typename T, bool GROW>
 __global__ void __launch_bounds__(256)
     lab_fill_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin,
                     int block_count, int apply_bc, T *__restrict__ out)
@@ -32,8 +32,8 @@ __global__ void __launch_bounds__(256)
         const int by = (block / L.nb[0]) % L.nb[1];
         const int bz = block / (L.nb[0] * L.nb[1]);
         T v;
-        if (lab_value<T>(comp, L, bc, block, bx, by, bz, x - L.lo[0], y - L.lo[1],
-                         z - L.lo[2], apply_bc != 0, v)) {
+        if (lab_value<T, GROW>(comp, L, bc, block, bx, by, bz, x - L.lo[0], y - L.lo[1],
+                               z - L.lo[2], apply_bc != 0, v)) {
             out[t] = v;
         }
     }
@@ -54,8 +54,12 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
     const int64_t cap = (int64_t)sms * 8;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    lab_fill_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(src, L, bc_view(g, comp), b0, cnt,
-                                                          apply_bc, reinterpret_cast<T *>(d_labs));
+    if (L.grow[0] || L.grow[1] || L.grow[2])
+        lab_fill_kernel<T, true><<<(unsigned)blocks, 256, 0, st>>>(src, L, bc_view(g, comp), b0, cnt, apply_bc,
+                                                                   reinterpret_cast<T *>(d_labs));
+    else
+        lab_fill_kernel<T, false><<<(unsigned)blocks, 256, 0, st>>>(src, L, bc_view(g, comp), b0, cnt, apply_bc,
+                                                                    reinterpret_cast<T *>(d_labs));
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }

@@ -588,6 +588,8 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
     *out = nullptr;
     if (k->dtype != CN_FLOAT32 || k->ncomp < 1)
         return fail(CN_ERR_UNSUPPORTED, "cn_mg_create: the coefficient grid must be FLOAT32");
+    if (k->entity != CN_ENTITY_CELL)
+        return fail(CN_ERR_UNSUPPORTED, "cn_mg_create: cell-centred grids only");
     if (k->h[0] != k->h[1] || k->h[0] != k->h[2])
         return fail(CN_ERR_UNSUPPORTED, "cn_mg_create: cubic cells are required");
     if (nu1 < 0 || nu2 < 0 || omega <= 0 || omega >= 2)

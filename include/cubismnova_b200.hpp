@@ -152,16 +152,19 @@ private:
     int flat_, comp_;
 };
 
-/// Grid::Cartesian(nblocks, block_cells, begin, end) with ncomp components on the GPU.
+/// Grid::Cartesian(nblocks, block_cells, begin, end) with ncomp components on
+/// the GPU.  `entity` as Cubism::EntityType (a FaceContainer grid is three
+/// face grids, one per direction): node and face fields have one more entity
+/// along a grown dimension in the last block of that dimension.
 template <typename T> class Cartesian {
 public:
     Cartesian(const MultiIndex &nblocks, const MultiIndex &block_cells,
               const std::array<double, 3> &begin = {0, 0, 0}, const std::array<double, 3> &end = {1, 1, 1},
-              int ncomp = 1)
-        : nb_(nblocks), n_(block_cells), ncomp_(ncomp)
+              int ncomp = 1, cn_entity entity = CN_ENTITY_CELL)
+        : nb_(nblocks), n_(block_cells), ncomp_(ncomp), entity_(entity)
     {
-        check(cn_grid_create(nblocks.data(), block_cells.data(), ncomp, DType<T>::value, begin.data(), end.data(),
-                             &g_));
+        check(cn_grid_create_entity(nblocks.data(), block_cells.data(), ncomp, DType<T>::value, entity, begin.data(),
+                                    end.data(), &g_));
         check(cn_grid_layout(g_, &bstride_, &cstride_, nullptr));
     }
     Cartesian(const Cartesian &) = delete;
@@ -174,6 +177,16 @@ public:
     size_t size() const { return (size_t)nb_[0] * nb_[1] * nb_[2]; }
     MultiIndex getSize() const { return nb_; }
     MultiIndex getBlockCells() const { return n_; }
+    cn_entity getEntity() const { return entity_; }
+    /// index-range extent of block field `flat` (Grid/BlockFieldAssembler.h:124-135)
+    MultiIndex getBlockExtent(int flat) const
+    {
+        MultiIndex e = n_;
+        const int bi[3] = {flat % nb_[0], (flat / nb_[0]) % nb_[1], flat / (nb_[0] * nb_[1])};
+        for (int d = 0; d < 3; ++d)
+            if ((entity_ == CN_ENTITY_NODE || entity_ == CN_ENTITY_FACE_X + d) && bi[d] == nb_[d] - 1) ++e[d];
+        return e;
+    }
     std::array<double, 3> getCellSize() const
     {
         std::array<double, 3> h;
@@ -211,6 +224,7 @@ private:
     cn_grid *g_ = nullptr;
     MultiIndex nb_, n_;
     int ncomp_;
+    cn_entity entity_;
     int64_t bstride_ = 0, cstride_ = 0;
     std::vector<std::unique_ptr<BC::Base>> owned_;
 };
@@ -236,7 +250,7 @@ template <typename T> typename BlockField<T>::State BlockField<T>::getState() co
 template <typename T> Core::IndexRange BlockField<T>::getIndexRange() const
 {
     Core::IndexRange r;
-    r.end = g_->getBlockCells();
+    r.end = g_->getBlockExtent(flat_);
     return r;
 }
 
@@ -271,12 +285,23 @@ public:
 
     /// Cartesian::loadLab / FieldLab::loadData (Grid/Cartesian.h:412-427,
     /// Block/FieldLab.h:180-224) for block field `f`.
+    /// The device buffer holds the grid's largest lab (cn_lab_extent: node and
+    /// face grids have one more entity in the last block of a grown dimension);
+    /// it grows here if the range given to allocate() was smaller.
     void loadData(Grid::BlockField<T> f, bool apply_bc = true, void *stream = nullptr)
     {
         if (!allocated_) throw std::runtime_error("FieldLab: can not load lab data when not allocated first");
+        int ext[3];
+        check(cn_lab_extent(f.grid().raw(), s_.raw(), ext));
+        const size_t need = (size_t)ext[0] * ext[1] * ext[2];
+        if (need > cap_) {
+            release_();
+            if (cudaMallocWrapper_(need)) throw std::runtime_error("FieldLab: device allocation failed");
+            cap_ = need;
+        }
         check(cn_lab_fill(f.grid().raw(), f.comp(), s_.raw(), f.flat(), 1, apply_bc ? 1 : 0, buf_, stream));
         field_ = f.flat();
-        range_.end = f.grid().getBlockCells();
+        range_.end = f.getIndexRange().end;
     }
     const Core::Stencil &getActiveStencil() const { return s_; }
     Core::IndexRange getActiveRange() const { return range_; }

@@ -34,7 +34,7 @@ class OrBC(C.Structure):
 class OrGeom(C.Structure):
     _fields_ = [("nb", C.c_int32 * 3), ("n", C.c_int32 * 3), ("lo", C.c_int32 * 3),
                 ("hi", C.c_int32 * 3), ("tensorial", C.c_int32),
-                ("block_stride", C.c_int64)]
+                ("block_stride", C.c_int64), ("grow", C.c_int32 * 3)]
 
 
 _lib = None
@@ -84,10 +84,14 @@ def block_stride(n, dtype) -> int:
     return nbytes // itemsize
 
 
-def make_geom(nb, n, lo, hi, tensorial, stride) -> OrGeom:
+ENTITY_GROW = {0: (0, 0, 0), 1: (1, 1, 1), 2: (1, 0, 0), 3: (0, 1, 0), 4: (0, 0, 1)}
+
+
+def make_geom(nb, n, lo, hi, tensorial, stride, entity=0) -> OrGeom:
     g = OrGeom()
     for d in range(3):
         g.nb[d], g.n[d], g.lo[d], g.hi[d] = int(nb[d]), int(n[d]), int(lo[d]), int(hi[d])
+        g.grow[d] = ENTITY_GROW[entity][d]
     g.tensorial = 1 if tensorial else 0
     g.block_stride = int(stride)
     return g
@@ -126,13 +130,14 @@ def entity_stride(cells, entity, dtype) -> int:
 def lab_fill(comp, nb, n, lo, hi, tensorial, bclists, block, use_ref=False,
              lab_init=None, stride=None, entity=0):
     """Lab of one block: returns (lab[Lz,Ly,Lx], defined[Lz,Ly,Lx] bool).
-    `n` is the block's index-range extent; `stride` the block stride (default:
-    the cell layout of `n`); `entity` (cn_entity numbering) selects the
-    reference's node / face grid for use_ref (the C oracle is extent-generic)."""
+    `n` is the largest block extent (cells, or cells + 1 for nodes and along
+    a face direction, where only the last block along that dimension has it);
+    `stride` the block stride (default: the cell layout of `n`); `entity`
+    (cn_entity numbering) selects node / face fields."""
     comp = np.ascontiguousarray(comp)
     sfx = _SUFFIX[comp.dtype]
     stride = block_stride(n, comp.dtype) if stride is None else int(stride)
-    g = make_geom(nb, n, lo, hi, tensorial, stride)
+    g = make_geom(nb, n, lo, hi, tensorial, stride, entity)
     nblocks = int(np.prod(nb))
     off, ents = bc_arrays(nblocks, bclists)
     L = [int(n[d]) + int(lo[d]) + int(hi[d]) for d in range(3)]

@@ -39,6 +39,13 @@ static int geom_ok(const or_geom *g)
     return 1;
 }
 
+/* extent of block coordinate bc along d (the last block of a grown
+ * dimension holds one more entity than the others) */
+static int block_extent(const or_geom *g, int d, int bc)
+{
+    return g->n[d] - (g->grow[d] && bc != g->nb[d] - 1 ? 1 : 0);
+}
+
 static int bc_valid(const or_geom *g, int dir)
 {
     /* BC/Base.h:73-78: no-op if either side of the stencil has zero width */
@@ -56,13 +63,15 @@ static int bc_valid(const or_geom *g, int dir)
         const int nblocks = nbx * nby * nbz;                                   \
         if (block < 0 || block >= nblocks)                                     \
             return 1;                                                          \
-        const int N[3] = {g->n[0], g->n[1], g->n[2]};                          \
         const int b[3] = {block % nbx, (block / nbx) % nby,                    \
                           block / (nbx * nby)};                                \
+        /* this block's extent; the lab array has the largest extent */        \
+        const int N[3] = {block_extent(g, 0, b[0]), block_extent(g, 1, b[1]),  \
+                          block_extent(g, 2, b[2])};                           \
         const T *self = comp + (size_t)block * g->block_stride;                \
-        memset(written, 0, (size_t)(N[0] + g->lo[0] + g->hi[0]) *             \
-                               (N[1] + g->lo[1] + g->hi[1]) *                  \
-                               (N[2] + g->lo[2] + g->hi[2]));                  \
+        memset(written, 0, (size_t)(g->n[0] + g->lo[0] + g->hi[0]) *          \
+                               (g->n[1] + g->lo[1] + g->hi[1]) *               \
+                               (g->n[2] + g->lo[2] + g->hi[2]));               \
         /* 1. inner */                                                         \
         for (int z = 0; z < N[2]; ++z)                                         \
             for (int y = 0; y < N[1]; ++y)                                     \
@@ -99,6 +108,9 @@ static int bc_valid(const or_geom *g, int dir)
                                 (b[2] + bi[2] + nbz) % nbz};                   \
             const T *nb = comp + (size_t)(nbi[0] + nbx * (nbi[1] + nby * nbi[2])) \
                                      * g->block_stride;                        \
+            /* neighbour extent; a lower neighbour is read from its end */     \
+            const int NN[3] = {block_extent(g, 0, nbi[0]), block_extent(g, 1, nbi[1]), \
+                               block_extent(g, 2, nbi[2])};                    \
             int beg[3], end[3];                                                \
             for (int d = 0; d < 3; ++d) {                                      \
                 beg[d] = bi[d] < 0 ? -g->lo[d] : (bi[d] == 0 ? 0 : N[d]);      \
@@ -107,11 +119,11 @@ static int bc_valid(const or_geom *g, int dir)
             for (int z = beg[2]; z < end[2]; ++z)                              \
                 for (int y = beg[1]; y < end[1]; ++y)                          \
                     for (int x = beg[0]; x < end[0]; ++x) {                    \
-                        const int sx = x - bi[0] * N[0];                       \
-                        const int sy = y - bi[1] * N[1];                       \
-                        const int sz = z - bi[2] * N[2];                       \
+                        const int sx = x - bi[0] * N[0] + (bi[0] < 0 ? NN[0] - N[0] : 0); \
+                        const int sy = y - bi[1] * N[1] + (bi[1] < 0 ? NN[1] - N[1] : 0); \
+                        const int sz = z - bi[2] * N[2] + (bi[2] < 0 ? NN[2] - N[2] : 0); \
                         const size_t li = LAB_INDEX(g, x, y, z);               \
-                        lab[li] = nb[sx + (size_t)N[0] * (sy + (size_t)N[1] * sz)]; \
+                        lab[li] = nb[sx + (size_t)NN[0] * (sy + (size_t)NN[1] * sz)]; \
                         written[li] = 1;                                       \
                     }                                                          \
         }                                                                      \

@@ -39,11 +39,15 @@ typedef struct {
 
 typedef struct {
     int32_t nb[3];    /* blocks per dimension */
-    int32_t n[3];     /* cells per block and dimension */
+    int32_t n[3];     /* largest block extent per dimension (labs are this large) */
     int32_t lo[3];    /* -stencil.begin */
     int32_t hi[3];    /* stencil.end - 1 */
     int32_t tensorial;
     int64_t block_stride; /* elements between consecutive blocks */
+    /* 1 where only the last block along a dimension holds n entities and the
+     * others n - 1 (node fields in every dimension, a face field along its
+     * direction: Grid/BlockFieldAssembler.h:124-135); 0 for cell fields */
+    int32_t grow[3];
 } or_geom;
 
 /* Lab fill of one block (FieldLab::loadData).  bc_off has nblocks+1 entries

@@ -5,9 +5,11 @@ import ctypes as C
 import numpy as np
 
 
-def make_grid(cn, comp, nb, n, bcl=None, ncomp=1, dtype=None, begin=(0, 0, 0), end=(1, 1, 1)):
+def make_grid(cn, comp, nb, n, bcl=None, ncomp=1, dtype=None, begin=(0, 0, 0), end=(1, 1, 1), entity="cell"):
+    """`n`: block cells (the mesh); node / face grids hold one more entity
+    along grown dimensions in the last block."""
     dtype = np.dtype(dtype or comp.dtype)
-    g = cn.Grid.Cartesian(nb, n, begin, end, ncomp=ncomp, dtype=dtype)
+    g = cn.Grid.Cartesian(nb, n, begin, end, ncomp=ncomp, dtype=dtype, entity=entity)
     g.upload(comp.astype(dtype), 0)
     for b, lst in (bcl or {}).items():
         for (d, s, k, v) in lst:

@@ -262,8 +262,9 @@ ENTITY_N = {1: lambda c: [v + 1 for v in c], 2: lambda c: [c[0] + 1, c[1], c[2]]
 @pytest.mark.parametrize("entity", [1, 2, 3, 4], ids=["node", "face_x", "face_y", "face_z"])
 def test_oracle_vs_reference_node_face(oracle_lib, entity):
     """Node grids and the three face fields of a FaceContainer grid
-    (Grid::Cartesian<T, Mesh, EntityType::Node|Face>): the extent-generic C
-    oracle against the reference's FieldLab on those fields, with randomised
+    (Grid::Cartesian<T, Mesh, EntityType::Node|Face>, where only the last
+    block along a grown dimension holds cells + 1 entities): the C oracle
+    against the reference's FieldLab on those fields, with randomised
     geometries, stencils and BC vectors."""
     O = oracle_lib
     rng = np.random.default_rng(100 + entity)
@@ -281,7 +282,7 @@ def test_oracle_vs_reference_node_face(oracle_lib, entity):
                     float(rng.integers(-3, 4))) for _ in range(int(rng.integers(0, 5)))]
                for b in range(nblocks)}
         for block in range(nblocks):
-            a, wa = O.lab_fill(comp, nb, n, lo, hi, tens, bcl, block, stride=stride)
+            a, wa = O.lab_fill(comp, nb, n, lo, hi, tens, bcl, block, stride=stride, entity=entity)
             r, wr = O.lab_fill(comp, nb, n, lo, hi, tens, bcl, block, use_ref=True, stride=stride, entity=entity)
             assert np.all(wa <= wr)
             assert np.array_equal(a[wa], r[wa])
@@ -298,7 +299,7 @@ def test_node_face_periodic_identities(oracle_lib, entity, tens):
     stride = O.entity_stride(cells, entity, np.float64)
     comp = np.zeros(stride)
     comp[: int(np.prod(n))] = np.arange(int(np.prod(n)), dtype=np.float64)
-    lab, w = O.lab_fill(comp, (1, 1, 1), n, (2, 2, 2), (2, 2, 2), tens, {}, 0, stride=stride)
+    lab, w = O.lab_fill(comp, (1, 1, 1), n, (2, 2, 2), (2, 2, 2), tens, {}, 0, stride=stride, entity=entity)
     f = comp[: int(np.prod(n))].reshape(n[2], n[1], n[0])
     L = LC.Lab(lab, n, (2, 2, 2), (2, 2, 2))
     W = LC.Lab(w, n, (2, 2, 2), (2, 2, 2))
