@@ -210,6 +210,230 @@ __global__ void __launch_bounds__(NTHREADS) conv3_tc_kernel(const __grid_constan
         tc::tmem_dealloc(tbase, TMEM_COLS);
 }
 
+// --------------------------------------------------------------------------
+// Persistent, warp-specialised form: one CTA per SM walks the bricks with a
+// stride of gridDim.x.  Warps 0-1 (producers) stage brick i into one of two
+// A buffers with asynchronous 16-byte copies whose completion arrives on
+// full[b]; warp 2 (one thread) waits for full[b], issues the brick's 270 MMAs
+// into one of two TMEM accumulators (columns 0 / 256) and commits them to
+// empty[b] (A buffer free) and tfull[a] (accumulator ready); warps 4-7
+// (epilogue, one TMEM lane quadrant each) drain accumulator a and arrive on
+// tempty[a].  So staging of brick i+1 and the epilogue of brick i-1 overlap
+// the MMAs of brick i.  Every wait is bounded; a role that gives up records
+// an error word and stops, and the others then give up too.
+constexpr int PIPE_THREADS = 256;
+constexpr int PRODUCERS = 64;                         // warps 0-1
+constexpr int MMA_WARP = 2;
+constexpr int EPI_WARP0 = 4;                          // warps 4-7
+constexpr uint32_t PIPE_TMEM_COLS = 512;              // 2 accumulators x 256 columns
+constexpr size_t PIPE_BAR_OFF = 4 * (size_t)PLANE + 27 * WTAP;
+constexpr size_t PIPE_SMEM = PIPE_BAR_OFF + 9 * 8 + 8 + 2 * 28 * 4;
+
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void named_sync(int id, int count)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+struct BrickPos {
+    int block, ox, oy, oz;
+};
+__device__ __forceinline__ BrickPos brick_pos(const Params &P, int i)
+{
+    const int per = P.bricks[0] * P.bricks[1] * P.bricks[2];
+    BrickPos b;
+    b.block = i / per;
+    int r = i - b.block * per;
+    b.ox = (r % P.bricks[0]) * BX;
+    r /= P.bricks[0];
+    b.oy = (r % P.bricks[1]) * BY;
+    b.oz = (r / P.bricks[1]) * BZ;
+    return b;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(PIPE_THREADS, 1) conv3_tc_pipe(const __grid_constant__ Params P, int nbricks)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *Abuf = smem;                             // [2][2 planes][SROWS][16 B]
+    unsigned char *Bw = smem + 4 * PLANE;                   // [27][2][16][16 B]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + PIPE_BAR_OFF);
+    uint64_t *full = bars, *empty = bars + 2, *tfull = bars + 4, *tempty = bars + 6, *fin = bars + 8;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 9);
+    int *snb = reinterpret_cast<int *>(slot + 2);           // [2][28]: neighbour blocks per A buffer
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cells = P.n[0] * P.n[1] * P.n[2];
+
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(full + b, PRODUCERS);
+            mbar_init(empty + b, 1);
+            mbar_init(tfull + b, 1);
+            mbar_init(tempty + b, 128);
+        }
+        mbar_init(fin, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(slot, PIPE_TMEM_COLS);
+        tc::tmem_relinquish();
+    }
+    // weights once; rows past the region stay zero in both A buffers
+    for (int i = threadIdx.x; i < 27 * 32; i += PIPE_THREADS)
+        reinterpret_cast<uint4 *>(Bw)[i] = __ldg(reinterpret_cast<const uint4 *>(P.w) + i);
+    for (int t = threadIdx.x; t < 4 * (SROWS - RCELLS); t += PIPE_THREADS) {
+        const int b = t / (2 * (SROWS - RCELLS)), r = t % (2 * (SROWS - RCELLS));
+        const int kc = r / (SROWS - RCELLS), u = RCELLS + r % (SROWS - RCELLS);
+        *reinterpret_cast<uint4 *>(Abuf + b * 2 * PLANE + kc * PLANE + u * 16) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *slot;
+
+    if (warp < 2) {
+        // ---------------- producers
+        int k = 0;
+        for (int i = blockIdx.x; i < nbricks; i += gridDim.x, ++k) {
+            const int b = k & 1;
+            int *nbt = snb + 28 * b;
+            // one thread waits for the buffer; the verdict is shared so that
+            // all producers leave together (the named barrier stays matched)
+            if (threadIdx.x == 0)
+                nbt[27] = (k < 2 || mbar_wait_bounded(empty + b, ((k >> 1) - 1) & 1)) ? 1 : 0;
+            named_sync(1, PRODUCERS);
+            if (!nbt[27]) {
+                if (threadIdx.x == 0 && P.err) atomicExch(P.err, kDevErrTimeout);
+                break;
+            }
+            const BrickPos q = brick_pos(P, i);
+            if (threadIdx.x < 27) {
+                const int t = threadIdx.x;
+                int bx = q.block % P.nb[0] + t % 3 - 1, by = (q.block / P.nb[0]) % P.nb[1] + (t / 3) % 3 - 1,
+                    bz = q.block / (P.nb[0] * P.nb[1]) + t / 9 - 1;
+                bx = bx < 0 ? bx + P.nb[0] : (bx >= P.nb[0] ? bx - P.nb[0] : bx);
+                by = by < 0 ? by + P.nb[1] : (by >= P.nb[1] ? by - P.nb[1] : by);
+                bz = bz < 0 ? bz + P.nb[2] : (bz >= P.nb[2] ? bz - P.nb[2] : bz);
+                nbt[t] = bx + P.nb[0] * (by + P.nb[1] * bz);
+            }
+            named_sync(1, PRODUCERS);
+            unsigned char *A = Abuf + b * 2 * PLANE;
+            for (int t = threadIdx.x; t < 2 * RCELLS; t += PRODUCERS) {
+                const int u = t >> 1, kc = t & 1;
+                const int ii = u % RX, jj = (u / RX) % RY, kk = u / (RX * RY);
+                const int x = q.ox + ii - 1, y = q.oy + jj - 1, z = q.oz + kk - 1;
+                const int r0 = x < 0 ? -1 : (x >= P.n[0] ? 1 : 0), r1 = y < 0 ? -1 : (y >= P.n[1] ? 1 : 0),
+                          r2 = z < 0 ? -1 : (z >= P.n[2] ? 1 : 0);
+                const int sb = nbt[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+                const int sc = (x - r0 * P.n[0]) + P.n[0] * ((y - r1 * P.n[1]) + P.n[1] * (z - r2 * P.n[2]));
+                const uint16_t *src = P.act + ((int64_t)sb * cells + sc) * 16 + kc * 8;
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(A + kc * PLANE + u * 16)),
+                             "l"(src)
+                             : "memory");
+            }
+            cp_async_arrive_noinc(full + b);
+            named_sync(1, PRODUCERS); // nbt of this buffer stays untouched until the next use
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else if (warp == MMA_WARP) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            const uint64_t db = tc::smem_desc(smem_u32(Bw), 256u, 128u);
+            int k = 0;
+            bool issued = false;
+            for (int i = blockIdx.x; i < nbricks; i += gridDim.x, ++k) {
+                const int b = k & 1;
+                if (!mbar_wait_bounded(full + b, (k >> 1) & 1) ||
+                    (k >= 2 && !mbar_wait_bounded(tempty + b, ((k >> 1) - 1) & 1))) {
+                    if (P.err) atomicExch(P.err, kDevErrTimeout);
+                    break;
+                }
+                fence_proxy_async_smem(); // the producers' copies -> the tensor cores' view
+                tc::fence_after_sync();
+                const uint64_t da = tc::smem_desc(smem_u32(Abuf + b * 2 * PLANE), PLANE, 128u);
+                const uint32_t acc = tbase + 256u * b;
+#pragma unroll 1
+                for (int t = 0; t < MT; ++t) {
+#pragma unroll
+                    for (int q = 0; q < 27; ++q) {
+                        const int off = (q % 3 - 1) + RX * ((q / 3) % 3 - 1) + RX * RY * (q / 9 - 1);
+                        tc::mma_bf16(acc + 16u * t, da + (uint64_t)(R0 + 128 * t + off),
+                                     db + (uint64_t)(q * (WTAP / 16)), IDESC, q > 0 ? 1u : 0u);
+                    }
+                }
+                tc::mma_commit(empty + b);
+                tc::mma_commit(tfull + b);
+                issued = true;
+            }
+            if (issued) { // everything issued has finished before TMEM is freed
+                tc::mma_commit(fin);
+                if (!mbar_wait_bounded(fin, 0) && P.err) atomicExch(P.err, kDevErrTimeout);
+            }
+        }
+    } else if (warp >= EPI_WARP0) {
+        // ---------------- epilogue
+        const int qd = warp - EPI_WARP0;
+        const uint32_t lane_base = (uint32_t)(32 * qd) << 16;
+        int k = 0;
+        for (int i = blockIdx.x; i < nbricks; i += gridDim.x, ++k) {
+            const int a = k & 1;
+            // warp-uniform verdict: the TMEM loads below are warp-collective
+            const int got = __shfl_sync(0xffffffffu, lane == 0 ? (mbar_wait_bounded(tfull + a, (k >> 1) & 1) ? 1 : 0) : 0, 0);
+            if (!got) {
+                if (lane == 0 && P.err) atomicExch(P.err, kDevErrTimeout);
+                break;
+            }
+            tc::fence_after_sync();
+            const BrickPos q = brick_pos(P, i);
+#pragma unroll 1
+            for (int t = 0; t < MT; ++t) {
+                float v[16];
+                tc::tmem_ld16(tbase + 256u * a + lane_base + 16u * t, v);
+                const int m = 128 * t + 32 * qd + lane;
+                const int z = m / (RX * RY), rem = m - z * (RX * RY);
+                const int y = rem / RX, x = rem - y * RX;
+                if (x >= BX || y >= BY || z >= BZ)
+                    continue;
+                const int c = (q.ox + x) + P.n[0] * ((q.oy + y) + P.n[1] * (q.oz + z));
+                if (MODE == 2) {
+                    const int64_t o = (int64_t)q.block * P.pbs + c;
+                    const float x0 = __ldg(P.x + (int64_t)q.block * P.xbs + c);
+                    const float pv = P.zero_guess ? 0.f : P.p[o];
+                    P.p[o] = pv + (P.omega * x0 + v[0]);
+                } else {
+                    uint32_t h[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        float a0 = v[2 * j], b0 = v[2 * j + 1];
+                        if (P.relu) {
+                            a0 = fmaxf(a0, 0.f);
+                            b0 = fmaxf(b0, 0.f);
+                        }
+                        h[j] = (uint32_t)bf16_bits(a0) | ((uint32_t)bf16_bits(b0) << 16);
+                    }
+                    uint4 *dst = reinterpret_cast<uint4 *>(P.out + ((int64_t)q.block * cells + c) * 16);
+                    dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                    dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+                }
+            }
+            tc::fence_before_sync();
+            mbar_arrive(tempty + a);
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0)
+        tc::tmem_dealloc(tbase, PIPE_TMEM_COLS);
+}
+
 // FP32 weights [27][cin][cout] -> BF16 B tiles [27][kc][co][8] (B[co][ci] = W[tap][ci][co])
 __global__ void pack_weights_kernel(const float *W, int cin, int cout, uint16_t *out)
 {
@@ -223,21 +447,39 @@ __global__ void pack_weights_kernel(const float *W, int cin, int cout, uint16_t 
     out[i] = bf16_bits(v);
 }
 
-static bool attr_set[3]; // per mode (1: hidden layer, 2: last layer + update)
+static bool attr_set[3], pipe_attr_set[3]; // per mode (1: hidden layer, 2: last layer + update)
+// kernel form: 1 = persistent warp-specialised pipeline, 0 = one brick per CTA
+static int g_conv_form = 1;
 
 template <int MODE>
 static cn_status launch(const Params &P, int nblocks, cudaStream_t st)
 {
+    const int64_t bricks = (int64_t)nblocks * P.bricks[0] * P.bricks[1] * P.bricks[2];
+    if (g_conv_form == 1) {
+        if (!pipe_attr_set[MODE]) {
+            CN_CUDA_TRY(cudaFuncSetAttribute(conv3_tc_pipe<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)PIPE_SMEM));
+            pipe_attr_set[MODE] = true;
+        }
+        int dev = 0, sms = 148;
+        CN_CUDA_TRY(cudaGetDevice(&dev));
+        CN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int64_t grid = bricks < sms ? bricks : sms;
+        conv3_tc_pipe<MODE><<<(unsigned)grid, PIPE_THREADS, PIPE_SMEM, st>>>(P, (int)bricks);
+        CN_CUDA_TRY(cudaGetLastError());
+        return CN_OK;
+    }
     if (!attr_set[MODE]) {
         CN_CUDA_TRY(cudaFuncSetAttribute(conv3_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)SMEM));
         attr_set[MODE] = true;
     }
-    const int64_t ctas = (int64_t)nblocks * P.bricks[0] * P.bricks[1] * P.bricks[2];
-    conv3_tc_kernel<MODE><<<(unsigned)ctas, NTHREADS, SMEM, st>>>(P);
+    conv3_tc_kernel<MODE><<<(unsigned)bricks, NTHREADS, SMEM, st>>>(P);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
+
+void set_form(int form) { g_conv_form = form ? 1 : 0; }
 
 bool supported(const int n[3])
 {
