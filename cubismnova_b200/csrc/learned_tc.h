@@ -12,6 +12,8 @@ namespace nntc {
 // bytes of one layer's packed BF16 weights ([27][2][16][8])
 constexpr size_t kPackedWeightBytes = 27 * 512;
 
+// kernel form: 1 (default) persistent warp-specialised pipeline, 0 one brick per CTA
+void set_form(int form);
 // block cells must be multiples of the 16 x 16 x 4 brick
 bool supported(const int n[3]);
 // FP32 [27][cin][cout] -> packed BF16 B tiles (cin, cout <= 16, zero padded)
