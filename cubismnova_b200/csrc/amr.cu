@@ -48,9 +48,10 @@ __global__ void __launch_bounds__(euler::NT, 3) stage_kernel(euler::StageParams<
     T *F = W + 5 * euler::Stg<T>::SV;
     __shared__ double red[euler::NT / 32][5];
     __shared__ int snb[28];
+    __shared__ euler::TileInfo<T> ts;
     // persistent: each CTA walks the work list with a grid stride
     for (int item = blockIdx.x; item < nitems; item += gridDim.x)
-        euler::stage_tile<T>(p, src, item, item, W, F, red, snb);
+        euler::stage_tile<T>(p, src, item, item, W, F, red, snb, &ts);
 }
 
 // dense lab of one block: (n+2g)^3, face ghosts only (non-tensorial)

@@ -36,7 +36,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) stage_kernel(Stage
     T *F = W + 5 * Stg<T>::SV;              // [5][NFACE]
     __shared__ double red[NT / 32][5];
     __shared__ int snb[28];
-    stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, F, red, snb);
+    __shared__ TileInfo<T> ts;
+    stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, F, red, snb, &ts);
 }
 
 // Fixed-order reduction of per-CTA partials: out[c] = sum_i partials[i][c].

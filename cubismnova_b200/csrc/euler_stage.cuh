@@ -265,10 +265,17 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
 // W [5][Stg<T>::SV], F [5][NFACE] and red [NT/32][5] in shared memory.
 template <typename T, typename Src>
 __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &src, int item, int slot, T *W, T *F,
-                                           double (*red)[5], int *snb)
+                                           double (*red)[5], int *snb, TileInfo<T> *ts)
 {
-    TileInfo<T> t;
-    src.template tile<T>(item, t);
+    // the tile's geometry is kept in shared memory (ts) and re-read after each
+    // barrier, so it does not occupy registers across the three sweeps
+    {
+        TileInfo<T> t0;
+        src.template tile<T>(item, t0);
+        if (threadIdx.x == 0) *ts = t0;
+    }
+    __syncthreads();
+    const TileInfo<T> &t = *ts;
     src.template prepare<T>(t, snb);
     __syncthreads(); // snb
     // ---- stage the tile's cells as primitives (the halo slot follows per sweep)
