@@ -356,8 +356,7 @@ struct FeatArgs {
     LabGeom L;
     BcView pbc, kbc;
     const float *p, *k, *f;
-    const float *coef; // level coefficients of the multigrid (component stride ccs)
-    int64_t ccs;
+    const float *coef; // level coefficients of the multigrid, 8 per cell
     float ih2;
     float *x0, *x1, *rout;
     uint16_t *packed;
@@ -366,28 +365,30 @@ struct FeatArgs {
 __global__ void __launch_bounds__(mg::kTileThreads, mg::kTileMinCtas) features_tile(const __grid_constant__ FeatArgs A,
                                                                   const __grid_constant__ mg::Tile T)
 {
-    __shared__ float sp[mg::kRegionMax];
+    __shared__ __align__(16) float sp[mg::kRegionMax];
     __shared__ int snb[27];
     const LabGeom &L = A.L;
-    const mg::TilePos q = mg::tile_pos(T);
+    mg::TilePos q = mg::tile_pos(T);
+    mg::region_layout<float>(q, L);
     mg::neighbour_blocks(L.nb, q.block, snb);
     __syncthreads();
     if (A.p)
         mg::stage_region<float>(A.p, L, A.pbc, q, false, snb, sp);
     else
-        for (int u = threadIdx.x; u < q.ex * q.ey * q.ez; u += mg::kTileThreads) sp[u] = 0.f;
+        for (int u = threadIdx.x; u < q.rs * q.ey * q.ez; u += mg::kTileThreads) sp[u] = 0.f;
     mg::cp_async_wait_all();
     __syncthreads();
     const int cells = T.t[0] * T.t[1] * T.t[2];
     const int64_t bcells = (int64_t)L.n[0] * L.n[1] * L.n[2];
-    const int st[3] = {1, q.ex, q.ex * q.ey};
+    const int st[3] = {1, q.rs, q.rs * q.ey};
     for (int c = threadIdx.x; c < cells; c += mg::kTileThreads) {
         int x, y, z;
         mg::tile_cell(T, c, x, y, z);
         const int64_t lc = (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
         const int64_t o = (int64_t)q.block * L.bstride + lc;
         float Lp, D, pc;
-        mg::op7_coef<float>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, A.coef, A.ccs, o, A.ih2, Lp, D, pc);
+        mg::op7_coef<float, float>(sp, mg::ridx(q, x, y, z), st, A.coef + ((int64_t)q.block * bcells + lc) * mg::kCoefPerCell,
+                                   A.ih2, Lp, D, pc);
         const float fc = __ldg(A.f + o);
         const float r = fc - Lp;
         const float a = (Lp - fc) / D;
@@ -729,8 +730,7 @@ static cn_status features(cn_mg *m, int l, const float *p, const float *f, float
     A.p = p;
     A.k = fptr(m->k[l]);
     A.f = f;
-    A.coef = reinterpret_cast<const float *>(m->coef[l]->d_data);
-    A.ccs = m->coef[l]->comp_stride;
+    A.coef = m->coef[l];
     A.ih2 = (float)(1.0 / (m->p[l]->h[0] * m->p[l]->h[0]));
     A.x0 = reinterpret_cast<float *>(X->d_data);
     A.x1 = A.x0 + X->comp_stride;

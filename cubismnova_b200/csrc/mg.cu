@@ -64,25 +64,30 @@ struct KArgs {
     Geo G;
     BcView kbc;
     const float *k;
-    const float *coef; // level coefficients (7 components, component stride ccs)
-    int64_t ccs;
+    const float *coef; // level coefficients, 8 per cell (see op7_coef)
     float ih2;
     double ih2d;
 };
+
+// dense index of tile cell (x, y, z) in its block
+__device__ __forceinline__ int64_t dense_cell(const LabGeom &L, const TilePos &q, int x, int y, int z)
+{
+    return (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z));
+}
 
 // Coefficients of one level (see op7_coef) in precision TC (float for the
 // V-cycle, double for the outer FP64 residual): k staged per tile with its
 // one-cell halo, then per cell the operations of op7_math in TC.
 template <typename TC>
 __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const __grid_constant__ KArgs a,
-                                                                          const __grid_constant__ Tile T,
-                                                                          const __grid_constant__ LabGeom Lo,
-                                                                          TC ih2, TC *coef, int64_t ccs)
+                                                                          const __grid_constant__ Tile T, TC ih2,
+                                                                          TC *coef)
 {
-    __shared__ float sk[kRegionMax];
+    __shared__ __align__(16) float sk[kRegionMax];
     __shared__ int snb[27];
     const LabGeom &L = a.G.L;
-    const TilePos q = tile_pos(T);
+    TilePos q = tile_pos(T);
+    region_layout<float>(q, a.G.Lk);
     neighbour_blocks(L.nb, q.block, snb);
     __syncthreads();
     stage_region<float>(a.k, a.G.Lk, a.kbc, q, false, snb, sk);
@@ -90,21 +95,23 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const 
     __syncthreads();
     int x, y, z0, zl;
     if (!column_run(T, x, y, z0, zl)) return;
-    const int st[3] = {1, q.ex, q.ex * q.ey};
+    const int st[3] = {1, q.rs, q.rs * q.ey};
+    const int64_t cells = (int64_t)L.n[0] * L.n[1] * L.n[2];
     for (int z = z0; z < z0 + zl; ++z) {
-        const int64_t o = (int64_t)q.block * Lo.bstride + (q.x0 + x) + (int64_t)Lo.n[0] * ((q.y0 + y) + (int64_t)Lo.n[1] * (q.z0 + z));
-        const int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1));
+        TC *cv = coef + ((int64_t)q.block * cells + dense_cell(L, q, x, y, z)) * kCoefPerCell;
+        const int u = ridx(q, x, y, z);
         const TC kc = (TC)sk[u];
         TC sd[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const TC kp = harm<TC>(kc, (TC)sk[u + st[d]]);
             const TC km = harm<TC>((TC)sk[u - st[d]], kc);
-            coef[d * ccs + o] = kp;
-            coef[(3 + d) * ccs + o] = km;
+            cv[d] = kp;
+            cv[3 + d] = km;
             sd[d] = kp + km;
         }
-        coef[6 * ccs + o] = ih2 * ((sd[0] + sd[1]) + sd[2]);
+        cv[6] = ih2 * ((sd[0] + sd[1]) + sd[2]);
+        cv[7] = TC(0);
     }
 }
 
@@ -113,10 +120,11 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) jacobi_kernel(cons
                                                               const __grid_constant__ Tile T, const float *pin,
                                                               const float *f, float *pout, float omega)
 {
-    __shared__ float sp[kRegionMax];
+    __shared__ __align__(16) float sp[kRegionMax];
     __shared__ int snb[27];
     const LabGeom &L = a.G.L;
-    const TilePos q = tile_pos(T);
+    TilePos q = tile_pos(T);
+    region_layout<float>(q, L);
     if (pin) {
         neighbour_blocks(L.nb, q.block, snb);
         __syncthreads();
@@ -126,19 +134,22 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) jacobi_kernel(cons
     }
     int x, y, z0, zl;
     if (!column_run(T, x, y, z0, zl)) return;
-    const int st[3] = {1, q.ex, q.ex * q.ey};
+    const int st[3] = {1, q.rs, q.rs * q.ey};
+    const int64_t cells = (int64_t)L.n[0] * L.n[1] * L.n[2];
     const int64_t oz = (int64_t)L.n[0] * L.n[1];
-    int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z0));
-    int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z0 + 1));
-    for (int k = 0; k < zl; ++k, o += oz, u += st[2]) {
+    int64_t c = dense_cell(L, q, x, y, z0);
+    int u = ridx(q, x, y, z0);
+    for (int k = 0; k < zl; ++k, c += oz, u += st[2]) {
+        const int64_t o = (int64_t)q.block * L.bstride + c;
+        const float *cv = a.coef + ((int64_t)q.block * cells + c) * kCoefPerCell;
         const float fc = __ldg(f + o);
         if (pin) {
             float Lp, D, pc;
-            op7_coef<float, float>(sp, u, st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
+            op7_coef<float, float>(sp, u, st, cv, a.ih2, Lp, D, pc);
             pout[o] = pc + omega * ((Lp - fc) / D);
         } else {
             // zero guess: L 0 = 0, only the diagonal is used
-            const float D = __ldg(a.coef + 6 * a.ccs + o);
+            const float D = __ldg(cv + 6);
             pout[o] = 0.0f + omega * ((0.0f - fc) / D);
         }
     }
@@ -152,11 +163,12 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) resid_restrict_ker
                                                                       const float *p, const float *f,
                                                                       const __grid_constant__ LabGeom Lc, float *fc)
 {
-    __shared__ float sp[kRegionMax];
+    __shared__ __align__(16) float sp[kRegionMax];
     __shared__ float sr[32 * 8 * 4];
     __shared__ int snb[27];
     const LabGeom &L = a.G.L;
-    const TilePos q = tile_pos(T);
+    TilePos q = tile_pos(T);
+    region_layout<float>(q, L);
     neighbour_blocks(L.nb, q.block, snb);
     __syncthreads();
     stage_region<float>(p, L, a.G.bc, q, false, snb, sp);
@@ -165,15 +177,17 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) resid_restrict_ker
     {
         int x, y, z0, zl;
         if (column_run(T, x, y, z0, zl)) {
-            const int st[3] = {1, q.ex, q.ex * q.ey};
+            const int st[3] = {1, q.rs, q.rs * q.ey};
+            const int64_t cells = (int64_t)L.n[0] * L.n[1] * L.n[2];
             const int64_t oz = (int64_t)L.n[0] * L.n[1];
-            int64_t o = (int64_t)q.block * L.bstride + (q.x0 + x) + (int64_t)L.n[0] * ((q.y0 + y) + (int64_t)L.n[1] * (q.z0 + z0));
-            int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z0 + 1));
-            int c = x + T.t[0] * (y + T.t[1] * z0);
-            for (int k = 0; k < zl; ++k, o += oz, u += st[2], c += T.t[0] * T.t[1]) {
+            int64_t c = dense_cell(L, q, x, y, z0);
+            int u = ridx(q, x, y, z0);
+            int ct = x + T.t[0] * (y + T.t[1] * z0);
+            for (int k = 0; k < zl; ++k, c += oz, u += st[2], ct += T.t[0] * T.t[1]) {
                 float Lp, D, pc;
-                op7_coef<float, float>(sp, u, st, a.coef, a.ccs, o, a.ih2, Lp, D, pc);
-                sr[c] = __ldg(f + o) - Lp;
+                op7_coef<float, float>(sp, u, st, a.coef + ((int64_t)q.block * cells + c) * kCoefPerCell, a.ih2, Lp,
+                                       D, pc);
+                sr[ct] = __ldg(f + (int64_t)q.block * L.bstride + c) - Lp;
             }
         }
     }
@@ -221,7 +235,7 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(con
                                                                const __grid_constant__ LabGeom Lct,
                                                                const __grid_constant__ BcView cbc, const float *e)
 {
-    __shared__ float se[(16 + 2) * (4 + 2) * (2 + 2)];
+    __shared__ __align__(16) float se[(16 + 8) * (4 + 2) * (2 + 2)];
     __shared__ int snb[27];
     const TilePos qf = tile_pos(T);
     neighbour_blocks(Lct.nb, qf.block, snb);
@@ -233,6 +247,9 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(con
     qc.ex = T.t[0] / 2 + 2;
     qc.ey = T.t[1] / 2 + 2;
     qc.ez = T.t[2] / 2 + 2;
+    qc.xo = 1;
+    qc.rs = qc.ex;
+    region_layout<float>(qc, Lct);
     stage_region<float>(e, Lct, cbc, qc, true, snb, se);
     cp_async_wait_all();
     __syncthreads();
@@ -242,8 +259,8 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(con
         tile_cell(T, c, x, y, z);
         const int X = x >> 1, Y = y >> 1, Z = z >> 1;
         const int sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1, sz = (z & 1) ? 1 : -1;
-        const int u = (X + 1) + qc.ex * ((Y + 1) + qc.ey * (Z + 1));
-        const int ox = sx, oy = sy * qc.ex, oz = sz * qc.ex * qc.ey;
+        const int u = ridx(qc, X, Y, Z);
+        const int ox = sx, oy = sy * qc.rs, oz = sz * qc.rs * qc.ey;
         const float v0 = se[u], v1 = se[u + ox], v2 = se[u + oy], v3 = se[u + ox + oy];
         const float v4 = se[u + oz], v5 = se[u + ox + oz], v6 = se[u + oy + oz], v7 = se[u + ox + oy + oz];
         const float a0 = 0.75f * v0 + 0.25f * v1;
@@ -263,13 +280,14 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(con
 __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_constant__ KArgs a,
                                                                const __grid_constant__ Tile T, const double *p64,
                                                                const float *f, float *r32, double *partials,
-                                                               const double *coef64, int64_t c64s)
+                                                               const double *coef64)
 {
-    __shared__ double sp[kRegionMax];
+    __shared__ __align__(16) double sp[kRegionMax];
     __shared__ double sh[2][kTileThreads / 32];
     __shared__ int snb[27];
     const LabGeom &L = a.G.L, &Lk = a.G.Lk;
-    const TilePos q = tile_pos(T);
+    TilePos q = tile_pos(T);
+    region_layout<double>(q, L);
     neighbour_blocks(L.nb, q.block, snb);
     __syncthreads();
     stage_region<double>(p64, L, a.G.bc, q, false, snb, sp);
@@ -278,14 +296,14 @@ __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_c
     double rr = 0, ff = 0;
     int x, y, z0, zl;
     if (column_run(T, x, y, z0, zl)) {
-        const int st[3] = {1, q.ex, q.ex * q.ey};
+        const int st[3] = {1, q.rs, q.rs * q.ey};
+        const int64_t cells = (int64_t)Lk.n[0] * Lk.n[1] * Lk.n[2];
         for (int z = z0; z < z0 + zl; ++z) {
-            const int64_t cell = (q.x0 + x) + (int64_t)Lk.n[0] * ((q.y0 + y) + (int64_t)Lk.n[1] * (q.z0 + z));
-            const int64_t o = (int64_t)q.block * Lk.bstride + cell;   // FP32 fields (f, r32)
-            const int64_t o64 = (int64_t)q.block * L.bstride + cell;  // FP64 fields (coefficients)
+            const int64_t cell = dense_cell(Lk, q, x, y, z);
+            const int64_t o = (int64_t)q.block * Lk.bstride + cell; // FP32 fields (f, r32)
             double Lp, D, pc;
-            op7_coef<double, double>(sp, (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1)), st, coef64, c64s, o64, a.ih2d, Lp,
-                             D, pc);
+            op7_coef<double, double>(sp, ridx(q, x, y, z), st, coef64 + ((int64_t)q.block * cells + cell) * kCoefPerCell,
+                                     a.ih2d, Lp, D, pc);
             const double fc = (double)__ldg(f + o);
             const double r = fc - Lp;
             if (r32) r32[o] = (float)r;
@@ -499,8 +517,7 @@ KArgs kargs(cn_mg *m, int l)
     a.G.nblocks = m->p[l]->nblocks;
     a.kbc = bc_view(m->k[l], 0);
     a.k = reinterpret_cast<const float *>(m->k[l]->d_data);
-    a.coef = (int)m->coef.size() > l && m->coef[l] ? reinterpret_cast<const float *>(m->coef[l]->d_data) : nullptr;
-    a.ccs = (int)m->coef.size() > l && m->coef[l] ? m->coef[l]->comp_stride : 0;
+    a.coef = (int)m->coef.size() > l ? m->coef[l] : nullptr;
     a.ih2d = 1.0 / (m->p[l]->h[0] * m->p[l]->h[0]);
     a.ih2 = (float)a.ih2d;
     return a;
@@ -652,30 +669,30 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
     }
     if (s == CN_OK) s = sync_bc(m->p[0], nullptr);
     if (s == CN_OK) s = sync_bc(k, nullptr);
-    // operator coefficients of every level (k is fixed from here on)
+    // operator coefficients of every level (k is fixed from here on): 8 per
+    // cell, FP32 for the V-cycle levels and FP64 for the finest level
     for (int l = 0; l < levels && s == CN_OK; ++l) {
-        cn_grid *c = nullptr;
-        s = cn_grid_create(k->nb, m->p[l]->n, 7, CN_FLOAT32, b0, e0, &c);
-        m->coef.push_back(c);
-        if (s != CN_OK) break;
-        if (c->block_stride != m->p[l]->block_stride) {
-            s = fail(CN_ERR_UNSUPPORTED, "cn_mg_create: coefficient layout");
+        const int64_t cells = (int64_t)k->nblocks * m->p[l]->n[0] * m->p[l]->n[1] * m->p[l]->n[2];
+        float *c = nullptr;
+        if (cudaMalloc(&c, sizeof(float) * kCoefPerCell * cells) != cudaSuccess) {
+            s = fail(CN_ERR_OUT_OF_MEMORY, "cn_mg_create: coefficients");
             break;
         }
+        m->coef.push_back(c);
         const KArgs a = kargs(m, l);
         const Tile T = tile_of(m->p[l]->n);
-        coef_kernel<float><<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads>>>(a, T, a.G.L, a.ih2, fptr(c),
-                                                                                      c->comp_stride);
+        coef_kernel<float><<<(unsigned)(m->p[l]->nblocks * T.count), kTileThreads>>>(a, T, a.ih2, c);
         if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
     }
-    // FP64 coefficients of the finest level for the outer residual
-    if (s == CN_OK) s = cn_grid_create(k->nb, k->n, 7, CN_FLOAT64, b0, e0, &m->coef64);
+    if (s == CN_OK) {
+        const int64_t cells = (int64_t)k->nblocks * k->n[0] * k->n[1] * k->n[2];
+        if (cudaMalloc(&m->coef64, sizeof(double) * kCoefPerCell * cells) != cudaSuccess)
+            s = fail(CN_ERR_OUT_OF_MEMORY, "cn_mg_create: coefficients");
+    }
     if (s == CN_OK) {
         const KArgs a = kargs(m, 0);
         const Tile T = tile_of(k->n);
-        const LabGeom L64 = make_geom(m->coef64, &kS1);
-        coef_kernel<double><<<(unsigned)(k->nblocks * T.count), kTileThreads>>>(
-            a, T, L64, a.ih2d, reinterpret_cast<double *>(m->coef64->d_data), m->coef64->comp_stride);
+        coef_kernel<double><<<(unsigned)(k->nblocks * T.count), kTileThreads>>>(a, T, a.ih2d, m->coef64);
         if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
     }
     if (s == CN_OK && cudaDeviceSynchronize() != cudaSuccess) s = fail(CN_ERR_CUDA, "cn_mg_create");
@@ -698,8 +715,9 @@ cn_status cn_mg_destroy(cn_mg *m)
         if (l > 0) cn_grid_destroy(m->k[l]);
     }
     cn_grid_destroy(m->r32);
-    for (cn_grid *g : m->coef) cn_grid_destroy(g);
-    cn_grid_destroy(m->coef64);
+    for (float *c : m->coef)
+        if (c) cudaFree(c);
+    if (m->coef64) cudaFree(m->coef64);
     for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
     for (void *a : m->nn_act)
         if (a) cudaFree(a);
@@ -754,12 +772,9 @@ cn_status cn_mg_residual(cn_mg *m, const cn_grid *p64, const cn_grid *f, cn_grid
     KArgs a = kargs(m, 0);
     a.G.L.bstride = p64->block_stride;
     a.G.bc = bc_view(p64, 0);
-    if (p64->block_stride != m->coef64->block_stride)
-        return fail(CN_ERR_SIZE_MISMATCH, "Cartesian: Can not assign two grids of unequal size.");
     resid64_kernel<<<m->nparts, kTileThreads, 0, st>>>(
         a, tile_of(p64->n), reinterpret_cast<const double *>(p64->d_data), reinterpret_cast<const float *>(f->d_data),
-        r32 ? fptr(r32) : nullptr, m->partials, reinterpret_cast<const double *>(m->coef64->d_data),
-        m->coef64->comp_stride);
+        r32 ? fptr(r32) : nullptr, m->partials, m->coef64);
     CN_CUDA_TRY(cudaGetLastError());
     sum_pairs_kernel<<<1, 256, 0, st>>>(m->partials, m->nparts, m->sums);
     CN_CUDA_TRY(cudaGetLastError());

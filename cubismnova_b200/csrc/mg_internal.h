@@ -12,8 +12,8 @@ struct cn_mg {
     int nu1, nu2;
     double omega;
     std::vector<cn_grid *> p, pt, f, k; // per level (FP32); k[0] is the caller's grid
-    std::vector<cn_grid *> coef;        // per level (FP32, 7 comps): k+ faces x,y,z, k- faces x,y,z, D
-    cn_grid *coef64 = nullptr;          // the same for the finest level in FP64 (outer residual)
+    std::vector<float *> coef;          // per level: 8 FP32 per cell (k+ faces x,y,z, k- faces x,y,z, D, 0)
+    double *coef64 = nullptr;           // the same for the finest level in FP64 (outer residual)
     cn_grid *r32 = nullptr;             // finest FP32 residual
     double *partials = nullptr;
     double *sums = nullptr;

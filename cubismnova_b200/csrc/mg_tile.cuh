@@ -37,24 +37,46 @@ __device__ __forceinline__ void op7_math(const TP (&v)[14], TP ih2, TP &Lp, TP &
 }
 
 // Operator coefficients of a level, precomputed once from k (they depend on
-// k only): per cell the harmonic face means kp_d = harm(k, k(+e_d)) and
-// km_d = harm(k(-e_d), k) (neighbours through the lab) and the diagonal
-// D = ih2 ((s0 + s1) + s2), s_d = kp_d + km_d: components 0-2 kp, 3-5 km,
-// 6 D of an FP32 grid laid out like p.  Evaluated with the same operations
-// as op7_math, so L p and D come out bit for bit the same.
-template <typename TP, typename TC>
-__device__ __forceinline__ void op7_coef(const TP *sp, int u, const int (&st)[3], const TC *coef, int64_t ccs,
-                                         int64_t o, TP ih2, TP &Lp, TP &D, TP &pc)
+// k only): per cell 8 contiguous values, the harmonic face means
+// kp_d = harm(k, k(+e_d)) (d = x, y, z), km_d = harm(k(-e_d), k) (neighbours
+// through the lab), the diagonal D = ih2 ((s0 + s1) + s2) with
+// s_d = kp_d + km_d, and a zero pad, so one cell's set is two (FP32) or four
+// (FP64) 16-byte loads.  Cell (block b, dense in-block index c) at
+// (b cells_per_block + c) * 8.  Evaluated with the same operations as
+// op7_math, so L p and D come out bit for bit the same.
+constexpr int kCoefPerCell = 8;
+
+template <typename TC> __device__ __forceinline__ void load_coef8(const TC *cv, TC (&c)[8])
 {
+    if constexpr (sizeof(TC) == 4) {
+        const float4 a = __ldg(reinterpret_cast<const float4 *>(cv)), b = __ldg(reinterpret_cast<const float4 *>(cv) + 1);
+        c[0] = a.x; c[1] = a.y; c[2] = a.z; c[3] = a.w;
+        c[4] = b.x; c[5] = b.y; c[6] = b.z; c[7] = b.w;
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const double2 v = __ldg(reinterpret_cast<const double2 *>(cv) + i);
+            c[2 * i] = v.x;
+            c[2 * i + 1] = v.y;
+        }
+    }
+}
+
+template <typename TP, typename TC>
+__device__ __forceinline__ void op7_coef(const TP *sp, int u, const int (&st)[3], const TC *cv, TP ih2, TP &Lp,
+                                         TP &D, TP &pc)
+{
+    TC c[8];
+    load_coef8<TC>(cv, c);
     pc = sp[u];
     TP f[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const TP kp = (TP)__ldg(coef + d * ccs + o), km = (TP)__ldg(coef + (3 + d) * ccs + o);
+        const TP kp = (TP)c[d], km = (TP)c[3 + d];
         f[d] = kp * (sp[u + st[d]] - pc) - km * (pc - sp[u - st[d]]);
     }
     Lp = ih2 * ((f[0] + f[1]) + f[2]);
-    D = (TP)__ldg(coef + 6 * ccs + o);
+    D = (TP)c[6];
 }
 
 // ---------------------------------------------------------------- tiles
@@ -74,7 +96,9 @@ struct Tile {
 };
 
 constexpr int kTileCap[3] = {32, 8, 4};
-constexpr int kRegionMax = (32 + 2) * (8 + 2) * (4 + 2); // 2040
+// staged region: tile + one-cell halo; rows padded to t0 + 8 entries so that
+// the in-block part of a row starts 16-byte aligned (vector staging)
+constexpr int kRegionMax = (32 + 8) * (8 + 2) * (4 + 2); // 2400
 constexpr int kTileThreads = 256;
 constexpr int kTileMinCtas = 4; // resident CTAs per SM the tile kernels are compiled for (<= 64 registers)
 
@@ -146,7 +170,14 @@ __device__ __forceinline__ void tile_cell(const Tile &T, int c, int &x, int &y, 
 struct TilePos {
     int block, x0, y0, z0;
     int ex, ey, ez; // staged region extents (tile + 2)
+    int xo, rs;     // region row: position of cell x = 0, row stride
 };
+
+// region index of tile-local cell (x, y, z), x in [-1, t0], y, z in [-1, t]
+__device__ __forceinline__ int ridx(const TilePos &q, int x, int y, int z)
+{
+    return (x + q.xo) + q.rs * ((y + 1) + q.ey * (z + 1));
+}
 
 __device__ __forceinline__ TilePos tile_pos(const Tile &T)
 {
@@ -160,7 +191,21 @@ __device__ __forceinline__ TilePos tile_pos(const Tile &T)
     q.ex = T.t[0] + 2;
     q.ey = T.t[1] + 2;
     q.ez = T.t[2] + 2;
+    q.xo = 1;
+    q.rs = q.ex;
     return q;
+}
+
+// Vector layout for a field of T on geometry L when the tile's rows allow it:
+// in-block row segments start 16-byte aligned in global and shared memory.
+template <typename T> __device__ __forceinline__ void region_layout(TilePos &q, const LabGeom &L)
+{
+    constexpr int V = 16 / (int)sizeof(T);
+    const int t0 = q.ex - 2;
+    if (t0 % V == 0 && L.n[0] % V == 0 && L.bstride % V == 0 && q.x0 % V == 0) {
+        q.xo = V;
+        q.rs = t0 + 2 * V;
+    }
 }
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
@@ -180,44 +225,80 @@ __device__ __forceinline__ void neighbour_blocks(const int nb[3], int b, int *sn
     }
 }
 
-// Stage one field over the region, one warp per region row.  Cells inside
-// the block, and outside it in blocks without BCs or skip flags (the
-// periodic neighbour, from the table snb of neighbour_blocks), are
-// asynchronous 4- or 8-byte copies, many in flight per thread; cells of
-// blocks with BCs resolve through the lab (cn::lab_fetch_slow).  Edge and
-// corner cells of the region are zero unless tensorial (the 7-point operator
-// does not read them).  The caller waits with cp_async_wait_all() and a
-// barrier.
+// Stage one field over the region.  Cells inside the block, and outside it
+// in blocks without BCs or skip flags (the periodic neighbour, from the
+// table snb of neighbour_blocks), are asynchronous copies: 16-byte chunks of
+// the in-block row segments in the vector layout (region_layout), single
+// cells otherwise; cells of blocks with BCs resolve through the lab
+// (cn::lab_fetch_slow).  Edge and corner cells of the region are zero unless
+// tensorial (the 7-point operator does not read them).  The caller waits with
+// cp_async_wait_all() and a barrier.
+template <typename T>
+__device__ __forceinline__ void stage_cell(const T *comp, const LabGeom &L, const BcView &bc, const TilePos &q,
+                                           bool tensorial, const int *snb, bool plain, int x, int y, int z, T *dst)
+{
+    const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0), r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0),
+              r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+    const int outside = (r0 != 0) + (r1 != 0) + (r2 != 0);
+    if (!tensorial && outside > 1) {
+        *dst = T(0);
+    } else if (outside == 0 || plain) {
+        const int sb = outside == 0 ? q.block : snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+        const T *src = comp + (int64_t)sb * L.bstride + (x - r0 * L.n[0]) +
+                       (int64_t)L.n[0] * ((y - r1 * L.n[1]) + (int64_t)L.n[1] * (z - r2 * L.n[2]));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"((int)sizeof(T))
+                     : "memory");
+    } else {
+        *dst = lab_fetch_slow<T>(comp, L, bc, q.block, x, y, z);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void stage_region(const T *comp, const LabGeom &L, const BcView &bc, const TilePos &q,
                                              bool tensorial, const int *snb, T *s)
 {
     static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte cells");
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int V = 16 / (int)sizeof(T);
     const int rows = q.ey * q.ez;
     const bool plain = __ldg(bc.mode + q.block) == 0;
-    for (int r = warp; r < rows; r += kTileThreads / 32) {
-        const int j = r % q.ey, k = r / q.ey;
-        const int y = q.y0 + j - 1, z = q.z0 + k - 1;
-        const int r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0), r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
-        const int yl = y - r1 * L.n[1], zl = z - r2 * L.n[2];
-        for (int i = lane; i < q.ex; i += 32) {
-            const int x = q.x0 + i - 1;
-            const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0);
-            const int outside = (r0 != 0) + (r1 != 0) + (r2 != 0);
-            T *dst = s + i + q.ex * r;
-            if (!tensorial && outside > 1) {
-                *dst = T(0);
-            } else if (outside == 0 || plain) {
-                const int sb = outside == 0 ? q.block : snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
-                const T *src = comp + (int64_t)sb * L.bstride + (x - r0 * L.n[0]) +
-                               (int64_t)L.n[0] * (yl + (int64_t)L.n[1] * zl);
-                asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
-                             "n"((int)sizeof(T))
-                             : "memory");
+    const int t0 = q.ex - 2;
+    if (q.xo == V) {
+        // per row: t0 / V in-block 16-byte chunks and the two x-halo cells
+        const int per = t0 / V + 2;
+        for (int it = threadIdx.x; it < rows * per; it += kTileThreads) {
+            const int r = it / per, k = it - r * per;
+            const int j = r % q.ey, kz = r / q.ey;
+            const int y = q.y0 + j - 1, z = q.z0 + kz - 1;
+            T *row = s + q.rs * r;
+            if (k < per - 2) {
+                const int x = q.x0 + k * V;
+                const int r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0), r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+                const int outside = (r1 != 0) + (r2 != 0);
+                T *dst = row + q.xo + k * V;
+                if (!tensorial && outside > 1) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) dst[v] = T(0);
+                } else if (outside == 0 || plain) {
+                    const int sb = outside == 0 ? q.block : snb[1 + 3 * (r1 + 1) + 9 * (r2 + 1)]; // r0 = 0
+                    const T *src = comp + (int64_t)sb * L.bstride + x +
+                                   (int64_t)L.n[0] * ((y - r1 * L.n[1]) + (int64_t)L.n[1] * (z - r2 * L.n[2]));
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) dst[v] = lab_fetch_slow<T>(comp, L, bc, q.block, x + v, y, z);
+                }
             } else {
-                *dst = lab_fetch_slow<T>(comp, L, bc, q.block, x, y, z);
+                const int xl = k == per - 2 ? -1 : t0; // tile-local x of the halo cell
+                stage_cell<T>(comp, L, bc, q, tensorial, snb, plain, q.x0 + xl, y, z, row + q.xo + xl);
             }
+        }
+    } else {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int r = warp; r < rows; r += kTileThreads / 32) {
+            const int j = r % q.ey, kz = r / q.ey;
+            const int y = q.y0 + j - 1, z = q.z0 + kz - 1;
+            for (int i = lane; i < q.ex; i += 32)
+                stage_cell<T>(comp, L, bc, q, tensorial, snb, plain, q.x0 + i - 1, y, z, s + (i - 1 + q.xo) + q.rs * r);
         }
     }
 }
@@ -227,8 +308,8 @@ template <typename TP>
 __device__ __forceinline__ void region7(const TP *sp, const float *sk, const TilePos &q, int x, int y, int z,
                                         TP (&v)[14])
 {
-    const int u = (x + 1) + q.ex * ((y + 1) + q.ey * (z + 1));
-    const int st[3] = {1, q.ex, q.ex * q.ey};
+    const int u = ridx(q, x, y, z);
+    const int st[3] = {1, q.rs, q.rs * q.ey};
     v[0] = sp[u];
     v[1] = (TP)sk[u];
 #pragma unroll
