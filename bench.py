@@ -207,6 +207,13 @@ class C1:
 
     launches_per_step = 1
     bytes_per_cell_step = 40
+    # DRAM bytes per cell per step from one ncu capture (dram__bytes_read.sum +
+    # dram__bytes_write.sum, mean of 3 launches) of this workload: the field
+    # (16.8 MB) is read from DRAM, the 67 MB of results mostly stay dirty in the
+    # 126 MB L2 and are written back during the flush that follows
+    traffic_per_cell_step = 11.12
+    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of fd_kernel on this workload, "
+                      "mean of 3 launches; results stay dirty in L2 and are written back during the flush")
 
     def e2e_step(self, stream):
         import ctypes as C
@@ -302,6 +309,12 @@ class Euler:
     stages = 3
     launches_per_step = 3
     bytes_per_cell_step = 80 + 120 + 120  # stage 1 reads U, writes U1; stages 2, 3 also read U^n
+    # DRAM bytes per cell per step of the three stage launches from one ncu
+    # capture on 8x8x4 blocks of 32^3 (8.4 M cells, inputs 5x larger than L2),
+    # scaled to the workload's cells: traffic grows with the cells processed
+    traffic_per_cell_step = 329.15
+    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 3 stage_kernel launches "
+                      "of one step on 8x8x4 blocks of 32^3, per cell, scaled by the workload's cells")
     sample_nb = (4, 4, 4)  # CPU sample grid: 64 blocks of the same block size
 
     def __init__(self):
@@ -410,6 +423,9 @@ class C4(Euler):
     nb, n = (32, 32, 32), (32, 32, 32)
     dtype = "f32"
     bytes_per_cell_step = (80 + 120 + 120) // 2
+    # capture on 8x8x4 blocks (168 MB of state, comparable to L2, so slightly
+    # under the full-size figure)
+    traffic_per_cell_step = 157.09
 
 
 class C3:
@@ -719,7 +735,10 @@ def run_ours(args, world, rank, local, pg):
     bytes_per_launch = W.bytes_per_cell_step * W.cells / L
     achieved = bytes_per_launch / avg_launch_s / 1e9
     roof = dict(bound="hbm", achieved=round(achieved, 1), peak=peaks["hbm_gbs"], unit="GB/s",
-                frac=round(achieved / peaks["hbm_gbs"], 4), traffic=args.traffic,
+                frac=round(achieved / peaks["hbm_gbs"], 4),
+                traffic=(args.traffic if args.traffic is not None else
+                         int(W.traffic_per_cell_step * W.cells / L) if getattr(W, "traffic_per_cell_step", None)
+                         else None),
                 peak_source=peaks["src"] + " (MEASURED_PEAKS.json hbm_gbs)" if peaks["src"] == "measured"
                 else "fallback 6.65 TB/s",
                 algorithmic_bytes_per_launch=int(bytes_per_launch),
@@ -727,6 +746,8 @@ def run_ours(args, world, rank, local, pg):
                 launch_ms_mean=[round(float(x), 4) for x in launch_ms.mean(0)])
     if getattr(W, "roofline_scope", None):
         roof["scope"] = W.roofline_scope
+    if args.traffic is None and getattr(W, "traffic_per_cell_step", None):
+        roof["traffic_source"] = W.traffic_source
     flops = getattr(W, "flops_per_cell_stage", None)
     if flops:
         dt_code = _lib.CN_FLOAT64 if W.dtype == "f64" else _lib.CN_FLOAT32
