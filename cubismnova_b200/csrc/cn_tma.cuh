@@ -81,4 +81,33 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
+// try_wait with a suspend-time hint: while the phase is incomplete the thread
+// is suspended for up to `ns` nanoseconds (waking early when the phase
+// completes) instead of returning at once, so a whole CTA waiting for a
+// bulk copy takes no issue slots from the warps of other CTAs on the SM.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+                 : "memory");
+    return done != 0;
+}
+
+constexpr uint32_t kSleepWaitLimit = 1u << 20; // x up to 2 us: about 2 s at most
+
+// Bounded sleeping wait; returns false (barrier left pending) on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t *bar, uint32_t parity, uint32_t ns = 2000)
+{
+    for (uint32_t i = 0; i < kSleepWaitLimit; ++i) {
+        if (mbar_try_wait_sleep(bar, parity, ns)) {
+            return true;
+        }
+    }
+    return false;
+}
+
 } // namespace cn

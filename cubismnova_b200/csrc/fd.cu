@@ -14,6 +14,9 @@
 // an FMA: results are bit-identical to the reference loops compiled without
 // contraction (Kernel/Laplacian/Laplacian.cpp:123-130,
 // Kernel/Divergence/nova/nova.cpp:113-126, ISPC .../ddxGold.cpp:9-33).
+#include <algorithm>
+
+#include "cn_fastdiv.h"
 #include "cn_internal.h"
 #include "cn_tma.cuh"
 
@@ -44,6 +47,7 @@ template <typename T> struct FdParams {
     int TZ;
     int use_bulk;
     int *err;
+    FastDiv dv0, dv1, dv01, dvh; // N0, N1, N0 * N1, N0 / 2: cell index -> (x, y, z) without divisions
 };
 
 // Shared-memory tile of one component: inner cells + the six faces.
@@ -51,10 +55,14 @@ template <typename T> struct Tile {
     T *in, *xlo, *xhi, *ylo, *yhi, *zlo, *zhi;
 };
 
-template <typename T>
-__device__ __forceinline__ size_t tile_elems(int N0, int N1, int TZ)
+// Every array of a tile starts on a multiple of 4 elements, so each one (and
+// the next component's tile) is 16-byte aligned for the bulk copy and the
+// two-element vector loads.
+__host__ __device__ __forceinline__ size_t pad4(size_t n) { return (n + 3) & ~(size_t)3; }
+
+__host__ __device__ __forceinline__ size_t tile_elems(int N0, int N1, int TZ)
 {
-    return (size_t)N0 * N1 * TZ + 2 * ((size_t)N1 * TZ + (size_t)N0 * TZ + (size_t)N0 * N1);
+    return pad4((size_t)N0 * N1 * TZ) + 2 * (pad4((size_t)N1 * TZ) + pad4((size_t)N0 * TZ) + pad4((size_t)N0 * N1));
 }
 
 template <typename T>
@@ -62,42 +70,86 @@ __device__ __forceinline__ Tile<T> carve(T *base, int N0, int N1, int TZ)
 {
     Tile<T> t;
     t.in = base;
-    t.xlo = t.in + (size_t)N0 * N1 * TZ;
-    t.xhi = t.xlo + (size_t)N1 * TZ;
-    t.ylo = t.xhi + (size_t)N1 * TZ;
-    t.yhi = t.ylo + (size_t)N0 * TZ;
-    t.zlo = t.yhi + (size_t)N0 * TZ;
-    t.zhi = t.zlo + (size_t)N0 * N1;
+    t.xlo = t.in + pad4((size_t)N0 * N1 * TZ);
+    t.xhi = t.xlo + pad4((size_t)N1 * TZ);
+    t.ylo = t.xhi + pad4((size_t)N1 * TZ);
+    t.yhi = t.ylo + pad4((size_t)N0 * TZ);
+    t.zlo = t.yhi + pad4((size_t)N0 * TZ);
+    t.zhi = t.zlo + pad4((size_t)N0 * N1);
     return t;
 }
 
-// Gathers the faces selected by mask (bit 0: x, 1: y, 2: z) of the tile that
-// starts at z0.  Blocks without BCs or skip flags (lab mode byte 0) read the
-// periodic neighbour blocks from the table snb (index (r0+1) + 3 (r1+1) +
-// 9 (r2+1)) with plain loads; the others resolve every face cell with
-// cn::lab_value.  Undefined lab cells (never read by these stencils unless
-// the BC set-up leaves a face undefined) are set to zero.
-template <typename T>
-__device__ __forceinline__ T face_value(const T *comp, const LabGeom &L, const BcView &bc, bool plain,
-                                        const int *snb, int block, int bx, int by, int bz, int x, int y, int z)
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+// Outputs of one cell from its six neighbours (kDiv: x neighbours of the
+// first component, y of the second, z of the third; c0 unused).
+template <typename T, int OP>
+__device__ __forceinline__ void cell_eval(const FdParams<T> &p, T c0, T xp, T xm, T yp, T ym, T zp, T zm,
+                                          T &lap, T &g0, T &g1, T &g2)
 {
-    if (plain) {
-        const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0), r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0),
-                  r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+    using A = Arith<T>;
+    if (OP == kDiv) {
+        const T t0 = A::mul(A::sub(xp, xm), p.ih[0]);
+        const T t1 = A::mul(A::sub(yp, ym), p.ih[1]);
+        const T t2 = A::mul(A::sub(zp, zm), p.ih[2]);
+        lap = A::mul(T(0.5), A::add(A::add(t0, t1), t2));
+        return;
+    }
+    if (OP == kLap || OP == kLapGrad) {
+        const T c2 = A::mul(T(2), c0);
+        const T ddx = A::mul(p.ih2[0], A::add(A::sub(xp, c2), xm));
+        const T ddy = A::mul(p.ih2[1], A::add(A::sub(yp, c2), ym));
+        const T ddz = A::mul(p.ih2[2], A::add(A::sub(zp, c2), zm));
+        lap = A::add(A::add(ddx, ddy), ddz);
+    }
+    if (OP == kGrad || OP == kLapGrad) {
+        g0 = A::mul(T(0.5), A::mul(A::sub(xp, xm), p.ih[0]));
+        g1 = A::mul(T(0.5), A::mul(A::sub(yp, ym), p.ih[1]));
+        g2 = A::mul(T(0.5), A::mul(A::sub(zp, zm), p.ih[2]));
+    }
+}
+
+// Stages one lab cell of a tile face into shared memory.  Cells inside the
+// block, and every cell of a block without BCs or skip flags (lab mode byte
+// 0: the periodic neighbour from the table snb, index (r0+1) + 3 (r1+1) +
+// 9 (r2+1)), are asynchronous copies (cp.async), so all of a thread's face
+// loads are in flight at once alongside the bulk copy of the interior; the
+// others are resolved with cn::lab_value.  Undefined lab cells (never read by
+// these stencils unless the BC set-up leaves a face undefined) are zero.
+template <typename T>
+__device__ __forceinline__ void face_cell(const T *comp, const LabGeom &L, const BcView &bc, bool plain,
+                                          const int *snb, int block, int bx, int by, int bz, int x, int y, int z,
+                                          T *dst)
+{
+    const int r0 = x < 0 ? -1 : (x >= L.n[0] ? 1 : 0), r1 = y < 0 ? -1 : (y >= L.n[1] ? 1 : 0),
+              r2 = z < 0 ? -1 : (z >= L.n[2] ? 1 : 0);
+    if (plain || (r0 | r1 | r2) == 0) {
         const int sb = snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
-        return __ldg(comp + (int64_t)sb * L.bstride + (x - r0 * L.n[0]) +
-                     (int64_t)L.n[0] * ((y - r1 * L.n[1]) + (int64_t)L.n[1] * (z - r2 * L.n[2])));
+        const T *src = comp + (int64_t)sb * L.bstride + (x - r0 * L.n[0]) +
+                       (int64_t)L.n[0] * ((y - r1 * L.n[1]) + (int64_t)L.n[1] * (z - r2 * L.n[2]));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src),
+                     "n"((int)sizeof(T))
+                     : "memory");
+        return;
     }
     T v;
     if (!lab_value<T>(comp, L, bc, block, bx, by, bz, x, y, z, true, v))
         v = T(0);
-    return v;
+    *dst = v;
 }
 
+__device__ __forceinline__ void fd_cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Gathers the faces selected by mask (bit 0: x, 1: y, 2: z) of the tile that
+// starts at z0; the caller waits for the copies (fd_cp_async_wait_all) and
+// synchronises the CTA before reading them.
 template <typename T>
 __device__ __forceinline__ void gather_faces(const T *comp, const LabGeom &L, const BcView &bc,
                                              int block, int bx, int by, int bz, int z0, int TZ,
-                                             const Tile<T> &t, unsigned mask, const int *snb)
+                                             const Tile<T> &t, unsigned mask, const int *snb,
+                                             const FastDiv &dv0, const FastDiv &dv1)
 {
     const int N0 = L.n[0], N1 = L.n[1];
     const int nth = blockDim.x;
@@ -105,38 +157,34 @@ __device__ __forceinline__ void gather_faces(const T *comp, const LabGeom &L, co
     if (mask & 1u) {
         const int m = N1 * TZ;
         for (int i = threadIdx.x; i < 2 * m; i += nth) {
-            const int side = i / m, r = i - side * m;
-            const int y = r % N1, z = r / N1;
-            (side ? t.xhi : t.xlo)[r] =
-                face_value<T>(comp, L, bc, plain, snb, block, bx, by, bz, side ? N0 : -1, y, z0 + z);
+            const int side = i >= m, r = side ? i - m : i;
+            const int z = dv1.div(r), y = r - z * N1;
+            face_cell<T>(comp, L, bc, plain, snb, block, bx, by, bz, side ? N0 : -1, y, z0 + z,
+                         (side ? t.xhi : t.xlo) + r);
         }
     }
     if (mask & 2u) {
         const int m = N0 * TZ;
         for (int i = threadIdx.x; i < 2 * m; i += nth) {
-            const int side = i / m, r = i - side * m;
-            const int x = r % N0, z = r / N0;
-            (side ? t.yhi : t.ylo)[r] =
-                face_value<T>(comp, L, bc, plain, snb, block, bx, by, bz, x, side ? N1 : -1, z0 + z);
+            const int side = i >= m, r = side ? i - m : i;
+            const int z = dv0.div(r), x = r - z * N0;
+            face_cell<T>(comp, L, bc, plain, snb, block, bx, by, bz, x, side ? N1 : -1, z0 + z,
+                         (side ? t.yhi : t.ylo) + r);
         }
     }
     if (mask & 4u) {
         const int m = N0 * N1;
         for (int i = threadIdx.x; i < 2 * m; i += nth) {
-            const int side = i / m, r = i - side * m;
-            const int x = r % N0, y = r / N0;
-            const int z = side ? z0 + TZ : z0 - 1;
-            // z faces inside the block (interior tiles) are plain loads
-            (side ? t.zhi : t.zlo)[r] =
-                (unsigned)z < (unsigned)L.n[2]
-                    ? __ldg(comp + (int64_t)block * L.bstride + x + (int64_t)N0 * (y + (int64_t)N1 * z))
-                    : face_value<T>(comp, L, bc, plain, snb, block, bx, by, bz, x, y, z);
+            const int side = i >= m, r = side ? i - m : i;
+            const int y = dv0.div(r), x = r - y * N0;
+            face_cell<T>(comp, L, bc, plain, snb, block, bx, by, bz, x, y, side ? z0 + TZ : z0 - 1,
+                         (side ? t.zhi : t.zlo) + r);
         }
     }
 }
 
 template <typename T, int OP>
-__global__ void __launch_bounds__(256) fd_kernel(FdParams<T> p)
+__global__ void __launch_bounds__(256, 8) fd_kernel(FdParams<T> p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw);
@@ -147,6 +195,24 @@ __global__ void __launch_bounds__(256) fd_kernel(FdParams<T> p)
     const int tiles_per_block = N2 / TZ;
     const int block = blockIdx.x / tiles_per_block;
     const int z0 = (blockIdx.x - block * tiles_per_block) * TZ;
+    constexpr int NC = (OP == kDiv) ? 3 : 1;
+    const size_t te = tile_elems(N0, N1, TZ);
+    Tile<T> tl[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+        tl[c] = carve<T>(base + c * te, N0, N1, TZ);
+    const uint32_t in_bytes = (uint32_t)((size_t)N0 * N1 * TZ * sizeof(T));
+    const int64_t in_off = (int64_t)block * L.bstride + (int64_t)z0 * N0 * N1;
+    // the interior's bulk copy goes out first; the barrier below publishes
+    // the mbarrier's initialisation to the other threads
+    if (p.use_bulk && threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(bar, in_bytes * NC);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            bulk_g2s(tl[c].in, p.in[c] + in_off, in_bytes, bar);
+    }
     const int bx = block % L.nb[0];
     const int by = (block / L.nb[0]) % L.nb[1];
     const int bz = block / (L.nb[0] * L.nb[1]);
@@ -159,95 +225,86 @@ __global__ void __launch_bounds__(256) fd_kernel(FdParams<T> p)
         nz = nz < 0 ? nz + L.nb[2] : (nz >= L.nb[2] ? nz - L.nb[2] : nz);
         snb[t] = nx + L.nb[0] * (ny + L.nb[1] * nz);
     }
-    constexpr int NC = (OP == kDiv) ? 3 : 1;
-    const size_t te = tile_elems<T>(N0, N1, TZ);
-    Tile<T> tl[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-        tl[c] = carve<T>(base + c * te, N0, N1, TZ);
-    const uint32_t in_bytes = (uint32_t)((size_t)N0 * N1 * TZ * sizeof(T));
-    const int64_t in_off = (int64_t)block * L.bstride + (int64_t)z0 * N0 * N1;
-
-    if (p.use_bulk) {
-        if (threadIdx.x == 0) {
-            mbar_init(bar, 1);
-            fence_mbar_init();
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            mbar_arrive_expect_tx(bar, in_bytes * NC);
-#pragma unroll
-            for (int c = 0; c < NC; ++c)
-                bulk_g2s(tl[c].in, p.in[c] + in_off, in_bytes, bar);
-        }
-    } else {
+    if (!p.use_bulk) {
         const int m = N0 * N1 * TZ;
 #pragma unroll
         for (int c = 0; c < NC; ++c)
             for (int i = threadIdx.x; i < m; i += blockDim.x)
                 tl[c].in[i] = p.in[c][in_off + i];
-        __syncthreads(); // snb
     }
+    __syncthreads(); // snb, mbarrier initialised
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
         const unsigned mask = (OP == kDiv) ? (1u << c) : 7u;
-        gather_faces<T>(p.in[c], L, p.bc[c], block, bx, by, bz, z0, TZ, tl[c], mask, snb);
+        gather_faces<T>(p.in[c], L, p.bc[c], block, bx, by, bz, z0, TZ, tl[c], mask, snb, p.dv0, p.dv1);
     }
+    fd_cp_async_wait_all();
     if (p.use_bulk) {
-        if (!mbar_wait_bounded(bar, 0)) {
+        if (!mbar_wait_bounded_sleep(bar, 0)) {
             atomicExch(p.err, kDevErrTimeout);
         }
     }
     __syncthreads();
 
-    using A = Arith<T>;
+    // x-even blocks: two neighbouring cells of a row per thread, with
+    // two-element shared loads and global stores
+    if ((N0 & 1) == 0) {
+        using V = typename Vec2<T>::type;
+        const int h0 = N0 >> 1;
+        const int mp = h0 * N1 * TZ;
+        const Tile<T> &a = tl[0], &b = tl[NC > 1 ? 1 : 0], &c = tl[NC > 2 ? 2 : 0];
+        for (int j = threadIdx.x; j < mp; j += blockDim.x) {
+            const int row = p.dvh.div(j), x = 2 * (j - row * h0); // row = y + N1 z
+            const int z = p.dv1.div(row), y = row - z * N1;
+            const int i = x + N0 * row;
+            const int64_t o = in_off + i;
+            const V ac = *reinterpret_cast<const V *>(a.in + i);
+            const T xm = x > 0 ? a.in[i - 1] : a.xlo[row];
+            const T xp = x + 2 < N0 ? a.in[i + 2] : a.xhi[row];
+            const V yp = *reinterpret_cast<const V *>(y + 1 < N1 ? b.in + i + N0 : b.yhi + x + N0 * z);
+            const V ym = *reinterpret_cast<const V *>(y > 0 ? b.in + i - N0 : b.ylo + x + N0 * z);
+            const V zp = *reinterpret_cast<const V *>(z + 1 < TZ ? c.in + i + N0 * N1 : c.zhi + x + N0 * y);
+            const V zm = *reinterpret_cast<const V *>(z > 0 ? c.in + i - N0 * N1 : c.zlo + x + N0 * y);
+            T l0 = T(0), l1 = T(0), g00 = T(0), g01 = T(0), g02 = T(0), g10 = T(0), g11 = T(0), g12 = T(0);
+            cell_eval<T, OP>(p, ac.x, ac.y, xm, yp.x, ym.x, zp.x, zm.x, l0, g00, g01, g02);
+            cell_eval<T, OP>(p, ac.y, xp, ac.x, yp.y, ym.y, zp.y, zm.y, l1, g10, g11, g12);
+            if (OP == kLap || OP == kLapGrad || OP == kDiv)
+                *reinterpret_cast<V *>(p.lap + o) = V{l0, l1};
+            if (OP == kGrad || OP == kLapGrad) {
+                *reinterpret_cast<V *>(p.grad + o) = V{g00, g10};
+                *reinterpret_cast<V *>(p.grad + o + p.out_cstride) = V{g01, g11};
+                *reinterpret_cast<V *>(p.grad + o + 2 * p.out_cstride) = V{g02, g12};
+            }
+        }
+        return;
+    }
     const int m = N0 * N1 * TZ;
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        const int x = i % N0;
-        const int y = (i / N0) % N1;
-        const int z = i / (N0 * N1);
+        const int z = p.dv01.div(i), r = i - z * (N0 * N1);
+        const int y = p.dv0.div(r), x = r - y * N0;
         const int64_t o = in_off + i;
-        if (OP == kDiv) {
-            const Tile<T> &a = tl[0], &b = tl[1], &c = tl[2];
-            const T axp = x + 1 < N0 ? a.in[i + 1] : a.xhi[y + N1 * z];
-            const T axm = x > 0 ? a.in[i - 1] : a.xlo[y + N1 * z];
-            const T byp = y + 1 < N1 ? b.in[i + N0] : b.yhi[x + N0 * z];
-            const T bym = y > 0 ? b.in[i - N0] : b.ylo[x + N0 * z];
-            const T czp = z + 1 < TZ ? c.in[i + N0 * N1] : c.zhi[x + N0 * y];
-            const T czm = z > 0 ? c.in[i - N0 * N1] : c.zlo[x + N0 * y];
-            const T t0 = A::mul(A::sub(axp, axm), p.ih[0]);
-            const T t1 = A::mul(A::sub(byp, bym), p.ih[1]);
-            const T t2 = A::mul(A::sub(czp, czm), p.ih[2]);
-            p.lap[o] = A::mul(T(0.5), A::add(A::add(t0, t1), t2));
-        } else {
-            const Tile<T> &a = tl[0];
-            const T c0 = a.in[i];
-            const T xp = x + 1 < N0 ? a.in[i + 1] : a.xhi[y + N1 * z];
-            const T xm = x > 0 ? a.in[i - 1] : a.xlo[y + N1 * z];
-            const T yp = y + 1 < N1 ? a.in[i + N0] : a.yhi[x + N0 * z];
-            const T ym = y > 0 ? a.in[i - N0] : a.ylo[x + N0 * z];
-            const T zp = z + 1 < TZ ? a.in[i + N0 * N1] : a.zhi[x + N0 * y];
-            const T zm = z > 0 ? a.in[i - N0 * N1] : a.zlo[x + N0 * y];
-            if (OP == kLap || OP == kLapGrad) {
-                const T c2 = A::mul(T(2), c0);
-                const T ddx = A::mul(p.ih2[0], A::add(A::sub(xp, c2), xm));
-                const T ddy = A::mul(p.ih2[1], A::add(A::sub(yp, c2), ym));
-                const T ddz = A::mul(p.ih2[2], A::add(A::sub(zp, c2), zm));
-                p.lap[o] = A::add(A::add(ddx, ddy), ddz);
-            }
-            if (OP == kGrad || OP == kLapGrad) {
-                p.grad[o] = A::mul(T(0.5), A::mul(A::sub(xp, xm), p.ih[0]));
-                p.grad[o + p.out_cstride] = A::mul(T(0.5), A::mul(A::sub(yp, ym), p.ih[1]));
-                p.grad[o + 2 * p.out_cstride] = A::mul(T(0.5), A::mul(A::sub(zp, zm), p.ih[2]));
-            }
+        const Tile<T> &a = tl[0], &b = tl[NC > 1 ? 1 : 0], &c = tl[NC > 2 ? 2 : 0];
+        const T c0 = a.in[i];
+        const T xp = x + 1 < N0 ? a.in[i + 1] : a.xhi[y + N1 * z];
+        const T xm = x > 0 ? a.in[i - 1] : a.xlo[y + N1 * z];
+        const T yp = y + 1 < N1 ? b.in[i + N0] : b.yhi[x + N0 * z];
+        const T ym = y > 0 ? b.in[i - N0] : b.ylo[x + N0 * z];
+        const T zp = z + 1 < TZ ? c.in[i + N0 * N1] : c.zhi[x + N0 * y];
+        const T zm = z > 0 ? c.in[i - N0 * N1] : c.zlo[x + N0 * y];
+        T l = T(0), g0 = T(0), g1 = T(0), g2 = T(0);
+        cell_eval<T, OP>(p, c0, xp, xm, yp, ym, zp, zm, l, g0, g1, g2);
+        if (OP == kLap || OP == kLapGrad || OP == kDiv) p.lap[o] = l;
+        if (OP == kGrad || OP == kLapGrad) {
+            p.grad[o] = g0;
+            p.grad[o + p.out_cstride] = g1;
+            p.grad[o + 2 * p.out_cstride] = g2;
         }
     }
 }
 
 static size_t fd_smem_bytes(int N0, int N1, int TZ, size_t es, int nc)
 {
-    const size_t te = (size_t)N0 * N1 * TZ + 2 * ((size_t)N1 * TZ + (size_t)N0 * TZ + (size_t)N0 * N1);
-    return 128 + te * es * nc;
+    return 128 + tile_elems(N0, N1, TZ) * es * nc;
 }
 
 // z-slab height: the largest divisor of N2 whose tile fits the budget and
@@ -304,12 +361,20 @@ static cn_status launch_fd(cn_grid *u, int comp, cn_grid *o1, int c1, cn_grid *o
     const int tz = pick_tz(N0, N1, N2, sizeof(T), NC, 100 * 1024);
     if (tz == 0) return fail(CN_ERR_UNSUPPORTED, "block too large for the fused stencil tile");
     p.TZ = tz;
+    p.dv0 = FastDiv((uint32_t)N0);
+    p.dv1 = FastDiv((uint32_t)N1);
+    p.dv01 = FastDiv((uint32_t)(N0 * N1));
+    p.dvh = FastDiv((uint32_t)(N0 / 2 > 0 ? N0 / 2 : 1));
     const size_t tile_bytes = (size_t)N0 * N1 * tz * sizeof(T);
     p.use_bulk = (tile_bytes % 16 == 0) && ((u->block_stride * sizeof(T)) % 16 == 0);
     p.err = u->d_err;
     const size_t smem = fd_smem_bytes(N0, N1, tz, sizeof(T), NC);
     CN_CUDA_TRY(cudaFuncSetAttribute(fd_kernel<T, OP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
+    // eight 256-thread CTAs per SM fit the registers (32 per thread): ask for
+    // the shared-memory carve-out that lets their tiles fit as well
+    CN_CUDA_TRY(cudaFuncSetAttribute(fd_kernel<T, OP>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
     const int64_t ctas = (int64_t)u->nblocks * (N2 / tz);
     fd_kernel<T, OP><<<(unsigned)ctas, 256, smem, st>>>(p);
     CN_CUDA_TRY(cudaGetLastError());
@@ -335,26 +400,27 @@ static cn_status dispatch_fd(cn_grid *u, int comp, int ncin, cn_grid *o1, int c1
 }
 
 // ---------------------------------------------------------------- ddx ABI
+// One thread per (x, y) column of 32 x 8 tiles, looping over z: no index
+// divisions, coalesced rows along x.
 template <typename T>
 __global__ void __launch_bounds__(256)
     ddx_kernel(int nx, int ny, int nz, const T *__restrict__ src, int xps, int xyps,
                T *__restrict__ dst, int xpd, int xypd, T fac)
 {
     using A = Arith<T>;
-    const int64_t total = (int64_t)nx * ny * nz;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % nx);
-        const int y = (int)((i / nx) % ny);
-        const int z = (int)(i / ((int64_t)nx * ny));
-        const T *s = src + x + (int64_t)xps * y + (int64_t)xyps * z;
-        T acc = A::add(s[-1], s[1]);
-        acc = A::add(acc, s[-xps]);
-        acc = A::add(acc, s[xps]);
-        acc = A::add(acc, s[-xyps]);
-        acc = A::add(acc, s[xyps]);
-        acc = A::sub(acc, A::mul(T(6), s[0]));
-        dst[x + (int64_t)xpd * y + (int64_t)xypd * z] = A::mul(fac, acc);
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    if (x >= nx) return;
+    for (int y = blockIdx.y * 8 + (threadIdx.x >> 5); y < ny; y += gridDim.y * 8) {
+        for (int z = blockIdx.z; z < nz; z += gridDim.z) {
+            const T *s = src + x + (int64_t)xps * y + (int64_t)xyps * z;
+            T acc = A::add(s[-1], s[1]);
+            acc = A::add(acc, s[-xps]);
+            acc = A::add(acc, s[xps]);
+            acc = A::add(acc, s[-xyps]);
+            acc = A::add(acc, s[xyps]);
+            acc = A::sub(acc, A::mul(T(6), s[0]));
+            dst[x + (int64_t)xpd * y + (int64_t)xypd * z] = A::mul(fac, acc);
+        }
     }
 }
 
@@ -364,10 +430,9 @@ static cn_status launch_ddx(int nx, int ny, int nz, const T *src, int xps, int x
 {
     if (nx < 1 || ny < 1 || nz < 1 || !src || !dst)
         return fail(CN_ERR_INVALID_ARGUMENT, "ddx: bad extent or pointer");
-    const int64_t total = (int64_t)nx * ny * nz;
-    int64_t blocks = (total + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    ddx_kernel<T><<<(unsigned)blocks, 256, 0, st>>>(nx, ny, nz, src, xps, xyps, dst, xpd, xypd, fac);
+    const int gx = (nx + 31) / 32;
+    const dim3 grid((unsigned)gx, (unsigned)std::min((ny + 7) / 8, 65535), (unsigned)std::min(nz, 65535));
+    ddx_kernel<T><<<grid, 256, 0, st>>>(nx, ny, nz, src, xps, xyps, dst, xpd, xypd, fac);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
