@@ -896,6 +896,75 @@ def run_reference(args, world, rank):
                 e2e=dict(value=round(v, 6), unit=unit, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
 
 
+def accuracy_fp32(args):
+    """FP32 against FP64 on the C4 geometry (1024^3 cells as 32^3 blocks of
+    32^3, the C2 pulse, BCs and CFL 0.3 time step from the FP64 state), both
+    on the GPU: `--acc-steps` SSP-RK3 steps each, then L1 / Linf of the
+    difference per conserved variable (relative to max |state| of rho and E)
+    and the drift of the FP64 integrals of mass and energy.  The two states
+    and their work grids (193 GB) do not fit one GPU together, so the FP64 run
+    goes first and its final state waits in host memory."""
+    import torch
+
+    import cubismnova_b200 as cn
+    nb = tuple(args.blocks) if args.blocks else C4.nb
+    n = C4.n
+    cells = int(np.prod(n))
+    steps = args.acc_steps
+
+    def make(dtype):
+        U = cn.Grid.Cartesian(nb, n, ncomp=5, dtype=dtype)
+        cn.workloads.euler_pulse(U)
+        torch.cuda.empty_cache()  # the pulse's FP64 temporaries
+        cn.workloads.euler_bcs(U)
+        U.sync_bcs()
+        return U, cn.euler.like(U), cn.euler.like(U)
+
+    def integrals(U):
+        vol = float(np.prod(U.getCellSize()))
+        return [float(U.tensor(c)[:, :cells].sum(dtype=torch.float64)) * vol for c in range(5)]
+
+    out = dict(impl="accuracy", workload=f"{nb[0] * n[0]}x{nb[1] * n[1]}x{nb[2] * n[2]} cells as "
+                                        f"{nb[0]}x{nb[1]}x{nb[2]} blocks of 32^3, Euler pulse, C2 BCs",
+               rk3_steps=steps)
+    runs = {}
+    host64 = None
+    dt = None
+    for name, dtype in (("f64", np.float64), ("f32", np.float32)):
+        U, w1, w2 = make(dtype)
+        if dt is None:
+            dt = cn.euler.cfl_dt(U, 0.3)
+        s0 = integrals(U)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sums = None
+        for i in range(steps):
+            sums = cn.euler.rk3_step(U, w1, w2, dt, want_sums=(i == steps - 1))
+        e1.record()
+        torch.cuda.synchronize()
+        runs[name] = dict(ms_per_step=round(e0.elapsed_time(e1) / steps, 3),
+                          mass_drift=(sums[0] - s0[0]) / s0[0], energy_drift=(sums[4] - s0[4]) / s0[4],
+                          momentum_change=[sums[c] - s0[c] for c in (1, 2, 3)])
+        if name == "f64":
+            host64 = [U.tensor(c)[:, :cells].cpu() for c in range(5)]
+            del U, w1, w2
+            torch.cuda.empty_cache()
+        else:
+            scale = max(float(host64[0].abs().max()), float(host64[4].abs().max()))
+            err = []
+            for c in range(5):
+                a = host64[c].cuda()
+                a.sub_(U.tensor(c)[:, :cells].double()).abs_()
+                err.append(dict(var=c, L1=float(a.mean()) / scale, Linf=float(a.max()) / scale))
+                del a
+                torch.cuda.empty_cache()
+            del U, w1, w2
+    out.update(dt=dt, runs=runs, fp32_vs_fp64=err,
+               note="errors relative to max(|rho|, |E|) of the FP64 state; drifts are (I_end - I_0) / I_0 "
+                    "of the FP64 integrals that the stage kernels accumulate")
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -912,8 +981,14 @@ def main():
                     help="c5: skip training and timing the learned smoother")
     ap.add_argument("--blocks", type=int, nargs=3, default=None,
                     help="override the block counts (reduced grids for profiling runs)")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="FP32 vs FP64 accuracy study on the C4 geometry (no timing line)")
+    ap.add_argument("--acc-steps", type=int, default=100, help="--accuracy: SSP-RK3 steps")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.accuracy:
+        accuracy_fp32(args)
+        return
     if args.impl == "reference":
         # the reference arm is the host CPU path: rank 0 alone runs it
         world = int(os.environ.get("WORLD_SIZE", "1"))

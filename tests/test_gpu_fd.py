@@ -138,3 +138,74 @@ def test_ddx_kernel_abi(cn, oracle_lib, dtype):
       C.c_void_p(tdst.data_ptr()), N, N * N, factor)
     torch.cuda.synchronize()
     assert np.array_equal(tdst.cpu().numpy(), dst)
+
+
+def _glob(a, nb, n, stride):
+    """Block-ordered component -> global periodic array (z, y, x)."""
+    nbk = int(np.prod(nb))
+    v = a.reshape(nbk, stride)[:, : int(np.prod(n))].reshape(nb[2], nb[1], nb[0], n[2], n[1], n[0])
+    return v.transpose(0, 3, 1, 4, 2, 5).reshape(nb[2] * n[2], nb[1] * n[1], nb[0] * n[0])
+
+
+@pytest.mark.parametrize("n", [(5, 3, 7), (7, 6, 4), (6, 5, 3), (2, 9, 2)])
+def test_lap_grad_odd_extents_vs_oracle(cn, oracle_lib, n):
+    """Block extents with odd x (one cell per thread) and odd y / z (two cells
+    per thread), periodic and with a BC chain, bit-exact vs the oracle."""
+    O = oracle_lib
+    nb = (3, 2, 2)
+    stride = O.block_stride(n, np.float64)
+    rng = np.random.default_rng(sum(n))
+    comp = rng.standard_normal(int(np.prod(nb)) * stride)
+    for bcl in ({}, {b: [(0, 0, O.BC_DIRICHLET, 0.25), (1, 1, O.BC_ABSORBING, 0), (2, 0, O.BC_SYMMETRY, -1)]
+                     for b in range(int(np.prod(nb)))}):
+        g = make_grid(cn, comp, nb, n, bcl)
+        lap = cn.Grid.Cartesian(nb, n)
+        grad = cn.Grid.Cartesian(nb, n, ncomp=3)
+        _run(cn, "lap_grad", g, (lap, grad))
+        hh = g.getCellSize()
+        want_lap = O.laplacian_f64(comp, nb, n, bcl, [1.0 / (x * x) for x in hh])
+        want_grad = O.gradient_f64(comp, nb, n, bcl, [1.0 / x for x in hh])
+        assert np.array_equal(lap.download(0), want_lap)
+        for d in range(3):
+            assert np.array_equal(grad.download(d), want_grad[d])
+
+
+@pytest.mark.parametrize("n", [(8, 4, 6), (5, 3, 7)])
+def test_fp32_lap_grad_div_periodic_vs_numpy(cn, oracle_lib, n):
+    """FP32 grids: the same operation order in float32 numpy (every operation
+    rounded on its own, no contraction) gives the same bits."""
+    O = oracle_lib
+    nb = (3, 2, 2)
+    stride = O.block_stride(n, np.float32)
+    rng = np.random.default_rng(7)
+    f32 = np.float32
+    comps = [rng.standard_normal(int(np.prod(nb)) * stride).astype(f32) for _ in range(3)]
+    g = cn.Grid.Cartesian(nb, n, ncomp=3, dtype=f32)
+    for c in range(3):
+        g.upload(comps[c], c)
+    lap = cn.Grid.Cartesian(nb, n, dtype=f32)
+    grad = cn.Grid.Cartesian(nb, n, ncomp=3, dtype=f32)
+    div = cn.Grid.Cartesian(nb, n, dtype=f32)
+    _run(cn, "lap_grad", g, (lap, grad))
+    cn.ops.divergence(g, div)
+    import torch
+    torch.cuda.synchronize()
+    hh = g.getCellSize()
+    ih = [f32(1.0 / x) for x in hh]
+    ih2 = [f32(1.0 / (x * x)) for x in hh]
+    u = _glob(comps[0], nb, n, stride)
+    xp, xm = np.roll(u, -1, 2), np.roll(u, 1, 2)
+    yp, ym = np.roll(u, -1, 1), np.roll(u, 1, 1)
+    zp, zm = np.roll(u, -1, 0), np.roll(u, 1, 0)
+    c2 = f32(2) * u
+    want_lap = (ih2[0] * ((xp - c2) + xm) + ih2[1] * ((yp - c2) + ym)) + ih2[2] * ((zp - c2) + zm)
+    want_g = [f32(0.5) * ((xp - xm) * ih[0]), f32(0.5) * ((yp - ym) * ih[1]), f32(0.5) * ((zp - zm) * ih[2])]
+    v0, v1, v2 = (_glob(a, nb, n, stride) for a in comps)
+    t0 = (np.roll(v0, -1, 2) - np.roll(v0, 1, 2)) * ih[0]
+    t1 = (np.roll(v1, -1, 1) - np.roll(v1, 1, 1)) * ih[1]
+    t2 = (np.roll(v2, -1, 0) - np.roll(v2, 1, 0)) * ih[2]
+    want_div = f32(0.5) * ((t0 + t1) + t2)
+    assert np.array_equal(_glob(lap.download(0), nb, n, stride), want_lap)
+    for d in range(3):
+        assert np.array_equal(_glob(grad.download(d), nb, n, stride), want_g[d])
+    assert np.array_equal(_glob(div.download(0), nb, n, stride), want_div)
