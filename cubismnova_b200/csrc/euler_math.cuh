@@ -13,7 +13,10 @@
 // alpha_k = d_k / t_k normalise to omega_k = d_k*prod_{j!=k} t_j / D with
 // D = sum_k d_k*prod_{j!=k} t_j, so one division per reconstruction suffices:
 //   v = (w0*n0 + w1*n1 + w2*n2) / (6*D),  w0 = d0*t1*t2, w1 = d1*t0*t2, w2 = d2*t0*t1,
-// where n_k = 6*q_k are the candidate stencils' numerators.
+// where n_k = 6*q_k are the candidate stencils' numerators.  The indicators
+// beta_k and the products t_i t_j belong to the cell, not to the face: a
+// cell's left-biased state (at its upper face) and right-biased state (at its
+// lower face) share them.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -41,56 +44,73 @@ __device__ __forceinline__ float dabs(float a) { return fabsf(a); }
 __device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float dmax(float a, float b) { return fmaxf(a, b); }
 
-// Left-biased WENO5-JS reconstruction at i+1/2 from v0..v4 = v[i-2..i+2],
-// returned as numerator and denominator: value = num / den.
+// Smoothness of cell j from u0..u4 = v[j-2..j+2]: with s_k = eps + beta_k
+// and t_k = s_k^2 for the stencils S0 = {j-2, j-1, j}, S1 = {j-1, j, j+1},
+// S2 = {j, j+1, j+2}, the products p12 = t1 t2, p02 = t0 t2, p01 = t0 t1.
+// They serve both states of the cell (left-biased at j+1/2, right-biased at
+// j-1/2), so a cell's indicators are computed once for its two faces.
 template <typename T>
-__device__ __forceinline__ void weno5_nd(T v0, T v1, T v2, T v3, T v4, T &num, T &den)
+__device__ __forceinline__ void weno5_beta(T u0, T u1, T u2, T u3, T u4, T &p12, T &p02, T &p01)
 {
     using C = K<T>;
-    // smoothness indicators
-    const T a0 = dfma(T(-2), v1, v0) + v2;            // v0 - 2v1 + v2
-    const T b0 = dfma(T(3), v2, dfma(T(-4), v1, v0)); // v0 - 4v1 + 3v2
-    const T a1 = dfma(T(-2), v2, v1) + v3;            // v1 - 2v2 + v3
-    const T b1 = v1 - v3;
-    const T a2 = dfma(T(-2), v3, v2) + v4;            // v2 - 2v3 + v4
-    const T b2 = dfma(T(3), v2, dfma(T(-4), v3, v4)); // 3v2 - 4v3 + v4
+    const T a0 = dfma(T(-2), u1, u0) + u2;            // u0 - 2u1 + u2
+    const T b0 = dfma(T(3), u2, dfma(T(-4), u1, u0)); // u0 - 4u1 + 3u2
+    const T a1 = dfma(T(-2), u2, u1) + u3;            // u1 - 2u2 + u3
+    const T b1 = u1 - u3;
+    const T a2 = dfma(T(-2), u3, u2) + u4;            // u2 - 2u3 + u4
+    const T b2 = dfma(T(3), u2, dfma(T(-4), u3, u4)); // 3u2 - 4u3 + u4
     const T s0 = C::eps + dfma(C::c1312 * a0, a0, C::quarter * (b0 * b0));
     const T s1 = C::eps + dfma(C::c1312 * a1, a1, C::quarter * (b1 * b1));
     const T s2 = C::eps + dfma(C::c1312 * a2, a2, C::quarter * (b2 * b2));
     const T t0 = s0 * s0, t1 = s1 * s1, t2 = s2 * s2;
-    const T w0 = C::d0 * (t1 * t2);
-    const T w1 = C::d1 * (t0 * t2);
-    const T w2 = C::d2 * (t0 * t1);
+    p12 = t1 * t2;
+    p02 = t0 * t2;
+    p01 = t0 * t1;
+}
+
+// Left-biased state of cell j at j+1/2 (linear weights 1/10, 6/10, 3/10 on
+// S0, S1, S2) as numerator and denominator: value = num / den.
+template <typename T>
+__device__ __forceinline__ void weno5_left(T u0, T u1, T u2, T u3, T u4, T p12, T p02, T p01, T &num, T &den)
+{
+    using C = K<T>;
+    const T w0 = C::d0 * p12, w1 = C::d1 * p02, w2 = C::d2 * p01;
     // candidate numerators 6*q_k
-    const T n0 = dfma(T(2), v0, dfma(T(-7), v1, T(11) * v2)); // 2v0 - 7v1 + 11v2
-    const T n1 = dfma(T(5), v2, dfma(T(2), v3, -v1));         // -v1 + 5v2 + 2v3
-    const T n2 = dfma(T(2), v2, dfma(T(5), v3, -v4));         // 2v2 + 5v3 - v4
+    const T n0 = dfma(T(2), u0, dfma(T(-7), u1, T(11) * u2)); // 2u0 - 7u1 + 11u2
+    const T n1 = dfma(T(5), u2, dfma(T(2), u3, -u1));         // -u1 + 5u2 + 2u3
+    const T n2 = dfma(T(2), u2, dfma(T(5), u3, -u4));         // 2u2 + 5u3 - u4
     num = dfma(w0, n0, dfma(w1, n1, w2 * n2));
     den = C::six * ((w0 + w1) + w2);
 }
 
-// Left and right states at the face between v2 and v3 from v0..v5 =
-// v[i-2..i+3].  FP64 shares one division between the two:
-//   inv = 1/(denL*denR), vL = (numL*denR)*inv, vR = (numR*denL)*inv
+// Right-biased state of cell j at j-1/2 (linear weights 3/10, 6/10, 1/10).
+template <typename T>
+__device__ __forceinline__ void weno5_right(T u0, T u1, T u2, T u3, T u4, T p12, T p02, T p01, T &num, T &den)
+{
+    using C = K<T>;
+    const T r0 = C::d2 * p12, r1 = C::d1 * p02, r2 = C::d0 * p01;
+    const T m0 = dfma(T(5), u1, dfma(T(2), u2, -u0));         // -u0 + 5u1 + 2u2
+    const T m1 = dfma(T(2), u1, dfma(T(5), u2, -u3));         // 2u1 + 5u2 - u3
+    const T m2 = dfma(T(2), u4, dfma(T(-7), u3, T(11) * u2)); // 11u2 - 7u3 + 2u4
+    num = dfma(r0, m0, dfma(r1, m1, r2 * m2));
+    den = C::six * ((r0 + r1) + r2);
+}
+
+// The two states at one face from the lower cell's left-biased (nl, dl) and
+// the upper cell's right-biased (nr, dr) reconstruction.  FP64 shares one
+// division between them:
+//   inv = 1/(dl*dr), vl = (nl*dr)*inv, vr = (nr*dl)*inv
 // (den >= 6e-25 since eps = 1e-6, so the product cannot underflow in FP64);
 // FP32 divides twice, as the product could leave the FP32 range.
-__device__ __forceinline__ void weno5_pair(double v0, double v1, double v2, double v3, double v4, double v5,
-                                           double &vl, double &vr)
+__device__ __forceinline__ void face_states(double nl, double dl, double nr, double dr, double &vl, double &vr)
 {
-    double nl, dl, nr, dr;
-    weno5_nd<double>(v0, v1, v2, v3, v4, nl, dl);
-    weno5_nd<double>(v5, v4, v3, v2, v1, nr, dr);
     const double inv = 1.0 / (dl * dr);
     vl = (nl * dr) * inv;
     vr = (nr * dl) * inv;
 }
 
-__device__ __forceinline__ void weno5_pair(float v0, float v1, float v2, float v3, float v4, float v5, float &vl,
-                                           float &vr)
+__device__ __forceinline__ void face_states(float nl, float dl, float nr, float dr, float &vl, float &vr)
 {
-    float nl, dl, nr, dr;
-    weno5_nd<float>(v0, v1, v2, v3, v4, nl, dl);
-    weno5_nd<float>(v5, v4, v3, v2, v1, nr, dr);
     vl = nl / dl;
     vr = nr / dr;
 }

@@ -16,18 +16,39 @@ constexpr int TB = 8;                 // tile edge
 constexpr int G = 3;                  // ghost width
 constexpr int NCORE = TB * TB * TB;   // tile cells: 512
 constexpr int NHALO = 2 * G * TB * TB; // one direction's halo slabs: 384
+// Shared-memory strides of the core (x: 1): rows padded to 9 entries and
+// planes to 72, so that the 16 lines of a half-warp in a sweep (8 values of
+// one coordinate x 2 of the other) hit distinct banks in every direction.
+constexpr int CY = 9, CZ = 72;
+constexpr int NCORE_SM = TB * CZ;     // 576 shared entries of the core
+// Halo slot of direction D (slab coordinate h = 0..5 along D: cells -3..-1
+// and 8..10), with the core's stride along D and padded like the core:
+//   D = 0: h + 6 y + 49 z,   D = 1: x + 9 h + 56 z,   D = 2: x + 9 y + 72 h.
+constexpr int HS0 = 392, HS1 = 448, HS2 = 432;
 // FP64 stages one direction's halo at a time (smaller shared memory, three
 // CTAs per SM); FP32 has room for all three halo slots at once and stages
 // them together, saving two barrier-separated load phases.
 template <typename T> struct Stg {
     static constexpr bool all = sizeof(T) == 4;
-    static constexpr int SV = NCORE + (all ? 3 : 1) * NHALO; // staged cells per variable
+    static constexpr int SV = NCORE_SM + (all ? HS0 + HS1 + HS2 : HS1); // shared entries per variable
+    // first entry of direction D's halo slot
+    static __device__ __forceinline__ int slot(int D)
+    {
+        return NCORE_SM + (all ? (D == 0 ? 0 : (D == 1 ? HS0 : HS0 + HS1)) : 0);
+    }
 };
-constexpr int SV = NCORE + NHALO; // FP64 staged cells per variable (896)
 constexpr int NCELL = TB * TB * TB;   // 512
 constexpr int NFACE = (TB + 1) * TB * TB; // 576
-constexpr int NT = 192;               // threads per CTA (576 = 3 * 192)
+constexpr int NT = 192;               // threads per CTA: 64 lines x 3 runs of 3 faces
 constexpr int CPT = (NCELL + NT - 1) / NT; // cells per thread: 3
+
+__device__ __forceinline__ int core_sm(int x, int y, int z) { return x + CY * y + CZ * z; }
+
+// entry of halo cell (x, y, z) with slab coordinate h in direction D's slot
+__device__ __forceinline__ int halo_sm(int D, int x, int y, int z, int h)
+{
+    return D == 0 ? h + 6 * y + 49 * z : (D == 1 ? x + 9 * h + 56 * z : x + 9 * y + 72 * h);
+}
 
 template <typename T> struct StageParams {
     const T *U[5];   // state whose lab is loaded (component bases)
@@ -100,6 +121,21 @@ struct CartSrc {
             snb[27] = (int)plain;
         }
     }
+    // Element offset (in every component) of a halo cell outside the tile's
+    // block when all five components are plain: the periodic neighbour's
+    // cell, what cn::lab_value gives for mode 0.  False otherwise.
+    template <typename T>
+    __device__ __forceinline__ bool plain_offset(const TileInfo<T> &t, int gx, int gy, int gz, const int *snb,
+                                                 int64_t &off) const
+    {
+        if (snb[27] != 31) return false;
+        const int r0 = gx < 0 ? -1 : (gx >= L.n[0] ? 1 : 0), r1 = gy < 0 ? -1 : (gy >= L.n[1] ? 1 : 0),
+                  r2 = gz < 0 ? -1 : (gz >= L.n[2] ? 1 : 0);
+        const int sb = snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
+        off = (int64_t)sb * L.bstride + (gx - r0 * L.n[0]) +
+              (int64_t)L.n[0] * ((gy - r1 * L.n[1]) + (int64_t)L.n[1] * (gz - r2 * L.n[2]));
+        return true;
+    }
     // A halo cell outside the tile's block: for a plain component the
     // periodic neighbour (what cn::lab_value gives for mode 0), else the lab.
     template <typename T>
@@ -120,21 +156,18 @@ struct CartSrc {
     }
 };
 
-// Shared-memory layout per variable: the tile's 512 core cells x-fastest,
-// then the halo slot(s).  The halo slot of direction D holds the two 3-cell
-// slabs of that direction, slab coordinate h = 0..5 (cells -3..-1 and 8..10
-// along D) with the same stride along D as the core (1, 8, 64):
-//   D = 0: (z*8 + y)*6 + h,   D = 1: (z*6 + h)*8 + x,   D = 2: (h*8 + y)*8 + x.
+// Shared-memory layout per variable: the tile's core (strides 1, CY, CZ),
+// then the halo slot(s), each with the core's stride along its direction.
 // FP64 keeps one slot and restages it before each sweep; FP32 keeps all three.
 //
 // The direction is a runtime (warp-uniform) value: one copy of the face code
 // serves all three sweeps, which keeps the kernel's hot code small enough for
 // the instruction caches.
 
-// tile-local coordinates of halo slot i of direction D
-__device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z)
+// tile-local coordinates and slab coordinate h of halo cell i (0..383) of
+// direction D
+__device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z, int &h)
 {
-    int h;
     if (D == 0) {
         h = i % (2 * G);
         y = (i / (2 * G)) % TB;
@@ -153,69 +186,84 @@ __device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z)
     }
 }
 
-// Face fluxes of direction D for the whole tile (one thread per face, each
-// face once), then flux differences into the per-cell accumulators.
+// Face fluxes of direction D for the whole tile, then flux differences into
+// the per-cell accumulators.  Each of the tile's 64 lines along D has 9 faces
+// (face a between cells a-1 and a); thread t takes the run of faces
+// 3r .. 3r+2, r = t / 64, of line t % 64, walking up the line so that each
+// cell's smoothness indicators serve both of its faces: the left-biased state
+// of cell a-1 is carried as (numerator, denominator) from one face to the
+// next, and the face's shared division is taken when the upper cell's
+// right-biased state is known.
 template <typename T>
 __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restrict__ F, T (&acc)[CPT][5],
                                       T gamma, T igm1, T ihd)
 {
-    constexpr bool ALL = Stg<T>::all;
-    const int cs = D == 0 ? 1 : (D == 1 ? TB : TB * TB); // stride along D (core and halo slot)
-    const int hslot = NCORE + (ALL ? D * NHALO : 0);
-    for (int f = threadIdx.x; f < NFACE; f += NT) {
-        // (x, y, z): the cell on the high side of face f; a: its coordinate along D
-        int x, y, z, a;
-        if (D == 0) {
-            x = f % (TB + 1);
-            y = (f / (TB + 1)) % TB;
-            z = f / ((TB + 1) * TB);
-            a = x;
-        } else if (D == 1) {
-            x = f % TB;
-            y = (f / TB) % (TB + 1);
-            z = f / (TB * (TB + 1));
-            a = y;
-        } else {
-            x = f % TB;
-            y = (f / TB) % TB;
-            z = f / (TB * TB);
-            a = z;
-        }
-        // row bases: core cell with coordinate 0 along D, halo slab cell h = 0
-        const int cbase = x + TB * (y + TB * z) - a * cs;
-        const int hbase = hslot + (D == 0 ? (z * TB + y) * (2 * G) : (D == 1 ? z * (2 * G * TB) + x : y * TB + x));
-        // cells a-3 .. a+2 along D
-        int idx[6];
+    const int cs = D == 0 ? 1 : (D == 1 ? CY : CZ);     // shared stride along D (core and halo slot)
+    const int fs = D == 0 ? 1 : (D == 1 ? TB : TB * TB); // face-array stride along D
+    const int run = threadIdx.x >> 6, line = threadIdx.x & 63;
+    const int l0 = line & 7, l1 = line >> 3;
+    const int x = D == 0 ? 0 : l0, y = D == 1 ? 0 : (D == 0 ? l0 : l1), z = D == 2 ? 0 : l1;
+    const int cbase = core_sm(x, y, z);                          // the line's cell 0
+    const int hbase = Stg<T>::slot(D) + halo_sm(D, x, y, z, 0);  // the line's slab cell h = 0
+    // face 0 of the line in the face arrays
+    const int fbase = D == 0 ? (TB + 1) * (y + TB * z) : (D == 1 ? x + TB * (TB + 1) * z : x + TB * y);
+    const int f0 = 3 * run;
+    auto sidx = [&](int a) {
+        return (unsigned)a < (unsigned)TB ? cbase + a * cs : hbase + (a < 0 ? a + G : a - TB + G) * cs;
+    };
+    // left-biased state of cell f0-1, the lower cell of the run's first face
+    T Ln[5], Ld[5];
+    {
+        int id[5];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const int q = a + k - 3;
-            idx[k] = (unsigned)q < (unsigned)TB ? cbase + q * cs : hbase + (q < 0 ? q + G : q - TB + G) * cs;
+        for (int k = 0; k < 5; ++k)
+            id[k] = sidx(f0 - 3 + k);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const T *Wc = W + c * Stg<T>::SV;
+            const T u0 = Wc[id[0]], u1 = Wc[id[1]], u2 = Wc[id[2]], u3 = Wc[id[3]], u4 = Wc[id[4]];
+            T p12, p02, p01;
+            weno5_beta(u0, u1, u2, u3, u4, p12, p02, p01);
+            weno5_left(u0, u1, u2, u3, u4, p12, p02, p01, Ln[c], Ld[c]);
         }
+    }
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+        const int a = f0 + i; // face a: cells a-1 (left state carried in Ln, Ld) and a
+        int id[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            id[k] = sidx(a - 2 + k);
         T WL[5], WR[5];
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const T *Wc = W + c * Stg<T>::SV;
-            const T v0 = Wc[idx[0]], v1 = Wc[idx[1]], v2 = Wc[idx[2]];
-            const T v3 = Wc[idx[3]], v4 = Wc[idx[4]], v5 = Wc[idx[5]];
-            weno5_pair(v0, v1, v2, v3, v4, v5, WL[c], WR[c]);
+            const T u0 = Wc[id[0]], u1 = Wc[id[1]], u2 = Wc[id[2]], u3 = Wc[id[3]], u4 = Wc[id[4]];
+            T p12, p02, p01, nr, dr;
+            weno5_beta(u0, u1, u2, u3, u4, p12, p02, p01);
+            weno5_right(u0, u1, u2, u3, u4, p12, p02, p01, nr, dr);
+            face_states(Ln[c], Ld[c], nr, dr, WL[c], WR[c]);
+            if (i < 2)
+                weno5_left(u0, u1, u2, u3, u4, p12, p02, p01, Ln[c], Ld[c]);
         }
         T Fl[5];
         rusanov<T>(WL, WR, D, gamma, igm1, Fl);
+        const int fi = fbase + a * fs;
 #pragma unroll
         for (int c = 0; c < 5; ++c)
-            F[c * NFACE + f] = Fl[c];
+            F[c * NFACE + fi] = Fl[c];
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const int cidx = threadIdx.x + k * NT;
         if (cidx < NCELL) {
-            const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
-            const int flo = D == 0 ? x + (TB + 1) * (y + TB * z)
-                                   : (D == 1 ? x + TB * (y + (TB + 1) * z) : x + TB * (y + TB * z));
+            const int cx = cidx % TB, cy = (cidx / TB) % TB, cz = cidx / (TB * TB);
+            const int flo = D == 0 ? cx + (TB + 1) * (cy + TB * cz)
+                                   : (D == 1 ? cx + TB * (cy + (TB + 1) * cz) : cx + TB * (cy + TB * cz));
 #pragma unroll
             for (int c = 0; c < 5; ++c) {
-                const T df = F[c * NFACE + flo + cs] - F[c * NFACE + flo];
+                const T df = F[c * NFACE + flo + fs] - F[c * NFACE + flo];
                 acc[k][c] = D == 0 ? df * ihd : dfma(df, ihd, acc[k][c]);
             }
         }
@@ -233,30 +281,51 @@ template <typename T, typename Src>
 __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const Src &src, const TileInfo<T> &t,
                                            T *W, const int *snb)
 {
-    T *slot = W + NCORE + (Stg<T>::all ? D * NHALO : 0);
-    for (int i = threadIdx.x; i < NHALO; i += NT) {
-        int x, y, z;
-        halo_cell(D, i, x, y, z);
+    static_assert(NHALO % NT == 0, "whole halo cells per thread");
+    constexpr int HPT = NHALO / NT; // halo cells per thread: 2
+    T *slot = W + Stg<T>::slot(D);
+    // first pass: the plain loads of all of the thread's cells (inside the
+    // block, or the periodic neighbour's cell when every component is plain)
+    // are issued together; the other cells are resolved into the slot
+    T u[HPT][5];
+    bool inb[HPT];
+    int si[HPT];
+#pragma unroll
+    for (int j = 0; j < HPT; ++j) {
+        const int i = threadIdx.x + j * NT;
+        int x, y, z, h;
+        halo_cell(D, i, x, y, z, h);
+        si[j] = halo_sm(D, x, y, z, h);
         const int gx = t.x0 + x, gy = t.y0 + y, gz = t.z0 + z;
-        T u[5];
-        if ((unsigned)gx < (unsigned)t.N0 && (unsigned)gy < (unsigned)t.N1 && (unsigned)gz < (unsigned)t.N2) {
-            const int64_t o = t.boff + gx + (int64_t)t.N0 * (gy + (int64_t)t.N1 * gz);
+        int64_t o = 0;
+        inb[j] = (unsigned)gx < (unsigned)t.N0 && (unsigned)gy < (unsigned)t.N1 && (unsigned)gz < (unsigned)t.N2;
+        if (inb[j])
+            o = t.boff + gx + (int64_t)t.N0 * (gy + (int64_t)t.N1 * gz);
+        else
+            inb[j] = src.plain_offset(t, gx, gy, gz, snb, o);
+        if (inb[j]) {
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                u[c] = p.U[c][o];
+                u[j][c] = p.U[c][o];
         } else {
 #pragma unroll 1
             for (int c = 0; c < 5; ++c)
-                slot[c * Stg<T>::SV + i] = src.halo(p.U[c], c, t, gx, gy, gz, snb);
+                slot[c * Stg<T>::SV + si[j]] = src.halo(p.U[c], c, t, gx, gy, gz, snb);
+        }
+    }
+    // second pass: conversion to primitives in place
+#pragma unroll
+    for (int j = 0; j < HPT; ++j) {
+        if (!inb[j]) {
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                u[c] = slot[c * Stg<T>::SV + i];
+                u[j][c] = slot[c * Stg<T>::SV + si[j]];
         }
         T w[5];
-        to_primitive<T>(u[0], u[1], u[2], u[3], u[4], p.gm1, w);
+        to_primitive<T>(u[j][0], u[j][1], u[j][2], u[j][3], u[j][4], p.gm1, w);
 #pragma unroll
         for (int c = 0; c < 5; ++c)
-            slot[c * Stg<T>::SV + i] = w[c];
+            slot[c * Stg<T>::SV + si[j]] = w[c];
     }
 }
 
@@ -278,15 +347,34 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
     const TileInfo<T> &t = *ts;
     src.template prepare<T>(t, snb);
     __syncthreads(); // snb
-    // ---- stage the tile's cells as primitives (the halo slot follows per sweep)
-    for (int i = threadIdx.x; i < NCORE; i += NT) {
-        const int x = i % TB, y = (i / TB) % TB, z = i / (TB * TB);
-        const int64_t o = t.boff + (t.x0 + x) + (int64_t)t.N0 * ((t.y0 + y) + (int64_t)t.N1 * (t.z0 + z));
-        T w[5];
-        to_primitive<T>(p.U[0][o], p.U[1][o], p.U[2][o], p.U[3][o], p.U[4][o], p.gm1, w);
+    // ---- stage the tile's cells as primitives (the halo slot follows per
+    // sweep): all of a thread's loads are issued before any conversion
+    {
+        T u[CPT][5];
 #pragma unroll
-        for (int c = 0; c < 5; ++c)
-            W[c * Stg<T>::SV + i] = w[c];
+        for (int k = 0; k < CPT; ++k) {
+            const int i = threadIdx.x + k * NT;
+            if (i < NCORE) {
+                const int x = i % TB, y = (i / TB) % TB, z = i / (TB * TB);
+                const int64_t o =
+                    t.boff + (t.x0 + x) + (int64_t)t.N0 * ((t.y0 + y) + (int64_t)t.N1 * (t.z0 + z));
+#pragma unroll
+                for (int c = 0; c < 5; ++c)
+                    u[k][c] = p.U[c][o];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int i = threadIdx.x + k * NT;
+            if (i < NCORE) {
+                T w[5];
+                to_primitive<T>(u[k][0], u[k][1], u[k][2], u[k][3], u[k][4], p.gm1, w);
+                const int e = core_sm(i % TB, (i / TB) % TB, i / (TB * TB));
+#pragma unroll
+                for (int c = 0; c < 5; ++c)
+                    W[c * Stg<T>::SV + e] = w[c];
+            }
+        }
     }
     if (Stg<T>::all) {
 #pragma unroll 1
@@ -314,32 +402,56 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
         sweep<T>(D, W, F, acc, p.gamma, p.igm1, ihd);
     }
 
-    // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows
+    // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows.
+    // One component at a time, with the next component's loads of U_s and
+    // U^n issued before this component's stores: `out` may alias U^n (stage
+    // 3 updates U in place), so loads cannot move above earlier stores, and
+    // issuing them early keeps one memory latency per tile instead of one per
+    // value.  Each (component, cell) is loaded before it is stored.
     double sums[5] = {0, 0, 0, 0, 0};
+    int64_t eo[CPT];
+    bool eok[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const int cidx = threadIdx.x + k * NT;
-        if (cidx < NCELL) {
-            const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
-            const int64_t o = t.boff + (t.x0 + x) + (int64_t)t.N0 * ((t.y0 + y) + (int64_t)t.N1 * (t.z0 + z));
+        eok[k] = cidx < NCELL;
+        const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
+        eo[k] = t.boff + (t.x0 + x) + (int64_t)t.N0 * ((t.y0 + y) + (int64_t)t.N1 * (t.z0 + z));
+    }
+    T us[2][CPT], un[2][CPT];
 #pragma unroll
-            for (int c = 0; c < 5; ++c) {
+    for (int k = 0; k < CPT; ++k) {
+        us[0][k] = (p.stage >= 1 && eok[k]) ? p.U[0][eo[k]] : T(0);
+        un[0][k] = (p.stage >= 2 && eok[k]) ? p.Un[0][eo[k]] : T(0);
+    }
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const int b = c & 1;
+        if (c + 1 < 5) {
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                us[b ^ 1][k] = (p.stage >= 1 && eok[k]) ? p.U[c + 1][eo[k]] : T(0);
+                un[b ^ 1][k] = (p.stage >= 2 && eok[k]) ? p.Un[c + 1][eo[k]] : T(0);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            if (eok[k]) {
                 const T rhs = -acc[k][c];
                 T v;
                 if (p.stage == 0) {
                     v = rhs;
                 } else {
-                    const T us = p.U[c][o];
-                    const T tt = dfma(p.dt, rhs, us);
+                    const T tt = dfma(p.dt, rhs, us[b][k]);
                     if (p.stage == 1) {
                         v = tt;
                     } else if (p.stage == 2) {
-                        v = dfma(T(0.75), p.Un[c][o], T(0.25) * tt);
+                        v = dfma(T(0.75), un[b][k], T(0.25) * tt);
                     } else {
-                        v = dfma(T(1.0 / 3.0), p.Un[c][o], T(2.0 / 3.0) * tt);
+                        v = dfma(T(1.0 / 3.0), un[b][k], T(2.0 / 3.0) * tt);
                     }
                 }
-                p.out[c][o] = v;
+                p.out[c][eo[k]] = v;
                 sums[c] += (double)v;
             }
         }

@@ -13,39 +13,66 @@
 #include <math.h>
 
 #define DEFINE_EULER_MATH(SUF, T, FMA, SQRT, FABS, FMAX, SHARED_DIV)                            \
-    static inline void weno5_nd_##SUF(T v0, T v1, T v2, T v3, T v4, T *num, T *den) \
+    /* smoothness of cell j from u0..u4 = v[j-2..j+2]: the products          \
+     * p12 = t1 t2, p02 = t0 t2, p01 = t0 t1 of t_k = (eps + beta_k)^2 for   \
+     * the stencils S0 = {j-2..j}, S1 = {j-1..j+1}, S2 = {j..j+2}; shared by  \
+     * the cell's left-biased (j+1/2) and right-biased (j-1/2) states */      \
+    static inline void weno5_beta_##SUF(T u0, T u1, T u2, T u3, T u4, T *p12, T *p02, T *p01) \
     {                                                                          \
         const T c1312 = (T)(13.0 / 12.0), quarter = (T)0.25, eps = (T)1e-6;    \
-        const T d0 = (T)0.1, d1 = (T)0.6, d2 = (T)0.3, six = (T)6;             \
-        const T a0 = FMA((T)-2, v1, v0) + v2;                                  \
-        const T b0 = FMA((T)3, v2, FMA((T)-4, v1, v0));                        \
-        const T a1 = FMA((T)-2, v2, v1) + v3;                                  \
-        const T b1 = v1 - v3;                                                  \
-        const T a2 = FMA((T)-2, v3, v2) + v4;                                  \
-        const T b2 = FMA((T)3, v2, FMA((T)-4, v3, v4));                        \
+        const T a0 = FMA((T)-2, u1, u0) + u2;                                  \
+        const T b0 = FMA((T)3, u2, FMA((T)-4, u1, u0));                        \
+        const T a1 = FMA((T)-2, u2, u1) + u3;                                  \
+        const T b1 = u1 - u3;                                                  \
+        const T a2 = FMA((T)-2, u3, u2) + u4;                                  \
+        const T b2 = FMA((T)3, u2, FMA((T)-4, u3, u4));                        \
         const T s0 = eps + FMA(c1312 * a0, a0, quarter * (b0 * b0));           \
         const T s1 = eps + FMA(c1312 * a1, a1, quarter * (b1 * b1));           \
         const T s2 = eps + FMA(c1312 * a2, a2, quarter * (b2 * b2));           \
         const T t0 = s0 * s0, t1 = s1 * s1, t2 = s2 * s2;                      \
-        const T w0 = d0 * (t1 * t2);                                           \
-        const T w1 = d1 * (t0 * t2);                                           \
-        const T w2 = d2 * (t0 * t1);                                           \
-        const T n0 = FMA((T)2, v0, FMA((T)-7, v1, (T)11 * v2));                \
-        const T n1 = FMA((T)5, v2, FMA((T)2, v3, -v1));                        \
-        const T n2 = FMA((T)2, v2, FMA((T)5, v3, -v4));                        \
+        *p12 = t1 * t2;                                                        \
+        *p02 = t0 * t2;                                                        \
+        *p01 = t0 * t1;                                                        \
+    }                                                                          \
+                                                                               \
+    /* left-biased state of cell j at j+1/2: linear weights 1/10, 6/10, 3/10  \
+     * on S0, S1, S2; value = num / den */                                     \
+    static inline void weno5_left_##SUF(T u0, T u1, T u2, T u3, T u4, T *num, T *den) \
+    {                                                                          \
+        T p12, p02, p01;                                                       \
+        weno5_beta_##SUF(u0, u1, u2, u3, u4, &p12, &p02, &p01);                \
+        const T w0 = (T)0.1 * p12, w1 = (T)0.6 * p02, w2 = (T)0.3 * p01;       \
+        const T n0 = FMA((T)2, u0, FMA((T)-7, u1, (T)11 * u2));                \
+        const T n1 = FMA((T)5, u2, FMA((T)2, u3, -u1));                        \
+        const T n2 = FMA((T)2, u2, FMA((T)5, u3, -u4));                        \
         *num = FMA(w0, n0, FMA(w1, n1, w2 * n2));                              \
-        *den = six * ((w0 + w1) + w2);                                         \
+        *den = (T)6 * ((w0 + w1) + w2);                                        \
+    }                                                                          \
+                                                                               \
+    /* right-biased state of cell j at j-1/2: linear weights 3/10, 6/10, 1/10 \
+     * on S0, S1, S2 */                                                        \
+    static inline void weno5_right_##SUF(T u0, T u1, T u2, T u3, T u4, T *num, T *den) \
+    {                                                                          \
+        T p12, p02, p01;                                                       \
+        weno5_beta_##SUF(u0, u1, u2, u3, u4, &p12, &p02, &p01);                \
+        const T r0 = (T)0.3 * p12, r1 = (T)0.6 * p02, r2 = (T)0.1 * p01;       \
+        const T m0 = FMA((T)5, u1, FMA((T)2, u2, -u0));                        \
+        const T m1 = FMA((T)2, u1, FMA((T)5, u2, -u3));                        \
+        const T m2 = FMA((T)2, u4, FMA((T)-7, u3, (T)11 * u2));                \
+        *num = FMA(r0, m0, FMA(r1, m1, r2 * m2));                              \
+        *den = (T)6 * ((r0 + r1) + r2);                                        \
     }                                                                          \
                                                                                \
     /* left and right states at the face between v2 and v3 (v0..v5 =         \
-     * v[i-2..i+3]); SHARED_DIV: one division for both, as the device's FP64  \
-     * path does, else one division each (FP32) */                            \
+     * v[i-2..i+3]): cell v2's left-biased and cell v3's right-biased state;  \
+     * SHARED_DIV: one division for both, as the device's FP64 path does,    \
+     * else one division each (FP32) */                                       \
     static inline void weno5_pair_##SUF(T v0, T v1, T v2, T v3, T v4, T v5,    \
                                         T *vl, T *vr)                          \
     {                                                                          \
         T nl, dl, nr, dr;                                                      \
-        weno5_nd_##SUF(v0, v1, v2, v3, v4, &nl, &dl);                          \
-        weno5_nd_##SUF(v5, v4, v3, v2, v1, &nr, &dr);                          \
+        weno5_left_##SUF(v0, v1, v2, v3, v4, &nl, &dl);                        \
+        weno5_right_##SUF(v1, v2, v3, v4, v5, &nr, &dr);                       \
         if (SHARED_DIV) {                                                      \
             const T inv = (T)1 / (dl * dr);                                    \
             *vl = (nl * dr) * inv;                                             \
