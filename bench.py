@@ -257,10 +257,14 @@ class C1:
         return self.cpu_sample_static(threads, reps=int(min(2000, max(1, 10.0 / t1))))
 
 
-# FP64/FP32 operations per cell and RK stage of the Euler kernel, each face
-# counted once (fma = 2, div = sqrt = 1): 3 faces x (10 WENO5 x 67 + Rusanov 72)
-# + primitive conversion 12 + flux differences 40 + stage update 20.
-EULER_FLOPS_PER_CELL_STAGE = 3 * (10 * 67 + 72) + 12 + 40 + 20
+# FP64/FP32 operations per cell and RK stage of the Euler kernel (fma = 2,
+# div = sqrt = 1), each cell and face counted once: per direction and
+# variable the cell's WENO5 smoothness indicators and weight products (42),
+# its left- and right-biased states (24 each) and the face's shared division
+# (6); per face the Rusanov flux (72); per cell the primitive conversion (12),
+# the flux differences (40) and the stage update (20).  Work the kernel
+# repeats at tile and run edges is not counted.
+EULER_FLOPS_PER_CELL_STAGE = 3 * (5 * (42 + 24 + 24 + 6) + 72) + 12 + 40 + 20
 
 
 def euler_host_state(nb, n, block_stride, gamma=1.4, seed=1234):
