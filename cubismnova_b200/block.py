@@ -85,7 +85,11 @@ class FieldLab:
                 for b in saved:
                     vec.push_back(b)
         self._field = grid.field(flat, comp)
-        self._range = IndexRange(ext)
+        # the device lab has the strides of the grid's largest lab; a node or
+        # face block that is not last along a grown direction is one smaller
+        self._layout = tuple(ext[d] - self._stencil.getBegin()[d] + self._stencil.getEnd()[d] - 1
+                             for d in range(3))
+        self._range = IndexRange(grid.block_extent(flat))
 
     def getActiveStencil(self):
         return self._stencil
@@ -111,10 +115,12 @@ class FieldLab:
 
     @property
     def data(self):
-        """Device tensor (Lz, Ly, Lx) of the active lab range."""
+        """Device tensor (Lz, Ly, Lx) of the active lab range (a view with the
+        strides of the grid's largest lab)."""
         lr = self.getActiveLabRange().getExtent()
-        n = lr[0] * lr[1] * lr[2]
-        return self._buf[:n].view(lr[2], lr[1], lr[0])
+        L = self._layout
+        n = L[0] * L[1] * L[2]
+        return self._buf[:n].view(L[2], L[1], L[0])[: lr[2], : lr[1], : lr[0]]
 
     def numpy(self):
         return self.data.cpu().numpy()

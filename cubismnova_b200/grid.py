@@ -85,7 +85,7 @@ class BlockField:
         return self._state
 
     def getIndexRange(self):
-        return IndexRange(self._g.getBlockExtent())
+        return IndexRange(self._g.block_extent(self.flat))
 
     def getBC(self):
         return BCVector(self._g, self.comp, self.flat)
@@ -110,16 +110,24 @@ class TensorBlock:
         return BlockField(self._g, self.flat, 0).getState()
 
     def getIndexRange(self):
-        return IndexRange(self._g.getBlockExtent())
+        return IndexRange(self._g.block_extent(self.flat))
 
 
 class Cartesian:
     """Grid::Cartesian(nblocks, block_cells, begin, end) with ``ncomp`` components.
 
     ``entity`` is the Cubism::EntityType of the values: "cell" (default),
-    "node", or one direction of a face container ("face_x", "face_y",
-    "face_z"); ``getBlockCells`` is the mesh, ``getBlockExtent`` the values
-    per block (cells + 1 for nodes and along the face direction)."""
+    "node", one direction of a face container ("face_x", "face_y",
+    "face_z"), or "face" for the whole container (a ``FaceCartesian``);
+    ``getBlockCells`` is the mesh, ``getBlockExtent`` the values per block
+    (cells + 1 for nodes and along the face direction)."""
+
+    def __new__(cls, *args, **kwargs):
+        entity = kwargs.get("entity", args[6] if len(args) > 6 else "cell")
+        if entity == "face":
+            kw = {k: v for k, v in kwargs.items() if k != "entity"}
+            return FaceCartesian(*args[:6], **kw)
+        return super().__new__(cls)
 
     def __init__(self, nblocks, block_cells, begin=(0.0, 0.0, 0.0), end=(1.0, 1.0, 1.0),
                  ncomp: int = 1, dtype=np.float64, entity: str = "cell"):
@@ -194,9 +202,19 @@ class Cartesian:
         return self._cells
 
     def getBlockExtent(self):
-        """Values per block and direction: the block field's index-range
-        extent (cells, or cells + 1 for nodes / along a face direction)."""
+        """Values per block and direction of the largest block field (cells,
+        or cells + 1 for nodes / along a face direction); the storage and lab
+        strides of every block follow it."""
         return self._n
+
+    def block_extent(self, flat):
+        """Index-range extent of block field ``flat``: node and face fields
+        hold cells + 1 entities along a grown direction only in the last block
+        of that direction (Grid/BlockFieldAssembler.h:124-135)."""
+        flat = self.flat_index(flat)
+        bi = (flat % self._nb[0], (flat // self._nb[0]) % self._nb[1], flat // (self._nb[0] * self._nb[1]))
+        cells = self.getBlockCells()
+        return tuple(self._n[d] if bi[d] == self._nb[d] - 1 else min(self._n[d], cells[d]) for d in range(3))
 
     def getCellSize(self):
         h = (C.c_double * 3)()
@@ -285,3 +303,100 @@ class Cartesian:
     def loadLab(self, field, lab, c=0, d=0):
         comp = field.comp if isinstance(field, BlockField) else int(c)
         lab.loadData(field.getState().block_index, self, comp=comp)
+
+
+class FaceContainerBlock:
+    """The FaceContainer of one block (Block/Field.h:1532-1670): ``[d]`` is the
+    face field of direction d, a scalar ``BlockField`` or, with several
+    components, a ``TensorBlock`` (``[d][c]``)."""
+
+    def __init__(self, fgrid, flat):
+        self._fg, self.flat = fgrid, flat
+
+    def __len__(self):
+        return 3
+
+    def __getitem__(self, d):
+        if not 0 <= d < 3:
+            raise IndexError("face direction out of range")
+        return self._fg.faces[d][self.flat]
+
+    def getState(self):
+        return self._fg.faces[0].field(self.flat, 0).getState()
+
+
+class FaceCartesian:
+    """Grid::Cartesian<T, Mesh, EntityType::Face, RANK>: every block holds a
+    FaceContainer of three face fields (directions x, y, z) with ``ncomp``
+    components each, kept as three face grids (``faces[d]``).  ``field(i, c,
+    d)``, ``getIndexFunctor(c, d)`` and ``loadLab(field, lab, c, d)`` follow
+    the reference's component map (block i, component c, direction d) ->
+    fields[i][d][c] (Block/FieldLabLoader.h:327-364, Grid/Cartesian.h:384-427).
+    Created by ``Cartesian(..., entity="face")``."""
+
+    entity = "face"
+
+    def __init__(self, nblocks, block_cells, begin=(0.0, 0.0, 0.0), end=(1.0, 1.0, 1.0),
+                 ncomp: int = 1, dtype=np.float64):
+        self.faces = tuple(Cartesian(nblocks, block_cells, begin, end, ncomp=ncomp, dtype=dtype,
+                                     entity="face_" + a) for a in "xyz")
+        self.ncomp = self.faces[0].ncomp
+        self.dtype = self.faces[0].dtype
+
+    def close(self):
+        for f in self.faces:
+            f.close()
+
+    def size(self):
+        return self.faces[0].size()
+
+    def getSize(self):
+        return self.faces[0].getSize()
+
+    def getBlockCells(self):
+        return self.faces[0].getBlockCells()
+
+    def getBlockExtent(self, d):
+        """Values per block of the face field of direction d (cells + 1 along d)."""
+        return self.faces[d].getBlockExtent()
+
+    def getCellSize(self):
+        return self.faces[0].getCellSize()
+
+    def flat_index(self, p):
+        return self.faces[0].flat_index(p)
+
+    def __getitem__(self, p):
+        return FaceContainerBlock(self, self.flat_index(p))
+
+    def __iter__(self):
+        for i in range(self.size()):
+            yield self[i]
+
+    def field(self, block, comp=0, d=0):
+        return self.faces[d].field(block, comp)
+
+    def getIndexFunctor(self, c=0, d=0):
+        g = self.faces[d]
+        return lambda p: g.field(p, c)
+
+    def loadLab(self, field, lab, c=0, d=0):
+        """Lab of component c of the face field of direction d of the block of
+        ``field`` (a FaceContainerBlock or any block field of this grid)."""
+        lab.loadData(field.getState().block_index, self.faces[d], comp=int(c))
+
+    def upload(self, host, comp=0, d=0, stream=None):
+        self.faces[d].upload(host, comp, stream)
+
+    def download(self, comp=0, d=0):
+        return self.faces[d].download(comp)
+
+    def push_boundary_bc(self, bc_factory, dir, side, comp=0, d=None):
+        """BCs on the boundary blocks of the face fields of direction d (all
+        three directions when d is None)."""
+        for dd in (range(3) if d is None else (d,)):
+            self.faces[dd].push_boundary_bc(bc_factory, dir, side, comp)
+
+    def sync_bcs(self, stream=None):
+        for f in self.faces:
+            f.sync_bcs(stream)

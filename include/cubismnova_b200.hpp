@@ -22,6 +22,7 @@
 #include "cubismnova_b200.h"
 
 #include <array>
+#include <functional>
 #include <cstddef>
 #include <memory>
 #include <stdexcept>
@@ -229,6 +230,44 @@ private:
     std::vector<std::unique_ptr<BC::Base>> owned_;
 };
 
+/// Grid::Cartesian<T, Mesh, EntityType::Face, RANK>: every block holds a
+/// FaceContainer of three face fields, one per direction, with `ncomp`
+/// components each (Block/Field.h:1532-1670), kept as three face grids.
+/// field(i, c, d) and getIndexFunctor(c, d) follow the reference's component
+/// map (block i, component c, direction d) -> fields[i][d][c]
+/// (Block/FieldLabLoader.h:327-364, Grid/Cartesian.h:384-427).
+template <typename T> class FaceCartesian {
+public:
+    FaceCartesian(const MultiIndex &nblocks, const MultiIndex &block_cells,
+                  const std::array<double, 3> &begin = {0, 0, 0}, const std::array<double, 3> &end = {1, 1, 1},
+                  int ncomp = 1)
+        : fx_(nblocks, block_cells, begin, end, ncomp, CN_ENTITY_FACE_X),
+          fy_(nblocks, block_cells, begin, end, ncomp, CN_ENTITY_FACE_Y),
+          fz_(nblocks, block_cells, begin, end, ncomp, CN_ENTITY_FACE_Z)
+    {
+    }
+    size_t size() const { return fx_.size(); }
+    MultiIndex getSize() const { return fx_.getSize(); }
+    MultiIndex getBlockCells() const { return fx_.getBlockCells(); }
+    std::array<double, 3> getCellSize() const { return fx_.getCellSize(); }
+    /// the face grid of direction d (0, 1, 2)
+    Cartesian<T> &face(int d)
+    {
+        if (d < 0 || d > 2) throw std::out_of_range("FaceCartesian: face direction out of range");
+        return d == 0 ? fx_ : (d == 1 ? fy_ : fz_);
+    }
+    BlockField<T> field(size_t i, int c = 0, int d = 0) { return face(d).field(i, c); }
+    /// block multi-index -> component c of the face field of direction d
+    std::function<BlockField<T>(const MultiIndex &)> getIndexFunctor(int c = 0, int d = 0)
+    {
+        Cartesian<T> *g = &face(d);
+        return [g, c](const MultiIndex &p) { return g->field((size_t)g->flatIndex(p), c); };
+    }
+
+private:
+    Cartesian<T> fx_, fy_, fz_;
+};
+
 template <typename T> void BCVector<T>::push_back(BC::Base *bc)
 {
     check(cn_bc_push(g_->raw(), comp_, block_, (int)bc->dir, (int)bc->side, bc->kind(), bc->value()));
@@ -318,7 +357,8 @@ public:
         return field_;
     }
     Core::IndexRange getMaximumRange() const { return max_; }
-    /// device pointer of the lab (active lab range, x fastest)
+    /// device pointer of the lab (active lab range from getActiveLabRange(),
+    /// x fastest, with the strides of the grid's largest lab: cn_lab_extent)
     T *deviceData() { return static_cast<T *>(buf_); }
 
 private:

@@ -106,6 +106,56 @@ int main()
         }
     EXPECT(lab.getActiveLabRange().getBegin()[0] == -3 && lab.getActiveLabRange().getEnd()[2] == 19);
     EXPECT(lab.getActiveField() == 0);
+    // FaceContainer grid, rank 1 (CartesianTest.cpp:85-103): three face grids;
+    // the component map (i, c, d) -> fields[i][d][c] (FieldLabLoader.h:327-364)
+    // and the periodic identities of a one-block face lab (FieldLabTest.cpp:
+    // 107-114): along its own direction a face field has cells + 1 entities
+    {
+        Grid::FaceCartesian<int> fg({1, 1, 1}, {4, 4, 4}, {0, 0, 0}, {1, 1, 1}, 2);
+        EXPECT(fg.size() == 1);
+        Block::FieldLab<int> flab;
+        flab.allocate(Core::Stencil(-1, 2), fg.field(0, 0, 0).getIndexRange());
+        for (int d = 0; d < 3; ++d) {
+            Grid::Cartesian<int> &gd = fg.face(d);
+            EXPECT(gd.getEntity() == CN_ENTITY_FACE_X + d);
+            const MultiIndex e = gd.getBlockExtent(0);
+            for (int k = 0; k < 3; ++k) EXPECT(e[k] == (k == d ? 5 : 4));
+            for (int c = 0; c < 2; ++c) {
+                std::vector<int> hv(gd.componentStride());
+                for (size_t i = 0; i < hv.size(); ++i) hv[i] = (int)(10000 * (d + 1) + 1000 * c + i);
+                gd.upload(hv.data(), c);
+                Grid::BlockField<int> f = fg.getIndexFunctor(c, d)({0, 0, 0});
+                EXPECT(f.comp() == c && &f.grid() == &gd && f.flat() == 0);
+                flab.loadData(f);
+                const int E0 = e[0] + 2, E1 = e[1] + 2, E2 = e[2] + 2;
+                std::vector<int> lv((size_t)E0 * E1 * E2);
+                check(cn_memcpy(lv.data(), flab.deviceData(), sizeof(int) * lv.size(), nullptr));
+                auto L = [&](int x, int y, int z) { return lv[(x + 1) + E0 * ((y + 1) + E1 * (z + 1))]; };
+                auto F = [&](int x, int y, int z) { return hv[x + e[0] * (y + e[1] * z)]; };
+                for (int z = 0; z < e[2]; ++z)
+                    for (int y = 0; y < e[1]; ++y) {
+                        EXPECT(L(-1, y, z) == F(e[0] - 1, y, z));
+                        EXPECT(L(e[0], y, z) == F(0, y, z));
+                        for (int x = 0; x < e[0]; ++x) EXPECT(L(x, y, z) == F(x, y, z));
+                    }
+                for (int z = 0; z < e[2]; ++z)
+                    for (int x = 0; x < e[0]; ++x) {
+                        EXPECT(L(x, -1, z) == F(x, e[1] - 1, z));
+                        EXPECT(L(x, e[1], z) == F(x, 0, z));
+                    }
+                for (int y = 0; y < e[1]; ++y)
+                    for (int x = 0; x < e[0]; ++x) {
+                        EXPECT(L(x, y, -1) == F(x, y, e[2] - 1));
+                        EXPECT(L(x, y, e[2]) == F(x, y, 0));
+                    }
+            }
+        }
+        try {
+            fg.face(3);
+            EXPECT(false);
+        } catch (const std::out_of_range &) {
+        }
+    }
     std::printf("%s (%d failures)\n", failures ? "FAIL" : "PASS", failures);
     return failures ? 1 : 0;
 }
