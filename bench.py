@@ -259,12 +259,14 @@ class C1:
 
 # FP64/FP32 operations per cell and RK stage of the Euler kernel (fma = 2,
 # div = sqrt = 1), each cell and face counted once: per direction and
-# variable the cell's WENO5 smoothness indicators and weight products (42),
-# its left- and right-biased states (24 each) and the face's shared division
-# (6); per face the Rusanov flux (72); per cell the primitive conversion (12),
-# the flux differences (40) and the stage update (20).  Work the kernel
+# variable the cell's WENO5 smoothness indicators and weight products (42)
+# and its left- and right-biased states (24 each); per face the divisions of
+# the five variables' states (FP64: variables paired, 2 x 14 + 6 = 34; FP32:
+# 5 x 6 = 30) and the Rusanov flux (74); per cell the primitive conversion
+# (12), the flux differences (40) and the stage update (20).  Work the kernel
 # repeats at tile and run edges is not counted.
-EULER_FLOPS_PER_CELL_STAGE = 3 * (5 * (42 + 24 + 24 + 6) + 72) + 12 + 40 + 20
+EULER_FLOPS_PER_CELL_STAGE = {"f64": 3 * (5 * (42 + 24 + 24) + 34 + 74) + 12 + 40 + 20,
+                              "f32": 3 * (5 * (42 + 24 + 24) + 30 + 74) + 12 + 40 + 20}
 
 
 def euler_host_state(nb, n, block_stride, gamma=1.4, seed=1234):
@@ -335,7 +337,7 @@ class Euler:
         self.dt = cn.euler.cfl_dt(self.U, 0.3)
         self.cells = int(np.prod(self.nb)) * int(np.prod(self.n))
         self.updates_per_step = self.cells * self.stages
-        self.flops_per_cell_stage = EULER_FLOPS_PER_CELL_STAGE
+        self.flops_per_cell_stage = EULER_FLOPS_PER_CELL_STAGE[self.dtype]
         self.h_state = None
 
     def needs_flush(self):
@@ -523,7 +525,7 @@ class C3:
         cn.workloads.euler_pulse_amr(self.U)
         self.cells = self.U.total_cells
         self.updates_per_step = self.cells * self.stages
-        self.flops_per_cell_stage = EULER_FLOPS_PER_CELL_STAGE
+        self.flops_per_cell_stage = EULER_FLOPS_PER_CELL_STAGE[self.dtype]
         self.nb, self.n = (len(l),), (int(F),)
         # CFL on the fine level (h = 1/F), sound speed of the pulse state < 1.3
         self.dt = 0.3 / (3 * 1.3 * F)

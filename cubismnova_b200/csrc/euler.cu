@@ -29,7 +29,7 @@ namespace cn {
 namespace euler {
 
 template <typename T>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) stage_kernel(StageParams<T> p, CartSrc src)
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 3) stage_kernel(StageParams<T> p, CartSrc src)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *W = reinterpret_cast<T *>(smem_raw); // [5][Stg<T>::SV]

@@ -115,6 +115,23 @@ __device__ __forceinline__ void face_states(float nl, float dl, float nr, float 
     vr = nr / dr;
 }
 
+// FP64: two variables' face states from one division (a = first, b = second
+// variable):  inv = 1/((dla*dra)*(dlb*drb)), q_a = (dlb*drb)*inv = 1/(dla*dra),
+// q_b = (dla*dra)*inv.  The product of four denominators stays in range: each
+// lies in [6e-25, 6 B^4] for smoothness indicators up to B, so up to B ~ 1e19.
+__device__ __forceinline__ void face_states2(double nla, double dla, double nra, double dra, double nlb, double dlb,
+                                             double nrb, double drb, double &vla, double &vra, double &vlb,
+                                             double &vrb)
+{
+    const double Da = dla * dra, Db = dlb * drb;
+    const double inv = 1.0 / (Da * Db);
+    const double qa = Db * inv, qb = Da * inv;
+    vla = (nla * dra) * qa;
+    vra = (nra * dla) * qa;
+    vlb = (nlb * drb) * qb;
+    vrb = (nrb * dlb) * qb;
+}
+
 // Rusanov flux through a face with normal direction `d` (0,1,2) from the
 // reconstructed primitive states WL, WR = (rho, u, v, w, p).
 template <typename T>
@@ -135,8 +152,10 @@ __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int 
     const T El = dfma(C::half * rl, kel, pl * igm1);
     const T Er = dfma(C::half * rr, ker, pr * igm1);
     // wave speeds
-    const T cl = dsqrt((gamma * pl) / rl);
-    const T cr = dsqrt((gamma * pr) / rr);
+    // one division for both sound speeds
+    const T irr = T(1) / (rl * rr);
+    const T cl = dsqrt(((gamma * pl) * rr) * irr);
+    const T cr = dsqrt(((gamma * pr) * rl) * irr);
     const T a = dmax(dabs(unl) + cl, dabs(unr) + cr);
     // physical fluxes
     const T fl0 = rl * unl, fr0 = rr * unr;

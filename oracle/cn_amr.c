@@ -151,12 +151,13 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double 
                     for (int y = 0; y < E1; ++y)
                         for (int x = 0; x < E0; ++x) {
                             const ptrdiff_t li = (x + 3) + (ptrdiff_t)L * ((y + 3) + (ptrdiff_t)L * (z + 3));
-                            double WL[5], WR[5], F[5];
+                            double WL[5], WR[5], F[5], nl[5], dl[5], nr[5], dr[5];
                             for (int c = 0; c < 5; ++c) {
                                 const double *P = prim + c * le + li;
-                                weno5_pair_f64(P[-3 * st], P[-2 * st], P[-st], P[0], P[st], P[2 * st], &WL[c],
-                                               &WR[c]);
+                                weno5_nd_face_f64(P[-3 * st], P[-2 * st], P[-st], P[0], P[st], P[2 * st], &nl[c],
+                                                  &dl[c], &nr[c], &dr[c]);
                             }
+                            face_states5_f64(nl, dl, nr, dr, WL, WR);
                             rusanov_f64(WL, WR, d, gamma, igm1, F);
                             const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
                             for (int c = 0; c < 5; ++c)

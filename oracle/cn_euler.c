@@ -67,13 +67,14 @@
                         /* face between cell (x,y,z)-e_d and (x,y,z) */        \
                         const ptrdiff_t li = (x + 3) + (ptrdiff_t)L0 *         \
                                              ((y + 3) + (ptrdiff_t)L1 * (z + 3)); \
-                        T WL[5], WR[5], F[5];                                  \
+                        T WL[5], WR[5], F[5], nl[5], dl[5], nr[5], dr[5];      \
                         for (int c = 0; c < 5; ++c) {                          \
                             const T *P = prim + c * le + li;                   \
                             const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st]; \
                             const T v3 = P[0], v4 = P[st], v5 = P[2 * st];     \
-                            weno5_pair_##SUF(v0, v1, v2, v3, v4, v5, &WL[c], &WR[c]); \
+                            weno5_nd_face_##SUF(v0, v1, v2, v3, v4, v5, &nl[c], &dl[c], &nr[c], &dr[c]); \
                         }                                                      \
+                        face_states5_##SUF(nl, dl, nr, dr, WL, WR);            \
                         rusanov_##SUF(WL, WR, d, gamma, igm1, F);              \
                         const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z); \
                         for (int c = 0; c < 5; ++c)                            \

@@ -63,23 +63,41 @@
         *den = (T)6 * ((r0 + r1) + r2);                                        \
     }                                                                          \
                                                                                \
-    /* left and right states at the face between v2 and v3 (v0..v5 =         \
-     * v[i-2..i+3]): cell v2's left-biased and cell v3's right-biased state;  \
-     * SHARED_DIV: one division for both, as the device's FP64 path does,    \
-     * else one division each (FP32) */                                       \
-    static inline void weno5_pair_##SUF(T v0, T v1, T v2, T v3, T v4, T v5,    \
-                                        T *vl, T *vr)                          \
+    /* the two reconstructions at the face between v2 and v3 (v0..v5 =      \
+     * v[i-2..i+3]): cell v2's left-biased and cell v3's right-biased state   \
+     * as numerators and denominators */                                      \
+    static inline void weno5_nd_face_##SUF(T v0, T v1, T v2, T v3, T v4, T v5, \
+                                           T *nl, T *dl, T *nr, T *dr)         \
     {                                                                          \
-        T nl, dl, nr, dr;                                                      \
-        weno5_left_##SUF(v0, v1, v2, v3, v4, &nl, &dl);                        \
-        weno5_right_##SUF(v1, v2, v3, v4, v5, &nr, &dr);                       \
+        weno5_left_##SUF(v0, v1, v2, v3, v4, nl, dl);                          \
+        weno5_right_##SUF(v1, v2, v3, v4, v5, nr, dr);                         \
+    }                                                                          \
+                                                                               \
+    /* face states of the 5 variables from their numerators and denominators. \
+     * SHARED_DIV (FP64, as the device): variables (0,1) and (2,3) share one  \
+     * division for their four states, variable 4 one for its two; FP32       \
+     * divides each state on its own (the products could leave the range) */   \
+    static inline void face_states5_##SUF(const T *nl, const T *dl, const T *nr, \
+                                          const T *dr, T *WL, T *WR)           \
+    {                                                                          \
         if (SHARED_DIV) {                                                      \
-            const T inv = (T)1 / (dl * dr);                                    \
-            *vl = (nl * dr) * inv;                                             \
-            *vr = (nr * dl) * inv;                                             \
+            for (int c = 0; c < 4; c += 2) {                                   \
+                const T Da = dl[c] * dr[c], Db = dl[c + 1] * dr[c + 1];        \
+                const T inv = (T)1 / (Da * Db);                                \
+                const T qa = Db * inv, qb = Da * inv;                          \
+                WL[c] = (nl[c] * dr[c]) * qa;                                  \
+                WR[c] = (nr[c] * dl[c]) * qa;                                  \
+                WL[c + 1] = (nl[c + 1] * dr[c + 1]) * qb;                      \
+                WR[c + 1] = (nr[c + 1] * dl[c + 1]) * qb;                      \
+            }                                                                  \
+            const T inv = (T)1 / (dl[4] * dr[4]);                              \
+            WL[4] = (nl[4] * dr[4]) * inv;                                     \
+            WR[4] = (nr[4] * dl[4]) * inv;                                     \
         } else {                                                               \
-            *vl = nl / dl;                                                     \
-            *vr = nr / dr;                                                     \
+            for (int c = 0; c < 5; ++c) {                                      \
+                WL[c] = nl[c] / dl[c];                                         \
+                WR[c] = nr[c] / dr[c];                                         \
+            }                                                                  \
         }                                                                      \
     }                                                                          \
                                                                                \
@@ -96,8 +114,10 @@
         const T ker = FMA(WR[1], WR[1], FMA(WR[2], WR[2], WR[3] * WR[3]));     \
         const T El = FMA(half * rl, kel, pl * igm1);                           \
         const T Er = FMA(half * rr, ker, pr * igm1);                           \
-        const T cl = SQRT((gamma * pl) / rl);                                  \
-        const T cr = SQRT((gamma * pr) / rr);                                  \
+        /* one division for both sound speeds */                               \
+        const T irr = (T)1 / (rl * rr);                                        \
+        const T cl = SQRT(((gamma * pl) * rr) * irr);                          \
+        const T cr = SQRT(((gamma * pr) * rl) * irr);                          \
         const T a = FMAX(FABS(unl) + cl, FABS(unr) + cr);                      \
         const T fl0 = rl * unl, fr0 = rr * unr;                                \
         T fl1 = mul0 * unl, fr1 = mur0 * unr;                                  \

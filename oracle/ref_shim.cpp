@@ -231,13 +231,14 @@ double eulerStage<double>(const int nb[3], const int n[3], const double *Us, con
                         for (int y = 0; y < E1; ++y)
                             for (int x = 0; x < E0; ++x) {
                                 const ptrdiff_t li = (x + 3) + (ptrdiff_t)L0 * ((y + 3) + (ptrdiff_t)L1 * (z + 3));
-                                T WL[5], WR[5], F[5];
+                                T WL[5], WR[5], F[5], nl[5], dl[5], nr[5], dr[5];
                                 for (int c = 0; c < 5; ++c) {
                                     const T *P = prim.data() + c * le + li;
                                     const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st];
                                     const T v3 = P[0], v4 = P[st], v5 = P[2 * st];
-                                    weno5_pair_f64(v0, v1, v2, v3, v4, v5, &WL[c], &WR[c]);
+                                    weno5_nd_face_f64(v0, v1, v2, v3, v4, v5, &nl[c], &dl[c], &nr[c], &dr[c]);
                                 }
+                                face_states5_f64(nl, dl, nr, dr, WL, WR);
                                 rusanov_f64(WL, WR, d, gam, igm1, F);
                                 const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
                                 for (int c = 0; c < 5; ++c) flux[c * nf + fi] = F[c];
