@@ -32,12 +32,13 @@ struct Src {
         t.bx = t.by = t.bz = 0;
     }
     template <typename T> __device__ __forceinline__ void prepare(const euler::TileInfo<T> &, int *) const {}
-    // interface ghosts are never a plain copy of one neighbour cell
+    // a ghost from a block on the same level is a plain copy of its cell;
+    // level-interface ghosts (prolongation, restriction) take halo()
     template <typename T>
-    __device__ __forceinline__ bool plain_offset(const euler::TileInfo<T> &, int, int, int, const int *,
-                                                 int64_t &) const
+    __device__ __forceinline__ bool plain_offset(const euler::TileInfo<T> &t, int gx, int gy, int gz, const int *,
+                                                 int64_t &off) const
     {
-        return false;
+        return same_level_offset(A, t.block, gx, gy, gz, off);
     }
     template <typename T>
     __device__ __forceinline__ T halo(const T *comp, int, const euler::TileInfo<T> &t, int gx, int gy, int gz,

@@ -46,6 +46,22 @@ __device__ __forceinline__ T cell(const T *comp, const BlockDev &B, int x, int y
     return comp[B.off + x + (int64_t)B.n * (y + (int64_t)B.n * z)];
 }
 
+// Element offset (in every component) of lab cell q of block b, outside b,
+// when the block covering it is on b's level: the ghost is a plain copy of
+// that cell, as value() gives it.  False for level-interface ghosts.
+__device__ __forceinline__ bool same_level_offset(const Geom &A, int b, int qx, int qy, int qz, int64_t &off)
+{
+    const BlockDev B = A.blk[b];
+    const int cs = B.level == 0 ? 2 : 1;
+    const int X = wrap(B.ox + qx * cs, A.L1), Y = wrap(B.oy + qy * cs, A.L1), Z = wrap(B.oz + qz * cs, A.L1);
+    const int s = A.lookup[(X >> 3) + A.lres * ((Y >> 3) + A.lres * (Z >> 3))];
+    const BlockDev S = A.blk[s];
+    if (S.level != B.level) return false;
+    const int fx = (X - S.ox) / cs, fy = (Y - S.oy) / cs, fz = (Z - S.oz) / cs;
+    off = S.off + fx + (int64_t)S.n * (fy + (int64_t)S.n * fz);
+    return true;
+}
+
 // value of lab cell q (tile coordinates of block b, possibly outside it)
 template <typename T>
 __device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, int qy, int qz)
