@@ -37,6 +37,11 @@ struct BcView {
     const int32_t *off;  // nblocks+1 offsets (CSR)
     const DevBC *ent;    // entries
     const uint8_t *mode; // nblocks summaries
+    // nblocks face masks: bit 2d+s set if face (d, s) of the block carries a
+    // BC other than Base or its neighbour across that face is skipped; a
+    // ghost outside the block across one clear face is the plain periodic
+    // neighbour's cell
+    const uint8_t *faces;
 };
 
 struct HostBC {

@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 3) stage_kernel(Stage
     T *W = reinterpret_cast<T *>(smem_raw); // [5][Stg<T>::SV]
     T *F = W + 5 * Stg<T>::SV;              // [5][NFACE]
     __shared__ double red[NT / 32][5];
-    __shared__ int snb[28];
+    __shared__ int snb[29];
     __shared__ TileInfo<T> ts;
     stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, F, red, snb, &ts);
 }

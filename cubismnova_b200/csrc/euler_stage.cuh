@@ -101,7 +101,8 @@ struct CartSrc {
     // Per tile, in shared memory (a barrier must follow): snb[0..26] the 27
     // periodic neighbour blocks of the tile's block (index (r0+1) + 3 (r1+1) +
     // 9 (r2+1)), snb[27] the mask of the components whose block carries
-    // neither BCs nor skip flags (lab mode byte 0).
+    // neither BCs nor skip flags (lab mode byte 0), snb[28] the union over
+    // the components of the block's face masks (BcView::faces).
     template <typename T>
     __device__ __forceinline__ void prepare(const TileInfo<T> &t, int *snb) const
     {
@@ -114,23 +115,32 @@ struct CartSrc {
             snb[q] = nx + L.nb[0] * (ny + L.nb[1] * nz);
         }
         if (threadIdx.x == 32) {
-            unsigned plain = 0;
+            unsigned plain = 0, faces = 0;
 #pragma unroll
-            for (int c = 0; c < 5; ++c)
+            for (int c = 0; c < 5; ++c) {
                 plain |= (__ldg(bc[c].mode + t.block) == 0 ? 1u : 0u) << c;
+                faces |= __ldg(bc[c].faces + t.block);
+            }
             snb[27] = (int)plain;
+            snb[28] = (int)faces;
         }
     }
     // Element offset (in every component) of a halo cell outside the tile's
-    // block when all five components are plain: the periodic neighbour's
-    // cell, what cn::lab_value gives for mode 0.  False otherwise.
+    // block when it is the periodic neighbour's cell in all five components
+    // (what cn::lab_value gives): every component's block is plain (mode 0),
+    // or the cell lies across one face that carries no BC other than Base
+    // and no skip flag in any component.  False otherwise.
     template <typename T>
     __device__ __forceinline__ bool plain_offset(const TileInfo<T> &t, int gx, int gy, int gz, const int *snb,
                                                  int64_t &off) const
     {
-        if (snb[27] != 31) return false;
         const int r0 = gx < 0 ? -1 : (gx >= L.n[0] ? 1 : 0), r1 = gy < 0 ? -1 : (gy >= L.n[1] ? 1 : 0),
                   r2 = gz < 0 ? -1 : (gz >= L.n[2] ? 1 : 0);
+        if (snb[27] != 31) {
+            if ((r0 != 0) + (r1 != 0) + (r2 != 0) != 1) return false;
+            const int bit = r0 != 0 ? (r0 < 0 ? 0 : 1) : (r1 != 0 ? (r1 < 0 ? 2 : 3) : (r2 < 0 ? 4 : 5));
+            if ((snb[28] >> bit) & 1) return false;
+        }
         const int sb = snb[(r0 + 1) + 3 * (r1 + 1) + 9 * (r2 + 1)];
         off = (int64_t)sb * L.bstride + (gx - r0 * L.n[0]) +
               (int64_t)L.n[0] * ((gy - r1 * L.n[1]) + (int64_t)L.n[1] * (gz - r2 * L.n[2]));

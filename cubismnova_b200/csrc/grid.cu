@@ -70,6 +70,19 @@ cn_status check_lab(const cn_grid *g, const cn_stencil *s)
     return CN_OK;
 }
 
+static uint8_t faces_of(const std::vector<HostBC> &v, uint8_t mode)
+{
+    uint8_t f = 0;
+    for (const HostBC &b : v)
+        if (b.kind != CN_BC_BASE) f |= (uint8_t)(1u << (2 * b.dir + b.side));
+    for (int d = 0; d < 3; ++d) {
+        const int c = (mode >> (2 * d)) & 3;
+        if (c == 1) f |= (uint8_t)(1u << (2 * d));
+        if (c == 2) f |= (uint8_t)(1u << (2 * d + 1));
+    }
+    return f;
+}
+
 static uint8_t mode_of(const std::vector<HostBC> &v)
 {
     int periodic[3] = {1, 1, 1};
@@ -94,7 +107,8 @@ cn_status sync_bc(cn_grid *g, cudaStream_t stream)
     }
     const int nb = g->nblocks;
     std::vector<int32_t> off((size_t)g->ncomp * (nb + 1));
-    std::vector<uint8_t> mode((size_t)g->ncomp * nb);
+    // mode summaries [comp][block], then face masks [comp][block]
+    std::vector<uint8_t> mode((size_t)2 * g->ncomp * nb);
     std::vector<DevBC> ent;
     for (int c = 0; c < g->ncomp; ++c) {
         // offsets are relative to the component's first entry
@@ -112,6 +126,7 @@ cn_status sync_bc(cn_grid *g, cudaStream_t stream)
             }
             o[b + 1] = (int32_t)(ent.size() - base);
             mode[(size_t)c * nb + b] = mode_of(v);
+            mode[(size_t)(g->ncomp + c) * nb + b] = faces_of(v, mode[(size_t)c * nb + b]);
         }
     }
     // per-component entry bases are folded into separate pointers by bc_view
@@ -157,6 +172,7 @@ BcView bc_view(const cn_grid *g, int comp)
     v.off = g->d_bc_off + (size_t)comp * (g->nblocks + 1);
     v.ent = g->d_bc_ent;
     v.mode = g->d_bc_mode + (size_t)comp * g->nblocks;
+    v.faces = g->d_bc_mode + (size_t)(g->ncomp + comp) * g->nblocks;
     return v;
 }
 
@@ -297,13 +313,13 @@ cn_status cn_grid_create_entity(const int nblocks[3], const int block_cells[3], 
     e = cudaMalloc(&g->d_data, total);
     if (e == cudaSuccess) e = cudaMemset(g->d_data, 0, total);
     if (e == cudaSuccess) e = cudaMalloc(&g->d_bc_off, sizeof(int32_t) * ncomp * (nbl + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&g->d_bc_mode, (size_t)ncomp * nbl);
+    if (e == cudaSuccess) e = cudaMalloc(&g->d_bc_mode, (size_t)2 * ncomp * nbl);
     if (e == cudaSuccess) e = cudaMalloc(&g->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(g->d_err, 0, sizeof(int));
     // valid empty BC tables from the start: every kernel may read them, even
     // on a grid whose BCs were never pushed or synchronised
     if (e == cudaSuccess) e = cudaMemset(g->d_bc_off, 0, sizeof(int32_t) * ncomp * (nbl + 1));
-    if (e == cudaSuccess) e = cudaMemset(g->d_bc_mode, 0, (size_t)ncomp * nbl);
+    if (e == cudaSuccess) e = cudaMemset(g->d_bc_mode, 0, (size_t)2 * ncomp * nbl);
     if (e == cudaSuccess) e = cudaMalloc(&g->d_bc_ent, sizeof(cn::DevBC));
     if (e == cudaSuccess) e = cudaMemset(g->d_bc_ent, 0, sizeof(cn::DevBC));
     if (e == cudaSuccess) g->bc_ent_cap = 1;
