@@ -139,19 +139,39 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) jacobi_kernel(cons
     const int64_t oz = (int64_t)L.n[0] * L.n[1];
     int64_t c = dense_cell(L, q, x, y, z0);
     int u = ridx(q, x, y, z0);
-    for (int k = 0; k < zl; ++k, c += oz, u += st[2]) {
-        const int64_t o = (int64_t)q.block * L.bstride + c;
-        const float *cv = a.coef + ((int64_t)q.block * cells + c) * kCoefPerCell;
-        const float fc = __ldg(f + o);
-        if (pin) {
-            float Lp, D, pc;
-            op7_coef<float, float>(sp, u, st, cv, a.ih2, Lp, D, pc);
-            pout[o] = pc + omega * ((Lp - fc) / D);
-        } else {
-            // zero guess: L 0 = 0, only the diagonal is used
-            const float D = __ldg(cv + 6);
-            pout[o] = 0.0f + omega * ((0.0f - fc) / D);
+    const float4 *cv = reinterpret_cast<const float4 *>(a.coef + ((int64_t)q.block * cells + c) * kCoefPerCell);
+    const int64_t cvz = oz * kCoefPerCell / 4;
+    int64_t o = (int64_t)q.block * L.bstride + c;
+    // the next cell's loads go out before this cell's store
+    float4 ca = __ldg(cv), cb = __ldg(cv + 1);
+    float fc = __ldg(f + o);
+    for (int k = 0; k < zl; ++k, u += st[2]) {
+        float4 na = ca, nb = cb;
+        float nf = fc;
+        if (k + 1 < zl) {
+            na = __ldg(cv + cvz);
+            nb = __ldg(cv + cvz + 1);
+            nf = __ldg(f + o + oz);
         }
+        if (pin) {
+            const float cc[8] = {ca.x, ca.y, ca.z, ca.w, cb.x, cb.y, cb.z, cb.w};
+            const float pc = sp[u];
+            float fl[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float kp = cc[d], km = cc[3 + d];
+                fl[d] = kp * (sp[u + st[d]] - pc) - km * (pc - sp[u - st[d]]);
+            }
+            const float Lp = a.ih2 * ((fl[0] + fl[1]) + fl[2]);
+            pout[o] = pc + omega * ((Lp - fc) / cb.z);
+        } else {
+            pout[o] = 0.0f + omega * ((0.0f - fc) / cb.z);
+        }
+        ca = na;
+        cb = nb;
+        fc = nf;
+        cv += cvz;
+        o += oz;
     }
 }
 

@@ -100,7 +100,7 @@ constexpr int kTileCap[3] = {32, 8, 4};
 // the in-block part of a row starts 16-byte aligned (vector staging)
 constexpr int kRegionMax = (32 + 8) * (8 + 2) * (4 + 2); // 2400
 constexpr int kTileThreads = 256;
-constexpr int kTileMinCtas = 4; // resident CTAs per SM the tile kernels are compiled for (<= 64 registers)
+constexpr int kTileMinCtas = 6; // resident CTAs per SM the tile kernels are compiled for (<= 40 registers)
 
 inline int tile_extent(int n, int cap)
 {
