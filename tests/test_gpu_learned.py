@@ -56,10 +56,18 @@ def test_training_and_learned_multigrid(cn):
     assert l1 < l0
     p64 = cn.Grid.Cartesian(nb, n, dtype=np.float64)
     cyc_plain, rel_plain = m.solve(f, p64, rtol=1e-8, max_cycles=60)
-    # the network was trained on finest-level residuals: it replaces Jacobi there
+    # what training gains: the same network untrained (near-zero weights,
+    # i.e. damped Jacobi) against the trained one, both replacing Jacobi on
+    # the finest level, where the training residuals came from
+    untrained = cn.learned.LearnedSmoother(seed=1, omega=0.8, init_scale=1e-3)
+    cn.learned.use_in(m, untrained, level_mask=0x1)
+    cyc_u, rel_u = m.solve(f, p64, rtol=1e-8, max_cycles=60)
     cn.learned.use_in(m, nn, level_mask=0x1)
     cyc_nn, rel_nn = m.solve(f, p64, rtol=1e-8, max_cycles=60)
-    print(f"plain: {cyc_plain} cycles ({rel_plain:.2e}); learned: {cyc_nn} cycles ({rel_nn:.2e})")
-    assert rel_nn <= 1e-8
+    print(f"plain: {cyc_plain} cycles ({rel_plain:.2e}); untrained: {cyc_u} ({rel_u:.2e}); "
+          f"trained: {cyc_nn} cycles ({rel_nn:.2e})")
+    assert rel_nn <= 1e-8 and rel_u <= 1e-8 and rel_plain <= 1e-8
     rr, ff = m.residual(p64, f)
     assert np.sqrt(rr / ff) <= 1e-8
+    # measured here: plain 15, untrained 15, trained 11 cycles
+    assert cyc_nn <= cyc_plain - 2 and cyc_nn <= cyc_u - 2
