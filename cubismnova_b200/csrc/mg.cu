@@ -516,6 +516,60 @@ __global__ void __launch_bounds__(kCoarseThreads)
     if (threadIdx.x == 0 && iters_out) *iters_out = it;
 }
 
+// Coarsest levels of at most kCoarseDenseMax cells are solved directly: the
+// operator A = -L (harmonic face means, as coarsest_cg_kernel applies it) is
+// singular on the periodic grid with the constants as null space, so the
+// set-up inverts A' = A + (s/N) 1 1^T (s: the mean diagonal), which is SPD
+// and maps every mean-zero b to the mean-zero solution of A x = b.  Per
+// V-cycle this kernel forms b = -f with its mean removed, as the CG does,
+// and x = A'^-1 b: each CTA takes 32 rows (one per lane), its 8 warps split
+// the columns, and the symmetric inverse is read column-wise (coalesced).
+constexpr int kCoarseDenseMax = 512;
+constexpr int kDenseRows = 32, kDenseThreads = 256;
+
+__global__ void __launch_bounds__(kDenseThreads)
+    coarsest_dense_kernel(LabGeom L, const float *f, float *p, const double *inv, int N)
+{
+    __shared__ double b[kCoarseDenseMax];
+    __shared__ double red[kDenseThreads / 32][kDenseRows];
+    __shared__ double wsum[kDenseThreads / 32];
+    const int GX = L.nb[0] * L.n[0], GY = L.nb[1] * L.n[1];
+    auto offset = [&](int i) {
+        const int gx = i % GX, gy = (i / GX) % GY, gz = i / (GX * GY);
+        const int bx = gx / L.n[0], by = gy / L.n[1], bz = gz / L.n[2];
+        const int blk = bx + L.nb[0] * (by + L.nb[1] * bz);
+        return (int64_t)blk * L.bstride + (gx % L.n[0]) +
+               (int64_t)L.n[0] * ((gy % L.n[1]) + (int64_t)L.n[1] * (gz % L.n[2]));
+    };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double s = 0;
+    for (int i = threadIdx.x; i < N; i += kDenseThreads) {
+        b[i] = -(double)f[offset(i)];
+        s += b[i];
+    }
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (lane == 0) wsum[warp] = s;
+    __syncthreads();
+    double tot = 0;
+    for (int w = 0; w < kDenseThreads / 32; ++w) tot += wsum[w];
+    const double mean = tot / N;
+    for (int i = threadIdx.x; i < N; i += kDenseThreads) b[i] -= mean;
+    __syncthreads();
+    const int row = blockIdx.x * kDenseRows + lane;
+    const int per = (N + kDenseThreads / 32 - 1) / (kDenseThreads / 32);
+    const int j0 = warp * per, j1 = min(N, j0 + per);
+    double acc = 0;
+    if (row < N)
+        for (int j = j0; j < j1; ++j) acc += inv[(int64_t)j * N + row] * b[j];
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0 && row < N) {
+        double x = 0;
+        for (int w = 0; w < kDenseThreads / 32; ++w) x += red[w][lane];
+        p[offset(row)] = (float)x;
+    }
+}
+
 } // namespace mg
 } // namespace cn
 
@@ -574,6 +628,13 @@ static cn_status smooth(cn_mg *m, int l, int sweeps, bool zero_guess, cudaStream
 static cn_status coarsest(cn_mg *m, int l, cudaStream_t st)
 {
     cn_grid *g = m->p[l];
+    if (m->coarse_inv) {
+        const LabGeom L = make_geom(g, &kS1);
+        coarsest_dense_kernel<<<(unsigned)((m->coarse_n + kDenseRows - 1) / kDenseRows), kDenseThreads, 0, st>>>(
+            L, fptr(m->f[l]), fptr(g), m->coarse_inv, m->coarse_n);
+        CN_CUDA_TRY(cudaGetLastError());
+        return CN_OK;
+    }
     const LabGeom L = make_geom(g, &kS1);
     const int N = g->nblocks * g->n[0] * g->n[1] * g->n[2];
     const size_t smem = (size_t)(2 * N + 32) * sizeof(double);
@@ -615,6 +676,82 @@ cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
         if (s != CN_OK) return s;
     }
     return smooth_any(m, l, m->nu2, false, st);
+}
+
+// Inverse of the regularised coarsest operator (see coarsest_dense_kernel),
+// built on the host in FP64 from the coarsest level's k: Cholesky A' = C C^T,
+// C^-1 by forward substitution, A'^-1 = C^-T C^-1.
+static cn_status coarse_inverse(cn_mg *m)
+{
+    const int l = m->nlevels - 1;
+    const cn_grid *g = m->p[l];
+    const int GX = g->nb[0] * g->n[0], GY = g->nb[1] * g->n[1], GZ = g->nb[2] * g->n[2];
+    const int N = GX * GY * GZ;
+    std::vector<float> kb((size_t)m->k[l]->comp_stride);
+    CN_CUDA_TRY(cudaMemcpy(kb.data(), m->k[l]->d_data, kb.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<double> kk(N);
+    for (int i = 0; i < N; ++i) {
+        const int gx = i % GX, gy = (i / GX) % GY, gz = i / (GX * GY);
+        const int blk = gx / g->n[0] + g->nb[0] * (gy / g->n[1] + g->nb[1] * (gz / g->n[2]));
+        kk[i] = (double)kb[(size_t)blk * m->k[l]->block_stride + (gx % g->n[0]) +
+                           (size_t)g->n[0] * ((gy % g->n[1]) + (size_t)g->n[1] * (gz % g->n[2]))];
+    }
+    const double ih2 = 1.0 / (g->h[0] * g->h[0]);
+    std::vector<double> A((size_t)N * N, 0.0);
+    for (int i = 0; i < N; ++i) {
+        const int gx = i % GX, gy = (i / GX) % GY, gz = i / (GX * GY);
+        const int nbr[6] = {((gx + 1) % GX) + GX * (gy + GY * gz), ((gx + GX - 1) % GX) + GX * (gy + GY * gz),
+                            gx + GX * (((gy + 1) % GY) + GY * gz), gx + GX * (((gy + GY - 1) % GY) + GY * gz),
+                            gx + GX * (gy + GY * ((gz + 1) % GZ)), gx + GX * (gy + GY * ((gz + GZ - 1) % GZ))};
+        for (int q = 0; q < 6; ++q) {
+            const double t = kk[i] * kk[nbr[q]];
+            const double kf = ih2 * ((t + t) / (kk[i] + kk[nbr[q]]));
+            A[(size_t)i * N + i] += kf;
+            A[(size_t)i * N + nbr[q]] -= kf;
+        }
+    }
+    double sd = 0;
+    for (int i = 0; i < N; ++i) sd += A[(size_t)i * N + i];
+    if (!(sd > 0)) return CN_OK; // a one-cell level: the CG keeps it (x = 0)
+    const double reg = sd / N / N;
+    for (size_t e = 0; e < A.size(); ++e) A[e] += reg;
+    // Cholesky, lower factor in A
+    for (int j = 0; j < N; ++j) {
+        double d = A[(size_t)j * N + j];
+        for (int q = 0; q < j; ++q) d -= A[(size_t)j * N + q] * A[(size_t)j * N + q];
+        if (!(d > 0)) return CN_OK; // not numerically definite: the CG keeps the level
+        const double c = std::sqrt(d);
+        A[(size_t)j * N + j] = c;
+        for (int i = j + 1; i < N; ++i) {
+            double v = A[(size_t)i * N + j];
+            for (int q = 0; q < j; ++q) v -= A[(size_t)i * N + q] * A[(size_t)j * N + q];
+            A[(size_t)i * N + j] = v / c;
+        }
+    }
+    // Ci = C^-1 (lower), column by column
+    std::vector<double> Ci((size_t)N * N, 0.0);
+    for (int c = 0; c < N; ++c) {
+        Ci[(size_t)c * N + c] = 1.0 / A[(size_t)c * N + c];
+        for (int i = c + 1; i < N; ++i) {
+            double v = 0;
+            for (int q = c; q < i; ++q) v -= A[(size_t)i * N + q] * Ci[(size_t)q * N + c];
+            Ci[(size_t)i * N + c] = v / A[(size_t)i * N + i];
+        }
+    }
+    // inverse = Ci^T Ci (symmetric)
+    std::vector<double> inv((size_t)N * N, 0.0);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double v = 0;
+            for (int q = i; q < N; ++q) v += Ci[(size_t)q * N + i] * Ci[(size_t)q * N + j];
+            inv[(size_t)i * N + j] = v;
+            inv[(size_t)j * N + i] = v;
+        }
+    if (cudaMalloc(&m->coarse_inv, inv.size() * sizeof(double)) != cudaSuccess)
+        return fail(CN_ERR_OUT_OF_MEMORY, "cn_mg_create: coarsest inverse");
+    CN_CUDA_TRY(cudaMemcpy(m->coarse_inv, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice));
+    m->coarse_n = N;
+    return CN_OK;
 }
 
 extern "C" {
@@ -716,6 +853,7 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
         if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
     }
     if (s == CN_OK && cudaDeviceSynchronize() != cudaSuccess) s = fail(CN_ERR_CUDA, "cn_mg_create");
+    if (s == CN_OK && coarse_cells <= kCoarseDenseMax) s = coarse_inverse(m);
     if (s != CN_OK) {
         extern cn_status cn_mg_destroy(cn_mg *);
         cn_mg_destroy(m);
@@ -738,6 +876,7 @@ cn_status cn_mg_destroy(cn_mg *m)
     for (float *c : m->coef)
         if (c) cudaFree(c);
     if (m->coef64) cudaFree(m->coef64);
+    if (m->coarse_inv) cudaFree(m->coarse_inv);
     for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
     for (void *a : m->nn_act)
         if (a) cudaFree(a);

@@ -20,6 +20,10 @@ struct cn_mg {
     int *iters = nullptr;
     int nparts = 0;
     int coarse_iters_max = 0;
+    // coarsest levels of at most kCoarseDenseMax cells: the inverse of the
+    // regularised coarsest operator (N x N FP64, symmetric), else null (CG)
+    double *coarse_inv = nullptr;
+    int coarse_n = 0;
     // learned smoother: network, the levels it replaces Jacobi on (bit l),
     // and per-level work grids (features, hidden activations, output)
     cn_nn *nn = nullptr;
