@@ -4,6 +4,7 @@
 // variable-coefficient 7-point operator evaluated from the staged region.
 #pragma once
 
+#include "cn_fastdiv.h"
 #include "cn_internal.h"
 #include "cn_tma.cuh"
 
@@ -93,6 +94,7 @@ struct Tile {
     int count;     // tiles per block
     int sh[2];     // log2 of t[0], t[1] when powers of two, else -1
     int zs;        // z groups: threads take (x, y) columns, split into zs runs along z
+    FastDiv dv_count, dv_per0, dv_per1; // CTA index -> (block, tile) without divisions
 };
 
 constexpr int kTileCap[3] = {32, 8, 4};
@@ -124,6 +126,9 @@ inline Tile tile_of(const int n[3])
         for (int b = 0; b < 31; ++b)
             if (T.t[d] == (1 << b)) T.sh[d] = b;
     }
+    T.dv_count = FastDiv((uint32_t)T.count);
+    T.dv_per0 = FastDiv((uint32_t)T.per[0]);
+    T.dv_per1 = FastDiv((uint32_t)T.per[1]);
     const int cols = T.t[0] * T.t[1];
     T.zs = 1;
     for (int g = T.t[2]; g >= 1; --g)
@@ -182,12 +187,12 @@ __device__ __forceinline__ int ridx(const TilePos &q, int x, int y, int z)
 __device__ __forceinline__ TilePos tile_pos(const Tile &T)
 {
     TilePos q;
-    q.block = blockIdx.x / T.count;
-    int r = blockIdx.x - q.block * T.count;
-    q.x0 = (r % T.per[0]) * T.t[0];
-    r /= T.per[0];
-    q.y0 = (r % T.per[1]) * T.t[1];
-    q.z0 = (r / T.per[1]) * T.t[2];
+    q.block = T.dv_count.div((int)blockIdx.x);
+    const int r = blockIdx.x - q.block * T.count;
+    const int ry = T.dv_per0.div(r), rz = T.dv_per1.div(ry);
+    q.x0 = (r - ry * T.per[0]) * T.t[0];
+    q.y0 = (ry - rz * T.per[1]) * T.t[1];
+    q.z0 = rz * T.t[2];
     q.ex = T.t[0] + 2;
     q.ey = T.t[1] + 2;
     q.ez = T.t[2] + 2;
@@ -263,11 +268,15 @@ __device__ __forceinline__ void stage_region(const T *comp, const LabGeom &L, co
     const bool plain = __ldg(bc.mode + q.block) == 0;
     const int t0 = q.ex - 2;
     if (q.xo == V) {
-        // per row: t0 / V in-block 16-byte chunks and the two x-halo cells
+        // per row: t0 / V in-block 16-byte chunks and the two x-halo cells;
+        // work item it = r per + k, row r = j + ey kz, indices advanced with
+        // carries instead of divided anew
         const int per = t0 / V + 2;
+        int r = threadIdx.x / per, k = threadIdx.x - r * per;
+        int j = r % q.ey, kz = r / q.ey;
+        const int dr = kTileThreads / per, dk = kTileThreads - dr * per;
+        const int dj = dr % q.ey, dkz = dr / q.ey;
         for (int it = threadIdx.x; it < rows * per; it += kTileThreads) {
-            const int r = it / per, k = it - r * per;
-            const int j = r % q.ey, kz = r / q.ey;
             const int y = q.y0 + j - 1, z = q.z0 + kz - 1;
             T *row = s + q.rs * r;
             if (k < per - 2) {
@@ -290,6 +299,19 @@ __device__ __forceinline__ void stage_region(const T *comp, const LabGeom &L, co
             } else {
                 const int xl = k == per - 2 ? -1 : t0; // tile-local x of the halo cell
                 stage_cell<T>(comp, L, bc, q, tensorial, snb, plain, q.x0 + xl, y, z, row + q.xo + xl);
+            }
+            k += dk;
+            r += dr;
+            j += dj;
+            kz += dkz;
+            if (k >= per) {
+                k -= per;
+                ++r;
+                ++j;
+            }
+            if (j >= q.ey) {
+                j -= q.ey;
+                ++kz;
             }
         }
     } else {
