@@ -118,14 +118,17 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double 
         return 2;
     const double gm1 = gamma - 1.0, igm1 = 1.0 / (gamma - 1.0);
     int rc = 0;
-    for (int b = 0; b < nblocks && !rc; ++b) {
+    /* blocks are independent: each writes its own cells of out */
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nblocks; ++b) {
+        int brc = 0;
         const int n = blk[b].n, L = n + 6;
         const size_t le = (size_t)L * L * L;
         double *prim = (double *)calloc(5 * le, sizeof(double));
         double *flux = (double *)malloc(sizeof(double) * 5 * (size_t)(n + 1) * (n + 1) * (n + 1));
         double *acc = (double *)malloc(sizeof(double) * 5 * (size_t)n * n * n);
         if (!prim || !flux || !acc) {
-            rc = 2;
+            brc = 2;
         } else {
             for (int z = -3; z < n + 3; ++z)
                 for (int y = -3; y < n + 3; ++y)
@@ -197,6 +200,10 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double 
         free(prim);
         free(flux);
         free(acc);
+        if (brc) {
+#pragma omp atomic write
+            rc = brc;
+        }
     }
     free(lk);
     return rc;

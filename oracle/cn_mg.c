@@ -88,6 +88,8 @@ void or_mg_jacobi(const int nb[3], const int n[3], int64_t stride, const float *
                   const float *k, const float *f, float omega, float ih2, float *pout)
 {
     const mgeo g = mk(nb, n, stride);
+    /* cells are independent: every thread writes its own */
+#pragma omp parallel for
     FOR_CELLS(&g)
     {
         const int64_t o = moff(&g, gx, gy, gz);
@@ -116,6 +118,8 @@ void or_mg_resid_restrict(const int nb[3], const int n[3], int64_t stride, const
     const mgeo g = mk(nb, n, stride);
     const int nc[3] = {n[0] / 2, n[1] / 2, n[2] / 2};
     const mgeo gc = mk(nb, nc, cstride);
+    /* cells are independent: every thread writes its own */
+#pragma omp parallel for
     FOR_CELLS(&gc)
     {
         float r[8];
@@ -136,6 +140,8 @@ void or_mg_restrict_mean(const int nb[3], const int n[3], int64_t stride, const 
     const mgeo g = mk(nb, n, stride);
     const int nc[3] = {n[0] / 2, n[1] / 2, n[2] / 2};
     const mgeo gc = mk(nb, nc, cstride);
+    /* cells are independent: every thread writes its own */
+#pragma omp parallel for
     FOR_CELLS(&gc)
     {
         float v[8];
@@ -154,6 +160,8 @@ void or_mg_prolong(const int nb[3], const int n[3], int64_t stride, float *p, in
     const mgeo g = mk(nb, n, stride);
     const int nc[3] = {n[0] / 2, n[1] / 2, n[2] / 2};
     const mgeo gc = mk(nb, nc, cstride);
+    /* cells are independent: every thread writes its own */
+#pragma omp parallel for
     FOR_CELLS(&g)
     {
         const int X = gx >> 1, Y = gy >> 1, Z = gz >> 1;
@@ -180,29 +188,42 @@ void or_mg_resid64(const int nb[3], const int n[3], int64_t stride64, const doub
                    double *rr, double *ff)
 {
     const mgeo gp = mk(nb, n, stride64), gk = mk(nb, n, stride32);
+    /* per z-plane partial sums, added in plane order: the same result for
+     * any number of threads */
+    const int GZ = nb[2] * n[2];
+    double *prr = (double *)calloc((size_t)GZ, sizeof(double));
+    double *pff = (double *)calloc((size_t)GZ, sizeof(double));
+#pragma omp parallel for
+    for (int gz = 0; gz < GZ; ++gz)
+        for (int gy = 0; gy < gp.nb[1] * gp.n[1]; ++gy)
+            for (int gx = 0; gx < gp.nb[0] * gp.n[0]; ++gx) {
+                const double pc = p[moff(&gp, gx, gy, gz)];
+                const double kc = (double)k[moff(&gk, gx, gy, gz)];
+                double fl[3];
+                for (int d = 0; d < 3; ++d) {
+                    const int ox = d == 0, oy = d == 1, oz = d == 2;
+                    const double pp = p[moff(&gp, gx + ox, gy + oy, gz + oz)];
+                    const double pm = p[moff(&gp, gx - ox, gy - oy, gz - oz)];
+                    const double kp = harmd(kc, (double)k[moff(&gk, gx + ox, gy + oy, gz + oz)]);
+                    const double km = harmd((double)k[moff(&gk, gx - ox, gy - oy, gz - oz)], kc);
+                    fl[d] = kp * (pp - pc) - km * (pc - pm);
+                }
+                const double Lp = ih2 * ((fl[0] + fl[1]) + fl[2]);
+                const int64_t o = moff(&gk, gx, gy, gz);
+                const double fc = (double)f[o];
+                const double r = fc - Lp;
+                if (r32)
+                    r32[o] = (float)r;
+                prr[gz] += r * r;
+                pff[gz] += fc * fc;
+            }
     double srr = 0, sff = 0;
-    FOR_CELLS(&gp)
-    {
-        const double pc = p[moff(&gp, gx, gy, gz)];
-        const double kc = (double)k[moff(&gk, gx, gy, gz)];
-        double fl[3];
-        for (int d = 0; d < 3; ++d) {
-            const int ox = d == 0, oy = d == 1, oz = d == 2;
-            const double pp = p[moff(&gp, gx + ox, gy + oy, gz + oz)];
-            const double pm = p[moff(&gp, gx - ox, gy - oy, gz - oz)];
-            const double kp = harmd(kc, (double)k[moff(&gk, gx + ox, gy + oy, gz + oz)]);
-            const double km = harmd((double)k[moff(&gk, gx - ox, gy - oy, gz - oz)], kc);
-            fl[d] = kp * (pp - pc) - km * (pc - pm);
-        }
-        const double Lp = ih2 * ((fl[0] + fl[1]) + fl[2]);
-        const int64_t o = moff(&gk, gx, gy, gz);
-        const double fc = (double)f[o];
-        const double r = fc - Lp;
-        if (r32)
-            r32[o] = (float)r;
-        srr += r * r;
-        sff += fc * fc;
+    for (int gz = 0; gz < GZ; ++gz) {
+        srr += prr[gz];
+        sff += pff[gz];
     }
+    free(prr);
+    free(pff);
     *rr = srr;
     *ff = sff;
 }
