@@ -376,10 +376,24 @@ class Euler:
                                                     nbytes, sh))
         return 5 * nbytes, 5 * nbytes
 
-    e2e_path = ("C ABI, device states in turn (three when their pinned host copies fit in 24 GB, else two): "
+    e2e_path = ("C ABI, device states in turn (three when the node's pinned host copies fit in 48 GB, else two): "
                 "step i+1's upload (cn_grid_upload from pinned host) and step i-1's download "
                 "(cn_grid_download to pinned host) run on their own streams while step i runs; "
                 "the stage work grids are shared")
+
+    # pinned host memory the pipelined leg may hold on one node, all ranks
+    E2E_PINNED_BUDGET = 48e9
+    ranks_per_node = 1
+
+    def e2e_slots(self):
+        """Device states (each with a pinned host copy) the pipelined leg
+        uses: three when the node's ranks' host copies fit the budget, else
+        two, else one (the pipelined leg is then not run)."""
+        state = 5 * self.U.comp_stride * self.U.dtype.itemsize
+        for n in (3, 2):
+            if n * state * self.ranks_per_node <= self.E2E_PINNED_BUDGET:
+                return n
+        return 1
 
     def e2e_pipelined(self, stream, k):
         """k independent steps (each: 5 components uploaded from pinned host
@@ -396,7 +410,7 @@ class Euler:
             self.e2e_step(stream)
             stream.synchronize()
         if getattr(self, "pipe", None) is None:
-            nslots = 3 if 3 * 5 * nbytes <= 24e9 else 2
+            nslots = self.e2e_slots()
             Us, hs = [self.U], [self.h_state]
             for _ in range(nslots - 1):
                 U2 = cn.Grid.Cartesian(self.nb, self.n, ncomp=5, dtype=self.U.dtype)
@@ -854,7 +868,8 @@ def run_ours(args, world, rank, local, pg):
 
     serial_ms, hb, db = timed_e2e(serial, ek)
     e2e_ms, path = serial_ms, "C ABI: cn_grid_upload from pinned host, the step, cn_grid_download to pinned host"
-    if getattr(W, "e2e_pipelined", None) and not args.e2e_serial:
+    W.ranks_per_node = int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+    if getattr(W, "e2e_pipelined", None) and not args.e2e_serial and W.e2e_slots() >= 2:
         # the pipeline's fill and drain (one upload, one download) are inside
         # the timed region: run as many steps as the main timed region
         e2e_ms, hb, db = timed_e2e(lambda k: W.e2e_pipelined(stream, k), max(ek, args.steps))
