@@ -259,14 +259,15 @@ class C1:
 
 # FP64/FP32 operations per cell and RK stage of the Euler kernel (fma = 2,
 # div = sqrt = 1), each cell and face counted once: per direction and
-# variable the cell's WENO5 smoothness indicators and weight products (42)
-# and its left- and right-biased states (24 each); per face the divisions of
-# the five variables' states (FP64: variables paired, 2 x 14 + 6 = 34; FP32:
-# 5 x 6 = 30) and the Rusanov flux (74); per cell the primitive conversion
-# (12), the flux differences (40) and the stage update (20).  Work the kernel
-# repeats at tile and run edges is not counted.
+# variable the cell's WENO5 smoothness indicators and weight products (42;
+# FP32 45 with the three power-of-two rescaling products) and its left- and
+# right-biased states (24 each); per face the divisions of the five
+# variables' states (variables paired, 2 x 14 + 6 = 34) and the Rusanov flux
+# (74); per cell the primitive conversion (12), the flux differences (40) and
+# the stage update (20).  Integer instructions and work the kernel repeats at
+# tile and run edges are not counted.
 EULER_FLOPS_PER_CELL_STAGE = {"f64": 3 * (5 * (42 + 24 + 24) + 34 + 74) + 12 + 40 + 20,
-                              "f32": 3 * (5 * (42 + 24 + 24) + 30 + 74) + 12 + 40 + 20}
+                              "f32": 3 * (5 * (45 + 24 + 24) + 34 + 74) + 12 + 40 + 20}
 
 
 def euler_host_state(nb, n, block_stride, gamma=1.4, seed=1234):

@@ -17,6 +17,18 @@
 // beta_k and the products t_i t_j belong to the cell, not to the face: a
 // cell's left-biased state (at its upper face) and right-biased state (at its
 // lower face) share them.
+//
+// Range.  A jump J in the data gives s ~ 3 J^2 and t_i t_j ~ 20 J^8, which
+// leaves the FP32 range above J ~ 4e4 (a pressure jump of one bar in SI
+// units).  So in FP32 t_k is formed from s_k * 2^-e, with e the mean of the
+// binary exponents of the largest and the middle s_k (rounded down).  Scaling
+// by a power of two is exact and cancels in every ratio below.  With it the
+// dominant product t_max t_mid lies in [1, 64): every FP32 denominator lies
+// in [0.6, 384], the only products that can underflow are those of
+// negligible weights, and the face states of two variables can share one
+// division.  FP64 needs no scaling: its denominators lie in
+// [6e-25, ~70 J^8], and the shared divisions below stay in range for jumps up
+// to ~2e9 in the paired variables (density, velocity) and ~4e18 in pressure.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -44,6 +56,19 @@ __device__ __forceinline__ float dabs(float a) { return fabsf(a); }
 __device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float dmax(float a, float b) { return fmaxf(a, b); }
 
+// The FP32 factor 2^-e of the range note above for s0, s1, s2 >= eps: e =
+// floor((E_max + E_mid) / 2) - 127 from the biased exponents of the largest
+// and the middle of the three (E_max + E_mid = E0 + E1 + E2 - E_min).  The
+// exponents come from the bit patterns (integer instructions only).  A NaN
+// or infinite s gives NaN states, and so do two sums above 2^127 (~1.7e38,
+// jumps ~1e19: the factor leaves the normal range there).
+__device__ __forceinline__ float weno5_scale(float s0, float s1, float s2)
+{
+    const int e0 = __float_as_int(s0) >> 23, e1 = __float_as_int(s1) >> 23, e2 = __float_as_int(s2) >> 23;
+    const int emin = min(min(e0, e1), e2);
+    return __int_as_float(int(unsigned(254 - ((e0 + e1 + e2 - emin) >> 1)) << 23));
+}
+
 // Smoothness of cell j from u0..u4 = v[j-2..j+2]: with s_k = eps + beta_k
 // and t_k = s_k^2 for the stencils S0 = {j-2, j-1, j}, S1 = {j-1, j, j+1},
 // S2 = {j, j+1, j+2}, the products p12 = t1 t2, p02 = t0 t2, p01 = t0 t1.
@@ -62,7 +87,14 @@ __device__ __forceinline__ void weno5_beta(T u0, T u1, T u2, T u3, T u4, T &p12,
     const T s0 = C::eps + dfma(C::c1312 * a0, a0, C::quarter * (b0 * b0));
     const T s1 = C::eps + dfma(C::c1312 * a1, a1, C::quarter * (b1 * b1));
     const T s2 = C::eps + dfma(C::c1312 * a2, a2, C::quarter * (b2 * b2));
-    const T t0 = s0 * s0, t1 = s1 * s1, t2 = s2 * s2;
+    T q0 = s0, q1 = s1, q2 = s2;
+    if constexpr (sizeof(T) == 4) { // FP32: exact power-of-two rescaling
+        const T sc = weno5_scale(s0, s1, s2);
+        q0 = s0 * sc;
+        q1 = s1 * sc;
+        q2 = s2 * sc;
+    }
+    const T t0 = q0 * q0, t1 = q1 * q1, t2 = q2 * q2;
     p12 = t1 * t2;
     p02 = t0 * t2;
     p01 = t0 * t1;
@@ -97,35 +129,27 @@ __device__ __forceinline__ void weno5_right(T u0, T u1, T u2, T u3, T u4, T p12,
 }
 
 // The two states at one face from the lower cell's left-biased (nl, dl) and
-// the upper cell's right-biased (nr, dr) reconstruction.  FP64 shares one
-// division between them:
+// the upper cell's right-biased (nr, dr) reconstruction, from one division:
 //   inv = 1/(dl*dr), vl = (nl*dr)*inv, vr = (nr*dl)*inv
-// (den >= 6e-25 since eps = 1e-6, so the product cannot underflow in FP64);
-// FP32 divides twice, as the product could leave the FP32 range.
-__device__ __forceinline__ void face_states(double nl, double dl, double nr, double dr, double &vl, double &vr)
+// (the product stays in range: see the range note).
+template <typename T> __device__ __forceinline__ void face_states(T nl, T dl, T nr, T dr, T &vl, T &vr)
 {
-    const double inv = 1.0 / (dl * dr);
+    const T inv = T(1) / (dl * dr);
     vl = (nl * dr) * inv;
     vr = (nr * dl) * inv;
 }
 
-__device__ __forceinline__ void face_states(float nl, float dl, float nr, float dr, float &vl, float &vr)
-{
-    vl = nl / dl;
-    vr = nr / dr;
-}
-
-// FP64: two variables' face states from one division (a = first, b = second
+// Two variables' face states from one division (a = first, b = second
 // variable):  inv = 1/((dla*dra)*(dlb*drb)), q_a = (dlb*drb)*inv = 1/(dla*dra),
-// q_b = (dla*dra)*inv.  The product of four denominators stays in range: each
-// lies in [6e-25, 6 B^4] for smoothness indicators up to B, so up to B ~ 1e19.
-__device__ __forceinline__ void face_states2(double nla, double dla, double nra, double dra, double nlb, double dlb,
-                                             double nrb, double drb, double &vla, double &vra, double &vlb,
-                                             double &vrb)
+// q_b = (dla*dra)*inv.  The product of four denominators lies in
+// [0.13, 2.2e10] in FP32 (rescaled weights); FP64 bounds in the range note.
+template <typename T>
+__device__ __forceinline__ void face_states2(T nla, T dla, T nra, T dra, T nlb, T dlb, T nrb, T drb, T &vla, T &vra,
+                                             T &vlb, T &vrb)
 {
-    const double Da = dla * dra, Db = dlb * drb;
-    const double inv = 1.0 / (Da * Db);
-    const double qa = Db * inv, qb = Da * inv;
+    const T Da = dla * dra, Db = dlb * drb;
+    const T inv = T(1) / (Da * Db);
+    const T qa = Db * inv, qb = Da * inv;
     vla = (nla * dra) * qa;
     vra = (nra * dla) * qa;
     vlb = (nlb * drb) * qb;

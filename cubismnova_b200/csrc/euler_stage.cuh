@@ -245,9 +245,8 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
         for (int k = 0; k < 5; ++k)
             id[k] = sidx(a - 2 + k);
         T WL[5], WR[5];
-        // FP64: variables (0,1) and (2,3) share one division; the first of a
-        // pair waits in (hnl, hdl, hnr, hdr) for the second
-        constexpr bool PAIR = sizeof(T) == 8;
+        // variables (0,1) and (2,3) share one division; the first of a pair
+        // waits in (hnl, hdl, hnr, hdr) for the second
         T hnl = T(0), hdl = T(1), hnr = T(0), hdr = T(1);
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
@@ -256,17 +255,13 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
             T p12, p02, p01, nr, dr;
             weno5_beta(u0, u1, u2, u3, u4, p12, p02, p01);
             weno5_right(u0, u1, u2, u3, u4, p12, p02, p01, nr, dr);
-            if constexpr (PAIR) {
-                if (c == 0 || c == 2) {
-                    hnl = Ln[c];
-                    hdl = Ld[c];
-                    hnr = nr;
-                    hdr = dr;
-                } else if (c == 1 || c == 3) {
-                    face_states2(hnl, hdl, hnr, hdr, Ln[c], Ld[c], nr, dr, WL[c - 1], WR[c - 1], WL[c], WR[c]);
-                } else {
-                    face_states(Ln[c], Ld[c], nr, dr, WL[c], WR[c]);
-                }
+            if (c == 0 || c == 2) {
+                hnl = Ln[c];
+                hdl = Ld[c];
+                hnr = nr;
+                hdr = dr;
+            } else if (c == 1 || c == 3) {
+                face_states2(hnl, hdl, hnr, hdr, Ln[c], Ld[c], nr, dr, WL[c - 1], WR[c - 1], WL[c], WR[c]);
             } else {
                 face_states(Ln[c], Ld[c], nr, dr, WL[c], WR[c]);
             }

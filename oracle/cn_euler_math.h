@@ -11,8 +11,42 @@
 #define CN_EULER_MATH_H
 
 #include <math.h>
+#include <stdint.h>
+#include <string.h>
 
-#define DEFINE_EULER_MATH(SUF, T, FMA, SQRT, FABS, FMAX, SHARED_DIV)                            \
+/* FP32 power-of-two factor 2^-e for the smoothness sums s0, s1, s2 (all
+ * >= eps): e = floor((E_max + E_mid) / 2) - 127 from the biased exponents of
+ * the largest and the middle sum (E_max + E_mid = E0 + E1 + E2 - E_min).
+ * t_k = (s_k 2^-e)^2: scaling by a power of two is exact and cancels in the
+ * weights, and keeps the dominant product t_max t_mid in [1, 64), so the
+ * products of a jump J (~20 J^8 unscaled) stay in the FP32 range.  The
+ * factor's bit pattern is formed as on the device (32-bit wrap-around); FP64
+ * is not rescaled (factor 1). */
+static inline int cn_imin_(int a, int b) { return a < b ? a : b; }
+
+static inline float weno5_scale_f32(float s0, float s1, float s2)
+{
+    int32_t b0, b1, b2;
+    memcpy(&b0, &s0, 4);
+    memcpy(&b1, &s1, 4);
+    memcpy(&b2, &s2, 4);
+    const int e0 = b0 >> 23, e1 = b1 >> 23, e2 = b2 >> 23;
+    const int emin = cn_imin_(cn_imin_(e0, e1), e2);
+    const uint32_t bits = (uint32_t)(254 - ((e0 + e1 + e2 - emin) >> 1)) << 23;
+    float r;
+    memcpy(&r, &bits, 4);
+    return r;
+}
+
+static inline double weno5_scale_f64(double s0, double s1, double s2)
+{
+    (void)s0;
+    (void)s1;
+    (void)s2;
+    return 1.0;
+}
+
+#define DEFINE_EULER_MATH(SUF, T, FMA, SQRT, FABS, FMAX)                        \
     /* smoothness of cell j from u0..u4 = v[j-2..j+2]: the products          \
      * p12 = t1 t2, p02 = t0 t2, p01 = t0 t1 of t_k = (eps + beta_k)^2 for   \
      * the stencils S0 = {j-2..j}, S1 = {j-1..j+1}, S2 = {j..j+2}; shared by  \
@@ -29,7 +63,9 @@
         const T s0 = eps + FMA(c1312 * a0, a0, quarter * (b0 * b0));           \
         const T s1 = eps + FMA(c1312 * a1, a1, quarter * (b1 * b1));           \
         const T s2 = eps + FMA(c1312 * a2, a2, quarter * (b2 * b2));           \
-        const T t0 = s0 * s0, t1 = s1 * s1, t2 = s2 * s2;                      \
+        const T sc = weno5_scale_##SUF(s0, s1, s2);                            \
+        const T q0 = s0 * sc, q1 = s1 * sc, q2 = s2 * sc;                      \
+        const T t0 = q0 * q0, t1 = q1 * q1, t2 = q2 * q2;                      \
         *p12 = t1 * t2;                                                        \
         *p02 = t0 * t2;                                                        \
         *p01 = t0 * t1;                                                        \
@@ -73,32 +109,25 @@
         weno5_right_##SUF(v1, v2, v3, v4, v5, nr, dr);                         \
     }                                                                          \
                                                                                \
-    /* face states of the 5 variables from their numerators and denominators. \
-     * SHARED_DIV (FP64, as the device): variables (0,1) and (2,3) share one  \
-     * division for their four states, variable 4 one for its two; FP32       \
-     * divides each state on its own (the products could leave the range) */   \
+    /* face states of the 5 variables from their numerators and denominators \
+     * (each in [0.6, 384] with the scaled weights): variables (0,1) and     \
+     * (2,3) share one division for their four states, variable 4 takes one  \
+     * for its two */                                                         \
     static inline void face_states5_##SUF(const T *nl, const T *dl, const T *nr, \
                                           const T *dr, T *WL, T *WR)           \
     {                                                                          \
-        if (SHARED_DIV) {                                                      \
-            for (int c = 0; c < 4; c += 2) {                                   \
-                const T Da = dl[c] * dr[c], Db = dl[c + 1] * dr[c + 1];        \
-                const T inv = (T)1 / (Da * Db);                                \
-                const T qa = Db * inv, qb = Da * inv;                          \
-                WL[c] = (nl[c] * dr[c]) * qa;                                  \
-                WR[c] = (nr[c] * dl[c]) * qa;                                  \
-                WL[c + 1] = (nl[c + 1] * dr[c + 1]) * qb;                      \
-                WR[c + 1] = (nr[c + 1] * dl[c + 1]) * qb;                      \
-            }                                                                  \
-            const T inv = (T)1 / (dl[4] * dr[4]);                              \
-            WL[4] = (nl[4] * dr[4]) * inv;                                     \
-            WR[4] = (nr[4] * dl[4]) * inv;                                     \
-        } else {                                                               \
-            for (int c = 0; c < 5; ++c) {                                      \
-                WL[c] = nl[c] / dl[c];                                         \
-                WR[c] = nr[c] / dr[c];                                         \
-            }                                                                  \
+        for (int c = 0; c < 4; c += 2) {                                       \
+            const T Da = dl[c] * dr[c], Db = dl[c + 1] * dr[c + 1];            \
+            const T inv = (T)1 / (Da * Db);                                    \
+            const T qa = Db * inv, qb = Da * inv;                              \
+            WL[c] = (nl[c] * dr[c]) * qa;                                      \
+            WR[c] = (nr[c] * dl[c]) * qa;                                      \
+            WL[c + 1] = (nl[c + 1] * dr[c + 1]) * qb;                          \
+            WR[c + 1] = (nr[c + 1] * dl[c + 1]) * qb;                          \
         }                                                                      \
+        const T inv = (T)1 / (dl[4] * dr[4]);                                  \
+        WL[4] = (nl[4] * dr[4]) * inv;                                         \
+        WR[4] = (nr[4] * dl[4]) * inv;                                         \
     }                                                                          \
                                                                                \
     static inline void rusanov_##SUF(const T *WL, const T *WR, int d, T gamma,        \
@@ -153,7 +182,7 @@
         W[4] = gm1 * (E - ke);                                                 \
     }                                                                          \
 
-DEFINE_EULER_MATH(f64, double, fma, sqrt, fabs, fmax, 1)
-DEFINE_EULER_MATH(f32, float, fmaf, sqrtf, fabsf, fmaxf, 0)
+DEFINE_EULER_MATH(f64, double, fma, sqrt, fabs, fmax)
+DEFINE_EULER_MATH(f32, float, fmaf, sqrtf, fabsf, fmaxf)
 
 #endif
