@@ -773,7 +773,160 @@ class C5:
         return self.cpu_sample_static(threads)
 
 
-WORKLOADS = {"c1": C1, "c2": C2, "c3": C3, "c4": C4, "c5": C5}
+class IOW:
+    """Grid -> file buffer of IO::CartesianWriteHDF<float> (IO/CartesianHDF.h:76-80,
+    Field2AOS of IO/FieldAOS.h:79-101): a rank-1 FP64 cell grid gathered into
+    one (z, y, x, 3) FP32 array-of-structures buffer."""
+    name = "io"
+    desc = ("Field2AOS block loop of CartesianWriteHDF<float>: 3-component FP64 cell grid, 512^3 cells as "
+            "16^3 blocks of 32^3, into one (z, y, x, 3) FP32 file buffer")
+    nb, n = (16, 16, 16), (32, 32, 32)
+    dtype = "f64"
+    metric = unit = "Gcell/s"
+    launches_per_step = 1
+    bytes_per_cell_step = 36  # 3 x 8 B read, 3 x 4 B written
+    cpu_blocks = (8, 8, 4)
+
+    def __init__(self):
+        import torch
+
+        import cubismnova_b200 as cn
+        self.cn, self.torch = cn, torch
+        self.u = cn.Grid.Cartesian(self.nb, self.n, ncomp=3)
+        gen = torch.Generator(device="cuda").manual_seed(1234)
+        for c in range(3):
+            self.u.tensor(c).uniform_(-1.0, 1.0, generator=gen)
+        top = [self.nb[d] * self.n[d] for d in range(3)]
+        self.buf = torch.empty((top[2], top[1], top[0], 3), dtype=torch.float32, device="cuda")
+        self.cells = int(np.prod(top))
+        self.updates_per_step = self.cells
+        # pinned host copies for the end-to-end leg: the grid's components in
+        # the reference layout and the file buffer
+        self.h_in = [self.u.tensor(c).cpu().pin_memory() for c in range(3)]
+        self.h_out = torch.empty(self.buf.shape, dtype=torch.float32).pin_memory()
+
+    def needs_flush(self):
+        return False  # 3.2 GB of input, 1.6 GB of output: far larger than L2
+
+    def step(self, stream, events=None):
+        if events is not None:
+            events[0].record(stream)
+        self.cn.IO.Field2AOS(self.u, file_dtype=np.float32, out=self.buf, stream=stream)
+        if events is not None:
+            events[1].record(stream)
+
+    def e2e_step(self, stream):
+        import ctypes as C
+        lib = self.cn._lib.lib()
+        sh = C.c_void_p(stream.cuda_stream)
+        nbytes = self.u.comp_stride * 8
+        for c in range(3):
+            self.cn._lib.check(lib.cn_grid_upload(self.u.handle, c, C.c_void_p(self.h_in[c].data_ptr()), nbytes, sh))
+        self.step(stream)
+        with self.torch.cuda.stream(stream):
+            self.h_out.copy_(self.buf, non_blocking=True)
+        return 3 * nbytes, self.buf.numel() * 4
+
+    @classmethod
+    def cpu_sample_static(cls, threads, reps=3):
+        """The reference's Field2AOS block loop (oracle/_ref, OpenMP over
+        blocks as CartesianWriteHDF) on 8x8x4 blocks of 32^3, or the oracle
+        restatement without the reference build."""
+        import oracle as O
+        from oracle import aos as A
+        nb, n = cls.cpu_blocks, cls.n
+        stride = O.block_stride(n, np.float64)
+        rng = np.random.default_rng(1234)
+        data = rng.uniform(-1.0, 1.0, size=(3, int(np.prod(nb)) * stride))
+        top = [nb[d] * n[d] for d in range(3)]
+        buf = np.empty(int(np.prod(top)) * 3, dtype=np.float32)
+        cells = int(np.prod(top))
+        if O.ref_available():
+            t, _ = O.ref_field_aos(data, nb, n, 0, stride, (0, 0, 0), top, np.float32, buf, to_aos=True,
+                                   threads=threads, reps=reps)
+            kind = "reference"
+        else:
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                A.grid_to_aos(list(data), nb, n, 0, stride, (0, 0, 0), top, buf)
+            t = (time.perf_counter() - t0) / reps
+            kind, threads = "port", 1
+        return dict(value=cells / t / 1e9, unit="Gcell/s", cores=threads, kind=kind,
+                    sample=f"Field2AOS of 3 FP64 components into FP32 AoS on {nb[0]}x{nb[1]}x{nb[2]} blocks of "
+                           f"32^3 ({cells / 1e6:.1f} M cells), best of {reps}, {threads} threads",
+                    seconds_per_sweep=t)
+
+    def cpu_sample(self, threads):
+        t1 = self.cpu_sample_static(threads, reps=1)["seconds_per_sweep"]
+        return self.cpu_sample_static(threads, reps=int(min(200, max(3, 10.0 / t1))))
+
+
+class IOR(IOW):
+    """File buffer -> grid of IO::CartesianReadHDF<float> (IO/CartesianHDF.h:182-186,
+    AOS2Field of IO/FieldAOS.h:103-124): one (z, y, x, 3) FP32 buffer scattered
+    into a rank-1 FP64 cell grid."""
+    name = "io_read"
+    desc = ("AOS2Field block loop of CartesianReadHDF<float>: one (z, y, x, 3) FP32 file buffer into a "
+            "3-component FP64 cell grid, 512^3 cells as 16^3 blocks of 32^3")
+    bytes_per_cell_step = 36  # 3 x 4 B read, 3 x 8 B written
+
+    def __init__(self):
+        super().__init__()
+        self.cn.IO.Field2AOS(self.u, file_dtype=np.float32, out=self.buf)
+        self.torch.cuda.synchronize()
+        self.h_file = self.buf.cpu().pin_memory()
+        self.h_grid = [self.torch.empty_like(self.h_in[c]).pin_memory() for c in range(3)]
+
+    def step(self, stream, events=None):
+        if events is not None:
+            events[0].record(stream)
+        self.cn.IO.AOS2Field(self.buf, self.u, stream=stream)
+        if events is not None:
+            events[1].record(stream)
+
+    def e2e_step(self, stream):
+        import ctypes as C
+        lib = self.cn._lib.lib()
+        sh = C.c_void_p(stream.cuda_stream)
+        with self.torch.cuda.stream(stream):
+            self.buf.copy_(self.h_file, non_blocking=True)
+        self.step(stream)
+        nbytes = self.u.comp_stride * 8
+        for c in range(3):
+            self.cn._lib.check(lib.cn_grid_download(self.u.handle, c, C.c_void_p(self.h_grid[c].data_ptr()),
+                                                    nbytes, sh))
+        return self.buf.numel() * 4, 3 * nbytes
+
+    @classmethod
+    def cpu_sample_static(cls, threads, reps=3):
+        """The reference's AOS2Field block loop (oracle/_ref) on 8x8x4 blocks
+        of 32^3, or the oracle restatement without the reference build."""
+        import oracle as O
+        from oracle import aos as A
+        nb, n = cls.cpu_blocks, cls.n
+        stride = O.block_stride(n, np.float64)
+        top = [nb[d] * n[d] for d in range(3)]
+        cells = int(np.prod(top))
+        rng = np.random.default_rng(1234)
+        buf = rng.uniform(-1.0, 1.0, size=cells * 3).astype(np.float32)
+        data = np.zeros((3, int(np.prod(nb)) * stride))
+        if O.ref_available():
+            t, _ = O.ref_field_aos(data, nb, n, 0, stride, (0, 0, 0), top, np.float32, buf, to_aos=False,
+                                   threads=threads, reps=reps)
+            kind = "reference"
+        else:
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                A.aos_to_grid(buf, list(data), nb, n, 0, stride, (0, 0, 0), top)
+            t = (time.perf_counter() - t0) / reps
+            kind, threads = "port", 1
+        return dict(value=cells / t / 1e9, unit="Gcell/s", cores=threads, kind=kind,
+                    sample=f"AOS2Field of an FP32 AoS buffer into 3 FP64 components on {nb[0]}x{nb[1]}x{nb[2]} "
+                           f"blocks of 32^3 ({cells / 1e6:.1f} M cells), best of {reps}, {threads} threads",
+                    seconds_per_sweep=t)
+
+
+WORKLOADS = {"c1": C1, "c2": C2, "c3": C3, "c4": C4, "c5": C5, "io": IOW, "io_read": IOR}
 DEFAULT_WORKLOAD = "c2"
 
 

@@ -1,7 +1,7 @@
 """cubismnova_b200 -- B200-native CubismNova lab fill + stencil hot path.
 
 Host-side mirror of the reference API for this path (namespaces ``Core``,
-``Grid``, ``Block``, ``BC`` and the stencil operators in ``ops``) over the C
+``Grid``, ``Block``, ``BC``, ``IO`` and the stencil operators in ``ops``) over the C
 ABI of ``libcubismnova_b200.so``.  Names, argument meaning and error messages
 follow CubismNova (``include/Cubism/...``); all data lives on the GPU.
 """
@@ -17,5 +17,6 @@ from . import workloads
 from . import mg
 from . import learned
 from . import amr
+from . import io as IO
 
-__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "amr", "CnError", "build"]
+__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "amr", "IO", "CnError", "build"]

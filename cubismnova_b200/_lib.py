@@ -58,6 +58,8 @@ _SIGS = {
     "cn_grid_data": (_I, [_P, _I, C.POINTER(_P)]),
     "cn_grid_upload": (_I, [_P, _I, _P, C.c_size_t, _P]),
     "cn_grid_download": (_I, [_P, _I, _P, C.c_size_t, _P]),
+    "cn_grid_to_aos": (_I, [_P, _I, _I, _I3, _I3, _I, _P, _P]),
+    "cn_grid_from_aos": (_I, [_P, _I, _I, _I3, _I3, _I, _P, _P]),
     "cn_grid_copy": (_I, [_P, _P, _P]),
     "cn_bc_push": (_I, [_P, _I, _I, _I, _I, _I, _D]),
     "cn_bc_push_boundary": (_I, [_P, _I, _I, _I, _I, _D]),

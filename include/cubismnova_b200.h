@@ -21,7 +21,8 @@
  *     block_cells[0]*block_cells[1]*block_cells[2] cells x-fastest, blocks
  *     block_stride elements apart (cells*sizeof rounded up to 32 bytes).
  *     A host array in the reference's SoA order uploads with one copy.
- *   - Only cell-centred fields are supported.
+ *   - Fused stencil operators take cell-centred grids; node and face grids
+ *     (cn_grid_create_entity) work with labs, BCs, the lab fill and IO.
  */
 #ifndef CUBISMNOVA_B200_H
 #define CUBISMNOVA_B200_H
@@ -135,6 +136,29 @@ cn_status cn_grid_upload(cn_grid *g, int comp, const void *host, size_t nbytes, 
 cn_status cn_grid_download(const cn_grid *g, int comp, void *host, size_t nbytes, void *stream);
 /* Cartesian::operator= (Grid/Cartesian.h:160-169): copy all block data. */
 cn_status cn_grid_copy(cn_grid *dst, const cn_grid *src, void *stream);
+
+/* -------------------------------------------------------------------- IO */
+/* Field2AOS over every block of a grid, as CartesianWriteHDF's block loop
+ * (IO/CartesianHDF.h:76-80; IO/FieldAOS.h:37-57 scalar, :79-101 tensor,
+ * :136-141 face field of one direction = that direction's face grid here).
+ * The file range [span_begin, span_end) is a box of global entity indices
+ * (the HDF dataset, x fastest); for every point p of it inside the grid,
+ *   d_buf[c + ncomp * flat(p - span_begin)] = (file type) component comp0 + c at p,
+ * c < ncomp <= 16.  Points of the range outside the grid are not written.
+ * d_buf is device memory of span volume * ncomp elements of file_dtype.
+ * Conversions follow C++ (double -> float rounds to nearest); a
+ * floating-point grid cannot be written as int32 (CN_ERR_UNSUPPORTED).
+ * Stream-ordered; no allocation. */
+cn_status cn_grid_to_aos(cn_grid *g, int comp0, int ncomp, const int span_begin[3], const int span_end[3],
+                         cn_dtype file_dtype, void *d_buf, void *stream);
+/* AOS2Field over every block (IO/FieldAOS.h:59-77, :103-124; the block loop
+ * of CartesianReadHDF, IO/CartesianHDF.h:182-186): component comp0 + c at p
+ *   = (grid type) d_buf[c + ncomp * flat(p - span_begin)]
+ * for every point p of the range inside the grid; other grid points keep
+ * their values.  A floating-point file cannot be read into an int32 grid
+ * (CN_ERR_UNSUPPORTED). */
+cn_status cn_grid_from_aos(cn_grid *g, int comp0, int ncomp, const int span_begin[3], const int span_end[3],
+                           cn_dtype file_dtype, const void *d_buf, void *stream);
 
 /* -------------------------------------------------------------------- BC */
 /* field.getBC().push_back(new BC::Kind(dir, side, value))

@@ -13,6 +13,8 @@
 //   BC::Base/Dirichlet/Absorbing/Symmetry   BC/*.h
 //   Core::Stencil          Core/Stencil.h:21-108
 //   Ops::laplacian/gradient/lapGrad/divergence   the benchmark stencils
+//   IO::Field2AOS/AOS2Field/gatherAOS   IO/FieldAOS.h over every block
+//   IO::CartesianWriteHDF/ReadHDF       IO/CartesianHDF.h without HDF5
 //
 // Errors raise std::runtime_error with the reference's message where the
 // reference throws (Core/Stencil.h:101-106, Block/FieldLab.h:189-190,
@@ -22,8 +24,9 @@
 #include "cubismnova_b200.h"
 
 #include <array>
-#include <functional>
 #include <cstddef>
+#include <cstdio>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -179,6 +182,7 @@ public:
     MultiIndex getSize() const { return nb_; }
     MultiIndex getBlockCells() const { return n_; }
     cn_entity getEntity() const { return entity_; }
+    int getComponents() const { return ncomp_; }
     /// index-range extent of block field `flat` (Grid/BlockFieldAssembler.h:124-135)
     MultiIndex getBlockExtent(int flat) const
     {
@@ -397,6 +401,70 @@ inline void divergence(Grid::Cartesian<T> &v, Grid::Cartesian<T> &out, void *str
     check(cn_divergence(v.raw(), 0, out.raw(), 0, stream));
 }
 } // namespace Ops
+
+namespace IO {
+/// Global index range of a grid's values: the file range of a whole-grid
+/// write (IO/CartesianHDF.h:63-69 with the grid's global mesh).
+template <typename T> Core::IndexRange indexRange(const Grid::Cartesian<T> &g)
+{
+    Core::IndexRange r;
+    const cn_entity e = g.getEntity();
+    for (int d = 0; d < 3; ++d)
+        r.end[d] = g.getSize()[d] * g.getBlockCells()[d] + ((e == CN_ENTITY_NODE || e == CN_ENTITY_FACE_X + d) ? 1 : 0);
+    return r;
+}
+
+/// Field2AOS over every block (IO/FieldAOS.h:186-194; the block loop of
+/// IO/CartesianHDF.h:76-80): d_buf (device, r.size() * ncomp values of
+/// FileT) receives components [comp0, comp0 + ncomp) of every point of r
+/// inside the grid, interleaved (c + ncomp * flat index, x fastest).
+template <typename FileT, typename T>
+void Field2AOS(Grid::Cartesian<T> &g, const Core::IndexRange &r, FileT *d_buf, int comp0 = 0, int ncomp = -1,
+               void *stream = nullptr)
+{
+    check(cn_grid_to_aos(g.raw(), comp0, ncomp < 0 ? g.getComponents() - comp0 : ncomp, r.begin.data(),
+                         r.end.data(), DType<FileT>::value, d_buf, stream));
+}
+
+/// AOS2Field over every block (IO/FieldAOS.h:196-206; IO/CartesianHDF.h:182-186).
+template <typename FileT, typename T>
+void AOS2Field(const FileT *d_buf, const Core::IndexRange &r, Grid::Cartesian<T> &g, int comp0 = 0, int ncomp = -1,
+               void *stream = nullptr)
+{
+    check(cn_grid_from_aos(g.raw(), comp0, ncomp < 0 ? g.getComponents() - comp0 : ncomp, r.begin.data(),
+                           r.end.data(), DType<FileT>::value, d_buf, stream));
+}
+
+/// The file buffer of CartesianWriteHDF<FileT> in host memory: gathered on
+/// the device, copied down once (synchronous).
+template <typename FileT, typename T> std::vector<FileT> gatherAOS(Grid::Cartesian<T> &g, const Core::IndexRange &r)
+{
+    const size_t n = r.size() * (size_t)g.getComponents();
+    std::vector<FileT> host(n);
+    void *d = nullptr;
+    check(cn_device_alloc(n * sizeof(FileT), &d));
+    const cn_status st = cn_grid_to_aos(g.raw(), 0, g.getComponents(), r.begin.data(), r.end.data(),
+                                        DType<FileT>::value, d, nullptr);
+    const cn_status cp = st == CN_OK ? cn_memcpy(host.data(), d, n * sizeof(FileT), nullptr) : st;
+    cn_device_free(d);
+    check(st);
+    check(cp);
+    return host;
+}
+
+/// IO::CartesianWriteHDF / CartesianReadHDF (IO/CartesianHDF.h:42-96,
+/// 147-192) as built without HDF5 (CUBISM_USE_HDF undefined): the
+/// reference's message on stderr, no file.
+template <typename FileT, typename GridT>
+void CartesianWriteHDF(const std::string &fname, const std::string &, const GridT &, double, size_t = 0, bool = true)
+{
+    std::fprintf(stderr, "CartesianWriteHDF: HDF not supported (%s)\n", fname.c_str());
+}
+template <typename FileT, typename GridT> void CartesianReadHDF(const std::string &fname, GridT &, size_t = 0)
+{
+    std::fprintf(stderr, "CartesianReadHDF: HDF not supported (%s)\n", fname.c_str());
+}
+} // namespace IO
 
 } // namespace cubism_b200
 

@@ -268,6 +268,29 @@ def ref_euler_stage(Us, Un, nb, n, bclists, stage, dt, gamma, h, threads=0, bloc
     return t, out
 
 
+# ------------------------------------------------------------------ IO (AoS)
+def ref_field_aos(data, nb, cells, entity, block_stride, span_begin, span_end, file_dtype, buf, to_aos=True,
+                  threads=1, reps=1):
+    """The reference's Field2AOS (to_aos) or AOS2Field block loop
+    (IO/CartesianHDF.h:76-80, 182-186) on a reference grid built from
+    `data` ((ncomp, comp_stride) array, grid layout; ncomp 1, or 3 for
+    cells).  Writes `buf` (to_aos) or returns the grid data after reading it.
+    Returns (best seconds per pass, data)."""
+    data = np.array(data, copy=True, order="C")
+    sfx = {np.dtype(np.float64): "f64", np.dtype(np.float32): "f32"}[data.dtype]
+    f = getattr(ref(), "ref_field_aos_" + sfx)
+    f.restype = C.c_double
+    fd = {np.dtype(np.float32): 0, np.dtype(np.float64): 1}[np.dtype(file_dtype)]
+    se = [span_end[d] - span_begin[d] for d in range(3)]
+    assert buf.dtype == np.dtype(file_dtype) and buf.size == int(np.prod(se)) * data.shape[0]
+    t = f((C.c_int * 3)(*nb), (C.c_int * 3)(*cells), C.c_int(entity), C.c_int(data.shape[0]), _ptr(data),
+          C.c_int64(data.shape[1]), C.c_int64(block_stride), (C.c_int * 3)(*span_begin), (C.c_int * 3)(*se),
+          C.c_int(fd), _ptr(buf), C.c_int(1 if to_aos else 0), C.c_int(threads), C.c_int(reps))
+    if t < 0:
+        raise ValueError("ref_field_aos: unsupported entity / component count")
+    return t, data
+
+
 # ---------------------------------------------------------------- multigrid
 def _i3(v):
     return (C.c_int * 3)(*[int(x) for x in v])

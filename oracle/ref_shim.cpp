@@ -11,6 +11,7 @@
 #include "Cubism/BC/Symmetry.h"
 #include "Cubism/Block/FieldLab.h"
 #include "Cubism/Grid/Cartesian.h"
+#include "Cubism/IO/FieldAOS.h"
 #include "Cubism/Mesh/StructuredUniform.h"
 
 #include "cn_oracle.h"
@@ -349,6 +350,90 @@ int labFillEntity(const or_geom *g, int face_dir, const T *comp, const int32_t *
     return 0;
 }
 
+// The block loop of IO::CartesianWriteHDF / CartesianReadHDF
+// (IO/CartesianHDF.h:76-80, 182-186) over the reference's own Field2AOS /
+// AOS2Field (IO/FieldAOS.h) on a reference grid holding `data` (ncomp
+// arrays cstride apart, blocks bstride apart, each block dense with its own
+// extent).  to_aos: fills buf; else reads buf into the grid and copies the
+// grid back into data.  Returns the best seconds per pass over the blocks.
+template <typename T, EntityType E, size_t RANK, typename F>
+double fieldAOS(const int nb[3], const int cells[3], int face_dir, int ncomp, T *data, int64_t cstride,
+                int64_t bstride, const int sb[3], const int se[3], F *buf, int to_aos, int threads, int reps)
+{
+    using G = Grid::Cartesian<T, Mesh, E, RANK>;
+    using IR = typename Mesh::IndexRangeType;
+    G grid(MIndex{nb[0], nb[1], nb[2]}, MIndex{cells[0], cells[1], cells[2]});
+    auto comp = [&](size_t i, int c) -> T * {
+        if constexpr (E == EntityType::Face) {
+            return grid[i][(size_t)face_dir].getData();
+        } else if constexpr (RANK == 0) {
+            return grid[i].getData();
+        } else {
+            return grid[i][(size_t)c].getData();
+        }
+    };
+    auto count = [&](size_t i) -> size_t {
+        if constexpr (E == EntityType::Face) {
+            return grid[i][(size_t)face_dir].getIndexRange().size();
+        } else if constexpr (RANK == 0) {
+            return grid[i].getIndexRange().size();
+        } else {
+            return grid[i][0].getIndexRange().size();
+        }
+    };
+    for (size_t i = 0; i < grid.size(); ++i)
+        for (int c = 0; c < ncomp; ++c)
+            std::memcpy(comp(i, c), data + c * cstride + (int64_t)i * bstride, count(i) * sizeof(T));
+    const IR span(MIndex{sb[0], sb[1], sb[2]}, MIndex{sb[0] + se[0], sb[1] + se[1], sb[2] + se[2]});
+    const long nblk = (long)grid.size();
+    double best = 1e30;
+    for (int r = 0; r < (reps > 0 ? reps : 1); ++r) {
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(static)
+        for (long i = 0; i < nblk; ++i) {
+            if (to_aos) {
+                IO::Field2AOS(grid[(size_t)i], span, buf, (size_t)(face_dir < 0 ? 0 : face_dir));
+            } else if constexpr (E == EntityType::Face) {
+                // AOSDriver<FaceContainer>::read (IO/FieldAOS.h:143-148) passes
+                // the face field where the buffer goes and does not compile;
+                // it means the scalar read of the direction's face field
+                IO::AOS2Field(buf, span, grid[(size_t)i][(size_t)face_dir], (size_t)face_dir);
+            } else {
+                IO::AOS2Field(buf, span, grid[(size_t)i], (size_t)0);
+            }
+        }
+        const auto t1 = std::chrono::steady_clock::now();
+        const double sec = std::chrono::duration<double>(t1 - t0).count();
+        best = sec < best ? sec : best;
+    }
+    if (!to_aos) {
+        for (size_t i = 0; i < grid.size(); ++i)
+            for (int c = 0; c < ncomp; ++c)
+                std::memcpy(data + c * cstride + (int64_t)i * bstride, comp(i, c), count(i) * sizeof(T));
+    }
+    return best;
+}
+
+template <typename T, typename F>
+double fieldAOSDispatch(const int nb[3], const int cells[3], int entity, int ncomp, T *data, int64_t cstride,
+                        int64_t bstride, const int sb[3], const int se[3], F *buf, int to_aos, int threads,
+                        int reps)
+{
+    if (entity == 0 && ncomp == 1)
+        return fieldAOS<T, EntityType::Cell, 0, F>(nb, cells, -1, 1, data, cstride, bstride, sb, se, buf, to_aos,
+                                                   threads, reps);
+    if (entity == 0 && ncomp == 3)
+        return fieldAOS<T, EntityType::Cell, 1, F>(nb, cells, -1, 3, data, cstride, bstride, sb, se, buf, to_aos,
+                                                   threads, reps);
+    if (entity == 1 && ncomp == 1)
+        return fieldAOS<T, EntityType::Node, 0, F>(nb, cells, -1, 1, data, cstride, bstride, sb, se, buf, to_aos,
+                                                   threads, reps);
+    if (entity >= 2 && entity <= 4 && ncomp == 1)
+        return fieldAOS<T, EntityType::Face, 0, F>(nb, cells, entity - 2, 1, data, cstride, bstride, sb, se, buf,
+                                                   to_aos, threads, reps);
+    return -1.0;
+}
+
 } // namespace
 
 extern "C" {
@@ -412,6 +497,31 @@ double ref_euler_stage_f64(const int nb[3], const int n[3], const double *Us, co
 {
     return eulerStage<double>(nb, n, Us, Un, out, stride, cstride, bc_off, bcs, stage, dt, gamma, h,
                               nthreads, b0, cnt, reps);
+}
+
+// Field2AOS / AOS2Field block loop on a reference grid.  entity: 0 cell,
+// 1 node, 2..4 faces normal to x, y, z; ncomp 1 (rank 0) or 3 (rank-1
+// cells); file_dtype 0 float, 1 double.  Returns the best seconds per pass,
+// or -1 for an unsupported combination.
+double ref_field_aos_f64(const int nb[3], const int cells[3], int entity, int ncomp, double *data, int64_t cstride,
+                         int64_t bstride, const int sb[3], const int se[3], int file_dtype, void *buf, int to_aos,
+                         int threads, int reps)
+{
+    if (file_dtype == 0)
+        return fieldAOSDispatch<double, float>(nb, cells, entity, ncomp, data, cstride, bstride, sb, se,
+                                               (float *)buf, to_aos, threads, reps);
+    return fieldAOSDispatch<double, double>(nb, cells, entity, ncomp, data, cstride, bstride, sb, se,
+                                            (double *)buf, to_aos, threads, reps);
+}
+double ref_field_aos_f32(const int nb[3], const int cells[3], int entity, int ncomp, float *data, int64_t cstride,
+                         int64_t bstride, const int sb[3], const int se[3], int file_dtype, void *buf, int to_aos,
+                         int threads, int reps)
+{
+    if (file_dtype == 0)
+        return fieldAOSDispatch<float, float>(nb, cells, entity, ncomp, data, cstride, bstride, sb, se,
+                                              (float *)buf, to_aos, threads, reps);
+    return fieldAOSDispatch<float, double>(nb, cells, entity, ncomp, data, cstride, bstride, sb, se,
+                                           (double *)buf, to_aos, threads, reps);
 }
 
 int ref_max_threads(void)

@@ -1,6 +1,7 @@
-// The reference's BC and FieldLab unit-test assertions, through the C++ facade
-// on the GPU (test/UnitTests/BC/DirichletTest.cpp, AbsorbingTest.cpp,
-// SymmetryTest.cpp, Block/FieldLabTest.cpp:223-291).  Exit status 0 = pass.
+// The reference's BC, FieldLab and FieldAOS unit-test assertions, through the
+// C++ facade on the GPU (test/UnitTests/BC/DirichletTest.cpp, AbsorbingTest.cpp,
+// SymmetryTest.cpp, Block/FieldLabTest.cpp:223-291, IO/FieldAOSTest.cpp).
+// Exit status 0 = pass.
 #include "cubismnova_b200.hpp"
 
 #include <cstdio>
@@ -155,6 +156,66 @@ int main()
             EXPECT(false);
         } catch (const std::out_of_range &) {
         }
+    }
+    {
+        // IO: the assertions of test/UnitTests/IO/FieldAOSTest.cpp on an 8^3
+        // block, then the same over a 2x2x2-block grid (the block loop)
+        Grid::Cartesian<float> cf({1, 1, 1}, {8, 8, 8});
+        std::vector<float> f(cf.componentStride(), 1.234f);
+        cf.upload(f.data());
+        const Core::IndexRange all = IO::indexRange(cf);
+        std::vector<float> buf = IO::gatherAOS<float>(cf, all);
+        EXPECT(buf.size() == 512);
+        for (size_t i = 0; i < 512; ++i) EXPECT(buf[i] == f[i]);
+        Grid::Cartesian<float> vf({1, 1, 1}, {8, 8, 8}, {0, 0, 0}, {1, 1, 1}, 3);
+        for (int c = 0; c < 3; ++c) {
+            std::vector<float> v(vf.componentStride(), (c + 1) * 1.234f);
+            vf.upload(v.data(), c);
+        }
+        buf = IO::gatherAOS<float>(vf, all);
+        for (size_t i = 0; i < 512; ++i)
+            for (int c = 0; c < 3; ++c) EXPECT(buf[c + 3 * i] == (c + 1) * 1.234f);
+        // sub-range [2, 5)^3 of a field that is 1.234 there and 0 elsewhere
+        Core::IndexRange sub;
+        sub.begin = {2, 2, 2};
+        sub.end = {5, 5, 5};
+        for (int z = 0; z < 8; ++z)
+            for (int y = 0; y < 8; ++y)
+                for (int x = 0; x < 8; ++x) {
+                    const bool in = x >= 2 && x < 5 && y >= 2 && y < 5 && z >= 2 && z < 5;
+                    f[x + 8 * (y + 8 * z)] = in ? 1.234f : 0.0f;
+                }
+        cf.upload(f.data());
+        buf = IO::gatherAOS<float>(cf, sub);
+        EXPECT(buf.size() == 27);
+        for (float v : buf) EXPECT(v == 1.234f);
+        // 2x2x2 blocks of 4^3, FP64 grid written as float: the file is the
+        // global array, x fastest
+        Grid::Cartesian<double> g2({2, 2, 2}, {4, 4, 4});
+        std::vector<double> h2(g2.componentStride());
+        for (int b = 0; b < 8; ++b)
+            for (int i = 0; i < 64; ++i) {
+                const int bx = b % 2, by = (b / 2) % 2, bz = b / 4;
+                const int x = 4 * bx + i % 4, y = 4 * by + (i / 4) % 4, z = 4 * bz + i / 16;
+                h2[(size_t)b * g2.blockStride() + i] = x + 8.0 * (y + 8.0 * z) + 0.5;
+            }
+        g2.upload(h2.data());
+        std::vector<float> b2 = IO::gatherAOS<float>(g2, IO::indexRange(g2));
+        for (size_t i = 0; i < b2.size(); ++i) EXPECT(b2[i] == (float)(i + 0.5));
+        // read back: AOS2Field of the file into a zeroed grid restores it
+        Grid::Cartesian<double> g3({2, 2, 2}, {4, 4, 4});
+        std::vector<double> z3(g3.componentStride(), 0.0);
+        g3.upload(z3.data());
+        void *d = nullptr;
+        check(cn_device_alloc(b2.size() * sizeof(float), &d));
+        check(cn_memcpy(d, b2.data(), b2.size() * sizeof(float), nullptr));
+        IO::AOS2Field(static_cast<const float *>(d), IO::indexRange(g3), g3);
+        std::vector<double> back(g3.componentStride());
+        g3.download(back.data());
+        cn_device_free(d);
+        for (int b = 0; b < 8; ++b)
+            for (int i = 0; i < 64; ++i)
+                EXPECT(back[(size_t)b * g3.blockStride() + i] == h2[(size_t)b * g2.blockStride() + i]);
     }
     std::printf("%s (%d failures)\n", failures ? "FAIL" : "PASS", failures);
     return failures ? 1 : 0;
