@@ -76,8 +76,9 @@ __device__ __forceinline__ int64_t dense_cell(const LabGeom &L, const TilePos &q
 }
 
 // Coefficients of one level (see op7_coef) in precision TC (float for the
-// V-cycle, double for the outer FP64 residual): k staged per tile with its
-// one-cell halo, then per cell the operations of op7_math in TC.
+// V-cycle; resid64_kernel forms the FP64 means itself with the same
+// operations): k staged per tile with its one-cell halo, then per cell the
+// operations of op7_math in TC.
 template <typename TC>
 __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const __grid_constant__ KArgs a,
                                                                           const __grid_constant__ Tile T, TC ih2,
@@ -112,6 +113,57 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) coef_kernel(const 
         }
         cv[6] = ih2 * ((sd[0] + sd[1]) + sd[2]);
         cv[7] = TC(0);
+    }
+}
+
+// FP64 harmonic face means of the finest level, each face once: per block
+// the x faces ((n0 + 1) n1 n2, face i between cells i - 1 and i), then the y
+// and z faces, x fastest.  A cell writes its +d faces, and cells on the
+// block's lower side also their -d face, with the operations of coef_kernel:
+// harm(kc, k(+e_d)) and harm(k(-e_d), kc), which are the same bits since
+// harm is symmetric.  Boundary faces use this block's lab of k.
+__host__ __device__ inline int64_t face_count(const int n[3])
+{
+    return (int64_t)(n[0] + 1) * n[1] * n[2] + (int64_t)n[0] * (n[1] + 1) * n[2] + (int64_t)n[0] * n[1] * (n[2] + 1);
+}
+
+__device__ __forceinline__ int64_t face_index(const int n[3], int d, int x, int y, int z)
+{
+    if (d == 0) return x + (int64_t)(n[0] + 1) * (y + (int64_t)n[1] * z);
+    const int64_t fx = (int64_t)(n[0] + 1) * n[1] * n[2];
+    if (d == 1) return fx + x + (int64_t)n[0] * (y + (int64_t)(n[1] + 1) * z);
+    return fx + (int64_t)n[0] * (n[1] + 1) * n[2] + x + (int64_t)n[0] * (y + (int64_t)n[1] * z);
+}
+
+__global__ void __launch_bounds__(kTileThreads, kTileMinCtas) face64_kernel(const __grid_constant__ KArgs a,
+                                                                            const __grid_constant__ Tile T,
+                                                                            double *faces)
+{
+    __shared__ __align__(16) float sk[kRegionMax];
+    __shared__ int snb[27];
+    const LabGeom &L = a.G.Lk;
+    TilePos q = tile_pos(T);
+    region_layout<float>(q, L);
+    neighbour_blocks(L.nb, q.block, snb);
+    __syncthreads();
+    stage_region<float>(a.k, L, a.kbc, q, false, snb, sk);
+    cp_async_wait_all();
+    __syncthreads();
+    int x, y, z0, zl;
+    if (!column_run(T, x, y, z0, zl)) return;
+    const int st[3] = {1, q.rs, q.rs * q.ey};
+    double *fb = faces + (int64_t)q.block * face_count(L.n);
+    for (int z = z0; z < z0 + zl; ++z) {
+        const int u = ridx(q, x, y, z);
+        const double kc = (double)sk[u];
+        const int g[3] = {q.x0 + x, q.y0 + y, q.z0 + z};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int ex = d == 0, ey = d == 1, ez = d == 2;
+            fb[face_index(L.n, d, g[0] + ex, g[1] + ey, g[2] + ez)] = harm<double>(kc, (double)sk[u + st[d]]);
+            if (g[d] == 0)
+                fb[face_index(L.n, d, g[0], g[1], g[2])] = harm<double>((double)sk[u - st[d]], kc);
+        }
     }
 }
 
@@ -295,12 +347,15 @@ __global__ void __launch_bounds__(kTileThreads, kTileMinCtas) prolong_kernel(con
     }
 }
 
-// FP64 residual of the outer iteration: r = f - L p64 (p64 += e first if e),
-// r32 = (float) r, per-CTA FP64 partial sums of r^2 (and f^2).
+// FP64 residual of the outer iteration: r = f - L p64, r32 = (float) r,
+// per-CTA FP64 partial sums of r^2 and f^2.  The tile's p64 is staged with
+// its one-cell halo; the six face means of a cell come from the FP64 face
+// arrays (face64_kernel) and are applied in op7_coef's order, so L p64 is
+// bit for bit the operator of the per-cell coefficients.
 __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_constant__ KArgs a,
                                                                const __grid_constant__ Tile T, const double *p64,
                                                                const float *f, float *r32, double *partials,
-                                                               const double *coef64)
+                                                               const double *faces)
 {
     __shared__ __align__(16) double sp[kRegionMax];
     __shared__ double sh[2][kTileThreads / 32];
@@ -317,13 +372,21 @@ __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_c
     int x, y, z0, zl;
     if (column_run(T, x, y, z0, zl)) {
         const int st[3] = {1, q.rs, q.rs * q.ey};
-        const int64_t cells = (int64_t)Lk.n[0] * Lk.n[1] * Lk.n[2];
+        const double *fb = faces + (int64_t)q.block * face_count(Lk.n);
         for (int z = z0; z < z0 + zl; ++z) {
-            const int64_t cell = dense_cell(Lk, q, x, y, z);
-            const int64_t o = (int64_t)q.block * Lk.bstride + cell; // FP32 fields (f, r32)
-            double Lp, D, pc;
-            op7_coef<double, double>(sp, ridx(q, x, y, z), st, coef64 + ((int64_t)q.block * cells + cell) * kCoefPerCell,
-                                     a.ih2d, Lp, D, pc);
+            const int64_t o = (int64_t)q.block * Lk.bstride + dense_cell(Lk, q, x, y, z); // FP32 fields (f, r32)
+            const int u = ridx(q, x, y, z);
+            const int g[3] = {q.x0 + x, q.y0 + y, q.z0 + z};
+            const double pc = sp[u];
+            double fd[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const int ex = d == 0, ey = d == 1, ez = d == 2;
+                const double kp = __ldg(fb + face_index(Lk.n, d, g[0] + ex, g[1] + ey, g[2] + ez));
+                const double km = __ldg(fb + face_index(Lk.n, d, g[0], g[1], g[2]));
+                fd[d] = kp * (sp[u + st[d]] - pc) - km * (pc - sp[u - st[d]]);
+            }
+            const double Lp = a.ih2d * ((fd[0] + fd[1]) + fd[2]);
             const double fc = (double)__ldg(f + o);
             const double r = fc - Lp;
             if (r32) r32[o] = (float)r;
@@ -826,8 +889,9 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
     }
     if (s == CN_OK) s = sync_bc(m->p[0], nullptr);
     if (s == CN_OK) s = sync_bc(k, nullptr);
-    // operator coefficients of every level (k is fixed from here on): 8 per
-    // cell, FP32 for the V-cycle levels and FP64 for the finest level
+    // operator coefficients of every level (k is fixed from here on): 8 FP32
+    // values per cell for the V-cycle, FP64 face means of the finest level for
+    // the outer residual
     for (int l = 0; l < levels && s == CN_OK; ++l) {
         const int64_t cells = (int64_t)k->nblocks * m->p[l]->n[0] * m->p[l]->n[1] * m->p[l]->n[2];
         float *c = nullptr;
@@ -842,15 +906,14 @@ cn_status cn_mg_create(cn_grid *k, int nu1, int nu2, double omega, int max_level
         if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
     }
     if (s == CN_OK) {
-        const int64_t cells = (int64_t)k->nblocks * k->n[0] * k->n[1] * k->n[2];
-        if (cudaMalloc(&m->coef64, sizeof(double) * kCoefPerCell * cells) != cudaSuccess)
-            s = fail(CN_ERR_OUT_OF_MEMORY, "cn_mg_create: coefficients");
-    }
-    if (s == CN_OK) {
-        const KArgs a = kargs(m, 0);
-        const Tile T = tile_of(k->n);
-        coef_kernel<double><<<(unsigned)(k->nblocks * T.count), kTileThreads>>>(a, T, a.ih2d, m->coef64);
-        if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "coef_kernel launch");
+        if (cudaMalloc(&m->face64, sizeof(double) * face_count(k->n) * k->nblocks) != cudaSuccess) {
+            s = fail(CN_ERR_OUT_OF_MEMORY, "cn_mg_create: face means");
+        } else {
+            const KArgs a = kargs(m, 0);
+            const Tile T = tile_of(k->n);
+            face64_kernel<<<(unsigned)(k->nblocks * T.count), kTileThreads>>>(a, T, m->face64);
+            if (cudaGetLastError() != cudaSuccess) s = fail(CN_ERR_CUDA, "face64_kernel launch");
+        }
     }
     if (s == CN_OK && cudaDeviceSynchronize() != cudaSuccess) s = fail(CN_ERR_CUDA, "cn_mg_create");
     if (s == CN_OK && coarse_cells <= kCoarseDenseMax) s = coarse_inverse(m);
@@ -873,9 +936,9 @@ cn_status cn_mg_destroy(cn_mg *m)
         if (l > 0) cn_grid_destroy(m->k[l]);
     }
     cn_grid_destroy(m->r32);
+    if (m->face64) cudaFree(m->face64);
     for (float *c : m->coef)
         if (c) cudaFree(c);
-    if (m->coef64) cudaFree(m->coef64);
     if (m->coarse_inv) cudaFree(m->coarse_inv);
     for (cn_grid *g : m->nn_bufs) cn_grid_destroy(g);
     for (void *a : m->nn_act)
@@ -933,7 +996,7 @@ cn_status cn_mg_residual(cn_mg *m, const cn_grid *p64, const cn_grid *f, cn_grid
     a.G.bc = bc_view(p64, 0);
     resid64_kernel<<<m->nparts, kTileThreads, 0, st>>>(
         a, tile_of(p64->n), reinterpret_cast<const double *>(p64->d_data), reinterpret_cast<const float *>(f->d_data),
-        r32 ? fptr(r32) : nullptr, m->partials, m->coef64);
+        r32 ? fptr(r32) : nullptr, m->partials, m->face64);
     CN_CUDA_TRY(cudaGetLastError());
     sum_pairs_kernel<<<1, 256, 0, st>>>(m->partials, m->nparts, m->sums);
     CN_CUDA_TRY(cudaGetLastError());

@@ -13,7 +13,7 @@ struct cn_mg {
     double omega;
     std::vector<cn_grid *> p, pt, f, k; // per level (FP32); k[0] is the caller's grid
     std::vector<float *> coef;          // per level: 8 FP32 per cell (k+ faces x,y,z, k- faces x,y,z, D, 0)
-    double *coef64 = nullptr;           // the same for the finest level in FP64 (outer residual)
+    double *face64 = nullptr;           // finest level: FP64 harmonic face means, per block x, y, z faces
     cn_grid *r32 = nullptr;             // finest FP32 residual
     double *partials = nullptr;
     double *sums = nullptr;
