@@ -253,6 +253,12 @@ cn_status run(cn_grid *g, int comp0, int ncomp, const int span_begin[3], const i
         return fail(CN_ERR_INVALID_ARGUMENT, std::string(who) + ": buffer is NULL");
     }
     if (G.ie[0] == 0 || rows == 0) return CN_OK; // empty intersection
+    // the kernel dereferences buf: device, managed or pinned host memory only
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, buf) != cudaSuccess || pa.type == cudaMemoryTypeUnregistered) {
+        cudaGetLastError();
+        return fail(CN_ERR_INVALID_ARGUMENT, std::string(who) + ": buffer is not device-accessible memory");
+    }
     G.comp0 = comp0;
     G.ncomp = ncomp;
     G.chunks = (G.ie[0] + kPts - 1) / kPts;

@@ -90,8 +90,9 @@ def Field2AOS(grid, span=None, file_dtype=None, comps=None, out=None, face_dir=0
     shape = (e[2] - b[2], e[1] - b[1], e[0] - b[0], nc)
     if out is None:
         out = torch.zeros(shape, dtype=_torch_dtype(fdt), device="cuda")
-    elif tuple(out.shape) != shape or out.dtype != _torch_dtype(fdt) or not out.is_contiguous():
-        raise ValueError(f"Field2AOS: out must be a contiguous {fdt} tensor of shape {shape}")
+    elif (tuple(out.shape) != shape or out.dtype != _torch_dtype(fdt) or not out.is_contiguous()
+          or not out.is_cuda):
+        raise ValueError(f"Field2AOS: out must be a contiguous CUDA {fdt} tensor of shape {shape}")
     _lib.check(_lib.lib().cn_grid_to_aos(g.handle, int(c0), int(nc), _lib.ivec3(b), _lib.ivec3(e), _DT[fdt],
                                          C.c_void_p(out.data_ptr()), _stream_handle(stream)))
     return out

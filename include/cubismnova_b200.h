@@ -145,7 +145,8 @@ cn_status cn_grid_copy(cn_grid *dst, const cn_grid *src, void *stream);
  * (the HDF dataset, x fastest); for every point p of it inside the grid,
  *   d_buf[c + ncomp * flat(p - span_begin)] = (file type) component comp0 + c at p,
  * c < ncomp <= 16.  Points of the range outside the grid are not written.
- * d_buf is device memory of span volume * ncomp elements of file_dtype.
+ * d_buf is device (or managed / pinned host) memory of span volume * ncomp
+ * elements of file_dtype; other host memory is rejected (CN_ERR_INVALID_ARGUMENT).
  * Conversions follow C++ (double -> float rounds to nearest); a
  * floating-point grid cannot be written as int32 (CN_ERR_UNSUPPORTED).
  * Stream-ordered; no allocation. */

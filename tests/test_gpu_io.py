@@ -217,6 +217,12 @@ def test_errors(cn):
     e = (C.c_int * 3)(4, -1, 4)
     st = _lib.lib().cn_grid_to_aos(g.handle, 0, 1, b, e, 1, C.c_void_p(buf.data_ptr()), None)
     assert st == 1 and b"end before begin" in _lib.lib().cn_last_error_string()
+    host = np.zeros(8 * 8 * 8, dtype=np.float64)  # pageable host memory: rejected before any launch
+    st = _lib.lib().cn_grid_to_aos(g.handle, 0, 1, (C.c_int * 3)(0, 0, 0), (C.c_int * 3)(8, 8, 8), 1,
+                                   C.c_void_p(host.ctypes.data), None)
+    assert st == 1 and b"not device-accessible" in _lib.lib().cn_last_error_string()
+    with pytest.raises(ValueError):
+        cn.IO.Field2AOS(g, comps=(0, 1), out=torch.zeros((8, 8, 8, 1), dtype=torch.float64))
     big = cn.Grid.Cartesian((1, 1, 1), (4, 4, 4), ncomp=17)
     with pytest.raises(cn.CnError):  # more than 16 components in one call
         cn.IO.Field2AOS(big)
