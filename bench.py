@@ -827,6 +827,85 @@ class IOW:
             self.h_out.copy_(self.buf, non_blocking=True)
         return 3 * nbytes, self.buf.numel() * 4
 
+    E2E_PINNED_BUDGET = 48e9
+    ranks_per_node = 1
+    e2e_path = ("C ABI, device slots in turn: step i+1's upload (cn_grid_upload from pinned host) and step "
+                "i-1's download of the file buffer to pinned host run on their own streams while step i "
+                "gathers (cn_grid_to_aos)")
+
+    def _pinned_bytes(self, n):
+        """Pinned host bytes of n slots: the shared input copy plus one output per slot."""
+        return 3 * self.u.comp_stride * 8 + n * self.buf.numel() * 4
+
+    def e2e_slots(self):
+        for n in (3, 2):
+            if self._pinned_bytes(n) * self.ranks_per_node <= self.E2E_PINNED_BUDGET:
+                return n
+        return 1
+
+    def _new_slot(self):
+        torch = self.torch
+        u = self.cn.Grid.Cartesian(self.nb, self.n, ncomp=3)
+        return dict(u=u, buf=torch.empty_like(self.buf), out=torch.empty_like(self.h_out).pin_memory())
+
+    def _slot0(self):
+        return dict(u=self.u, buf=self.buf, out=self.h_out)
+
+    def _upload(self, slot, s):
+        import ctypes as C
+        lib = self.cn._lib.lib()
+        for c in range(3):
+            self.cn._lib.check(lib.cn_grid_upload(slot["u"].handle, c, C.c_void_p(self.h_in[c].data_ptr()),
+                                                  self.u.comp_stride * 8, C.c_void_p(s.cuda_stream)))
+
+    def _compute(self, slot, s):
+        self.cn.IO.Field2AOS(slot["u"], file_dtype=np.float32, out=slot["buf"], stream=s)
+
+    def _download(self, slot, s):
+        with self.torch.cuda.stream(s):
+            slot["out"].copy_(slot["buf"], non_blocking=True)
+
+    def _bytes(self):
+        return 3 * self.u.comp_stride * 8, self.buf.numel() * 4
+
+    def e2e_pipelined(self, stream, k):
+        """k independent steps (upload, gather or scatter, download) over
+        several device slots so that both copy directions overlap the
+        neighbouring steps' kernels.  A slot's next upload waits until its
+        kernel has read it, its next kernel until its result is home."""
+        torch = self.torch
+        if getattr(self, "pipe", None) is None:
+            slots = [self._slot0()] + [self._new_slot() for _ in range(self.e2e_slots() - 1)]
+            self.pipe = dict(slots=slots, s_in=torch.cuda.Stream(), s_out=torch.cuda.Stream())
+        P = self.pipe
+        s_in, s_out, slots = P["s_in"], P["s_out"], P["slots"]
+        start = torch.cuda.Event()
+        start.record(stream)
+        s_in.wait_event(start)
+        s_out.wait_event(start)
+        used, home = [None] * len(slots), [None] * len(slots)
+        for i in range(k):
+            j = i % len(slots)
+            if used[j] is not None:
+                s_in.wait_event(used[j])
+            self._upload(slots[j], s_in)
+            up = torch.cuda.Event()
+            up.record(s_in)
+            stream.wait_event(up)
+            if home[j] is not None:
+                stream.wait_event(home[j])
+            self._compute(slots[j], stream)
+            used[j] = torch.cuda.Event()
+            used[j].record(stream)
+            s_out.wait_event(used[j])
+            self._download(slots[j], s_out)
+            home[j] = torch.cuda.Event()
+            home[j].record(s_out)
+        for ev in home:
+            if ev is not None:
+                stream.wait_event(ev)
+        return self._bytes()
+
     @classmethod
     def cpu_sample_static(cls, threads, reps=3):
         """The reference's Field2AOS block loop (oracle/_ref, OpenMP over
@@ -883,6 +962,38 @@ class IOR(IOW):
         self.cn.IO.AOS2Field(self.buf, self.u, stream=stream)
         if events is not None:
             events[1].record(stream)
+
+    e2e_path = ("C ABI, device slots in turn: step i+1's upload of the file buffer from pinned host and step "
+                "i-1's download of the grid (cn_grid_download to pinned host) run on their own streams while "
+                "step i scatters (cn_grid_from_aos)")
+
+    def _pinned_bytes(self, n):
+        return self.buf.numel() * 4 + n * 3 * self.u.comp_stride * 8
+
+    def _new_slot(self):
+        torch = self.torch
+        return dict(u=self.cn.Grid.Cartesian(self.nb, self.n, ncomp=3), buf=torch.empty_like(self.buf),
+                    out=[torch.empty_like(self.h_in[c]).pin_memory() for c in range(3)])
+
+    def _slot0(self):
+        return dict(u=self.u, buf=self.buf, out=self.h_grid)
+
+    def _upload(self, slot, s):
+        with self.torch.cuda.stream(s):
+            slot["buf"].copy_(self.h_file, non_blocking=True)
+
+    def _compute(self, slot, s):
+        self.cn.IO.AOS2Field(slot["buf"], slot["u"], stream=s)
+
+    def _download(self, slot, s):
+        import ctypes as C
+        lib = self.cn._lib.lib()
+        for c in range(3):
+            self.cn._lib.check(lib.cn_grid_download(slot["u"].handle, c, C.c_void_p(slot["out"][c].data_ptr()),
+                                                    self.u.comp_stride * 8, C.c_void_p(s.cuda_stream)))
+
+    def _bytes(self):
+        return self.buf.numel() * 4, 3 * self.u.comp_stride * 8
 
     def e2e_step(self, stream):
         import ctypes as C
