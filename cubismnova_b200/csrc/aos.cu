@@ -157,11 +157,10 @@ __global__ void __launch_bounds__(kThreads, min_ctas(TO_AOS, MAXC))
 template <typename T, typename F, bool TO_AOS, int MAXC>
 cn_status launch_one(const Geo &G, T *data, F *buf, size_t smem, int grid, cudaStream_t s)
 {
-    static bool opted = false;
-    if (smem > kSmemDefault && !opted) {
+    // the opt-in is a property of the current device's context: set it on every large launch
+    if (smem > kSmemDefault) {
         CN_CUDA_TRY(cudaFuncSetAttribute(aos_kernel<T, F, TO_AOS, MAXC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kPts * kMaxComp * sizeof(F))));
-        opted = true;
     }
     aos_kernel<T, F, TO_AOS, MAXC><<<grid, kThreads, smem, s>>>(G, data, buf);
     CN_CUDA_TRY(cudaGetLastError());
@@ -171,12 +170,9 @@ cn_status launch_one(const Geo &G, T *data, F *buf, size_t smem, int grid, cudaS
 template <typename T, typename F>
 cn_status launch(const Geo &G, cn_grid *g, void *buf, bool to_aos, cudaStream_t s)
 {
-    static int nsm = 0;
-    if (nsm == 0) {
-        int dev = 0;
-        CN_CUDA_TRY(cudaGetDevice(&dev));
-        CN_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    }
+    int dev = 0, nsm = 0;
+    CN_CUDA_TRY(cudaGetDevice(&dev));
+    CN_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     // up to 8 resident CTAs of 256 threads per SM, grid-stride over the items
     const int grid = G.items < nsm * 8 ? G.items : nsm * 8;
     const size_t smem = (size_t)kPts * G.ncomp * sizeof(F);
