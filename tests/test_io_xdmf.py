@@ -61,3 +61,35 @@ def test_without_hdf5_the_writers_report(capsys):
     err = capsys.readouterr().err
     assert "CartesianWriteHDF: HDF not supported (out/f)" in err
     assert "CartesianReadHDF: HDF not supported (out/f)" in err
+
+
+class _Topo:
+    def __init__(self, entity, nb, cells):
+        self.entity, self._nb, self._cells = entity, nb, cells
+
+    def getSize(self):
+        return self._nb
+
+    def getBlockCells(self):
+        return self._cells
+
+
+def test_whole_grid_file_range_per_entity():
+    """The file range of a whole-grid write (IO/CartesianHDF.h:63-69 with the
+    global mesh): cells, or cells + 1 along grown dimensions."""
+    nb, cells = (2, 3, 4), (5, 6, 7)
+    want = {"cell": (10, 18, 28), "node": (11, 19, 29), "face_x": (11, 18, 28), "face_y": (10, 19, 28),
+            "face_z": (10, 18, 29)}
+    for ent, e in want.items():
+        assert IO.index_range(_Topo(ent, nb, cells)) == ((0, 0, 0), e)
+
+
+def test_file_range_validation():
+    g = _Topo("cell", (1, 1, 1), (4, 4, 4))
+    assert IO._span(g, None, 0) == ((0, 0, 0), (4, 4, 4))
+    assert IO._span(g, ((-1, 0, 2), (5, 4, 2)), 0) == ((-1, 0, 2), (5, 4, 2))  # empty z extent is allowed
+    try:
+        IO._span(g, ((0, 0, 0), (4, -1, 4)), 0)
+        raise AssertionError("end before begin accepted")
+    except ValueError as e:
+        assert "end before begin" in str(e)
