@@ -485,11 +485,12 @@ class Euler:
                             f"best of {reps}, {threads} threads"),
                     seconds_per_sweep=t)
 
+    cpu_nb = (8, 8, 4)  # blocks of the CPU sample (cpu_baseline and the reference arm)
+
     def cpu_sample(self, threads):
         """About 10 s of host work: the stage on 8x8x4 blocks, repeated."""
-        nb = (8, 8, 4)
-        t1 = self.cpu_sample_static(threads, reps=1, nb=nb)["seconds_per_sweep"]
-        return self.cpu_sample_static(threads, reps=int(min(100, max(1, 10.0 / t1))), nb=nb)
+        t1 = self.cpu_sample_static(threads, reps=1, nb=self.cpu_nb)["seconds_per_sweep"]
+        return self.cpu_sample_static(threads, reps=int(min(100, max(1, 10.0 / t1))), nb=self.cpu_nb)
 
 
 class C2(Euler):
@@ -1166,12 +1167,14 @@ def run_reference(args, world, rank):
         return None
     W = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
+    # the sample of the cpu_baseline leg (same blocks), best of 3 per step
+    kw = {"nb": W.cpu_nb} if hasattr(W, "cpu_nb") else {}
     for _ in range(args.warmup):
-        W.cpu_sample_static(threads, reps=1)
+        W.cpu_sample_static(threads, reps=1, **kw)
     vals, secs = [], []
     r = None
     for _ in range(args.steps):
-        r = W.cpu_sample_static(threads, reps=1)
+        r = W.cpu_sample_static(threads, reps=3, **kw)
         vals.append(r["value"])
         secs.append(r["seconds_per_sweep"])
     v = float(np.median(vals))

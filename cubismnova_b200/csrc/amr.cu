@@ -153,13 +153,9 @@ static Geom geom(const cn_amr *a)
 
 template <typename T> static cn_status set_smem_once()
 {
-    static bool done = false;
-    if (!done) {
-        const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NFACE) * sizeof(T);
-        CN_CUDA_TRY(cudaFuncSetAttribute(amr::stage_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        done = true;
-    }
-    return CN_OK;
+    static DeviceOnce once; // per device
+    const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NFACE) * sizeof(T);
+    return smem_opt_in(once, amr::stage_kernel<T>, smem);
 }
 
 template <typename T>

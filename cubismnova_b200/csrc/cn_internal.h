@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -95,9 +96,45 @@ cn_status check_stencil(const cn_stencil *s);
 cn_status check_lab(const cn_grid *g, const cn_stencil *s);
 // Uploads the BC tables if they changed.
 cn_status sync_bc(cn_grid *g, cudaStream_t stream);
+// True when sync_bc would have to grow the device BC entry table (cudaMalloc).
+bool sync_bc_would_allocate(const cn_grid *g);
 BcView bc_view(const cn_grid *g, int comp);
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Runs a set-up step once per device, on the current device: a kernel's
+// shared-memory opt-in belongs to each device's context, so a process-wide
+// flag would leave the second device without it.  Thread-safe; a failed step
+// is retried on the next call.
+class DeviceOnce {
+  public:
+    template <typename F> cn_status run(F &&fn)
+    {
+        int dev = 0;
+        const cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+        if (dev < 0 || dev >= kMaxDevices) return fail(CN_ERR_UNSUPPORTED, "device index out of range");
+        std::lock_guard<std::mutex> lk(mu_);
+        if (done_[dev]) return CN_OK;
+        const cn_status s = fn();
+        if (s == CN_OK) done_[dev] = true;
+        return s;
+    }
+
+  private:
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu_;
+    bool done_[kMaxDevices] = {};
+};
+
+// Opts `kernel` into `bytes` of dynamic shared memory, once per device.
+template <typename K> inline cn_status smem_opt_in(DeviceOnce &once, K kernel, size_t bytes)
+{
+    return once.run([&]() -> cn_status {
+        CN_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        return CN_OK;
+    });
+}
 
 // Geometry of a lab for one stencil on one grid.
 struct LabGeom {

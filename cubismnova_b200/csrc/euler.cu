@@ -142,12 +142,9 @@ static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, 
     p.partials = partials;
     p.err = Us->d_err;
     const size_t smem = (size_t)(5 * Stg<T>::SV + 5 * NFACE) * sizeof(T);
-    // set once (outside any graph capture: the first call is an eager one)
-    static bool attr_done = false;
-    if (!attr_done) {
-        CN_CUDA_TRY(cudaFuncSetAttribute(stage_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_done = true;
-    }
+    static DeviceOnce attr_once; // per device (the first call on a device is an eager one)
+    r = smem_opt_in(attr_once, stage_kernel<T>, smem);
+    if (r != CN_OK) return r;
     const int64_t ctas = (int64_t)Us->nblocks * (Us->n[0] / TB) * (Us->n[1] / TB) * (Us->n[2] / TB);
     stage_kernel<T><<<(unsigned)ctas, NT, smem, st>>>(p, src);
     CN_CUDA_TRY(cudaGetLastError());
@@ -296,13 +293,14 @@ cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stre
 // SSP-RK3 stage with conservation sums and no device allocation.
 //
 // cn_euler_rk3_stage grows its per-CTA partials with cudaMalloc on first use
-// and whenever a larger grid arrives.  Some callers cannot allow that: a
-// solver that captures its time step into a CUDA graph (a cudaMalloc during
-// capture is not a stream operation and breaks the capture), a host that runs
-// with a fixed device-memory budget reserved up front, or one that must not
-// synchronise the device mid-run the way a first-time cudaMalloc/cudaFree may.
-// This variant takes its scratch from a fixed file-scope device array instead,
-// so a call never allocates; the price is a hard limit on the grid size.
+// and whenever a larger grid arrives.  Some callers cannot allow that: a host
+// that runs with a fixed device-memory budget reserved up front (a solver
+// sharing the GPU with a pool allocator that owns the rest of the memory), or
+// one that must not let a first-time cudaMalloc/cudaFree synchronise the
+// device mid-run.  This variant takes its scratch from a fixed file-scope
+// device array instead, so a call never allocates; the price is a hard limit
+// on the grid size.  Like cn_euler_rk3_stage it copies the sums to the host
+// and waits for the stream before it returns.
 //
 // Size: one 5-double partial per 8^3 tile plus the 5 totals, for at most
 // kStaticSumTiles tiles (16.8M cells, e.g. 256^3), 1.25 MiB per device.
@@ -312,8 +310,11 @@ cn_status cn_euler_max_speed(cn_grid *U, double gamma, double out[3], void *stre
 // overlap on the same device (two streams, or two host threads) race on it
 // and may return each other's sums; callers serialise them.
 // Set-up: the first call on a device, with that device current, looks up the
-// array's device address with cudaGetSymbolAddress and keeps it; that first
-// call should be made before any stream capture begins.
+// array's device address with cudaGetSymbolAddress and keeps it.
+// BC tables: the stage uploads changed BC vectors of `bcsrc` before its
+// launch; if they grew beyond the device table's capacity that upload would
+// allocate, so the call is refused (CN_ERR_INVALID_ARGUMENT) and the caller
+// runs cn_bc_sync once after changing the BCs, before the no-allocation calls.
 // --------------------------------------------------------------------------
 static constexpr int64_t kStaticSumTiles = 32768;
 static __device__ __align__(256) double g_static_sums[kStaticSumTiles * 5 + 5];
@@ -353,6 +354,10 @@ extern "C" cn_status cn_euler_rk3_stage_noalloc(cn_grid *bcsrc, cn_grid *Us, cn_
         return fail(CN_ERR_UNSUPPORTED,
                     "cn_euler_rk3_stage_noalloc: grid has more than 32768 8^3 tiles (16.8M cells), "
                     "the size of its fixed scratch");
+    if (sync_bc_would_allocate(bcsrc))
+        return fail(CN_ERR_INVALID_ARGUMENT,
+                    "cn_euler_rk3_stage_noalloc: the BC vectors grew since the last upload; call cn_bc_sync "
+                    "before the no-allocation stage");
     double *scratch = nullptr;
     s = static_sum_scratch(&scratch);
     if (s != CN_OK) return s;

@@ -166,6 +166,16 @@ cn_status sync_bc(cn_grid *g, cudaStream_t stream)
     return CN_OK;
 }
 
+bool sync_bc_would_allocate(const cn_grid *g)
+{
+    if (!g->bc_dirty) return false;
+    size_t n = 0;
+    for (const auto &comp : g->bcs)
+        for (const auto &v : comp) n += v.size();
+    if (n == 0) n = 1; // an empty table still holds one entry
+    return n > g->bc_ent_cap;
+}
+
 BcView bc_view(const cn_grid *g, int comp)
 {
     BcView v;

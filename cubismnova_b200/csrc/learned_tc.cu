@@ -447,7 +447,7 @@ __global__ void pack_weights_kernel(const float *W, int cin, int cout, uint16_t 
     out[i] = bf16_bits(v);
 }
 
-static bool attr_set[3], pipe_attr_set[3]; // per mode (1: hidden layer, 2: last layer + update)
+static DeviceOnce attr_set[3], pipe_attr_set[3]; // per mode (1: hidden layer, 2: last layer + update) and device
 // kernel form: 1 = persistent warp-specialised pipeline, 0 = one brick per CTA
 static int g_conv_form = 1;
 
@@ -456,11 +456,8 @@ static cn_status launch(const Params &P, int nblocks, cudaStream_t st)
 {
     const int64_t bricks = (int64_t)nblocks * P.bricks[0] * P.bricks[1] * P.bricks[2];
     if (g_conv_form == 1) {
-        if (!pipe_attr_set[MODE]) {
-            CN_CUDA_TRY(cudaFuncSetAttribute(conv3_tc_pipe<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)PIPE_SMEM));
-            pipe_attr_set[MODE] = true;
-        }
+        cn_status s = smem_opt_in(pipe_attr_set[MODE], conv3_tc_pipe<MODE>, PIPE_SMEM);
+        if (s != CN_OK) return s;
         int dev = 0, sms = 148;
         CN_CUDA_TRY(cudaGetDevice(&dev));
         CN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -469,11 +466,8 @@ static cn_status launch(const Params &P, int nblocks, cudaStream_t st)
         CN_CUDA_TRY(cudaGetLastError());
         return CN_OK;
     }
-    if (!attr_set[MODE]) {
-        CN_CUDA_TRY(cudaFuncSetAttribute(conv3_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM));
-        attr_set[MODE] = true;
-    }
+    cn_status s = smem_opt_in(attr_set[MODE], conv3_tc_kernel<MODE>, SMEM);
+    if (s != CN_OK) return s;
     conv3_tc_kernel<MODE><<<(unsigned)bricks, NTHREADS, SMEM, st>>>(P);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;

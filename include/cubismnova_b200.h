@@ -246,10 +246,14 @@ cn_status cn_euler_rk3_stage(cn_grid *bcsrc, cn_grid *Us, cn_grid *Un, cn_grid *
 /* cn_euler_rk3_stage with sums_out required and no device allocation: the
  * per-tile partials live in a fixed device array of the library (no
  * counterpart in the reference).  For callers that must not allocate during a
- * run (a step captured into a CUDA graph, a fixed memory budget).  Limit: at
- * most 32768 8^3 tiles (16.8M cells), else CN_ERR_UNSUPPORTED.  The first call
- * on a device looks the array up (make it before any stream capture); calls
- * that overlap on one device share the array and race. */
+ * run (a fixed device-memory budget owned by another allocator, no
+ * cudaMalloc/cudaFree synchronisation mid-run).  Like cn_euler_rk3_stage with
+ * sums it copies the sums to the host and waits for the stream.  Limit: at
+ * most 32768 8^3 tiles (16.8M cells), else CN_ERR_UNSUPPORTED.  BC vectors of
+ * bcsrc changed since the last upload must fit the device table it already
+ * has (else CN_ERR_INVALID_ARGUMENT: call cn_bc_sync first).  The first call
+ * on a device looks the array up; calls that overlap on one device share the
+ * array and race. */
 cn_status cn_euler_rk3_stage_noalloc(cn_grid *bcsrc, cn_grid *Us, cn_grid *Un, cn_grid *out, int stage,
                                      double dt, double gamma, double *sums_out, void *stream);
 /* U <- U^{n+1}: three stages through work1, work2 (same shape as U). */

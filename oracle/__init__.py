@@ -184,11 +184,6 @@ def gradient_f64(comp, nb, n, bclists, ih):
     return out
 
 
-def ddx(src, pitches, extent, factor, dst_pitches):
-    """ddx gold kernel on a pitched array; src is the full lab, offset given."""
-    raise NotImplementedError
-
-
 def ref_c1_sweep(comp, nb, n, ih2, ih, threads=0, nblocks=0, reps=1,
                  want_lap=True, want_grad=True):
     """Reference FieldLab + Laplacian/gradient loops with OpenMP; returns
