@@ -13,7 +13,8 @@
 // alpha_k = d_k / t_k normalise to omega_k = d_k*prod_{j!=k} t_j / D with
 // D = sum_k d_k*prod_{j!=k} t_j, so one division per reconstruction suffices:
 //   v = (w0*n0 + w1*n1 + w2*n2) / (6*D),  w0 = d0*t1*t2, w1 = d1*t0*t2, w2 = d2*t0*t1,
-// where n_k = 6*q_k are the candidate stencils' numerators.  The indicators
+// where n_k = 6*q_k are the candidate stencils' numerators, written as
+// 6*u_j plus differences so that v = u_j + (sum w_k e_k) / (6*D).  The indicators
 // beta_k and the products t_i t_j belong to the cell, not to the face: a
 // cell's left-biased state (at its upper face) and right-biased state (at its
 // lower face) share them.
@@ -69,24 +70,35 @@ __device__ __forceinline__ float weno5_scale(float s0, float s1, float s2)
     return __int_as_float(int(unsigned(254 - ((e0 + e1 + e2 - emin) >> 1)) << 23));
 }
 
-// Smoothness of cell j from u0..u4 = v[j-2..j+2]: with s_k = eps + beta_k
-// and t_k = s_k^2 for the stencils S0 = {j-2, j-1, j}, S1 = {j-1, j, j+1},
-// S2 = {j, j+1, j+2}, the products p12 = t1 t2, p02 = t0 t2, p01 = t0 t1.
+// Differences of the 5-point stencil u0..u4 = v[j-2..j+2] of cell j: the
+// smoothness indicators and both reconstructions are written in them, and a
+// state is the cell value u2 plus a correction, so that smooth data loses no
+// digits to the cancellation inside the candidate stencils.
+template <typename T> struct Diff5 {
+    T d01, d12, d23, d34;
+};
+template <typename T> __device__ __forceinline__ Diff5<T> weno5_diff(T u0, T u1, T u2, T u3, T u4)
+{
+    return {u1 - u0, u2 - u1, u3 - u2, u4 - u3};
+}
+
+// Smoothness of cell j: with s_k = eps + beta_k and t_k = s_k^2 for the
+// stencils S0 = {j-2, j-1, j}, S1 = {j-1, j, j+1}, S2 = {j, j+1, j+2}, the
+// products p12 = t1 t2, p02 = t0 t2, p01 = t0 t1.  beta_k = 13/12 a_k^2 +
+// 1/4 b_k^2 with a0 = d12 - d01, a1 = d23 - d12, a2 = d34 - d23 and
+// b0/2 = a0/2 + d12, b1/2 = (d12 + d23)/2 (up to sign), b2/2 = a2/2 - d23.
 // They serve both states of the cell (left-biased at j+1/2, right-biased at
 // j-1/2), so a cell's indicators are computed once for its two faces.
-template <typename T>
-__device__ __forceinline__ void weno5_beta(T u0, T u1, T u2, T u3, T u4, T &p12, T &p02, T &p01)
+template <typename T> __device__ __forceinline__ void weno5_beta(const Diff5<T> &d, T &p12, T &p02, T &p01)
 {
     using C = K<T>;
-    const T a0 = dfma(T(-2), u1, u0) + u2;            // u0 - 2u1 + u2
-    const T b0 = dfma(T(3), u2, dfma(T(-4), u1, u0)); // u0 - 4u1 + 3u2
-    const T a1 = dfma(T(-2), u2, u1) + u3;            // u1 - 2u2 + u3
-    const T b1 = u1 - u3;
-    const T a2 = dfma(T(-2), u3, u2) + u4;            // u2 - 2u3 + u4
-    const T b2 = dfma(T(3), u2, dfma(T(-4), u3, u4)); // 3u2 - 4u3 + u4
-    const T s0 = C::eps + dfma(C::c1312 * a0, a0, C::quarter * (b0 * b0));
-    const T s1 = C::eps + dfma(C::c1312 * a1, a1, C::quarter * (b1 * b1));
-    const T s2 = C::eps + dfma(C::c1312 * a2, a2, C::quarter * (b2 * b2));
+    const T a0 = d.d12 - d.d01, a1 = d.d23 - d.d12, a2 = d.d34 - d.d23;
+    const T h0 = dfma(C::half, a0, d.d12);
+    const T h1 = C::half * (d.d12 + d.d23);
+    const T h2 = dfma(C::half, a2, -d.d23);
+    const T s0 = dfma(C::c1312 * a0, a0, dfma(h0, h0, C::eps));
+    const T s1 = dfma(C::c1312 * a1, a1, dfma(h1, h1, C::eps));
+    const T s2 = dfma(C::c1312 * a2, a2, dfma(h2, h2, C::eps));
     T q0 = s0, q1 = s1, q2 = s2;
     if constexpr (sizeof(T) == 4) { // FP32: exact power-of-two rescaling
         const T sc = weno5_scale(s0, s1, s2);
@@ -101,42 +113,47 @@ __device__ __forceinline__ void weno5_beta(T u0, T u1, T u2, T u3, T u4, T &p12,
 }
 
 // Left-biased state of cell j at j+1/2 (linear weights 1/10, 6/10, 3/10 on
-// S0, S1, S2) as numerator and denominator: value = num / den.
+// S0, S1, S2): value = u2 + num / den.  The candidates' numerators 6 q_k are
+// 6 u2 + e_k with e0 = 5 d12 - 2 d01, e1 = d12 + 2 d23, e2 = 4 d23 - d34.
+// w1 = 0.6 p02 is the middle weight of both states of the cell.
 template <typename T>
-__device__ __forceinline__ void weno5_left(T u0, T u1, T u2, T u3, T u4, T p12, T p02, T p01, T &num, T &den)
+__device__ __forceinline__ void weno5_left(const Diff5<T> &d, T p12, T w1, T p01, T &num, T &den)
 {
     using C = K<T>;
-    const T w0 = C::d0 * p12, w1 = C::d1 * p02, w2 = C::d2 * p01;
-    // candidate numerators 6*q_k
-    const T n0 = dfma(T(2), u0, dfma(T(-7), u1, T(11) * u2)); // 2u0 - 7u1 + 11u2
-    const T n1 = dfma(T(5), u2, dfma(T(2), u3, -u1));         // -u1 + 5u2 + 2u3
-    const T n2 = dfma(T(2), u2, dfma(T(5), u3, -u4));         // 2u2 + 5u3 - u4
-    num = dfma(w0, n0, dfma(w1, n1, w2 * n2));
+    const T w0 = C::d0 * p12, w2 = C::d2 * p01;
+    const T e0 = dfma(T(-2), d.d01, T(5) * d.d12);
+    const T e1 = dfma(T(2), d.d23, d.d12);
+    const T e2 = dfma(T(4), d.d23, -d.d34);
+    num = dfma(w0, e0, dfma(w1, e1, w2 * e2));
     den = C::six * ((w0 + w1) + w2);
 }
 
-// Right-biased state of cell j at j-1/2 (linear weights 3/10, 6/10, 1/10).
+// Right-biased state of cell j at j-1/2 (linear weights 3/10, 6/10, 1/10):
+// value = u2 + num / den with candidates 6 u2 + f_k, f0 = d01 - 4 d12,
+// f1 = -2 d12 - d23, f2 = 2 d34 - 5 d23.
 template <typename T>
-__device__ __forceinline__ void weno5_right(T u0, T u1, T u2, T u3, T u4, T p12, T p02, T p01, T &num, T &den)
+__device__ __forceinline__ void weno5_right(const Diff5<T> &d, T p12, T w1, T p01, T &num, T &den)
 {
     using C = K<T>;
-    const T r0 = C::d2 * p12, r1 = C::d1 * p02, r2 = C::d0 * p01;
-    const T m0 = dfma(T(5), u1, dfma(T(2), u2, -u0));         // -u0 + 5u1 + 2u2
-    const T m1 = dfma(T(2), u1, dfma(T(5), u2, -u3));         // 2u1 + 5u2 - u3
-    const T m2 = dfma(T(2), u4, dfma(T(-7), u3, T(11) * u2)); // 11u2 - 7u3 + 2u4
-    num = dfma(r0, m0, dfma(r1, m1, r2 * m2));
-    den = C::six * ((r0 + r1) + r2);
+    const T r0 = C::d2 * p12, r2 = C::d0 * p01;
+    const T f0 = dfma(T(-4), d.d12, d.d01);
+    const T f1 = dfma(T(-2), d.d12, -d.d23);
+    const T f2 = dfma(T(2), d.d34, T(-5) * d.d23);
+    num = dfma(r0, f0, dfma(w1, f1, r2 * f2));
+    den = C::six * ((r0 + w1) + r2);
 }
 
-// The two states at one face from the lower cell's left-biased (nl, dl) and
-// the upper cell's right-biased (nr, dr) reconstruction, from one division:
-//   inv = 1/(dl*dr), vl = (nl*dr)*inv, vr = (nr*dl)*inv
+// The two states at one face from the lower cell's value ul and left-biased
+// correction (nl, dl) and the upper cell's value ur and right-biased
+// correction (nr, dr), from one division:
+//   inv = 1/(dl*dr), vl = ul + (nl*dr)*inv, vr = ur + (nr*dl)*inv
 // (the product stays in range: see the range note).
-template <typename T> __device__ __forceinline__ void face_states(T nl, T dl, T nr, T dr, T &vl, T &vr)
+template <typename T>
+__device__ __forceinline__ void face_states(T ul, T nl, T dl, T ur, T nr, T dr, T &vl, T &vr)
 {
     const T inv = T(1) / (dl * dr);
-    vl = (nl * dr) * inv;
-    vr = (nr * dl) * inv;
+    vl = dfma(nl * dr, inv, ul);
+    vr = dfma(nr * dl, inv, ur);
 }
 
 // Two variables' face states from one division (a = first, b = second
@@ -144,20 +161,23 @@ template <typename T> __device__ __forceinline__ void face_states(T nl, T dl, T 
 // q_b = (dla*dra)*inv.  The product of four denominators lies in
 // [0.13, 2.2e10] in FP32 (rescaled weights); FP64 bounds in the range note.
 template <typename T>
-__device__ __forceinline__ void face_states2(T nla, T dla, T nra, T dra, T nlb, T dlb, T nrb, T drb, T &vla, T &vra,
-                                             T &vlb, T &vrb)
+__device__ __forceinline__ void face_states2(T ula, T nla, T dla, T ura, T nra, T dra, T ulb, T nlb, T dlb, T urb,
+                                             T nrb, T drb, T &vla, T &vra, T &vlb, T &vrb)
 {
     const T Da = dla * dra, Db = dlb * drb;
     const T inv = T(1) / (Da * Db);
     const T qa = Db * inv, qb = Da * inv;
-    vla = (nla * dra) * qa;
-    vra = (nra * dla) * qa;
-    vlb = (nlb * drb) * qb;
-    vrb = (nrb * dlb) * qb;
+    vla = dfma(nla * dra, qa, ula);
+    vra = dfma(nra * dla, qa, ura);
+    vlb = dfma(nlb * drb, qb, ulb);
+    vrb = dfma(nrb * dlb, qb, urb);
 }
 
-// Rusanov flux through a face with normal direction `d` (0,1,2) from the
-// reconstructed primitive states WL, WR = (rho, u, v, w, p).
+// Twice the Rusanov flux through a face with normal direction `d` (0,1,2)
+// from the reconstructed primitive states WL, WR = (rho, u, v, w, p):
+// F = (f(UL) + f(UR)) - a (UR - UL), a = max(|u_n| + c) of both sides.  The
+// factor 1/2 of the flux is exact and is taken with 1/h by the flux
+// differences.
 template <typename T>
 __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int d, T gamma,
                                         T igm1, T (&F)[5])
@@ -168,40 +188,32 @@ __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int 
     const T unl = d == 0 ? WL[1] : (d == 1 ? WL[2] : WL[3]);
     const T unr = d == 0 ? WR[1] : (d == 1 ? WR[2] : WR[3]);
     const T pl = WL[4], pr = WR[4];
-    // conservative states
-    const T mul0 = rl * WL[1], mul1 = rl * WL[2], mul2 = rl * WL[3];
-    const T mur0 = rr * WR[1], mur1 = rr * WR[2], mur2 = rr * WR[3];
-    const T kel = dfma(WL[1], WL[1], dfma(WL[2], WL[2], WL[3] * WL[3]));
-    const T ker = dfma(WR[1], WR[1], dfma(WR[2], WR[2], WR[3] * WR[3]));
-    const T El = dfma(C::half * rl, kel, pl * igm1);
-    const T Er = dfma(C::half * rr, ker, pr * igm1);
-    // wave speeds
-    // one division for both sound speeds
+    // wave speeds: one division for both sound speeds
     const T irr = T(1) / (rl * rr);
     const T cl = dsqrt(((gamma * pl) * rr) * irr);
     const T cr = dsqrt(((gamma * pr) * rl) * irr);
     const T a = dmax(dabs(unl) + cl, dabs(unr) + cr);
-    // physical fluxes
+    // mass
     const T fl0 = rl * unl, fr0 = rr * unr;
-    T fl1 = mul0 * unl, fr1 = mur0 * unr;
-    T fl2 = mul1 * unl, fr2 = mur1 * unr;
-    T fl3 = mul2 * unl, fr3 = mur2 * unr;
-    if (d == 0) {
-        fl1 = fl1 + pl;
-        fr1 = fr1 + pr;
-    } else if (d == 1) {
-        fl2 = fl2 + pl;
-        fr2 = fr2 + pr;
-    } else {
-        fl3 = fl3 + pl;
-        fr3 = fr3 + pr;
+    F[0] = dfma(-a, rr - rl, fl0 + fr0);
+    // momentum: flux = mass flux * velocity (+ p along the normal)
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const T ml = rl * WL[k], mr = rr * WR[k];
+        T fl = fl0 * WL[k], fr = fr0 * WR[k];
+        if (k - 1 == d) {
+            fl = fl + pl;
+            fr = fr + pr;
+        }
+        F[k] = dfma(-a, mr - ml, fl + fr);
     }
+    // energy
+    const T kel = dfma(WL[1], WL[1], dfma(WL[2], WL[2], WL[3] * WL[3]));
+    const T ker = dfma(WR[1], WR[1], dfma(WR[2], WR[2], WR[3] * WR[3]));
+    const T El = dfma(C::half * rl, kel, pl * igm1);
+    const T Er = dfma(C::half * rr, ker, pr * igm1);
     const T fl4 = (El + pl) * unl, fr4 = (Er + pr) * unr;
-    F[0] = C::half * dfma(-a, rr - rl, fl0 + fr0);
-    F[1] = C::half * dfma(-a, mur0 - mul0, fl1 + fr1);
-    F[2] = C::half * dfma(-a, mur1 - mul1, fl2 + fr2);
-    F[3] = C::half * dfma(-a, mur2 - mul2, fl3 + fr3);
-    F[4] = C::half * dfma(-a, Er - El, fl4 + fr4);
+    F[4] = dfma(-a, Er - El, fl4 + fr4);
 }
 
 // Conservative -> primitive (rho, u, v, w, p).

@@ -231,10 +231,10 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const T *Wc = W + c * Stg<T>::SV;
-            const T u0 = Wc[id[0]], u1 = Wc[id[1]], u2 = Wc[id[2]], u3 = Wc[id[3]], u4 = Wc[id[4]];
+            const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], Wc[id[2]], Wc[id[3]], Wc[id[4]]);
             T p12, p02, p01;
-            weno5_beta(u0, u1, u2, u3, u4, p12, p02, p01);
-            weno5_left(u0, u1, u2, u3, u4, p12, p02, p01, Ln[c], Ld[c]);
+            weno5_beta(df, p12, p02, p01);
+            weno5_left(df, p12, K<T>::d1 * p02, p01, Ln[c], Ld[c]);
         }
     }
 #pragma unroll 1
@@ -246,27 +246,32 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
             id[k] = sidx(a - 2 + k);
         T WL[5], WR[5];
         // variables (0,1) and (2,3) share one division; the first of a pair
-        // waits in (hnl, hdl, hnr, hdr) for the second
-        T hnl = T(0), hdl = T(1), hnr = T(0), hdr = T(1);
+        // waits in (hul, hnl, hdl, hur, hnr, hdr) for the second
+        T hul = T(0), hnl = T(0), hdl = T(1), hur = T(0), hnr = T(0), hdr = T(1);
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const T *Wc = W + c * Stg<T>::SV;
-            const T u0 = Wc[id[0]], u1 = Wc[id[1]], u2 = Wc[id[2]], u3 = Wc[id[3]], u4 = Wc[id[4]];
+            const T u1 = Wc[id[1]], u2 = Wc[id[2]]; // cells a-1 and a
+            const Diff5<T> df = weno5_diff(Wc[id[0]], u1, u2, Wc[id[3]], Wc[id[4]]);
             T p12, p02, p01, nr, dr;
-            weno5_beta(u0, u1, u2, u3, u4, p12, p02, p01);
-            weno5_right(u0, u1, u2, u3, u4, p12, p02, p01, nr, dr);
+            weno5_beta(df, p12, p02, p01);
+            const T w1 = K<T>::d1 * p02;
+            weno5_right(df, p12, w1, p01, nr, dr);
             if (c == 0 || c == 2) {
+                hul = u1;
                 hnl = Ln[c];
                 hdl = Ld[c];
+                hur = u2;
                 hnr = nr;
                 hdr = dr;
             } else if (c == 1 || c == 3) {
-                face_states2(hnl, hdl, hnr, hdr, Ln[c], Ld[c], nr, dr, WL[c - 1], WR[c - 1], WL[c], WR[c]);
+                face_states2(hul, hnl, hdl, hur, hnr, hdr, u1, Ln[c], Ld[c], u2, nr, dr, WL[c - 1], WR[c - 1], WL[c],
+                             WR[c]);
             } else {
-                face_states(Ln[c], Ld[c], nr, dr, WL[c], WR[c]);
+                face_states(u1, Ln[c], Ld[c], u2, nr, dr, WL[c], WR[c]);
             }
             if (i < 2)
-                weno5_left(u0, u1, u2, u3, u4, p12, p02, p01, Ln[c], Ld[c]);
+                weno5_left(df, p12, w1, p01, Ln[c], Ld[c]);
         }
         T Fl[5];
         rusanov<T>(WL, WR, D, gamma, igm1, Fl);
@@ -420,7 +425,8 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
             stage_halo<T>(D, p, src, t, W, snb);
             __syncthreads();
         }
-        const T ihd = D == 0 ? t.ih[0] : (D == 1 ? t.ih[1] : t.ih[2]);
+        // the Rusanov fluxes are twice the flux: 1/(2h) (exact)
+        const T ihd = T(0.5) * (D == 0 ? t.ih[0] : (D == 1 ? t.ih[1] : t.ih[2]));
         sweep<T>(D, W, F, acc, p.gamma, p.igm1, ihd);
     }
 

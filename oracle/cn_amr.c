@@ -145,7 +145,7 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double 
                             prim[c * le + li] = W[c];
                     }
             const size_t cells = (size_t)n * n * n;
-            const double ih = blk[b].ih;
+            const double ih = 0.5 * blk[b].ih; /* 1/(2h): the Rusanov fluxes are twice the flux */
             for (int d = 0; d < 3; ++d) {
                 const int E0 = n + (d == 0), E1 = n + (d == 1), E2 = n + (d == 2);
                 const size_t nf = (size_t)E0 * E1 * E2;
@@ -154,13 +154,13 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double 
                     for (int y = 0; y < E1; ++y)
                         for (int x = 0; x < E0; ++x) {
                             const ptrdiff_t li = (x + 3) + (ptrdiff_t)L * ((y + 3) + (ptrdiff_t)L * (z + 3));
-                            double WL[5], WR[5], F[5], nl[5], dl[5], nr[5], dr[5];
+                            double WL[5], WR[5], F[5], bl[5], nl[5], dl[5], br[5], nr[5], dr[5];
                             for (int c = 0; c < 5; ++c) {
                                 const double *P = prim + c * le + li;
-                                weno5_nd_face_f64(P[-3 * st], P[-2 * st], P[-st], P[0], P[st], P[2 * st], &nl[c],
-                                                  &dl[c], &nr[c], &dr[c]);
+                                weno5_nd_face_f64(P[-3 * st], P[-2 * st], P[-st], P[0], P[st], P[2 * st], &bl[c],
+                                                  &nl[c], &dl[c], &br[c], &nr[c], &dr[c]);
                             }
-                            face_states5_f64(nl, dl, nr, dr, WL, WR);
+                            face_states5_f64(bl, nl, dl, br, nr, dr, WL, WR);
                             rusanov_f64(WL, WR, d, gamma, igm1, F);
                             const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
                             for (int c = 0; c < 5; ++c)

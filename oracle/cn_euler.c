@@ -67,14 +67,15 @@
                         /* face between cell (x,y,z)-e_d and (x,y,z) */        \
                         const ptrdiff_t li = (x + 3) + (ptrdiff_t)L0 *         \
                                              ((y + 3) + (ptrdiff_t)L1 * (z + 3)); \
-                        T WL[5], WR[5], F[5], nl[5], dl[5], nr[5], dr[5];      \
+                        T WL[5], WR[5], F[5], bl[5], nl[5], dl[5], br[5], nr[5], dr[5]; \
                         for (int c = 0; c < 5; ++c) {                          \
                             const T *P = prim + c * le + li;                   \
                             const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st]; \
                             const T v3 = P[0], v4 = P[st], v5 = P[2 * st];     \
-                            weno5_nd_face_##SUF(v0, v1, v2, v3, v4, v5, &nl[c], &dl[c], &nr[c], &dr[c]); \
+                            weno5_nd_face_##SUF(v0, v1, v2, v3, v4, v5, &bl[c], &nl[c], &dl[c], \
+                                                &br[c], &nr[c], &dr[c]);        \
                         }                                                      \
-                        face_states5_##SUF(nl, dl, nr, dr, WL, WR);            \
+                        face_states5_##SUF(bl, nl, dl, br, nr, dr, WL, WR);    \
                         rusanov_##SUF(WL, WR, d, gamma, igm1, F);              \
                         const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z); \
                         for (int c = 0; c < 5; ++c)                            \
@@ -129,7 +130,9 @@
         }                                                                      \
         g.tensorial = 0;                                                       \
         const int nblocks = g.nb[0] * g.nb[1] * g.nb[2];                       \
-        const T ih[3] = {(T)(1.0 / h[0]), (T)(1.0 / h[1]), (T)(1.0 / h[2])};   \
+        /* 1/(2h): the Rusanov fluxes are twice the flux (exact) */            \
+        const T ih[3] = {(T)0.5 * (T)(1.0 / h[0]), (T)0.5 * (T)(1.0 / h[1]),   \
+                         (T)0.5 * (T)(1.0 / h[2])};                            \
         const size_t le = (size_t)(g.n[0] + 6) * (g.n[1] + 6) * (g.n[2] + 6);  \
         const size_t fl = 5 * (size_t)(g.n[0] + 1) * (g.n[1] + 1) * (g.n[2] + 1) + \
                           5 * (size_t)g.n[0] * g.n[1] * g.n[2];                \

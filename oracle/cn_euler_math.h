@@ -47,22 +47,23 @@ static inline double weno5_scale_f64(double s0, double s1, double s2)
 }
 
 #define DEFINE_EULER_MATH(SUF, T, FMA, SQRT, FABS, FMAX)                        \
-    /* smoothness of cell j from u0..u4 = v[j-2..j+2]: the products          \
-     * p12 = t1 t2, p02 = t0 t2, p01 = t0 t1 of t_k = (eps + beta_k)^2 for   \
-     * the stencils S0 = {j-2..j}, S1 = {j-1..j+1}, S2 = {j..j+2}; shared by  \
-     * the cell's left-biased (j+1/2) and right-biased (j-1/2) states */      \
-    static inline void weno5_beta_##SUF(T u0, T u1, T u2, T u3, T u4, T *p12, T *p02, T *p01) \
+    /* smoothness of cell j from the differences of u0..u4 = v[j-2..j+2]     \
+     * (d01 = u1 - u0, ...): the products p12 = t1 t2, p02 = t0 t2,          \
+     * p01 = t0 t1 of t_k = (eps + beta_k)^2 for the stencils S0 = {j-2..j}, \
+     * S1 = {j-1..j+1}, S2 = {j..j+2}, beta_k = 13/12 a_k^2 + 1/4 b_k^2 with \
+     * a0 = d12 - d01, a1 = d23 - d12, a2 = d34 - d23, b0/2 = a0/2 + d12,     \
+     * b1/2 = (d12 + d23)/2 (up to sign), b2/2 = a2/2 - d23; shared by the    \
+     * cell's left-biased (j+1/2) and right-biased (j-1/2) states */          \
+    static inline void weno5_beta_##SUF(T d01, T d12, T d23, T d34, T *p12, T *p02, T *p01) \
     {                                                                          \
-        const T c1312 = (T)(13.0 / 12.0), quarter = (T)0.25, eps = (T)1e-6;    \
-        const T a0 = FMA((T)-2, u1, u0) + u2;                                  \
-        const T b0 = FMA((T)3, u2, FMA((T)-4, u1, u0));                        \
-        const T a1 = FMA((T)-2, u2, u1) + u3;                                  \
-        const T b1 = u1 - u3;                                                  \
-        const T a2 = FMA((T)-2, u3, u2) + u4;                                  \
-        const T b2 = FMA((T)3, u2, FMA((T)-4, u3, u4));                        \
-        const T s0 = eps + FMA(c1312 * a0, a0, quarter * (b0 * b0));           \
-        const T s1 = eps + FMA(c1312 * a1, a1, quarter * (b1 * b1));           \
-        const T s2 = eps + FMA(c1312 * a2, a2, quarter * (b2 * b2));           \
+        const T c1312 = (T)(13.0 / 12.0), half = (T)0.5, eps = (T)1e-6;        \
+        const T a0 = d12 - d01, a1 = d23 - d12, a2 = d34 - d23;                \
+        const T h0 = FMA(half, a0, d12);                                       \
+        const T h1 = half * (d12 + d23);                                       \
+        const T h2 = FMA(half, a2, -d23);                                      \
+        const T s0 = FMA(c1312 * a0, a0, FMA(h0, h0, eps));                    \
+        const T s1 = FMA(c1312 * a1, a1, FMA(h1, h1, eps));                    \
+        const T s2 = FMA(c1312 * a2, a2, FMA(h2, h2, eps));                    \
         const T sc = weno5_scale_##SUF(s0, s1, s2);                            \
         const T q0 = s0 * sc, q1 = s1 * sc, q2 = s2 * sc;                      \
         const T t0 = q0 * q0, t1 = q1 * q1, t2 = q2 * q2;                      \
@@ -72,64 +73,77 @@ static inline double weno5_scale_f64(double s0, double s1, double s2)
     }                                                                          \
                                                                                \
     /* left-biased state of cell j at j+1/2: linear weights 1/10, 6/10, 3/10  \
-     * on S0, S1, S2; value = num / den */                                     \
+     * on S0, S1, S2; value = u2 + num / den, the candidates' numerators      \
+     * 6 q_k = 6 u2 + e_k, e0 = 5 d12 - 2 d01, e1 = d12 + 2 d23,             \
+     * e2 = 4 d23 - d34 */                                                     \
     static inline void weno5_left_##SUF(T u0, T u1, T u2, T u3, T u4, T *num, T *den) \
     {                                                                          \
+        const T d01 = u1 - u0, d12 = u2 - u1, d23 = u3 - u2, d34 = u4 - u3;    \
         T p12, p02, p01;                                                       \
-        weno5_beta_##SUF(u0, u1, u2, u3, u4, &p12, &p02, &p01);                \
-        const T w0 = (T)0.1 * p12, w1 = (T)0.6 * p02, w2 = (T)0.3 * p01;       \
-        const T n0 = FMA((T)2, u0, FMA((T)-7, u1, (T)11 * u2));                \
-        const T n1 = FMA((T)5, u2, FMA((T)2, u3, -u1));                        \
-        const T n2 = FMA((T)2, u2, FMA((T)5, u3, -u4));                        \
-        *num = FMA(w0, n0, FMA(w1, n1, w2 * n2));                              \
+        weno5_beta_##SUF(d01, d12, d23, d34, &p12, &p02, &p01);                \
+        const T w1 = (T)0.6 * p02;                                             \
+        const T w0 = (T)0.1 * p12, w2 = (T)0.3 * p01;                          \
+        const T e0 = FMA((T)-2, d01, (T)5 * d12);                              \
+        const T e1 = FMA((T)2, d23, d12);                                      \
+        const T e2 = FMA((T)4, d23, -d34);                                     \
+        *num = FMA(w0, e0, FMA(w1, e1, w2 * e2));                              \
         *den = (T)6 * ((w0 + w1) + w2);                                        \
     }                                                                          \
                                                                                \
     /* right-biased state of cell j at j-1/2: linear weights 3/10, 6/10, 1/10 \
-     * on S0, S1, S2 */                                                        \
+     * on S0, S1, S2; candidates 6 u2 + f_k, f0 = d01 - 4 d12,               \
+     * f1 = -2 d12 - d23, f2 = 2 d34 - 5 d23 */                                \
     static inline void weno5_right_##SUF(T u0, T u1, T u2, T u3, T u4, T *num, T *den) \
     {                                                                          \
+        const T d01 = u1 - u0, d12 = u2 - u1, d23 = u3 - u2, d34 = u4 - u3;    \
         T p12, p02, p01;                                                       \
-        weno5_beta_##SUF(u0, u1, u2, u3, u4, &p12, &p02, &p01);                \
-        const T r0 = (T)0.3 * p12, r1 = (T)0.6 * p02, r2 = (T)0.1 * p01;       \
-        const T m0 = FMA((T)5, u1, FMA((T)2, u2, -u0));                        \
-        const T m1 = FMA((T)2, u1, FMA((T)5, u2, -u3));                        \
-        const T m2 = FMA((T)2, u4, FMA((T)-7, u3, (T)11 * u2));                \
-        *num = FMA(r0, m0, FMA(r1, m1, r2 * m2));                              \
-        *den = (T)6 * ((r0 + r1) + r2);                                        \
+        weno5_beta_##SUF(d01, d12, d23, d34, &p12, &p02, &p01);                \
+        const T w1 = (T)0.6 * p02;                                             \
+        const T r0 = (T)0.3 * p12, r2 = (T)0.1 * p01;                          \
+        const T f0 = FMA((T)-4, d12, d01);                                     \
+        const T f1 = FMA((T)-2, d12, -d23);                                    \
+        const T f2 = FMA((T)2, d34, (T)-5 * d23);                              \
+        *num = FMA(r0, f0, FMA(w1, f1, r2 * f2));                              \
+        *den = (T)6 * ((r0 + w1) + r2);                                        \
     }                                                                          \
                                                                                \
     /* the two reconstructions at the face between v2 and v3 (v0..v5 =      \
      * v[i-2..i+3]): cell v2's left-biased and cell v3's right-biased state   \
-     * as numerators and denominators */                                      \
+     * as base value, numerator and denominator (state = b + n / d) */         \
     static inline void weno5_nd_face_##SUF(T v0, T v1, T v2, T v3, T v4, T v5, \
-                                           T *nl, T *dl, T *nr, T *dr)         \
+                                           T *bl, T *nl, T *dl, T *br, T *nr, T *dr) \
     {                                                                          \
         weno5_left_##SUF(v0, v1, v2, v3, v4, nl, dl);                          \
         weno5_right_##SUF(v1, v2, v3, v4, v5, nr, dr);                         \
+        *bl = v2;                                                              \
+        *br = v3;                                                              \
     }                                                                          \
                                                                                \
-    /* face states of the 5 variables from their numerators and denominators \
-     * (each in [0.6, 384] with the scaled weights): variables (0,1) and     \
-     * (2,3) share one division for their four states, variable 4 takes one  \
-     * for its two */                                                         \
-    static inline void face_states5_##SUF(const T *nl, const T *dl, const T *nr, \
-                                          const T *dr, T *WL, T *WR)           \
+    /* face states of the 5 variables from their base values, numerators and \
+     * denominators (each denominator in [0.6, 384] with the scaled          \
+     * weights): variables (0,1) and (2,3) share one division for their four \
+     * states, variable 4 takes one for its two */                            \
+    static inline void face_states5_##SUF(const T *bl, const T *nl, const T *dl, \
+                                          const T *br, const T *nr, const T *dr, \
+                                          T *WL, T *WR)                        \
     {                                                                          \
         for (int c = 0; c < 4; c += 2) {                                       \
             const T Da = dl[c] * dr[c], Db = dl[c + 1] * dr[c + 1];            \
             const T inv = (T)1 / (Da * Db);                                    \
             const T qa = Db * inv, qb = Da * inv;                              \
-            WL[c] = (nl[c] * dr[c]) * qa;                                      \
-            WR[c] = (nr[c] * dl[c]) * qa;                                      \
-            WL[c + 1] = (nl[c + 1] * dr[c + 1]) * qb;                          \
-            WR[c + 1] = (nr[c + 1] * dl[c + 1]) * qb;                          \
+            WL[c] = FMA(nl[c] * dr[c], qa, bl[c]);                             \
+            WR[c] = FMA(nr[c] * dl[c], qa, br[c]);                             \
+            WL[c + 1] = FMA(nl[c + 1] * dr[c + 1], qb, bl[c + 1]);             \
+            WR[c + 1] = FMA(nr[c + 1] * dl[c + 1], qb, br[c + 1]);             \
         }                                                                      \
         const T inv = (T)1 / (dl[4] * dr[4]);                                  \
-        WL[4] = (nl[4] * dr[4]) * inv;                                         \
-        WR[4] = (nr[4] * dl[4]) * inv;                                         \
+        WL[4] = FMA(nl[4] * dr[4], inv, bl[4]);                                \
+        WR[4] = FMA(nr[4] * dl[4], inv, br[4]);                                \
     }                                                                          \
                                                                                \
+    /* twice the Rusanov flux: (f(UL) + f(UR)) - a (UR - UL) with            \
+     * a = max(|u_n| + c) of both sides; the factor 1/2 is taken with 1/h    \
+     * by the flux differences (exact) */                                     \
     static inline void rusanov_##SUF(const T *WL, const T *WR, int d, T gamma,        \
                               T igm1, T *F)                                    \
     {                                                                          \
@@ -137,37 +151,28 @@ static inline double weno5_scale_f64(double s0, double s1, double s2)
         const T rl = WL[0], rr = WR[0];                                        \
         const T unl = WL[1 + d], unr = WR[1 + d];                              \
         const T pl = WL[4], pr = WR[4];                                        \
-        const T mul0 = rl * WL[1], mul1 = rl * WL[2], mul2 = rl * WL[3];       \
-        const T mur0 = rr * WR[1], mur1 = rr * WR[2], mur2 = rr * WR[3];       \
-        const T kel = FMA(WL[1], WL[1], FMA(WL[2], WL[2], WL[3] * WL[3]));     \
-        const T ker = FMA(WR[1], WR[1], FMA(WR[2], WR[2], WR[3] * WR[3]));     \
-        const T El = FMA(half * rl, kel, pl * igm1);                           \
-        const T Er = FMA(half * rr, ker, pr * igm1);                           \
         /* one division for both sound speeds */                               \
         const T irr = (T)1 / (rl * rr);                                        \
         const T cl = SQRT(((gamma * pl) * rr) * irr);                          \
         const T cr = SQRT(((gamma * pr) * rl) * irr);                          \
         const T a = FMAX(FABS(unl) + cl, FABS(unr) + cr);                      \
         const T fl0 = rl * unl, fr0 = rr * unr;                                \
-        T fl1 = mul0 * unl, fr1 = mur0 * unr;                                  \
-        T fl2 = mul1 * unl, fr2 = mur1 * unr;                                  \
-        T fl3 = mul2 * unl, fr3 = mur2 * unr;                                  \
-        if (d == 0) {                                                          \
-            fl1 = fl1 + pl;                                                    \
-            fr1 = fr1 + pr;                                                    \
-        } else if (d == 1) {                                                   \
-            fl2 = fl2 + pl;                                                    \
-            fr2 = fr2 + pr;                                                    \
-        } else {                                                               \
-            fl3 = fl3 + pl;                                                    \
-            fr3 = fr3 + pr;                                                    \
+        F[0] = FMA(-a, rr - rl, fl0 + fr0);                                    \
+        for (int k = 1; k <= 3; ++k) {                                         \
+            const T ml = rl * WL[k], mr = rr * WR[k];                          \
+            T fl = fl0 * WL[k], fr = fr0 * WR[k];                              \
+            if (k - 1 == d) {                                                  \
+                fl = fl + pl;                                                  \
+                fr = fr + pr;                                                  \
+            }                                                                  \
+            F[k] = FMA(-a, mr - ml, fl + fr);                                  \
         }                                                                      \
+        const T kel = FMA(WL[1], WL[1], FMA(WL[2], WL[2], WL[3] * WL[3]));     \
+        const T ker = FMA(WR[1], WR[1], FMA(WR[2], WR[2], WR[3] * WR[3]));     \
+        const T El = FMA(half * rl, kel, pl * igm1);                           \
+        const T Er = FMA(half * rr, ker, pr * igm1);                           \
         const T fl4 = (El + pl) * unl, fr4 = (Er + pr) * unr;                  \
-        F[0] = half * FMA(-a, rr - rl, fl0 + fr0);                             \
-        F[1] = half * FMA(-a, mur0 - mul0, fl1 + fr1);                         \
-        F[2] = half * FMA(-a, mur1 - mul1, fl2 + fr2);                         \
-        F[3] = half * FMA(-a, mur2 - mul2, fl3 + fr3);                         \
-        F[4] = half * FMA(-a, Er - El, fl4 + fr4);                             \
+        F[4] = FMA(-a, Er - El, fl4 + fr4);                                    \
     }                                                                          \
                                                                                \
     static inline void prim_##SUF(T r, T m0, T m1, T m2, T E, T gm1, T *W)            \

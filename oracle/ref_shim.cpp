@@ -194,7 +194,8 @@ double eulerStage<double>(const int nb[3], const int n[3], const double *Us, con
         g.emplace_back(new R(nb, n, Us + c * cstride, stride));
         g.back()->attach(bc_off ? bc_off[c] : nullptr, bcs ? bcs[c] : nullptr);
     }
-    const T ih[3] = {(T)(1.0 / h[0]), (T)(1.0 / h[1]), (T)(1.0 / h[2])};
+    // 1/(2h): the Rusanov fluxes are twice the flux (exact)
+    const T ih[3] = {T(0.5) * (T)(1.0 / h[0]), T(0.5) * (T)(1.0 / h[1]), T(0.5) * (T)(1.0 / h[2])};
     const T gm1 = (T)(gamma - 1.0), igm1 = (T)(1.0 / (gamma - 1.0)), gam = (T)gamma, dtt = (T)dt;
     const int N0 = n[0], N1 = n[1], N2 = n[2];
     double best = 1e300;
@@ -232,14 +233,15 @@ double eulerStage<double>(const int nb[3], const int n[3], const double *Us, con
                         for (int y = 0; y < E1; ++y)
                             for (int x = 0; x < E0; ++x) {
                                 const ptrdiff_t li = (x + 3) + (ptrdiff_t)L0 * ((y + 3) + (ptrdiff_t)L1 * (z + 3));
-                                T WL[5], WR[5], F[5], nl[5], dl[5], nr[5], dr[5];
+                                T WL[5], WR[5], F[5], bl[5], nl[5], dl[5], br[5], nr[5], dr[5];
                                 for (int c = 0; c < 5; ++c) {
                                     const T *P = prim.data() + c * le + li;
                                     const T v0 = P[-3 * st], v1 = P[-2 * st], v2 = P[-st];
                                     const T v3 = P[0], v4 = P[st], v5 = P[2 * st];
-                                    weno5_nd_face_f64(v0, v1, v2, v3, v4, v5, &nl[c], &dl[c], &nr[c], &dr[c]);
+                                    weno5_nd_face_f64(v0, v1, v2, v3, v4, v5, &bl[c], &nl[c], &dl[c], &br[c], &nr[c],
+                                                      &dr[c]);
                                 }
-                                face_states5_f64(nl, dl, nr, dr, WL, WR);
+                                face_states5_f64(bl, nl, dl, br, nr, dr, WL, WR);
                                 rusanov_f64(WL, WR, d, gam, igm1, F);
                                 const size_t fi = x + (size_t)E0 * (y + (size_t)E1 * z);
                                 for (int c = 0; c < 5; ++c) flux[c * nf + fi] = F[c];

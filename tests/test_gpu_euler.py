@@ -8,6 +8,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 GAMMA = 1.4
 TOL_F64 = 1e-13
+TOL_F32 = 1e-6  # max |device - oracle| relative to the component's max |oracle|
 
 
 def _state(cn, nb, n, dtype, seed=7, bcs=True):
@@ -48,6 +49,29 @@ def test_rhs_matches_oracle(cn, oracle_lib, dtype, bcs):
     else:
         _assert_close(got, want, 1e-6)
     assert np.array_equal(got, want), "device and oracle differ in the last bits"
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("stage", [1, 2, 3])
+def test_stages_on_c2_blocks_match_oracle(cn, oracle_lib, dtype, stage):
+    """2x2x2 blocks of 32^3 cells (the C2/C4 block size: 64 tiles per block,
+    tiles on every block face and edge), C2 BCs, each SSP-RK3 stage."""
+    import torch
+    nb, n = (2, 2, 2), (32, 32, 32)
+    U = _state(cn, nb, n, dtype, seed=21)
+    Un = _state(cn, nb, n, dtype, seed=22)
+    out = Un if stage == 3 else cn.euler.like(U)
+    host, hn = _host(U), _host(Un)
+    dt = 0.5 * cn.euler.cfl_dt(U, 0.3)
+    cn.euler.rk3_stage(U, U, Un if stage > 1 else None, out, stage, dt)
+    torch.cuda.synchronize()
+    want = oracle_lib.euler_stage(host, hn if stage > 1 else None, nb, n, cn.workloads.euler_bclists(nb), stage,
+                                  dt, GAMMA, U.getCellSize())
+    got = _host(out)
+    if dtype == np.float64:
+        assert np.array_equal(got, want), "device and oracle differ"
+    else:
+        _assert_close(got, want, TOL_F32)
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])

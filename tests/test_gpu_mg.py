@@ -22,9 +22,14 @@ def _setup(cn, nb, n, seed=1):
     return k, f
 
 
-def test_jacobi_and_restriction_match_oracle(cn, oracle_lib):
+# blocks of 8^3 (one tile per block) and of 32^3, the C5 block size (the
+# 32x8x4 tile path, several tiles per block)
+BLOCKS = [((2, 3, 2), (8, 8, 8)), ((2, 2, 2), (32, 32, 32))]
+
+
+@pytest.mark.parametrize("nb,n", BLOCKS)
+def test_jacobi_and_restriction_match_oracle(cn, oracle_lib, nb, n):
     import torch
-    nb, n = (2, 3, 2), (8, 8, 8)
     k, f = _setup(cn, nb, n)
     m = cn.mg.Multigrid(k, omega=0.8)
     p = cn.Grid.Cartesian(nb, n, end=_end(nb, n), dtype=np.float32)
@@ -59,9 +64,9 @@ def test_jacobi_and_restriction_match_oracle(cn, oracle_lib):
     assert np.array_equal(p.blocks_view(p.download()), p.blocks_view(want))
 
 
-def test_fp64_residual_matches_oracle(cn, oracle_lib):
+@pytest.mark.parametrize("nb,n", [((2, 2, 2), (8, 8, 8)), ((2, 2, 2), (32, 32, 32))])
+def test_fp64_residual_matches_oracle(cn, oracle_lib, nb, n):
     import torch
-    nb, n = (2, 2, 2), (8, 8, 8)
     k, f = _setup(cn, nb, n)
     m = cn.mg.Multigrid(k)
     p64 = cn.Grid.Cartesian(nb, n, dtype=np.float64)
