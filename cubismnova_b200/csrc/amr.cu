@@ -53,13 +53,13 @@ __global__ void __launch_bounds__(euler::NT, 3) stage_kernel(euler::StageParams<
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *W = reinterpret_cast<T *>(smem_raw);
-    T *F = W + 5 * euler::Stg<T>::SV;
+    T *A = W + 5 * euler::Stg<T>::SV;
     __shared__ double red[euler::NT / 32][5];
     __shared__ int snb[28];
     __shared__ euler::TileInfo<T> ts;
     // persistent: each CTA walks the work list with a grid stride
     for (int item = blockIdx.x; item < nitems; item += gridDim.x)
-        euler::stage_tile<T>(p, src, item, item, W, F, red, snb, &ts);
+        euler::stage_tile<T>(p, src, item, item, W, A, red, snb, &ts);
 }
 
 // dense lab of one block: (n+2g)^3, face ghosts only (non-tensorial)
@@ -154,7 +154,7 @@ static Geom geom(const cn_amr *a)
 template <typename T> static cn_status set_smem_once()
 {
     static DeviceOnce once; // per device
-    const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NFACE) * sizeof(T);
+    const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NACC) * sizeof(T);
     return smem_opt_in(once, amr::stage_kernel<T>, smem);
 }
 
@@ -181,7 +181,7 @@ static cn_status launch_amr_stage(cn_amr *Us, cn_amr *Un, cn_amr *out, int stage
     src.work = Us->d_work;
     const int nitems = (int)Us->work.size();
     int grid = Us->ctas > 0 ? std::min(Us->ctas, nitems) : nitems;
-    const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NFACE) * sizeof(T);
+    const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NACC) * sizeof(T);
     amr::stage_kernel<T><<<grid, euler::NT, smem, st>>>(p, src, nitems);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;

@@ -8,15 +8,16 @@
 // Block/FieldLab.h:180-224): halo cells inside the block are plain loads,
 // cells outside are resolved by cn::lab_value (periodic neighbour, skip rule
 // and BC chain of each component's BC vector).  Per direction every face flux
-// of the tile is computed exactly once (one thread per face: 2 x 5 WENO5
-// reconstructions + Rusanov), stored in shared memory, and differenced into
-// per-cell accumulators held in registers.  The epilogue
+// of the tile is computed exactly once (runs of three faces per thread, each
+// cell's WENO5 smoothness indicators shared by its two faces, Rusanov) and
+// differenced into per-cell accumulators in shared memory.  The epilogue
 // applies the SSP-RK3 (Shu & Osher 1988) convex combination and optionally
 // accumulates FP64 conservation sums per CTA (reduced in a fixed order by a
 // second kernel, so the sums are deterministic).
 //
-// Shared memory per CTA: 5 x 896 primitives (the tile plus one direction's
-// halo slabs, restaged before each sweep) + 5 x 576 face fluxes.
+// Shared memory per CTA: 5 x 1024 primitives (the tile plus one direction's
+// halo slabs, restaged before each sweep; FP32 keeps all three directions'
+// slabs) + 5 x 704 accumulators and exchanged face fluxes.
 #include "cn_internal.h"
 #include "cn_tma.cuh"
 #include "euler_math.cuh"
@@ -33,11 +34,11 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 3) stage_kernel(Stage
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     T *W = reinterpret_cast<T *>(smem_raw); // [5][Stg<T>::SV]
-    T *F = W + 5 * Stg<T>::SV;              // [5][NFACE]
+    T *A = W + 5 * Stg<T>::SV;              // [5][NACC]
     __shared__ double red[NT / 32][5];
     __shared__ int snb[29];
     __shared__ TileInfo<T> ts;
-    stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, F, red, snb, &ts);
+    stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, A, red, snb, &ts);
 }
 
 // Fixed-order reduction of per-CTA partials: out[c] = sum_i partials[i][c].
@@ -141,7 +142,7 @@ static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, 
     p.stage = stage;
     p.partials = partials;
     p.err = Us->d_err;
-    const size_t smem = (size_t)(5 * Stg<T>::SV + 5 * NFACE) * sizeof(T);
+    const size_t smem = (size_t)(5 * Stg<T>::SV + 5 * NACC) * sizeof(T);
     static DeviceOnce attr_once; // per device (the first call on a device is an eager one)
     r = smem_opt_in(attr_once, stage_kernel<T>, smem);
     if (r != CN_OK) return r;

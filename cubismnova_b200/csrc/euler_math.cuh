@@ -5,9 +5,15 @@
 // flux, gamma-law gas.  The reference library only promises these operators
 // (README.rst:28-31); this is an implementation of the published method.
 //
-// Every operation is written out explicitly: contractions are only the fma()
-// calls below (the file is compiled with --fmad=false), so the CPU oracle can
-// repeat the computation bit for bit.
+// Floating-point contract.  The file is compiled with FMA contraction on
+// (nvcc's default --fmad=true): beyond the fma() calls written out below, the
+// compiler fuses any multiply feeding an add.  Reciprocals and square roots
+// are not IEEE-rounded: FP64 uses the hardware approximations refined by one
+// third-order step (rcp_pos / rsqrt_pos below, within a few ulp), FP32 calls
+// CUDA's fast intrinsics (__fdividef, rsqrtf: about 2 ulp).  The CPU oracle
+// computes the same formulas with IEEE division and square root and no
+// contraction; FP64 results agree with it within 1e-13 relative, FP32 results
+// are judged by their error against FP64.
 //
 // Nonlinear weights: with s_k = eps + beta_k and t_k = s_k^2 the JS weights
 // alpha_k = d_k / t_k normalise to omega_k = d_k*prod_{j!=k} t_j / D with
@@ -24,12 +30,9 @@
 // units).  So in FP32 t_k is formed from s_k * 2^-e, with e the mean of the
 // binary exponents of the largest and the middle s_k (rounded down).  Scaling
 // by a power of two is exact and cancels in every ratio below.  With it the
-// dominant product t_max t_mid lies in [1, 64): every FP32 denominator lies
-// in [0.6, 384], the only products that can underflow are those of
-// negligible weights, and the face states of two variables can share one
-// division.  FP64 needs no scaling: its denominators lie in
-// [6e-25, ~70 J^8], and the shared divisions below stay in range for jumps up
-// to ~2e9 in the paired variables (density, velocity) and ~4e18 in pressure.
+// dominant product t_max t_mid lies in [1, 64) and every FP32 denominator in
+// [0.6, 384]; the only products that can underflow are those of negligible
+// weights.  FP64 needs no scaling: its denominators lie in [6e-25, ~70 J^8].
 #pragma once
 
 #include <cuda_runtime.h>
@@ -56,6 +59,33 @@ __device__ __forceinline__ double dabs(double a) { return fabs(a); }
 __device__ __forceinline__ float dabs(float a) { return fabsf(a); }
 __device__ __forceinline__ double dmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float dmax(float a, float b) { return fmaxf(a, b); }
+
+// 1/x for a positive normal x (denominators of the face states, densities).
+// FP64: the PTX approximation rcp.approx.ftz.f64 refined by one step of the
+// third-order iteration that truncates the series 1/x = r / (1 - e) =
+// r (1 + e + e^2 + ...), e = 1 - x r:  r' = r + r (e + e^2), relative error
+// e^3 plus rounding.  FP32: CUDA's __fdividef (valid for x < 2^126).
+__device__ __forceinline__ double rcp_pos(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double e = fma(-x, r, 1.0);
+    return fma(r, fma(e, e, e), r);
+}
+__device__ __forceinline__ float rcp_pos(float x) { return __fdividef(1.0f, x); }
+
+// 1/sqrt(x) for a positive normal x.  FP64: rsqrt.approx.ftz.f64 refined by one
+// step of the third-order iteration from the series (1 - h)^(-1/2) =
+// 1 + h/2 + 3h^2/8 + ..., h = 1 - x y^2:  y' = y + y h (1/2 + 3/8 h).
+// FP32: CUDA's rsqrtf.
+__device__ __forceinline__ double rsqrt_pos(double x)
+{
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = fma(-x * y, y, 1.0);
+    return fma(y * h, fma(0.375, h, 0.5), y);
+}
+__device__ __forceinline__ float rsqrt_pos(float x) { return rsqrtf(x); }
 
 // The FP32 factor 2^-e of the range note above for s0, s1, s2 >= eps: e =
 // floor((E_max + E_mid) / 2) - 127 from the biased exponents of the largest
@@ -143,34 +173,10 @@ __device__ __forceinline__ void weno5_right(const Diff5<T> &d, T p12, T w1, T p0
     den = C::six * ((r0 + w1) + r2);
 }
 
-// The two states at one face from the lower cell's value ul and left-biased
-// correction (nl, dl) and the upper cell's value ur and right-biased
-// correction (nr, dr), from one division:
-//   inv = 1/(dl*dr), vl = ul + (nl*dr)*inv, vr = ur + (nr*dl)*inv
-// (the product stays in range: see the range note).
-template <typename T>
-__device__ __forceinline__ void face_states(T ul, T nl, T dl, T ur, T nr, T dr, T &vl, T &vr)
+// A reconstructed state u2 + num / den (den > 0: a sum of positive weights).
+template <typename T> __device__ __forceinline__ T weno5_value(T u2, T num, T den)
 {
-    const T inv = T(1) / (dl * dr);
-    vl = dfma(nl * dr, inv, ul);
-    vr = dfma(nr * dl, inv, ur);
-}
-
-// Two variables' face states from one division (a = first, b = second
-// variable):  inv = 1/((dla*dra)*(dlb*drb)), q_a = (dlb*drb)*inv = 1/(dla*dra),
-// q_b = (dla*dra)*inv.  The product of four denominators lies in
-// [0.13, 2.2e10] in FP32 (rescaled weights); FP64 bounds in the range note.
-template <typename T>
-__device__ __forceinline__ void face_states2(T ula, T nla, T dla, T ura, T nra, T dra, T ulb, T nlb, T dlb, T urb,
-                                             T nrb, T drb, T &vla, T &vra, T &vlb, T &vrb)
-{
-    const T Da = dla * dra, Db = dlb * drb;
-    const T inv = T(1) / (Da * Db);
-    const T qa = Db * inv, qb = Da * inv;
-    vla = dfma(nla * dra, qa, ula);
-    vra = dfma(nra * dla, qa, ura);
-    vlb = dfma(nlb * drb, qb, ulb);
-    vrb = dfma(nrb * dlb, qb, urb);
+    return dfma(num, rcp_pos(den), u2);
 }
 
 // Twice the Rusanov flux through a face with normal direction `d` (0,1,2)
@@ -188,10 +194,10 @@ __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int 
     const T unl = d == 0 ? WL[1] : (d == 1 ? WL[2] : WL[3]);
     const T unr = d == 0 ? WR[1] : (d == 1 ? WR[2] : WR[3]);
     const T pl = WL[4], pr = WR[4];
-    // wave speeds: one division for both sound speeds
-    const T irr = T(1) / (rl * rr);
-    const T cl = dsqrt(((gamma * pl) * rr) * irr);
-    const T cr = dsqrt(((gamma * pr) * rl) * irr);
+    // sound speeds c = sqrt(gamma p / rho) = (gamma p) / sqrt(gamma p rho)
+    const T gpl = gamma * pl, gpr = gamma * pr;
+    const T cl = gpl * rsqrt_pos(gpl * rl);
+    const T cr = gpr * rsqrt_pos(gpr * rr);
     const T a = dmax(dabs(unl) + cl, dabs(unr) + cr);
     // mass
     const T fl0 = rl * unl, fr0 = rr * unr;
@@ -220,7 +226,7 @@ __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int 
 template <typename T>
 __device__ __forceinline__ void to_primitive(T r, T m0, T m1, T m2, T E, T gm1, T (&W)[5])
 {
-    const T inv = T(1) / r;
+    const T inv = rcp_pos(r);
     const T u = m0 * inv, v = m1 * inv, w = m2 * inv;
     const T ke = K<T>::half * dfma(m0, u, dfma(m1, v, m2 * w));
     W[0] = r;

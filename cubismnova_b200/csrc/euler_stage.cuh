@@ -38,7 +38,9 @@ template <typename T> struct Stg {
     }
 };
 constexpr int NCELL = TB * TB * TB;   // 512
-constexpr int NFACE = (TB + 1) * TB * TB; // 576
+// per variable: the cells' flux-difference accumulators (core layout) and
+// the 2 x 64 face fluxes exchanged between the runs of a line
+constexpr int NACC = NCORE_SM + 2 * 64;
 constexpr int NT = 192;               // threads per CTA: 64 lines x 3 runs of 3 faces
 constexpr int CPT = (NCELL + NT - 1) / NT; // cells per thread: 3
 
@@ -196,33 +198,32 @@ __device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z, 
     }
 }
 
-// Face fluxes of direction D for the whole tile, then flux differences into
-// the per-cell accumulators.  Each of the tile's 64 lines along D has 9 faces
-// (face a between cells a-1 and a); thread t takes the run of faces
-// 3r .. 3r+2, r = t / 64, of line t % 64, walking up the line so that each
-// cell's smoothness indicators serve both of its faces: the left-biased state
-// of cell a-1 is carried as (numerator, denominator) from one face to the
-// next, and the face's shared division is taken when the upper cell's
-// right-biased state is known.
+// Face fluxes of direction D for the whole tile, differenced into the
+// per-cell accumulators R (shared memory, the core's padded layout).  Each of
+// the tile's 64 lines along D has 9 faces (face a between cells a-1 and a);
+// thread t takes the run of faces 3r .. 3r+2, r = t / 64, of line t % 64,
+// walking up the line so that each cell's smoothness indicators serve both of
+// its faces: the left-biased state of cell a-1 is carried from one face to
+// the next.  The flux of the previous face stays in registers, so a run
+// completes its cells 3r and 3r+1 by itself; the third cell of runs 0 and 1
+// takes the next run's first face through the exchange slots X after a
+// barrier.  R and X: [5][NACC] with R at entry core_sm(x, y, z) and X at
+// NCORE_SM + 64 (r - 1) + line.
 template <typename T>
-__device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restrict__ F, T (&acc)[CPT][5],
-                                      T gamma, T igm1, T ihd)
+__device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restrict__ A, T gamma, T igm1, T ihd)
 {
     const int cs = D == 0 ? 1 : (D == 1 ? CY : CZ);     // shared stride along D (core and halo slot)
-    const int fs = D == 0 ? 1 : (D == 1 ? TB : TB * TB); // face-array stride along D
     const int run = threadIdx.x >> 6, line = threadIdx.x & 63;
     const int l0 = line & 7, l1 = line >> 3;
     const int x = D == 0 ? 0 : l0, y = D == 1 ? 0 : (D == 0 ? l0 : l1), z = D == 2 ? 0 : l1;
     const int cbase = core_sm(x, y, z);                          // the line's cell 0
     const int hbase = Stg<T>::slot(D) + halo_sm(D, x, y, z, 0);  // the line's slab cell h = 0
-    // face 0 of the line in the face arrays
-    const int fbase = D == 0 ? (TB + 1) * (y + TB * z) : (D == 1 ? x + TB * (TB + 1) * z : x + TB * y);
     const int f0 = 3 * run;
     auto sidx = [&](int a) {
         return (unsigned)a < (unsigned)TB ? cbase + a * cs : hbase + (a < 0 ? a + G : a - TB + G) * cs;
     };
     // left-biased state of cell f0-1, the lower cell of the run's first face
-    T Ln[5], Ld[5];
+    T VL[5];
     {
         int id[5];
 #pragma unroll
@@ -231,68 +232,69 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const T *Wc = W + c * Stg<T>::SV;
-            const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], Wc[id[2]], Wc[id[3]], Wc[id[4]]);
-            T p12, p02, p01;
+            const T u2 = Wc[id[2]];
+            const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
+            T p12, p02, p01, nl, dl;
             weno5_beta(df, p12, p02, p01);
-            weno5_left(df, p12, K<T>::d1 * p02, p01, Ln[c], Ld[c]);
+            weno5_left(df, p12, K<T>::d1 * p02, p01, nl, dl);
+            VL[c] = weno5_value(u2, nl, dl);
         }
     }
+    T Fq[5]; // flux of the previous face of the run
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-        const int a = f0 + i; // face a: cells a-1 (left state carried in Ln, Ld) and a
+        const int a = f0 + i; // face a: cells a-1 (left state carried in VL) and a
         int id[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k)
             id[k] = sidx(a - 2 + k);
         T WL[5], WR[5];
-        // variables (0,1) and (2,3) share one division; the first of a pair
-        // waits in (hul, hnl, hdl, hur, hnr, hdr) for the second
-        T hul = T(0), hnl = T(0), hdl = T(1), hur = T(0), hnr = T(0), hdr = T(1);
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const T *Wc = W + c * Stg<T>::SV;
-            const T u1 = Wc[id[1]], u2 = Wc[id[2]]; // cells a-1 and a
-            const Diff5<T> df = weno5_diff(Wc[id[0]], u1, u2, Wc[id[3]], Wc[id[4]]);
+            const T u2 = Wc[id[2]]; // cell a
+            const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
             T p12, p02, p01, nr, dr;
             weno5_beta(df, p12, p02, p01);
             const T w1 = K<T>::d1 * p02;
             weno5_right(df, p12, w1, p01, nr, dr);
-            if (c == 0 || c == 2) {
-                hul = u1;
-                hnl = Ln[c];
-                hdl = Ld[c];
-                hur = u2;
-                hnr = nr;
-                hdr = dr;
-            } else if (c == 1 || c == 3) {
-                face_states2(hul, hnl, hdl, hur, hnr, hdr, u1, Ln[c], Ld[c], u2, nr, dr, WL[c - 1], WR[c - 1], WL[c],
-                             WR[c]);
-            } else {
-                face_states(u1, Ln[c], Ld[c], u2, nr, dr, WL[c], WR[c]);
+            WR[c] = weno5_value(u2, nr, dr);
+            WL[c] = VL[c];
+            if (i < 2) { // cell a's left-biased state: the left state of face a+1
+                T nl, dl;
+                weno5_left(df, p12, w1, p01, nl, dl);
+                VL[c] = weno5_value(u2, nl, dl);
             }
-            if (i < 2)
-                weno5_left(df, p12, w1, p01, Ln[c], Ld[c]);
         }
         T Fl[5];
         rusanov<T>(WL, WR, D, gamma, igm1, Fl);
-        const int fi = fbase + a * fs;
+        if (i == 0) {
+            if (run > 0) {
 #pragma unroll
-        for (int c = 0; c < 5; ++c)
-            F[c * NFACE + fi] = Fl[c];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const int cidx = threadIdx.x + k * NT;
-        if (cidx < NCELL) {
-            const int cx = cidx % TB, cy = (cidx / TB) % TB, cz = cidx / (TB * TB);
-            const int flo = D == 0 ? cx + (TB + 1) * (cy + TB * cz)
-                                   : (D == 1 ? cx + TB * (cy + (TB + 1) * cz) : cx + TB * (cy + TB * cz));
+                for (int c = 0; c < 5; ++c)
+                    A[c * NACC + NCORE_SM + 64 * (run - 1) + line] = Fl[c];
+            }
+        } else {
+            // cell a-1 is complete: faces a-1 (Fq) and a (Fl)
+            const int e = cbase + (a - 1) * cs;
 #pragma unroll
             for (int c = 0; c < 5; ++c) {
-                const T df = F[c * NFACE + flo + fs] - F[c * NFACE + flo];
-                acc[k][c] = D == 0 ? df * ihd : dfma(df, ihd, acc[k][c]);
+                const T df = Fl[c] - Fq[c];
+                A[c * NACC + e] = D == 0 ? df * ihd : dfma(df, ihd, A[c * NACC + e]);
             }
+        }
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+            Fq[c] = Fl[c];
+    }
+    __syncthreads(); // X
+    if (run < 2) {
+        // cell f0+2: faces f0+2 (Fq) and f0+3, the first face of run r+1
+        const int e = cbase + (f0 + 2) * cs;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const T df = A[c * NACC + NCORE_SM + 64 * run + line] - Fq[c];
+            A[c * NACC + e] = D == 0 ? df * ihd : dfma(df, ihd, A[c * NACC + e]);
         }
     }
     __syncthreads();
@@ -358,9 +360,9 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
 
 // The whole stage for one tile: staging, three sweeps, RK epilogue and the
 // tile's FP64 sums (written to p.partials[slot] if requested).  Uses
-// W [5][Stg<T>::SV], F [5][NFACE] and red [NT/32][5] in shared memory.
+// W [5][Stg<T>::SV], A [5][NACC] and red [NT/32][5] in shared memory.
 template <typename T, typename Src>
-__device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &src, int item, int slot, T *W, T *F,
+__device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &src, int item, int slot, T *W, T *A,
                                            double (*red)[5], int *snb, TileInfo<T> *ts)
 {
     // the tile's geometry is kept in shared memory (ts) and re-read after each
@@ -412,13 +414,6 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
     }
     __syncthreads();
 
-    T acc[CPT][5];
-#pragma unroll
-    for (int k = 0; k < CPT; ++k)
-#pragma unroll
-        for (int c = 0; c < 5; ++c)
-            acc[k][c] = T(0);
-
 #pragma unroll 1
     for (int D = 0; D < 3; ++D) {
         if (!Stg<T>::all && D > 0) {
@@ -427,7 +422,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
         }
         // the Rusanov fluxes are twice the flux: 1/(2h) (exact)
         const T ihd = T(0.5) * (D == 0 ? t.ih[0] : (D == 1 ? t.ih[1] : t.ih[2]));
-        sweep<T>(D, W, F, acc, p.gamma, p.igm1, ihd);
+        sweep<T>(D, W, A, p.gamma, p.igm1, ihd);
     }
 
     // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows.
@@ -438,6 +433,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
     // value.  Each (component, cell) is loaded before it is stored.
     double sums[5] = {0, 0, 0, 0, 0};
     int64_t eo[CPT];
+    int ea[CPT];
     bool eok[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
@@ -445,6 +441,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
         eok[k] = cidx < NCELL;
         const int x = cidx % TB, y = (cidx / TB) % TB, z = cidx / (TB * TB);
         eo[k] = t.boff + (t.x0 + x) + (int64_t)t.N0 * ((t.y0 + y) + (int64_t)t.N1 * (t.z0 + z));
+        ea[k] = core_sm(x, y, z);
     }
     T us[2][CPT], un[2][CPT];
 #pragma unroll
@@ -465,7 +462,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             if (eok[k]) {
-                const T rhs = -acc[k][c];
+                const T rhs = -A[c * NACC + ea[k]];
                 T v;
                 if (p.stage == 0) {
                     v = rhs;

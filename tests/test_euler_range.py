@@ -5,11 +5,13 @@ FP32 range above J ~ 4e4: a pressure jump of one bar in pascals.  FP32 forms
 them from the smoothness sums rescaled by an exact power of two (largest and
 middle exponent), so the FP32 Euler RHS stays finite and tracks FP64 at any
 pressure scale.  CPU tests check the oracle; GPU tests check the device
-against the oracle bit for bit on the same data."""
+against the oracle on the same data, within the tolerances of
+tests/numerics.py."""
 import numpy as np
 import pytest
 
 import oracle as O
+from numerics import TOL_F32_RHS, TOL_F32_STATE, TOL_F64, assert_close
 
 GAMMA = 1.4
 PRESSURES = [1e5, 1e9, 1e12]  # Pa: one bar, 10 kbar, 10 Mbar
@@ -101,8 +103,8 @@ def test_device_rhs_si_units_matches_oracle(cn, oracle_lib, P, dtype):
     torch.cuda.synchronize()
     want = oracle_lib.euler_stage(host, None, NB, N, None, 0, 0.0, GAMMA, U.getCellSize())
     got = np.stack([R.download(c) for c in range(5)])
-    assert np.isfinite(_cells(got, N, dtype)).all()
-    assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+    assert_close(_cells(got, N, dtype), _cells(want, N, dtype),
+                 TOL_F64 if dtype == np.float64 else TOL_F32_RHS, f"SI rhs P={P:g} {np.dtype(dtype).name}")
 
 
 @pytest.mark.gpu
@@ -117,5 +119,5 @@ def test_device_rk3_step_si_units_matches_oracle(cn, oracle_lib, dtype):
     torch.cuda.synchronize()
     want = oracle_lib.euler_rk3_step(host, NB, N, None, dt, GAMMA, U.getCellSize())
     got = np.stack([U.download(c) for c in range(5)])
-    assert np.isfinite(_cells(got, N, dtype)).all()
-    assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+    assert_close(_cells(got, N, dtype), _cells(want, N, dtype),
+                 TOL_F64 if dtype == np.float64 else TOL_F32_STATE, f"SI rk3 step {np.dtype(dtype).name}")

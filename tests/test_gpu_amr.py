@@ -1,8 +1,11 @@
-"""Two-level AMR layouts: interface ghost fill and the fused Euler stage vs
-the CPU oracle (bit-exact), a steady uniform state at the full size,
-schedule independence, and CUDA-graph replay of the RK3 step."""
+"""Two-level AMR layouts: interface ghost fill (bit-exact) and the fused
+Euler stage (within the FP64 tolerance of tests/numerics.py) vs the CPU
+oracle, a steady uniform state at the full size, schedule independence, and
+CUDA-graph replay of the RK3 step."""
 import numpy as np
 import pytest
+
+from numerics import TOL_F64, assert_close
 
 pytestmark = pytest.mark.gpu
 GAMMA = 1.4
@@ -48,7 +51,7 @@ def test_amr_stage_matches_oracle(cn, oracle_lib, stage):
     blk, _ = oracle_lib.amr_blocks(l, c, o, F)
     want = oracle_lib.amr_stage(host, hn if stage > 1 else None, blk, F, stage, 2e-4, GAMMA)
     got = np.stack([out.download(k) for k in range(5)])
-    assert np.array_equal(got, want)
+    assert_close(got, want, TOL_F64, f"amr stage {stage}")
 
 
 def test_amr_schedules_and_graph_are_bitwise_identical(cn):
