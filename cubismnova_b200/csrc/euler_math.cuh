@@ -179,6 +179,77 @@ template <typename T> __device__ __forceinline__ T weno5_value(T u2, T num, T de
     return dfma(num, rcp_pos(den), u2);
 }
 
+// ---------------------------------------------------------------------------
+// FP32, two variables per instruction.  Blackwell executes FP32 add, multiply
+// and fused multiply-add on a pair of values per thread (PTX add/mul/fma
+// .rn.f32x2, CUDA's __fadd2_rn / __fmul2_rn / __ffma2_rn); the WENO5 formulas
+// above are evaluated for two primitive variables at once, lane x holding
+// one variable and lane y the other.  Same operations as the scalar forms,
+// one packed instruction per pair.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.0f), a); }
+
+struct Diff5x2 {
+    float2 d01, d12, d23, d34;
+};
+__device__ __forceinline__ Diff5x2 weno5_diff2(float2 u0, float2 u1, float2 u2, float2 u3, float2 u4)
+{
+    return {sub2(u1, u0), sub2(u2, u1), sub2(u3, u2), sub2(u4, u3)};
+}
+
+// weno5_beta for a pair; the rescaling factor is formed per lane.  h2 enters
+// squared only, so its sign is dropped: h2' = d23 - a2/2.
+__device__ __forceinline__ void weno5_beta2(const Diff5x2 &d, float2 &p12, float2 &p02, float2 &p01)
+{
+    using C = K<float>;
+    const float2 a0 = sub2(d.d12, d.d01), a1 = sub2(d.d23, d.d12), a2 = sub2(d.d34, d.d23);
+    const float2 h0 = fma2(f2(C::half), a0, d.d12);
+    const float2 h1 = mul2(f2(C::half), add2(d.d12, d.d23));
+    const float2 h2 = fma2(f2(-C::half), a2, d.d23);
+    const float2 s0 = fma2(mul2(f2(C::c1312), a0), a0, fma2(h0, h0, f2(C::eps)));
+    const float2 s1 = fma2(mul2(f2(C::c1312), a1), a1, fma2(h1, h1, f2(C::eps)));
+    const float2 s2 = fma2(mul2(f2(C::c1312), a2), a2, fma2(h2, h2, f2(C::eps)));
+    const float2 sc = make_float2(weno5_scale(s0.x, s1.x, s2.x), weno5_scale(s0.y, s1.y, s2.y));
+    const float2 q0 = mul2(s0, sc), q1 = mul2(s1, sc), q2 = mul2(s2, sc);
+    const float2 t0 = mul2(q0, q0), t1 = mul2(q1, q1), t2 = mul2(q2, q2);
+    p12 = mul2(t1, t2);
+    p02 = mul2(t0, t2);
+    p01 = mul2(t0, t1);
+}
+
+__device__ __forceinline__ void weno5_left2(const Diff5x2 &d, float2 p12, float2 w1, float2 p01, float2 &num,
+                                            float2 &den)
+{
+    using C = K<float>;
+    const float2 w0 = mul2(f2(C::d0), p12), w2 = mul2(f2(C::d2), p01);
+    const float2 e0 = fma2(f2(-2.0f), d.d01, mul2(f2(5.0f), d.d12));
+    const float2 e1 = fma2(f2(2.0f), d.d23, d.d12);
+    const float2 e2 = sub2(mul2(f2(4.0f), d.d23), d.d34);
+    num = fma2(w0, e0, fma2(w1, e1, mul2(w2, e2)));
+    den = mul2(f2(C::six), add2(add2(w0, w1), w2));
+}
+
+__device__ __forceinline__ void weno5_right2(const Diff5x2 &d, float2 p12, float2 w1, float2 p01, float2 &num,
+                                             float2 &den)
+{
+    using C = K<float>;
+    const float2 r0 = mul2(f2(C::d2), p12), r2 = mul2(f2(C::d0), p01);
+    const float2 f0 = fma2(f2(-4.0f), d.d12, d.d01);
+    const float2 f1 = sub2(mul2(f2(-2.0f), d.d12), d.d23);
+    const float2 g2 = fma2(f2(2.0f), d.d34, mul2(f2(-5.0f), d.d23));
+    num = fma2(r0, f0, fma2(w1, f1, mul2(r2, g2)));
+    den = mul2(f2(C::six), add2(add2(r0, w1), r2));
+}
+
+__device__ __forceinline__ float2 weno5_value2(float2 u2, float2 num, float2 den)
+{
+    return fma2(num, make_float2(rcp_pos(den.x), rcp_pos(den.y)), u2);
+}
+
 // Twice the Rusanov flux through a face with normal direction `d` (0,1,2)
 // from the reconstructed primitive states WL, WR = (rho, u, v, w, p):
 // F = (f(UL) + f(UR)) - a (UR - UL), a = max(|u_n| + c) of both sides.  The
@@ -220,6 +291,39 @@ __device__ __forceinline__ void rusanov(const T (&WL)[5], const T (&WR)[5], int 
     const T Er = dfma(C::half * rr, ker, pr * igm1);
     const T fl4 = (El + pl) * unl, fr4 = (Er + pr) * unr;
     F[4] = dfma(-a, Er - El, fl4 + fr4);
+}
+
+// FP32 Rusanov flux with the two sides of the face in the two lanes of a
+// pair: lane x the left state, lane y the right state.  Same operations as
+// rusanov<float>; the side sums and differences are scalar.
+__device__ __forceinline__ void rusanov2(const float (&WL)[5], const float (&WR)[5], int d, float gamma,
+                                         float igm1, float (&F)[5])
+{
+    const float2 r = make_float2(WL[0], WR[0]);
+    const float2 un = d == 0 ? make_float2(WL[1], WR[1]) : (d == 1 ? make_float2(WL[2], WR[2]) : make_float2(WL[3], WR[3]));
+    const float2 p = make_float2(WL[4], WR[4]);
+    // sound speeds c = (gamma p) / sqrt(gamma p rho)
+    const float2 gp = mul2(f2(gamma), p);
+    const float2 arg = mul2(gp, r);
+    const float2 c = mul2(gp, make_float2(rsqrt_pos(arg.x), rsqrt_pos(arg.y)));
+    const float2 s = add2(make_float2(fabsf(un.x), fabsf(un.y)), c);
+    const float a = fmaxf(s.x, s.y);
+    const float2 f0 = mul2(r, un);
+    F[0] = fmaf(-a, r.y - r.x, f0.x + f0.y);
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const float2 v = make_float2(WL[k], WR[k]);
+        const float2 m = mul2(r, v);
+        float2 f = mul2(f0, v);
+        if (k - 1 == d)
+            f = add2(f, p);
+        F[k] = fmaf(-a, m.y - m.x, f.x + f.y);
+    }
+    const float2 v1 = make_float2(WL[1], WR[1]), v2 = make_float2(WL[2], WR[2]), v3 = make_float2(WL[3], WR[3]);
+    const float2 ke = fma2(v1, v1, fma2(v2, v2, mul2(v3, v3)));
+    const float2 E = fma2(mul2(f2(K<float>::half), r), ke, mul2(p, f2(igm1)));
+    const float2 f4 = mul2(add2(E, p), un);
+    F[4] = fmaf(-a, E.y - E.x, f4.x + f4.y);
 }
 
 // Conservative -> primitive (rho, u, v, w, p).

@@ -37,6 +37,17 @@ template <typename T> struct Stg {
         return NCORE_SM + (all ? (D == 0 ? 0 : (D == 1 ? HS0 : HS0 + HS1)) : 0);
     }
 };
+// Where primitive variable c of shared entry e (core cell or halo-slot cell)
+// lives.  FP64: one array per variable, [5][SV].  FP32: variables (0, 1) and
+// (2, 3) interleaved as pairs, so that one 64-bit shared access and one
+// packed FP32x2 instruction serve two variables, and variable 4 alone:
+// [pairs (0,1): 2 SV][pairs (2,3): 2 SV][variable 4: SV].
+__device__ __forceinline__ double &prim(double *W, int c, int e) { return W[c * Stg<double>::SV + e]; }
+__device__ __forceinline__ float &prim(float *W, int c, int e)
+{
+    constexpr int SV = Stg<float>::SV;
+    return c < 2 ? W[2 * e + c] : (c < 4 ? W[2 * SV + 2 * e + (c - 2)] : W[4 * SV + e]);
+}
 constexpr int NCELL = TB * TB * TB;   // 512
 // per variable: the cells' flux-difference accumulators (core layout) and
 // the 2 x 64 face fluxes exchanged between the runs of a line
@@ -198,13 +209,127 @@ __device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z, 
     }
 }
 
+// WENO5 states along a line of a sweep: a cell's smoothness indicators serve
+// its right-biased state (lower face) and its left-biased state (upper face);
+// the left state waits in a carry for the next face.  id[0..4]: shared
+// entries of the cells a-2 .. a+2 around cell a.
+template <typename T>
+__device__ __forceinline__ T cell_left(const T *Wc, const int (&id)[5])
+{
+    const T u2 = Wc[id[2]];
+    const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
+    T p12, p02, p01, nl, dl;
+    weno5_beta(df, p12, p02, p01);
+    weno5_left(df, p12, K<T>::d1 * p02, p01, nl, dl);
+    return weno5_value(u2, nl, dl);
+}
+// face a: WL = carried left state of cell a-1, WR = right state of cell a;
+// with `more` the carry becomes cell a's left state
+template <typename T>
+__device__ __forceinline__ void cell_face(const T *Wc, const int (&id)[5], bool more, T &carry, T &wl, T &wr)
+{
+    const T u2 = Wc[id[2]];
+    const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
+    T p12, p02, p01, nr, dr;
+    weno5_beta(df, p12, p02, p01);
+    const T w1 = K<T>::d1 * p02;
+    weno5_right(df, p12, w1, p01, nr, dr);
+    wr = weno5_value(u2, nr, dr);
+    wl = carry;
+    if (more) {
+        T nl, dl;
+        weno5_left(df, p12, w1, p01, nl, dl);
+        carry = weno5_value(u2, nl, dl);
+    }
+}
+__device__ __forceinline__ float2 pair_left(const float2 *P, const int (&id)[5])
+{
+    const float2 u2 = P[id[2]];
+    const Diff5x2 df = weno5_diff2(P[id[0]], P[id[1]], u2, P[id[3]], P[id[4]]);
+    float2 p12, p02, p01, nl, dl;
+    weno5_beta2(df, p12, p02, p01);
+    weno5_left2(df, p12, mul2(f2(K<float>::d1), p02), p01, nl, dl);
+    return weno5_value2(u2, nl, dl);
+}
+__device__ __forceinline__ void pair_face(const float2 *P, const int (&id)[5], bool more, float2 &carry, float2 &wl,
+                                          float2 &wr)
+{
+    const float2 u2 = P[id[2]];
+    const Diff5x2 df = weno5_diff2(P[id[0]], P[id[1]], u2, P[id[3]], P[id[4]]);
+    float2 p12, p02, p01, nr, dr;
+    weno5_beta2(df, p12, p02, p01);
+    const float2 w1 = mul2(f2(K<float>::d1), p02);
+    weno5_right2(df, p12, w1, p01, nr, dr);
+    wr = weno5_value2(u2, nr, dr);
+    wl = carry;
+    if (more) {
+        float2 nl, dl;
+        weno5_left2(df, p12, w1, p01, nl, dl);
+        carry = weno5_value2(u2, nl, dl);
+    }
+}
+
+// Carried left states of the five variables: FP64 one by one, FP32 as the
+// pairs (0,1), (2,3) and variable 4.
+struct CarryD {
+    double v[5];
+};
+struct CarryF {
+    float2 p01, p23;
+    float v4;
+};
+__device__ __forceinline__ void line_left(const double *W, const int (&id)[5], CarryD &cl)
+{
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+        cl.v[c] = cell_left(W + c * Stg<double>::SV, id);
+}
+__device__ __forceinline__ void line_face(const double *W, const int (&id)[5], bool more, CarryD &cl,
+                                          double (&WL)[5], double (&WR)[5])
+{
+#pragma unroll
+    for (int c = 0; c < 5; ++c)
+        cell_face(W + c * Stg<double>::SV, id, more, cl.v[c], WL[c], WR[c]);
+}
+__device__ __forceinline__ void line_left(const float *W, const int (&id)[5], CarryF &cl)
+{
+    constexpr int SV = Stg<float>::SV;
+    cl.p01 = pair_left(reinterpret_cast<const float2 *>(W), id);
+    cl.p23 = pair_left(reinterpret_cast<const float2 *>(W + 2 * SV), id);
+    cl.v4 = cell_left(W + 4 * SV, id);
+}
+__device__ __forceinline__ void line_face(const float *W, const int (&id)[5], bool more, CarryF &cl,
+                                          float (&WL)[5], float (&WR)[5])
+{
+    constexpr int SV = Stg<float>::SV;
+    float2 l01, r01, l23, r23;
+    pair_face(reinterpret_cast<const float2 *>(W), id, more, cl.p01, l01, r01);
+    pair_face(reinterpret_cast<const float2 *>(W + 2 * SV), id, more, cl.p23, l23, r23);
+    cell_face(W + 4 * SV, id, more, cl.v4, WL[4], WR[4]);
+    WL[0] = l01.x;
+    WL[1] = l01.y;
+    WL[2] = l23.x;
+    WL[3] = l23.y;
+    WR[0] = r01.x;
+    WR[1] = r01.y;
+    WR[2] = r23.x;
+    WR[3] = r23.y;
+}
+template <typename T> struct CarryOf;
+template <> struct CarryOf<double> {
+    using type = CarryD;
+};
+template <> struct CarryOf<float> {
+    using type = CarryF;
+};
+
 // Face fluxes of direction D for the whole tile, differenced into the
 // per-cell accumulators R (shared memory, the core's padded layout).  Each of
 // the tile's 64 lines along D has 9 faces (face a between cells a-1 and a);
 // thread t takes the run of faces 3r .. 3r+2, r = t / 64, of line t % 64,
 // walking up the line so that each cell's smoothness indicators serve both of
 // its faces: the left-biased state of cell a-1 is carried from one face to
-// the next.  The flux of the previous face stays in registers, so a run
+// the next (line_left / line_face).  The flux of the previous face stays in registers, so a run
 // completes its cells 3r and 3r+1 by itself; the third cell of runs 0 and 1
 // takes the next run's first face through the exchange slots X after a
 // barrier.  R and X: [5][NACC] with R at entry core_sm(x, y, z) and X at
@@ -223,22 +348,13 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
         return (unsigned)a < (unsigned)TB ? cbase + a * cs : hbase + (a < 0 ? a + G : a - TB + G) * cs;
     };
     // left-biased state of cell f0-1, the lower cell of the run's first face
-    T VL[5];
+    typename CarryOf<T>::type carry;
     {
         int id[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k)
             id[k] = sidx(f0 - 3 + k);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            const T *Wc = W + c * Stg<T>::SV;
-            const T u2 = Wc[id[2]];
-            const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
-            T p12, p02, p01, nl, dl;
-            weno5_beta(df, p12, p02, p01);
-            weno5_left(df, p12, K<T>::d1 * p02, p01, nl, dl);
-            VL[c] = weno5_value(u2, nl, dl);
-        }
+        line_left(W, id, carry);
     }
     T Fq[5]; // flux of the previous face of the run
 #pragma unroll 1
@@ -249,25 +365,12 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
         for (int k = 0; k < 5; ++k)
             id[k] = sidx(a - 2 + k);
         T WL[5], WR[5];
-#pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            const T *Wc = W + c * Stg<T>::SV;
-            const T u2 = Wc[id[2]]; // cell a
-            const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
-            T p12, p02, p01, nr, dr;
-            weno5_beta(df, p12, p02, p01);
-            const T w1 = K<T>::d1 * p02;
-            weno5_right(df, p12, w1, p01, nr, dr);
-            WR[c] = weno5_value(u2, nr, dr);
-            WL[c] = VL[c];
-            if (i < 2) { // cell a's left-biased state: the left state of face a+1
-                T nl, dl;
-                weno5_left(df, p12, w1, p01, nl, dl);
-                VL[c] = weno5_value(u2, nl, dl);
-            }
-        }
+        line_face(W, id, i < 2, carry, WL, WR);
         T Fl[5];
-        rusanov<T>(WL, WR, D, gamma, igm1, Fl);
+        if constexpr (sizeof(T) == 4)
+            rusanov2(WL, WR, D, gamma, igm1, Fl);
+        else
+            rusanov<T>(WL, WR, D, gamma, igm1, Fl);
         if (i == 0) {
             if (run > 0) {
 #pragma unroll
@@ -312,7 +415,7 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
 {
     static_assert(NHALO % NT == 0, "whole halo cells per thread");
     constexpr int HPT = NHALO / NT; // halo cells per thread: 2
-    T *slot = W + Stg<T>::slot(D);
+    const int sb = Stg<T>::slot(D); // first shared entry of the halo slot
     // first pass: the plain loads of all of the thread's cells (inside the
     // block, or the periodic neighbour's cell when every component is plain)
     // are issued together; the other cells are resolved into the slot
@@ -339,7 +442,7 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
         } else {
 #pragma unroll 1
             for (int c = 0; c < 5; ++c)
-                slot[c * Stg<T>::SV + si[j]] = src.halo(p.U[c], c, t, gx, gy, gz, snb);
+                prim(W, c, sb + si[j]) = src.halo(p.U[c], c, t, gx, gy, gz, snb);
         }
     }
     // second pass: conversion to primitives in place
@@ -348,13 +451,13 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
         if (!inb[j]) {
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                u[j][c] = slot[c * Stg<T>::SV + si[j]];
+                u[j][c] = prim(W, c, sb + si[j]);
         }
         T w[5];
         to_primitive<T>(u[j][0], u[j][1], u[j][2], u[j][3], u[j][4], p.gm1, w);
 #pragma unroll
         for (int c = 0; c < 5; ++c)
-            slot[c * Stg<T>::SV + si[j]] = w[c];
+            prim(W, c, sb + si[j]) = w[c];
     }
 }
 
@@ -401,7 +504,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
                 const int e = core_sm(i % TB, (i / TB) % TB, i / (TB * TB));
 #pragma unroll
                 for (int c = 0; c < 5; ++c)
-                    W[c * Stg<T>::SV + e] = w[c];
+                    prim(W, c, e) = w[c];
             }
         }
     }
