@@ -11,8 +11,9 @@ descriptions; FP64 unless stated):
          stage update; BCs x periodic, y absorbing, z Dirichlet (far field).
          Metric counts cell-updates per RK stage.
   c4     the same Euler step at 1024^3 cells (32^3 blocks of 32^3), FP32.
-  c3     two-level AMR layout, 2136 blocks of 8^3/16^3/32^3 cells, FP64 Euler,
-         one CUDA graph (3 persistent launches) per SSP-RK3 step.
+  c3     two-level AMR layout, 2048 blocks drawn by seed from 8^3/16^3/32^3
+         cells (50/35/15 %), FP64 Euler, one CUDA graph (3 persistent
+         launches) per SSP-RK3 step.
   c1     128^3 cells = 8^3 blocks of 16^3, one scalar, lab (-1,2) + 7-point
          Laplacian + central gradient fused (one kernel per step).
   c5     variable-coefficient Poisson div(k grad p) = f, 256^3 cells = 8^3
@@ -515,15 +516,16 @@ class C4(Euler):
 
 
 class C3:
-    """Batched two-level AMR step: 2136 blocks of 8^3/16^3/32^3 cells (seeded
-    octree, 652 on the refined level), level-interface ghosts by trilinear
-    prolongation and conservative restriction, FP64 Euler; each SSP-RK3 step
-    is one CUDA graph of three persistent launches over the tile work list,
-    schedule chosen by the autotuner."""
+    """Batched two-level AMR step: 2048 blocks whose sizes are drawn by seed
+    from {8^3: 50 %, 16^3: 35 %, 32^3: 15 %} (workloads.amr_layout: about
+    13.5 M cells, a level-0 tiling refined in a seeded ball), level-interface
+    ghosts by trilinear prolongation and conservative restriction, FP64
+    Euler; each SSP-RK3 step is one CUDA graph of three persistent launches
+    over the tile work list, schedule chosen by the autotuner."""
     name = "c3"
-    desc = ("AMR Euler SSP-RK3 step, 2136 blocks of {8,16,32}^3 cells on 2 levels (18.3 M cells), FP64, "
-            "interface ghosts by trilinear prolongation / conservative restriction, one CUDA graph per step "
-            "(3 persistent launches), autotuned schedule")
+    desc = ("AMR Euler SSP-RK3 step, 2048 blocks drawn by seed from {8^3: 50%, 16^3: 35%, 32^3: 15%} cells on "
+            "2 levels (ratio 2), FP64, interface ghosts by trilinear prolongation / conservative restriction, "
+            "one CUDA graph per step (3 persistent launches), autotuned schedule")
     dtype = "f64"
     stages = 3
     launches_per_step = 3
@@ -537,14 +539,17 @@ class C3:
         self.cn, self.torch = cn, torch
         l, c, o, F = cn.workloads.amr_layout()
         self.U = cn.amr.AmrGrid(l, c, o, F)
+        self.layout = dict(blocks=len(l), box_level1_cells=list(F),
+                           level1_blocks=[int(np.sum((l == 1) & (c == k))) for k in (8, 16, 32)],
+                           level0_blocks=[int(np.sum((l == 0) & (c == k))) for k in (8, 16, 32)])
         self.w1, self.w2 = self.U.like(), self.U.like()
         cn.workloads.euler_pulse_amr(self.U)
         self.cells = self.U.total_cells
         self.updates_per_step = self.cells * self.stages
         self.flops_per_cell_stage = EULER_FLOPS_PER_CELL_STAGE[self.dtype]
-        self.nb, self.n = (len(l),), (int(F),)
-        # CFL on the fine level (h = 1/F), sound speed of the pulse state < 1.3
-        self.dt = 0.3 / (3 * 1.3 * F)
+        self.nb, self.n = (len(l),), tuple(int(e) for e in F)
+        # CFL on the fine level (h = 1/Lx), sound speed of the pulse state < 1.3
+        self.dt = 0.3 / (3 * 1.3 * F[0])
         order, ctas, ms = cn.amr.autotune(self.U, self.w1, self.w2, self.dt, reps=2)
         self.schedule = dict(order=["block order", "largest blocks first", "Morton"][order], ctas=ctas,
                              ms_per_step=round(ms, 3))
@@ -556,7 +561,7 @@ class C3:
         self.graph = cn.amr.Graph.capture(
             lambda: cn.amr.rk3_step(self.U, self.w1, self.w2, self.dt, stream=self.stream), self.stream)
         self.h_state = None
-        self.desc = self.desc + f"; schedule {self.schedule}"
+        self.desc = self.desc + f"; layout {self.layout}; schedule {self.schedule}"
 
     def needs_flush(self):
         return False

@@ -14,6 +14,7 @@ _P, _I, _D = C.c_void_p, C.c_int, C.c_double
 _I64 = C.c_int64
 _lib.register({
     "cn_amr_create": (_I, [_I, _P, _P, _P, _I, _I, _I, C.POINTER(_P)]),
+    "cn_amr_create_box": (_I, [_I, _P, _P, _P, C.POINTER(_I), _I, _I, C.POINTER(_P)]),
     "cn_amr_destroy": (_I, [_P]),
     "cn_amr_info": (_I, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I)]),
     "cn_amr_block_offset": (_I, [_P, _I, C.POINTER(_I64)]),
@@ -32,19 +33,23 @@ _lib.register({
 
 class AmrGrid:
     """Blocks (level, cells, origin in level-1 units) tiling a periodic unit box
-    of ``fine_extent`` level-1 cells; ``ncomp`` components."""
+    of ``fine_extent`` level-1 cells (one extent for a cube, or (Lx, Ly, Lz));
+    cells are cubic with h = cell size / Lx; ``ncomp`` components."""
 
-    def __init__(self, levels, cells, origins, fine_extent: int, ncomp: int = 5, dtype=np.float64):
+    def __init__(self, levels, cells, origins, fine_extent, ncomp: int = 5, dtype=np.float64):
         self.levels = np.asarray(levels, dtype=np.int32)
         self.cells = np.asarray(cells, dtype=np.int32)
         self.origins = np.ascontiguousarray(np.asarray(origins, dtype=np.int32).reshape(-1, 3))
-        self.L1, self.ncomp, self.dtype = int(fine_extent), int(ncomp), np.dtype(dtype)
+        ext = np.broadcast_to(np.asarray(fine_extent, dtype=np.int64), (3,))
+        self.L = tuple(int(e) for e in ext)
+        self.L1 = self.L[0]
+        self.ncomp, self.dtype = int(ncomp), np.dtype(dtype)
         dt = {np.dtype(np.float32): _lib.CN_FLOAT32, np.dtype(np.float64): _lib.CN_FLOAT64}[self.dtype]
         h = C.c_void_p()
-        _lib.check(_lib.lib().cn_amr_create(len(self.levels), self.levels.ctypes.data_as(C.c_void_p),
-                                            self.cells.ctypes.data_as(C.c_void_p),
-                                            self.origins.ctypes.data_as(C.c_void_p), self.L1, self.ncomp, dt,
-                                            C.byref(h)))
+        _lib.check(_lib.lib().cn_amr_create_box(len(self.levels), self.levels.ctypes.data_as(C.c_void_p),
+                                                self.cells.ctypes.data_as(C.c_void_p),
+                                                self.origins.ctypes.data_as(C.c_void_p), _lib.ivec3(self.L),
+                                                self.ncomp, dt, C.byref(h)))
         self._h = h
         tc, cs, ni = C.c_int64(), C.c_int64(), C.c_int()
         _lib.check(_lib.lib().cn_amr_info(h, C.byref(tc), C.byref(cs), C.byref(ni)))
@@ -71,7 +76,7 @@ class AmrGrid:
         return len(self.levels)
 
     def like(self):
-        return AmrGrid(self.levels, self.cells, self.origins, self.L1, self.ncomp, self.dtype)
+        return AmrGrid(self.levels, self.cells, self.origins, self.L, self.ncomp, self.dtype)
 
     def tensor(self, comp=0):
         import torch
@@ -104,8 +109,13 @@ class AmrGrid:
     def set_schedule(self, order: int, ctas: int):
         _lib.check(_lib.lib().cn_amr_set_schedule(self._h, order, ctas))
 
+    def box(self):
+        """Physical extents of the periodic box: (1, Ly/Lx, Lz/Lx)."""
+        return tuple(e / self.L[0] for e in self.L)
+
     def cell_centres(self):
-        """(x, y, z) cell-centre coordinates of all cells, block order (torch, cuda)."""
+        """(x, y, z) cell-centre coordinates of all cells, block order (torch,
+        cuda), in the box [0,1] x [0, Ly/Lx] x [0, Lz/Lx]."""
         import torch
         dev = "cuda"
         n = torch.tensor(self.cells, device=dev, dtype=torch.int64)

@@ -84,7 +84,7 @@ using namespace cn;
 using namespace cn::amr;
 
 struct cn_amr {
-    int nblocks = 0, L1 = 0, lres = 0, ncomp = 0;
+    int nblocks = 0, L[3] = {0, 0, 0}, lr[3] = {0, 0, 0}, ncomp = 0;
     cn_dtype dtype = CN_FLOAT64;
     size_t es = 8;
     std::vector<BlockDev> blocks;
@@ -146,8 +146,10 @@ static Geom geom(const cn_amr *a)
     Geom g;
     g.blk = a->d_blocks;
     g.lookup = a->d_lookup;
-    g.L1 = a->L1;
-    g.lres = a->lres;
+    for (int d = 0; d < 3; ++d) {
+        g.L[d] = a->L[d];
+        g.lr[d] = a->lr[d];
+    }
     return g;
 }
 
@@ -200,24 +202,27 @@ struct cn_graph {
 
 extern "C" {
 
-cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const int *origin, int fine_extent,
-                        int ncomp, cn_dtype dtype, cn_amr **out)
+cn_status cn_amr_create_box(int nblocks, const int *level, const int *cells, const int *origin,
+                            const int fine_extent[3], int ncomp, cn_dtype dtype, cn_amr **out)
 {
-    if (!out || !level || !cells || !origin || nblocks < 1 || ncomp < 1)
+    if (!out || !level || !cells || !origin || !fine_extent || nblocks < 1 || ncomp < 1)
         return fail(CN_ERR_INVALID_ARGUMENT, "cn_amr_create: bad argument");
     *out = nullptr;
     if (dtype != CN_FLOAT64 && dtype != CN_FLOAT32)
         return fail(CN_ERR_UNSUPPORTED, "cn_amr_create: dtype must be FLOAT32 or FLOAT64");
-    if (fine_extent < 8 || fine_extent % 8)
-        return fail(CN_ERR_INVALID_ARGUMENT, "cn_amr_create: the extent must be a multiple of 8 level-1 cells");
+    for (int d = 0; d < 3; ++d)
+        if (fine_extent[d] < 8 || fine_extent[d] % 8)
+            return fail(CN_ERR_INVALID_ARGUMENT, "cn_amr_create: the extent must be a multiple of 8 level-1 cells");
     cn_amr *a = new cn_amr();
     a->nblocks = nblocks;
-    a->L1 = fine_extent;
-    a->lres = fine_extent / 8;
+    for (int d = 0; d < 3; ++d) {
+        a->L[d] = fine_extent[d];
+        a->lr[d] = fine_extent[d] / 8;
+    }
     a->ncomp = ncomp;
     a->dtype = dtype;
     a->es = dtype == CN_FLOAT64 ? 8 : 4;
-    std::vector<int32_t> lookup((size_t)a->lres * a->lres * a->lres, -1);
+    std::vector<int32_t> lookup((size_t)a->lr[0] * a->lr[1] * a->lr[2], -1);
     int64_t off = 0;
     for (int b = 0; b < nblocks; ++b) {
         BlockDev B;
@@ -229,10 +234,10 @@ cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const i
         B.pad = 0;
         B.off = off;
         const int cs = B.level == 0 ? 2 : 1;
-        B.ih = (double)fine_extent / cs; // h = cs / L1 on the unit box
+        B.ih = (double)fine_extent[0] / cs; // cubic cells: h = cs / Lx (the box is [0,1] x [0,Ly/Lx] x [0,Lz/Lx])
         if ((B.level != 0 && B.level != 1) || B.n < 8 || B.n % 8 || B.ox % 8 || B.oy % 8 || B.oz % 8 || B.ox < 0 ||
-            B.oy < 0 || B.oz < 0 || B.ox + B.n * cs > fine_extent || B.oy + B.n * cs > fine_extent ||
-            B.oz + B.n * cs > fine_extent) {
+            B.oy < 0 || B.oz < 0 || B.ox + B.n * cs > fine_extent[0] || B.oy + B.n * cs > fine_extent[1] ||
+            B.oz + B.n * cs > fine_extent[2]) {
             delete a;
             return fail(CN_ERR_INVALID_ARGUMENT, "cn_amr_create: block level, cells or origin out of range");
         }
@@ -240,7 +245,7 @@ cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const i
         for (int k = 0; k < span; ++k)
             for (int j = 0; j < span; ++j)
                 for (int i = 0; i < span; ++i) {
-                    int32_t &e = lookup[(B.ox / 8 + i) + (size_t)a->lres * ((B.oy / 8 + j) + (size_t)a->lres * (B.oz / 8 + k))];
+                    int32_t &e = lookup[(B.ox / 8 + i) + (size_t)a->lr[0] * ((B.oy / 8 + j) + (size_t)a->lr[1] * (B.oz / 8 + k))];
                     if (e != -1) {
                         delete a;
                         return fail(CN_ERR_INVALID_ARGUMENT, "cn_amr_create: blocks overlap");
@@ -272,6 +277,13 @@ cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const i
     }
     *out = a;
     return CN_OK;
+}
+
+cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const int *origin, int fine_extent,
+                        int ncomp, cn_dtype dtype, cn_amr **out)
+{
+    const int e[3] = {fine_extent, fine_extent, fine_extent};
+    return cn_amr_create_box(nblocks, level, cells, origin, e, ncomp, dtype, out);
 }
 
 cn_status cn_amr_destroy(cn_amr *a)

@@ -1,9 +1,10 @@
 // amr.cuh -- ghost cells of blocks on two refinement levels (ratio 2).
 //
-// A layout is a set of cubic blocks tiling a periodic box; each block has a
-// level (0 coarse, 1 fine; cell size 2 or 1 in level-1 units), n^3 cells and
-// an origin in level-1 cell units (multiples of 8).  A lookup grid with one
-// entry per 8^3 level-1 cells maps a position to the block that covers it.
+// A layout is a set of cubic blocks tiling a periodic box of Lx x Ly x Lz
+// level-1 cells; each block has a level (0 coarse, 1 fine; cell size 2 or 1
+// in level-1 units), n^3 cells and an origin in level-1 cell units (multiples
+// of 8).  A lookup grid with one entry per 8^3 level-1 cells maps a position
+// to the block that covers it.
 // A ghost cell of block b takes its value from the block s covering it:
 //   same level   copy of the cell;
 //   s coarser    trilinear prolongation from s (cell-centred weights 3/4, 1/4
@@ -32,9 +33,13 @@ struct BlockDev {
 
 struct Geom {
     const BlockDev *blk;
-    const int32_t *lookup; // lres^3 block ids
-    int L1;                // domain extent in level-1 cells (periodic)
-    int lres;              // L1 / 8
+    const int32_t *lookup; // lr[0] x lr[1] x lr[2] block ids
+    int L[3];              // domain extents in level-1 cells (periodic)
+    int lr[3];             // L / 8
+    __device__ __forceinline__ int block_at(int X, int Y, int Z) const
+    {
+        return lookup[(X >> 3) + lr[0] * ((Y >> 3) + lr[1] * (Z >> 3))];
+    }
 };
 
 __device__ __forceinline__ int wrap(int x, int L) { return x < 0 ? x + L : (x >= L ? x - L : x); }
@@ -53,8 +58,8 @@ __device__ __forceinline__ bool same_level_offset(const Geom &A, int b, int qx, 
 {
     const BlockDev B = A.blk[b];
     const int cs = B.level == 0 ? 2 : 1;
-    const int X = wrap(B.ox + qx * cs, A.L1), Y = wrap(B.oy + qy * cs, A.L1), Z = wrap(B.oz + qz * cs, A.L1);
-    const int s = A.lookup[(X >> 3) + A.lres * ((Y >> 3) + A.lres * (Z >> 3))];
+    const int X = wrap(B.ox + qx * cs, A.L[0]), Y = wrap(B.oy + qy * cs, A.L[1]), Z = wrap(B.oz + qz * cs, A.L[2]);
+    const int s = A.block_at(X, Y, Z);
     const BlockDev S = A.blk[s];
     if (S.level != B.level) return false;
     const int fx = (X - S.ox) / cs, fy = (Y - S.oy) / cs, fz = (Z - S.oz) / cs;
@@ -70,8 +75,8 @@ __device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, 
     if ((unsigned)qx < (unsigned)B.n && (unsigned)qy < (unsigned)B.n && (unsigned)qz < (unsigned)B.n)
         return cell<T>(comp, B, qx, qy, qz);
     const int cs = B.level == 0 ? 2 : 1;
-    const int X = wrap(B.ox + qx * cs, A.L1), Y = wrap(B.oy + qy * cs, A.L1), Z = wrap(B.oz + qz * cs, A.L1);
-    const int s = A.lookup[(X >> 3) + A.lres * ((Y >> 3) + A.lres * (Z >> 3))];
+    const int X = wrap(B.ox + qx * cs, A.L[0]), Y = wrap(B.oy + qy * cs, A.L[1]), Z = wrap(B.oz + qz * cs, A.L[2]);
+    const int s = A.block_at(X, Y, Z);
     const BlockDev S = A.blk[s];
     const int fx = X - S.ox, fy = Y - S.oy, fz = Z - S.oz; // level-1 units inside S
     if (S.level == B.level) {

@@ -153,63 +153,132 @@ def _global_to_blocks(g: Cartesian, arr, torch):
     torch.cuda.synchronize()
 
 
-def amr_layout(seed: int = 1, roots: int = 8, keep_root: float = 0.9, keep16: float = 0.8,
-               split16_in: float = 0.5, split32_in: float = 0.3, radius: float = 0.15,
-               centre=(0.5, 0.5, 0.5)):
-    """Two-level block layout of the periodic unit box by seeded octree splitting.
+def _pack(level, counts, slots, levels, cells, origins):
+    """Places blocks of each edge (level-1 cells; counts {edge: number}) in
+    descending size into free aligned cubic slots ({edge: [origins]}),
+    splitting a larger slot into its 8 octants when no slot of the edge is
+    left.  Returns False when a size finds no room."""
+    for e in sorted(counts, reverse=True):
+        for _ in range(counts[e]):
+            if not slots.get(e):
+                bigger = [k for k in slots if k > e and slots[k]]
+                if not bigger:
+                    return False
+                k = min(bigger)
+                while k > e:
+                    o = slots[k].pop(0)
+                    h = k // 2
+                    slots.setdefault(h, [])[:0] = [(o[0] + (q & 1) * h, o[1] + ((q >> 1) & 1) * h, o[2] + (q >> 2) * h)
+                                                   for q in range(8)]
+                    k = h
+            levels.append(level)
+            cells.append(e if level == 1 else e // 2)
+            origins.append(slots[e].pop(0))
+    return not any(slots.values())
 
-    The box is cut into roots^3 cubes of edge 1/roots; with F = 64 * roots
-    level-1 cells across the box, a cube of edge F/roots/2^k (level-1 cells)
-    becomes one block.  Outside a sphere (radius, centre) blocks are level 0
-    (cell = 2 level-1 cells): a root stays one 32^3 block with probability
-    keep_root, else its 16^3 children stay with probability keep16, else they
-    split into 8^3 blocks.  Inside the sphere blocks are level 1: 1/16-edge
-    cubes stay 32^3 blocks unless split (split16_in), 1/32-edge cubes stay
-    16^3 unless split (split32_in) into 8^3 blocks.  The defaults give 2045
-    blocks (55 % 8^3, 21 % 16^3, 24 % 32^3, 651 on level 1, 18.3 M cells).
-    Returns (levels, cells, origins, F)."""
-    rng = np.random.default_rng(seed)
-    F = 64 * roots
+
+def amr_layout(seed: int = 1, nblocks: int = 2048, probs=(0.5, 0.35, 0.15), refined=(0.03, 0.2),
+               max_tries: int = 100):
+    """The batched AMR layout: `nblocks` blocks whose cells per side are drawn
+    by seed from {8, 16, 32} with probabilities `probs`, on two levels (ratio
+    2), tiling a periodic box: a level-0 tiling refined to level 1 inside a
+    seeded ball.
+
+    A level-1 block of n cells spans n level-1 cells, a level-0 block 2n.  In
+    units of 8^3 level-1 cells every block's volume is a power of 8, i.e. 1
+    modulo 7, so blocks tile a box of volume V only if V = nblocks (mod 7); for
+    2048 blocks no cube qualifies (cubes are 0, 1 or 6 modulo 7).  The box is
+    therefore Px x Py x Pz cubes of 32 level-1 cells (volume 64 Px Py Pz
+    units) whose level-1 volume
+        V1 = (8 n8 + 64 n16 + 512 n32 - 64 Px Py Pz) / 7
+    is a fraction `refined` of the box; candidates are tried from the most
+    nearly cubic.  The refined region is the V1 / 8 cubes of 16 level-1 cells
+    nearest (periodically) to a seeded centre.  Level-1 blocks fill it exactly
+    (a_k of the k^3 blocks, a8 + 8 a16 + 64 a32 = V1, near the drawn size mix
+    but with enough 32^3 blocks that the level-0 32^3 blocks find whole
+    unrefined 64-cubes) and level-0 blocks fill the rest, each level packed by
+    _pack.  Draws (generator seeded with [seed, try]) that pack in no
+    candidate box are redrawn.  Defaults: 2048 blocks, about 13.5 M cells.
+    Returns (levels, cells, origins, (Lx, Ly, Lz))."""
+    for attempt in range(max_tries):
+        rng = np.random.default_rng([seed, attempt])
+        sizes = rng.choice(np.array([8, 16, 32]), size=nblocks, p=np.asarray(probs, float))
+        n8, n16, n32 = (int(np.sum(sizes == k)) for k in (8, 16, 32))
+        S = 8 * n8 + 64 * n16 + 512 * n32
+        boxes = []
+        for Px in range(2, 65):
+            for Py in range(2, Px + 1):
+                for Pz in range(2, Py + 1):
+                    P = Px * Py * Pz
+                    if S - 64 * P <= 0 or (S - 64 * P) % 56:
+                        continue
+                    V1 = (S - 64 * P) // 7
+                    if refined[0] <= V1 / (64 * P) <= refined[1]:
+                        boxes.append((Px / Pz, (Px % 2) + (Py % 2) + (Pz % 2), (Px, Py, Pz), V1))
+        centre_frac = rng.random(3)
+        for _, _, (Px, Py, Pz), V1 in sorted(boxes)[:40]:
+            out = _amr_fill(Px, Py, Pz, V1, n8, n16, n32, centre_frac)
+            if out is not None:
+                return out
+    raise RuntimeError("amr_layout: no draw tiles a box; change the seed or the refined fraction")
+
+
+def _amr_fill(Px, Py, Pz, V1, n8, n16, n32, centre_frac):
+    """One candidate box of amr_layout: refined region, level mix, packing.
+    Returns (levels, cells, origins, L) or None."""
+    G = (2 * Px, 2 * Py, 2 * Pz)  # 16-cubes per side
+    L = (32 * Px, 32 * Py, 32 * Pz)
+    K16 = V1 // 8
+    centre = centre_frac * np.array(L)
+    iz, iy, ix = np.meshgrid(*[np.arange(G[d]) for d in (2, 1, 0)], indexing="ij")
+    pos = np.stack([(ix + 0.5) * 16, (iy + 0.5) * 16, (iz + 0.5) * 16], -1).reshape(-1, 3) - centre
+    pos -= np.round(pos / np.array(L)) * np.array(L)
+    order = np.lexsort((np.arange(pos.shape[0]), np.sum(pos * pos, 1)))
+    ref = np.zeros(pos.shape[0], bool)
+    ref[order[:K16]] = True
+    ref = ref.reshape(G[2], G[1], G[0])  # [z, y, x] of 16-cubes
+    ref32 = ref.reshape(Pz, 2, Py, 2, Px, 2)
+    full32 = ref32.all(axis=(1, 3, 5))   # [z, y, x] of 32-cubes
+    free32 = ~ref32.any(axis=(1, 3, 5))
+    # level-1 slots: whole refined 32-cubes, then the other refined 16-cubes
+    s32 = [(32 * i, 32 * j, 32 * k) for k in range(Pz) for j in range(Py) for i in range(Px) if full32[k, j, i]]
+    s16 = [(16 * i, 16 * j, 16 * k) for k in range(G[2]) for j in range(G[1]) for i in range(G[0])
+           if ref[k, j, i] and not full32[k // 2, j // 2, i // 2]]
+    # level-0 slots: whole unrefined 64-cubes, other unrefined 32-cubes,
+    # unrefined 16-cubes of partly refined 32-cubes
+    in64 = np.zeros_like(free32)
+    s64 = []
+    for k in range(Pz // 2):
+        for j in range(Py // 2):
+            for i in range(Px // 2):
+                if free32[2 * k:2 * k + 2, 2 * j:2 * j + 2, 2 * i:2 * i + 2].all():
+                    s64.append((64 * i, 64 * j, 64 * k))
+                    in64[2 * k:2 * k + 2, 2 * j:2 * j + 2, 2 * i:2 * i + 2] = True
+    t32 = [(32 * i, 32 * j, 32 * k) for k in range(Pz) for j in range(Py) for i in range(Px)
+           if free32[k, j, i] and not in64[k, j, i]]
+    t16 = [(16 * i, 16 * j, 16 * k) for k in range(G[2]) for j in range(G[1]) for i in range(G[0])
+           if not ref[k, j, i] and not free32[k // 2, j // 2, i // 2]]
+    # level mix: near the drawn mix, enough level-1 32^3 blocks for the
+    # level-0 ones to fit the whole 64-cubes
+    x = V1 / (n8 + 8 * n16 + 64 * n32)
+    a32 = min(n32, len(s32), max(int(round(n32 * x)), n32 - len(s64)))
+    if n32 - a32 > len(s64):
+        return None
+    a16 = min(n16, int(round(n16 * x)))
+    a8 = V1 - 8 * a16 - 64 * a32
+    while a8 < 0 and a16 > 0:
+        a16, a8 = a16 - 1, a8 + 8
+    while a8 > n8 and a16 < n16:
+        a16, a8 = a16 + 1, a8 - 8
+    if not 0 <= a8 <= n8:
+        return None
     levels, cells, origins = [], [], []
-    c = np.array(centre)
-
-    def inside(o, s):
-        d = (np.array(o) + s / 2) / F - c
-        d -= np.round(d)
-        return np.linalg.norm(d) < radius
-
-    def leaf(level, n, o):
-        levels.append(level)
-        cells.append(n)
-        origins.append(o)
-
-    def rec(o, s):  # s: edge in level-1 cells
-        l1 = inside(o, s)
-        if s == 64:
-            if not l1 and rng.random() < keep_root:
-                return leaf(0, 32, o)
-        elif s == 32:
-            if l1:
-                if rng.random() > split16_in:
-                    return leaf(1, 32, o)
-            elif rng.random() < keep16:
-                return leaf(0, 16, o)
-        elif s == 16:
-            if not l1:
-                return leaf(0, 8, o)
-            if rng.random() > split32_in:
-                return leaf(1, 16, o)
-        else:
-            return leaf(1, 8, o)
-        h = s // 2
-        for k in range(8):
-            rec((o[0] + (k & 1) * h, o[1] + ((k >> 1) & 1) * h, o[2] + (k >> 2) * h), h)
-
-    for k in range(roots):
-        for j in range(roots):
-            for i in range(roots):
-                rec((64 * i, 64 * j, 64 * k), 64)
-    return np.array(levels), np.array(cells), np.array(origins), F
+    if not _pack(1, {32: a32, 16: a16, 8: a8}, {32: s32, 16: s16}, levels, cells, origins):
+        return None
+    if not _pack(0, {64: n32 - a32, 32: n16 - a16, 16: n8 - a8}, {64: s64, 32: t32, 16: t16}, levels, cells,
+                 origins):
+        return None
+    return np.array(levels), np.array(cells), np.array(origins), L
 
 
 def amr_small_layout(seed: int = 3):
@@ -242,11 +311,13 @@ def amr_small_layout(seed: int = 3):
 
 def euler_pulse_amr(U, seed: int = 1234, amp: float = 0.5, sigma: float = 0.1, noise: float = 1e-2,
                     gamma: float = 1.4, centre=(0.5, 0.5, 0.5)):
-    """The Euler pulse state on an AMR layout (periodic minimum-image distance)."""
+    """The Euler pulse state on an AMR layout (periodic minimum-image distance;
+    `centre` in fractions of the box, whose extents are U.box())."""
     import torch
     x, y, z = U.cell_centres()
-    d = [x - centre[0], y - centre[1], z - centre[2]]
-    r2 = sum((t - torch.round(t)) ** 2 for t in d)
+    box = U.box()
+    d = [x - centre[0] * box[0], y - centre[1] * box[1], z - centre[2] * box[2]]
+    r2 = sum((t - box[k] * torch.round(t / box[k])) ** 2 for k, t in enumerate(d))
     rho = 1.0 + amp * torch.exp(-r2 / (2 * sigma * sigma))
     gen = torch.Generator(device="cuda").manual_seed(seed)
     vel = [(torch.rand(rho.shape, generator=gen, device="cuda", dtype=torch.float64) * 2 - 1) * noise

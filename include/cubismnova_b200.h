@@ -353,6 +353,12 @@ cn_status cn_conv3_bf16(const void *in, void *out, const int nblocks[3], const i
 typedef struct cn_amr cn_amr;
 cn_status cn_amr_create(int nblocks, const int *level, const int *cells, const int *origin, int fine_extent,
                         int ncomp, cn_dtype dtype, cn_amr **out);
+/* The same on a periodic box of fine_extent[0] x [1] x [2] level-1 cells
+ * (each a multiple of 8); cells stay cubic, h = cell size / fine_extent[0]
+ * (the box is [0,1] x [0, Ly/Lx] x [0, Lz/Lx]).  cn_amr_create is the cubic
+ * case. */
+cn_status cn_amr_create_box(int nblocks, const int *level, const int *cells, const int *origin,
+                            const int fine_extent[3], int ncomp, cn_dtype dtype, cn_amr **out);
 cn_status cn_amr_destroy(cn_amr *a);
 cn_status cn_amr_info(const cn_amr *a, int64_t *total_cells, int64_t *comp_stride, int *nitems);
 cn_status cn_amr_block_offset(const cn_amr *a, int block, int64_t *offset);

@@ -396,14 +396,22 @@ AMR_BLOCK = np.dtype([("level", "<i4"), ("n", "<i4"), ("ox", "<i4"), ("oy", "<i4
                       ("pad", "<i4"), ("off", "<i8"), ("ih", "<f8")])
 
 
+def _extents(L1):
+    """Box extents (Lx, Ly, Lz) in level-1 cells from one extent or three."""
+    return (C.c_int * 3)(*[int(e) for e in np.broadcast_to(np.asarray(L1), (3,))])
+
+
 def amr_blocks(levels, cells, origins, L1):
-    """Oracle block table (offsets: blocks contiguous in block order)."""
+    """Oracle block table (offsets: blocks contiguous in block order); L1 is
+    the box extent in level-1 cells, one value (cube) or (Lx, Ly, Lz); cells
+    are cubic with h = cell size / Lx."""
     nb = len(levels)
     blk = np.zeros(nb, dtype=AMR_BLOCK)
     off = 0
+    lx = int(np.broadcast_to(np.asarray(L1), (3,))[0])
     for b in range(nb):
         cs = 2 if levels[b] == 0 else 1
-        blk[b] = (levels[b], cells[b], origins[b][0], origins[b][1], origins[b][2], 0, off, L1 / cs)
+        blk[b] = (levels[b], cells[b], origins[b][0], origins[b][1], origins[b][2], 0, off, lx / cs)
         off += cells[b] ** 3
     return blk, off
 
@@ -413,7 +421,7 @@ def amr_lab(comp, blk, L1, b, g):
     E = n + 2 * g
     lab = np.zeros((E, E, E))
     w = np.zeros((E, E, E), dtype=np.uint8)
-    rc = lib().or_amr_lab_f64(blk.ctypes.data_as(C.c_void_p), C.c_int(len(blk)), C.c_int(L1),
+    rc = lib().or_amr_lab_f64(blk.ctypes.data_as(C.c_void_p), C.c_int(len(blk)), _extents(L1),
                               _ptr(np.ascontiguousarray(comp, dtype=np.float64)), C.c_int(b), C.c_int(g),
                               _ptr(lab), _ptr(w))
     if rc:
@@ -424,7 +432,7 @@ def amr_lab(comp, blk, L1, b, g):
 def amr_stage(Us, Un, blk, L1, stage, dt, gamma):
     Us = np.ascontiguousarray(Us, dtype=np.float64)
     out = np.array(Un, copy=True) if (Un is not None and stage == 3) else np.zeros_like(Us)
-    rc = lib().or_amr_stage_f64(blk.ctypes.data_as(C.c_void_p), C.c_int(len(blk)), C.c_int(L1), _ptr(Us),
+    rc = lib().or_amr_stage_f64(blk.ctypes.data_as(C.c_void_p), C.c_int(len(blk)), _extents(L1), _ptr(Us),
                                 _ptr(np.ascontiguousarray(Un)) if Un is not None else None, _ptr(out),
                                 C.c_int64(Us.shape[-1]), C.c_int(stage), C.c_double(dt), C.c_double(gamma))
     if rc:

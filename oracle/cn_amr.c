@@ -9,8 +9,8 @@
  *   1/4 per direction (x, then y, then z), neighbour index clamped to the
  *   source block; finer source: ((c0+c1)+(c2+c3)) + ((c4+c5)+(c6+c7)) times
  *   1/8, child c = dx | dy<<1 | dz<<2.
- * Positions are in level-1 cell units on a periodic box of L1 cells; a block
- * of level l has cell size 2 - l.
+ * Positions are in level-1 cell units on a periodic box of L[0] x L[1] x L[2]
+ * cells; a block of level l has cell size 2 - l.
  */
 #include "cn_euler_math.h"
 #include "cn_oracle.h"
@@ -32,33 +32,33 @@ static double cellv(const double *c, const or_amr_block *B, int x, int y, int z)
     return c[B->off + x + (int64_t)B->n * (y + (int64_t)B->n * z)];
 }
 
-static int *build_lookup(const or_amr_block *blk, int nblocks, int L1)
+static int *build_lookup(const or_amr_block *blk, int nblocks, const int *L)
 {
-    const int lres = L1 / 8;
-    int *lk = (int *)malloc(sizeof(int) * lres * lres * lres);
+    const int lx = L[0] / 8, ly = L[1] / 8, lz = L[2] / 8;
+    int *lk = (int *)malloc(sizeof(int) * (size_t)lx * ly * lz);
     if (!lk)
         return NULL;
-    for (int i = 0; i < lres * lres * lres; ++i)
+    for (size_t i = 0; i < (size_t)lx * ly * lz; ++i)
         lk[i] = -1;
     for (int b = 0; b < nblocks; ++b) {
         const int cs = blk[b].level == 0 ? 2 : 1, span = blk[b].n * cs / 8;
         for (int k = 0; k < span; ++k)
             for (int j = 0; j < span; ++j)
                 for (int i = 0; i < span; ++i)
-                    lk[(blk[b].ox / 8 + i) + lres * ((blk[b].oy / 8 + j) + lres * (blk[b].oz / 8 + k))] = b;
+                    lk[(blk[b].ox / 8 + i) + lx * ((blk[b].oy / 8 + j) + ly * (blk[b].oz / 8 + k))] = b;
     }
     return lk;
 }
 
-static double amr_value(const double *comp, const or_amr_block *blk, const int *lk, int L1, int b, int qx,
+static double amr_value(const double *comp, const or_amr_block *blk, const int *lk, const int *L, int b, int qx,
                         int qy, int qz)
 {
     const or_amr_block *B = &blk[b];
     if (qx >= 0 && qx < B->n && qy >= 0 && qy < B->n && qz >= 0 && qz < B->n)
         return cellv(comp, B, qx, qy, qz);
-    const int lres = L1 / 8, cs = B->level == 0 ? 2 : 1;
-    const int X = wrapi(B->ox + qx * cs, L1), Y = wrapi(B->oy + qy * cs, L1), Z = wrapi(B->oz + qz * cs, L1);
-    const or_amr_block *S = &blk[lk[(X >> 3) + lres * ((Y >> 3) + lres * (Z >> 3))]];
+    const int lx = L[0] / 8, ly = L[1] / 8, cs = B->level == 0 ? 2 : 1;
+    const int X = wrapi(B->ox + qx * cs, L[0]), Y = wrapi(B->oy + qy * cs, L[1]), Z = wrapi(B->oz + qz * cs, L[2]);
+    const or_amr_block *S = &blk[lk[(X >> 3) + lx * ((Y >> 3) + ly * (Z >> 3))]];
     const int fx = X - S->ox, fy = Y - S->oy, fz = Z - S->oz;
     if (S->level == B->level) {
         const int css = S->level == 0 ? 2 : 1;
@@ -88,10 +88,10 @@ static double amr_value(const double *comp, const or_amr_block *blk, const int *
 }
 
 /* dense lab (n+2g)^3 of block b, face ghosts only; written[] marks defined cells */
-int or_amr_lab_f64(const or_amr_block *blk, int nblocks, int L1, const double *comp, int b, int g, double *lab,
-                   uint8_t *written)
+int or_amr_lab_f64(const or_amr_block *blk, int nblocks, const int *L, const double *comp, int b, int g,
+                   double *lab, uint8_t *written)
 {
-    int *lk = build_lookup(blk, nblocks, L1);
+    int *lk = build_lookup(blk, nblocks, L);
     if (!lk)
         return 2;
     const int n = blk[b].n, E = n + 2 * g;
@@ -102,7 +102,7 @@ int or_amr_lab_f64(const or_amr_block *blk, int nblocks, int L1, const double *c
                 const int out = (x < 0 || x >= n) + (y < 0 || y >= n) + (z < 0 || z >= n);
                 written[i] = out <= 1;
                 if (out <= 1)
-                    lab[i] = amr_value(comp, blk, lk, L1, b, x, y, z);
+                    lab[i] = amr_value(comp, blk, lk, L, b, x, y, z);
             }
     free(lk);
     return 0;
@@ -110,10 +110,10 @@ int or_amr_lab_f64(const or_amr_block *blk, int nblocks, int L1, const double *c
 
 /* Euler RHS (stage 0) / SSP-RK3 stage on all AMR blocks, FP64, periodic box;
  * face loops and stage update of cn_euler.c with each block's own 1/h. */
-int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double *Us, const double *Un,
+int or_amr_stage_f64(const or_amr_block *blk, int nblocks, const int *L, const double *Us, const double *Un,
                      double *out, int64_t cstride, int stage, double dt, double gamma)
 {
-    int *lk = build_lookup(blk, nblocks, L1);
+    int *lk = build_lookup(blk, nblocks, L);
     if (!lk)
         return 2;
     const double gm1 = gamma - 1.0, igm1 = 1.0 / (gamma - 1.0);
@@ -138,7 +138,7 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, int L1, const double 
                             continue;
                         double u[5], W[5];
                         for (int c = 0; c < 5; ++c)
-                            u[c] = amr_value(Us + c * cstride, blk, lk, L1, b, x, y, z);
+                            u[c] = amr_value(Us + c * cstride, blk, lk, L, b, x, y, z);
                         prim_f64(u[0], u[1], u[2], u[3], u[4], gm1, W);
                         const size_t li = (x + 3) + (size_t)L * ((y + 3) + (size_t)L * (z + 3));
                         for (int c = 0; c < 5; ++c)
