@@ -110,10 +110,10 @@ int or_amr_lab_f64(const or_amr_block *blk, int nblocks, const int *L, const dou
 
 /* Euler RHS (stage 0) / SSP-RK3 stage on all AMR blocks, FP64, periodic box;
  * face loops and stage update of cn_euler.c with each block's own 1/h. */
-int or_amr_stage_f64(const or_amr_block *blk, int nblocks, const int *L, const double *Us, const double *Un,
+int or_amr_stage_f64(const or_amr_block *blk, int nblocks, const int *ext, const double *Us, const double *Un,
                      double *out, int64_t cstride, int stage, double dt, double gamma)
 {
-    int *lk = build_lookup(blk, nblocks, L);
+    int *lk = build_lookup(blk, nblocks, ext);
     if (!lk)
         return 2;
     const double gm1 = gamma - 1.0, igm1 = 1.0 / (gamma - 1.0);
@@ -138,7 +138,7 @@ int or_amr_stage_f64(const or_amr_block *blk, int nblocks, const int *L, const d
                             continue;
                         double u[5], W[5];
                         for (int c = 0; c < 5; ++c)
-                            u[c] = amr_value(Us + c * cstride, blk, lk, L, b, x, y, z);
+                            u[c] = amr_value(Us + c * cstride, blk, lk, ext, b, x, y, z);
                         prim_f64(u[0], u[1], u[2], u[3], u[4], gm1, W);
                         const size_t li = (x + 3) + (size_t)L * ((y + 3) + (size_t)L * (z + 3));
                         for (int c = 0; c < 5; ++c)

@@ -53,3 +53,15 @@ def test_oracle_block_table_on_the_layout(oracle_lib):
     blk, tot = oracle_lib.amr_blocks(l, c, o, L)
     assert tot == int(np.sum(c.astype(np.int64) ** 3))
     assert np.all(blk["ih"] == np.where(l == 0, L[0] / 2, L[0]))
+
+
+def test_oracle_stage_on_a_box_keeps_a_uniform_state(oracle_lib):
+    """The oracle's AMR stage on a small rectangular layout (40 blocks): a
+    uniform state with exactly representable values has a zero RHS."""
+    l, c, o, L = W.amr_layout(1, nblocks=40)
+    blk, tot = oracle_lib.amr_blocks(l, c, o, L)
+    U = np.empty((5, tot))
+    for k, v in enumerate((1.0, 0.5, -0.25, 0.0, 2.5)):
+        U[k] = v
+    R = oracle_lib.amr_stage(U, None, blk, L, 0, 0.0, 1.4)
+    assert np.count_nonzero(R) == 0
