@@ -367,10 +367,7 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
         T WL[5], WR[5];
         line_face(W, id, i < 2, carry, WL, WR);
         T Fl[5];
-        if constexpr (sizeof(T) == 4)
-            rusanov2(WL, WR, D, gamma, igm1, Fl);
-        else
-            rusanov<T>(WL, WR, D, gamma, igm1, Fl);
+        rusanov<T>(WL, WR, D, gamma, igm1, Fl);
         if (i == 0) {
             if (run > 0) {
 #pragma unroll
