@@ -58,6 +58,21 @@ __device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gsrc, uint3
                  : "memory");
 }
 
+// 5-D tiled TMA load global -> shared (tensor map `tmap`, a generic address
+// of a CUtensorMap in parameter, constant or global memory): the map's box
+// at coordinates c0..c4 (innermost first, all non-negative, c0 x element
+// size a multiple of 16 bytes) lands densely at smem_dst (128-byte aligned);
+// completion on `bar`.  No multicast.
+__device__ __forceinline__ void tma_load_5d(void *smem_dst, const void *tmap, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                 "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(smem_dst)),
+                 "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+                 "r"(smem_u32(bar))
+                 : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t done;

@@ -15,30 +15,56 @@
 // accumulates FP64 conservation sums per CTA (reduced in a fixed order by a
 // second kernel, so the sums are deterministic).
 //
+// The tile's cells of all five components arrive in shared memory by one TMA
+// copy (a 5-D tensor map over the state, cuTensorMapEncodeTiled) while the
+// threads stage the halo slabs; they are then converted to primitives.
+//
 // Shared memory per CTA: 5 x 1024 primitives (the tile plus one direction's
 // halo slabs, restaged before each sweep; FP32 keeps all three directions'
-// slabs) + 5 x 704 accumulators and exchanged face fluxes.
+// slabs) + 5 x 704 accumulators and exchanged face fluxes (the TMA landing
+// area of the tile's conservative cells before the sweeps).
 #include "cn_internal.h"
 #include "cn_tma.cuh"
 #include "euler_math.cuh"
 #include "euler_stage.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cstring>
 #include <mutex>
 
 namespace cn {
 namespace euler {
 
+// Dynamic shared memory, from its first 128-byte aligned address: W
+// [5][Stg<T>::SV], then A [5][NACC] from a 128-byte aligned offset (the TMA
+// destination of the tile's cells); 128 bytes of slack for the alignment.
+template <typename T> constexpr size_t acc_offset()
+{
+    return (5 * Stg<T>::SV * sizeof(T) + 127) / 128 * 128;
+}
+template <typename T> constexpr size_t stage_smem()
+{
+    return 128 + acc_offset<T>() + 5 * NACC * sizeof(T);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 3) stage_kernel(StageParams<T> p, CartSrc src)
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 3)
+    stage_kernel(StageParams<T> p, CartSrc src, const __grid_constant__ CUtensorMap core)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    T *W = reinterpret_cast<T *>(smem_raw); // [5][Stg<T>::SV]
-    T *A = W + 5 * Stg<T>::SV;              // [5][NACC]
+    unsigned char *base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    T *W = reinterpret_cast<T *>(base);                    // [5][Stg<T>::SV]
+    T *A = reinterpret_cast<T *>(base + acc_offset<T>()); // [5][NACC]
     __shared__ double red[NT / 32][5];
     __shared__ int snb[29];
     __shared__ TileInfo<T> ts;
-    stage_tile<T>(p, src, blockIdx.x, blockIdx.x, W, A, red, snb, &ts);
+    __shared__ __align__(8) uint64_t core_bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&core_bar, 1);
+        fence_mbar_init();
+    }
+    stage_tile<T, CartSrc, true>(p, src, blockIdx.x, blockIdx.x, W, A, red, snb, &ts, &core, &core_bar);
 }
 
 // Fixed-order reduction of per-CTA partials: out[c] = sum_i partials[i][c].
@@ -114,6 +140,41 @@ static bool same_shape(const cn_grid *a, const cn_grid *b)
            a->n[2] == b->n[2] && a->dtype == b->dtype && a->block_stride == b->block_stride;
 }
 
+// Tensor map of the five components cs..cs+4 of grid g as the 5-D array
+// [comp][block][z][y][x] (innermost first: x, y, z, block, comp), box
+// 8 x 8 x 8 x 1 x 5: one TMA copy brings a tile's cells of all components.
+// Strides are byte multiples of 16 (block storage is padded to 32 bytes).
+static cn_status core_map(const cn_grid *g, int cs, size_t es, CUtensorMap *m)
+{
+    void *base = static_cast<char *>(g->d_data) + (size_t)cs * g->comp_stride * es;
+    const cuuint64_t dims[5] = {(cuuint64_t)g->n[0], (cuuint64_t)g->n[1], (cuuint64_t)g->n[2],
+                                (cuuint64_t)g->nblocks, 5};
+    const cuuint64_t strides[4] = {(cuuint64_t)g->n[0] * es, (cuuint64_t)g->n[0] * g->n[1] * es,
+                                   (cuuint64_t)g->block_stride * es, (cuuint64_t)g->comp_stride * es};
+    const cuuint32_t box[5] = {TB, TB, TB, 1, 5};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    for (int i = 0; i < 4; ++i)
+        if (strides[i] % 16) return fail(CN_ERR_UNSUPPORTED, "Euler stage: grid strides are not 16-byte multiples");
+    // the driver's encoder through the runtime's entry-point query (the
+    // library does not link the driver library itself)
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!encode) return fail(CN_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const CUresult r = encode(
+        m, es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base, dims, strides, box,
+        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(CN_ERR_CUDA, "cuTensorMapEncodeTiled failed for the Euler tile map");
+    return CN_OK;
+}
+
 template <typename T>
 static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, int cn_,
                               cn_grid *out, int co, int stage, double dt, double gamma,
@@ -142,12 +203,15 @@ static cn_status launch_stage(cn_grid *bcsrc, cn_grid *Us, int cs, cn_grid *Un, 
     p.stage = stage;
     p.partials = partials;
     p.err = Us->d_err;
-    const size_t smem = (size_t)(5 * Stg<T>::SV + 5 * NACC) * sizeof(T);
+    CUtensorMap core;
+    r = core_map(Us, cs, sizeof(T), &core);
+    if (r != CN_OK) return r;
+    const size_t smem = stage_smem<T>();
     static DeviceOnce attr_once; // per device (the first call on a device is an eager one)
     r = smem_opt_in(attr_once, stage_kernel<T>, smem);
     if (r != CN_OK) return r;
     const int64_t ctas = (int64_t)Us->nblocks * (Us->n[0] / TB) * (Us->n[1] / TB) * (Us->n[2] / TB);
-    stage_kernel<T><<<(unsigned)ctas, NT, smem, st>>>(p, src);
+    stage_kernel<T><<<(unsigned)ctas, NT, smem, st>>>(p, src, core);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }

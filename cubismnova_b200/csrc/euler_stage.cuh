@@ -7,6 +7,7 @@
 #pragma once
 
 #include "cn_internal.h"
+#include "cn_tma.cuh"
 #include "euler_math.cuh"
 
 namespace cn {
@@ -461,9 +462,15 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
 // The whole stage for one tile: staging, three sweeps, RK epilogue and the
 // tile's FP64 sums (written to p.partials[slot] if requested).  Uses
 // W [5][Stg<T>::SV], A [5][NACC] and red [NT/32][5] in shared memory.
-template <typename T, typename Src>
+// With CORE_TMA, `core_map` (a tensor map over the five components of U as
+// [comp][block][z][y][x], box 8 x 8 x 8 x 1 x 5) brings the tile's cells by
+// one TMA copy into A, which is free until the sweeps; `core_bar`
+// (initialised with count 1, used once per CTA: parity 0) signals its
+// completion.  Without it each thread loads its cells.
+template <typename T, typename Src, bool CORE_TMA = false>
 __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &src, int item, int slot, T *W, T *A,
-                                           double (*red)[5], int *snb, TileInfo<T> *ts)
+                                           double (*red)[5], int *snb, TileInfo<T> *ts,
+                                           const void *core_map = nullptr, uint64_t *core_bar = nullptr)
 {
     // the tile's geometry is kept in shared memory (ts) and re-read after each
     // barrier, so it does not occupy registers across the three sweeps
@@ -478,7 +485,44 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
     __syncthreads(); // snb
     // ---- stage the tile's cells as primitives (the halo slot follows per
     // sweep): all of a thread's loads are issued before any conversion
-    {
+    auto convert_core = [&](T (&u)[CPT][5]) {
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int i = threadIdx.x + k * NT;
+            if (i < NCORE) {
+                T w[5];
+                to_primitive<T>(u[k][0], u[k][1], u[k][2], u[k][3], u[k][4], p.gm1, w);
+                const int e = core_sm(i % TB, (i / TB) % TB, i / (TB * TB));
+#pragma unroll
+                for (int c = 0; c < 5; ++c)
+                    prim(W, c, e) = w[c];
+            }
+        }
+    };
+    if constexpr (CORE_TMA) {
+        // one copy brings the tile's cells of all five components, dense
+        // [5][8][8][8] in A; converted before the halo staging (converting
+        // after it keeps both sets of values live and spills)
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(core_bar, 5u * NCORE * (uint32_t)sizeof(T));
+            tma_load_5d(A, core_map, t.x0, t.y0, t.z0, t.block, 0, core_bar);
+        }
+        if (!mbar_wait_bounded_sleep(core_bar, 0, 100)) {
+            // record the error, then give the copy a second bounded wait so
+            // that it is not left writing into this CTA's shared memory
+            if (p.err) atomicExch(p.err, kDevErrTimeout);
+            mbar_wait_bounded_sleep(core_bar, 0, 100);
+        }
+        T u[CPT][5];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int i = threadIdx.x + k * NT;
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                u[k][c] = i < NCORE ? A[c * NCORE + i] : T(0);
+        }
+        convert_core(u);
+    } else {
         T u[CPT][5];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
@@ -492,18 +536,7 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
                     u[k][c] = p.U[c][o];
             }
         }
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int i = threadIdx.x + k * NT;
-            if (i < NCORE) {
-                T w[5];
-                to_primitive<T>(u[k][0], u[k][1], u[k][2], u[k][3], u[k][4], p.gm1, w);
-                const int e = core_sm(i % TB, (i / TB) % TB, i / (TB * TB));
-#pragma unroll
-                for (int c = 0; c < 5; ++c)
-                    prim(W, c, e) = w[c];
-            }
-        }
+        convert_core(u);
     }
     if (Stg<T>::all) {
 #pragma unroll 1
