@@ -890,19 +890,28 @@ cn_status cn_mg_collect_patches(cn_mg *m, const cn_grid *f, int cycles, int per_
 
 // Smoother selection: nn == NULL restores weighted Jacobi everywhere; else the
 // network replaces Jacobi on the levels whose bit is set in level_mask.
-cn_status cn_mg_set_smoother(cn_mg *m, cn_nn *nn, unsigned level_mask)
+cn_status cn_mg_set_smoother_phases(cn_mg *m, cn_nn *nn, unsigned pre_mask, unsigned post_mask, int pre_apps,
+                                    int post_apps)
 {
     if (!m) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
     m->nn = nn;
-    m->nn_levels = nn ? level_mask : 0;
+    m->nn_levels = nn ? pre_mask : 0;
+    m->nn_post_levels = nn ? post_mask : 0;
+    m->nn_pre_apps = pre_apps;
+    m->nn_post_apps = post_apps;
     if (nn) {
         for (int l = 0; l < m->nlevels - 1; ++l)
-            if ((level_mask >> l) & 1) {
+            if (((pre_mask | post_mask) >> l) & 1) {
                 cn_status s = level_bufs(m, l);
                 if (s != CN_OK) return s;
             }
     }
     return CN_OK;
+}
+
+cn_status cn_mg_set_smoother(cn_mg *m, cn_nn *nn, unsigned level_mask)
+{
+    return cn_mg_set_smoother_phases(m, nn, level_mask, level_mask, -1, -1);
 }
 
 } // extern "C"

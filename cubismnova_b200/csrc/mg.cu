@@ -710,16 +710,23 @@ static cn_status coarsest(cn_mg *m, int l, cudaStream_t st)
 }
 
 
-static cn_status smooth_any(cn_mg *m, int l, int sweeps, bool zero_guess, cudaStream_t st)
+// pre-smoothing (post = false, from a zero guess) or post-smoothing of level
+// l: the learned smoother where its level masks select it, else Jacobi
+static cn_status smooth_any(cn_mg *m, int l, bool post, cudaStream_t st)
 {
-    if (m->nn && ((m->nn_levels >> l) & 1)) return nn_smooth(m, l, sweeps, zero_guess, st);
-    return smooth(m, l, sweeps, zero_guess, st);
+    const int sweeps = post ? m->nu2 : m->nu1;
+    const unsigned mask = post ? m->nn_post_levels : m->nn_levels;
+    if (m->nn && ((mask >> l) & 1)) {
+        const int apps = post ? m->nn_post_apps : m->nn_pre_apps;
+        return nn_smooth(m, l, apps >= 0 ? apps : sweeps, !post, st);
+    }
+    return smooth(m, l, sweeps, !post, st);
 }
 
 cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
 {
     if (l == m->nlevels - 1) return coarsest(m, l, st);
-    cn_status s = smooth_any(m, l, m->nu1, true, st);
+    cn_status s = smooth_any(m, l, false, st);
     if (s != CN_OK) return s;
     KArgs a = kargs(m, l);
     const LabGeom Lc = make_geom(m->p[l + 1], &kS1);
@@ -738,7 +745,7 @@ cn_status vcycle(cn_mg *m, int l, cudaStream_t st)
         s = m->capture(m, st);
         if (s != CN_OK) return s;
     }
-    return smooth_any(m, l, m->nu2, false, st);
+    return smooth_any(m, l, true, st);
 }
 
 // Inverse of the regularised coarsest operator (see coarsest_dense_kernel),

@@ -27,7 +27,9 @@ struct cn_mg {
     // learned smoother: network, the levels it replaces Jacobi on (bit l),
     // and per-level work grids (features, hidden activations, output)
     cn_nn *nn = nullptr;
-    unsigned nn_levels = 0;
+    unsigned nn_levels = 0;      // pre-smoothing levels (bit l)
+    unsigned nn_post_levels = 0; // post-smoothing levels (bit l)
+    int nn_pre_apps = -1, nn_post_apps = -1; // applications per smoothing (-1: nu1 / nu2)
     std::vector<cn_grid *> nn_bufs; // 4 per level: X (2 comps), H1 (16), H2 (16), Y (1)
     std::vector<void *> nn_act;     // 2 per level: BF16 channels-last activations (tensor-core path)
     // optional hook run at the finest level after the coarse-grid correction

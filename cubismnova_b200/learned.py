@@ -22,6 +22,7 @@ _lib.register({
     "cn_nn_train": (_I, [_P, _P, _P, _P, _I, _I, _D, _I, _I, _D, C.c_uint64, C.POINTER(C.c_double), _P]),
     "cn_mg_collect_patches": (_I, [_P, _P, _I, _I, C.c_uint64, _P, _P, _P, _I, C.POINTER(_I), _P]),
     "cn_mg_set_smoother": (_I, [_P, _P, C.c_uint]),
+    "cn_mg_set_smoother_phases": (_I, [_P, _P, C.c_uint, C.c_uint, _I, _I]),
     "cn_nn_set_inference": (_I, [_P, _I]),
     "cn_conv3_bf16": (_I, [_P, _P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P, _I, _P]),
 })
@@ -130,7 +131,15 @@ def conv3_bf16(x, nblocks, block_cells, weights, relu: bool = False, stream=None
     return out
 
 
-def use_in(mg, smoother, level_mask: int = 0xFFFF):
+def use_in(mg, smoother, level_mask: int = 0xFFFF, post_mask=None, pre_apps: int = -1, post_apps: int = -1):
     """Replace Jacobi by the learned smoother on the levels in level_mask
-    (smoother None: back to Jacobi everywhere)."""
-    _lib.check(_lib.lib().cn_mg_set_smoother(mg.handle, smoother.handle if smoother else None, level_mask))
+    (pre- and post-smoothing; with post_mask, level_mask selects the
+    pre-smoothing levels and post_mask the post-smoothing ones), with
+    pre_apps / post_apps applications (-1: the solver's nu1 / nu2); smoother
+    None: back to Jacobi everywhere."""
+    h = smoother.handle if smoother else None
+    if post_mask is None and pre_apps < 0 and post_apps < 0:
+        _lib.check(_lib.lib().cn_mg_set_smoother(mg.handle, h, level_mask))
+    else:
+        pm = level_mask if post_mask is None else post_mask
+        _lib.check(_lib.lib().cn_mg_set_smoother_phases(mg.handle, h, level_mask, pm, pre_apps, post_apps))

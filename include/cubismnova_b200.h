@@ -328,6 +328,12 @@ cn_status cn_mg_collect_patches(cn_mg *m, const cn_grid *f, int cycles, int per_
 /* Use the network instead of Jacobi on the levels set in level_mask (bit l);
  * nn == NULL restores Jacobi everywhere. */
 cn_status cn_mg_set_smoother(cn_mg *m, cn_nn *nn, unsigned level_mask);
+/* The same per smoothing phase: the network pre-smooths the levels in
+ * pre_mask and post-smooths those in post_mask, with pre_apps / post_apps
+ * applications (-1: nu1 / nu2 of cn_mg_create); Jacobi elsewhere.
+ * cn_mg_set_smoother(m, nn, mask) is (mask, mask, -1, -1). */
+cn_status cn_mg_set_smoother_phases(cn_mg *m, cn_nn *nn, unsigned pre_mask, unsigned post_mask, int pre_apps,
+                                    int post_apps);
 /* Grid inference precision: 1 (default) = BF16 activations and weights on
  * the tensor cores (tcgen05, FP32 accumulation) on levels whose block cells
  * are multiples of (16, 16, 4), else FP32; 0 = FP32 on the CUDA cores. */
