@@ -350,21 +350,28 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
     };
     // left-biased state of cell f0-1, the lower cell of the run's first face
     typename CarryOf<T>::type carry;
-    {
-        int id[5];
+    // shared entries of the stencil cells a-2 .. a+2.  FP32 shifts the window
+    // by one cell per face (one new entry); FP64 recomputes it (its registers
+    // are the scarcer resource)
+    int id[5];
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
-            id[k] = sidx(f0 - 3 + k);
-        line_left(W, id, carry);
-    }
+    for (int k = 0; k < 5; ++k)
+        id[k] = sidx(f0 - 3 + k);
+    line_left(W, id, carry);
     T Fq[5]; // flux of the previous face of the run
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
         const int a = f0 + i; // face a: cells a-1 (left state carried in VL) and a
-        int id[5];
+        if constexpr (sizeof(T) == 4) {
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
-            id[k] = sidx(a - 2 + k);
+            for (int k = 0; k < 4; ++k)
+                id[k] = id[k + 1];
+            id[4] = sidx(a + 2);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+                id[k] = sidx(a - 2 + k);
+        }
         T WL[5], WR[5];
         line_face(W, id, i < 2, carry, WL, WR);
         T Fl[5];
