@@ -43,6 +43,10 @@ struct Geom {
 };
 
 __device__ __forceinline__ int wrap(int x, int L) { return x < 0 ? x + L : (x >= L ? x - L : x); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ int clampi(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
 template <typename T>
@@ -93,14 +97,16 @@ __device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, 
         const T e010 = cell<T>(comp, S, px, qy1, pz), e110 = cell<T>(comp, S, qx1, qy1, pz);
         const T e001 = cell<T>(comp, S, px, py, qz1), e101 = cell<T>(comp, S, qx1, py, qz1);
         const T e011 = cell<T>(comp, S, px, qy1, qz1), e111 = cell<T>(comp, S, qx1, qy1, qz1);
+        // weights 3/4, 1/4 per direction; products and sums rounded one by
+        // one (never contracted, whatever the compiler's FMA setting)
         const T a = T(0.75), c = T(0.25);
-        const T a0 = a * e000 + c * e100;
-        const T a1 = a * e010 + c * e110;
-        const T a2 = a * e001 + c * e101;
-        const T a3 = a * e011 + c * e111;
-        const T b0 = a * a0 + c * a1;
-        const T b1 = a * a2 + c * a3;
-        return a * b0 + c * b1;
+        const T a0 = add_rn(mul_rn(a, e000), mul_rn(c, e100));
+        const T a1 = add_rn(mul_rn(a, e010), mul_rn(c, e110));
+        const T a2 = add_rn(mul_rn(a, e001), mul_rn(c, e101));
+        const T a3 = add_rn(mul_rn(a, e011), mul_rn(c, e111));
+        const T b0 = add_rn(mul_rn(a, a0), mul_rn(c, a1));
+        const T b1 = add_rn(mul_rn(a, a2), mul_rn(c, a3));
+        return add_rn(mul_rn(a, b0), mul_rn(c, b1));
     }
     // coarse ghost cell over a fine block: mean of its 8 children
     T v[8];
