@@ -742,8 +742,11 @@ static cn_status features(cn_mg *m, int l, const float *p, const float *f, float
     return CN_OK;
 }
 
-// Tensor-core inference: features (FP32) -> three tcgen05 convolution
-// layers, the last fused with the update of p.
+// Grid inference with the hidden layer on the tensor cores: features (FP32)
+// -> first layer on the CUDA cores (2 -> 16, BF16 out) -> hidden layer on the
+// tensor cores (tcgen05, 16 -> 16) -> last layer on the CUDA cores fused with
+// the update of p.  (The first and last layers' 2 input / 1 output channels
+// would be padded to 16 on the tensor cores.)
 static cn_status nn_smooth_tc(cn_mg *m, int l, int apps, bool zero_guess, cudaStream_t st)
 {
     cn_grid *P = m->p[l], *X = m->nn_bufs[4 * l];
@@ -752,22 +755,20 @@ static cn_status nn_smooth_tc(cn_mg *m, int l, int apps, bool zero_guess, cudaSt
     for (int i = 0; i < 2; ++i)
         if (!m->nn_act[2 * l + i]) CN_CUDA_TRY(cudaMalloc(&m->nn_act[2 * l + i], abytes));
     cn_nn *nn = m->nn;
-    if (!nn->wpack) CN_CUDA_TRY(cudaMalloc(&nn->wpack, 3 * nntc::kPackedWeightBytes));
-    uint16_t *w1 = nn->wpack, *w2 = w1 + nntc::kPackedWeightBytes / 2, *w3 = w2 + nntc::kPackedWeightBytes / 2;
+    if (!nn->wpack) CN_CUDA_TRY(cudaMalloc(&nn->wpack, nntc::kPackedWeightBytes));
+    uint16_t *w2 = nn->wpack;
     cn_status s;
-    if ((s = nntc::pack_weights(nn->w, CI, CH, w1, st)) != CN_OK) return s;
     if ((s = nntc::pack_weights(nn->w + NW1, CH, CH, w2, st)) != CN_OK) return s;
-    if ((s = nntc::pack_weights(nn->w + NW1 + NW2, CH, 1, w3, st)) != CN_OK) return s;
     uint16_t *h1 = static_cast<uint16_t *>(m->nn_act[2 * l]), *h2 = static_cast<uint16_t *>(m->nn_act[2 * l + 1]);
     const float *x = reinterpret_cast<const float *>(X->d_data);
     for (int a = 0; a < apps; ++a) {
         const bool zg = zero_guess && a == 0;
-        // features -> packed BF16 in h2 -> layer 1 -> h1 -> layer 2 -> h2 -> layer 3 + update
-        if ((s = features(m, l, zg ? nullptr : fptr(P), fptr(m->f[l]), nullptr, st, h2)) != CN_OK) return s;
-        if ((s = nntc::conv_hidden(h2, P->nb, P->n, w1, 1, h1, P->d_err, st)) != CN_OK) return s;
+        if ((s = features(m, l, zg ? nullptr : fptr(P), fptr(m->f[l]), nullptr, st)) != CN_OK) return s;
+        if ((s = nntc::conv_first_cc(x, x + X->comp_stride, X->block_stride, P->nb, P->n, nn->w, h1, st)) != CN_OK)
+            return s;
         if ((s = nntc::conv_hidden(h1, P->nb, P->n, w2, 1, h2, P->d_err, st)) != CN_OK) return s;
-        if ((s = nntc::conv_update(h2, P->nb, P->n, w3, x, X->block_stride, fptr(P), P->block_stride,
-                                   (float)nn->omega, zg ? 1 : 0, P->d_err, st)) != CN_OK)
+        if ((s = nntc::conv_update_cc(h2, P->nb, P->n, nn->w + NW1 + NW2, x, X->block_stride, fptr(P),
+                                      P->block_stride, (float)nn->omega, zg ? 1 : 0, st)) != CN_OK)
             return s;
     }
     return CN_OK;

@@ -24,6 +24,14 @@ cn_status conv_hidden(const uint16_t *act, const int nb[3], const int n[3], cons
 // last layer (output channel 0) fused with p = (zero_guess ? 0 : p) + (omega x0 + y)
 cn_status conv_update(const uint16_t *act, const int nb[3], const int n[3], const uint16_t *w, const float *x0,
                       int64_t xbs, float *p, int64_t pbs, float omega, int zero_guess, int *err, cudaStream_t st);
+// CUDA-core forms of the first and last layers (learned_cc.cu): the first
+// layer from the FP32 features (x0, x1; block stride xbs) to 16 BF16
+// channels with ReLU; the last from 16 BF16 channels to the update of p.
+// Weights FP32 [27][cin][cout].
+cn_status conv_first_cc(const float *x0, const float *x1, int64_t xbs, const int nb[3], const int n[3],
+                        const float *W1, uint16_t *out, cudaStream_t st);
+cn_status conv_update_cc(const uint16_t *act, const int nb[3], const int n[3], const float *W3, const float *x0,
+                         int64_t xbs, float *p, int64_t pbs, float omega, int zero_guess, cudaStream_t st);
 
 } // namespace nntc
 } // namespace cn
