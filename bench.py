@@ -320,7 +320,7 @@ class Euler:
     # DRAM bytes per cell per step of the three stage launches from one ncu
     # capture on 8x8x4 blocks of 32^3 (8.4 M cells, inputs 5x larger than L2),
     # scaled to the workload's cells: traffic grows with the cells processed
-    traffic_per_cell_step = 343.11
+    traffic_per_cell_step = 327.80
     traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 3 stage_kernel launches "
                       "of one step on 8x8x4 blocks of 32^3, per cell, scaled by the workload's cells")
     sample_nb = (4, 4, 4)  # CPU sample grid: 64 blocks of the same block size
@@ -512,7 +512,7 @@ class C4(Euler):
     bytes_per_cell_step = (80 + 120 + 120) // 2
     # capture on 8x8x4 blocks (168 MB of state, comparable to L2, so slightly
     # under the full-size figure)
-    traffic_per_cell_step = 157.70
+    traffic_per_cell_step = 156.84
 
 
 class C3:
