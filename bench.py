@@ -516,6 +516,7 @@ class C4(Euler):
 
 
 class C3:
+    autotune = True  # bench.py --no-autotune: the default schedule (profiling runs)
     """Batched two-level AMR step: 2048 blocks whose sizes are drawn by seed
     from {8^3: 50 %, 16^3: 35 %, 32^3: 15 %} (workloads.amr_layout: about
     13.5 M cells, a level-0 tiling refined in a seeded ball), level-interface
@@ -550,9 +551,12 @@ class C3:
         self.nb, self.n = (len(l),), tuple(int(e) for e in F)
         # CFL on the fine level (h = 1/Lx), sound speed of the pulse state < 1.3
         self.dt = 0.3 / (3 * 1.3 * F[0])
-        order, ctas, ms = cn.amr.autotune(self.U, self.w1, self.w2, self.dt, reps=2)
-        self.schedule = dict(order=["block order", "largest blocks first", "Morton"][order], ctas=ctas,
-                             ms_per_step=round(ms, 3))
+        if self.autotune:
+            order, ctas, ms = cn.amr.autotune(self.U, self.w1, self.w2, self.dt, reps=2)
+            self.schedule = dict(order=["block order", "largest blocks first", "Morton"][order], ctas=ctas,
+                                 ms_per_step=round(ms, 3))
+        else:
+            self.schedule = dict(order="largest blocks first", ctas=0, autotuned=False)
         cn.workloads.euler_pulse_amr(self.U)
         self.stream = torch.cuda.Stream()
         cn.amr.rk3_step(self.U, self.w1, self.w2, self.dt, stream=self.stream)  # eager once before capture
@@ -1088,6 +1092,8 @@ def run_ours(args, world, rank, local, pg):
     if args.blocks:
         cls = type(cls.__name__, (cls,), {"nb": tuple(args.blocks),
                                           "desc": cls.desc + f" [reduced: {tuple(args.blocks)} blocks]"})
+    if getattr(args, "no_autotune", False) and hasattr(cls, "autotune"):
+        cls = type(cls.__name__, (cls,), {"autotune": False})
     W = cls()
     stream = torch.cuda.Stream()
     peaks = measured_peaks()
@@ -1306,6 +1312,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-learned", action="store_true",
                     help="c5: skip training and timing the learned smoother")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="c3: keep the default schedule instead of autotuning it (profiling runs)")
     ap.add_argument("--blocks", type=int, nargs=3, default=None,
                     help="override the block counts (reduced grids for profiling runs)")
     ap.add_argument("--accuracy", action="store_true",
