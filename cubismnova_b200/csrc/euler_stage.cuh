@@ -359,7 +359,8 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
         id[k] = sidx(f0 - 3 + k);
     line_left(W, id, carry);
     T Fq[5]; // flux of the previous face of the run
-    auto face = [&](int i) {
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
         const int a = f0 + i; // face a: cells a-1 (left state carried in VL) and a
         if constexpr (sizeof(T) == 4) {
 #pragma unroll
@@ -393,18 +394,6 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
 #pragma unroll
         for (int c = 0; c < 5; ++c)
             Fq[c] = Fl[c];
-    };
-    // FP32 unrolls the run's three faces (the instruction stream has room in
-    // the caches and the registers suffice); FP64 keeps one copy (unrolled it
-    // spills about 0.7 KB per thread)
-    if constexpr (sizeof(T) == 4) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-            face(i);
-    } else {
-#pragma unroll 1
-        for (int i = 0; i < 3; ++i)
-            face(i);
     }
     __syncthreads(); // X
     if (run < 2) {
