@@ -458,6 +458,11 @@ struct cn_nn {
     // allows, 0 = FP32 CUDA cores; packed BF16 weights of the three layers
     int inference = 1;
     uint16_t *wpack = nullptr;
+    // training: 1 = hidden layer on the tensor cores with BF16 channels-last
+    // activations (learned_train_tc.cu), 0 = FP32 CUDA cores throughout
+    int training = 1;
+    uint16_t *bh1 = nullptr, *bh2 = nullptr, *bgh1 = nullptr, *bgh2 = nullptr, *bw = nullptr;
+    int *d_err = nullptr; // device error word of the tensor-core training kernels
 };
 
 static constexpr int NW1 = 27 * CI * CH, NW2 = 27 * CH * CH, NW3 = 27 * CH;
@@ -470,19 +475,45 @@ static unsigned nblk(int64_t n)
     return (unsigned)(b < 1 ? 1 : b);
 }
 
-static cn_status nn_work(cn_nn *nn, int B, int P)
+static void free_work(cn_nn *nn)
 {
-    if (nn->wB >= B && nn->wP == P) return CN_OK;
     float *bufs[] = {nn->h1, nn->h2, nn->y, nn->c, nn->res, nn->gc, nn->gh2, nn->gh1};
     for (float *b : bufs)
         if (b) cudaFree(b);
+    uint16_t *hb[] = {nn->bh1, nn->bh2, nn->bgh1, nn->bgh2};
+    for (uint16_t *b : hb)
+        if (b) cudaFree(b);
     if (nn->sums) cudaFree(nn->sums);
+    nn->h1 = nn->h2 = nn->y = nn->c = nn->res = nn->gc = nn->gh2 = nn->gh1 = nullptr;
+    nn->bh1 = nn->bh2 = nn->bgh1 = nn->bgh2 = nullptr;
+    nn->sums = nullptr;
+    nn->wB = nn->wP = 0;
+}
+
+// work buffers for batches of B patches of P^3 cells in the current training mode
+static cn_status nn_work(cn_nn *nn, int B, int P)
+{
+    const bool have = nn->training == 1 ? nn->bh1 != nullptr : nn->h1 != nullptr;
+    if (nn->wB >= B && nn->wP == P && have) return CN_OK;
+    free_work(nn);
     const int64_t s6 = (int64_t)(P + 6) * (P + 6) * (P + 6), s4 = (int64_t)(P + 4) * (P + 4) * (P + 4),
                   s2 = (int64_t)(P + 2) * (P + 2) * (P + 2), s0 = (int64_t)P * P * P;
-    CN_CUDA_TRY(cudaMalloc(&nn->h1, sizeof(float) * B * CH * s6));
-    CN_CUDA_TRY(cudaMalloc(&nn->gh1, sizeof(float) * B * CH * s6));
-    CN_CUDA_TRY(cudaMalloc(&nn->h2, sizeof(float) * B * CH * s4));
-    CN_CUDA_TRY(cudaMalloc(&nn->gh2, sizeof(float) * B * CH * s4));
+    if (nn->training == 1) {
+        CN_CUDA_TRY(cudaMalloc(&nn->bh1, sizeof(uint16_t) * B * CH * s6));
+        CN_CUDA_TRY(cudaMalloc(&nn->bgh1, sizeof(uint16_t) * B * CH * s6));
+        CN_CUDA_TRY(cudaMalloc(&nn->bh2, sizeof(uint16_t) * B * CH * s4));
+        CN_CUDA_TRY(cudaMalloc(&nn->bgh2, sizeof(uint16_t) * B * CH * s4));
+        if (!nn->bw) CN_CUDA_TRY(cudaMalloc(&nn->bw, 2 * nntc::kPackedWeightBytes));
+        if (!nn->d_err) {
+            CN_CUDA_TRY(cudaMalloc(&nn->d_err, sizeof(int)));
+            CN_CUDA_TRY(cudaMemset(nn->d_err, 0, sizeof(int)));
+        }
+    } else {
+        CN_CUDA_TRY(cudaMalloc(&nn->h1, sizeof(float) * B * CH * s6));
+        CN_CUDA_TRY(cudaMalloc(&nn->gh1, sizeof(float) * B * CH * s6));
+        CN_CUDA_TRY(cudaMalloc(&nn->h2, sizeof(float) * B * CH * s4));
+        CN_CUDA_TRY(cudaMalloc(&nn->gh2, sizeof(float) * B * CH * s4));
+    }
     CN_CUDA_TRY(cudaMalloc(&nn->y, sizeof(float) * B * s2));
     CN_CUDA_TRY(cudaMalloc(&nn->c, sizeof(float) * B * s2));
     CN_CUDA_TRY(cudaMalloc(&nn->gc, sizeof(float) * B * s2));
@@ -491,6 +522,19 @@ static cn_status nn_work(cn_nn *nn, int B, int P)
     nn->wB = B;
     nn->wP = P;
     return CN_OK;
+}
+
+// the tensor-core training kernels' error word (set when a bounded wait ran
+// out); read after a synchronisation, cleared when set
+static cn_status nn_check_error(cn_nn *nn)
+{
+    if (!nn->d_err) return CN_OK;
+    int e = 0;
+    CN_CUDA_TRY(cudaMemcpy(&e, nn->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e == 0) return CN_OK;
+    CN_CUDA_TRY(cudaMemset(nn->d_err, 0, sizeof(int)));
+    return fail(CN_ERR_DEVICE, "learned smoother training: a tensor-core kernel gave up waiting (error word " +
+                                    std::to_string(e) + ")");
 }
 
 template <int Cin, int Cout, bool RELU>
@@ -553,14 +597,23 @@ cn_status cn_nn_set_inference(cn_nn *nn, int mode)
     return CN_OK;
 }
 
+cn_status cn_nn_set_training(cn_nn *nn, int mode)
+{
+    if (!nn || mode < 0 || mode > 1) return fail(CN_ERR_INVALID_ARGUMENT, "cn_nn_set_training: bad argument");
+    nn->training = mode;
+    return CN_OK;
+}
+
 cn_status cn_nn_destroy(cn_nn *nn)
 {
     if (!nn) return CN_OK;
-    float *bufs[] = {nn->w, nn->m, nn->v, nn->g, nn->h1, nn->h2, nn->y, nn->c, nn->res, nn->gc, nn->gh2, nn->gh1};
+    free_work(nn);
+    float *bufs[] = {nn->w, nn->m, nn->v, nn->g};
     for (float *b : bufs)
         if (b) cudaFree(b);
-    if (nn->sums) cudaFree(nn->sums);
     if (nn->wpack) cudaFree(nn->wpack);
+    if (nn->bw) cudaFree(nn->bw);
+    if (nn->d_err) cudaFree(nn->d_err);
     delete nn;
     return CN_OK;
 }
@@ -593,24 +646,35 @@ cn_status cn_nn_loss_grad(cn_nn *nn, const float *x, const float *k, const float
     if (s != CN_OK) return s;
     const float *W1 = nn->w, *W2 = nn->w + NW1, *W3 = nn->w + NW1 + NW2;
     const int S = P + 8;
-    fwd_patch<CI, CH, true>(x, W1, nn->h1, B, S, st);
-    fwd_patch<CH, CH, true>(nn->h1, W2, nn->h2, B, S - 2, st);
-    fwd_patch<CH, 1, false>(nn->h2, W3, nn->y, B, S - 4, st);
+    const nntc::TrainBufs T = {nn->bh1,  nn->bh2, nn->bgh1, nn->bgh2, nn->bw, nn->bw + nntc::kPackedWeightBytes / 2,
+                               nn->y,    nn->gc,  nn->d_err};
+    if (nn->training == 1) {
+        if ((s = nntc::train_forward_tc(T, x, nn->w, B, P, st)) != CN_OK) return s;
+    } else {
+        fwd_patch<CI, CH, true>(x, W1, nn->h1, B, S, st);
+        fwd_patch<CH, CH, true>(nn->h1, W2, nn->h2, B, S - 2, st);
+        fwd_patch<CH, 1, false>(nn->h2, W3, nn->y, B, S - 4, st);
+    }
     const int64_t s2 = (int64_t)(P + 2) * (P + 2) * (P + 2), s0 = (int64_t)P * P * P;
     loss_fwd<<<nblk(B * s2), 256, 0, st>>>(x, nn->y, (float)nn->omega, B, P, nn->c);
     CN_CUDA_TRY(cudaMemsetAsync(nn->sums, 0, sizeof(double) * 2 * B, st));
     loss_res<<<nblk(B * s0), 256, 0, st>>>(nn->c, k, r, (float)ih2, B, P, nn->res, nn->sums);
     loss_adjoint<<<nblk(B * s2), 256, 0, st>>>(nn->res, k, nn->sums, (float)ih2, B, P, nn->gc);
-    CN_CUDA_TRY(cudaMemsetAsync(nn->g, 0, sizeof(float) * NWT, st));
-    bwd_patch<CH, 1>(nn->h2, nn->gc, W3, nn->h2, nn->gh2, nn->g + NW1 + NW2, B, S - 4, st);
-    bwd_patch<CH, CH>(nn->h1, nn->gh2, W2, nn->h1, nn->gh1, nn->g + NW1, B, S - 2, st);
-    bwd_patch<CI, CH>(x, nn->gh1, W1, nullptr, nullptr, nn->g, B, S, st);
+    if (nn->training == 1) {
+        if ((s = nntc::train_backward_tc(T, x, nn->w, nn->g, B, P, st)) != CN_OK) return s;
+    } else {
+        CN_CUDA_TRY(cudaMemsetAsync(nn->g, 0, sizeof(float) * NWT, st));
+        bwd_patch<CH, 1>(nn->h2, nn->gc, W3, nn->h2, nn->gh2, nn->g + NW1 + NW2, B, S - 4, st);
+        bwd_patch<CH, CH>(nn->h1, nn->gh2, W2, nn->h1, nn->gh1, nn->g + NW1, B, S - 2, st);
+        bwd_patch<CI, CH>(x, nn->gh1, W1, nullptr, nullptr, nn->g, B, S, st);
+    }
     CN_CUDA_TRY(cudaGetLastError());
     if (grad_out) CN_CUDA_TRY(cudaMemcpyAsync(grad_out, nn->g, sizeof(float) * NWT, cudaMemcpyDefault, st));
     if (loss) {
         std::vector<double> h(2 * B);
         CN_CUDA_TRY(cudaMemcpyAsync(h.data(), nn->sums, sizeof(double) * 2 * B, cudaMemcpyDeviceToHost, st));
         CN_CUDA_TRY(cudaStreamSynchronize(st));
+        if ((s = nn_check_error(nn)) != CN_OK) return s;
         double l = 0;
         for (int b = 0; b < B; ++b) l += h[2 * b] > 0 ? h[2 * b + 1] / h[2 * b] : 0.0;
         *loss = l / B;
@@ -669,6 +733,7 @@ cn_status cn_nn_train(cn_nn *nn, const float *x, const float *k, const float *r,
         ep_loss /= (nb > 0 ? nb : 1);
     }
     cudaStreamSynchronize(st);
+    if (s == CN_OK) s = nn_check_error(nn);
     cudaFree(bx);
     cudaFree(bk);
     cudaFree(br);

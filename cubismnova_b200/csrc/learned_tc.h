@@ -33,5 +33,21 @@ cn_status conv_first_cc(const float *x0, const float *x1, int64_t xbs, const int
 cn_status conv_update_cc(const uint16_t *act, const int nb[3], const int n[3], const float *W3, const float *x0,
                          int64_t xbs, float *p, int64_t pbs, float omega, int zero_guess, cudaStream_t st);
 
+
+// Training with the hidden layer on the tensor cores (learned_train_tc.cu):
+// batches of B patches, x [B][2][(P+8)^3] FP32, weights W and gradients gW
+// FP32 [W1 | W2 | W3].  The forward writes y [B][(P+2)^3]; the backward
+// reads gc = d loss / d y and writes gW.
+struct TrainBufs {
+    uint16_t *h1, *h2;     // BF16 channels-last activations [B][(P+6)^3][16], [B][(P+4)^3][16]
+    uint16_t *gh1, *gh2;   // their gradients (ReLU-masked)
+    uint16_t *wfwd, *wbwd; // packed hidden-layer B tiles: forward, backward-data (kPackedWeightBytes each)
+    float *y, *gc;         // the last layer's output and its gradient [B][(P+2)^3]
+    int *err;              // device error word (bounded waits that ran out)
+};
+cn_status train_forward_tc(const TrainBufs &T, const float *x, const float *W, int B, int P, cudaStream_t st);
+cn_status train_backward_tc(const TrainBufs &T, const float *x, const float *W, float *gW, int B, int P,
+                            cudaStream_t st);
+
 } // namespace nntc
 } // namespace cn

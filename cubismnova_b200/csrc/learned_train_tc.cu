@@ -1,0 +1,554 @@
+// learned_train_tc.cu -- training of the learned smoother with its hidden
+// layer (16 -> 16 channels, 84 % of the network's multiply-adds) on the
+// tensor cores (tcgen05, BF16 operands, FP32 accumulation in tensor memory),
+// and the first and last layers on the CUDA cores, all on BF16 channels-last
+// activations (32 bytes per cell).
+//
+// Patches are cubes: the input x has side S = P + 8, the activations h1 side
+// S1 = S - 2, h2 side S2 = S - 4, the output y side S3 = S - 6 (valid 3x3x3
+// convolutions; tap d = (dx, dy, dz) in {0,1,2}^3, index dx + 3 dy + 9 dz).
+//
+// The three GEMMs of the hidden layer share one operand form.  A chunk of
+// 128 consecutive output cells (linear over batch and cube) gathers, for
+// every tap t and channel half h, a plane of 128 rows x 16 bytes: row r =
+// channels 8h..8h+7 of the source cell (cell r) + d(t) + shift, zero outside
+// the source cube.  Each row is one 16-byte asynchronous copy (cp.async) of
+// channels-last data, so no transposition is needed:
+//   forward        out[q][co] = sum_{t,ci} h1[q + d][ci] W[t][ci][co]
+//                  A = plane pair (t, 0..1) read K-major (M = 128 cells, K =
+//                  16 channels: the two planes are the two 8-channel K
+//                  chunks), B = W[t] (N = 16 output channels); 27 MMAs.
+//   backward-data  gin[c][ci] = sum_e gout[c - 2 + e][co] W[26 - e][ci][co],
+//                  the same with the source gout, shift -2, taps flipped and
+//                  W transposed; the ReLU mask of the layer's input applied
+//                  in the epilogue.
+//   weight grad    gW[t][ci][co] = sum_q h1[q + d][ci] gout[q][co]: the
+//                  forward's planes read MN-major (M = (tap, channel), 8 taps
+//                  = 16 planes per M = 128 tile, planes one SBO apart; K =
+//                  cells, 16 rows per MMA), B = the chunk's gout rows
+//                  MN-major (N = 16 channels); 4 tiles x 8 MMAs per chunk,
+//                  accumulated over all chunks of a CTA in tensor memory and
+//                  added to gW with atomics at the end.  Rows of taps >= 27 in
+//                  the last tile read whatever the buffer holds; those
+//                  accumulator rows are never read.
+// Taps are gathered in 4 groups of 8 into two 32 KB buffers: the MMAs of one
+// group (issued by one thread, committed to the buffer's mbarrier) overlap
+// the gather of the next.  Persistent CTAs, two per SM; every wait bounded
+// (an error word is set and the CTA stops issuing).
+#include "cn_internal.h"
+#include "cn_tc.cuh"
+#include "cn_tma.cuh"
+#include "learned_tc.h"
+
+#include <cuda_bf16.h>
+
+namespace cn {
+namespace nntr {
+
+constexpr int ROWS = 128;                        // cells per chunk
+constexpr int GT = 8;                            // taps per gather group
+constexpr int NG = 4;                            // groups per chunk (taps 0-7, 8-15, 16-23, 24-26)
+constexpr uint32_t PL = ROWS * 16;               // bytes of one plane
+constexpr uint32_t GBUF = 2 * GT * PL;           // one group buffer: 16 planes, 32 KB
+constexpr int NT = ROWS;                         // thread r owns row r
+constexpr uint32_t WBYTES = 27 * 512;            // packed weights of one layer
+constexpr uint32_t GOUT_BYTES = 2 * PL;          // weight gradient: gout rows of a chunk (2 planes)
+constexpr size_t OFF_W = 2 * (size_t)GBUF;       // weights (forward / backward-data) or gout buffers
+constexpr size_t OFF_BAR = OFF_W + (WBYTES > 2 * GOUT_BYTES ? WBYTES : 2 * GOUT_BYTES);
+constexpr size_t SMEM = OFF_BAR + 4 * 8 + 16;
+constexpr uint32_t IDESC_K = tc::idesc_bf16_f32(128, 16);
+// both operands MN-major (bits 15 and 16)
+constexpr uint32_t IDESC_MN = tc::idesc_bf16_f32(128, 16) | (1u << 15) | (1u << 16);
+
+enum { FWD = 0, BWD = 1, WGRAD = 2 };
+
+struct Args {
+    const uint16_t *src;  // gathered activations [B][Sin^3][16] BF16
+    const uint16_t *gout; // weight gradient: [B][Sout^3][16] gradient at the layer's output
+    const uint16_t *act;  // backward-data: the layer's input at the output cells (ReLU mask)
+    const uint16_t *w;    // forward / backward-data: packed B tiles [27][2][16][8]
+    uint16_t *out;        // forward / backward-data: [B][Sout^3][16]
+    float *gw;            // weight gradient: [27][16][16] FP32, accumulated
+    int Sin, Sout, shift;
+    int relu;
+    int64_t total;        // B * Sout^3
+    int64_t chunks;       // ceil(total / ROWS)
+    int *err;
+};
+
+__device__ __forceinline__ uint16_t bf16_bits(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
+
+// 16-byte asynchronous copy; src_bytes 0 writes zeros (nothing is read)
+__device__ __forceinline__ void cp16(void *dst, const void *src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__ Args a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *Abuf = smem;                 // [2][16 planes][ROWS][16 B]
+    unsigned char *Wb = smem + OFF_W;           // forward / backward-data weights; weight gradient: [2][2][ROWS][16 B]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OFF_BAR);
+    uint64_t *empty = bars, *dready = bars + 2; // empty[2]: group buffer free; dready: accumulator complete
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 4);
+    int *flag = reinterpret_cast<int *>(slot + 1); // [0]: buffer waits, [1]: accumulator waits
+    constexpr uint32_t TCOLS = MODE == WGRAD ? 64 : 32;
+    const int r = threadIdx.x, warp = r >> 5;
+
+    if (r == 0) {
+        mbar_init(empty, 1);
+        mbar_init(empty + 1, 1);
+        mbar_init(dready, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(slot, TCOLS);
+        tc::tmem_relinquish();
+    }
+    if (MODE != WGRAD)
+        for (int i = r; i < (int)(WBYTES / 16); i += NT)
+            reinterpret_cast<uint4 *>(Wb)[i] = __ldg(reinterpret_cast<const uint4 *>(a.w) + i);
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *slot;
+
+    const int64_t so3 = (int64_t)a.Sout * a.Sout * a.Sout, si3 = (int64_t)a.Sin * a.Sin * a.Sin;
+    int it = 0, nch = 0;
+    bool ok = true;
+    for (int64_t c = blockIdx.x; c < a.chunks && ok; c += gridDim.x, ++nch) {
+        // ---- this thread's row: output cell L
+        const int64_t L = c * ROWS + r;
+        const bool valid = L < a.total;
+        int64_t bq = 0, rem = 0;
+        int x = 0, y = 0, z = 0;
+        if (valid) {
+            bq = L / so3;
+            rem = L - bq * so3;
+            x = (int)(rem % a.Sout);
+            y = (int)((rem / a.Sout) % a.Sout);
+            z = (int)(rem / ((int64_t)a.Sout * a.Sout));
+        }
+        unsigned char *G = Wb + (nch & 1) * GOUT_BYTES;
+        for (int g = 0; g < NG; ++g, ++it) {
+            const int buf = it & 1;
+            // ---- the buffer's previous MMAs (item it - 2) must be done
+            if (it >= 2) {
+                if (r == 0) flag[0] = mbar_wait_bounded(empty + buf, ((it >> 1) - 1) & 1) ? 1 : 0;
+                __syncthreads();
+                if (!flag[0]) {
+                    ok = false;
+                    break;
+                }
+            }
+            unsigned char *A = Abuf + buf * GBUF;
+            if (MODE == WGRAD && g == 0) {
+                // the chunk's gradient rows (the buffer of chunk nch - 2 is free: its MMAs precede item it - 2)
+                const uint16_t *s = a.gout + (valid ? L : 0) * 16;
+                cp16(G + r * 16, s, valid ? 16u : 0u);
+                cp16(G + PL + r * 16, s + 8, valid ? 16u : 0u);
+            }
+#pragma unroll
+            for (int tl = 0; tl < GT; ++tl) {
+                const int t = g * GT + tl;
+                if (t < 27) {
+                    const int sx = x + t % 3 + a.shift, sy = y + (t / 3) % 3 + a.shift, sz = z + t / 9 + a.shift;
+                    const bool in = valid && (unsigned)sx < (unsigned)a.Sin && (unsigned)sy < (unsigned)a.Sin &&
+                                    (unsigned)sz < (unsigned)a.Sin;
+                    const int64_t e = in ? bq * si3 + sx + (int64_t)a.Sin * (sy + (int64_t)a.Sin * sz) : 0;
+                    const uint16_t *s = a.src + e * 16;
+                    cp16(A + (2 * tl) * PL + r * 16, s, in ? 16u : 0u);
+                    cp16(A + (2 * tl + 1) * PL + r * 16, s + 8, in ? 16u : 0u);
+                }
+            }
+            asm volatile("cp.async.wait_all;" ::: "memory");
+            fence_proxy_async_smem(); // generic-proxy smem writes -> visible to the tensor cores
+            tc::fence_before_sync();
+            __syncthreads();
+            if (r == 0) {
+                tc::fence_after_sync();
+                if (MODE == WGRAD) {
+#pragma unroll
+                    for (int ks = 0; ks < ROWS / 16; ++ks) {
+                        const uint64_t da = tc::smem_desc(smem_u32(A) + 256u * ks, 128u, PL);
+                        const uint64_t db = tc::smem_desc(smem_u32(G) + 256u * ks, 128u, PL);
+                        tc::mma_bf16(tbase + 16u * g, da, db, IDESC_MN, (nch > 0 || ks > 0) ? 1u : 0u);
+                    }
+                } else {
+#pragma unroll
+                    for (int tl = 0; tl < GT; ++tl) {
+                        const int t = g * GT + tl;
+                        if (t < 27) {
+                            const uint64_t da = tc::smem_desc(smem_u32(A) + 2u * tl * PL, PL, 128u);
+                            const uint64_t db = tc::smem_desc(smem_u32(Wb) + 512u * t, 256u, 128u);
+                            tc::mma_bf16(tbase, da, db, IDESC_K, t > 0 ? 1u : 0u);
+                        }
+                    }
+                }
+                tc::mma_commit(empty + buf);
+                if (MODE != WGRAD && g == NG - 1) tc::mma_commit(dready);
+            }
+        }
+        if (!ok) break;
+        if (MODE != WGRAD) {
+            // ---- epilogue: thread r drains accumulator row r (TMEM lane r)
+            if (r == 0) flag[1] = mbar_wait_bounded(dready, nch & 1) ? 1 : 0;
+            __syncthreads();
+            if (!flag[1]) {
+                ok = false;
+                break;
+            }
+            tc::fence_after_sync();
+            float v[16];
+            tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16), v);
+            tc::fence_before_sync();
+            if (valid) {
+                uint32_t h[8];
+                if (MODE == BWD) {
+                    const uint4 *m = reinterpret_cast<const uint4 *>(a.act + L * 16);
+                    const uint4 m0 = m[0], m1 = m[1];
+                    const uint32_t mw[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        // BF16 = the top 16 bits of an FP32: > 0 test on the widened value
+                        const float lo = __uint_as_float(mw[j] << 16), hi = __uint_as_float(mw[j] & 0xFFFF0000u);
+                        h[j] = (uint32_t)bf16_bits(lo > 0.f ? v[2 * j] : 0.f) |
+                               ((uint32_t)bf16_bits(hi > 0.f ? v[2 * j + 1] : 0.f) << 16);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        float p = v[2 * j], q = v[2 * j + 1];
+                        if (a.relu) {
+                            p = fmaxf(p, 0.f);
+                            q = fmaxf(q, 0.f);
+                        }
+                        h[j] = (uint32_t)bf16_bits(p) | ((uint32_t)bf16_bits(q) << 16);
+                    }
+                }
+                uint4 *dst = reinterpret_cast<uint4 *>(a.out + L * 16);
+                dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+            }
+        }
+    }
+    // ---- weight gradient: wait for every MMA of this CTA, then add the
+    // 4 accumulator tiles (row m = 16 (tap - 8 g) + ci, column co) to gW
+    if (MODE == WGRAD && ok && nch > 0) {
+        if (r == 0) {
+            tc::mma_commit(dready);
+            flag[1] = mbar_wait_bounded(dready, 0) ? 1 : 0;
+        }
+        __syncthreads();
+        ok = flag[1] != 0;
+        if (ok) {
+            tc::fence_after_sync();
+#pragma unroll 1
+            for (int g = 0; g < NG; ++g) {
+                float v[16];
+                tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + 16u * g, v);
+                const int t = g * GT + r / 16, ci = r % 16;
+                if (t < 27) {
+#pragma unroll
+                    for (int co = 0; co < 16; ++co) atomicAdd(a.gw + (t * 16 + ci) * 16 + co, v[co]);
+                }
+            }
+        }
+    }
+    if (!ok && r == 0 && a.err) atomicExch(a.err, kDevErrTimeout);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, TCOLS);
+}
+
+// backward-data B tiles: tap e, K = the layer's output channel co, N = its
+// input channel ci: B[e][kc][ci][8] = W[26 - e][ci][kc * 8 + j]
+__global__ void pack_bwd_kernel(const float *W, uint16_t *out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 27 * 256) return;
+    const int e = i / 256, rr = i % 256;
+    const int kc = rr / 128, ci = (rr / 8) % 16, j = rr % 8;
+    out[i] = bf16_bits(W[((26 - e) * 16 + ci) * 16 + kc * 8 + j]);
+}
+
+// ---------------------------------------------------- CUDA-core layers
+// layer 1 forward: x [B][2][S^3] FP32 -> h1 [B][(S-2)^3][16] BF16, ReLU
+__global__ void __launch_bounds__(128) l1_fwd_cl(const float *__restrict__ x, const float *__restrict__ W1,
+                                                  uint16_t *__restrict__ h1, int B, int S)
+{
+    __shared__ __align__(16) float sw[27 * 2 * 16];
+    for (int i = threadIdx.x; i < 27 * 32; i += blockDim.x) sw[i] = W1[i];
+    __syncthreads();
+    const int So = S - 2;
+    const int64_t per = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = per * B;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(q / per);
+        const int64_t c = q - b * per;
+        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
+        const float *x0 = x + (int64_t)b * 2 * s3, *x1 = x0 + s3;
+        float acc[16];
+#pragma unroll
+        for (int o = 0; o < 16; ++o) acc[o] = 0.f;
+#pragma unroll 1
+        for (int t = 0; t < 27; ++t) {
+            const int64_t e = (xx + t % 3) + (int64_t)S * ((yy + (t / 3) % 3) + (int64_t)S * (zz + t / 9));
+            const float v0 = __ldg(x0 + e), v1 = __ldg(x1 + e);
+            const float *w = sw + t * 32;
+#pragma unroll
+            for (int o = 0; o < 16; ++o) acc[o] = fmaf(v0, w[o], fmaf(v1, w[16 + o], acc[o]));
+        }
+        uint32_t h[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            h[j] = (uint32_t)bf16_bits(fmaxf(acc[2 * j], 0.f)) | ((uint32_t)bf16_bits(fmaxf(acc[2 * j + 1], 0.f)) << 16);
+        uint4 *dst = reinterpret_cast<uint4 *>(h1 + q * 16);
+        dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
+}
+
+__device__ __forceinline__ void unpack16(const uint16_t *p, float (&v)[16])
+{
+    const uint4 *s = reinterpret_cast<const uint4 *>(p);
+    const uint4 a = __ldg(s), b = __ldg(s + 1);
+    const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        v[2 * j] = __uint_as_float(w[j] << 16);
+        v[2 * j + 1] = __uint_as_float(w[j] & 0xFFFF0000u);
+    }
+}
+
+// layer 3 forward: h2 [B][S^3][16] BF16 -> y [B][(S-2)^3] FP32
+__global__ void __launch_bounds__(128) l3_fwd_cl(const uint16_t *__restrict__ h2, const float *__restrict__ W3,
+                                                  float *__restrict__ y, int B, int S)
+{
+    __shared__ __align__(16) float sw[27 * 16];
+    for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) sw[i] = W3[i];
+    __syncthreads();
+    const int So = S - 2;
+    const int64_t per = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = per * B;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(q / per);
+        const int64_t c = q - b * per;
+        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
+        float acc = 0.f;
+#pragma unroll 1
+        for (int t = 0; t < 27; ++t) {
+            const int64_t e = (xx + t % 3) + (int64_t)S * ((yy + (t / 3) % 3) + (int64_t)S * (zz + t / 9));
+            float v[16];
+            unpack16(h2 + ((int64_t)b * s3 + e) * 16, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc = fmaf(v[i], sw[t * 16 + i], acc);
+        }
+        y[q] = acc;
+    }
+}
+
+// layer 3 backward-data: gh2[c][ci] = (h2[c][ci] > 0) sum_e gc[c - 2 + e] W3[26 - e][ci]
+// for c in S^3 (gc on (S-2)^3, zero outside)
+__global__ void __launch_bounds__(128) l3_bwd_data_cl(const float *__restrict__ gc, const float *__restrict__ W3,
+                                                       const uint16_t *__restrict__ h2, uint16_t *__restrict__ gh2,
+                                                       int B, int S)
+{
+    __shared__ __align__(16) float sw[27 * 16];
+    for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) sw[i] = W3[i];
+    __syncthreads();
+    const int So = S - 2;
+    const int64_t per = (int64_t)S * S * S, pero = (int64_t)So * So * So, total = per * B;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(q / per);
+        const int64_t c = q - b * per;
+        const int xx = (int)(c % S), yy = (int)((c / S) % S), zz = (int)(c / ((int64_t)S * S));
+        float acc[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[i] = 0.f;
+#pragma unroll 1
+        for (int e = 0; e < 27; ++e) {
+            const int ox = xx - 2 + e % 3, oy = yy - 2 + (e / 3) % 3, oz = zz - 2 + e / 9;
+            if ((unsigned)ox >= (unsigned)So || (unsigned)oy >= (unsigned)So || (unsigned)oz >= (unsigned)So) continue;
+            const float g = __ldg(gc + (int64_t)b * pero + ox + (int64_t)So * (oy + (int64_t)So * oz));
+            const float *w = sw + (26 - e) * 16;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] = fmaf(g, w[i], acc[i]);
+        }
+        float m[16];
+        unpack16(h2 + q * 16, m);
+        uint32_t h[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            h[j] = (uint32_t)bf16_bits(m[2 * j] > 0.f ? acc[2 * j] : 0.f) |
+                   ((uint32_t)bf16_bits(m[2 * j + 1] > 0.f ? acc[2 * j + 1] : 0.f) << 16);
+        uint4 *dst = reinterpret_cast<uint4 *>(gh2 + q * 16);
+        dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+        dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
+}
+
+// warp sum of v[0..N) into lane 0
+template <int N> __device__ __forceinline__ void warp_sum(float (&v)[N])
+{
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+}
+
+// layer 3 weight gradient: gW3[t][ci] += sum_q h2[q + d(t)][ci] gc[q], q in
+// (S-2)^3, h2 side S.  Grid (chunks, 27 taps).
+__global__ void __launch_bounds__(256) l3_wgrad_cl(const uint16_t *__restrict__ h2, const float *__restrict__ gc,
+                                                    float *__restrict__ gW3, int B, int S)
+{
+    const int t = blockIdx.y, dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+    const int So = S - 2;
+    const int64_t pero = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = pero * B;
+    float acc[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] = 0.f;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(q / pero);
+        const int64_t c = q - b * pero;
+        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
+        const float g = __ldg(gc + q);
+        float v[16];
+        unpack16(h2 + ((int64_t)b * s3 + (xx + dx) + (int64_t)S * ((yy + dy) + (int64_t)S * (zz + dz))) * 16, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) acc[i] = fmaf(v[i], g, acc[i]);
+    }
+    warp_sum(acc);
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int i = 0; i < 16; ++i) atomicAdd(gW3 + t * 16 + i, acc[i]);
+}
+
+// layer 1 weight gradient: gW1[t][i][o] += sum_q x[i][q + d(t)] gh1[q][o],
+// q in (S-2)^3, x side S.  Grid (chunks, 27 taps).
+__global__ void __launch_bounds__(256) l1_wgrad_cl(const float *__restrict__ x, const uint16_t *__restrict__ gh1,
+                                                    float *__restrict__ gW1, int B, int S)
+{
+    const int t = blockIdx.y, dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+    const int So = S - 2;
+    const int64_t pero = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = pero * B;
+    float acc[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) acc[i] = 0.f;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int b = (int)(q / pero);
+        const int64_t c = q - b * pero;
+        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
+        const int64_t e = (int64_t)b * 2 * s3 + (xx + dx) + (int64_t)S * ((yy + dy) + (int64_t)S * (zz + dz));
+        const float v0 = __ldg(x + e), v1 = __ldg(x + e + s3);
+        float g[16];
+        unpack16(gh1 + q * 16, g);
+#pragma unroll
+        for (int o = 0; o < 16; ++o) {
+            acc[o] = fmaf(v0, g[o], acc[o]);
+            acc[16 + o] = fmaf(v1, g[o], acc[16 + o]);
+        }
+    }
+    warp_sum(acc);
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int i = 0; i < 32; ++i) atomicAdd(gW1 + t * 32 + i, acc[i]);
+}
+
+static unsigned grid_of(int64_t n, int threads, int64_t cap)
+{
+    int64_t b = (n + threads - 1) / threads;
+    if (b > cap) b = cap;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+static DeviceOnce attr_once[3];
+
+template <int MODE>
+static cn_status launch_patch(Args &a, cudaStream_t st)
+{
+    cn_status s = smem_opt_in(attr_once[MODE], patch_tc_kernel<MODE>, SMEM);
+    if (s != CN_OK) return s;
+    int dev = 0, sms = 148;
+    CN_CUDA_TRY(cudaGetDevice(&dev));
+    CN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    a.chunks = (a.total + ROWS - 1) / ROWS;
+    const int64_t grid = a.chunks < 2LL * sms ? a.chunks : 2LL * sms;
+    patch_tc_kernel<MODE><<<(unsigned)grid, NT, SMEM, st>>>(a);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+} // namespace nntr
+
+namespace nntc {
+
+cn_status train_forward_tc(const TrainBufs &T, const float *x, const float *W, int B, int P, cudaStream_t st)
+{
+    using namespace nntr;
+    const int S = P + 8, S1 = S - 2, S2 = S - 4, S3 = S - 6;
+    const float *W1 = W, *W2 = W + 27 * 2 * 16, *W3 = W + 27 * 2 * 16 + 27 * 16 * 16;
+    cn_status s;
+    // packed B tiles of the hidden layer: forward, backward-data
+    if ((s = pack_weights(W2, 16, 16, T.wfwd, st)) != CN_OK) return s;
+    pack_bwd_kernel<<<27, 256, 0, st>>>(W2, T.wbwd);
+    l1_fwd_cl<<<grid_of((int64_t)B * S1 * S1 * S1, 128, 148 * 64), 128, 0, st>>>(x, W1, T.h1, B, S);
+    CN_CUDA_TRY(cudaGetLastError());
+    Args a = {};
+    a.src = T.h1;
+    a.w = T.wfwd;
+    a.out = T.h2;
+    a.Sin = S1;
+    a.Sout = S2;
+    a.shift = 0;
+    a.relu = 1;
+    a.total = (int64_t)B * S2 * S2 * S2;
+    a.err = T.err;
+    if ((s = launch_patch<FWD>(a, st)) != CN_OK) return s;
+    l3_fwd_cl<<<grid_of((int64_t)B * S3 * S3 * S3, 128, 148 * 64), 128, 0, st>>>(T.h2, W3, T.y, B, S2);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+cn_status train_backward_tc(const TrainBufs &T, const float *x, const float *W, float *gW, int B, int P,
+                            cudaStream_t st)
+{
+    using namespace nntr;
+    const int S = P + 8, S1 = S - 2, S2 = S - 4, S3 = S - 6;
+    const float *W3 = W + 27 * 2 * 16 + 27 * 16 * 16;
+    float *gW1 = gW, *gW2 = gW + 27 * 2 * 16, *gW3 = gW + 27 * 2 * 16 + 27 * 16 * 16;
+    cn_status s;
+    CN_CUDA_TRY(cudaMemsetAsync(gW, 0, sizeof(float) * (27 * 2 * 16 + 27 * 16 * 16 + 27 * 16), st));
+    l3_wgrad_cl<<<dim3(grid_of((int64_t)B * S3 * S3 * S3, 256, 64), 27), 256, 0, st>>>(T.h2, T.gc, gW3, B, S2);
+    l3_bwd_data_cl<<<grid_of((int64_t)B * S2 * S2 * S2, 128, 148 * 64), 128, 0, st>>>(T.gc, W3, T.h2, T.gh2, B, S2);
+    CN_CUDA_TRY(cudaGetLastError());
+    Args w = {};
+    w.src = T.h1;
+    w.gout = T.gh2;
+    w.gw = gW2;
+    w.Sin = S1;
+    w.Sout = S2;
+    w.shift = 0;
+    w.total = (int64_t)B * S2 * S2 * S2;
+    w.err = T.err;
+    if ((s = launch_patch<WGRAD>(w, st)) != CN_OK) return s;
+    Args d = {};
+    d.src = T.gh2;
+    d.act = T.h1;
+    d.w = T.wbwd;
+    d.out = T.gh1;
+    d.Sin = S2;
+    d.Sout = S1;
+    d.shift = -2;
+    d.total = (int64_t)B * S1 * S1 * S1;
+    d.err = T.err;
+    if ((s = launch_patch<BWD>(d, st)) != CN_OK) return s;
+    l1_wgrad_cl<<<dim3(grid_of((int64_t)B * S1 * S1 * S1, 256, 64), 27), 256, 0, st>>>(x, T.gh1, gW1, B, S);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+} // namespace nntc
+} // namespace cn

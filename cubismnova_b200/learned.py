@@ -24,6 +24,7 @@ _lib.register({
     "cn_mg_set_smoother": (_I, [_P, _P, C.c_uint]),
     "cn_mg_set_smoother_phases": (_I, [_P, _P, C.c_uint, C.c_uint, _I, _I]),
     "cn_nn_set_inference": (_I, [_P, _I]),
+    "cn_nn_set_training": (_I, [_P, _I]),
     "cn_conv3_bf16": (_I, [_P, _P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P, _I, _P]),
 })
 
@@ -70,6 +71,13 @@ class LearnedSmoother:
         """Grid inference on "tensor" cores (BF16 activations and weights,
         tcgen05, FP32 accumulation; the default) or "fp32" CUDA cores."""
         _lib.check(_lib.lib().cn_nn_set_inference(self._h, {"fp32": 0, "tensor": 1}[mode]))
+
+    def set_training(self, mode: str):
+        """Training arithmetic: "tensor" (the default: the hidden layer's
+        forward, data gradient and weight gradient on the tensor cores with
+        BF16 operands and activations, FP32 accumulation) or "fp32" (CUDA
+        cores throughout)."""
+        _lib.check(_lib.lib().cn_nn_set_training(self._h, {"fp32": 0, "tensor": 1}[mode]))
 
     def set_weights(self, W1, W2, W3):
         w = np.concatenate([np.asarray(a, dtype=np.float32).ravel() for a in (W1, W2, W3)])

@@ -338,6 +338,14 @@ cn_status cn_mg_set_smoother_phases(cn_mg *m, cn_nn *nn, unsigned pre_mask, unsi
  * the tensor cores (tcgen05, FP32 accumulation) on levels whose block cells
  * are multiples of (16, 16, 4), else FP32; 0 = FP32 on the CUDA cores. */
 cn_status cn_nn_set_inference(cn_nn *nn, int mode);
+/* Training precision (cn_nn_loss_grad, cn_nn_train): 1 (default) = the
+ * hidden 16 -> 16 layer's forward, data gradient and weight gradient on the
+ * tensor cores (tcgen05, BF16 operands, FP32 accumulation) with BF16
+ * activations and activation gradients, the first and last layers on the
+ * CUDA cores in FP32 arithmetic; 0 = FP32 throughout on the CUDA cores.
+ * A tensor-core kernel whose bounded wait ran out makes the call return
+ * CN_ERR_DEVICE. */
+cn_status cn_nn_set_training(cn_nn *nn, int mode);
 /* One 3x3x3 convolution, 16 -> 16 channels, on the tensor cores: in and out
  * are device arrays [nblocks][cells][16] of BF16 (channels last, blocks and
  * cells in grid order), neighbours across blocks periodic; weights FP32

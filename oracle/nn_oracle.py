@@ -11,6 +11,13 @@ cubismnova_b200/csrc/learned.cu (the reference has no learned components):
 Patch arrays are (B, C, S, S, S) in (z, y, x) order; weights (27, Cin, Cout)
 with tap = dx + 3 dy + 9 dz.  ``loss_and_grad`` is checked against central
 finite differences by ``fd_check``.
+
+With ``bf16=True`` the forward and backward round where the tensor-core
+training path (cubismnova_b200/csrc/learned_train_tc.cu) stores BF16: the
+hidden layer's weights W2, the activations h1 and h2 after the ReLU, and the
+activation gradients gh2 and gh1 after the ReLU mask (each value first
+rounded to float32, as the device computes it, then to BF16 with
+round-to-nearest-even).
 """
 from __future__ import annotations
 
@@ -42,6 +49,14 @@ def conv_valid_bwd(x, W, gout):
                 gW[t] += np.einsum("bizyx,bozyx->io", xs, gout)
                 gx[:, :, dz:dz + So, dy:dy + So, dx:dx + So] += np.einsum("bozyx,io->bizyx", gout, W[t])
     return gx, gW
+
+
+def bf16(a):
+    """Round to BF16 (nearest, ties to even) via float32; returns float64."""
+    f = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    u = f.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
 def harm(a, b):
@@ -86,11 +101,10 @@ def A_adjoint(g, k, ih2):
     return out
 
 
-def forward(x, k, r, W1, W2, W3, omega, ih2):
-    h1p = conv_valid(x, W1)
-    h1 = np.maximum(h1p, 0)
-    h2p = conv_valid(h1, W2)
-    h2 = np.maximum(h2p, 0)
+def forward(x, k, r, W1, W2, W3, omega, ih2, bf16_path=False):
+    rnd = bf16 if bf16_path else (lambda a: a)
+    h1 = rnd(np.maximum(conv_valid(x, W1), 0))
+    h2 = rnd(np.maximum(conv_valid(h1, rnd(W2)), 0))
     y = conv_valid(h2, W3)[:, 0]
     c = omega * x[:, 0, 3:-3, 3:-3, 3:-3] + y
     res = r - apply_A(c, k, ih2)
@@ -100,16 +114,17 @@ def forward(x, k, r, W1, W2, W3, omega, ih2):
     return loss, dict(h1=h1, h2=h2, y=y, c=c, res=res, rr=rr)
 
 
-def loss_and_grad(x, k, r, W1, W2, W3, omega, ih2):
+def loss_and_grad(x, k, r, W1, W2, W3, omega, ih2, bf16_path=False):
+    rnd = bf16 if bf16_path else (lambda a: a)
     B = x.shape[0]
-    loss, t = forward(x, k, r, W1, W2, W3, omega, ih2)
+    loss, t = forward(x, k, r, W1, W2, W3, omega, ih2, bf16_path)
     g = (-2.0 / (t["rr"] * B))[:, None, None, None] * t["res"]
     gc = A_adjoint(g, k, ih2)
     gy = gc[:, None]
     gh2, gW3 = conv_valid_bwd(t["h2"], W3, gy)
-    gh2 *= t["h2"] > 0
-    gh1, gW2 = conv_valid_bwd(t["h1"], W2, gh2)
-    gh1 *= t["h1"] > 0
+    gh2 = rnd(gh2 * (t["h2"] > 0))
+    gh1, gW2 = conv_valid_bwd(t["h1"], rnd(W2), gh2)
+    gh1 = rnd(gh1 * (t["h1"] > 0))
     _, gW1 = conv_valid_bwd(x, W1, gh1)
     return loss, gW1, gW2, gW3
 
