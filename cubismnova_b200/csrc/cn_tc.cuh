@@ -3,7 +3,8 @@
 // operand descriptors, completion through an mbarrier, and TMEM loads.
 //
 // Only the single-CTA forms (cta_group::1), dense kind::f16 with BF16 inputs
-// and FP32 accumulation, and unswizzled K-major operands are used.
+// and FP32 accumulation, and unswizzled operands (K-major, or MN-major with
+// the instruction descriptor's transpose bits 15 / 16) are used.
 #pragma once
 
 #include "cn_tma.cuh"
@@ -13,11 +14,12 @@
 namespace cn {
 namespace tc {
 
-// Shared-memory matrix descriptor for an unswizzled K-major operand.  The
-// canonical layout is built from core matrices of 8 rows x 16 bytes (each row
-// 16 contiguous bytes, the 8 rows 16 bytes apart); `lbo` is the byte distance
-// between core matrices adjacent along K, `sbo` between core matrices
-// adjacent along M (or N).  Bits: start address >> 4 [0,14), lbo >> 4
+// Shared-memory matrix descriptor for an unswizzled operand.  The canonical
+// layout is built from core matrices of 128 contiguous bytes: for a K-major
+// operand 8 rows (M or N) of 16 bytes (8 BF16 along K), for an MN-major one
+// 8 rows along K of 16 bytes (8 BF16 along M or N); `lbo` is the byte
+// distance between core matrices adjacent along K, `sbo` between core
+// matrices adjacent along M (or N).  Bits: start address >> 4 [0,14), lbo >> 4
 // [16,30), sbo >> 4 [32,46), descriptor version 1 at bit 46, base offset 0,
 // layout type 0 (no swizzle) in bits [61,64).
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
@@ -91,6 +93,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
                  : "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i)
+        v[i] = __uint_as_float(r[i]);
+}
+
+// 32 lanes x 8 columns of 32 bits (as tmem_ld16, half the columns)
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8])
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"
+                 "tcgen05.wait::ld.sync.aligned;"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr)
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
         v[i] = __uint_as_float(r[i]);
 }
 

@@ -205,16 +205,18 @@ __global__ void __launch_bounds__(256) loss_fwd(const float *x, const float *y, 
     }
 }
 
+// Grid (chunks, B): blockIdx.y is the sample; per-sample sums reduced in the
+// block (warp shuffles, then one warp) before one atomic pair per block.
 __global__ void __launch_bounds__(256) loss_res(const float *c, const float *k, const float *r, float ih2, int B, int P,
                                                 float *res_out, double *sums)
 {
     const int R = P + 2;
     const int64_t perR = (int64_t)R * R * R, perP = (int64_t)P * P * P;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < perP * B; t += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(t / perP);
-        const int64_t cc = t - b * perP;
+    const int b = blockIdx.y;
+    const float *cb = c + b * perR, *kb = k + b * perR;
+    double srr = 0.0, see = 0.0;
+    for (int64_t cc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cc < perP; cc += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(cc % P) + 1, y = (int)((cc / P) % P) + 1, z = (int)(cc / (P * P)) + 1;
-        const float *cb = c + b * perR, *kb = k + b * perR;
         const int64_t i = x + (int64_t)R * (y + (int64_t)R * z);
         const float pc = cb[i], kc = kb[i];
         const int64_t st[3] = {1, R, (int64_t)R * R};
@@ -225,11 +227,33 @@ __global__ void __launch_bounds__(256) loss_res(const float *c, const float *k, 
             f[d] = kp * (cb[i + st[d]] - pc) - km * (pc - cb[i - st[d]]);
         }
         const float Ac = ih2 * ((f[0] + f[1]) + f[2]);
+        const int64_t t = b * perP + cc;
         const float rv = r[t];
         const float e = rv - Ac;
         res_out[t] = e;
-        atomicAdd(sums + 2 * b, (double)rv * rv);
-        atomicAdd(sums + 2 * b + 1, (double)e * e);
+        srr += (double)rv * rv;
+        see += (double)e * e;
+    }
+    __shared__ double part[2][8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        srr += __shfl_xor_sync(0xffffffffu, srr, o);
+        see += __shfl_xor_sync(0xffffffffu, see, o);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        part[0][w] = srr;
+        part[1][w] = see;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, e2 = 0.0;
+        for (int j = 0; j < (int)(blockDim.x >> 5); ++j) {
+            a += part[0][j];
+            e2 += part[1][j];
+        }
+        atomicAdd(sums + 2 * b, a);
+        atomicAdd(sums + 2 * b + 1, e2);
     }
 }
 
@@ -658,7 +682,11 @@ cn_status cn_nn_loss_grad(cn_nn *nn, const float *x, const float *k, const float
     const int64_t s2 = (int64_t)(P + 2) * (P + 2) * (P + 2), s0 = (int64_t)P * P * P;
     loss_fwd<<<nblk(B * s2), 256, 0, st>>>(x, nn->y, (float)nn->omega, B, P, nn->c);
     CN_CUDA_TRY(cudaMemsetAsync(nn->sums, 0, sizeof(double) * 2 * B, st));
-    loss_res<<<nblk(B * s0), 256, 0, st>>>(nn->c, k, r, (float)ih2, B, P, nn->res, nn->sums);
+    {
+        int64_t gx = (s0 + 255) / 256;
+        if (gx > 64) gx = 64;
+        loss_res<<<dim3((unsigned)gx, (unsigned)B), 256, 0, st>>>(nn->c, k, r, (float)ih2, B, P, nn->res, nn->sums);
+    }
     loss_adjoint<<<nblk(B * s2), 256, 0, st>>>(nn->res, k, nn->sums, (float)ih2, B, P, nn->gc);
     if (nn->training == 1) {
         if ((s = nntc::train_backward_tc(T, x, nn->w, nn->g, B, P, st)) != CN_OK) return s;

@@ -31,16 +31,20 @@
 //                  added to gW with atomics at the end.  Rows of taps >= 27 in
 //                  the last tile read whatever the buffer holds; those
 //                  accumulator rows are never read.
-// Taps are gathered in 4 groups of 8 into two 32 KB buffers: the MMAs of one
-// group (issued by one thread, committed to the buffer's mbarrier) overlap
-// the gather of the next.  Persistent CTAs, two per SM; every wait bounded
-// (an error word is set and the CTA stops issuing).
+// Taps are gathered in 4 groups of 8 into two 32 KB buffers, one group
+// ahead: the copies of group i + 1 are in flight while group i's MMAs
+// (issued by one thread, committed to the buffer's mbarrier) run.  Lanes 2i
+// and 2i+1 of a warp copy the two channel halves of one row, so one copy
+// instruction reads 512 contiguous bytes.  Persistent CTAs, two per SM;
+// every wait bounded (an error word is set and the CTA stops issuing).
 #include "cn_internal.h"
 #include "cn_tc.cuh"
 #include "cn_tma.cuh"
 #include "learned_tc.h"
 
 #include <cuda_bf16.h>
+
+#include <type_traits>
 
 namespace cn {
 namespace nntr {
@@ -50,7 +54,7 @@ constexpr int GT = 8;                            // taps per gather group
 constexpr int NG = 4;                            // groups per chunk (taps 0-7, 8-15, 16-23, 24-26)
 constexpr uint32_t PL = ROWS * 16;               // bytes of one plane
 constexpr uint32_t GBUF = 2 * GT * PL;           // one group buffer: 16 planes, 32 KB
-constexpr int NT = ROWS;                         // thread r owns row r
+constexpr int NT = 2 * ROWS;                     // two threads per row (channel halves)
 constexpr uint32_t WBYTES = 27 * 512;            // packed weights of one layer
 constexpr uint32_t GOUT_BYTES = 2 * PL;          // weight gradient: gout rows of a chunk (2 planes)
 constexpr size_t OFF_W = 2 * (size_t)GBUF;       // weights (forward / backward-data) or gout buffers
@@ -78,12 +82,30 @@ struct Args {
 
 __device__ __forceinline__ uint16_t bf16_bits(float v) { return __bfloat16_as_ushort(__float2bfloat16_rn(v)); }
 
+// cell index q of a batch of cubes of side n (n3 = n^3; indices below 2^31,
+// checked on the host) -> patch b and (x, y, z); 32-bit divisions
+struct CubeIdx {
+    int b, x, y, z;
+};
+__device__ __forceinline__ CubeIdx cube_idx(uint32_t q, uint32_t n, uint32_t n3)
+{
+    CubeIdx c;
+    const uint32_t b = q / n3, rem = q - b * n3, zy = rem / n, z = zy / n;
+    c.b = (int)b;
+    c.x = (int)(rem - zy * n);
+    c.z = (int)z;
+    c.y = (int)(zy - z * n);
+    return c;
+}
+
 // 16-byte asynchronous copy; src_bytes 0 writes zeros (nothing is read)
 __device__ __forceinline__ void cp16(void *dst, const void *src, uint32_t src_bytes)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
                  : "memory");
 }
+
+template <int V> using ic = std::integral_constant<int, V>;
 
 template <int MODE>
 __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__ Args a)
@@ -117,128 +139,150 @@ __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__
     tc::fence_after_sync();
     const uint32_t tbase = *slot;
 
-    const int64_t so3 = (int64_t)a.Sout * a.Sout * a.Sout, si3 = (int64_t)a.Sin * a.Sin * a.Sin;
-    int it = 0, nch = 0;
-    bool ok = true;
-    for (int64_t c = blockIdx.x; c < a.chunks && ok; c += gridDim.x, ++nch) {
-        // ---- this thread's row: output cell L
-        const int64_t L = c * ROWS + r;
-        const bool valid = L < a.total;
-        int64_t bq = 0, rem = 0;
-        int x = 0, y = 0, z = 0;
-        if (valid) {
-            bq = L / so3;
-            rem = L - bq * so3;
-            x = (int)(rem % a.Sout);
-            y = (int)((rem / a.Sout) % a.Sout);
-            z = (int)(rem / ((int64_t)a.Sout * a.Sout));
+    const uint32_t so3 = (uint32_t)a.Sout * a.Sout * a.Sout;
+    const int64_t si3 = (int64_t)a.Sin * a.Sin * a.Sin, sin1 = a.Sin, sin2 = (int64_t)a.Sin * a.Sin;
+    const int nch = (int64_t)blockIdx.x < a.chunks ? (int)((a.chunks - 1 - blockIdx.x) / gridDim.x + 1) : 0;
+    const int nitems = NG * nch; // items (chunk j of this CTA, tap group g): i = NG j + g, buffer g & 1
+    // gather: thread r copies channel half hh of row rho (a warp: 16 rows =
+    // 512 contiguous source bytes where the cells are contiguous)
+    const int hh = r & 1, rho = r >> 1;
+    int64_t rL = 0, roff = 0; // the row's cell; source element of its tap (0, 0, 0) (may lie outside)
+    uint32_t mx = 0, my = 0, mz = 0; // per axis: offsets k = 0..2 with the source inside the cube
+    auto set_row = [&](int j) {
+        rL = (blockIdx.x + (int64_t)j * gridDim.x) * ROWS + rho;
+        mx = my = mz = 0;
+        if (rL < a.total) {
+            const CubeIdx ci = cube_idx((uint32_t)rL, (uint32_t)a.Sout, so3);
+            const int x0 = ci.x + a.shift, y0 = ci.y + a.shift, z0 = ci.z + a.shift;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                mx |= ((unsigned)(x0 + k) < (unsigned)a.Sin ? 1u : 0u) << k;
+                my |= ((unsigned)(y0 + k) < (unsigned)a.Sin ? 1u : 0u) << k;
+                mz |= ((unsigned)(z0 + k) < (unsigned)a.Sin ? 1u : 0u) << k;
+            }
+            roff = (int64_t)ci.b * si3 + x0 + sin1 * y0 + sin2 * z0;
         }
-        unsigned char *G = Wb + (nch & 1) * GOUT_BYTES;
-        for (int g = 0; g < NG; ++g, ++it) {
-            const int buf = it & 1;
-            // ---- the buffer's previous MMAs (item it - 2) must be done
-            if (it >= 2) {
-                if (r == 0) flag[0] = mbar_wait_bounded(empty + buf, ((it >> 1) - 1) & 1) ? 1 : 0;
+    };
+    auto gather = [&](int j, auto G) {
+        constexpr int g = decltype(G)::value;
+        if (g == 0) set_row(j);
+        unsigned char *A = Abuf + (g & 1) * GBUF;
+        if (MODE == WGRAD && g == 0) {
+            // the chunk's gradient rows (buffer j & 1 was last read by chunk j - 2's
+            // MMAs, complete before item NG j - 2's)
+            const bool v = rL < a.total;
+            cp16(Wb + (j & 1) * GOUT_BYTES + hh * PL + rho * 16, v ? a.gout + rL * 16 + 8 * hh : a.gout, v ? 16u : 0u);
+        }
+#pragma unroll
+        for (int tl = 0; tl < GT; ++tl) {
+            const int t = g * GT + tl;
+            if (t < 27) {
+                const int dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+                const bool in = ((mx >> dx) & (my >> dy) & (mz >> dz) & 1u) != 0;
+                const uint16_t *src = in ? a.src + (roff + dx + sin1 * dy + sin2 * dz) * 16 + 8 * hh : a.src;
+                cp16(A + (2 * tl + hh) * PL + rho * 16, src, in ? 16u : 0u);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    // one item: gather the next (after its buffer's previous MMAs), wait
+    // for this item's copies, issue its MMAs; after the last group of a
+    // chunk (forward / backward-data) drain the accumulator.  False when a
+    // bounded wait ran out.
+    auto item = [&](int j, auto G) -> bool {
+        constexpr int g = decltype(G)::value;
+        const int i = NG * j + g;
+        if (i + 1 < nitems) {
+            if (i >= 1) {
+                if (r == 0)
+                    flag[0] = mbar_wait_bounded(empty + ((g + 1) & 1), (((i + 1) >> 1) - 1) & 1) ? 1 : 0;
                 __syncthreads();
-                if (!flag[0]) {
-                    ok = false;
-                    break;
-                }
+                if (!flag[0]) return false;
             }
-            unsigned char *A = Abuf + buf * GBUF;
-            if (MODE == WGRAD && g == 0) {
-                // the chunk's gradient rows (the buffer of chunk nch - 2 is free: its MMAs precede item it - 2)
-                const uint16_t *s = a.gout + (valid ? L : 0) * 16;
-                cp16(G + r * 16, s, valid ? 16u : 0u);
-                cp16(G + PL + r * 16, s + 8, valid ? 16u : 0u);
-            }
-#pragma unroll
-            for (int tl = 0; tl < GT; ++tl) {
-                const int t = g * GT + tl;
-                if (t < 27) {
-                    const int sx = x + t % 3 + a.shift, sy = y + (t / 3) % 3 + a.shift, sz = z + t / 9 + a.shift;
-                    const bool in = valid && (unsigned)sx < (unsigned)a.Sin && (unsigned)sy < (unsigned)a.Sin &&
-                                    (unsigned)sz < (unsigned)a.Sin;
-                    const int64_t e = in ? bq * si3 + sx + (int64_t)a.Sin * (sy + (int64_t)a.Sin * sz) : 0;
-                    const uint16_t *s = a.src + e * 16;
-                    cp16(A + (2 * tl) * PL + r * 16, s, in ? 16u : 0u);
-                    cp16(A + (2 * tl + 1) * PL + r * 16, s + 8, in ? 16u : 0u);
-                }
-            }
-            asm volatile("cp.async.wait_all;" ::: "memory");
-            fence_proxy_async_smem(); // generic-proxy smem writes -> visible to the tensor cores
-            tc::fence_before_sync();
-            __syncthreads();
-            if (r == 0) {
-                tc::fence_after_sync();
-                if (MODE == WGRAD) {
-#pragma unroll
-                    for (int ks = 0; ks < ROWS / 16; ++ks) {
-                        const uint64_t da = tc::smem_desc(smem_u32(A) + 256u * ks, 128u, PL);
-                        const uint64_t db = tc::smem_desc(smem_u32(G) + 256u * ks, 128u, PL);
-                        tc::mma_bf16(tbase + 16u * g, da, db, IDESC_MN, (nch > 0 || ks > 0) ? 1u : 0u);
-                    }
-                } else {
-#pragma unroll
-                    for (int tl = 0; tl < GT; ++tl) {
-                        const int t = g * GT + tl;
-                        if (t < 27) {
-                            const uint64_t da = tc::smem_desc(smem_u32(A) + 2u * tl * PL, PL, 128u);
-                            const uint64_t db = tc::smem_desc(smem_u32(Wb) + 512u * t, 256u, 128u);
-                            tc::mma_bf16(tbase, da, db, IDESC_K, t > 0 ? 1u : 0u);
-                        }
-                    }
-                }
-                tc::mma_commit(empty + buf);
-                if (MODE != WGRAD && g == NG - 1) tc::mma_commit(dready);
-            }
+            if constexpr (g == NG - 1) gather(j + 1, ic<0>{});
+            else gather(j, ic<g + 1>{});
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
-        if (!ok) break;
-        if (MODE != WGRAD) {
-            // ---- epilogue: thread r drains accumulator row r (TMEM lane r)
-            if (r == 0) flag[1] = mbar_wait_bounded(dready, nch & 1) ? 1 : 0;
-            __syncthreads();
-            if (!flag[1]) {
-                ok = false;
-                break;
-            }
+        fence_proxy_async_smem(); // generic-proxy smem writes -> visible to the tensor cores
+        tc::fence_before_sync();
+        __syncthreads();
+        if (r == 0) {
             tc::fence_after_sync();
-            float v[16];
-            tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16), v);
-            tc::fence_before_sync();
-            if (valid) {
-                uint32_t h[8];
-                if (MODE == BWD) {
-                    const uint4 *m = reinterpret_cast<const uint4 *>(a.act + L * 16);
-                    const uint4 m0 = m[0], m1 = m[1];
-                    const uint32_t mw[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+            const uint32_t A = smem_u32(Abuf + (g & 1) * GBUF);
+            if (MODE == WGRAD) {
+                const uint32_t Gs = smem_u32(Wb + (j & 1) * GOUT_BYTES);
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
+                for (int ks = 0; ks < ROWS / 16; ++ks) {
+                    const uint64_t da = tc::smem_desc(A + 256u * ks, 128u, PL);
+                    const uint64_t db = tc::smem_desc(Gs + 256u * ks, 128u, PL);
+                    tc::mma_bf16(tbase + 16u * g, da, db, IDESC_MN, (j > 0 || ks > 0) ? 1u : 0u);
+                }
+            } else {
+#pragma unroll
+                for (int tl = 0; tl < GT; ++tl) {
+                    const int t = g * GT + tl;
+                    if (t < 27) {
+                        const uint64_t da = tc::smem_desc(A + 2u * tl * PL, PL, 128u);
+                        const uint64_t db = tc::smem_desc(smem_u32(Wb) + 512u * t, 256u, 128u);
+                        tc::mma_bf16(tbase, da, db, IDESC_K, t > 0 ? 1u : 0u);
+                    }
+                }
+            }
+            tc::mma_commit(empty + (g & 1));
+            if (MODE != WGRAD && g == NG - 1) tc::mma_commit(dready);
+        }
+        if constexpr (MODE != WGRAD && g == NG - 1) {
+            // ---- epilogue of chunk j: warp w reads TMEM lanes 32 (w % 4) + lane
+            // (= the chunk's row m), columns (channels) 8 (w / 4) .. + 7
+            const int m = 32 * (warp & 3) + (r & 31), ch = 8 * (warp >> 2);
+            const int64_t L = (blockIdx.x + (int64_t)j * gridDim.x) * ROWS + m;
+            if (r == 0) flag[1] = mbar_wait_bounded(dready, j & 1) ? 1 : 0;
+            __syncthreads();
+            if (!flag[1]) return false;
+            tc::fence_after_sync();
+            float v[8];
+            tc::tmem_ld8(tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)ch, v);
+            tc::fence_before_sync();
+            if (L < a.total) {
+                uint32_t h[4];
+                if (MODE == BWD) {
+                    const uint4 mk = *reinterpret_cast<const uint4 *>(a.act + L * 16 + ch);
+                    const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
                         // BF16 = the top 16 bits of an FP32: > 0 test on the widened value
-                        const float lo = __uint_as_float(mw[j] << 16), hi = __uint_as_float(mw[j] & 0xFFFF0000u);
-                        h[j] = (uint32_t)bf16_bits(lo > 0.f ? v[2 * j] : 0.f) |
-                               ((uint32_t)bf16_bits(hi > 0.f ? v[2 * j + 1] : 0.f) << 16);
+                        const float lo = __uint_as_float(mw[q] << 16), hi = __uint_as_float(mw[q] & 0xFFFF0000u);
+                        h[q] = (uint32_t)bf16_bits(lo > 0.f ? v[2 * q] : 0.f) |
+                               ((uint32_t)bf16_bits(hi > 0.f ? v[2 * q + 1] : 0.f) << 16);
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        float p = v[2 * j], q = v[2 * j + 1];
+                    for (int q = 0; q < 4; ++q) {
+                        float p = v[2 * q], u = v[2 * q + 1];
                         if (a.relu) {
                             p = fmaxf(p, 0.f);
-                            q = fmaxf(q, 0.f);
+                            u = fmaxf(u, 0.f);
                         }
-                        h[j] = (uint32_t)bf16_bits(p) | ((uint32_t)bf16_bits(q) << 16);
+                        h[q] = (uint32_t)bf16_bits(p) | ((uint32_t)bf16_bits(u) << 16);
                     }
                 }
-                uint4 *dst = reinterpret_cast<uint4 *>(a.out + L * 16);
-                dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
-                dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+                *reinterpret_cast<uint4 *>(a.out + L * 16 + ch) = make_uint4(h[0], h[1], h[2], h[3]);
             }
         }
-    }
-    // ---- weight gradient: wait for every MMA of this CTA, then add the
-    // 4 accumulator tiles (row m = 16 (tap - 8 g) + ci, column co) to gW
-    if (MODE == WGRAD && ok && nch > 0) {
+        return true;
+    };
+
+    bool ok = true;
+    if (nitems > 0) gather(0, ic<0>{});
+    for (int j = 0; j < nch && ok; ++j)
+        ok = item(j, ic<0>{}) && item(j, ic<1>{}) && item(j, ic<2>{}) && item(j, ic<3>{});
+    asm volatile("cp.async.wait_all;" ::: "memory"); // nothing in flight past this point
+    // ---- weight gradient: wait for every MMA of this CTA, then add the 4
+    // accumulator tiles (row m = 16 (tap - 8 g) + ci, column co) to gW; warp
+    // w reads rows 32 (w % 4) + lane, columns 8 (w / 4) .. + 7
+    if (MODE == WGRAD && ok && nitems > 0) {
         if (r == 0) {
             tc::mma_commit(dready);
             flag[1] = mbar_wait_bounded(dready, 0) ? 1 : 0;
@@ -247,14 +291,15 @@ __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__
         ok = flag[1] != 0;
         if (ok) {
             tc::fence_after_sync();
+            const int m = 32 * (warp & 3) + (r & 31), ch = 8 * (warp >> 2);
 #pragma unroll 1
             for (int g = 0; g < NG; ++g) {
-                float v[16];
-                tc::tmem_ld16(tbase + ((uint32_t)(32 * warp) << 16) + 16u * g, v);
-                const int t = g * GT + r / 16, ci = r % 16;
+                float v[8];
+                tc::tmem_ld8(tbase + ((uint32_t)(32 * (warp & 3)) << 16) + 16u * g + (uint32_t)ch, v);
+                const int t = g * GT + m / 16, ci = m % 16;
                 if (t < 27) {
 #pragma unroll
-                    for (int co = 0; co < 16; ++co) atomicAdd(a.gw + (t * 16 + ci) * 16 + co, v[co]);
+                    for (int k = 0; k < 8; ++k) atomicAdd(a.gw + (t * 16 + ci) * 16 + ch + k, v[k]);
                 }
             }
         }
@@ -287,9 +332,8 @@ __global__ void __launch_bounds__(128) l1_fwd_cl(const float *__restrict__ x, co
     const int So = S - 2;
     const int64_t per = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = per * B;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(q / per);
-        const int64_t c = q - b * per;
-        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
+        const CubeIdx ci = cube_idx((uint32_t)q, (uint32_t)So, (uint32_t)per);
+        const int b = ci.b, xx = ci.x, yy = ci.y, zz = ci.z;
         const float *x0 = x + (int64_t)b * 2 * s3, *x1 = x0 + s3;
         float acc[16];
 #pragma unroll
@@ -334,9 +378,8 @@ __global__ void __launch_bounds__(128) l3_fwd_cl(const uint16_t *__restrict__ h2
     const int So = S - 2;
     const int64_t per = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = per * B;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(q / per);
-        const int64_t c = q - b * per;
-        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
+        const CubeIdx ci = cube_idx((uint32_t)q, (uint32_t)So, (uint32_t)per);
+        const int b = ci.b, xx = ci.x, yy = ci.y, zz = ci.z;
         float acc = 0.f;
 #pragma unroll 1
         for (int t = 0; t < 27; ++t) {
@@ -362,9 +405,8 @@ __global__ void __launch_bounds__(128) l3_bwd_data_cl(const float *__restrict__ 
     const int So = S - 2;
     const int64_t per = (int64_t)S * S * S, pero = (int64_t)So * So * So, total = per * B;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(q / per);
-        const int64_t c = q - b * per;
-        const int xx = (int)(c % S), yy = (int)((c / S) % S), zz = (int)(c / ((int64_t)S * S));
+        const CubeIdx ci = cube_idx((uint32_t)q, (uint32_t)S, (uint32_t)per);
+        const int b = ci.b, xx = ci.x, yy = ci.y, zz = ci.z;
         float acc[16];
 #pragma unroll
         for (int i = 0; i < 16; ++i) acc[i] = 0.f;
@@ -399,60 +441,86 @@ template <int N> __device__ __forceinline__ void warp_sum(float (&v)[N])
         for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
 }
 
-// layer 3 weight gradient: gW3[t][ci] += sum_q h2[q + d(t)][ci] gc[q], q in
-// (S-2)^3, h2 side S.  Grid (chunks, 27 taps).
-__global__ void __launch_bounds__(256) l3_wgrad_cl(const uint16_t *__restrict__ h2, const float *__restrict__ gc,
-                                                    float *__restrict__ gW3, int B, int S)
+// The weight gradients of the first and last layers: blocks of 27 warps,
+// warp w = tap w.  A block walks whole planes (patch b, z) of the output
+// cells; the lanes of all 27 warps take the same cells of the plane (index
+// y So + x, advanced without divisions), so the per-cell operand (gc or
+// gh1) is read from DRAM once and the 27 taps' shifted reads hit L1.
+// Per-warp sums, then atomics.
+constexpr int WG_THREADS = 27 * 32;
+
+// layer 3: gW3[t][ci] += sum_q h2[q + d(t)][ci] gc[q], q in (S-2)^3, h2 side S
+__global__ void __launch_bounds__(WG_THREADS) l3_wgrad_cl(const uint16_t *__restrict__ h2,
+                                                           const float *__restrict__ gc, float *__restrict__ gW3,
+                                                           int B, int S)
 {
-    const int t = blockIdx.y, dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
-    const int So = S - 2;
-    const int64_t pero = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = pero * B;
+    const int t = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+    const int So = S - 2, plane = So * So;
+    const int64_t s3 = (int64_t)S * S * S;
     float acc[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) acc[i] = 0.f;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(q / pero);
-        const int64_t c = q - b * pero;
-        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
-        const float g = __ldg(gc + q);
-        float v[16];
-        unpack16(h2 + ((int64_t)b * s3 + (xx + dx) + (int64_t)S * ((yy + dy) + (int64_t)S * (zz + dz))) * 16, v);
+    for (int pz = blockIdx.x; pz < B * So; pz += gridDim.x) {
+        const int b = pz / So, zz = pz - b * So;
+        const float *gp = gc + (int64_t)pz * plane;
+        const uint16_t *hp = h2 + ((int64_t)b * s3 + dx + (int64_t)S * (dy + (int64_t)S * (zz + dz))) * 16;
+        int xx = lane, yy = 0;
+        for (int idx = lane; idx < plane; idx += 32) {
+            while (xx >= So) {
+                xx -= So;
+                ++yy;
+            }
+            const float g = __ldg(gp + idx);
+            float v[16];
+            unpack16(hp + (xx + (int64_t)S * yy) * 16, v);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) acc[i] = fmaf(v[i], g, acc[i]);
+            for (int i = 0; i < 16; ++i) acc[i] = fmaf(v[i], g, acc[i]);
+            xx += 32;
+        }
     }
     warp_sum(acc);
-    if ((threadIdx.x & 31) == 0)
+    if (lane == 0)
 #pragma unroll
         for (int i = 0; i < 16; ++i) atomicAdd(gW3 + t * 16 + i, acc[i]);
 }
 
-// layer 1 weight gradient: gW1[t][i][o] += sum_q x[i][q + d(t)] gh1[q][o],
-// q in (S-2)^3, x side S.  Grid (chunks, 27 taps).
-__global__ void __launch_bounds__(256) l1_wgrad_cl(const float *__restrict__ x, const uint16_t *__restrict__ gh1,
-                                                    float *__restrict__ gW1, int B, int S)
+// layer 1: gW1[t][i][o] += sum_q x[i][q + d(t)] gh1[q][o], q in (S-2)^3, x side S
+__global__ void __launch_bounds__(WG_THREADS) l1_wgrad_cl(const float *__restrict__ x,
+                                                           const uint16_t *__restrict__ gh1, float *__restrict__ gW1,
+                                                           int B, int S)
 {
-    const int t = blockIdx.y, dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
-    const int So = S - 2;
-    const int64_t pero = (int64_t)So * So * So, s3 = (int64_t)S * S * S, total = pero * B;
+    const int t = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+    const int So = S - 2, plane = So * So;
+    const int64_t s3 = (int64_t)S * S * S;
     float acc[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) acc[i] = 0.f;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
-        const int b = (int)(q / pero);
-        const int64_t c = q - b * pero;
-        const int xx = (int)(c % So), yy = (int)((c / So) % So), zz = (int)(c / ((int64_t)So * So));
-        const int64_t e = (int64_t)b * 2 * s3 + (xx + dx) + (int64_t)S * ((yy + dy) + (int64_t)S * (zz + dz));
-        const float v0 = __ldg(x + e), v1 = __ldg(x + e + s3);
-        float g[16];
-        unpack16(gh1 + q * 16, g);
+    for (int pz = blockIdx.x; pz < B * So; pz += gridDim.x) {
+        const int b = pz / So, zz = pz - b * So;
+        const uint16_t *gp = gh1 + (int64_t)pz * plane * 16;
+        const float *xp = x + (int64_t)b * 2 * s3 + dx + (int64_t)S * (dy + (int64_t)S * (zz + dz));
+        int xx = lane, yy = 0;
+        for (int idx = lane; idx < plane; idx += 32) {
+            while (xx >= So) {
+                xx -= So;
+                ++yy;
+            }
+            const int64_t e = xx + (int64_t)S * yy;
+            const float v0 = __ldg(xp + e), v1 = __ldg(xp + e + s3);
+            float g[16];
+            unpack16(gp + (int64_t)idx * 16, g);
 #pragma unroll
-        for (int o = 0; o < 16; ++o) {
-            acc[o] = fmaf(v0, g[o], acc[o]);
-            acc[16 + o] = fmaf(v1, g[o], acc[16 + o]);
+            for (int o = 0; o < 16; ++o) {
+                acc[o] = fmaf(v0, g[o], acc[o]);
+                acc[16 + o] = fmaf(v1, g[o], acc[16 + o]);
+            }
+            xx += 32;
         }
     }
     warp_sum(acc);
-    if ((threadIdx.x & 31) == 0)
+    if (lane == 0)
 #pragma unroll
         for (int i = 0; i < 32; ++i) atomicAdd(gW1 + t * 32 + i, acc[i]);
 }
@@ -490,6 +558,8 @@ cn_status train_forward_tc(const TrainBufs &T, const float *x, const float *W, i
     using namespace nntr;
     const int S = P + 8, S1 = S - 2, S2 = S - 4, S3 = S - 6;
     const float *W1 = W, *W2 = W + 27 * 2 * 16, *W3 = W + 27 * 2 * 16 + 27 * 16 * 16;
+    if ((int64_t)B * S * S * S >= (int64_t)1 << 31)
+        return fail(CN_ERR_UNSUPPORTED, "learned smoother training: batch too large for 32-bit cell indices");
     cn_status s;
     // packed B tiles of the hidden layer: forward, backward-data
     if ((s = pack_weights(W2, 16, 16, T.wfwd, st)) != CN_OK) return s;
@@ -521,7 +591,10 @@ cn_status train_backward_tc(const TrainBufs &T, const float *x, const float *W, 
     float *gW1 = gW, *gW2 = gW + 27 * 2 * 16, *gW3 = gW + 27 * 2 * 16 + 27 * 16 * 16;
     cn_status s;
     CN_CUDA_TRY(cudaMemsetAsync(gW, 0, sizeof(float) * (27 * 2 * 16 + 27 * 16 * 16 + 27 * 16), st));
-    l3_wgrad_cl<<<dim3(grid_of((int64_t)B * S3 * S3 * S3, 256, 64), 27), 256, 0, st>>>(T.h2, T.gc, gW3, B, S2);
+    int dev = 0, sms = 148;
+    CN_CUDA_TRY(cudaGetDevice(&dev));
+    CN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    l3_wgrad_cl<<<grid_of((int64_t)B * S3, 1, sms), WG_THREADS, 0, st>>>(T.h2, T.gc, gW3, B, S2);
     l3_bwd_data_cl<<<grid_of((int64_t)B * S2 * S2 * S2, 128, 148 * 64), 128, 0, st>>>(T.gc, W3, T.h2, T.gh2, B, S2);
     CN_CUDA_TRY(cudaGetLastError());
     Args w = {};
@@ -545,7 +618,7 @@ cn_status train_backward_tc(const TrainBufs &T, const float *x, const float *W, 
     d.total = (int64_t)B * S1 * S1 * S1;
     d.err = T.err;
     if ((s = launch_patch<BWD>(d, st)) != CN_OK) return s;
-    l1_wgrad_cl<<<dim3(grid_of((int64_t)B * S1 * S1 * S1, 256, 64), 27), 256, 0, st>>>(x, T.gh1, gW1, B, S);
+    l1_wgrad_cl<<<grid_of((int64_t)B * S1, 1, sms), WG_THREADS, 0, st>>>(x, T.gh1, gW1, B, S);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
