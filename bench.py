@@ -27,6 +27,10 @@ the launching stream); ``e2e`` is the same metric through the C ABI with the
 input uploaded from pinned host memory and the outputs read back every step.
 Multi-GPU runs are independent replicas (the path does not shard across GPUs
 in this build): scaling "weak", value = all ranks' cells / max-over-ranks time.
+
+The default run (c2 at N = 1) then times the other workloads briefly on the
+same GPU (``companions``: 3 warm-up and 5 timed steps each; --no-companions
+skips them, as profiling runs do).
 """
 from __future__ import annotations
 
@@ -719,9 +723,10 @@ class C5:
     )
 
     def _learned(self):
-        """Train the learned smoother (untimed) on 2000 residual/error pairs
-        of the plain V-cycle, then time solves with it under each schedule of
-        LEARNED_SCHEDULES and the plain solve, on the same problem."""
+        """Train the learned smoother (untimed in the metric; its wall time is
+        reported) on 2000 residual/error pairs of the plain V-cycle, then time
+        solves with it under each schedule of LEARNED_SCHEDULES and the plain
+        solve, on the same problem."""
         cn, torch = self.cn, self.torch
         try:
             x, k, r, P = cn.learned.collect_patches(self.mg, self.f, cycles=8, per_snapshot=125, max_patches=2000,
@@ -755,8 +760,13 @@ class C5:
                 del m2
             ok = [t for t in table[1:] if t["relres"] <= self.rtol]
             best = min(ok, key=lambda t: t["ms_per_solve"]) if ok else None
+            nbatches = 8 * (npatch // 32)
             return dict(train_patches=npatch, train_loss=round(float(loss), 4),
-                        train_seconds=round(train_s, 2), schedules=table,
+                        train_seconds=round(train_s, 2), train_ms_per_batch=round(1e3 * train_s / nbatches, 3),
+                        training="hidden layer forward, data and weight gradients on tcgen05 (BF16 operands, "
+                                 "FP32 accumulation); first and last layers on the CUDA cores; 8 epochs of "
+                                 "batches of 32, Adam",
+                        schedules=table,
                         best=best["schedule"] if best else None,
                         ms_per_solve=best["ms_per_solve"] if best else None,
                         cycles=best["cycles"] if best else None,
@@ -1199,7 +1209,81 @@ def run_ours(args, world, rank, local, pg):
         out["config"]["learned_smoother"] = W.learned
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = W.cpu_sample(os.cpu_count() or 1)
+    if world == 1 and args.workload == DEFAULT_WORKLOAD and not args.no_companions and not args.blocks:
+        W = None
+        import gc
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        out["companions"] = run_companions(args, local)
     return out
+
+
+# The other workloads, timed briefly on the same GPU after the main one so
+# that one default run measures them all (rank 0 at N = 1 only).
+COMPANIONS = ("c1", "c4", "c5", "c3")
+
+
+def run_companions(args, local):
+    """Device-timed short runs of COMPANIONS: 3 warm-up steps, then
+    args.companion_steps steps (L2 handled as in the main run); value,
+    roofline fractions against the measured peaks, and each workload's own
+    extras (the C5 learned-smoother table, the C3 layout and schedule)."""
+    import gc
+
+    import torch
+
+    from cubismnova_b200 import _lib
+    peaks = measured_peaks()
+    res = {}
+    for name in COMPANIONS:
+        t0 = time.perf_counter()
+        W = None
+        try:
+            W = WORKLOADS[name]()
+            stream = torch.cuda.Stream()
+            L = W.launches_per_step
+            for _ in range(3):
+                if W.needs_flush():
+                    W.flush(stream)
+                W.step(stream)
+            torch.cuda.synchronize()
+            k = max(1, args.companion_steps)
+            ev = [[torch.cuda.Event(enable_timing=True) for _ in range(L + 1)] for _ in range(k)]
+            for i in range(k):
+                if W.needs_flush():
+                    W.flush(stream)
+                W.step(stream, ev[i])
+            torch.cuda.synchronize()
+            launch_ms = np.array([[ev[i][j].elapsed_time(ev[i][j + 1]) for j in range(L)] for i in range(k)])
+            ms = float(launch_ms.sum())
+            unit = getattr(W, "unit", "Gcell-updates/s")
+            d = dict(metric=getattr(W, "metric", unit), value=round(W.updates_per_step * k / (ms / 1e3) / 1e9, 4),
+                     unit=unit, dtype=W.dtype, ms_per_step=round(ms / k, 4), steps=k, warmup=3, cells=W.cells,
+                     workload=W.desc)
+            ach = W.bytes_per_cell_step * W.cells / L / (ms / (k * L) / 1e3) / 1e9
+            d["hbm"] = dict(achieved_gbs=round(ach, 1), frac=round(ach / peaks["hbm_gbs"], 4),
+                            algorithmic_bytes_per_cell_step=W.bytes_per_cell_step)
+            flops = getattr(W, "flops_per_cell_stage", None)
+            if flops:
+                peak_tf = _lib.fma_peak_tflops(_lib.CN_FLOAT64 if W.dtype == "f64" else _lib.CN_FLOAT32)
+                tf = flops * W.updates_per_step / (ms / k / 1e3) / 1e12
+                d["alu"] = dict(achieved_tflops=round(tf, 2), peak_tflops=round(peak_tf, 2),
+                                frac=round(tf / peak_tf, 4))
+            if getattr(W, "learned", None) is not None:
+                d["learned_smoother"] = W.learned
+            for extra in ("layout", "schedule"):
+                if getattr(W, extra, None) is not None:
+                    d[extra] = getattr(W, extra)
+        except Exception as e:  # reported, not fatal: the main line stands
+            d = dict(error=str(e)[:300])
+        d["wall_seconds"] = round(time.perf_counter() - t0, 1)
+        res[name] = d
+        del W
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return res
 
 
 def run_reference(args, world, rank):
@@ -1310,6 +1394,9 @@ def main():
     ap.add_argument("--traffic", type=float, default=None,
                     help="ncu DRAM bytes per launch of the dominant kernel, if measured")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-companions", action="store_true",
+                    help="skip the short runs of the other workloads that follow the default one")
+    ap.add_argument("--companion-steps", type=int, default=5, help="timed steps of each companion workload")
     ap.add_argument("--no-learned", action="store_true",
                     help="c5: skip training and timing the learned smoother")
     ap.add_argument("--no-autotune", action="store_true",
