@@ -668,6 +668,7 @@ class C5:
     solve from p = 0.  The learned smoother (trained untimed on this problem's
     residual patches, replacing Jacobi on the finest level) is timed beside it
     and reported in the config."""
+    nn_training = "tensor"  # bench.py --nn-training fp32: the CUDA-core training path
     name = "c5"
     desc = ("Poisson div(k grad p) = f, 256^3 cells as 8^3 blocks of 32^3, k = box-filtered lognormal "
             "(sigma 0.5), f = 32 Gaussians; multigrid V(2,2) weighted Jacobi (omega 0.8), FP32 cycles in "
@@ -733,6 +734,7 @@ class C5:
                                                     seed=5)
             npatch = int(x.shape[0])
             nn = cn.learned.LearnedSmoother(seed=1, omega=0.8, init_scale=1e-3)
+            nn.set_training(self.nn_training)
             ih2 = 1.0 / self.k.getCellSize()[0] ** 2
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -763,9 +765,10 @@ class C5:
             nbatches = 8 * (npatch // 32)
             return dict(train_patches=npatch, train_loss=round(float(loss), 4),
                         train_seconds=round(train_s, 2), train_ms_per_batch=round(1e3 * train_s / nbatches, 3),
-                        training="hidden layer forward, data and weight gradients on tcgen05 (BF16 operands, "
-                                 "FP32 accumulation); first and last layers on the CUDA cores; 8 epochs of "
-                                 "batches of 32, Adam",
+                        training=("hidden layer forward, data and weight gradients on tcgen05 (BF16 operands, "
+                                  "FP32 accumulation); first and last layers on the CUDA cores"
+                                  if self.nn_training == "tensor" else "FP32 on the CUDA cores throughout")
+                        + "; 8 epochs of batches of 32, Adam",
                         schedules=table,
                         best=best["schedule"] if best else None,
                         ms_per_solve=best["ms_per_solve"] if best else None,
@@ -1102,6 +1105,8 @@ def run_ours(args, world, rank, local, pg):
     if args.blocks:
         cls = type(cls.__name__, (cls,), {"nb": tuple(args.blocks),
                                           "desc": cls.desc + f" [reduced: {tuple(args.blocks)} blocks]"})
+    if getattr(args, "nn_training", None) and hasattr(cls, "nn_training"):
+        cls = type(cls.__name__, (cls,), {"nn_training": args.nn_training})
     if getattr(args, "no_autotune", False) and hasattr(cls, "autotune"):
         cls = type(cls.__name__, (cls,), {"autotune": False})
     W = cls()
@@ -1399,6 +1404,8 @@ def main():
     ap.add_argument("--companion-steps", type=int, default=5, help="timed steps of each companion workload")
     ap.add_argument("--no-learned", action="store_true",
                     help="c5: skip training and timing the learned smoother")
+    ap.add_argument("--nn-training", default=None, choices=["tensor", "fp32"],
+                    help="c5: training arithmetic of the learned smoother (default tensor)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="c3: keep the default schedule instead of autotuning it (profiling runs)")
     ap.add_argument("--blocks", type=int, nargs=3, default=None,
