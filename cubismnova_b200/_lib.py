@@ -54,6 +54,8 @@ _SIGS = {
     "cn_grid_destroy": (_I, [_P]),
     "cn_grid_layout": (_I, [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_size_t)]),
     "cn_grid_cell_size": (_I, [_P, _D3]),
+    "cn_grid_device_error": (_I, [_P, C.POINTER(C.c_int), _I]),
+    "cn_debug_wait_timeout": (_I, [_P, _I, _P]),
     "cn_grid_shape": (_I, [_P, _I3]),
     "cn_grid_data": (_I, [_P, _I, C.POINTER(_P)]),
     "cn_grid_upload": (_I, [_P, _I, _P, C.c_size_t, _P]),

@@ -83,6 +83,9 @@ namespace cn {
 cn_status fail(cn_status s, const std::string &msg);
 cn_status ok();
 cn_status cuda_fail(cudaError_t e, const char *what);
+// reads a grid's device error word after the caller synchronised; nonzero:
+// CN_ERR_DEVICE (the word is cleared)
+cn_status grid_check_error(cn_grid *g);
 
 #define CN_CUDA_TRY(call)                                                      \
     do {                                                                       \

@@ -300,6 +300,7 @@ cn_status cn_euler_rk3_stage(cn_grid *bcsrc, cn_grid *Us, cn_grid *Un, cn_grid *
         double t[5];
         CN_CUDA_TRY(cudaMemcpyAsync(t, sc->totals, sizeof(t), cudaMemcpyDeviceToHost, st));
         CN_CUDA_TRY(cudaStreamSynchronize(st));
+        if ((s = grid_check_error(const_cast<cn_grid *>(Us))) != CN_OK) return s;
         for (int c = 0; c < 5; ++c) sums_out[c] = t[c] * vol;
     }
     return CN_OK;
@@ -435,6 +436,7 @@ extern "C" cn_status cn_euler_rk3_stage_noalloc(cn_grid *bcsrc, cn_grid *Us, cn_
     double t[5];
     CN_CUDA_TRY(cudaMemcpyAsync(t, totals, sizeof(t), cudaMemcpyDeviceToHost, st));
     CN_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((s = grid_check_error(const_cast<cn_grid *>(Us))) != CN_OK) return s;
     const double vol = Us->h[0] * Us->h[1] * Us->h[2];
     for (int c = 0; c < 5; ++c) sums_out[c] = t[c] * vol;
     return CN_OK;

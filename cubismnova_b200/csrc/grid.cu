@@ -6,6 +6,7 @@
 // (Block/Field.h:437-442) live on the host and are flattened into CSR tables
 // on the device when a kernel first needs them.
 #include "cn_internal.h"
+#include "cn_tma.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -22,6 +23,16 @@ cn_status fail(cn_status s, const std::string &msg)
 }
 
 cn_status ok() { return CN_OK; }
+
+cn_status grid_check_error(cn_grid *g)
+{
+    if (!g || !g->d_err) return CN_OK;
+    int e = 0;
+    CN_CUDA_TRY(cudaMemcpy(&e, g->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e == 0) return CN_OK;
+    CN_CUDA_TRY(cudaMemset(g->d_err, 0, sizeof(int)));
+    return fail(CN_ERR_DEVICE, "a kernel on this grid gave up a bounded wait (error word " + std::to_string(e) + ")");
+}
 
 cn_status cuda_fail(cudaError_t e, const char *what)
 {
@@ -387,6 +398,41 @@ cn_status cn_grid_entity(const cn_grid *g, int *entity, int block_cells[3])
     if (entity) *entity = g->entity;
     if (block_cells)
         for (int d = 0; d < 3; ++d) block_cells[d] = g->cells[d];
+    return CN_OK;
+}
+
+// One CTA waits `polls` times on an mbarrier that nothing completes, as a
+// kernel whose TMA copy or tensor-core pipeline never finished would, then
+// records the timeout in the error word.
+__global__ void wait_timeout_kernel(int polls, int *err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool done = false;
+        for (int i = 0; i < polls && !done; ++i) done = mbar_try_wait(&bar, 0);
+        if (!done && err) atomicExch(err, kDevErrTimeout);
+    }
+}
+
+cn_status cn_grid_device_error(cn_grid *g, int *word, int clear)
+{
+    if (!g || !word) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    CN_CUDA_TRY(cudaDeviceSynchronize());
+    CN_CUDA_TRY(cudaMemcpy(word, g->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (clear && *word) CN_CUDA_TRY(cudaMemset(g->d_err, 0, sizeof(int)));
+    return CN_OK;
+}
+
+cn_status cn_debug_wait_timeout(cn_grid *g, int polls, void *stream)
+{
+    if (!g || polls < 1 || polls > (1 << 20)) return fail(CN_ERR_INVALID_ARGUMENT, "cn_debug_wait_timeout: bad argument");
+    wait_timeout_kernel<<<1, 32, 0, as_stream(stream)>>>(polls, g->d_err);
+    CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
 

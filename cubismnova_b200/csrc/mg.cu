@@ -1039,6 +1039,10 @@ cn_status cn_mg_solve(cn_mg *m, const cn_grid *f, cn_grid *p64, double rtol, int
         rel = std::sqrt(rr) / fn;
         ++c;
     }
+    // the learned smoother's tensor-core layers record bounded-wait failures
+    // in the level grids' error words (cn_mg_residual has synchronised)
+    for (int l = 0; l < m->nlevels; ++l)
+        if ((s = grid_check_error(m->p[l])) != CN_OK) return s;
     if (cycles) *cycles = c;
     if (relres) *relres = rel;
     return CN_OK;

@@ -222,6 +222,14 @@ class Cartesian:
         _lib.check(_lib.lib().cn_grid_cell_size(self._h, h))
         return tuple(h)
 
+    def device_error(self, clear: bool = True) -> int:
+        """The grid's device error word (cn_grid_device_error): 0, or the code
+        a kernel recorded when it gave up a bounded wait; waits for the device
+        and, with clear, resets the word."""
+        w = C.c_int()
+        _lib.check(_lib.lib().cn_grid_device_error(self._h, C.byref(w), 1 if clear else 0))
+        return w.value
+
     def flat_index(self, p):
         if isinstance(p, (int, np.integer)):
             if not 0 <= int(p) < self.size():

@@ -128,6 +128,18 @@ cn_status cn_grid_shape(const cn_grid *g, int info[8]);
 /* Mesh::StructuredUniform cell size h = (end-begin)/cells
  * (Mesh/StructuredUniform.h:61, :333-336). */
 cn_status cn_grid_cell_size(const cn_grid *g, double h[3]);
+/* Device error word of a grid.  A kernel that reads the grid and gives up a
+ * bounded wait (a TMA copy or tensor-core pipeline that did not complete)
+ * records a nonzero word instead of hanging (1: a wait ran out, 2: a table
+ * entry out of range, 3: unusable launch configuration) and skips its
+ * results.  Waits for the device; clear != 0 resets the word.  The calls that
+ * synchronise anyway (cn_euler_rk3_stage with sums, the no-allocation stage,
+ * cn_mg_solve) return CN_ERR_DEVICE when it is set. */
+cn_status cn_grid_device_error(cn_grid *g, int *word, int clear);
+/* Test hook of that path: one CTA polls `polls` times (1..2^20) an mbarrier
+ * that nothing completes, then records 1 in g's error word.  Stream-ordered;
+ * no fault, the context stays usable. */
+cn_status cn_debug_wait_timeout(cn_grid *g, int polls, void *stream);
 /* Device pointer of one component (component-major SoA). */
 cn_status cn_grid_data(cn_grid *g, int comp, void **device_ptr);
 /* Host <-> device copy of one component, reference SoA order; nbytes must be
