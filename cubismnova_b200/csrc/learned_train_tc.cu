@@ -8,35 +8,33 @@
 // S1 = S - 2, h2 side S2 = S - 4, the output y side S3 = S - 6 (valid 3x3x3
 // convolutions; tap d = (dx, dy, dz) in {0,1,2}^3, index dx + 3 dy + 9 dz).
 //
-// The three GEMMs of the hidden layer share one operand form.  A chunk of
-// 128 consecutive output cells (linear over batch and cube) gathers, for
-// every tap t and channel half h, a plane of 128 rows x 16 bytes: row r =
-// channels 8h..8h+7 of the source cell (cell r) + d(t) + shift, zero outside
-// the source cube.  Each row is one 16-byte asynchronous copy (cp.async) of
-// channels-last data, so no transposition is needed:
+// The hidden layer's three GEMMs:
 //   forward        out[q][co] = sum_{t,ci} h1[q + d][ci] W[t][ci][co]
-//                  A = plane pair (t, 0..1) read K-major (M = 128 cells, K =
-//                  16 channels: the two planes are the two 8-channel K
-//                  chunks), B = W[t] (N = 16 output channels); 27 MMAs.
 //   backward-data  gin[c][ci] = sum_e gout[c - 2 + e][co] W[26 - e][ci][co],
-//                  the same with the source gout, shift -2, taps flipped and
-//                  W transposed; the ReLU mask of the layer's input applied
-//                  in the epilogue.
-//   weight grad    gW[t][ci][co] = sum_q h1[q + d][ci] gout[q][co]: the
-//                  forward's planes read MN-major (M = (tap, channel), 8 taps
-//                  = 16 planes per M = 128 tile, planes one SBO apart; K =
-//                  cells, 16 rows per MMA), B = the chunk's gout rows
-//                  MN-major (N = 16 channels); 4 tiles x 8 MMAs per chunk,
-//                  accumulated over all chunks of a CTA in tensor memory and
-//                  added to gW with atomics at the end.  Rows of taps >= 27 in
-//                  the last tile read whatever the buffer holds; those
-//                  accumulator rows are never read.
-// Taps are gathered in 4 groups of 8 into two 32 KB buffers, one group
-// ahead: the copies of group i + 1 are in flight while group i's MMAs
-// (issued by one thread, committed to the buffer's mbarrier) run.  Lanes 2i
-// and 2i+1 of a warp copy the two channel halves of one row, so one copy
-// instruction reads 512 contiguous bytes.  Persistent CTAs, two per SM;
-// every wait bounded (an error word is set and the CTA stops issuing).
+//                  the forward's form with the source gout, shift -2, taps
+//                  flipped and W transposed; the ReLU mask of the layer's
+//                  input applied in the epilogue
+// run brick-staged (brick_tc_kernel): a brick of output cells with its
+// source region in shared memory, each tap's A operand the same rows
+// shifted (K-major, M = 128 cells, K = 16 channels, N = 16), 27 MMAs per
+// 128-row tile.
+//   weight grad    gW[t][ci][co] = sum_q h1[q + d][ci] gout[q][co]
+// needs M = (tap, channel), which no shifted descriptor gives (the tap
+// offsets are not evenly spaced): wgrad_tc_kernel gathers, for a chunk of
+// 128 consecutive output cells (linear over batch and cube), per tap t and
+// channel half h a plane of 128 rows x 16 bytes (row r = channels
+// 8h..8h+7 of source cell (cell r) + d(t), zero outside the cube; one
+// 16-byte cp.async each), reads them MN-major (8 taps = 16 planes per
+// M = 128 tile, planes one SBO apart; K = cells, 16 rows per MMA) against
+// the chunk's gout rows (MN-major B, N = 16): 4 tiles x 8 MMAs per chunk,
+// accumulated over all chunks of a CTA in tensor memory, added to gW with
+// atomics at the end.  Rows of taps >= 27 in the last tile read whatever
+// the buffer holds; those accumulator rows are never read.  Taps are
+// gathered in 4 groups of 8 into two 32 KB buffers, one group ahead of the
+// MMAs (issued by one thread, committed to the buffer's mbarrier); lanes 2i
+// and 2i+1 copy the two channel halves of one row.  Persistent CTAs, two
+// per SM.  Every wait in both kernels is bounded (an error word is set and
+// the CTA stops issuing).
 #include "cn_internal.h"
 #include "cn_tc.cuh"
 #include "cn_tma.cuh"
@@ -56,15 +54,15 @@ constexpr uint32_t PL = ROWS * 16;               // bytes of one plane
 constexpr uint32_t GBUF = 2 * GT * PL;           // one group buffer: 16 planes, 32 KB
 constexpr int NT = 2 * ROWS;                     // two threads per row (channel halves)
 constexpr uint32_t WBYTES = 27 * 512;            // packed weights of one layer
-constexpr uint32_t GOUT_BYTES = 2 * PL;          // weight gradient: gout rows of a chunk (2 planes)
-constexpr size_t OFF_W = 2 * (size_t)GBUF;       // weights (forward / backward-data) or gout buffers
-constexpr size_t OFF_BAR = OFF_W + (WBYTES > 2 * GOUT_BYTES ? WBYTES : 2 * GOUT_BYTES);
+constexpr uint32_t GOUT_BYTES = 2 * PL;          // gout rows of a chunk (2 planes)
+constexpr size_t OFF_G = 2 * (size_t)GBUF;       // two gout buffers
+constexpr size_t OFF_BAR = OFF_G + 2 * GOUT_BYTES;
 constexpr size_t SMEM = OFF_BAR + 4 * 8 + 16;
 constexpr uint32_t IDESC_K = tc::idesc_bf16_f32(128, 16);
 // both operands MN-major (bits 15 and 16)
 constexpr uint32_t IDESC_MN = tc::idesc_bf16_f32(128, 16) | (1u << 15) | (1u << 16);
 
-enum { FWD = 0, BWD = 1, WGRAD = 2 };
+enum { FWD = 0, BWD = 1 };
 
 struct Args {
     const uint16_t *src;  // gathered activations [B][Sin^3][16] BF16
@@ -107,33 +105,28 @@ __device__ __forceinline__ void cp16(void *dst, const void *src, uint32_t src_by
 
 template <int V> using ic = std::integral_constant<int, V>;
 
-template <int MODE>
-__global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__ Args a)
+__global__ void __launch_bounds__(NT, 2) wgrad_tc_kernel(const __grid_constant__ Args a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *Abuf = smem;                 // [2][16 planes][ROWS][16 B]
-    unsigned char *Wb = smem + OFF_W;           // forward / backward-data weights; weight gradient: [2][2][ROWS][16 B]
+    unsigned char *Gbuf = smem + OFF_G;         // [2][2 planes][ROWS][16 B]
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OFF_BAR);
-    uint64_t *empty = bars, *dready = bars + 2; // empty[2]: group buffer free; dready: accumulator complete
+    uint64_t *empty = bars, *done = bars + 2;   // empty[2]: group buffer free; done: all MMAs complete
     uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 4);
-    int *flag = reinterpret_cast<int *>(slot + 1); // [0]: buffer waits, [1]: accumulator waits
-    constexpr uint32_t TCOLS = MODE == WGRAD ? 64 : 32;
+    int *flag = reinterpret_cast<int *>(slot + 1); // [0]: buffer waits, [1]: the final wait
+    constexpr uint32_t TCOLS = 64;                 // 4 accumulator tiles x 16 columns
     const int r = threadIdx.x, warp = r >> 5;
 
     if (r == 0) {
         mbar_init(empty, 1);
         mbar_init(empty + 1, 1);
-        mbar_init(dready, 1);
+        mbar_init(done, 1);
         fence_mbar_init();
     }
     if (warp == 0) {
         tc::tmem_alloc(slot, TCOLS);
         tc::tmem_relinquish();
     }
-    if (MODE != WGRAD)
-        for (int i = r; i < (int)(WBYTES / 16); i += NT)
-            reinterpret_cast<uint4 *>(Wb)[i] = __ldg(reinterpret_cast<const uint4 *>(a.w) + i);
-    fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -146,33 +139,33 @@ __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__
     // gather: thread r copies channel half hh of row rho (a warp: 16 rows =
     // 512 contiguous source bytes where the cells are contiguous)
     const int hh = r & 1, rho = r >> 1;
-    int64_t rL = 0, roff = 0; // the row's cell; source element of its tap (0, 0, 0) (may lie outside)
+    int64_t rL = 0, roff = 0; // the row's cell; source element of its tap (0, 0, 0)
     uint32_t mx = 0, my = 0, mz = 0; // per axis: offsets k = 0..2 with the source inside the cube
     auto set_row = [&](int j) {
         rL = (blockIdx.x + (int64_t)j * gridDim.x) * ROWS + rho;
         mx = my = mz = 0;
         if (rL < a.total) {
             const CubeIdx ci = cube_idx((uint32_t)rL, (uint32_t)a.Sout, so3);
-            const int x0 = ci.x + a.shift, y0 = ci.y + a.shift, z0 = ci.z + a.shift;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
-                mx |= ((unsigned)(x0 + k) < (unsigned)a.Sin ? 1u : 0u) << k;
-                my |= ((unsigned)(y0 + k) < (unsigned)a.Sin ? 1u : 0u) << k;
-                mz |= ((unsigned)(z0 + k) < (unsigned)a.Sin ? 1u : 0u) << k;
+                mx |= ((unsigned)(ci.x + k) < (unsigned)a.Sin ? 1u : 0u) << k;
+                my |= ((unsigned)(ci.y + k) < (unsigned)a.Sin ? 1u : 0u) << k;
+                mz |= ((unsigned)(ci.z + k) < (unsigned)a.Sin ? 1u : 0u) << k;
             }
-            roff = (int64_t)ci.b * si3 + x0 + sin1 * y0 + sin2 * z0;
+            roff = (int64_t)ci.b * si3 + ci.x + sin1 * ci.y + sin2 * ci.z;
         }
     };
     auto gather = [&](int j, auto G) {
         constexpr int g = decltype(G)::value;
-        if (g == 0) set_row(j);
-        unsigned char *A = Abuf + (g & 1) * GBUF;
-        if (MODE == WGRAD && g == 0) {
+        if (g == 0) {
+            set_row(j);
             // the chunk's gradient rows (buffer j & 1 was last read by chunk j - 2's
             // MMAs, complete before item NG j - 2's)
             const bool v = rL < a.total;
-            cp16(Wb + (j & 1) * GOUT_BYTES + hh * PL + rho * 16, v ? a.gout + rL * 16 + 8 * hh : a.gout, v ? 16u : 0u);
+            cp16(Gbuf + (j & 1) * GOUT_BYTES + hh * PL + rho * 16, v ? a.gout + rL * 16 + 8 * hh : a.gout,
+                 v ? 16u : 0u);
         }
+        unsigned char *A = Abuf + (g & 1) * GBUF;
 #pragma unroll
         for (int tl = 0; tl < GT; ++tl) {
             const int t = g * GT + tl;
@@ -186,9 +179,8 @@ __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     // one item: gather the next (after its buffer's previous MMAs), wait
-    // for this item's copies, issue its MMAs; after the last group of a
-    // chunk (forward / backward-data) drain the accumulator.  False when a
-    // bounded wait ran out.
+    // for this item's copies, issue its MMAs.  False when a bounded wait ran
+    // out.
     auto item = [&](int j, auto G) -> bool {
         constexpr int g = decltype(G)::value;
         const int i = NG * j + g;
@@ -210,66 +202,14 @@ __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__
         __syncthreads();
         if (r == 0) {
             tc::fence_after_sync();
-            const uint32_t A = smem_u32(Abuf + (g & 1) * GBUF);
-            if (MODE == WGRAD) {
-                const uint32_t Gs = smem_u32(Wb + (j & 1) * GOUT_BYTES);
+            const uint32_t A = smem_u32(Abuf + (g & 1) * GBUF), Gs = smem_u32(Gbuf + (j & 1) * GOUT_BYTES);
 #pragma unroll
-                for (int ks = 0; ks < ROWS / 16; ++ks) {
-                    const uint64_t da = tc::smem_desc(A + 256u * ks, 128u, PL);
-                    const uint64_t db = tc::smem_desc(Gs + 256u * ks, 128u, PL);
-                    tc::mma_bf16(tbase + 16u * g, da, db, IDESC_MN, (j > 0 || ks > 0) ? 1u : 0u);
-                }
-            } else {
-#pragma unroll
-                for (int tl = 0; tl < GT; ++tl) {
-                    const int t = g * GT + tl;
-                    if (t < 27) {
-                        const uint64_t da = tc::smem_desc(A + 2u * tl * PL, PL, 128u);
-                        const uint64_t db = tc::smem_desc(smem_u32(Wb) + 512u * t, 256u, 128u);
-                        tc::mma_bf16(tbase, da, db, IDESC_K, t > 0 ? 1u : 0u);
-                    }
-                }
+            for (int ks = 0; ks < ROWS / 16; ++ks) {
+                const uint64_t da = tc::smem_desc(A + 256u * ks, 128u, PL);
+                const uint64_t db = tc::smem_desc(Gs + 256u * ks, 128u, PL);
+                tc::mma_bf16(tbase + 16u * g, da, db, IDESC_MN, (j > 0 || ks > 0) ? 1u : 0u);
             }
             tc::mma_commit(empty + (g & 1));
-            if (MODE != WGRAD && g == NG - 1) tc::mma_commit(dready);
-        }
-        if constexpr (MODE != WGRAD && g == NG - 1) {
-            // ---- epilogue of chunk j: warp w reads TMEM lanes 32 (w % 4) + lane
-            // (= the chunk's row m), columns (channels) 8 (w / 4) .. + 7
-            const int m = 32 * (warp & 3) + (r & 31), ch = 8 * (warp >> 2);
-            const int64_t L = (blockIdx.x + (int64_t)j * gridDim.x) * ROWS + m;
-            if (r == 0) flag[1] = mbar_wait_bounded(dready, j & 1) ? 1 : 0;
-            __syncthreads();
-            if (!flag[1]) return false;
-            tc::fence_after_sync();
-            float v[8];
-            tc::tmem_ld8(tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)ch, v);
-            tc::fence_before_sync();
-            if (L < a.total) {
-                uint32_t h[4];
-                if (MODE == BWD) {
-                    const uint4 mk = *reinterpret_cast<const uint4 *>(a.act + L * 16 + ch);
-                    const uint32_t mw[4] = {mk.x, mk.y, mk.z, mk.w};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        // BF16 = the top 16 bits of an FP32: > 0 test on the widened value
-                        const float lo = __uint_as_float(mw[q] << 16), hi = __uint_as_float(mw[q] & 0xFFFF0000u);
-                        h[q] = (uint32_t)bf16_bits(lo > 0.f ? v[2 * q] : 0.f) |
-                               ((uint32_t)bf16_bits(hi > 0.f ? v[2 * q + 1] : 0.f) << 16);
-                    }
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float p = v[2 * q], u = v[2 * q + 1];
-                        if (a.relu) {
-                            p = fmaxf(p, 0.f);
-                            u = fmaxf(u, 0.f);
-                        }
-                        h[q] = (uint32_t)bf16_bits(p) | ((uint32_t)bf16_bits(u) << 16);
-                    }
-                }
-                *reinterpret_cast<uint4 *>(a.out + L * 16 + ch) = make_uint4(h[0], h[1], h[2], h[3]);
-            }
         }
         return true;
     };
@@ -279,13 +219,13 @@ __global__ void __launch_bounds__(NT, 2) patch_tc_kernel(const __grid_constant__
     for (int j = 0; j < nch && ok; ++j)
         ok = item(j, ic<0>{}) && item(j, ic<1>{}) && item(j, ic<2>{}) && item(j, ic<3>{});
     asm volatile("cp.async.wait_all;" ::: "memory"); // nothing in flight past this point
-    // ---- weight gradient: wait for every MMA of this CTA, then add the 4
-    // accumulator tiles (row m = 16 (tap - 8 g) + ci, column co) to gW; warp
-    // w reads rows 32 (w % 4) + lane, columns 8 (w / 4) .. + 7
-    if (MODE == WGRAD && ok && nitems > 0) {
+    // ---- wait for every MMA of this CTA, then add the 4 accumulator tiles
+    // (row m = 16 (tap - 8 g) + ci, column co) to gW; warp w reads rows
+    // 32 (w % 4) + lane, columns 8 (w / 4) .. + 7
+    if (ok && nitems > 0) {
         if (r == 0) {
-            tc::mma_commit(dready);
-            flag[1] = mbar_wait_bounded(dready, 0) ? 1 : 0;
+            tc::mma_commit(done);
+            flag[1] = mbar_wait_bounded(done, 0) ? 1 : 0;
         }
         __syncthreads();
         ok = flag[1] != 0;
@@ -319,6 +259,190 @@ __global__ void pack_bwd_kernel(const float *W, uint16_t *out)
     const int e = i / 256, rr = i % 256;
     const int kc = rr / 128, ci = (rr / 8) % 16, j = rr % 8;
     out[i] = bf16_bits(W[((26 - e) * 16 + ci) * 16 + kc * 8 + j]);
+}
+
+// ------------------------------------------------ brick-staged forward
+// The forward and data-gradient GEMMs without im2col, as the grid inference
+// kernel does it: a CTA owns a brick of BX x BY x BZ output cells of one
+// patch (BX the whole row) and stages the source region around it, (BX+2) x
+// (BY+2) x (BZ+2) cells starting at the brick origin + shift, zero outside
+// the source cube, one row of 16 channels per region cell (two K planes of
+// 16-byte rows).  Output cell (x, y, z) sits at row m = x + RX y + RX RY z
+// and its tap e source at row m + e_x + RX e_y + RX RY e_z, so a tap's A
+// operand for a 128-row tile is the same run of rows shifted: 27 MMAs (M =
+// 128, N = 16, K = 16) per tile into one TMEM accumulator.  Rows whose (x,
+// y, z) fall outside the brick or the output cube are computed and dropped.
+// One brick per CTA; the wait for the MMAs is bounded (error word, skipped
+// epilogue).
+struct BrickGeo {
+    int BX, BY, BZ;        // brick of output cells
+    int RX, RY, RZ;        // source region = brick + 2
+    int MT;                // 128-row M tiles covering the brick's rows
+    int SROWS;             // staged rows: 128 MT + the largest tap offset (zero past the region)
+    int bricks[3];         // bricks per patch along x, y, z
+};
+
+constexpr int BRICK_NT = 256;
+constexpr int BRICK_MAX_ROWS = 2880;    // 2 planes x 2880 x 16 B = 90 KB: two CTAs per SM
+constexpr int BRICK_MAX_MT = 16;        // 256 TMEM columns
+
+template <int MODE>
+__global__ void __launch_bounds__(BRICK_NT, 2) brick_tc_kernel(const __grid_constant__ Args a,
+                                                                const __grid_constant__ BrickGeo g)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const uint32_t plane = (uint32_t)g.SROWS * 16u;
+    unsigned char *A = smem;                          // [2][SROWS][16 B]
+    unsigned char *Wb = smem + 2 * plane;             // [27][2][16][16 B]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Wb + WBYTES);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
+    int *okf = reinterpret_cast<int *>(slot + 1);
+    const int r = threadIdx.x, warp = r >> 5;
+    constexpr uint32_t TCOLS = 256;
+
+    const int per = g.bricks[0] * g.bricks[1] * g.bricks[2];
+    const int b = blockIdx.x / per;
+    int br = blockIdx.x - b * per;
+    const int ox = (br % g.bricks[0]) * g.BX;
+    br /= g.bricks[0];
+    const int oy = (br % g.bricks[1]) * g.BY;
+    const int oz = (br / g.bricks[1]) * g.BZ;
+
+    if (r == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(slot, TCOLS);
+        tc::tmem_relinquish();
+    }
+    for (int i = r; i < (int)(WBYTES / 16); i += BRICK_NT)
+        reinterpret_cast<uint4 *>(Wb)[i] = __ldg(reinterpret_cast<const uint4 *>(a.w) + i);
+    // ---- source region: lanes 2i, 2i+1 copy the two channel halves of a row
+    const int64_t si3 = (int64_t)a.Sin * a.Sin * a.Sin;
+    const int rrows = g.RX * g.RY * g.RZ;
+    for (int t = r; t < 2 * g.SROWS; t += BRICK_NT) {
+        const int u = t >> 1, hh = t & 1;
+        unsigned char *dst = A + hh * plane + u * 16;
+        bool in = false;
+        int64_t e = 0;
+        if (u < rrows) {
+            const int i = u % g.RX, j = (u / g.RX) % g.RY, k = u / (g.RX * g.RY);
+            const int sx = ox + i + a.shift, sy = oy + j + a.shift, sz = oz + k + a.shift;
+            in = (unsigned)sx < (unsigned)a.Sin && (unsigned)sy < (unsigned)a.Sin && (unsigned)sz < (unsigned)a.Sin;
+            if (in) e = (int64_t)b * si3 + sx + (int64_t)a.Sin * (sy + (int64_t)a.Sin * sz);
+        }
+        cp16(dst, in ? a.src + e * 16 + 8 * hh : a.src, in ? 16u : 0u);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tbase = *slot;
+
+    if (r == 0) {
+        const uint32_t a0 = smem_u32(A), b0 = smem_u32(Wb);
+        const int sy = g.RX, sz = g.RX * g.RY;
+#pragma unroll 1
+        for (int t = 0; t < g.MT; ++t) {
+#pragma unroll
+            for (int q = 0; q < 27; ++q) {
+                const int off = q % 3 + sy * ((q / 3) % 3) + sz * (q / 9);
+                const uint64_t da = tc::smem_desc(a0 + 16u * (uint32_t)(128 * t + off), plane, 128u);
+                const uint64_t db = tc::smem_desc(b0 + 512u * q, 256u, 128u);
+                tc::mma_bf16(tbase + 16u * t, da, db, IDESC_K, q > 0 ? 1u : 0u);
+            }
+        }
+        tc::mma_commit(bar);
+        *okf = mbar_wait_bounded(bar, 0) ? 1 : 0;
+    }
+    __syncthreads();
+    const int ok = *okf;
+    tc::fence_after_sync();
+    if (ok) {
+        // warp w: TMEM lanes 32 (w % 4) .. + 31 of tiles w / 4, w / 4 + 2, ...
+        const uint32_t lanes = (uint32_t)(32 * (warp & 3)) << 16;
+        const int64_t so3 = (int64_t)a.Sout * a.Sout * a.Sout;
+#pragma unroll 1
+        for (int t = warp >> 2; t < g.MT; t += 2) {
+            float v[16];
+            tc::tmem_ld16(tbase + lanes + 16u * t, v);
+            const int m = 128 * t + 32 * (warp & 3) + (r & 31);
+            const int z = m / (g.RX * g.RY), rem = m - z * (g.RX * g.RY);
+            const int y = rem / g.RX, x = rem - y * g.RX;
+            const int X = ox + x, Y = oy + y, Z = oz + z;
+            if (x >= g.BX || y >= g.BY || z >= g.BZ || X >= a.Sout || Y >= a.Sout || Z >= a.Sout) continue;
+            const int64_t L = (int64_t)b * so3 + X + (int64_t)a.Sout * (Y + (int64_t)a.Sout * Z);
+            uint32_t h[8];
+            if (MODE == BWD) {
+                const uint4 *mk = reinterpret_cast<const uint4 *>(a.act + L * 16);
+                const uint4 m0 = mk[0], m1 = mk[1];
+                const uint32_t mw[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float lo = __uint_as_float(mw[q] << 16), hi = __uint_as_float(mw[q] & 0xFFFF0000u);
+                    h[q] = (uint32_t)bf16_bits(lo > 0.f ? v[2 * q] : 0.f) |
+                           ((uint32_t)bf16_bits(hi > 0.f ? v[2 * q + 1] : 0.f) << 16);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    float p = v[2 * q], u = v[2 * q + 1];
+                    if (a.relu) {
+                        p = fmaxf(p, 0.f);
+                        u = fmaxf(u, 0.f);
+                    }
+                    h[q] = (uint32_t)bf16_bits(p) | ((uint32_t)bf16_bits(u) << 16);
+                }
+            }
+            uint4 *dst = reinterpret_cast<uint4 *>(a.out + L * 16);
+            dst[0] = make_uint4(h[0], h[1], h[2], h[3]);
+            dst[1] = make_uint4(h[4], h[5], h[6], h[7]);
+        }
+    } else if (r == 0 && a.err) {
+        atomicExch(a.err, kDevErrTimeout);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tbase, TCOLS);
+}
+
+// Brick shape for an output cube of side So: whole rows (BX = So, at most
+// 64), and the (BY, BZ), BZ <= 4, of least cost while the staged rows fit
+// BRICK_MAX_ROWS and the tiles BRICK_MAX_MT; cost = bricks x (tiles + 3),
+// a brick's set-up (weights, barrier, TMEM, staging latency) counted as
+// three tiles of MMAs.  False if none fits.
+static bool brick_geo(int So, BrickGeo &g)
+{
+    g.BX = So < 64 ? So : 64;
+    g.RX = g.BX + 2;
+    const int64_t bx = (So + g.BX - 1) / g.BX;
+    int64_t best = -1;
+    for (int bz = 1; bz <= 4 && bz <= So; ++bz)
+        for (int by = 1; by <= So; ++by) {
+            const int ry = by + 2, rz = bz + 2;
+            const int span = (g.BX - 1) + g.RX * (by - 1) + g.RX * ry * (bz - 1) + 1;
+            const int mt = (span + 127) / 128;
+            const int offmax = 2 + 2 * g.RX + 2 * g.RX * ry;
+            const int srows = ((128 * mt + offmax + 7) / 8) * 8;
+            if (mt > BRICK_MAX_MT || srows > BRICK_MAX_ROWS || srows < g.RX * ry * rz) continue;
+            const int64_t cost = bx * ((So + by - 1) / by) * ((So + bz - 1) / bz) * (mt + 3);
+            if (best < 0 || cost < best) {
+                best = cost;
+                g.BY = by;
+                g.BZ = bz;
+                g.RY = ry;
+                g.RZ = rz;
+                g.MT = mt;
+                g.SROWS = srows;
+            }
+        }
+    if (best < 0) return false;
+    g.bricks[0] = (int)bx;
+    g.bricks[1] = (So + g.BY - 1) / g.BY;
+    g.bricks[2] = (So + g.BZ - 1) / g.BZ;
+    return true;
 }
 
 // ---------------------------------------------------- CUDA-core layers
@@ -532,19 +656,36 @@ static unsigned grid_of(int64_t n, int threads, int64_t cap)
     return (unsigned)(b < 1 ? 1 : b);
 }
 
-static DeviceOnce attr_once[3];
+static DeviceOnce wgrad_once, brick_once[2];
 
-template <int MODE>
-static cn_status launch_patch(Args &a, cudaStream_t st)
+// weight gradient: persistent CTAs, two per SM
+static cn_status launch_wgrad(Args &a, cudaStream_t st)
 {
-    cn_status s = smem_opt_in(attr_once[MODE], patch_tc_kernel<MODE>, SMEM);
+    cn_status s = smem_opt_in(wgrad_once, wgrad_tc_kernel, SMEM);
     if (s != CN_OK) return s;
     int dev = 0, sms = 148;
     CN_CUDA_TRY(cudaGetDevice(&dev));
     CN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     a.chunks = (a.total + ROWS - 1) / ROWS;
     const int64_t grid = a.chunks < 2LL * sms ? a.chunks : 2LL * sms;
-    patch_tc_kernel<MODE><<<(unsigned)grid, NT, SMEM, st>>>(a);
+    wgrad_tc_kernel<<<(unsigned)grid, NT, SMEM, st>>>(a);
+    CN_CUDA_TRY(cudaGetLastError());
+    return CN_OK;
+}
+
+// forward / backward-data: one CTA per brick
+template <int MODE>
+static cn_status launch_conv(Args &a, int B, cudaStream_t st)
+{
+    BrickGeo g;
+    if (!brick_geo(a.Sout, g)) return fail(CN_ERR_INVALID_ARGUMENT, "learned smoother training: empty patch");
+    const size_t smem = 2 * (size_t)g.SROWS * 16 + WBYTES + 16;
+    // one opt-in per device, at the largest brick any patch size can take
+    constexpr size_t smem_max = 2 * (size_t)BRICK_MAX_ROWS * 16 + WBYTES + 16;
+    cn_status s = smem_opt_in(brick_once[MODE], brick_tc_kernel<MODE>, smem_max);
+    if (s != CN_OK) return s;
+    const int64_t ctas = (int64_t)B * g.bricks[0] * g.bricks[1] * g.bricks[2];
+    brick_tc_kernel<MODE><<<(unsigned)ctas, BRICK_NT, smem, st>>>(a, g);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }
@@ -576,7 +717,7 @@ cn_status train_forward_tc(const TrainBufs &T, const float *x, const float *W, i
     a.relu = 1;
     a.total = (int64_t)B * S2 * S2 * S2;
     a.err = T.err;
-    if ((s = launch_patch<FWD>(a, st)) != CN_OK) return s;
+    if ((s = launch_conv<FWD>(a, B, st)) != CN_OK) return s;
     l3_fwd_cl<<<grid_of((int64_t)B * S3 * S3 * S3, 128, 148 * 64), 128, 0, st>>>(T.h2, W3, T.y, B, S2);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
@@ -606,7 +747,7 @@ cn_status train_backward_tc(const TrainBufs &T, const float *x, const float *W, 
     w.shift = 0;
     w.total = (int64_t)B * S2 * S2 * S2;
     w.err = T.err;
-    if ((s = launch_patch<WGRAD>(w, st)) != CN_OK) return s;
+    if ((s = launch_wgrad(w, st)) != CN_OK) return s;
     Args d = {};
     d.src = T.gh2;
     d.act = T.h1;
@@ -617,7 +758,7 @@ cn_status train_backward_tc(const TrainBufs &T, const float *x, const float *W, 
     d.shift = -2;
     d.total = (int64_t)B * S1 * S1 * S1;
     d.err = T.err;
-    if ((s = launch_patch<BWD>(d, st)) != CN_OK) return s;
+    if ((s = launch_conv<BWD>(d, B, st)) != CN_OK) return s;
     l1_wgrad_cl<<<grid_of((int64_t)B * S1, 1, sms), WG_THREADS, 0, st>>>(x, T.gh1, gW1, B, S);
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
