@@ -1272,6 +1272,9 @@ def run_companions(args, local):
             ach = W.bytes_per_cell_step * W.cells / L / (ms / (k * L) / 1e3) / 1e9
             d["hbm"] = dict(achieved_gbs=round(ach, 1), frac=round(ach / peaks["hbm_gbs"], 4),
                             algorithmic_bytes_per_cell_step=W.bytes_per_cell_step)
+            if getattr(W, "traffic_per_cell_step", None):
+                d["hbm"]["traffic_per_cell_step"] = W.traffic_per_cell_step
+                d["hbm"]["traffic_source"] = W.traffic_source
             flops = getattr(W, "flops_per_cell_stage", None)
             if flops:
                 peak_tf = _lib.fma_peak_tflops(_lib.CN_FLOAT64 if W.dtype == "f64" else _lib.CN_FLOAT32)
