@@ -677,6 +677,7 @@ class C5:
     # local Fourier analysis of damped Jacobi); measured on this problem: 15
     # V(2,2) cycles, 23.4 ms, against 16 cycles, 25.0 ms at omega 0.8
     omega = 6.0 / 7.0
+    nu = (2, 2)  # pre- and post-smoothing sweeps (bench.py --mg-nu, --mg-omega)
     name = "c5"
     desc = ("Poisson div(k grad p) = f, 256^3 cells as 8^3 blocks of 32^3, k = box-filtered lognormal "
             "(sigma 0.5), f = 32 Gaussians; multigrid V(2,2) weighted Jacobi (omega 6/7), FP32 cycles in "
@@ -701,7 +702,10 @@ class C5:
         self.f = cn.Grid.Cartesian(self.nb, self.n, dtype=np.float32)
         cn.workloads.poisson_rhs(self.f, seed=2)
         self.p64 = cn.Grid.Cartesian(self.nb, self.n, dtype=np.float64)
-        self.mg = cn.mg.Multigrid(self.k, nu1=2, nu2=2, omega=self.omega)
+        self.mg = cn.mg.Multigrid(self.k, nu1=self.nu[0], nu2=self.nu[1], omega=self.omega)
+        om = "6/7" if abs(self.omega - 6.0 / 7.0) < 1e-12 else f"{self.omega:g}"
+        self.desc = self.desc.replace("V(2,2) weighted Jacobi (omega 6/7)",
+                                      f"V({self.nu[0]},{self.nu[1]}) weighted Jacobi (omega {om})")
         self.cells = int(np.prod(self.nb)) * int(np.prod(self.n))
         self.updates_per_step = self.cells
         self.cycles, self.relres = self.mg.solve(self.f, self.p64, self.rtol, max_cycles=100)
@@ -1121,6 +1125,10 @@ def run_ours(args, world, rank, local, pg):
     if args.blocks:
         cls = type(cls.__name__, (cls,), {"nb": tuple(args.blocks),
                                           "desc": cls.desc + f" [reduced: {tuple(args.blocks)} blocks]"})
+    if getattr(args, "mg_omega", None) is not None and hasattr(cls, "omega"):
+        cls = type(cls.__name__, (cls,), {"omega": args.mg_omega})
+    if getattr(args, "mg_nu", None) is not None and hasattr(cls, "nu"):
+        cls = type(cls.__name__, (cls,), {"nu": tuple(args.mg_nu)})
     if getattr(args, "nn_training", None) and hasattr(cls, "nn_training"):
         cls = type(cls.__name__, (cls,), {"nn_training": args.nn_training})
     if getattr(args, "no_autotune", False) and hasattr(cls, "autotune"):
@@ -1423,6 +1431,8 @@ def main():
     ap.add_argument("--companion-steps", type=int, default=5, help="timed steps of each companion workload")
     ap.add_argument("--no-learned", action="store_true",
                     help="c5: skip training and timing the learned smoother")
+    ap.add_argument("--mg-omega", type=float, default=None, help="c5: Jacobi damping (default 6/7)")
+    ap.add_argument("--mg-nu", type=int, nargs=2, default=None, help="c5: pre- and post-smoothing sweeps (default 2 2)")
     ap.add_argument("--nn-training", default=None, choices=["tensor", "fp32"],
                     help="c5: training arithmetic of the learned smoother (default tensor)")
     ap.add_argument("--no-autotune", action="store_true",
