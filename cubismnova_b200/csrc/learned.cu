@@ -9,7 +9,7 @@
 //   smoothing step:  p <- p + omega * x0 + y        (Jacobi plus a learned term)
 // Weights are stored [tap][cin][cout], tap = dx+1 + 3*(dy+1) + 9*(dz+1).
 //
-// Training (all on the device, FP32): samples are block-sized patches of
+// Training (all on the device): samples are block-sized patches of
 // residuals r taken from the plain V-cycle (before pre-smoothing and after the
 // coarse-grid correction) with the coefficients k; the loss is the residual
 // left after one smoothing step, normalised per sample,
@@ -18,6 +18,10 @@
 // Patches carry a 4-cell halo: three valid convolutions and A each shrink the
 // region by one cell.  Backward: the adjoint of A (gather form), transposed
 // convolutions masked by the ReLU, weight gradients reduced per tap, Adam.
+// The network's forward and backward run either on the tensor cores with
+// BF16 activations (learned_train_tc.cu, the default) or in FP32 on the CUDA
+// cores (the patch kernels below; cn_nn_set_training); the loss, its
+// adjoint and Adam are shared.
 //
 // Inference on the grid runs layer by layer on grids of 16 channels, each
 // convolution reading its input through the lab of a (-1,2) tensorial stencil
