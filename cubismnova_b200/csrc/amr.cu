@@ -13,10 +13,12 @@
 namespace cn {
 namespace amr {
 
-// Euler tiles of AMR blocks: work item -> (block, tile of 8^3 cells)
+// Euler tiles of AMR blocks: tile index -> (block, tile of 8^3 cells); a
+// work item (a CTA's unit of work) is a run of consecutive tiles of the list
 struct Src {
     Geom A;
-    const int2 *work;
+    const int2 *work;  // tiles: (block, tile index in the block)
+    const int2 *items; // work items: (first tile, tile count)
     template <typename T> __device__ __forceinline__ void tile(int item, euler::TileInfo<T> &t) const
     {
         const int2 w = work[item];
@@ -57,9 +59,13 @@ __global__ void __launch_bounds__(euler::NT, 3) stage_kernel(euler::StageParams<
     __shared__ double red[euler::NT / 32][5];
     __shared__ int snb[28];
     __shared__ euler::TileInfo<T> ts;
-    // persistent: each CTA walks the work list with a grid stride
-    for (int item = blockIdx.x; item < nitems; item += gridDim.x)
-        euler::stage_tile<T>(p, src, item, item, W, A, red, snb, &ts);
+    // persistent: each CTA walks the work items with a grid stride, the
+    // tiles of an item in order
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const int2 it = src.items[item];
+        for (int k = 0; k < it.y; ++k)
+            euler::stage_tile<T>(p, src, it.x + k, it.x + k, W, A, red, snb, &ts);
+    }
 }
 
 // dense lab of one block: (n+2g)^3, face ghosts only (non-tensorial)
@@ -92,10 +98,12 @@ struct cn_amr {
     BlockDev *d_blocks = nullptr;
     int32_t *d_lookup = nullptr;
     void *d_data = nullptr;
-    std::vector<int2> work;
-    int2 *d_work = nullptr;
+    std::vector<int2> work;   // tiles in work-list order
+    std::vector<int2> items;  // work items: (first tile, tile count)
+    int2 *d_work = nullptr, *d_items = nullptr;
     int order = 1;   // work-list order (see cn_amr_set_schedule)
     int ctas = 0;    // persistent grid size (0: one CTA per item)
+    int unit = 1;    // tiles per work item along x (cn_amr_set_work_unit)
 };
 
 static uint64_t spread3(uint32_t v)
@@ -109,35 +117,46 @@ static uint64_t spread3(uint32_t v)
     return x;
 }
 
+// Work list: units of up to a->unit consecutive tiles along x of one block
+// (fewer where the block's row of tiles is shorter), ordered by the
+// schedule's key of their first tile, emitted tile by tile; one work item
+// per unit.
 static cn_status build_work(cn_amr *a)
 {
-    struct Item {
-        int2 w;
-        int n;
+    struct Unit {
+        int block, t0, count, n;
         uint64_t key;
     };
-    std::vector<Item> items;
+    std::vector<Unit> units;
     for (int b = 0; b < a->nblocks; ++b) {
         const BlockDev &B = a->blocks[b];
         const int tpd = B.n / 8, cs = B.level == 0 ? 2 : 1;
-        for (int t = 0; t < tpd * tpd * tpd; ++t) {
+        const int run = a->unit < tpd ? a->unit : tpd;
+        for (int t = 0; t < tpd * tpd * tpd; t += run) {
             const int tx = t % tpd, ty = (t / tpd) % tpd, tz = t / (tpd * tpd);
             const uint32_t X = (uint32_t)(B.ox + tx * 8 * cs), Y = (uint32_t)(B.oy + ty * 8 * cs),
                            Z = (uint32_t)(B.oz + tz * 8 * cs);
-            items.push_back({make_int2(b, t), B.n, spread3(X) | spread3(Y) << 1 | spread3(Z) << 2});
+            units.push_back({b, t, run, B.n, spread3(X) | spread3(Y) << 1 | spread3(Z) << 2});
         }
     }
     if (a->order == 1) {
-        std::stable_sort(items.begin(), items.end(), [](const Item &l, const Item &r) { return l.n > r.n; });
+        std::stable_sort(units.begin(), units.end(), [](const Unit &l, const Unit &r) { return l.n > r.n; });
     } else if (a->order == 2) {
-        std::stable_sort(items.begin(), items.end(), [](const Item &l, const Item &r) { return l.key < r.key; });
+        std::stable_sort(units.begin(), units.end(), [](const Unit &l, const Unit &r) { return l.key < r.key; });
     }
     a->work.clear();
-    for (const Item &it : items) a->work.push_back(it.w);
+    a->items.clear();
+    for (const Unit &u : units) {
+        a->items.push_back(make_int2((int)a->work.size(), u.count));
+        for (int k = 0; k < u.count; ++k) a->work.push_back(make_int2(u.block, u.t0 + k));
+    }
     if (a->d_work) cudaFree(a->d_work);
-    a->d_work = nullptr;
+    if (a->d_items) cudaFree(a->d_items);
+    a->d_work = a->d_items = nullptr;
     CN_CUDA_TRY(cudaMalloc(&a->d_work, sizeof(int2) * a->work.size()));
     CN_CUDA_TRY(cudaMemcpy(a->d_work, a->work.data(), sizeof(int2) * a->work.size(), cudaMemcpyHostToDevice));
+    CN_CUDA_TRY(cudaMalloc(&a->d_items, sizeof(int2) * a->items.size()));
+    CN_CUDA_TRY(cudaMemcpy(a->d_items, a->items.data(), sizeof(int2) * a->items.size(), cudaMemcpyHostToDevice));
     return CN_OK;
 }
 
@@ -181,7 +200,8 @@ static cn_status launch_amr_stage(cn_amr *Us, cn_amr *Un, cn_amr *out, int stage
     Src src;
     src.A = geom(Us);
     src.work = Us->d_work;
-    const int nitems = (int)Us->work.size();
+    src.items = Us->d_items;
+    const int nitems = (int)Us->items.size();
     int grid = Us->ctas > 0 ? std::min(Us->ctas, nitems) : nitems;
     const size_t smem = (size_t)(5 * euler::Stg<T>::SV + 5 * euler::NACC) * sizeof(T);
     amr::stage_kernel<T><<<grid, euler::NT, smem, st>>>(p, src, nitems);
@@ -293,6 +313,7 @@ cn_status cn_amr_destroy(cn_amr *a)
     if (a->d_lookup) cudaFree(a->d_lookup);
     if (a->d_data) cudaFree(a->d_data);
     if (a->d_work) cudaFree(a->d_work);
+    if (a->d_items) cudaFree(a->d_items);
     delete a;
     return CN_OK;
 }
@@ -361,9 +382,9 @@ cn_status cn_amr_rk3_step(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double g
 }
 
 // Work-list order (0: block order, 1: largest blocks first, 2: Morton order
-// of tile positions) and persistent grid size (0: one CTA per tile).  Every
-// layout sharing a step should use the same schedule (the stage kernels take
-// the schedule of the state they read).
+// of tile positions) and persistent grid size (0: one CTA per work item).
+// Every layout sharing a step should use the same schedule (the stage
+// kernels take the schedule of the state they read).
 cn_status cn_amr_set_schedule(cn_amr *a, int order, int ctas)
 {
     if (!a || order < 0 || order > 2 || ctas < 0) return fail(CN_ERR_INVALID_ARGUMENT, "bad schedule");
@@ -375,9 +396,32 @@ cn_status cn_amr_set_schedule(cn_amr *a, int order, int ctas)
     return CN_OK;
 }
 
-// Times every schedule candidate (orders 0..2, grid = k x SMs x 3 CTAs for k
-// in {1, 2, 4} or one CTA per tile) over `reps` RK3 steps and keeps the
-// fastest on all three layouts.  U is advanced by the trial steps.
+// Work unit: 1, 2 or 4 consecutive 8^3 tiles along x of a block per work
+// item (a CTA's unit: 8x8x8, 16x8x8 or 32x8x8 cells; fewer tiles where a
+// block's row is shorter).
+cn_status cn_amr_set_work_unit(cn_amr *a, int tiles)
+{
+    if (!a || (tiles != 1 && tiles != 2 && tiles != 4)) return fail(CN_ERR_INVALID_ARGUMENT, "bad work unit");
+    if (tiles != a->unit) {
+        a->unit = tiles;
+        return build_work(a);
+    }
+    return CN_OK;
+}
+
+cn_status cn_amr_get_schedule(const cn_amr *a, int out[3])
+{
+    if (!a || !out) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    out[0] = a->order;
+    out[1] = a->ctas;
+    out[2] = a->unit;
+    return CN_OK;
+}
+
+// Times every schedule candidate (orders 0..2, work units of 1, 2 and 4
+// tiles, grid = k x SMs x 3 CTAs for k in {1, 2, 4} or one CTA per work item)
+// over `reps` RK3 steps and keeps the fastest on all three layouts.  U is
+// advanced by the trial steps.
 cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, int reps, int *order_out,
                           int *ctas_out, double *ms_out, void *stream)
 {
@@ -387,37 +431,43 @@ cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double g
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grids[4] = {0, sms * 3, sms * 6, sms * 12};
+    const int units[3] = {1, 2, 4};
     double best = 1e300;
-    int bo = 1, bc = 0;
+    int bo = 1, bc = 0, bu = 1;
     cudaEvent_t e0, e1;
     CN_CUDA_TRY(cudaEventCreate(&e0));
     CN_CUDA_TRY(cudaEventCreate(&e1));
-    for (int order = 0; order < 3; ++order)
-        for (int gi = 0; gi < 4; ++gi) {
-            cn_status s;
-            cn_amr *all[3] = {U, w1, w2};
-            for (cn_amr *a : all)
-                if ((s = cn_amr_set_schedule(a, order, grids[gi])) != CN_OK) return s;
-            if ((s = cn_amr_rk3_step(U, w1, w2, dt, gamma, stream)) != CN_OK) return s; // warm-up
-            CN_CUDA_TRY(cudaEventRecord(e0, st));
-            for (int r = 0; r < (reps < 1 ? 1 : reps); ++r)
-                if ((s = cn_amr_rk3_step(U, w1, w2, dt, gamma, stream)) != CN_OK) return s;
-            CN_CUDA_TRY(cudaEventRecord(e1, st));
-            CN_CUDA_TRY(cudaEventSynchronize(e1));
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= (reps < 1 ? 1 : reps);
-            if (ms < best) {
-                best = ms;
-                bo = order;
-                bc = grids[gi];
+    for (int unit : units)
+        for (int order = 0; order < 3; ++order)
+            for (int gi = 0; gi < 4; ++gi) {
+                cn_status s;
+                cn_amr *all[3] = {U, w1, w2};
+                for (cn_amr *a : all) {
+                    if ((s = cn_amr_set_work_unit(a, unit)) != CN_OK) return s;
+                    if ((s = cn_amr_set_schedule(a, order, grids[gi])) != CN_OK) return s;
+                }
+                if ((s = cn_amr_rk3_step(U, w1, w2, dt, gamma, stream)) != CN_OK) return s; // warm-up
+                CN_CUDA_TRY(cudaEventRecord(e0, st));
+                for (int r = 0; r < (reps < 1 ? 1 : reps); ++r)
+                    if ((s = cn_amr_rk3_step(U, w1, w2, dt, gamma, stream)) != CN_OK) return s;
+                CN_CUDA_TRY(cudaEventRecord(e1, st));
+                CN_CUDA_TRY(cudaEventSynchronize(e1));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= (reps < 1 ? 1 : reps);
+                if (ms < best) {
+                    best = ms;
+                    bo = order;
+                    bc = grids[gi];
+                    bu = unit;
+                }
             }
-        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cn_amr *all[3] = {U, w1, w2};
     for (cn_amr *a : all) {
-        cn_status s = cn_amr_set_schedule(a, bo, bc);
+        cn_status s = cn_amr_set_work_unit(a, bu);
+        if (s == CN_OK) s = cn_amr_set_schedule(a, bo, bc);
         if (s != CN_OK) return s;
     }
     if (order_out) *order_out = bo;

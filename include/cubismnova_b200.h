@@ -398,9 +398,17 @@ cn_status cn_amr_rk3_stage(cn_amr *Us, cn_amr *Un, cn_amr *out, int stage, doubl
                            void *stream);
 cn_status cn_amr_rk3_step(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, void *stream);
 /* Work-list order (0 block order, 1 largest blocks first, 2 Morton order of
- * tiles) and persistent grid (0: one CTA per tile). */
+ * tiles) and persistent grid (0: one CTA per work item). */
 cn_status cn_amr_set_schedule(cn_amr *a, int order, int ctas);
-/* Times all schedules over `reps` steps (advancing U) and keeps the fastest. */
+/* Work unit of a CTA: 1, 2 or 4 consecutive 8^3 tiles along x of one block
+ * per work item (8x8x8, 16x8x8 or 32x8x8 cells, fewer where a block's row is
+ * shorter); the stage's compute tile stays 8^3. */
+cn_status cn_amr_set_work_unit(cn_amr *a, int tiles);
+/* out = {order, ctas, work-unit tiles} of a layout. */
+cn_status cn_amr_get_schedule(const cn_amr *a, int out[3]);
+/* Times all schedules (orders x work units x grid sizes) over `reps` steps
+ * (advancing U) and keeps the fastest; the unit chosen is read back with
+ * cn_amr_get_schedule. */
 cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, int reps,
                           int *order_out, int *ctas_out, double *ms_out, void *stream);
 

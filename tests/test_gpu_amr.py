@@ -61,15 +61,19 @@ def test_amr_schedules_and_graph_are_bitwise_identical(cn):
     w1, w2 = U.like(), U.like()
     start = [U.tensor(k).clone() for k in range(5)]
     results = []
-    for order in range(3):
-        for ctas in (0, 148 * 3):
-            for k in range(5):
-                U.tensor(k).copy_(start[k])
-            for g in (U, w1, w2):
-                g.set_schedule(order, ctas)
-            cn.amr.rk3_step(U, w1, w2, 1e-4, GAMMA)
-            torch.cuda.synchronize()
-            results.append(torch.cat([U.tensor(k).clone() for k in range(5)]))
+    for unit in (1, 2, 4):
+        for order in range(3):
+            for ctas in (0, 148 * 3):
+                for k in range(5):
+                    U.tensor(k).copy_(start[k])
+                for g in (U, w1, w2):
+                    g.set_schedule(order, ctas, unit)
+                    assert g.schedule() == (order, ctas, unit)
+                cn.amr.rk3_step(U, w1, w2, 1e-4, GAMMA)
+                torch.cuda.synchronize()
+                results.append(torch.cat([U.tensor(k).clone() for k in range(5)]))
+    for g in (U, w1, w2):
+        g.set_schedule(1, 0, 1)
     for r in results[1:]:
         assert torch.equal(r, results[0])
     # graph replay of the step
