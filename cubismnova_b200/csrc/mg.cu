@@ -373,25 +373,64 @@ __global__ void __launch_bounds__(kTileThreads, 4) resid64_kernel(const __grid_c
     if (column_run(T, x, y, z0, zl)) {
         const int st[3] = {1, q.rs, q.rs * q.ey};
         const double *fb = faces + (int64_t)q.block * face_count(Lk.n);
-        for (int z = z0; z < z0 + zl; ++z) {
-            const int64_t o = (int64_t)q.block * Lk.bstride + dense_cell(Lk, q, x, y, z); // FP32 fields (f, r32)
-            const int u = ridx(q, x, y, z);
-            const int g[3] = {q.x0 + x, q.y0 + y, q.z0 + z};
+        // the six face indices of the column's first cell; along z they
+        // advance by each face array's plane size, and the next cell's
+        // loads go out before this cell's arithmetic
+        const int gx = q.x0 + x, gy = q.y0 + y, gz = q.z0 + z0;
+        const int64_t dz[3] = {(int64_t)(Lk.n[0] + 1) * Lk.n[1], (int64_t)Lk.n[0] * (Lk.n[1] + 1),
+                               (int64_t)Lk.n[0] * Lk.n[1]};
+        int64_t im[3], ip[3];
+        im[0] = face_index(Lk.n, 0, gx, gy, gz);
+        ip[0] = im[0] + 1;
+        im[1] = face_index(Lk.n, 1, gx, gy, gz);
+        ip[1] = im[1] + Lk.n[0];
+        im[2] = face_index(Lk.n, 2, gx, gy, gz);
+        ip[2] = im[2] + dz[2];
+        int64_t o = (int64_t)q.block * Lk.bstride + dense_cell(Lk, q, x, y, z0); // FP32 fields (f, r32)
+        const int64_t oz = (int64_t)Lk.n[0] * Lk.n[1];
+        double km[3], kp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            km[d] = __ldg(fb + im[d]);
+            kp[d] = __ldg(fb + ip[d]);
+        }
+        float fcf = __ldg(f + o);
+        int u = ridx(q, x, y, z0);
+        for (int k = 0; k < zl; ++k, u += st[2], o += oz) {
+            double nkm[3], nkp[3];
+            float nf = fcf;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                nkm[d] = km[d];
+                nkp[d] = kp[d];
+            }
+            if (k + 1 < zl) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    im[d] += dz[d];
+                    ip[d] += dz[d];
+                    nkm[d] = __ldg(fb + im[d]);
+                    nkp[d] = __ldg(fb + ip[d]);
+                }
+                nf = __ldg(f + o + oz);
+            }
             const double pc = sp[u];
             double fd[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const int ex = d == 0, ey = d == 1, ez = d == 2;
-                const double kp = __ldg(fb + face_index(Lk.n, d, g[0] + ex, g[1] + ey, g[2] + ez));
-                const double km = __ldg(fb + face_index(Lk.n, d, g[0], g[1], g[2]));
-                fd[d] = kp * (sp[u + st[d]] - pc) - km * (pc - sp[u - st[d]]);
-            }
+            for (int d = 0; d < 3; ++d)
+                fd[d] = kp[d] * (sp[u + st[d]] - pc) - km[d] * (pc - sp[u - st[d]]);
             const double Lp = a.ih2d * ((fd[0] + fd[1]) + fd[2]);
-            const double fc = (double)__ldg(f + o);
+            const double fc = (double)fcf;
             const double r = fc - Lp;
             if (r32) r32[o] = (float)r;
             rr += r * r;
             ff += fc * fc;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                km[d] = nkm[d];
+                kp[d] = nkp[d];
+            }
+            fcf = nf;
         }
     }
     for (int off = 16; off > 0; off >>= 1) {
