@@ -5,7 +5,7 @@ CUDA-graph replay of the RK3 step."""
 import numpy as np
 import pytest
 
-from numerics import TOL_F64, assert_close
+from numerics import TOL_F32_RHS, TOL_F32_STATE, TOL_F64, assert_close
 
 pytestmark = pytest.mark.gpu
 GAMMA = 1.4
@@ -52,6 +52,30 @@ def test_amr_stage_matches_oracle(cn, oracle_lib, stage):
     want = oracle_lib.amr_stage(host, hn if stage > 1 else None, blk, F, stage, 2e-4, GAMMA)
     got = np.stack([out.download(k) for k in range(5)])
     assert_close(got, want, TOL_F64, f"amr stage {stage}")
+
+
+@pytest.mark.parametrize("stage", [0, 1, 3])
+def test_amr_stage_fp32_matches_fp64_oracle(cn, oracle_lib, stage):
+    """The FP32 AMR stage (interface ghosts and WENO5 in FP32) against the
+    FP64 oracle on the same FP32-rounded inputs: the FP32 tolerances of
+    tests/numerics.py (right-hand side, and stage updates)."""
+    import torch
+    l, c, o, F = cn.workloads.amr_small_layout(3)
+    U = cn.amr.AmrGrid(l, c, o, F, dtype=np.float32)
+    cn.workloads.euler_pulse_amr(U, seed=7)
+    Un = U.like()
+    cn.workloads.euler_pulse_amr(Un, seed=8)
+    out = U.like()
+    host = np.stack([U.download(k) for k in range(5)]).astype(np.float64)
+    hn = np.stack([Un.download(k) for k in range(5)]).astype(np.float64)
+    if stage == 3:
+        out = Un
+    cn.amr.rk3_stage(U, Un if stage > 1 else None, out, stage, 2e-4, GAMMA)
+    torch.cuda.synchronize()
+    blk, _ = oracle_lib.amr_blocks(l, c, o, F)
+    want = oracle_lib.amr_stage(host, hn if stage > 1 else None, blk, F, stage, 2e-4, GAMMA)
+    got = np.stack([out.download(k) for k in range(5)]).astype(np.float64)
+    assert_close(got, want, TOL_F32_RHS if stage == 0 else TOL_F32_STATE, f"amr float32 stage {stage}")
 
 
 def test_amr_schedules_and_graph_are_bitwise_identical(cn):

@@ -59,12 +59,13 @@ def test_loss_and_gradient_match_oracle(cn):
     assert N.fd_check(x32, k32, r32, W1, W2, W3, 0.8, ih2, n=4) < 1e-5
 
 
-@pytest.mark.parametrize("B,P", [(3, 4), (2, 16)])
+@pytest.mark.parametrize("B,P", [(3, 4), (2, 5), (2, 16)])
 def test_tensor_core_training_matches_bf16_oracle(cn, B, P):
     """Tensor-core training path (tcgen05 forward, data gradient and weight
     gradient of the hidden layer) against the float64 oracle rounded to BF16
     where the device stores BF16; 3 x 4^3 patches end in partial 128-cell
-    chunks (1536 and 3000 rows), 2 x 16^3 patches span many chunks."""
+    chunks (1536 and 3000 rows), 2 x 5^3 patches have odd cube sides (ragged
+    bricks), 2 x 16^3 patches span many chunks."""
     from oracle import nn_oracle as N
     x, k, r = _batch(B, P, 7 + P)
     nn = cn.learned.LearnedSmoother(seed=5, omega=0.8, init_scale=0.05)
