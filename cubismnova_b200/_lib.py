@@ -78,6 +78,12 @@ _SIGS = {
     "cn_ddx_f32": (None, [_I, _I, _I, _P, _I, _I, _P, _I, _I, C.c_float]),
     "cn_ddx_async": (_I, [_I, _I, _I, _I, _P, _I, _I, _P, _I, _I, _D, _P]),
     "cn_calib_fma_peak": (_I, [_I, C.POINTER(C.c_double)]),
+    "cn_grid_write_hdf": (_I, [_P, C.c_char_p, C.c_char_p, _I, _I, _I3, _I3, _I, _D, _I, _P]),
+    "cn_grid_read_hdf": (_I, [_P, C.c_char_p, _I, _I, _I3, _I3, _I, _P]),
+    "cn_h5_write": (_I, [C.c_char_p, C.c_char_p, _I, C.POINTER(C.c_longlong), _I, _P, _I]),
+    "cn_h5_query": (_I, [C.c_char_p, C.c_char_p, C.POINTER(_I), C.POINTER(C.c_longlong), C.POINTER(_I)]),
+    "cn_h5_read": (_I, [C.c_char_p, C.c_char_p, _I, C.POINTER(C.c_longlong), _I, _P]),
+    "cn_xdmf_write": (_I, [C.c_char_p, C.c_char_p, _I, _I3, _I3, _D3, _D3, _I, _I, _D, _I]),
 }
 
 

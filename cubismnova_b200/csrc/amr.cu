@@ -16,6 +16,9 @@ namespace amr {
 // Euler tiles of AMR blocks: tile index -> (block, tile of 8^3 cells); a
 // work item (a CTA's unit of work) is a run of consecutive tiles of the list
 struct Src {
+    // a level-interface ghost cell resolves its geometry once for all five
+    // components (halo5)
+    static constexpr bool kHalo5 = true;
     Geom A;
     const int2 *work;  // tiles: (block, tile index in the block)
     const int2 *items; // work items: (first tile, tile count)
@@ -42,11 +45,14 @@ struct Src {
     {
         return same_level_offset(A, t.block, gx, gy, gz, off);
     }
+    // all five components of a level-interface ghost: the geometry once
     template <typename T>
-    __device__ __forceinline__ T halo(const T *comp, int, const euler::TileInfo<T> &t, int gx, int gy, int gz,
-                                      const int *) const
+    __device__ __forceinline__ void halo5(const T *const (&U)[5], const euler::TileInfo<T> &t, int gx, int gy, int gz,
+                                          const int *, T (&v)[5]) const
     {
-        return value<T>(comp, A, t.block, gx, gy, gz);
+        const Ghost g = resolve(A, t.block, gx, gy, gz);
+#pragma unroll 1
+        for (int c = 0; c < 5; ++c) v[c] = gather<T>(U[c], g);
     }
 };
 

@@ -71,28 +71,58 @@ __device__ __forceinline__ bool same_level_offset(const Geom &A, int b, int qx, 
     return true;
 }
 
-// value of lab cell q (tile coordinates of block b, possibly outside it)
-template <typename T>
-__device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, int qy, int qz)
+// Where lab cell q (tile coordinates of block b, possibly outside it) takes
+// its value from: a cell of b or of a block on b's level (kind 0, cell
+// (fx, fy, fz) of S), trilinear prolongation from the coarser S (kind 1),
+// or the mean of 8 cells of the finer S (kind 2); (fx, fy, fz) are level-1
+// offsets inside S for kinds 1 and 2.  The geometry does not depend on the
+// component, so a halo cell resolves it once for all of them.
+struct Ghost {
+    int kind;
+    BlockDev S;
+    int fx, fy, fz;
+};
+
+__device__ __forceinline__ Ghost resolve(const Geom &A, int b, int qx, int qy, int qz)
 {
+    Ghost g;
     const BlockDev B = A.blk[b];
-    if ((unsigned)qx < (unsigned)B.n && (unsigned)qy < (unsigned)B.n && (unsigned)qz < (unsigned)B.n)
-        return cell<T>(comp, B, qx, qy, qz);
+    if ((unsigned)qx < (unsigned)B.n && (unsigned)qy < (unsigned)B.n && (unsigned)qz < (unsigned)B.n) {
+        g.kind = 0;
+        g.S = B;
+        g.fx = qx;
+        g.fy = qy;
+        g.fz = qz;
+        return g;
+    }
     const int cs = B.level == 0 ? 2 : 1;
     const int X = wrap(B.ox + qx * cs, A.L[0]), Y = wrap(B.oy + qy * cs, A.L[1]), Z = wrap(B.oz + qz * cs, A.L[2]);
-    const int s = A.block_at(X, Y, Z);
-    const BlockDev S = A.blk[s];
-    const int fx = X - S.ox, fy = Y - S.oy, fz = Z - S.oz; // level-1 units inside S
-    if (S.level == B.level) {
-        const int css = S.level == 0 ? 2 : 1;
-        return cell<T>(comp, S, fx / css, fy / css, fz / css);
+    g.S = A.blk[A.block_at(X, Y, Z)];
+    g.fx = X - g.S.ox;
+    g.fy = Y - g.S.oy;
+    g.fz = Z - g.S.oz;
+    if (g.S.level == B.level) {
+        const int css = g.S.level == 0 ? 2 : 1;
+        g.kind = 0;
+        g.fx /= css;
+        g.fy /= css;
+        g.fz /= css;
+    } else {
+        g.kind = g.S.level < B.level ? 1 : 2;
     }
-    if (S.level < B.level) {
+    return g;
+}
+
+template <typename T> __device__ __forceinline__ T gather(const T *comp, const Ghost &g)
+{
+    const BlockDev &S = g.S;
+    if (g.kind == 0) return cell<T>(comp, S, g.fx, g.fy, g.fz);
+    if (g.kind == 1) {
         // fine ghost cell inside a coarse block: trilinear prolongation
-        const int px = fx >> 1, py = fy >> 1, pz = fz >> 1;
-        const int qx1 = clampi(px + ((fx & 1) ? 1 : -1), 0, S.n - 1);
-        const int qy1 = clampi(py + ((fy & 1) ? 1 : -1), 0, S.n - 1);
-        const int qz1 = clampi(pz + ((fz & 1) ? 1 : -1), 0, S.n - 1);
+        const int px = g.fx >> 1, py = g.fy >> 1, pz = g.fz >> 1;
+        const int qx1 = clampi(px + ((g.fx & 1) ? 1 : -1), 0, S.n - 1);
+        const int qy1 = clampi(py + ((g.fy & 1) ? 1 : -1), 0, S.n - 1);
+        const int qz1 = clampi(pz + ((g.fz & 1) ? 1 : -1), 0, S.n - 1);
         const T e000 = cell<T>(comp, S, px, py, pz), e100 = cell<T>(comp, S, qx1, py, pz);
         const T e010 = cell<T>(comp, S, px, qy1, pz), e110 = cell<T>(comp, S, qx1, qy1, pz);
         const T e001 = cell<T>(comp, S, px, py, qz1), e101 = cell<T>(comp, S, qx1, py, qz1);
@@ -112,8 +142,15 @@ __device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, 
     T v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k)
-        v[k] = cell<T>(comp, S, fx + (k & 1), fy + ((k >> 1) & 1), fz + (k >> 2));
+        v[k] = cell<T>(comp, S, g.fx + (k & 1), g.fy + ((k >> 1) & 1), g.fz + (k >> 2));
     return (((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]))) * T(0.125);
+}
+
+// value of lab cell q (tile coordinates of block b, possibly outside it)
+template <typename T>
+__device__ __forceinline__ T value(const T *comp, const Geom &A, int b, int qx, int qy, int qz)
+{
+    return gather<T>(comp, resolve(A, b, qx, qy, qz));
 }
 
 } // namespace amr

@@ -88,6 +88,8 @@ template <typename T> struct TileInfo {
 // Uniform Cartesian grid: tiles in block order, halo cells through the
 // FieldLab lab resolution (cn::lab_value) with each component's BC vector.
 struct CartSrc {
+    // halo cells resolve per component (each has its own BC chain)
+    static constexpr bool kHalo5 = false;
     LabGeom L;
     BcView bc[5];
     double ih[3];
@@ -444,6 +446,12 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
 #pragma unroll
             for (int c = 0; c < 5; ++c)
                 u[j][c] = p.U[c][o];
+        } else if constexpr (Src::kHalo5) {
+            T v[5];
+            src.halo5(p.U, t, gx, gy, gz, snb, v);
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                prim(W, c, sb + si[j]) = v[c];
         } else {
 #pragma unroll 1
             for (int c = 0; c < 5; ++c)

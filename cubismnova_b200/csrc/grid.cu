@@ -233,6 +233,7 @@ const char *cn_status_string(cn_status s)
     case CN_ERR_DEVICE: return "device kernel reported an error";
     case CN_ERR_UNSUPPORTED: return "unsupported";
     case CN_ERR_TOO_MANY_BC: return "too many boundary conditions on one block field";
+    case CN_ERR_FILE: return "file could not be opened, read or written";
     }
     return "unknown status";
 }

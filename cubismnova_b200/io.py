@@ -1,4 +1,5 @@
-"""IO: grids to and from array-of-structures (AoS) file buffers on the GPU.
+"""IO: grids to and from array-of-structures (AoS) file buffers on the GPU,
+HDF5 container files and their XDMF wrappers.
 
 The reference writes a grid by gathering every block field into one AoS
 buffer on the host (IO/CartesianHDF.h:76-80, Field2AOS of IO/FieldAOS.h) and
@@ -8,19 +9,20 @@ gather (and the scatter of the read) is one kernel over the whole grid
 (``cn_grid_to_aos`` / ``cn_grid_from_aos``); the buffer is a CUDA tensor of
 shape (z, y, x, components).
 
-No HDF5 library is part of this build, so ``CartesianWriteHDF`` and
-``CartesianReadHDF`` behave as the reference built without HDF
-(``CUBISM_USE_HDF`` undefined, IO/CartesianHDF.h:92-95, 188-191): they print
-"HDF not supported" and return.  ``CartesianWriteXDMF`` / ``CartesianReadXDMF``
-write and read the same dataset as a raw little-endian binary file with the
-reference's XDMF wrapper pointing at it (``Format="Binary"`` instead of
-``"HDF"``), which XDMF readers open directly.
+``CartesianWriteHDF`` / ``CartesianReadHDF`` write and read that dataset in
+an HDF5 file (``fname.h5``) and the reference's XDMF wrapper
+(``Format="HDF"``).  The library lays the HDF5 file out itself, from the
+published file-format specification (no libhdf5 in this build): superblock
+version 0, an old-style root group, version 1 object headers, the data
+contiguous.  ``h5_write`` / ``h5_query`` / ``h5_read`` are the host-side file
+calls (no GPU).  ``CartesianWriteXDMF`` / ``CartesianReadXDMF`` keep the
+dataset as a raw little-endian binary file beside the same wrapper
+(``Format="Binary"``).
 """
 from __future__ import annotations
 
 import ctypes as C
 import os
-import sys
 
 import numpy as np
 
@@ -113,65 +115,85 @@ def AOS2Field(buf, grid, span=None, comps=None, face_dir=0, stream=None):
                                            C.c_void_p(buf.data_ptr()), _stream_handle(stream)))
 
 
-def CartesianWriteHDF(fname, aname, grid, time=0.0, face_dir=0, create_xdmf=True, file_dtype=None, span=None):
-    """IO::CartesianWriteHDF (IO/CartesianHDF.h:42-96, 113-131) of a build without
-    HDF5: prints the reference's message and writes nothing."""
-    sys.stderr.write(f"CartesianWriteHDF: HDF not supported ({fname})\n")
+_DT_OF_CODE = {v: k for k, v in _DT.items()}
 
 
-def CartesianReadHDF(fname, grid, face_dir=0, file_dtype=None, span=None):
-    """IO::CartesianReadHDF (IO/CartesianHDF.h:147-192, 206-220) of a build without
-    HDF5: prints the reference's message and reads nothing."""
-    sys.stderr.write(f"CartesianReadHDF: HDF not supported ({fname})\n")
+def h5_write(path, array, dataset="data", chunked=False):
+    """Writes a host array (float64, float32 or int32) as dataset ``dataset``
+    of an HDF5 file (root group); ``chunked``: one chunk over the dataset, the
+    layout the reference's ``H5Pset_chunk(dims)`` gives (under 4 GiB)."""
+    a = np.ascontiguousarray(array)
+    if a.dtype.newbyteorder("=") not in _DT or a.ndim < 1:
+        raise ValueError(f"h5_write: float64, float32 or int32 arrays of rank >= 1, not {a.dtype} rank {a.ndim}")
+    a = a.astype(a.dtype.newbyteorder("<"), copy=False)
+    dims = (C.c_longlong * a.ndim)(*a.shape)
+    _lib.check(_lib.lib().cn_h5_write(os.fsencode(path), dataset.encode(), a.ndim, dims,
+                                      _DT[np.dtype(a.dtype.newbyteorder("="))], C.c_void_p(a.ctypes.data),
+                                      int(bool(chunked))))
 
 
-def _xdmf(fname, aname, g, b, e, nc, fdt, time):
+def h5_query(path, dataset="data"):
+    """(shape, dtype) of a dataset in the root group of an HDF5 file."""
+    rank, dt = C.c_int(), C.c_int()
+    dims = (C.c_longlong * 32)()
+    _lib.check(_lib.lib().cn_h5_query(os.fsencode(path), dataset.encode(), C.byref(rank), dims, C.byref(dt)))
+    return tuple(int(dims[i]) for i in range(rank.value)), _DT_OF_CODE[dt.value]
+
+
+def h5_read(path, dataset="data", count=None, dtype=None):
+    """The hyperslab [0, count) (default: the whole dataset) of a dataset as a
+    host array of ``dtype`` (default: the file's)."""
+    shape, fdt = h5_query(path, dataset)
+    cnt = tuple(shape if count is None else (int(c) for c in count))
+    out = np.empty(cnt, dtype=np.dtype(dtype or fdt))
+    if out.dtype not in _DT:
+        raise ValueError(f"h5_read: float64, float32 or int32 output, not {out.dtype}")
+    _lib.check(_lib.lib().cn_h5_read(os.fsencode(path), dataset.encode(), len(cnt), (C.c_longlong * len(cnt))(*cnt),
+                                     _DT[out.dtype], C.c_void_p(out.ctypes.data)))
+    return out
+
+
+def CartesianWriteHDF(fname, aname, grid, time=0.0, face_dir=0, create_xdmf=True, file_dtype=None, span=None,
+                      stream=None):
+    """IO::CartesianWriteHDF (IO/CartesianHDF.h:42-96, 113-131 with
+    src/IO/HDFDriver.cpp:25-111): the grid's values on the file range
+    ``span`` (default: the whole grid) as dataset "data" of dims
+    (z, y, x, components) and type ``file_dtype`` (default: the grid's) in
+    ``fname.h5``, plus ``fname.xmf`` for cell and node data when
+    ``create_xdmf``.  Gathered on the GPU in one kernel, copied down once."""
+    g = _scalar_grid(grid, face_dir)
+    b, e = _span(grid, span, face_dir)
+    fdt = np.dtype(file_dtype or g.dtype)
+    _lib.check(_lib.lib().cn_grid_write_hdf(g.handle, os.fsencode(fname), aname.encode(), 0, g.ncomp,
+                                            _lib.ivec3(b), _lib.ivec3(e), _DT[fdt], float(time),
+                                            int(bool(create_xdmf)), _stream_handle(stream)))
+
+
+def CartesianReadHDF(fname, grid, face_dir=0, file_dtype=None, span=None, stream=None):
+    """IO::CartesianReadHDF (IO/CartesianHDF.h:147-192, 206-220 with
+    src/IO/HDFDriver.cpp:113-165): the hyperslab [0, count) of dataset
+    "data" in ``fname.h5`` (count: the range's extent and the grid's
+    components) into the grid's file range; a missing file raises the
+    reference's "CartesianReadHDF: File 'fname' does not exist"."""
+    g = _scalar_grid(grid, face_dir)
+    b, e = _span(grid, span, face_dir)
+    fdt = np.dtype(file_dtype or g.dtype)
+    _lib.check(_lib.lib().cn_grid_read_hdf(g.handle, os.fsencode(fname), 0, g.ncomp, _lib.ivec3(b), _lib.ivec3(e),
+                                           _DT[fdt], _stream_handle(stream)))
+
+
+_ENTITY_CODE = {"cell": 0, "node": 1}
+
+
+def _xdmf(fname, aname, g, b, e, nc, fdt, time, fmt="Binary"):
     """XDMF wrapper of IO/XDMFDriver.h:31-160 (uniform mesh, cell or node
-    data) for the dataset in fname.bin."""
-    dims = 3
-    h = g.getCellSize()
-    origin = getattr(g, "_begin", (0.0, 0.0, 0.0))
-    node = g.entity == "node"
-    ext = [e[d] - b[d] for d in range(3)]
-    # the mesh of the range: its cells (nodes minus one for node data)
-    mesh_nodes = [ext[d] if node else ext[d] + 1 for d in range(3)]
-    org = [origin[d] + b[d] * h[d] for d in range(3)]
-    attr = "Scalar" if nc == 1 else ("Vector" if nc == dims else "Tensor")
-    ntype = "Int" if fdt == np.dtype(np.int32) else "Float"
-    zyx = lambda v: " ".join(str(v[2 - i]) for i in range(3))
-    fmt = lambda v: " ".join(repr(float(v[2 - i])) for i in range(3))
-    base = os.path.basename(fname)
-    lines = [
-        '<?xml version="1.0" ?>',
-        '<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>',
-        '<Xdmf Version="2.0">',
-        "<Domain>",
-        '\t<Grid GridType="Uniform">',
-        f'\t\t<Time Value="{time:e}"/>',
-        "",
-        f'\t\t<Topology TopologyType="3DCoRectMesh" Dimensions="{zyx(mesh_nodes)}"/>',
-        "",
-        '\t\t<Geometry GeometryType="Origin_DxDyDz">',
-        '\t\t\t<DataItem Name="Origin" Dimensions="3" NumberType="Float" Precision="8" Format="XML">',
-        f"\t\t\t\t{fmt(org)}",
-        "\t\t\t</DataItem>",
-        '\t\t\t<DataItem Name="Spacing" Dimensions="3" NumberType="Float" Precision="8" Format="XML">',
-        f"\t\t\t\t{fmt(h)}",
-        "\t\t\t</DataItem>",
-        "\t\t</Geometry>",
-        "",
-        f'\t\t<Attribute Name="{aname}" AttributeType="{attr}" Center="{"Node" if node else "Cell"}">',
-        f'\t\t\t<DataItem Dimensions="{zyx(ext)} {nc}" NumberType="{ntype}" Precision="{fdt.itemsize}" '
-        f'Format="Binary" Endian="Little">',
-        f"\t\t\t\t./{base}.bin",
-        "\t\t\t</DataItem>",
-        "\t\t</Attribute>",
-        "\t</Grid>",
-        "</Domain>",
-        "</Xdmf>",
-    ]
-    with open(fname + ".xmf", "w") as f:
-        f.write("\n".join(lines) + "\n")
+    data, ``cn_xdmf_write``) for the dataset in fname.bin (``fmt`` "Binary")
+    or fname.h5:/data ("HDF")."""
+    h = (C.c_double * 3)(*[float(v) for v in g.getCellSize()])
+    origin = (C.c_double * 3)(*[float(v) for v in getattr(g, "_begin", (0.0, 0.0, 0.0))])
+    _lib.check(_lib.lib().cn_xdmf_write(os.fsencode(fname), aname.encode(), _ENTITY_CODE[g.entity], _lib.ivec3(b),
+                                        _lib.ivec3(e), origin, h, int(nc), _DT[np.dtype(fdt)], float(time),
+                                        0 if fmt == "HDF" else 1))
 
 
 def CartesianWriteXDMF(fname, aname, grid, time=0.0, face_dir=0, create_xdmf=True, file_dtype=None, span=None,

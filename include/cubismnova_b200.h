@@ -50,7 +50,8 @@ typedef enum cn_status {
     CN_ERR_OUT_OF_MEMORY = 10,
     CN_ERR_DEVICE = 11,          /* a kernel reported an error word */
     CN_ERR_UNSUPPORTED = 12,
-    CN_ERR_TOO_MANY_BC = 13
+    CN_ERR_TOO_MANY_BC = 13,
+    CN_ERR_FILE = 14             /* a file could not be opened, read or written, or is not a readable HDF5 file */
 } cn_status;
 
 typedef enum cn_dtype { CN_FLOAT32 = 0, CN_FLOAT64 = 1, CN_INT32 = 2 } cn_dtype;
@@ -172,6 +173,53 @@ cn_status cn_grid_to_aos(cn_grid *g, int comp0, int ncomp, const int span_begin[
  * (CN_ERR_UNSUPPORTED). */
 cn_status cn_grid_from_aos(cn_grid *g, int comp0, int ncomp, const int span_begin[3], const int span_end[3],
                            cn_dtype file_dtype, const void *d_buf, void *stream);
+
+/* ------------------------------------------------------- HDF5 / XDMF files */
+/* IO::CartesianWriteHDF of a grid (IO/CartesianHDF.h:42-96 with
+ * src/IO/HDFDriver.cpp:25-111): the file range [begin, end) of components
+ * [comp0, comp0 + ncomp) (ncomp < 0: all from comp0) gathered on the device
+ * (cn_grid_to_aos), written as dataset "data" of dims (z, y, x, ncomp) and
+ * type file_dtype into `fname.h5`; with create_xdmf, the reference's
+ * message "CartesianWriteHDF: Allocating %.1f MB file buffer (fname)" on
+ * stdout and, for cell and node data, the XDMF wrapper `fname.xmf`
+ * (IO/XDMFDriver.h:31-160, Format="HDF", "./basename.h5:/data").
+ * The HDF5 file is written without libhdf5, in the format libhdf5 writes
+ * with its default bounds (superblock 0, v1 object headers); the data is
+ * contiguous.  Synchronises the stream. */
+cn_status cn_grid_write_hdf(cn_grid *g, const char *fname, const char *aname, int comp0, int ncomp,
+                            const int begin[3], const int end[3], cn_dtype file_dtype, double time,
+                            int create_xdmf, void *stream);
+/* IO::CartesianReadHDF (IO/CartesianHDF.h:147-192 with
+ * src/IO/HDFDriver.cpp:113-165): reads the hyperslab [0, count) of dataset
+ * "data" in `fname.h5` (count = the range's (z, y, x) extent and ncomp,
+ * values converted to file_dtype) into the range of the grid
+ * (cn_grid_from_aos).  A missing file: CN_ERR_FILE with the reference's
+ * message "CartesianReadHDF: File 'fname' does not exist".  Synchronises
+ * the stream. */
+cn_status cn_grid_read_hdf(cn_grid *g, const char *fname, int comp0, int ncomp, const int begin[3],
+                           const int end[3], cn_dtype file_dtype, void *stream);
+/* Host-side HDF5 files of one dataset (no GPU needed).
+ * cn_h5_write: `path` with dataset `dataset` (root group) of `rank` dims,
+ * row-major values of dtype from host_buf; chunked != 0 stores it as one
+ * chunk (the reference's H5Pset_chunk(dims) layout, < 4 GiB), else
+ * contiguous.
+ * cn_h5_query: rank, dims and type of a dataset in the root group.
+ * cn_h5_read: the hyperslab [0, count) of a dataset into host_buf (row-major,
+ * dtype; file values converted: FP64 <-> FP32, integers -> any).  Reads files
+ * of superblock version 0 or 1 (after a user block), old-style groups, v1
+ * object headers and compact, contiguous or chunked (unfiltered) layouts. */
+cn_status cn_h5_write(const char *path, const char *dataset, int rank, const long long *dims, cn_dtype dtype,
+                      const void *host_buf, int chunked);
+cn_status cn_h5_query(const char *path, const char *dataset, int *rank, long long dims[32], cn_dtype *dtype);
+cn_status cn_h5_read(const char *path, const char *dataset, int rank, const long long *count, cn_dtype dtype,
+                     void *host_buf);
+/* The XDMF wrapper (IO/XDMFDriver.h:31-160) `fname.xmf` of the file range
+ * [begin, end) of cell or node data on the uniform mesh with origin and
+ * spacing h: format 0 refers to "./basename.h5:/data" (Format="HDF"),
+ * format 1 to the raw little-endian file "./basename.bin" (Format="Binary"). */
+cn_status cn_xdmf_write(const char *fname, const char *aname, cn_entity entity, const int begin[3],
+                        const int end[3], const double origin[3], const double h[3], int ncomp,
+                        cn_dtype file_dtype, double time, int format);
 
 /* -------------------------------------------------------------------- BC */
 /* field.getBC().push_back(new BC::Kind(dir, side, value))

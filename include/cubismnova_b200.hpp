@@ -14,7 +14,7 @@
 //   Core::Stencil          Core/Stencil.h:21-108
 //   Ops::laplacian/gradient/lapGrad/divergence   the benchmark stencils
 //   IO::Field2AOS/AOS2Field/gatherAOS   IO/FieldAOS.h over every block
-//   IO::CartesianWriteHDF/ReadHDF       IO/CartesianHDF.h without HDF5
+//   IO::CartesianWriteHDF/ReadHDF       IO/CartesianHDF.h (HDF5 files written by the library)
 //
 // Errors raise std::runtime_error with the reference's message where the
 // reference throws (Core/Stencil.h:101-106, Block/FieldLab.h:189-190,
@@ -452,17 +452,41 @@ template <typename FileT, typename T> std::vector<FileT> gatherAOS(Grid::Cartesi
     return host;
 }
 
-/// IO::CartesianWriteHDF / CartesianReadHDF (IO/CartesianHDF.h:42-96,
-/// 147-192) as built without HDF5 (CUBISM_USE_HDF undefined): the
-/// reference's message on stderr, no file.
-template <typename FileT, typename GridT>
-void CartesianWriteHDF(const std::string &fname, const std::string &, const GridT &, double, size_t = 0, bool = true)
+/// IO::CartesianWriteHDF (IO/CartesianHDF.h:113-131 with
+/// src/IO/HDFDriver.cpp:25-111): the whole grid as dataset "data" of dims
+/// (z, y, x, components) and type FileT in `fname.h5`, plus the XDMF wrapper
+/// `fname.xmf` for cell and node data when create_xdmf.  The HDF5 file is
+/// written by the library (no libhdf5 needed).
+template <typename FileT, typename T>
+void CartesianWriteHDF(const std::string &fname, const std::string &aname, Grid::Cartesian<T> &grid, double time,
+                       size_t = 0, bool create_xdmf = true)
 {
-    std::fprintf(stderr, "CartesianWriteHDF: HDF not supported (%s)\n", fname.c_str());
+    const Core::IndexRange r = indexRange(grid);
+    check(cn_grid_write_hdf(grid.raw(), fname.c_str(), aname.c_str(), 0, grid.getComponents(), r.begin.data(),
+                            r.end.data(), DType<FileT>::value, time, create_xdmf ? 1 : 0, nullptr));
 }
-template <typename FileT, typename GridT> void CartesianReadHDF(const std::string &fname, GridT &, size_t = 0)
+/// The face grid of direction face_dir of a face container
+/// (IO/FieldAOS.h:136-149); no XDMF wrapper for face data, as in the reference.
+template <typename FileT, typename T>
+void CartesianWriteHDF(const std::string &fname, const std::string &aname, Grid::FaceCartesian<T> &grid, double time,
+                       size_t face_dir = 0, bool create_xdmf = true)
 {
-    std::fprintf(stderr, "CartesianReadHDF: HDF not supported (%s)\n", fname.c_str());
+    CartesianWriteHDF<FileT>(fname, aname, grid.face((int)face_dir), time, 0, create_xdmf);
+}
+/// IO::CartesianReadHDF (IO/CartesianHDF.h:206-220 with
+/// src/IO/HDFDriver.cpp:113-165): the hyperslab of the grid's extent from
+/// `fname.h5`; a missing file throws "CartesianReadHDF: File 'fname' does not
+/// exist", as the reference.
+template <typename FileT, typename T> void CartesianReadHDF(const std::string &fname, Grid::Cartesian<T> &grid, size_t = 0)
+{
+    const Core::IndexRange r = indexRange(grid);
+    check(cn_grid_read_hdf(grid.raw(), fname.c_str(), 0, grid.getComponents(), r.begin.data(), r.end.data(),
+                           DType<FileT>::value, nullptr));
+}
+template <typename FileT, typename T>
+void CartesianReadHDF(const std::string &fname, Grid::FaceCartesian<T> &grid, size_t face_dir = 0)
+{
+    CartesianReadHDF<FileT>(fname, grid.face((int)face_dir));
 }
 } // namespace IO
 

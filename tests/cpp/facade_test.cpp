@@ -216,6 +216,24 @@ int main()
         for (int b = 0; b < 8; ++b)
             for (int i = 0; i < 64; ++i)
                 EXPECT(back[(size_t)b * g3.blockStride() + i] == h2[(size_t)b * g2.blockStride() + i]);
+        // CartesianWriteHDF / CartesianReadHDF through an HDF5 file (FP32
+        // file values of an FP64 grid whose values are exact in FP32)
+        IO::CartesianWriteHDF<float>("facade_u", "u", g2, 0.5);
+        g3.upload(z3.data());
+        IO::CartesianReadHDF<float>("facade_u", g3);
+        g3.download(back.data());
+        for (size_t i = 0; i < back.size(); ++i) EXPECT(back[i] == h2[i]);
+        int rank = 0;
+        long long dims[32];
+        cn_dtype dt;
+        check(cn_h5_query("facade_u.h5", "data", &rank, dims, &dt));
+        EXPECT(rank == 4 && dims[0] == 8 && dims[1] == 8 && dims[2] == 8 && dims[3] == 1 && dt == CN_FLOAT32);
+        try {
+            IO::CartesianReadHDF<float>("no_such_file", g3);
+            EXPECT(false);
+        } catch (const std::runtime_error &e) {
+            EXPECT(std::string(e.what()) == "CartesianReadHDF: File 'no_such_file' does not exist");
+        }
     }
     std::printf("%s (%d failures)\n", failures ? "FAIL" : "PASS", failures);
     return failures ? 1 : 0;

@@ -2,7 +2,8 @@
 the block loops of IO::CartesianWriteHDF / CartesianReadHDF over Field2AOS /
 AOS2Field) against the oracle (oracle/aos.py, itself pinned to the
 reference's FieldAOS.h), bit for bit; a full-size round trip; the XDMF
-writer and reader; error behaviour."""
+writer and reader; HDF5 files of grids (CartesianWriteHDF / ReadHDF); error
+behaviour."""
 import ctypes as C
 import os
 import xml.etree.ElementTree as ET
@@ -192,10 +193,49 @@ def test_xdmf_write_read(cn, tmp_path, capsys):
     for c in range(3):
         assert np.array_equal(h.download(c), A.aos_to_grid(data, [np.zeros(g.comp_stride)] * 3, nb, cells, 0,
                                                            g.block_stride, b, e)[c])
-    # without HDF5 the reference's writer reports and writes nothing
-    cn.IO.CartesianWriteHDF(str(tmp_path / "u"), "U", g, 0.0)
-    assert "CartesianWriteHDF: HDF not supported" in capsys.readouterr().err
-    assert not os.path.exists(str(tmp_path / "u.h5"))
+    g.close()
+    h.close()
+
+
+@pytest.mark.parametrize("entity,file_dtype", [(0, np.float64), (0, np.float32), (1, np.float64), (2, np.float32),
+                                               (4, np.float64)])
+def test_hdf_write_read(cn, tmp_path, capfd, entity, file_dtype):
+    """CartesianWriteHDF: the HDF5 dataset "data" (z, y, x, components) equals
+    the oracle's AoS buffer of the grid bit for bit, the XDMF wrapper points
+    at it (cell and node data only); CartesianReadHDF restores the grid."""
+    import torch
+    rng = np.random.default_rng(40 + entity)
+    nb, cells = (2, 1, 3), (4, 6, 4)
+    ncomp = 3 if entity == 0 else 2
+    g, comps = _grid(cn, rng, entity, ncomp, np.float64, nb, cells)
+    fname = str(tmp_path / f"q{entity}")
+    cn.IO.CartesianWriteHDF(fname, "q", g, time=1.5, file_dtype=file_dtype)
+    torch.cuda.synchronize()
+    b, e = cn.IO.index_range(g)
+    shape, fdt = cn.IO.h5_query(fname + ".h5")
+    assert shape == (e[2], e[1], e[0], ncomp) and fdt == np.dtype(file_dtype)
+    data = cn.IO.h5_read(fname + ".h5")
+    want = A.grid_to_aos(comps, nb, cells, entity, g.block_stride, b, e,
+                         np.zeros(int(np.prod(e)) * ncomp, file_dtype))
+    assert np.array_equal(data.ravel().view(np.uint8), want.view(np.uint8))
+    out = capfd.readouterr().out
+    mb = data.nbytes / 1024.0 / 1024.0
+    assert f"CartesianWriteHDF: Allocating {mb:.1f} MB file buffer ({fname})" in out
+    if entity in (0, 1):
+        item = ET.parse(fname + ".xmf").getroot().find("Domain/Grid/Attribute/DataItem")
+        assert item.get("Format") == "HDF" and item.text.strip() == f"./q{entity}.h5:/data"
+        assert item.get("Dimensions") == f"{e[2]} {e[1]} {e[0]} {ncomp}"
+    else:
+        assert not os.path.exists(fname + ".xmf")  # no wrapper for face data (src/IO/HDFDriver.cpp:53-57)
+    h = cn.Grid.Cartesian(nb, cells, ncomp=ncomp, entity=ENT[entity])
+    cn.IO.CartesianReadHDF(fname, h, file_dtype=file_dtype)
+    torch.cuda.synchronize()
+    back = A.aos_to_grid(data.ravel(), [np.zeros(g.comp_stride)] * ncomp, nb, cells, entity, g.block_stride, b, e)
+    for c in range(ncomp):
+        assert np.array_equal(h.download(c), back[c])
+    with pytest.raises(cn.CnError) as err:
+        cn.IO.CartesianReadHDF(str(tmp_path / "none"), h)
+    assert str(err.value) == f"CartesianReadHDF: File '{tmp_path / 'none'}' does not exist"
     g.close()
     h.close()
 

@@ -4,6 +4,7 @@ node centring, file ranges, attribute types."""
 import xml.etree.ElementTree as ET
 
 import numpy as np
+import pytest
 
 from cubismnova_b200 import io as IO
 
@@ -55,12 +56,25 @@ def test_node_data_subrange_and_types(tmp_path):
     assert x["type"] == "Tensor" and x["ntype"] == "Int" and x["prec"] == "4" and x["dims"] == "2 2 2 9"
 
 
-def test_without_hdf5_the_writers_report(capsys):
-    IO.CartesianWriteHDF("out/f", "rho", None, 0.0)
-    IO.CartesianReadHDF("out/f", None)
-    err = capsys.readouterr().err
-    assert "CartesianWriteHDF: HDF not supported (out/f)" in err
-    assert "CartesianReadHDF: HDF not supported (out/f)" in err
+def test_hdf_wrapper_points_at_the_dataset(tmp_path):
+    """Format="HDF" and "./basename.h5:/data", as IO/XDMFDriver.h:155-156."""
+    g = _Grid("cell", (1.0, 1.0, 1.0), (0.0, 0.0, 0.0))
+    IO._xdmf(str(tmp_path / "p"), "p", g, (0, 0, 0), (4, 4, 4), 1, np.dtype(np.float64), 2.0, fmt="HDF")
+    x = _parse(tmp_path / "p.xmf")
+    assert x["fmt"] == "HDF" and x["file"] == "./p.h5:/data" and x["endian"] is None
+    assert x["dims"] == "4 4 4 1" and x["prec"] == "8" and x["time"] == 2.0
+
+
+def test_face_data_gets_no_wrapper(tmp_path):
+    from cubismnova_b200 import _lib
+    g = _Grid("face_x", (1.0, 1.0, 1.0), (0.0, 0.0, 0.0))
+    IO._ENTITY_CODE["face_x"] = 2
+    try:
+        with pytest.raises(_lib.CnError) as e:
+            IO._xdmf(str(tmp_path / "f"), "f", g, (0, 0, 0), (2, 2, 2), 1, np.dtype(np.float64), 0.0)
+        assert e.value.status == 12
+    finally:
+        del IO._ENTITY_CODE["face_x"]
 
 
 class _Topo:
