@@ -521,7 +521,7 @@ class C4(Euler):
 
 class C3:
     autotune = True  # bench.py --no-autotune: the default schedule (profiling runs)
-    fixed_schedule = None  # bench.py --amr-schedule ORDER CTAS UNIT
+    fixed_schedule = None  # bench.py --amr-schedule ORDER CTAS TX TY TZ
     """Batched two-level AMR step: 2048 blocks whose sizes are drawn by seed
     from {8^3: 50 %, 16^3: 35 %, 32^3: 15 %} (workloads.amr_layout: about
     13.5 M cells, a level-0 tiling refined in a seeded ball), level-interface
@@ -559,21 +559,21 @@ class C3:
         self.nb, self.n = (len(l),), tuple(int(e) for e in F)
         # CFL on the fine level (h = 1/Lx), sound speed of the pulse state < 1.3
         self.dt = 0.3 / (3 * 1.3 * F[0])
+        def work_tile(shape):
+            return (f"{8 * shape[0]}x{8 * shape[1]}x{8 * shape[2]} cells "
+                    f"({shape[0]}x{shape[1]}x{shape[2]} tiles of 8^3, clipped to the block)")
         if self.fixed_schedule is not None:
-            order, ctas, unit = self.fixed_schedule
+            order, ctas, shape = self.fixed_schedule[0], self.fixed_schedule[1], tuple(self.fixed_schedule[2:])
             for g in (self.U, self.w1, self.w2):
-                g.set_schedule(order, ctas, unit)
+                g.set_schedule(order, ctas, shape=shape)
             self.schedule = dict(order=["block order", "largest blocks first", "Morton"][order], ctas=ctas,
-                                 work_unit=f"{8 * unit}x8x8 cells ({unit} tile{'s' if unit > 1 else ''} of 8^3)",
-                                 autotuned=False)
+                                 work_tile=work_tile(shape), autotuned=False)
         elif self.autotune:
             order, ctas, ms = cn.amr.autotune(self.U, self.w1, self.w2, self.dt, reps=2)
-            unit = self.U.schedule()[2]
             self.schedule = dict(order=["block order", "largest blocks first", "Morton"][order], ctas=ctas,
-                                 work_unit=f"{8 * unit}x8x8 cells ({unit} tile{'s' if unit > 1 else ''} of 8^3)",
-                                 ms_per_step=round(ms, 3))
+                                 work_tile=work_tile(self.U.work_shape()), ms_per_step=round(ms, 3))
         else:
-            self.schedule = dict(order="largest blocks first", ctas=0, work_unit="8x8x8 cells (1 tile)",
+            self.schedule = dict(order="largest blocks first", ctas=0, work_tile=work_tile((1, 1, 1)),
                                  autotuned=False)
         cn.workloads.euler_pulse_amr(self.U)
         self.stream = torch.cuda.Stream()
@@ -1448,9 +1448,9 @@ def main():
     ap.add_argument("--mg-nu", type=int, nargs=2, default=None, help="c5: pre- and post-smoothing sweeps (default 2 2)")
     ap.add_argument("--nn-training", default=None, choices=["tensor", "fp32"],
                     help="c5: training arithmetic of the learned smoother (default tensor)")
-    ap.add_argument("--amr-schedule", type=int, nargs=3, default=None, metavar=("ORDER", "CTAS", "UNIT"),
+    ap.add_argument("--amr-schedule", type=int, nargs=5, default=None, metavar=("ORDER", "CTAS", "TX", "TY", "TZ"),
                     help="c3: a fixed schedule instead of the autotuner's (order 0-2, persistent CTAs, "
-                         "work-unit tiles 1/2/4)")
+                         "work tile of TX x TY x TZ 8^3 tiles, each 1/2/4)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="c3: keep the default schedule instead of autotuning it (profiling runs)")
     ap.add_argument("--blocks", type=int, nargs=3, default=None,

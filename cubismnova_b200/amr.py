@@ -25,6 +25,8 @@ _lib.register({
     "cn_amr_set_schedule": (_I, [_P, _I, _I]),
     "cn_amr_set_work_unit": (_I, [_P, _I]),
     "cn_amr_get_schedule": (_I, [_P, C.POINTER(C.c_int)]),
+    "cn_amr_set_work_shape": (_I, [_P, C.POINTER(C.c_int)]),
+    "cn_amr_get_work_shape": (_I, [_P, C.POINTER(C.c_int)]),
     "cn_amr_autotune": (_I, [_P, _P, _P, _D, _D, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_D), _P]),
     "cn_graph_begin": (_I, [_P]),
     "cn_graph_end": (_I, [_P, C.POINTER(_P)]),
@@ -108,17 +110,26 @@ class AmrGrid:
                                               _stream_handle(None)))
         return buf
 
-    def set_schedule(self, order: int, ctas: int, unit: int = None):
-        """Work-list order, persistent grid size and (optionally) the work
-        unit: 1, 2 or 4 consecutive 8^3 tiles along x per CTA work item."""
+    def set_schedule(self, order: int, ctas: int, unit: int = None, shape=None):
+        """Work-list order, persistent grid size and (optionally) the CTA's
+        work tile: ``shape`` = 8^3 tiles along (x, y, z), each 1, 2 or 4, or
+        ``unit`` = t for the shape (t, 1, 1)."""
         if unit is not None:
             _lib.check(_lib.lib().cn_amr_set_work_unit(self._h, unit))
+        if shape is not None:
+            _lib.check(_lib.lib().cn_amr_set_work_shape(self._h, (C.c_int * 3)(*[int(v) for v in shape])))
         _lib.check(_lib.lib().cn_amr_set_schedule(self._h, order, ctas))
 
     def schedule(self):
-        """(order, ctas, work-unit tiles) of this layout."""
+        """(order, ctas, tiles per work tile) of this layout."""
         out = (C.c_int * 3)()
         _lib.check(_lib.lib().cn_amr_get_schedule(self._h, out))
+        return tuple(out)
+
+    def work_shape(self):
+        """The CTA's work tile in 8^3 tiles along (x, y, z)."""
+        out = (C.c_int * 3)()
+        _lib.check(_lib.lib().cn_amr_get_work_shape(self._h, out))
         return tuple(out)
 
     def box(self):
@@ -155,8 +166,9 @@ def rk3_step(U: AmrGrid, w1: AmrGrid, w2: AmrGrid, dt: float, gamma: float = 1.4
 
 
 def autotune(U: AmrGrid, w1: AmrGrid, w2: AmrGrid, dt: float, gamma: float = 1.4, reps: int = 2, stream=None):
-    """Picks the fastest work-list order, work unit and persistent grid
-    (advances U); returns (order, ctas, ms), the unit by U.schedule()."""
+    """Picks the fastest work-list order, work-tile shape and persistent
+    grid (advances U); returns (order, ctas, ms), the shape by
+    U.work_shape()."""
     o, c, ms = C.c_int(), C.c_int(), C.c_double()
     _lib.check(_lib.lib().cn_amr_autotune(U.handle, w1.handle, w2.handle, dt, gamma, reps, C.byref(o), C.byref(c),
                                           C.byref(ms), _stream_handle(stream)))

@@ -109,7 +109,7 @@ struct cn_amr {
     int2 *d_work = nullptr, *d_items = nullptr;
     int order = 1;   // work-list order (see cn_amr_set_schedule)
     int ctas = 0;    // persistent grid size (0: one CTA per item)
-    int unit = 1;    // tiles per work item along x (cn_amr_set_work_unit)
+    int shape[3] = {1, 1, 1}; // work tile: 8^3 tiles per work item along x, y, z (cn_amr_set_work_shape)
 };
 
 static uint64_t spread3(uint32_t v)
@@ -123,27 +123,35 @@ static uint64_t spread3(uint32_t v)
     return x;
 }
 
-// Work list: units of up to a->unit consecutive tiles along x of one block
-// (fewer where the block's row of tiles is shorter), ordered by the
-// schedule's key of their first tile, emitted tile by tile; one work item
-// per unit.
+// Work list: each block cut into work tiles of up to shape[0] x shape[1] x
+// shape[2] 8^3 tiles (clipped to the block), one work item per work tile,
+// its tiles emitted x fastest; items ordered by the schedule's key of their
+// first tile.
 static cn_status build_work(cn_amr *a)
 {
     struct Unit {
-        int block, t0, count, n;
+        int block, first, count, n; // tiles [first, first + count) of `tiles`
         uint64_t key;
     };
     std::vector<Unit> units;
+    std::vector<int> tiles;
     for (int b = 0; b < a->nblocks; ++b) {
         const BlockDev &B = a->blocks[b];
         const int tpd = B.n / 8, cs = B.level == 0 ? 2 : 1;
-        const int run = a->unit < tpd ? a->unit : tpd;
-        for (int t = 0; t < tpd * tpd * tpd; t += run) {
-            const int tx = t % tpd, ty = (t / tpd) % tpd, tz = t / (tpd * tpd);
-            const uint32_t X = (uint32_t)(B.ox + tx * 8 * cs), Y = (uint32_t)(B.oy + ty * 8 * cs),
-                           Z = (uint32_t)(B.oz + tz * 8 * cs);
-            units.push_back({b, t, run, B.n, spread3(X) | spread3(Y) << 1 | spread3(Z) << 2});
-        }
+        int u[3];
+        for (int d = 0; d < 3; ++d) u[d] = a->shape[d] < tpd ? a->shape[d] : tpd;
+        for (int bz = 0; bz < tpd; bz += u[2])
+            for (int by = 0; by < tpd; by += u[1])
+                for (int bx = 0; bx < tpd; bx += u[0]) {
+                    const int first = (int)tiles.size();
+                    for (int tz = bz; tz < bz + u[2]; ++tz)
+                        for (int ty = by; ty < by + u[1]; ++ty)
+                            for (int tx = bx; tx < bx + u[0]; ++tx) tiles.push_back(tx + tpd * (ty + tpd * tz));
+                    const uint32_t X = (uint32_t)(B.ox + bx * 8 * cs), Y = (uint32_t)(B.oy + by * 8 * cs),
+                                   Z = (uint32_t)(B.oz + bz * 8 * cs);
+                    units.push_back({b, first, (int)tiles.size() - first, B.n,
+                                     spread3(X) | spread3(Y) << 1 | spread3(Z) << 2});
+                }
     }
     if (a->order == 1) {
         std::stable_sort(units.begin(), units.end(), [](const Unit &l, const Unit &r) { return l.n > r.n; });
@@ -154,7 +162,7 @@ static cn_status build_work(cn_amr *a)
     a->items.clear();
     for (const Unit &u : units) {
         a->items.push_back(make_int2((int)a->work.size(), u.count));
-        for (int k = 0; k < u.count; ++k) a->work.push_back(make_int2(u.block, u.t0 + k));
+        for (int k = 0; k < u.count; ++k) a->work.push_back(make_int2(u.block, tiles[u.first + k]));
     }
     if (a->d_work) cudaFree(a->d_work);
     if (a->d_items) cudaFree(a->d_items);
@@ -402,16 +410,32 @@ cn_status cn_amr_set_schedule(cn_amr *a, int order, int ctas)
     return CN_OK;
 }
 
-// Work unit: 1, 2 or 4 consecutive 8^3 tiles along x of a block per work
-// item (a CTA's unit: 8x8x8, 16x8x8 or 32x8x8 cells; fewer tiles where a
-// block's row is shorter).
+// Work tile of a CTA's work item: shape[d] in {1, 2, 4} 8^3 tiles along d
+// (8x8x8 up to 32x32x32 cells, clipped to the block).
+cn_status cn_amr_set_work_shape(cn_amr *a, const int shape[3])
+{
+    if (!a || !shape) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int d = 0; d < 3; ++d)
+        if (shape[d] != 1 && shape[d] != 2 && shape[d] != 4) return fail(CN_ERR_INVALID_ARGUMENT, "bad work shape");
+    if (shape[0] != a->shape[0] || shape[1] != a->shape[1] || shape[2] != a->shape[2]) {
+        for (int d = 0; d < 3; ++d) a->shape[d] = shape[d];
+        return build_work(a);
+    }
+    return CN_OK;
+}
+
+// 1, 2 or 4 consecutive tiles along x: the work shape (tiles, 1, 1)
 cn_status cn_amr_set_work_unit(cn_amr *a, int tiles)
 {
     if (!a || (tiles != 1 && tiles != 2 && tiles != 4)) return fail(CN_ERR_INVALID_ARGUMENT, "bad work unit");
-    if (tiles != a->unit) {
-        a->unit = tiles;
-        return build_work(a);
-    }
+    const int shape[3] = {tiles, 1, 1};
+    return cn_amr_set_work_shape(a, shape);
+}
+
+cn_status cn_amr_get_work_shape(const cn_amr *a, int shape[3])
+{
+    if (!a || !shape) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int d = 0; d < 3; ++d) shape[d] = a->shape[d];
     return CN_OK;
 }
 
@@ -420,14 +444,14 @@ cn_status cn_amr_get_schedule(const cn_amr *a, int out[3])
     if (!a || !out) return fail(CN_ERR_INVALID_ARGUMENT, "NULL argument");
     out[0] = a->order;
     out[1] = a->ctas;
-    out[2] = a->unit;
+    out[2] = a->shape[0] * a->shape[1] * a->shape[2];
     return CN_OK;
 }
 
-// Times every schedule candidate (orders 0..2, work units of 1, 2 and 4
-// tiles, grid = k x SMs x 3 CTAs for k in {1, 2, 4} or one CTA per work item)
-// over `reps` RK3 steps and keeps the fastest on all three layouts.  U is
-// advanced by the trial steps.
+// Times every schedule candidate (orders 0..2; work tiles of 1x1x1, 2x1x1,
+// 4x1x1, 1x2x1, 1x1x2, 2x2x1 and 2x2x2 8^3 tiles; grid = k x SMs x 3 CTAs
+// for k in {1, 2, 4} or one CTA per work item) over `reps` RK3 steps and
+// keeps the fastest on all three layouts.  U is advanced by the trial steps.
 cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, int reps, int *order_out,
                           int *ctas_out, double *ms_out, void *stream)
 {
@@ -437,19 +461,19 @@ cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double g
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grids[4] = {0, sms * 3, sms * 6, sms * 12};
-    const int units[3] = {1, 2, 4};
+    const int shapes[7][3] = {{1, 1, 1}, {2, 1, 1}, {4, 1, 1}, {1, 2, 1}, {1, 1, 2}, {2, 2, 1}, {2, 2, 2}};
     double best = 1e300;
-    int bo = 1, bc = 0, bu = 1;
+    int bo = 1, bc = 0, bs = 0;
     cudaEvent_t e0, e1;
     CN_CUDA_TRY(cudaEventCreate(&e0));
     CN_CUDA_TRY(cudaEventCreate(&e1));
-    for (int unit : units)
+    for (int si = 0; si < 7; ++si)
         for (int order = 0; order < 3; ++order)
             for (int gi = 0; gi < 4; ++gi) {
                 cn_status s;
                 cn_amr *all[3] = {U, w1, w2};
                 for (cn_amr *a : all) {
-                    if ((s = cn_amr_set_work_unit(a, unit)) != CN_OK) return s;
+                    if ((s = cn_amr_set_work_shape(a, shapes[si])) != CN_OK) return s;
                     if ((s = cn_amr_set_schedule(a, order, grids[gi])) != CN_OK) return s;
                 }
                 if ((s = cn_amr_rk3_step(U, w1, w2, dt, gamma, stream)) != CN_OK) return s; // warm-up
@@ -465,14 +489,14 @@ cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double g
                     best = ms;
                     bo = order;
                     bc = grids[gi];
-                    bu = unit;
+                    bs = si;
                 }
             }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cn_amr *all[3] = {U, w1, w2};
     for (cn_amr *a : all) {
-        cn_status s = cn_amr_set_work_unit(a, bu);
+        cn_status s = cn_amr_set_work_shape(a, shapes[bs]);
         if (s == CN_OK) s = cn_amr_set_schedule(a, bo, bc);
         if (s != CN_OK) return s;
     }

@@ -448,15 +448,18 @@ cn_status cn_amr_rk3_step(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double g
 /* Work-list order (0 block order, 1 largest blocks first, 2 Morton order of
  * tiles) and persistent grid (0: one CTA per work item). */
 cn_status cn_amr_set_schedule(cn_amr *a, int order, int ctas);
-/* Work unit of a CTA: 1, 2 or 4 consecutive 8^3 tiles along x of one block
- * per work item (8x8x8, 16x8x8 or 32x8x8 cells, fewer where a block's row is
- * shorter); the stage's compute tile stays 8^3. */
+/* Work tile of a CTA's work item: shape[d] in {1, 2, 4} 8^3 tiles along
+ * x, y, z of one block (8x8x8 up to 32x32x32 cells, clipped to the block),
+ * processed in turn by one CTA; the stage's compute tile stays 8^3.
+ * cn_amr_set_work_unit(a, t) is the shape (t, 1, 1). */
+cn_status cn_amr_set_work_shape(cn_amr *a, const int shape[3]);
 cn_status cn_amr_set_work_unit(cn_amr *a, int tiles);
-/* out = {order, ctas, work-unit tiles} of a layout. */
+cn_status cn_amr_get_work_shape(const cn_amr *a, int shape[3]);
+/* out = {order, ctas, tiles per work tile} of a layout. */
 cn_status cn_amr_get_schedule(const cn_amr *a, int out[3]);
-/* Times all schedules (orders x work units x grid sizes) over `reps` steps
- * (advancing U) and keeps the fastest; the unit chosen is read back with
- * cn_amr_get_schedule. */
+/* Times all schedules (orders x work-tile shapes x grid sizes) over `reps`
+ * steps (advancing U) and keeps the fastest; the shape chosen is read back
+ * with cn_amr_get_work_shape. */
 cn_status cn_amr_autotune(cn_amr *U, cn_amr *w1, cn_amr *w2, double dt, double gamma, int reps,
                           int *order_out, int *ctas_out, double *ms_out, void *stream);
 

@@ -85,18 +85,22 @@ def test_amr_schedules_and_graph_are_bitwise_identical(cn):
     w1, w2 = U.like(), U.like()
     start = [U.tensor(k).clone() for k in range(5)]
     results = []
-    for unit in (1, 2, 4):
+    shapes = [(1, 1, 1), (2, 1, 1), (4, 1, 1), (1, 2, 1), (1, 1, 2), (2, 2, 1), (2, 2, 2), (4, 4, 4)]
+    for shape in shapes:
         for order in range(3):
             for ctas in (0, 148 * 3):
                 for k in range(5):
                     U.tensor(k).copy_(start[k])
                 for g in (U, w1, w2):
-                    g.set_schedule(order, ctas, unit)
-                    assert g.schedule() == (order, ctas, unit)
+                    g.set_schedule(order, ctas, shape=shape)
+                    assert g.work_shape() == shape
+                    assert g.schedule() == (order, ctas, shape[0] * shape[1] * shape[2])
                 cn.amr.rk3_step(U, w1, w2, 1e-4, GAMMA)
                 torch.cuda.synchronize()
                 results.append(torch.cat([U.tensor(k).clone() for k in range(5)]))
     for g in (U, w1, w2):
+        g.set_schedule(1, 0, 2)  # the unit form: shape (2, 1, 1)
+        assert g.work_shape() == (2, 1, 1)
         g.set_schedule(1, 0, 1)
     for r in results[1:]:
         assert torch.equal(r, results[0])
