@@ -20,6 +20,10 @@ descriptions; FP64 unless stated):
          blocks of 32^3: one step = one multigrid solve from zero to relative
          residual 1e-8 (metric: cells solved per second); the learned
          smoother's solve is reported beside it.
+  lab    FieldLab::loadData of every block of the c2 state (cn_lab_fill, one
+         launch per component), stencil (-3,4): the explicit ghost fill.
+  io / io_read   the Field2AOS / AOS2Field gathers of CartesianWriteHDF /
+         CartesianReadHDF (512^3 cells, 3 components).
 
 A step is one pass of the path over the whole grid.  ``value`` is whole-job
 Gcell-updates/s with inputs resident in HBM (kernel time from CUDA events on
@@ -856,6 +860,121 @@ class C5:
         return self.cpu_sample_static(threads)
 
 
+class LAB:
+    """FieldLab::loadData of every block (Cartesian::loadLab over the grid,
+    Block/FieldLab.h:180-224; ``cn_lab_fill`` over a block range, one launch
+    per component): the C2 state (512^3 cells as 16^3 blocks of 32^3, FP64,
+    5 components, x periodic, y absorbing, z Dirichlet), stencil (-3, 4)
+    non-tensorial: 38^3 labs whose 6 x 3 x 32^2 face ghosts are written and
+    whose edges and corners stay undefined, as in the reference."""
+    name = "lab"
+    desc = ("FieldLab::loadData of all 4096 blocks (cn_lab_fill, one launch per component): C2 state, 512^3 "
+            "cells as 16^3 blocks of 32^3, 5 FP64 components, stencil (-3,4) non-tensorial, BCs x periodic, "
+            "y absorbing, z Dirichlet; 38^3 labs")
+    nb, n = (16, 16, 16), (32, 32, 32)
+    dtype = "f64"
+    metric = unit = "Gcell/s"
+    launches_per_step = 5
+    # per block cell and component: the block's cell read (8 B) and its share
+    # of the written lab cells, (32^3 + 6 x 3 x 32^2) / 32^3 x 8 B = 12.5 B;
+    # ghost cells read from neighbours are re-reads and not counted
+    bytes_per_cell_step = 5 * (8 + 8 * (32 ** 3 + 6 * 3 * 32 ** 2) / 32 ** 3)
+    cpu_nb = (8, 8, 4)
+
+    def __init__(self):
+        import torch
+
+        import cubismnova_b200 as cn
+        self.cn, self.torch = cn, torch
+        self.U = cn.Grid.Cartesian(self.nb, self.n, ncomp=5)
+        cn.workloads.euler_pulse(self.U)
+        cn.workloads.euler_bcs(self.U)
+        self.U.sync_bcs()
+        self.stencil = cn.Core.Stencil(-3, 4, False)
+        self.labs = cn.ops.load_labs(self.U, self.stencil, comp=0)
+        self.cells = int(np.prod(self.nb)) * int(np.prod(self.n))
+        self.updates_per_step = 5 * self.cells
+        self.h_state = None
+        self.h_labs = None
+
+    def needs_flush(self):
+        return False  # 1.07 GB read and 1.8 GB written per launch
+
+    def step(self, stream, events=None):
+        for c in range(5):
+            if events is not None:
+                events[c].record(stream)
+            self.cn.ops.load_labs(self.U, self.stencil, out=self.labs, comp=c, stream=stream)
+        if events is not None:
+            events[5].record(stream)
+
+    def e2e_step(self, stream):
+        """Each component uploaded from pinned host memory, its labs filled
+        and downloaded to pinned host memory."""
+        import ctypes as C
+        torch = self.torch
+        lib = self.cn._lib.lib()
+        nbytes = self.U.comp_stride * 8
+        if self.h_state is None:
+            self.h_state = torch.empty((5, self.U.comp_stride), dtype=torch.float64).pin_memory()
+            for c in range(5):
+                self.h_state[c].copy_(self.U.tensor(c).reshape(-1))
+            self.h_labs = torch.empty(self.labs.shape, dtype=self.labs.dtype).pin_memory()
+        sh = C.c_void_p(stream.cuda_stream)
+        for c in range(5):
+            self.cn._lib.check(lib.cn_grid_upload(self.U.handle, c, C.c_void_p(self.h_state[c].data_ptr()),
+                                                  nbytes, sh))
+            self.cn.ops.load_labs(self.U, self.stencil, out=self.labs, comp=c, stream=stream)
+            with torch.cuda.stream(stream):
+                self.h_labs.copy_(self.labs, non_blocking=True)
+        return 5 * nbytes, 5 * self.labs.numel() * 8
+
+    @classmethod
+    def cpu_sample_static(cls, threads, reps=1, nb=None):
+        """The reference's FieldLab::loadData (oracle/_ref) of every block of a
+        8x8x4-block grid of 32^3 with the C2 BCs, all 5 components, on
+        `threads` host threads with one lab each (the loadLab pattern of the
+        reference's own threaded tests); the C oracle, one lab at a time,
+        without the reference build."""
+        import ctypes as C
+
+        import oracle as O
+        nb = tuple(nb or cls.cpu_nb)
+        n = cls.n
+        stride = O.block_stride(n, np.float64)
+        U = euler_host_state(nb, n, stride)
+        bcl = euler_bclists_host(nb)
+        nblocks = int(np.prod(nb))
+        kind = "reference" if O.ref_available() else "port"
+        if kind == "reference":
+            best = O.ref_lab_sweep(U, nb, n, bcl, 3, 3, threads=threads, reps=max(1, reps))
+        else:
+            threads = 1
+            g = O.make_geom(nb, n, (3, 3, 3), (3, 3, 3), False, stride)
+            E = [n[d] + 6 for d in range(3)]
+            lab = np.zeros((E[2], E[1], E[0]))
+            w = np.zeros((E[2], E[1], E[0]), dtype=np.uint8)
+            best = 1e300
+            for _ in range(max(1, reps)):
+                t0 = time.perf_counter()
+                for c in range(5):
+                    off, ents = O.bc_arrays(nblocks, bcl[c])
+                    for b in range(nblocks):
+                        O.lib().or_lab_fill_f64(C.byref(g), O._ptr(np.ascontiguousarray(U[c])), O._ptr(off), ents,
+                                                C.c_int(b), O._ptr(lab), O._ptr(w))
+                best = min(best, time.perf_counter() - t0)
+        cells = nblocks * int(np.prod(n)) * 5
+        return dict(value=cells / best / 1e9, unit="Gcell/s", cores=threads, kind=kind,
+                    sample=f"labs of all {nblocks} blocks of 32^3 ({nb[0]}x{nb[1]}x{nb[2]}) x 5 components, "
+                           f"stencil (-3,4), C2 BCs, {threads} threads, best of {max(1, reps)}",
+                    seconds_per_sweep=best)
+
+    def cpu_sample(self, threads):
+        """About 10 s of host work: the sample repeated."""
+        t1 = self.cpu_sample_static(threads, reps=1)["seconds_per_sweep"]
+        return self.cpu_sample_static(threads, reps=int(min(500, max(1, 10.0 / t1))))
+
+
 class IOW:
     """Grid -> file buffer of IO::CartesianWriteHDF<float> (IO/CartesianHDF.h:76-80,
     Field2AOS of IO/FieldAOS.h:79-101): a rank-1 FP64 cell grid gathered into
@@ -1120,7 +1239,7 @@ class IOR(IOW):
                     seconds_per_sweep=t)
 
 
-WORKLOADS = {"c1": C1, "c2": C2, "c3": C3, "c4": C4, "c5": C5, "io": IOW, "io_read": IOR}
+WORKLOADS = {"c1": C1, "c2": C2, "c3": C3, "c4": C4, "c5": C5, "io": IOW, "io_read": IOR, "lab": LAB}
 DEFAULT_WORKLOAD = "c2"
 
 
@@ -1263,7 +1382,7 @@ def run_ours(args, world, rank, local, pg):
 
 # The other workloads, timed briefly on the same GPU after the main one so
 # that one default run measures them all (rank 0 at N = 1 only).
-COMPANIONS = ("c1", "c4", "c5", "c3")
+COMPANIONS = ("c1", "c4", "c5", "c3", "lab")
 
 
 def run_companions(args, local):

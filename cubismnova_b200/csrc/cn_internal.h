@@ -195,11 +195,14 @@ inline LabGeom make_geom(const cn_grid *g, const cn_stencil *s)
 __device__ __forceinline__ int pick3(int d, int a, int b, int c) { return d == 0 ? a : (d == 1 ? b : c); }
 
 // GROW: the grid may hold node / face fields (per-block extents); cell grids
-// (every fused stencil kernel) compile without that logic.
-template <typename T, bool GROW = false>
-__device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabGeom &L,
-                                          const BcView &bc, int block, int bx, int by, int bz,
-                                          int q0, int q1, int q2, bool apply_bc, T &out)
+// (every fused stencil kernel) compile without that logic.  The resolution
+// ends in the sink: sink.value(v) for a Dirichlet value (the chain's signs
+// applied), sink.load(idx, nsign, s0, s1, s2) for comp[idx] times the chain's
+// signs, innermost first.  lab_value's sink loads at once; a kernel can
+// instead collect several cells' sources and issue their loads together.
+template <typename T, bool GROW, typename Sink>
+__device__ __forceinline__ bool lab_resolve(const LabGeom &L, const BcView &bc, uint8_t mode, int block, int bx,
+                                            int by, int bz, int q0, int q1, int q2, bool apply_bc, Sink &sink)
 {
     // this block's extents (node / face fields: the last block along a grown
     // dimension holds one more entity); cells past its lab range are not part
@@ -210,7 +213,6 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
     if (GROW && (q0 >= e0 + L.hi[0] || q1 >= e1 + L.hi[1] || q2 >= e2 + L.hi[2]))
         return false;
     // skip flags hold even when the BCs themselves are not applied
-    const uint8_t mode = bc.mode[block];
     T s0 = T(1), s1 = T(1), s2 = T(1); // symmetry signs of the chain, outermost first
     int nsign = 0;
     if (apply_bc && (mode & kHasBc)) {
@@ -253,7 +255,7 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
                 if (nsign > 2) v = s2 * v;
                 if (nsign > 1) v = s1 * v;
                 if (nsign > 0) v = s0 * v;
-                out = v;
+                sink.value(v);
                 return true;
             }
             int qd = pick3(d, q0, q1, q2);
@@ -303,12 +305,32 @@ __device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabG
         s0e = ne0;
         s1e = ne1;
     }
-    T v = comp[(int64_t)src_block * L.bstride + q0 + (int64_t)s0e * (q1 + (int64_t)s1e * q2)];
-    if (nsign > 2) v = s2 * v;
-    if (nsign > 1) v = s1 * v;
-    if (nsign > 0) v = s0 * v;
-    out = v;
+    sink.load((int64_t)src_block * L.bstride + q0 + (int64_t)s0e * (q1 + (int64_t)s1e * q2), nsign, s0, s1, s2);
     return true;
+}
+
+// the sink of lab_value: the value at once
+template <typename T> struct LabLoad {
+    const T *__restrict__ comp;
+    T &out;
+    __device__ __forceinline__ void value(T v) { out = v; }
+    __device__ __forceinline__ void load(int64_t idx, int nsign, T s0, T s1, T s2)
+    {
+        T v = comp[idx];
+        if (nsign > 2) v = s2 * v;
+        if (nsign > 1) v = s1 * v;
+        if (nsign > 0) v = s0 * v;
+        out = v;
+    }
+};
+
+template <typename T, bool GROW = false>
+__device__ __forceinline__ bool lab_value(const T *__restrict__ comp, const LabGeom &L,
+                                          const BcView &bc, int block, int bx, int by, int bz,
+                                          int q0, int q1, int q2, bool apply_bc, T &out)
+{
+    LabLoad<T> sink{comp, out};
+    return lab_resolve<T, GROW>(L, bc, bc.mode[block], block, bx, by, bz, q0, q1, q2, apply_bc, sink);
 }
 
 // Lab value through the full BC chain (out of line: only blocks with BCs or

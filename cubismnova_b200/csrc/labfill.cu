@@ -1,40 +1,342 @@
 // labfill.cu -- K0: explicit lab fill (Cartesian::loadLab into lab buffers).
 //
-// One thread per lab cell; each cell is resolved independently by
-// cn::lab_value (inner copy, periodic neighbour gather, BC chain).  Writes are
-// coalesced along x of the lab; reads of inner and face cells are coalesced
-// along x of the source block.  This kernel exists so the device ghost fill
-// can be compared with the reference FieldLab bit for bit; the stencil
-// kernels fuse the same resolution into their shared-memory staging.
+// One CTA per (block, slab of lab planes along z): the slab's cells are
+// written in order by consecutive threads (coalesced stores; inner and face
+// cells read along x of the source block).  Each cell is resolved on its own
+// by the FieldLab resolution (cn::lab_resolve: inner copy, periodic
+// neighbour gather, BC chain); a thread resolves KL cells first and then
+// issues their loads together, so that KL loads per thread are in flight
+// (the kernel is a stream of loads and stores, bound by HBM).  The block's
+// coordinates and BC summary are read once per CTA and a cell's (x, y, z)
+// come from multiply-high divisions.  The stencil kernels fuse the same
+// resolution into their shared-memory staging; this kernel gives the
+// reference's FieldLab contents for user stencils and the bit-exact
+// comparison with it.
+#include "cn_fastdiv.h"
 #include "cn_internal.h"
+
+#include <algorithm>
 
 namespace cn {
 
-template <typename T, bool GROW>
+constexpr int KL = 4;              // cells per thread resolved before their loads
+constexpr int KL0 = 8;             // pairs of the block's own cells per thread in flight
+constexpr int kCellsPerCta = 8192; // target cells of a CTA's slab
+
+// a cell's source, collected from lab_resolve
+template <typename T> struct LabSource {
+    int kind = 0; // 0 undefined, 1 the value v, 2 comp[idx] times the signs
+    int nsign = 0;
+    int64_t idx = 0;
+    T v = T(0), s0 = T(1), s1 = T(1), s2 = T(1);
+    __device__ __forceinline__ void value(T x)
+    {
+        kind = 1;
+        v = x;
+    }
+    __device__ __forceinline__ void load(int64_t i, int n, T a, T b, T c)
+    {
+        kind = 2;
+        idx = i;
+        nsign = n;
+        s0 = a;
+        s1 = b;
+        s2 = c;
+    }
+};
+
+// Loads the sources of up to KL cells, then stores them: src[k] for cell
+// dst[k] (offsets in the CTA's output, -1: no cell).
+template <typename T>
+__device__ __forceinline__ void lab_store(const T *__restrict__ comp, const LabSource<T> (&src)[KL],
+                                          const int (&dst)[KL], T *__restrict__ o)
+{
+    T v[KL];
+#pragma unroll
+    for (int k = 0; k < KL; ++k)
+        v[k] = src[k].kind == 2 ? comp[src[k].idx] : src[k].v;
+#pragma unroll
+    for (int k = 0; k < KL; ++k) {
+        if (dst[k] < 0 || src[k].kind == 0) continue;
+        T x = v[k];
+        if (src[k].kind == 2) {
+            if (src[k].nsign > 2) x = src[k].s2 * x;
+            if (src[k].nsign > 1) x = src[k].s1 * x;
+            if (src[k].nsign > 0) x = src[k].s0 * x;
+        }
+        o[dst[k]] = x;
+    }
+}
+
+// Node and face grids (per-block extents): every cell of the CTA's slab
+// resolved on its own.
+template <typename T>
 __global__ void __launch_bounds__(256)
-    lab_fill_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin,
-                    int block_count, int apply_bc, T *__restrict__ out)
+    lab_fill_grow_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin, int pz, FastDiv dE0,
+                         FastDiv dPlane, int apply_bc, T *__restrict__ out)
 {
     const int E0 = L.n[0] + L.lo[0] + L.hi[0];
     const int E1 = L.n[1] + L.lo[1] + L.hi[1];
     const int E2 = L.n[2] + L.lo[2] + L.hi[2];
-    const int64_t lab_cells = (int64_t)E0 * E1 * E2;
-    const int64_t total = lab_cells * block_count;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int bl = (int)(t / lab_cells);
-        const int64_t c = t - (int64_t)bl * lab_cells;
-        const int x = (int)(c % E0);
-        const int y = (int)((c / E0) % E1);
-        const int z = (int)(c / ((int64_t)E0 * E1));
-        const int block = block_begin + bl;
-        const int bx = block % L.nb[0];
-        const int by = (block / L.nb[0]) % L.nb[1];
-        const int bz = block / (L.nb[0] * L.nb[1]);
-        T v;
-        if (lab_value<T, GROW>(comp, L, bc, block, bx, by, bz, x - L.lo[0], y - L.lo[1],
-                               z - L.lo[2], apply_bc != 0, v)) {
-            out[t] = v;
+    const int plane = E0 * E1;
+    const int bl = blockIdx.x, z0 = blockIdx.y * pz;
+    const int nz = min(pz, E2 - z0);
+    const int block = block_begin + bl;
+    const int bx = block % L.nb[0];
+    const int by = (block / L.nb[0]) % L.nb[1];
+    const int bz = block / (L.nb[0] * L.nb[1]);
+    const uint8_t mode = bc.mode[block];
+    const int cells = nz * plane;
+    T *o = out + ((int64_t)bl * E2 + z0) * plane;
+    for (int t0 = threadIdx.x; t0 < cells; t0 += KL * blockDim.x) {
+        LabSource<T> src[KL];
+        int dst[KL];
+#pragma unroll
+        for (int k = 0; k < KL; ++k) {
+            const int t = t0 + k * blockDim.x;
+            dst[k] = -1;
+            if (t < cells) {
+                const int zz = dPlane.div(t), r = t - zz * plane;
+                const int y = dE0.div(r), x = r - y * E0;
+                dst[k] = t;
+                lab_resolve<T, true>(L, bc, mode, block, bx, by, bz, x - L.lo[0], y - L.lo[1], z0 + zz - L.lo[2],
+                                     apply_bc != 0, src[k]);
+            }
+        }
+        lab_store<T>(comp, src, dst, o);
+    }
+}
+
+// a row of class 2 or 3: the source of its first cell and its first cell's
+// offset in the lab
+template <typename T> struct RowSrc {
+    LabSource<T> s;
+    int dst;
+};
+constexpr int kRows = 256; // rows resolved per round
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double> {
+    using type = double2;
+};
+template <> struct Vec2<float> {
+    using type = float2;
+};
+template <> struct Vec2<int32_t> {
+    using type = int2;
+};
+
+// Divisors of the cell-grid kernel's four cell classes (fixed per launch).
+struct LabDivs {
+    FastDiv n0, n1;   // block extents along x, y
+    FastDiv gx;       // x ghosts per row: lo0 + hi0
+    FastDiv wrow, gy; // cells per ghost row (n0, or E0 if tensorial); y ghost rows: lo1 + hi1
+    FastDiv wpl;      // rows per z-ghost plane (n1, or E1 if tensorial)
+};
+
+// Cell grids: the CTA's slab of lab planes as four classes of cells, each
+// walked by all threads so that a warp's cells take the same path:
+//   0  the block's own cells (planes and rows inside): plain copies;
+//   1  the x ghosts of those rows;
+//   2  the y-ghost rows of inside planes (x inside, or the whole row when
+//      tensorial);
+//   3  the z-ghost planes (x, y inside, or the whole plane when tensorial).
+// Class 1-3 cells beyond faces that carry no BC and no skipped neighbour are
+// the periodic neighbour's cells (closed form); the others take lab_resolve
+// (skips, BC chains).  Without tensorial ghosts, classes 2 and 3 are walked
+// as rows resolved once each.  Cells no class lists are the edges and corners of a
+// non-tensorial lab, which the reference leaves undefined.
+template <typename T>
+__global__ void __launch_bounds__(256, 4)
+    lab_fill_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin, int pz, LabDivs dv,
+                    int apply_bc, T *__restrict__ out)
+{
+    const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    const int E0 = n0 + L.lo[0] + L.hi[0];
+    const int E1 = n1 + L.lo[1] + L.hi[1];
+    const int E2 = n2 + L.lo[2] + L.hi[2];
+    const int bl = blockIdx.x, z0 = blockIdx.y * pz;
+    const int z1 = min(z0 + pz, E2);
+    const int block = block_begin + bl;
+    const int bx = block % L.nb[0];
+    const int by = (block / L.nb[0]) % L.nb[1];
+    const int bz = block / (L.nb[0] * L.nb[1]);
+    const uint8_t mode = bc.mode[block];
+    // faces of the block that carry a BC (other than Base) or a skipped
+    // neighbour: cells beyond them take the full resolution
+    const uint8_t faces = bc.faces[block];
+    const bool abc = apply_bc != 0, tens = L.tensorial != 0;
+    // planes of the slab inside the block, and its z-ghost planes below / above
+    const int zi0 = max(z0, L.lo[2]), zi1 = min(z1, L.lo[2] + n2);
+    const int nin = max(0, zi1 - zi0);
+    const int nlo = max(0, min(z1, L.lo[2]) - z0);
+    const int zhi = max(z0, L.lo[2] + n2);
+    const int nghost = nlo + max(0, z1 - zhi);
+    const int wrow = tens ? E0 : n0, wpl = tens ? E1 : n1;
+    const int gx = L.lo[0] + L.hi[0], gy = L.lo[1] + L.hi[1];
+    T *o = out + (int64_t)bl * E0 * E1 * E2;
+    // class 0: rows of the block's own cells, plain copies (KL loads in flight)
+    {
+        const T *blk = comp + (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
+        T *ob = o + L.lo[0] + E0 * (L.lo[1] + E1 * zi0);
+        const int cnt = nin * n1 * n0;
+        if ((n0 & 1) == 0) {
+            // pairs of cells along x: one 2-element load (the block's rows
+            // start on 2-element boundaries), two stores (lab rows need not)
+            using V = typename Vec2<T>::type;
+            const V *blk2 = reinterpret_cast<const V *>(blk);
+            const int cnt2 = cnt >> 1;
+            for (int p0 = threadIdx.x; p0 < cnt2; p0 += KL0 * blockDim.x) {
+                V v[KL0];
+                int d[KL0];
+#pragma unroll
+                for (int k = 0; k < KL0; ++k) {
+                    const int p = p0 + k * blockDim.x, t = 2 * p;
+                    const int r = dv.n0.div(t), zp = dv.n1.div(r);
+                    d[k] = p < cnt2 ? (t - r * n0) + E0 * ((r - zp * n1) + E1 * zp) : -1;
+                    if (p < cnt2) v[k] = blk2[p];
+                }
+#pragma unroll
+                for (int k = 0; k < KL0; ++k)
+                    if (d[k] >= 0) {
+                        ob[d[k]] = v[k].x;
+                        ob[d[k] + 1] = v[k].y;
+                    }
+            }
+        } else {
+            for (int t0 = threadIdx.x; t0 < cnt; t0 += KL * blockDim.x) {
+                T v[KL];
+                int d[KL];
+#pragma unroll
+                for (int k = 0; k < KL; ++k) {
+                    const int t = t0 + k * blockDim.x;
+                    const int r = dv.n0.div(t), zp = dv.n1.div(r);
+                    d[k] = t < cnt ? (t - r * n0) + E0 * ((r - zp * n1) + E1 * zp) : -1;
+                    v[k] = t < cnt ? blk[t] : T(0);
+                }
+#pragma unroll
+                for (int k = 0; k < KL; ++k)
+                    if (d[k] >= 0) ob[d[k]] = v[k];
+            }
+        }
+    }
+    // classes 1-3 cell by cell; without tensorial ghosts, classes 2 and 3 go
+    // by rows below
+#pragma unroll 1
+    for (int cls = 1; cls < (tens ? 4 : 2); ++cls) {
+        const int cnt = cls == 1 ? nin * n1 * gx : (cls == 2 ? nin * gy * wrow : nghost * wpl * wrow);
+        for (int t0 = threadIdx.x; t0 < cnt; t0 += KL * blockDim.x) {
+            LabSource<T> src[KL];
+            int dst[KL];
+#pragma unroll
+            for (int k = 0; k < KL; ++k) {
+                const int t = t0 + k * blockDim.x;
+                dst[k] = -1;
+                if (t >= cnt) continue;
+                int x, y, z; // lab coordinates
+                if (cls == 1) {
+                    const int r = dv.gx.div(t), zp = dv.n1.div(r);
+                    const int g = t - r * gx;
+                    x = g < L.lo[0] ? g : g + n0;
+                    y = r - zp * n1 + L.lo[1];
+                    z = zi0 + zp;
+                } else if (cls == 2) {
+                    const int r = dv.wrow.div(t), zp = dv.gy.div(r);
+                    const int g = r - zp * gy;
+                    x = t - r * wrow + (tens ? 0 : L.lo[0]);
+                    y = g < L.lo[1] ? g : g + n1;
+                    z = zi0 + zp;
+                } else {
+                    const int r = dv.wrow.div(t), zp = dv.wpl.div(r);
+                    x = t - r * wrow + (tens ? 0 : L.lo[0]);
+                    y = r - zp * wpl + (tens ? 0 : L.lo[1]);
+                    z = zp < nlo ? z0 + zp : zhi + (zp - nlo);
+                }
+                dst[k] = x + E0 * (y + E1 * z);
+                {
+                    const int q0 = x - L.lo[0], q1 = y - L.lo[1], q2 = z - L.lo[2];
+                    const int r0 = q0 < 0 ? -1 : (q0 >= n0 ? 1 : 0), r1 = q1 < 0 ? -1 : (q1 >= n1 ? 1 : 0),
+                              r2 = q2 < 0 ? -1 : (q2 >= n2 ? 1 : 0);
+                    const int crossed = (r0 ? (r0 < 0 ? 1 : 2) : 0) | (r1 ? (r1 < 0 ? 4 : 8) : 0) |
+                                        (r2 ? (r2 < 0 ? 16 : 32) : 0);
+                    if (faces & crossed) {
+                        lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, q0, q1, q2, abc, src[k]);
+                    } else {
+                        // beyond clear faces only: no BC covers the cell, and it is the
+                        // periodic neighbour's cell (as lab_resolve gives it)
+                        int nbx = bx + r0, nby = by + r1, nbz = bz + r2;
+                        nbx = nbx < 0 ? nbx + L.nb[0] : (nbx >= L.nb[0] ? nbx - L.nb[0] : nbx);
+                        nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
+                        nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
+                        src[k].kind = 2;
+                        src[k].idx = (int64_t)(nbx + L.nb[0] * (nby + L.nb[1] * nbz)) * L.bstride + (q0 - r0 * n0) +
+                                     n0 * ((q1 - r1 * n1) + n1 * (q2 - r2 * n2));
+                    }
+                }
+            }
+            lab_store<T>(comp, src, dst, o);
+        }
+    }
+    if (tens) return;
+    // Classes 2 and 3 of a non-tensorial lab by rows: a y-ghost row of an
+    // inside plane, or a row of a z-ghost plane, holds the n0 cells with x
+    // inside the block, and x passes through every step of the resolution
+    // unchanged (no x BC covers them, the neighbour is the same), so the
+    // cells of a row are the row's first cell's source shifted by x (or its
+    // one value).  One thread resolves a row's first cell into shared
+    // memory; all threads then copy the rows' cells.
+    __shared__ __align__(16) unsigned char rows_raw[kRows * sizeof(RowSrc<T>)];
+    RowSrc<T> *rows = reinterpret_cast<RowSrc<T> *>(rows_raw);
+    const int ny = nin * gy, nrows = ny + nghost * n1;
+#pragma unroll 1
+    for (int rb = 0; rb < nrows; rb += kRows) {
+        const int nr = min(kRows, nrows - rb);
+        __syncthreads(); // the previous rows are copied
+        for (int j = threadIdx.x; j < nr; j += blockDim.x) {
+            const int row = rb + j;
+            int y, z; // lab coordinates of the row
+            if (row < ny) {
+                const int zp = dv.gy.div(row), g = row - zp * gy;
+                y = g < L.lo[1] ? g : g + n1;
+                z = zi0 + zp;
+            } else {
+                const int rr = row - ny, zp = dv.n1.div(rr);
+                y = rr - zp * n1 + L.lo[1];
+                z = zp < nlo ? z0 + zp : zhi + (zp - nlo);
+            }
+            const int q1 = y - L.lo[1], q2 = z - L.lo[2];
+            const int r1 = q1 < 0 ? -1 : (q1 >= n1 ? 1 : 0), r2 = q2 < 0 ? -1 : (q2 >= n2 ? 1 : 0);
+            const int crossed = (r1 ? (r1 < 0 ? 4 : 8) : 0) | (r2 ? (r2 < 0 ? 16 : 32) : 0);
+            LabSource<T> sr;
+            if (faces & crossed) {
+                lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, 0, q1, q2, abc, sr);
+            } else {
+                int nby = by + r1, nbz = bz + r2;
+                nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
+                nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
+                sr.kind = 2;
+                sr.idx = (int64_t)(bx + L.nb[0] * (nby + L.nb[1] * nbz)) * L.bstride +
+                         n0 * ((q1 - r1 * n1) + n1 * (q2 - r2 * n2));
+            }
+            rows[j].s = sr;
+            rows[j].dst = L.lo[0] + E0 * (y + E1 * z);
+        }
+        __syncthreads();
+        const int cells = nr * n0;
+        for (int t0 = threadIdx.x; t0 < cells; t0 += KL * blockDim.x) {
+            LabSource<T> src[KL];
+            int dst[KL];
+#pragma unroll
+            for (int k = 0; k < KL; ++k) {
+                const int t = t0 + k * blockDim.x;
+                dst[k] = -1;
+                if (t >= cells) continue;
+                const int j = dv.n0.div(t), x = t - j * n0;
+                src[k] = rows[j].s;
+                src[k].idx += x;
+                dst[k] = rows[j].dst + x;
+            }
+            lab_store<T>(comp, src, dst, o);
         }
     }
 }
@@ -45,21 +347,30 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
 {
     const LabGeom L = make_geom(g, s);
     const T *src = reinterpret_cast<const T *>(g->d_data) + (size_t)comp * g->comp_stride;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
-    const int64_t E = (int64_t)(L.n[0] + L.lo[0] + L.hi[0]) * (L.n[1] + L.lo[1] + L.hi[1]) *
-                      (L.n[2] + L.lo[2] + L.hi[2]);
-    const int64_t total = E * cnt;
-    int64_t blocks = (total + 255) / 256;
-    const int64_t cap = (int64_t)sms * 8;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
-    if (L.grow[0] || L.grow[1] || L.grow[2])
-        lab_fill_kernel<T, true><<<(unsigned)blocks, 256, 0, st>>>(src, L, bc_view(g, comp), b0, cnt, apply_bc,
-                                                                   reinterpret_cast<T *>(d_labs));
-    else
-        lab_fill_kernel<T, false><<<(unsigned)blocks, 256, 0, st>>>(src, L, bc_view(g, comp), b0, cnt, apply_bc,
-                                                                    reinterpret_cast<T *>(d_labs));
+    const int64_t E0 = L.n[0] + L.lo[0] + L.hi[0], E1 = L.n[1] + L.lo[1] + L.hi[1], E2 = L.n[2] + L.lo[2] + L.hi[2];
+    const int64_t plane = E0 * E1;
+    if (plane * E2 >= (int64_t(1) << 31))
+        return fail(CN_ERR_UNSUPPORTED, "cn_lab_fill: labs of 2^31 cells or more");
+    // planes per CTA: about kCellsPerCta cells
+    const int pz = (int)std::max<int64_t>(1, std::min<int64_t>(E2, kCellsPerCta / plane));
+    const int64_t slabs = (E2 + pz - 1) / pz;
+    if (slabs > 65535) return fail(CN_ERR_UNSUPPORTED, "cn_lab_fill: more than 65535 lab slabs per block");
+    const dim3 grid((unsigned)cnt, (unsigned)slabs);
+    const int threads = plane * pz >= 1024 ? 256 : 128;
+    T *out = reinterpret_cast<T *>(d_labs);
+    if (L.grow[0] || L.grow[1] || L.grow[2]) {
+        lab_fill_grow_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, FastDiv((uint32_t)E0),
+                                                          FastDiv((uint32_t)plane), apply_bc, out);
+    } else {
+        LabDivs dv;
+        dv.n0 = FastDiv((uint32_t)L.n[0]);
+        dv.n1 = FastDiv((uint32_t)L.n[1]);
+        dv.gx = FastDiv((uint32_t)(L.lo[0] + L.hi[0]));
+        dv.wrow = FastDiv((uint32_t)(L.tensorial ? E0 : L.n[0]));
+        dv.gy = FastDiv((uint32_t)(L.lo[1] + L.hi[1]));
+        dv.wpl = FastDiv((uint32_t)(L.tensorial ? E1 : L.n[1]));
+        lab_fill_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, out);
+    }
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
 }

@@ -34,6 +34,31 @@ def divergence(v: Cartesian, out: Cartesian, comp: int = 0, out_comp: int = 0, s
     _lib.check(_lib.lib().cn_divergence(v.handle, comp, out.handle, out_comp, _stream_handle(stream)))
 
 
+def load_labs(u: Cartesian, stencil, out=None, comp: int = 0, block_begin: int = 0, count: int = None,
+              apply_bc: bool = True, stream=None):
+    """Cartesian::loadLab for a range of blocks in one launch (the block loop
+    of Grid/Cartesian.h:412-427 over FieldLab::loadData, Block/FieldLab.h:180-224):
+    the labs of blocks [block_begin, block_begin + count) of component
+    ``comp`` for ``stencil`` (a Core.Stencil) into ``out``, a CUDA tensor of
+    count x (E2, E1, E0) values (x fastest; cells the reference leaves
+    undefined keep out's values).  Returns out."""
+    import torch
+    st = stencil.as_struct()
+    ext = (C.c_int * 3)()
+    _lib.check(_lib.lib().cn_lab_extent(u.handle, C.byref(st), ext))
+    n = u.getSize()[0] * u.getSize()[1] * u.getSize()[2]
+    count = n - block_begin if count is None else count
+    shape = (count, ext[2], ext[1], ext[0])
+    tdt = {4: torch.float32, 8: torch.float64}[u.dtype.itemsize] if u.dtype.kind == "f" else torch.int32
+    if out is None:
+        out = torch.zeros(shape, dtype=tdt, device="cuda")
+    elif tuple(out.shape) != shape or out.dtype != tdt or not out.is_contiguous() or not out.is_cuda:
+        raise ValueError(f"load_labs: out must be a contiguous CUDA {tdt} tensor of shape {shape}")
+    _lib.check(_lib.lib().cn_lab_fill(u.handle, comp, C.byref(st), int(block_begin), int(count),
+                                      1 if apply_bc else 0, C.c_void_p(out.data_ptr()), _stream_handle(stream)))
+    return out
+
+
 def ddx(src_ptr: int, dst_ptr: int, extent, src_pitch, dst_pitch, factor: float, dtype="f64",
         stream=None):
     """The ISPC benchmark kernel ABI (BaseBenchmark.h:27-37) on device pointers.

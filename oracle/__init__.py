@@ -237,6 +237,28 @@ def euler_rk3_step(U, nb, n, bclists, dt, gamma, h, threads=0):
     return euler_stage(U2, U, nb, n, bclists, 3, dt, gamma, h, threads)
 
 
+def ref_lab_sweep(comps, nb, n, bclists, lo, hi, threads=0, reps=1):
+    """The labs of every block of each component of ``comps`` (rows in the
+    grid layout) loaded by the reference FieldLab (oracle/_ref), stencil
+    (-lo, hi+1) non-tensorial; returns the best seconds per sweep."""
+    comps = np.ascontiguousarray(comps, dtype=np.float64)
+    ncomp = comps.shape[0]
+    stride = block_stride(n, np.float64)
+    nblocks = int(np.prod(nb))
+    offs, ents = [], []
+    for c in range(ncomp):
+        o, e = bc_arrays(nblocks, (bclists[c] if bclists else {}))
+        offs.append(o)
+        ents.append(e)
+    off_ptrs = (C.c_void_p * ncomp)(*[o.ctypes.data for o in offs])
+    ent_ptrs = (C.c_void_p * ncomp)(*[C.addressof(e) for e in ents])
+    f = ref().ref_lab_sweep_f64
+    f.restype = C.c_double
+    return f((C.c_int * 3)(*nb), (C.c_int * 3)(*n), _ptr(comps), C.c_int64(stride), C.c_int64(comps.shape[-1]),
+             off_ptrs, ent_ptrs, C.c_int(ncomp), C.c_int(lo), C.c_int(hi),
+             C.c_int(threads if threads > 0 else (os.cpu_count() or 1)), C.c_int(reps))
+
+
 def ref_euler_stage(Us, Un, nb, n, bclists, stage, dt, gamma, h, threads=0, blocks=None, reps=1):
     """The Euler stage with labs loaded by the reference FieldLab (oracle/_ref).
     Returns (seconds for the sampled blocks, out)."""

@@ -489,6 +489,40 @@ double ref_c1_sweep_f64(const int nb[3], const int n[3], const double *comp,
     return best;
 }
 
+// FieldLab::loadData of every block of ncomp components (stencil (-lo, hi+1)
+// in every direction, non-tensorial, per-component BC vectors): the
+// reference's grids built once, one lab per thread, blocks
+// schedule(dynamic, 1) as in test/UnitTests/Grid/CartesianTest.cpp:283-317.
+// Returns the best seconds per sweep over reps.
+double ref_lab_sweep_f64(const int nb[3], const int n[3], const double *comps, int64_t stride, int64_t cstride,
+                         const int32_t *const *bc_off, const or_bc *const *bcs, int ncomp, int lo, int hi,
+                         int nthreads, int reps)
+{
+    using R = RefGrid<double>;
+    std::vector<std::unique_ptr<R>> g;
+    for (int c = 0; c < ncomp; ++c) {
+        g.emplace_back(new R(nb, n, comps + c * cstride, stride));
+        g.back()->attach(bc_off ? bc_off[c] : nullptr, bcs ? bcs[c] : nullptr);
+    }
+    const int nbk = (int)g[0]->grid->size();
+    double best = 1e300;
+    for (int rep = 0; rep < (reps < 1 ? 1 : reps); ++rep) {
+        const auto t0 = std::chrono::steady_clock::now();
+#pragma omp parallel num_threads(nthreads)
+        {
+            typename R::Lab lab;
+            const typename R::S s(-lo, hi + 1, false);
+            lab.allocate(s, (*g[0]->grid)[0].getIndexRange());
+#pragma omp for schedule(dynamic, 1) collapse(2)
+            for (int c = 0; c < ncomp; ++c)
+                for (int b = 0; b < nbk; ++b) g[c]->grid->loadLab((*g[c]->grid)[(size_t)b], lab);
+        }
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        best = dt < best ? dt : best;
+    }
+    return best;
+}
+
 // Euler RHS (stage 0) / SSP-RK3 stage (1..3) of blocks [b0, b0+cnt) on the
 // reference FieldLab; returns the best seconds over reps.
 double ref_euler_stage_f64(const int nb[3], const int n[3], const double *Us, const double *Un,
