@@ -21,6 +21,7 @@ namespace cn {
 
 constexpr int KL = 4;              // cells per thread resolved before their loads
 constexpr int KL0 = 8;             // pairs of the block's own cells per thread in flight
+constexpr int KLM = 8;             // cells per thread in flight in the one-pass form
 constexpr int kCellsPerCta = 8192; // target cells of a CTA's slab
 
 // a cell's source, collected from lab_resolve
@@ -134,6 +135,70 @@ struct LabDivs {
     FastDiv wpl;      // rows per z-ghost plane (n1, or E1 if tensorial)
 };
 
+// lab coordinates of class-1 cell u (the x ghosts of the inside rows)
+__device__ __forceinline__ void class1_cell(const LabDivs &dv, int u, int gx, int n0, int n1, int lo0, int lo1, int zi0,
+                                            int &x, int &y, int &z)
+{
+    const int r = dv.gx.div(u), zp = dv.n1.div(r);
+    const int g = u - r * gx;
+    x = g < lo0 ? g : g + n0;
+    y = r - zp * n1 + lo1;
+    z = zi0 + zp;
+}
+
+// Row `row` of classes 2 and 3 of a non-tensorial lab (rows [0, ny): the
+// y-ghost rows of the slab's inside planes; then the rows of its z-ghost
+// planes): the source of its first cell (x = 0 of the block) and that
+// cell's offset in the lab.  x passes through every step of the resolution
+// unchanged, so cell x of the row is the source shifted by x (or the same
+// value).
+template <typename T>
+__device__ __forceinline__ RowSrc<T> lab_row(const LabGeom &L, const BcView &bc, uint8_t mode, uint8_t faces,
+                                             int block, int bx, int by, int bz, bool abc, const LabDivs &dv, int row,
+                                             int ny, int gy, int zi0, int nlo, int zhi, int z0, int E0, int E1)
+{
+    const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+    int y, z; // lab coordinates of the row
+    if (row < ny) {
+        const int zp = dv.gy.div(row), g = row - zp * gy;
+        y = g < L.lo[1] ? g : g + n1;
+        z = zi0 + zp;
+    } else {
+        const int rr = row - ny, zp = dv.n1.div(rr);
+        y = rr - zp * n1 + L.lo[1];
+        z = zp < nlo ? z0 + zp : zhi + (zp - nlo);
+    }
+    const int q1 = y - L.lo[1], q2 = z - L.lo[2];
+    const int r1 = q1 < 0 ? -1 : (q1 >= n1 ? 1 : 0), r2 = q2 < 0 ? -1 : (q2 >= n2 ? 1 : 0);
+    const int crossed = (r1 ? (r1 < 0 ? 4 : 8) : 0) | (r2 ? (r2 < 0 ? 16 : 32) : 0);
+    RowSrc<T> R;
+    if (faces & crossed) {
+        lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, 0, q1, q2, abc, R.s);
+    } else {
+        int nby = by + r1, nbz = bz + r2;
+        nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
+        nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
+        R.s.kind = 2;
+        R.s.idx = (int64_t)(bx + L.nb[0] * (nby + L.nb[1] * nbz)) * L.bstride + n0 * ((q1 - r1 * n1) + n1 * (q2 - r2 * n2));
+    }
+    R.dst = L.lo[0] + E0 * (y + E1 * z);
+    return R;
+}
+
+// one cell's source stored (kind 0: nothing)
+template <typename T>
+__device__ __forceinline__ void lab_store1(const T *__restrict__ comp, const LabSource<T> &s, int dst, T *__restrict__ o)
+{
+    if (dst < 0 || s.kind == 0) return;
+    T x = s.kind == 2 ? comp[s.idx] : s.v;
+    if (s.kind == 2) {
+        if (s.nsign > 2) x = s.s2 * x;
+        if (s.nsign > 1) x = s.s1 * x;
+        if (s.nsign > 0) x = s.s0 * x;
+    }
+    o[dst] = x;
+}
+
 // Cell grids: the CTA's slab of lab planes as four classes of cells, each
 // walked by all threads so that a warp's cells take the same path:
 //   0  the block's own cells (planes and rows inside): plain copies;
@@ -175,6 +240,90 @@ __global__ void __launch_bounds__(256, 4)
     const int wrow = tens ? E0 : n0, wpl = tens ? E1 : n1;
     const int gx = L.lo[0] + L.hi[0], gy = L.lo[1] + L.hi[1];
     T *o = out + (int64_t)bl * E0 * E1 * E2;
+    const int ny = nin * gy, nrows = ny + nghost * n1;
+    __shared__ __align__(16) unsigned char rows_raw[kRows * sizeof(RowSrc<T>)];
+    RowSrc<T> *rows = reinterpret_cast<RowSrc<T> *>(rows_raw);
+    if (!tens && nrows <= kRows) {
+        // One pass over all three kinds of plain copies, KLM loads in flight
+        // per thread: the block's own cells, the x ghosts behind clear faces
+        // and the rows (classes 2, 3) whose source is a plain cell run.  The
+        // rows are resolved first; cells that need BC chains or skips are
+        // left to a second pass.
+        for (int j = threadIdx.x; j < nrows; j += blockDim.x)
+            rows[j] = lab_row<T>(L, bc, mode, faces, block, bx, by, bz, abc, dv, j, ny, gy, zi0, nlo, zhi, z0, E0, E1);
+        __syncthreads();
+        const int A = nin * n1 * n0, B = nin * n1 * gx, tot = A + B + nrows * n0;
+        const int64_t bbase = (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
+        bool deferred = false;
+        for (int t0 = threadIdx.x; t0 < tot; t0 += KLM * blockDim.x) {
+            int64_t idx[KLM];
+            int dst[KLM];
+#pragma unroll
+            for (int k = 0; k < KLM; ++k) {
+                const int t = t0 + k * blockDim.x;
+                dst[k] = -1;
+                idx[k] = 0;
+                if (t < A) {
+                    const int r = dv.n0.div(t), zp = dv.n1.div(r);
+                    dst[k] = (t - r * n0 + L.lo[0]) + E0 * ((r - zp * n1 + L.lo[1]) + E1 * (zi0 + zp));
+                    idx[k] = bbase + t;
+                } else if (t < A + B) {
+                    int x, y, z;
+                    class1_cell(dv, t - A, gx, n0, n1, L.lo[0], L.lo[1], zi0, x, y, z);
+                    const int q0 = x - L.lo[0], r0 = q0 < 0 ? -1 : 1;
+                    if (faces & (r0 < 0 ? 1 : 2)) {
+                        deferred = true;
+                    } else {
+                        const int nbx = bx + r0 < 0 ? bx + r0 + L.nb[0] : (bx + r0 >= L.nb[0] ? bx + r0 - L.nb[0] : bx + r0);
+                        dst[k] = x + E0 * (y + E1 * z);
+                        idx[k] = (int64_t)(nbx + L.nb[0] * (by + L.nb[1] * bz)) * L.bstride + (q0 - r0 * n0) +
+                                 n0 * ((y - L.lo[1]) + n1 * (z - L.lo[2]));
+                    }
+                } else if (t < tot) {
+                    const int u = t - A - B, j = dv.n0.div(u), x = u - j * n0;
+                    const RowSrc<T> &R = rows[j];
+                    if (R.s.kind == 2 && R.s.nsign == 0) {
+                        dst[k] = R.dst + x;
+                        idx[k] = R.s.idx + x;
+                    } else {
+                        deferred = true;
+                    }
+                }
+            }
+            T v[KLM];
+#pragma unroll
+            for (int k = 0; k < KLM; ++k)
+                if (dst[k] >= 0) v[k] = comp[idx[k]];
+#pragma unroll
+            for (int k = 0; k < KLM; ++k)
+                if (dst[k] >= 0) o[dst[k]] = v[k];
+        }
+        if (deferred) {
+            // the second pass: the same items of this thread
+            const int nt = (int)blockDim.x;
+            for (int t = A + ((((int)threadIdx.x - A) % nt) + nt) % nt; t < tot; t += nt) {
+                LabSource<T> src[1];
+                int dst[1] = {-1};
+                if (t < A + B) {
+                    int x, y, z;
+                    class1_cell(dv, t - A, gx, n0, n1, L.lo[0], L.lo[1], zi0, x, y, z);
+                    if (!(faces & (x < L.lo[0] ? 1 : 2))) continue;
+                    lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, x - L.lo[0], y - L.lo[1], z - L.lo[2], abc,
+                                          src[0]);
+                    dst[0] = x + E0 * (y + E1 * z);
+                } else {
+                    const int u = t - A - B, j = dv.n0.div(u), x = u - j * n0;
+                    const RowSrc<T> &R = rows[j];
+                    if (R.s.kind == 2 && R.s.nsign == 0) continue;
+                    src[0] = R.s;
+                    src[0].idx += x;
+                    dst[0] = R.dst + x;
+                }
+                lab_store1<T>(comp, src[0], dst[0], o);
+            }
+        }
+        return;
+    }
     // class 0: rows of the block's own cells, plain copies (KL loads in flight)
     {
         const T *blk = comp + (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
@@ -285,42 +434,13 @@ __global__ void __launch_bounds__(256, 4)
     // cells of a row are the row's first cell's source shifted by x (or its
     // one value).  One thread resolves a row's first cell into shared
     // memory; all threads then copy the rows' cells.
-    __shared__ __align__(16) unsigned char rows_raw[kRows * sizeof(RowSrc<T>)];
-    RowSrc<T> *rows = reinterpret_cast<RowSrc<T> *>(rows_raw);
-    const int ny = nin * gy, nrows = ny + nghost * n1;
 #pragma unroll 1
     for (int rb = 0; rb < nrows; rb += kRows) {
         const int nr = min(kRows, nrows - rb);
         __syncthreads(); // the previous rows are copied
-        for (int j = threadIdx.x; j < nr; j += blockDim.x) {
-            const int row = rb + j;
-            int y, z; // lab coordinates of the row
-            if (row < ny) {
-                const int zp = dv.gy.div(row), g = row - zp * gy;
-                y = g < L.lo[1] ? g : g + n1;
-                z = zi0 + zp;
-            } else {
-                const int rr = row - ny, zp = dv.n1.div(rr);
-                y = rr - zp * n1 + L.lo[1];
-                z = zp < nlo ? z0 + zp : zhi + (zp - nlo);
-            }
-            const int q1 = y - L.lo[1], q2 = z - L.lo[2];
-            const int r1 = q1 < 0 ? -1 : (q1 >= n1 ? 1 : 0), r2 = q2 < 0 ? -1 : (q2 >= n2 ? 1 : 0);
-            const int crossed = (r1 ? (r1 < 0 ? 4 : 8) : 0) | (r2 ? (r2 < 0 ? 16 : 32) : 0);
-            LabSource<T> sr;
-            if (faces & crossed) {
-                lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, 0, q1, q2, abc, sr);
-            } else {
-                int nby = by + r1, nbz = bz + r2;
-                nby = nby < 0 ? nby + L.nb[1] : (nby >= L.nb[1] ? nby - L.nb[1] : nby);
-                nbz = nbz < 0 ? nbz + L.nb[2] : (nbz >= L.nb[2] ? nbz - L.nb[2] : nbz);
-                sr.kind = 2;
-                sr.idx = (int64_t)(bx + L.nb[0] * (nby + L.nb[1] * nbz)) * L.bstride +
-                         n0 * ((q1 - r1 * n1) + n1 * (q2 - r2 * n2));
-            }
-            rows[j].s = sr;
-            rows[j].dst = L.lo[0] + E0 * (y + E1 * z);
-        }
+        for (int j = threadIdx.x; j < nr; j += blockDim.x)
+            rows[j] = lab_row<T>(L, bc, mode, faces, block, bx, by, bz, abc, dv, rb + j, ny, gy, zi0, nlo, zhi, z0, E0,
+                                 E1);
         __syncthreads();
         const int cells = nr * n0;
         for (int t0 = threadIdx.x; t0 < cells; t0 += KL * blockDim.x) {
