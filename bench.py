@@ -879,6 +879,12 @@ class LAB:
     # of the written lab cells, (32^3 + 6 x 3 x 32^2) / 32^3 x 8 B = 12.5 B;
     # ghost cells read from neighbours are re-reads and not counted
     bytes_per_cell_step = 5 * (8 + 8 * (32 ** 3 + 6 * 3 * 32 ** 2) / 32 ** 3)
+    # DRAM bytes per cell of one ncu capture of a launch on 8x8x8 blocks of
+    # 32^3 (175.0 MB read + 174.4 MB written for 16.8 M cells), times the 5
+    # launches of a step; traffic grows with the blocks processed
+    traffic_per_cell_step = 104.1
+    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one lab_fill_kernel launch on 8x8x8 "
+                      "blocks of 32^3, per cell, times the 5 launches of a step")
     cpu_nb = (8, 8, 4)
 
     def __init__(self):
