@@ -153,3 +153,24 @@ def test_load_labs_c2_geometry_vs_oracle(cn, oracle_lib):
         _, wdef = O.lab_fill(comp, nb, n, (3, 3, 3), (3, 3, 3), False, bcl[2], 5 + i)
         assert torch.equal(part[i][torch.from_numpy(wdef).cuda()], full[5 + i][torch.from_numpy(wdef).cuda()])
     U.close()
+
+
+def test_lab_fill_long_rows_vs_oracle(cn, oracle_lib):
+    """Blocks whose lab slabs hold more ghost rows than the kernel resolves in
+    one round (2 x 200 x 6 cells: 412 rows per slab), with BCs and skips on
+    every face, non-tensorial and tensorial: bit-exact against the oracle."""
+    O = oracle_lib
+    rng = np.random.default_rng(21)
+    nb, n = (2, 2, 2), (2, 200, 6)
+    nblocks = 8
+    stride = O.block_stride(n, np.float64)
+    comp = rng.standard_normal(nblocks * stride)
+    bcl = {b: [(int(rng.integers(0, 3)), int(rng.integers(0, 2)), int(rng.integers(0, 4)),
+                float(rng.choice([-1, 0.5, 2]))) for _ in range(3)] for b in range(nblocks) if b % 2}
+    for tens in (False, True):
+        g = make_grid(cn, comp, nb, n, bcl)
+        labs, written = lab_fill_all(cn, g, (1, 1, 1), (1, 1, 1), tens)
+        for b in range(nblocks):
+            want, wdef = O.lab_fill(comp, nb, n, (1, 1, 1), (1, 1, 1), tens, bcl, b)
+            LC.compare_defined(labs[b], written[b], want, wdef)
+        g.close()
