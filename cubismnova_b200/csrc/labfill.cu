@@ -14,6 +14,7 @@
 // comparison with it.
 #include "cn_fastdiv.h"
 #include "cn_internal.h"
+#include "cn_tma.cuh"
 
 #include <algorithm>
 
@@ -22,6 +23,7 @@ namespace cn {
 constexpr int KL = 4;              // cells per thread resolved before their loads
 constexpr int KL0 = 8;             // pairs of the block's own cells per thread in flight
 constexpr int KLM = 8;             // cells per thread in flight in the one-pass form
+constexpr int kBulkBytes = 40960;  // largest bulk copy of a slab's block planes
 constexpr int kCellsPerCta = 8192; // target cells of a CTA's slab
 
 // a cell's source, collected from lab_resolve
@@ -214,7 +216,7 @@ __device__ __forceinline__ void lab_store1(const T *__restrict__ comp, const Lab
 template <typename T>
 __global__ void __launch_bounds__(256, 4)
     lab_fill_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin, int pz, LabDivs dv,
-                    int apply_bc, T *__restrict__ out)
+                    int apply_bc, int bulk, int *err, T *__restrict__ out)
 {
     const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
     const int E0 = n0 + L.lo[0] + L.hi[0];
@@ -249,13 +251,27 @@ __global__ void __launch_bounds__(256, 4)
         // and the rows (classes 2, 3) whose source is a plain cell run.  The
         // rows are resolved first; cells that need BC chains or skips are
         // left to a second pass.
-        for (int j = threadIdx.x; j < nrows; j += blockDim.x)
-            rows[j] = lab_row<T>(L, bc, mode, faces, block, bx, by, bz, abc, dv, j, ny, gy, zi0, nlo, zhi, z0, E0, E1);
-        __syncthreads();
         const int A = nin * n1 * n0, B = nin * n1 * gx, tot = A + B + nrows * n0;
         const int64_t bbase = (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
+        // The block's own planes of the slab are one contiguous run of
+        // memory: with room in the dynamic shared memory (`bulk` bytes) one
+        // bulk copy brings them while the threads work on the ghosts.
+        extern __shared__ __align__(128) unsigned char lab_bulk[];
+        __shared__ __align__(8) uint64_t bulk_bar;
+        const uint32_t bytes0 = (uint32_t)A * (uint32_t)sizeof(T);
+        const bool use_bulk = A > 0 && bytes0 <= (uint32_t)bulk && ((uint32_t)(n0 * n1) * sizeof(T)) % 16 == 0;
+        if (use_bulk && threadIdx.x == 0) {
+            mbar_init(&bulk_bar, 1);
+            fence_mbar_init();
+            mbar_arrive_expect_tx(&bulk_bar, bytes0);
+            bulk_g2s(lab_bulk, comp + bbase, bytes0, &bulk_bar);
+        }
+        for (int j = threadIdx.x; j < nrows; j += blockDim.x)
+            rows[j] = lab_row<T>(L, bc, mode, faces, block, bx, by, bz, abc, dv, j, ny, gy, zi0, nlo, zhi, z0, E0, E1);
+        __syncthreads(); // the rows, and the barrier's initialisation
         bool deferred = false;
-        for (int t0 = threadIdx.x; t0 < tot; t0 += KLM * blockDim.x) {
+        const int base = use_bulk ? A : 0; // the first item of the pass
+        for (int t0 = base + threadIdx.x; t0 < tot; t0 += KLM * blockDim.x) {
             int64_t idx[KLM];
             int dst[KLM];
 #pragma unroll
@@ -298,10 +314,31 @@ __global__ void __launch_bounds__(256, 4)
             for (int k = 0; k < KLM; ++k)
                 if (dst[k] >= 0) o[dst[k]] = v[k];
         }
+        if (use_bulk) {
+            // the block's cells from shared memory
+            if (!mbar_wait_bounded_sleep(&bulk_bar, 0, 200)) {
+                // record the error; a second bounded wait keeps the copy from
+                // landing in a later CTA's shared memory
+                if (threadIdx.x == 0 && err) atomicExch(err, kDevErrTimeout);
+                mbar_wait_bounded_sleep(&bulk_bar, 0, 200);
+            } else {
+                const T *sb = reinterpret_cast<const T *>(lab_bulk);
+                for (int t0 = threadIdx.x; t0 < A; t0 += KLM * blockDim.x) {
+#pragma unroll
+                    for (int k = 0; k < KLM; ++k) {
+                        const int t = t0 + k * blockDim.x;
+                        if (t < A) {
+                            const int r = dv.n0.div(t), zp = dv.n1.div(r);
+                            o[(t - r * n0 + L.lo[0]) + E0 * ((r - zp * n1 + L.lo[1]) + E1 * (zi0 + zp))] = sb[t];
+                        }
+                    }
+                }
+            }
+        }
         if (deferred) {
             // the second pass: the same items of this thread
             const int nt = (int)blockDim.x;
-            for (int t = A + ((((int)threadIdx.x - A) % nt) + nt) % nt; t < tot; t += nt) {
+            for (int t = A + ((((int)threadIdx.x + base - A) % nt) + nt) % nt; t < tot; t += nt) {
                 LabSource<T> src[1];
                 int dst[1] = {-1};
                 if (t < A + B) {
@@ -489,7 +526,14 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
         dv.wrow = FastDiv((uint32_t)(L.tensorial ? E0 : L.n[0]));
         dv.gy = FastDiv((uint32_t)(L.lo[1] + L.hi[1]));
         dv.wpl = FastDiv((uint32_t)(L.tensorial ? E1 : L.n[1]));
-        lab_fill_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, out);
+        // dynamic shared memory for the bulk copy of a slab's block planes
+        const int64_t bulk = (int64_t)pz * L.n[0] * L.n[1] * (int64_t)sizeof(T);
+        const int nbulk = bulk <= kBulkBytes ? (int)bulk : 0;
+        static DeviceOnce once;
+        cn_status r = smem_opt_in(once, lab_fill_kernel<T>, (size_t)kBulkBytes);
+        if (r != CN_OK) return r;
+        lab_fill_kernel<T><<<grid, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, nbulk,
+                                                         g->d_err, out);
     }
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
