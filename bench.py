@@ -540,9 +540,9 @@ class C3:
     stages = 3
     launches_per_step = 3
     bytes_per_cell_step = 320
-    traffic_per_cell_step = 447.0
+    traffic_per_cell_step = 394.0
     traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 3 stage_kernel launches of one "
-                      "step on this layout (6016 MB per step), per cell and scaled to a launch")
+                      "step on this layout (5302 MB per step), per cell and scaled to a launch")
     nb, n = ("amr", "amr")
 
     def __init__(self):
