@@ -18,5 +18,6 @@ from . import mg
 from . import learned
 from . import amr
 from . import io as IO
+from . import partition
 
-__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "amr", "IO", "CnError", "build"]
+__all__ = ["Core", "BC", "Grid", "Block", "ops", "euler", "workloads", "mg", "learned", "amr", "IO", "partition", "CnError", "build"]

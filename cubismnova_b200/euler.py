@@ -61,6 +61,13 @@ def cfl_dt(U: Cartesian, cfl: float = 0.3, gamma: float = GAMMA, stream=None) ->
 
 
 def like(U: Cartesian) -> Cartesian:
-    """A work grid of the same geometry and dtype (no BCs)."""
+    """A work grid of the same geometry (blocks, cells and physical extent)
+    and dtype (no BCs)."""
     nb, n = U.getSize(), U.getBlockCells()
-    return Cartesian(nb, n, ncomp=5, dtype=U.dtype)
+    begin = getattr(U, "_begin", None)
+    end = getattr(U, "_end", None)
+    if begin is None or end is None:  # a view of a library-made grid: its extent from the cell size
+        begin = (0.0, 0.0, 0.0)
+        h = U.getCellSize()
+        end = tuple(nb[d] * n[d] * h[d] for d in range(3))
+    return Cartesian(nb, n, begin, end, ncomp=5, dtype=U.dtype)

@@ -140,6 +140,7 @@ class Cartesian:
         h = C.c_void_p()
         self.entity = entity
         self._begin = tuple(float(v) for v in begin)
+        self._end = tuple(float(v) for v in end)
         _lib.check(_lib.lib().cn_grid_create_entity(_lib.ivec3(nb), _lib.ivec3(bc), self.ncomp, _DT[self.dtype],
                                                     ENTITIES[entity], _lib.dvec3(begin), _lib.dvec3(end),
                                                     C.byref(h)))
