@@ -33,12 +33,20 @@
 // dominant product t_max t_mid lies in [1, 64) and every FP32 denominator in
 // [0.6, 384]; the only products that can underflow are those of negligible
 // weights.  FP64 needs no scaling: its denominators lie in [6e-25, ~70 J^8].
+// Since the factor is an exact power of two, the scaled and unscaled forms
+// give the same values wherever the unscaled one stays in range; a tile whose
+// primitives are all within kUnscaledMax in magnitude (then t_i t_j < 1.3e30
+// and the numerators < 2e34, eps keeps them above 1e-24) skips the scaling
+// (`scaled` false).
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace cn {
 namespace euler {
+
+// largest primitive magnitude of a tile for the unscaled FP32 WENO5 weights
+constexpr float kUnscaledMax = 1000.0f;
 
 template <typename T> struct K {
     static constexpr T c1312 = T(13.0 / 12.0);
@@ -119,7 +127,8 @@ template <typename T> __device__ __forceinline__ Diff5<T> weno5_diff(T u0, T u1,
 // b0/2 = a0/2 + d12, b1/2 = (d12 + d23)/2 (up to sign), b2/2 = a2/2 - d23.
 // They serve both states of the cell (left-biased at j+1/2, right-biased at
 // j-1/2), so a cell's indicators are computed once for its two faces.
-template <typename T> __device__ __forceinline__ void weno5_beta(const Diff5<T> &d, T &p12, T &p02, T &p01)
+template <typename T>
+__device__ __forceinline__ void weno5_beta(const Diff5<T> &d, T &p12, T &p02, T &p01, bool scaled = true)
 {
     using C = K<T>;
     const T a0 = d.d12 - d.d01, a1 = d.d23 - d.d12, a2 = d.d34 - d.d23;
@@ -131,10 +140,12 @@ template <typename T> __device__ __forceinline__ void weno5_beta(const Diff5<T> 
     const T s2 = dfma(C::c1312 * a2, a2, dfma(h2, h2, C::eps));
     T q0 = s0, q1 = s1, q2 = s2;
     if constexpr (sizeof(T) == 4) { // FP32: exact power-of-two rescaling
-        const T sc = weno5_scale(s0, s1, s2);
-        q0 = s0 * sc;
-        q1 = s1 * sc;
-        q2 = s2 * sc;
+        if (scaled) {
+            const T sc = weno5_scale(s0, s1, s2);
+            q0 = s0 * sc;
+            q1 = s1 * sc;
+            q2 = s2 * sc;
+        }
     }
     const T t0 = q0 * q0, t1 = q1 * q1, t2 = q2 * q2;
     p12 = t1 * t2;
@@ -223,7 +234,8 @@ __device__ __forceinline__ float2 weno5_scale2(float2 s0, float2 s1, float2 s2)
 
 // weno5_beta for a pair (rescaling factors from weno5_scale2).  h2 enters
 // squared only, so its sign is dropped: h2' = d23 - a2/2.
-__device__ __forceinline__ void weno5_beta2(const Diff5x2 &d, float2 &p12, float2 &p02, float2 &p01)
+__device__ __forceinline__ void weno5_beta2(const Diff5x2 &d, float2 &p12, float2 &p02, float2 &p01,
+                                            bool scaled = true)
 {
     using C = K<float>;
     const float2 a0 = sub2(d.d12, d.d01), a1 = sub2(d.d23, d.d12), a2 = sub2(d.d34, d.d23);
@@ -233,8 +245,13 @@ __device__ __forceinline__ void weno5_beta2(const Diff5x2 &d, float2 &p12, float
     const float2 s0 = fma2(mul2(f2(C::c1312), a0), a0, fma2(h0, h0, f2(C::eps)));
     const float2 s1 = fma2(mul2(f2(C::c1312), a1), a1, fma2(h1, h1, f2(C::eps)));
     const float2 s2 = fma2(mul2(f2(C::c1312), a2), a2, fma2(h2, h2, f2(C::eps)));
-    const float2 sc = weno5_scale2(s0, s1, s2);
-    const float2 q0 = mul2(s0, sc), q1 = mul2(s1, sc), q2 = mul2(s2, sc);
+    float2 q0 = s0, q1 = s1, q2 = s2;
+    if (scaled) {
+        const float2 sc = weno5_scale2(s0, s1, s2);
+        q0 = mul2(s0, sc);
+        q1 = mul2(s1, sc);
+        q2 = mul2(s2, sc);
+    }
     const float2 t0 = mul2(q0, q0), t1 = mul2(q1, q1), t2 = mul2(q2, q2);
     p12 = mul2(t1, t2);
     p02 = mul2(t0, t2);

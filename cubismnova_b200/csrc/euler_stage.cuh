@@ -217,24 +217,25 @@ __device__ __forceinline__ void halo_cell(int D, int i, int &x, int &y, int &z, 
 // the left state waits in a carry for the next face.  id[0..4]: shared
 // entries of the cells a-2 .. a+2 around cell a.
 template <typename T>
-__device__ __forceinline__ T cell_left(const T *Wc, const int (&id)[5])
+__device__ __forceinline__ T cell_left(const T *Wc, const int (&id)[5], bool scaled = true)
 {
     const T u2 = Wc[id[2]];
     const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
     T p12, p02, p01, nl, dl;
-    weno5_beta(df, p12, p02, p01);
+    weno5_beta(df, p12, p02, p01, scaled);
     weno5_left(df, p12, K<T>::d1 * p02, p01, nl, dl);
     return weno5_value(u2, nl, dl);
 }
 // face a: WL = carried left state of cell a-1, WR = right state of cell a;
 // with `more` the carry becomes cell a's left state
 template <typename T>
-__device__ __forceinline__ void cell_face(const T *Wc, const int (&id)[5], bool more, T &carry, T &wl, T &wr)
+__device__ __forceinline__ void cell_face(const T *Wc, const int (&id)[5], bool more, T &carry, T &wl, T &wr,
+                                          bool scaled = true)
 {
     const T u2 = Wc[id[2]];
     const Diff5<T> df = weno5_diff(Wc[id[0]], Wc[id[1]], u2, Wc[id[3]], Wc[id[4]]);
     T p12, p02, p01, nr, dr;
-    weno5_beta(df, p12, p02, p01);
+    weno5_beta(df, p12, p02, p01, scaled);
     const T w1 = K<T>::d1 * p02;
     weno5_right(df, p12, w1, p01, nr, dr);
     wr = weno5_value(u2, nr, dr);
@@ -245,22 +246,22 @@ __device__ __forceinline__ void cell_face(const T *Wc, const int (&id)[5], bool 
         carry = weno5_value(u2, nl, dl);
     }
 }
-__device__ __forceinline__ float2 pair_left(const float2 *P, const int (&id)[5])
+__device__ __forceinline__ float2 pair_left(const float2 *P, const int (&id)[5], bool scaled)
 {
     const float2 u2 = P[id[2]];
     const Diff5x2 df = weno5_diff2(P[id[0]], P[id[1]], u2, P[id[3]], P[id[4]]);
     float2 p12, p02, p01, nl, dl;
-    weno5_beta2(df, p12, p02, p01);
+    weno5_beta2(df, p12, p02, p01, scaled);
     weno5_left2(df, p12, mul2(f2(K<float>::d1), p02), p01, nl, dl);
     return weno5_value2(u2, nl, dl);
 }
 __device__ __forceinline__ void pair_face(const float2 *P, const int (&id)[5], bool more, float2 &carry, float2 &wl,
-                                          float2 &wr)
+                                          float2 &wr, bool scaled)
 {
     const float2 u2 = P[id[2]];
     const Diff5x2 df = weno5_diff2(P[id[0]], P[id[1]], u2, P[id[3]], P[id[4]]);
     float2 p12, p02, p01, nr, dr;
-    weno5_beta2(df, p12, p02, p01);
+    weno5_beta2(df, p12, p02, p01, scaled);
     const float2 w1 = mul2(f2(K<float>::d1), p02);
     weno5_right2(df, p12, w1, p01, nr, dr);
     wr = weno5_value2(u2, nr, dr);
@@ -281,34 +282,34 @@ struct CarryF {
     float2 p01, p23;
     float v4;
 };
-__device__ __forceinline__ void line_left(const double *W, const int (&id)[5], CarryD &cl)
+__device__ __forceinline__ void line_left(const double *W, const int (&id)[5], CarryD &cl, bool)
 {
 #pragma unroll
     for (int c = 0; c < 5; ++c)
         cl.v[c] = cell_left(W + c * Stg<double>::SV, id);
 }
 __device__ __forceinline__ void line_face(const double *W, const int (&id)[5], bool more, CarryD &cl,
-                                          double (&WL)[5], double (&WR)[5])
+                                          double (&WL)[5], double (&WR)[5], bool)
 {
 #pragma unroll
     for (int c = 0; c < 5; ++c)
         cell_face(W + c * Stg<double>::SV, id, more, cl.v[c], WL[c], WR[c]);
 }
-__device__ __forceinline__ void line_left(const float *W, const int (&id)[5], CarryF &cl)
+__device__ __forceinline__ void line_left(const float *W, const int (&id)[5], CarryF &cl, bool scaled)
 {
     constexpr int SV = Stg<float>::SV;
-    cl.p01 = pair_left(reinterpret_cast<const float2 *>(W), id);
-    cl.p23 = pair_left(reinterpret_cast<const float2 *>(W + 2 * SV), id);
-    cl.v4 = cell_left(W + 4 * SV, id);
+    cl.p01 = pair_left(reinterpret_cast<const float2 *>(W), id, scaled);
+    cl.p23 = pair_left(reinterpret_cast<const float2 *>(W + 2 * SV), id, scaled);
+    cl.v4 = cell_left(W + 4 * SV, id, scaled);
 }
 __device__ __forceinline__ void line_face(const float *W, const int (&id)[5], bool more, CarryF &cl,
-                                          float (&WL)[5], float (&WR)[5])
+                                          float (&WL)[5], float (&WR)[5], bool scaled)
 {
     constexpr int SV = Stg<float>::SV;
     float2 l01, r01, l23, r23;
-    pair_face(reinterpret_cast<const float2 *>(W), id, more, cl.p01, l01, r01);
-    pair_face(reinterpret_cast<const float2 *>(W + 2 * SV), id, more, cl.p23, l23, r23);
-    cell_face(W + 4 * SV, id, more, cl.v4, WL[4], WR[4]);
+    pair_face(reinterpret_cast<const float2 *>(W), id, more, cl.p01, l01, r01, scaled);
+    pair_face(reinterpret_cast<const float2 *>(W + 2 * SV), id, more, cl.p23, l23, r23, scaled);
+    cell_face(W + 4 * SV, id, more, cl.v4, WL[4], WR[4], scaled);
     WL[0] = l01.x;
     WL[1] = l01.y;
     WL[2] = l23.x;
@@ -338,7 +339,8 @@ template <> struct CarryOf<float> {
 // barrier.  R and X: [5][NACC] with R at entry core_sm(x, y, z) and X at
 // NCORE_SM + 64 (r - 1) + line.
 template <typename T>
-__device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restrict__ A, T gamma, T igm1, T ihd)
+__device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restrict__ A, T gamma, T igm1, T ihd,
+                                      bool scaled)
 {
     const int cs = D == 0 ? 1 : (D == 1 ? CY : CZ);     // shared stride along D (core and halo slot)
     const int run = threadIdx.x >> 6, line = threadIdx.x & 63;
@@ -359,7 +361,7 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
 #pragma unroll
     for (int k = 0; k < 5; ++k)
         id[k] = sidx(f0 - 3 + k);
-    line_left(W, id, carry);
+    line_left(W, id, carry, scaled);
     T Fq[5]; // flux of the previous face of the run
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
@@ -375,7 +377,7 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
                 id[k] = sidx(a - 2 + k);
         }
         T WL[5], WR[5];
-        line_face(W, id, i < 2, carry, WL, WR);
+        line_face(W, id, i < 2, carry, WL, WR, scaled);
         T Fl[5];
         rusanov<T>(WL, WR, D, gamma, igm1, Fl);
         if (i == 0) {
@@ -418,7 +420,7 @@ __device__ __forceinline__ void sweep(int D, const T *__restrict__ W, T *__restr
 // exists once.
 template <typename T, typename Src>
 __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const Src &src, const TileInfo<T> &t,
-                                           T *W, const int *snb)
+                                           T *W, const int *snb, T &vmax)
 {
     static_assert(NHALO % NT == 0, "whole halo cells per thread");
     constexpr int HPT = NHALO / NT; // halo cells per thread: 2
@@ -469,8 +471,10 @@ __device__ __forceinline__ void stage_halo(int D, const StageParams<T> &p, const
         T w[5];
         to_primitive<T>(u[j][0], u[j][1], u[j][2], u[j][3], u[j][4], p.gm1, w);
 #pragma unroll
-        for (int c = 0; c < 5; ++c)
+        for (int c = 0; c < 5; ++c) {
             prim(W, c, sb + si[j]) = w[c];
+            if constexpr (sizeof(T) == 4) vmax = fmaxf(vmax, fabsf(w[c]));
+        }
     }
 }
 
@@ -500,6 +504,9 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
     __syncthreads(); // snb
     // ---- stage the tile's cells as primitives (the halo slot follows per
     // sweep): all of a thread's loads are issued before any conversion
+    // FP32: the largest primitive magnitude the thread stages (NaN data
+    // gives NaN states on either form of the weights)
+    T vmax = T(0);
     auto convert_core = [&](T (&u)[CPT][5]) {
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
@@ -509,8 +516,10 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
                 to_primitive<T>(u[k][0], u[k][1], u[k][2], u[k][3], u[k][4], p.gm1, w);
                 const int e = core_sm(i % TB, (i / TB) % TB, i / (TB * TB));
 #pragma unroll
-                for (int c = 0; c < 5; ++c)
+                for (int c = 0; c < 5; ++c) {
                     prim(W, c, e) = w[c];
+                    if constexpr (sizeof(T) == 4) vmax = fmaxf(vmax, fabsf(w[c]));
+                }
             }
         }
     };
@@ -553,24 +562,29 @@ __device__ __forceinline__ void stage_tile(const StageParams<T> &p, const Src &s
         }
         convert_core(u);
     }
+    // FP32 stages all three halo slots here; the tile's WENO5 weights skip
+    // the range rescaling when every staged primitive is within
+    // kUnscaledMax (same values, fewer instructions: see euler_math.cuh)
+    bool scaled = true;
     if (Stg<T>::all) {
 #pragma unroll 1
         for (int D = 0; D < 3; ++D)
-            stage_halo<T>(D, p, src, t, W, snb);
+            stage_halo<T>(D, p, src, t, W, snb, vmax);
+        scaled = __syncthreads_or(!(vmax <= T(kUnscaledMax))) != 0;
     } else {
-        stage_halo<T>(0, p, src, t, W, snb);
+        stage_halo<T>(0, p, src, t, W, snb, vmax);
+        __syncthreads();
     }
-    __syncthreads();
 
 #pragma unroll 1
     for (int D = 0; D < 3; ++D) {
         if (!Stg<T>::all && D > 0) {
-            stage_halo<T>(D, p, src, t, W, snb);
+            stage_halo<T>(D, p, src, t, W, snb, vmax);
             __syncthreads();
         }
         // the Rusanov fluxes are twice the flux: 1/(2h) (exact)
         const T ihd = T(0.5) * (D == 0 ? t.ih[0] : (D == 1 ? t.ih[1] : t.ih[2]));
-        sweep<T>(D, W, A, p.gamma, p.igm1, ihd);
+        sweep<T>(D, W, A, p.gamma, p.igm1, ihd, scaled);
     }
 
     // ---- epilogue: RHS or SSP-RK3 stage, coalesced along x of the tile rows.
