@@ -1,17 +1,21 @@
 // labfill.cu -- K0: explicit lab fill (Cartesian::loadLab into lab buffers).
 //
-// One CTA per (block, slab of lab planes along z): the slab's cells are
-// written in order by consecutive threads (coalesced stores; inner and face
-// cells read along x of the source block).  Each cell is resolved on its own
-// by the FieldLab resolution (cn::lab_resolve: inner copy, periodic
-// neighbour gather, BC chain); a thread resolves KL cells first and then
-// issues their loads together, so that KL loads per thread are in flight
-// (the kernel is a stream of loads and stores, bound by HBM).  The block's
-// coordinates and BC summary are read once per CTA and a cell's (x, y, z)
-// come from multiply-high divisions.  The stencil kernels fuse the same
-// resolution into their shared-memory staging; this kernel gives the
-// reference's FieldLab contents for user stencils and the bit-exact
-// comparison with it.
+// One CTA per (block, slab of lab planes along z).  The slab's lab cells
+// fall into four classes: the block's own cells, the x ghosts of the rows
+// inside the block, the y-ghost rows of the inside planes and the z-ghost
+// planes (non-tensorial labs: edges and corners stay undefined, as in the
+// reference).  The block's own planes are one contiguous run of memory,
+// brought by one bulk copy into shared memory; meanwhile the threads walk
+// the ghosts, those behind faces without a BC or a skipped neighbour in
+// closed form (the periodic neighbour's cell), eight loads in flight per
+// thread; ghost rows behind faces with BCs are resolved once per row (x
+// passes through the FieldLab resolution unchanged), other BC-chain cells
+// one by one (cn::lab_resolve: skip rule, BC chain).  Tensorial labs, node
+// and face grids take per-class or per-cell resolution throughout.  Stores
+// are coalesced along the lab's rows; the kernel is bound by memory
+// latency and HBM.  The stencil kernels fuse the same resolution into their
+// shared-memory staging; this kernel gives the reference's FieldLab
+// contents for user stencils and the bit-exact comparison with it.
 #include "cn_fastdiv.h"
 #include "cn_internal.h"
 #include "cn_tma.cuh"
