@@ -27,8 +27,13 @@ namespace cn {
 constexpr int KL = 4;              // cells per thread resolved before their loads
 constexpr int KL0 = 8;             // pairs of the block's own cells per thread in flight
 constexpr int KLM = 8;             // cells per thread in flight in the one-pass form
-constexpr int kBulkBytes = 40960;  // largest bulk copy of a slab's block planes
-constexpr int kCellsPerCta = 8192; // target cells of a CTA's slab
+constexpr int kBulkBytes = 24576;  // largest bulk copy of a slab's block planes
+// target cells of a CTA's slab: three planes of the 38^2 lab of 32^3 blocks
+// with three ghosts.  Thinner slabs leave more of the SM's on-chip memory
+// to the L1 cache (the shared-memory carve-out follows the resident CTAs'
+// needs), which measured faster than thicker slabs
+constexpr int kCellsPerCta = 4332;
+constexpr int kRowsCtas = 4;       // resident CTAs per SM of the one-pass kernel
 
 // a cell's source, collected from lab_resolve
 template <typename T> struct LabSource {
@@ -120,7 +125,7 @@ template <typename T> struct RowSrc {
     LabSource<T> s;
     int dst;
 };
-constexpr int kRows = 256; // rows resolved per round
+constexpr int kRows = 96; // rows resolved per round
 
 template <typename T> struct Vec2;
 template <> struct Vec2<double> {
@@ -191,6 +196,25 @@ __device__ __forceinline__ RowSrc<T> lab_row(const LabGeom &L, const BcView &bc,
     return R;
 }
 
+// Lab planes [z0, z1) of a CTA's slab: the planes inside the block
+// [zi0, zi0 + nin), nlo z-ghost planes below them and the z-ghost planes
+// from zhi up (nghost in all).
+struct SlabPlanes {
+    int zi0, nin, nlo, zhi, nghost;
+};
+__host__ __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+__host__ __device__ __forceinline__ SlabPlanes slab_planes(const LabGeom &L, int z0, int z1)
+{
+    SlabPlanes P;
+    P.zi0 = imax(z0, L.lo[2]);
+    P.nin = imax(0, imin(z1, L.lo[2] + L.n[2]) - P.zi0);
+    P.nlo = imax(0, imin(z1, L.lo[2]) - z0);
+    P.zhi = imax(z0, L.lo[2] + L.n[2]);
+    P.nghost = P.nlo + imax(0, z1 - P.zhi);
+    return P;
+}
+
 // one cell's source stored (kind 0: nothing)
 template <typename T>
 __device__ __forceinline__ void lab_store1(const T *__restrict__ comp, const LabSource<T> &s, int dst, T *__restrict__ o)
@@ -203,6 +227,150 @@ __device__ __forceinline__ void lab_store1(const T *__restrict__ comp, const Lab
         if (s.nsign > 0) x = s.s0 * x;
     }
     o[dst] = x;
+}
+
+// Cell grids with non-tensorial labs whose ghost rows (classes 2 and 3
+// below) fit in shared memory (kRows per slab), the common case: the
+// one-pass form.  It is a kernel of its own so that the general form's
+// per-class loops do not set its register count (it holds none of their
+// spill slots and runs at kRowsCtas CTAs per SM).
+template <typename T>
+__global__ void __launch_bounds__(256, kRowsCtas)
+    lab_fill_rows_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin, int pz, LabDivs dv,
+                         int apply_bc, int bulk, int *err, T *__restrict__ out)
+{
+    const int n0 = L.n[0], n1 = L.n[1];
+    const int E0 = n0 + L.lo[0] + L.hi[0];
+    const int E1 = n1 + L.lo[1] + L.hi[1];
+    const int E2 = L.n[2] + L.lo[2] + L.hi[2];
+    const int bl = blockIdx.x, z0 = blockIdx.y * pz;
+    const int block = block_begin + bl;
+    const int bx = block % L.nb[0];
+    const int by = (block / L.nb[0]) % L.nb[1];
+    const int bz = block / (L.nb[0] * L.nb[1]);
+    const uint8_t mode = bc.mode[block];
+    const uint8_t faces = bc.faces[block];
+    const bool abc = apply_bc != 0;
+    const SlabPlanes P = slab_planes(L, z0, min(z0 + pz, E2));
+    const int zi0 = P.zi0, nin = P.nin, nlo = P.nlo, zhi = P.zhi;
+    const int gx = L.lo[0] + L.hi[0], gy = L.lo[1] + L.hi[1];
+    T *o = out + (int64_t)bl * E0 * E1 * E2;
+    const int ny = nin * gy, nrows = ny + P.nghost * n1;
+    __shared__ __align__(16) unsigned char rows_raw[kRows * sizeof(RowSrc<T>)];
+    RowSrc<T> *rows = reinterpret_cast<RowSrc<T> *>(rows_raw);
+    // One pass over all three kinds of plain copies, KLM loads in flight
+    // per thread: the block's own cells, the x ghosts behind clear faces
+    // and the rows (classes 2, 3) whose source is a plain cell run.  The
+    // rows are resolved first; cells that need BC chains or skips are
+    // left to a second pass.
+    const int A = nin * n1 * n0, B = nin * n1 * gx, tot = A + B + nrows * n0;
+    const int64_t bbase = (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
+    // The block's own planes of the slab are one contiguous run of
+    // memory: with room in the dynamic shared memory (`bulk` bytes) one
+    // bulk copy brings them while the threads work on the ghosts.
+    extern __shared__ __align__(128) unsigned char lab_bulk[];
+    __shared__ __align__(8) uint64_t bulk_bar;
+    const uint32_t bytes0 = (uint32_t)A * (uint32_t)sizeof(T);
+    const bool use_bulk = A > 0 && bytes0 <= (uint32_t)bulk && ((uint32_t)(n0 * n1) * sizeof(T)) % 16 == 0;
+    if (use_bulk && threadIdx.x == 0) {
+        mbar_init(&bulk_bar, 1);
+        fence_mbar_init();
+        mbar_arrive_expect_tx(&bulk_bar, bytes0);
+        bulk_g2s(lab_bulk, comp + bbase, bytes0, &bulk_bar);
+    }
+    for (int j = threadIdx.x; j < nrows; j += blockDim.x)
+        rows[j] = lab_row<T>(L, bc, mode, faces, block, bx, by, bz, abc, dv, j, ny, gy, zi0, nlo, zhi, z0, E0, E1);
+    __syncthreads(); // the rows, and the barrier's initialisation
+    bool deferred = false;
+    const int base = use_bulk ? A : 0; // the first item of the pass
+    for (int t0 = base + threadIdx.x; t0 < tot; t0 += KLM * blockDim.x) {
+        int64_t idx[KLM];
+        int dst[KLM];
+#pragma unroll
+        for (int k = 0; k < KLM; ++k) {
+            const int t = t0 + k * blockDim.x;
+            dst[k] = -1;
+            idx[k] = 0;
+            if (t < A) {
+                const int r = dv.n0.div(t), zp = dv.n1.div(r);
+                dst[k] = (t - r * n0 + L.lo[0]) + E0 * ((r - zp * n1 + L.lo[1]) + E1 * (zi0 + zp));
+                idx[k] = bbase + t;
+            } else if (t < A + B) {
+                int x, y, z;
+                class1_cell(dv, t - A, gx, n0, n1, L.lo[0], L.lo[1], zi0, x, y, z);
+                const int q0 = x - L.lo[0], r0 = q0 < 0 ? -1 : 1;
+                if (faces & (r0 < 0 ? 1 : 2)) {
+                    deferred = true;
+                } else {
+                    const int nbx = bx + r0 < 0 ? bx + r0 + L.nb[0] : (bx + r0 >= L.nb[0] ? bx + r0 - L.nb[0] : bx + r0);
+                    dst[k] = x + E0 * (y + E1 * z);
+                    idx[k] = (int64_t)(nbx + L.nb[0] * (by + L.nb[1] * bz)) * L.bstride + (q0 - r0 * n0) +
+                             n0 * ((y - L.lo[1]) + n1 * (z - L.lo[2]));
+                }
+            } else if (t < tot) {
+                const int u = t - A - B, j = dv.n0.div(u), x = u - j * n0;
+                const RowSrc<T> &R = rows[j];
+                if (R.s.kind == 2 && R.s.nsign == 0) {
+                    dst[k] = R.dst + x;
+                    idx[k] = R.s.idx + x;
+                } else {
+                    deferred = true;
+                }
+            }
+        }
+        T v[KLM];
+#pragma unroll
+        for (int k = 0; k < KLM; ++k)
+            if (dst[k] >= 0) v[k] = comp[idx[k]];
+#pragma unroll
+        for (int k = 0; k < KLM; ++k)
+            if (dst[k] >= 0) o[dst[k]] = v[k];
+    }
+    if (use_bulk) {
+        // the block's cells from shared memory
+        if (!mbar_wait_bounded_sleep(&bulk_bar, 0, 200)) {
+            // record the error; a second bounded wait keeps the copy from
+            // landing in a later CTA's shared memory
+            if (threadIdx.x == 0 && err) atomicExch(err, kDevErrTimeout);
+            mbar_wait_bounded_sleep(&bulk_bar, 0, 200);
+        } else {
+            const T *sb = reinterpret_cast<const T *>(lab_bulk);
+            for (int t0 = threadIdx.x; t0 < A; t0 += KLM * blockDim.x) {
+#pragma unroll
+                for (int k = 0; k < KLM; ++k) {
+                    const int t = t0 + k * blockDim.x;
+                    if (t < A) {
+                        const int r = dv.n0.div(t), zp = dv.n1.div(r);
+                        o[(t - r * n0 + L.lo[0]) + E0 * ((r - zp * n1 + L.lo[1]) + E1 * (zi0 + zp))] = sb[t];
+                    }
+                }
+            }
+        }
+    }
+    if (deferred) {
+        // the second pass: the same items of this thread
+        const int nt = (int)blockDim.x;
+        for (int t = A + ((((int)threadIdx.x + base - A) % nt) + nt) % nt; t < tot; t += nt) {
+            LabSource<T> src[1];
+            int dst[1] = {-1};
+            if (t < A + B) {
+                int x, y, z;
+                class1_cell(dv, t - A, gx, n0, n1, L.lo[0], L.lo[1], zi0, x, y, z);
+                if (!(faces & (x < L.lo[0] ? 1 : 2))) continue;
+                lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, x - L.lo[0], y - L.lo[1], z - L.lo[2], abc,
+                                      src[0]);
+                dst[0] = x + E0 * (y + E1 * z);
+            } else {
+                const int u = t - A - B, j = dv.n0.div(u), x = u - j * n0;
+                const RowSrc<T> &R = rows[j];
+                if (R.s.kind == 2 && R.s.nsign == 0) continue;
+                src[0] = R.s;
+                src[0].idx += x;
+                dst[0] = R.dst + x;
+            }
+            lab_store1<T>(comp, src[0], dst[0], o);
+        }
+    }
 }
 
 // Cell grids: the CTA's slab of lab planes as four classes of cells, each
@@ -220,7 +388,7 @@ __device__ __forceinline__ void lab_store1(const T *__restrict__ comp, const Lab
 template <typename T>
 __global__ void __launch_bounds__(256, 4)
     lab_fill_kernel(const T *__restrict__ comp, LabGeom L, BcView bc, int block_begin, int pz, LabDivs dv,
-                    int apply_bc, int bulk, int *err, T *__restrict__ out)
+                    int apply_bc, T *__restrict__ out)
 {
     const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
     const int E0 = n0 + L.lo[0] + L.hi[0];
@@ -238,133 +406,14 @@ __global__ void __launch_bounds__(256, 4)
     const uint8_t faces = bc.faces[block];
     const bool abc = apply_bc != 0, tens = L.tensorial != 0;
     // planes of the slab inside the block, and its z-ghost planes below / above
-    const int zi0 = max(z0, L.lo[2]), zi1 = min(z1, L.lo[2] + n2);
-    const int nin = max(0, zi1 - zi0);
-    const int nlo = max(0, min(z1, L.lo[2]) - z0);
-    const int zhi = max(z0, L.lo[2] + n2);
-    const int nghost = nlo + max(0, z1 - zhi);
+    const SlabPlanes P = slab_planes(L, z0, z1);
+    const int zi0 = P.zi0, nin = P.nin, nlo = P.nlo, zhi = P.zhi, nghost = P.nghost;
     const int wrow = tens ? E0 : n0, wpl = tens ? E1 : n1;
     const int gx = L.lo[0] + L.hi[0], gy = L.lo[1] + L.hi[1];
     T *o = out + (int64_t)bl * E0 * E1 * E2;
     const int ny = nin * gy, nrows = ny + nghost * n1;
     __shared__ __align__(16) unsigned char rows_raw[kRows * sizeof(RowSrc<T>)];
     RowSrc<T> *rows = reinterpret_cast<RowSrc<T> *>(rows_raw);
-    if (!tens && nrows <= kRows) {
-        // One pass over all three kinds of plain copies, KLM loads in flight
-        // per thread: the block's own cells, the x ghosts behind clear faces
-        // and the rows (classes 2, 3) whose source is a plain cell run.  The
-        // rows are resolved first; cells that need BC chains or skips are
-        // left to a second pass.
-        const int A = nin * n1 * n0, B = nin * n1 * gx, tot = A + B + nrows * n0;
-        const int64_t bbase = (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
-        // The block's own planes of the slab are one contiguous run of
-        // memory: with room in the dynamic shared memory (`bulk` bytes) one
-        // bulk copy brings them while the threads work on the ghosts.
-        extern __shared__ __align__(128) unsigned char lab_bulk[];
-        __shared__ __align__(8) uint64_t bulk_bar;
-        const uint32_t bytes0 = (uint32_t)A * (uint32_t)sizeof(T);
-        const bool use_bulk = A > 0 && bytes0 <= (uint32_t)bulk && ((uint32_t)(n0 * n1) * sizeof(T)) % 16 == 0;
-        if (use_bulk && threadIdx.x == 0) {
-            mbar_init(&bulk_bar, 1);
-            fence_mbar_init();
-            mbar_arrive_expect_tx(&bulk_bar, bytes0);
-            bulk_g2s(lab_bulk, comp + bbase, bytes0, &bulk_bar);
-        }
-        for (int j = threadIdx.x; j < nrows; j += blockDim.x)
-            rows[j] = lab_row<T>(L, bc, mode, faces, block, bx, by, bz, abc, dv, j, ny, gy, zi0, nlo, zhi, z0, E0, E1);
-        __syncthreads(); // the rows, and the barrier's initialisation
-        bool deferred = false;
-        const int base = use_bulk ? A : 0; // the first item of the pass
-        for (int t0 = base + threadIdx.x; t0 < tot; t0 += KLM * blockDim.x) {
-            int64_t idx[KLM];
-            int dst[KLM];
-#pragma unroll
-            for (int k = 0; k < KLM; ++k) {
-                const int t = t0 + k * blockDim.x;
-                dst[k] = -1;
-                idx[k] = 0;
-                if (t < A) {
-                    const int r = dv.n0.div(t), zp = dv.n1.div(r);
-                    dst[k] = (t - r * n0 + L.lo[0]) + E0 * ((r - zp * n1 + L.lo[1]) + E1 * (zi0 + zp));
-                    idx[k] = bbase + t;
-                } else if (t < A + B) {
-                    int x, y, z;
-                    class1_cell(dv, t - A, gx, n0, n1, L.lo[0], L.lo[1], zi0, x, y, z);
-                    const int q0 = x - L.lo[0], r0 = q0 < 0 ? -1 : 1;
-                    if (faces & (r0 < 0 ? 1 : 2)) {
-                        deferred = true;
-                    } else {
-                        const int nbx = bx + r0 < 0 ? bx + r0 + L.nb[0] : (bx + r0 >= L.nb[0] ? bx + r0 - L.nb[0] : bx + r0);
-                        dst[k] = x + E0 * (y + E1 * z);
-                        idx[k] = (int64_t)(nbx + L.nb[0] * (by + L.nb[1] * bz)) * L.bstride + (q0 - r0 * n0) +
-                                 n0 * ((y - L.lo[1]) + n1 * (z - L.lo[2]));
-                    }
-                } else if (t < tot) {
-                    const int u = t - A - B, j = dv.n0.div(u), x = u - j * n0;
-                    const RowSrc<T> &R = rows[j];
-                    if (R.s.kind == 2 && R.s.nsign == 0) {
-                        dst[k] = R.dst + x;
-                        idx[k] = R.s.idx + x;
-                    } else {
-                        deferred = true;
-                    }
-                }
-            }
-            T v[KLM];
-#pragma unroll
-            for (int k = 0; k < KLM; ++k)
-                if (dst[k] >= 0) v[k] = comp[idx[k]];
-#pragma unroll
-            for (int k = 0; k < KLM; ++k)
-                if (dst[k] >= 0) o[dst[k]] = v[k];
-        }
-        if (use_bulk) {
-            // the block's cells from shared memory
-            if (!mbar_wait_bounded_sleep(&bulk_bar, 0, 200)) {
-                // record the error; a second bounded wait keeps the copy from
-                // landing in a later CTA's shared memory
-                if (threadIdx.x == 0 && err) atomicExch(err, kDevErrTimeout);
-                mbar_wait_bounded_sleep(&bulk_bar, 0, 200);
-            } else {
-                const T *sb = reinterpret_cast<const T *>(lab_bulk);
-                for (int t0 = threadIdx.x; t0 < A; t0 += KLM * blockDim.x) {
-#pragma unroll
-                    for (int k = 0; k < KLM; ++k) {
-                        const int t = t0 + k * blockDim.x;
-                        if (t < A) {
-                            const int r = dv.n0.div(t), zp = dv.n1.div(r);
-                            o[(t - r * n0 + L.lo[0]) + E0 * ((r - zp * n1 + L.lo[1]) + E1 * (zi0 + zp))] = sb[t];
-                        }
-                    }
-                }
-            }
-        }
-        if (deferred) {
-            // the second pass: the same items of this thread
-            const int nt = (int)blockDim.x;
-            for (int t = A + ((((int)threadIdx.x + base - A) % nt) + nt) % nt; t < tot; t += nt) {
-                LabSource<T> src[1];
-                int dst[1] = {-1};
-                if (t < A + B) {
-                    int x, y, z;
-                    class1_cell(dv, t - A, gx, n0, n1, L.lo[0], L.lo[1], zi0, x, y, z);
-                    if (!(faces & (x < L.lo[0] ? 1 : 2))) continue;
-                    lab_resolve<T, false>(L, bc, mode, block, bx, by, bz, x - L.lo[0], y - L.lo[1], z - L.lo[2], abc,
-                                          src[0]);
-                    dst[0] = x + E0 * (y + E1 * z);
-                } else {
-                    const int u = t - A - B, j = dv.n0.div(u), x = u - j * n0;
-                    const RowSrc<T> &R = rows[j];
-                    if (R.s.kind == 2 && R.s.nsign == 0) continue;
-                    src[0] = R.s;
-                    src[0].idx += x;
-                    dst[0] = R.dst + x;
-                }
-                lab_store1<T>(comp, src[0], dst[0], o);
-            }
-        }
-        return;
-    }
     // class 0: rows of the block's own cells, plain copies (KL loads in flight)
     {
         const T *blk = comp + (int64_t)block * L.bstride + (int64_t)n0 * n1 * (zi0 - L.lo[2]);
@@ -513,13 +562,28 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
     if (plane * E2 >= (int64_t(1) << 31))
         return fail(CN_ERR_UNSUPPORTED, "cn_lab_fill: labs of 2^31 cells or more");
     // planes per CTA: about kCellsPerCta cells
-    const int pz = (int)std::max<int64_t>(1, std::min<int64_t>(E2, kCellsPerCta / plane));
+    int pz = (int)std::max<int64_t>(1, std::min<int64_t>(E2, kCellsPerCta / plane));
+    const bool grow = L.grow[0] || L.grow[1] || L.grow[2];
+    // The one-pass kernel holds a slab's ghost rows (classes 2, 3) in a
+    // table of kRows: slabs of fewer planes until every slab's rows fit.
+    auto rows_fit = [&](int p) {
+        for (int z0 = 0; z0 < E2; z0 += p) {
+            const SlabPlanes P = slab_planes(L, z0, (int)std::min<int64_t>(z0 + p, E2));
+            if (P.nin * (L.lo[1] + L.hi[1]) + P.nghost * L.n[1] > kRows) return false;
+        }
+        return true;
+    };
+    bool rows_form = !grow && !L.tensorial;
+    if (rows_form) {
+        while (pz > 1 && !rows_fit(pz)) --pz;
+        rows_form = rows_fit(pz);
+    }
     const int64_t slabs = (E2 + pz - 1) / pz;
     if (slabs > 65535) return fail(CN_ERR_UNSUPPORTED, "cn_lab_fill: more than 65535 lab slabs per block");
     const dim3 grid((unsigned)cnt, (unsigned)slabs);
     const int threads = plane * pz >= 1024 ? 256 : 128;
     T *out = reinterpret_cast<T *>(d_labs);
-    if (L.grow[0] || L.grow[1] || L.grow[2]) {
+    if (grow) {
         lab_fill_grow_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, FastDiv((uint32_t)E0),
                                                           FastDiv((uint32_t)plane), apply_bc, out);
     } else {
@@ -530,14 +594,18 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
         dv.wrow = FastDiv((uint32_t)(L.tensorial ? E0 : L.n[0]));
         dv.gy = FastDiv((uint32_t)(L.lo[1] + L.hi[1]));
         dv.wpl = FastDiv((uint32_t)(L.tensorial ? E1 : L.n[1]));
-        // dynamic shared memory for the bulk copy of a slab's block planes
-        const int64_t bulk = (int64_t)pz * L.n[0] * L.n[1] * (int64_t)sizeof(T);
-        const int nbulk = bulk <= kBulkBytes ? (int)bulk : 0;
-        static DeviceOnce once;
-        cn_status r = smem_opt_in(once, lab_fill_kernel<T>, (size_t)kBulkBytes);
-        if (r != CN_OK) return r;
-        lab_fill_kernel<T><<<grid, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, nbulk,
-                                                         g->d_err, out);
+        if (rows_form) {
+            // dynamic shared memory for the bulk copy of a slab's block planes
+            const int64_t bulk = (int64_t)pz * L.n[0] * L.n[1] * (int64_t)sizeof(T);
+            const int nbulk = bulk <= kBulkBytes ? (int)bulk : 0;
+            static DeviceOnce once;
+            cn_status r = smem_opt_in(once, lab_fill_rows_kernel<T>, (size_t)kBulkBytes);
+            if (r != CN_OK) return r;
+            lab_fill_rows_kernel<T><<<grid, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc,
+                                                                  nbulk, g->d_err, out);
+        } else {
+            lab_fill_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, out);
+        }
     }
     CN_CUDA_TRY(cudaGetLastError());
     return CN_OK;
