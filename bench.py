@@ -880,11 +880,11 @@ class LAB:
     # ghost cells read from neighbours are re-reads and not counted
     bytes_per_cell_step = 5 * (8 + 8 * (32 ** 3 + 6 * 3 * 32 ** 2) / 32 ** 3)
     # DRAM bytes per cell of one ncu capture of a launch on 8x8x8 blocks of
-    # 32^3 (175.0 MB read + 174.4 MB written for 16.8 M cells), times the 5
+    # 32^3 (169.7 MB read + 166.4 MB written for 16.8 M cells), times the 5
     # launches of a step; traffic grows with the blocks processed
-    traffic_per_cell_step = 104.1
-    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one lab_fill_kernel launch on 8x8x8 "
-                      "blocks of 32^3, per cell, times the 5 launches of a step")
+    traffic_per_cell_step = 100.2
+    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one lab_fill_rows_kernel launch on "
+                      "8x8x8 blocks of 32^3, per cell, times the 5 launches of a step")
     cpu_nb = (8, 8, 4)
 
     def __init__(self):
