@@ -157,8 +157,9 @@ def test_load_labs_c2_geometry_vs_oracle(cn, oracle_lib):
 
 def test_lab_fill_long_rows_vs_oracle(cn, oracle_lib):
     """Blocks whose lab slabs hold more ghost rows than the kernel resolves in
-    one round (2 x 200 x 6 cells: 412 rows per slab), with BCs and skips on
-    every face, non-tensorial and tensorial: bit-exact against the oracle."""
+    one round (2 x 200 x 6 cells: slabs of 208 and 204 ghost rows against a
+    table of 96), with BCs and skips on every face, non-tensorial and
+    tensorial: bit-exact against the oracle."""
     O = oracle_lib
     rng = np.random.default_rng(21)
     nb, n = (2, 2, 2), (2, 200, 6)
@@ -172,5 +173,27 @@ def test_lab_fill_long_rows_vs_oracle(cn, oracle_lib):
         labs, written = lab_fill_all(cn, g, (1, 1, 1), (1, 1, 1), tens)
         for b in range(nblocks):
             want, wdef = O.lab_fill(comp, nb, n, (1, 1, 1), (1, 1, 1), tens, bcl, b)
+            LC.compare_defined(labs[b], written[b], want, wdef)
+        g.close()
+
+
+def test_lab_fill_thinner_slabs_vs_oracle(cn, oracle_lib):
+    """Blocks of 4 x 40 x 6 cells with two ghost planes along z: a slab of the
+    whole lab (10 planes) holds 172 ghost rows, more than the one-pass
+    kernel's table, so the host takes slabs of 8 planes (92 and 80 rows) and
+    keeps that kernel; BCs on some faces, bit-exact against the oracle."""
+    O = oracle_lib
+    rng = np.random.default_rng(31)
+    nb, n, lo, hi = (2, 2, 2), (4, 40, 6), (1, 1, 2), (1, 1, 2)
+    nblocks = 8
+    for dt in (np.float64, np.float32):
+        stride = O.block_stride(n, dt)
+        comp = (rng.standard_normal(nblocks * stride) * 10).astype(dt)
+        bcl = {b: [(int(rng.integers(0, 3)), int(rng.integers(0, 2)), int(rng.integers(0, 4)),
+                    float(rng.choice([-1, 0.5, 2]))) for _ in range(2)] for b in range(nblocks) if b % 3 == 0}
+        g = make_grid(cn, comp, nb, n, bcl)
+        labs, written = lab_fill_all(cn, g, lo, hi, False)
+        for b in range(nblocks):
+            want, wdef = O.lab_fill(comp, nb, n, lo, hi, False, bcl, b)
             LC.compare_defined(labs[b], written[b], want, wdef)
         g.close()
