@@ -10,8 +10,10 @@
 // closed form (the periodic neighbour's cell), eight loads in flight per
 // thread; ghost rows behind faces with BCs are resolved once per row (x
 // passes through the FieldLab resolution unchanged), other BC-chain cells
-// one by one (cn::lab_resolve: skip rule, BC chain).  Tensorial labs, node
-// and face grids take per-class or per-cell resolution throughout.  Stores
+// one by one (cn::lab_resolve: skip rule, BC chain); this one-pass form is
+// lab_fill_rows_kernel.  Tensorial labs and labs with ghost rows longer than
+// its row table (lab_fill_kernel), node and face grids
+// (lab_fill_grow_kernel) take per-class or per-cell resolution.  Stores
 // are coalesced along the lab's rows; the kernel is bound by memory
 // latency and HBM.  The stencil kernels fuse the same resolution into their
 // shared-memory staging; this kernel gives the reference's FieldLab
