@@ -245,7 +245,9 @@ __global__ void __launch_bounds__(256, kRowsCtas)
     const int E0 = n0 + L.lo[0] + L.hi[0];
     const int E1 = n1 + L.lo[1] + L.hi[1];
     const int E2 = L.n[2] + L.lo[2] + L.hi[2];
-    const int bl = blockIdx.x, z0 = blockIdx.y * pz;
+    // one CTA per (slab, block): x the slab, so that a block's slabs run
+    // together (CTAs start in the order of their linear index)
+    const int bl = blockIdx.y, z0 = blockIdx.x * pz;
     const int block = block_begin + bl;
     const int bx = block % L.nb[0];
     const int by = (block / L.nb[0]) % L.nb[1];
@@ -603,8 +605,13 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
             static DeviceOnce once;
             cn_status r = smem_opt_in(once, lab_fill_rows_kernel<T>, (size_t)kBulkBytes);
             if (r != CN_OK) return r;
-            lab_fill_rows_kernel<T><<<grid, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc,
-                                                                  nbulk, g->d_err, out);
+            // blocks along y, at most 65535 per launch
+            for (int c0 = 0; c0 < cnt; c0 += 65535) {
+                const dim3 grid_bm((unsigned)slabs, (unsigned)std::min(65535, cnt - c0));
+                lab_fill_rows_kernel<T><<<grid_bm, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0 + c0, pz, dv,
+                                                                         apply_bc, nbulk, g->d_err,
+                                                                         out + (int64_t)c0 * plane * E2);
+            }
         } else {
             lab_fill_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, out);
         }
