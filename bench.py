@@ -880,11 +880,12 @@ class LAB:
     # ghost cells read from neighbours are re-reads and not counted
     bytes_per_cell_step = 5 * (8 + 8 * (32 ** 3 + 6 * 3 * 32 ** 2) / 32 ** 3)
     # DRAM bytes per cell of one ncu capture of a launch on 8x8x8 blocks of
-    # 32^3 (169.7 MB read + 166.4 MB written for 16.8 M cells), times the 5
-    # launches of a step; traffic grows with the blocks processed
-    traffic_per_cell_step = 100.2
-    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one lab_fill_rows_kernel launch on "
-                      "8x8x8 blocks of 32^3, per cell, times the 5 launches of a step")
+    # 32^3 (147.6 MB read + 163.6 MB written for 16.8 M cells, mean of 3
+    # launches), times the 5 launches of a step; traffic grows with the
+    # blocks processed
+    traffic_per_cell_step = 92.7
+    traffic_source = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of lab_fill_rows_kernel on 8x8x8 blocks "
+                      "of 32^3 (mean of 3 launches), per cell, times the 5 launches of a step")
     cpu_nb = (8, 8, 4)
 
     def __init__(self):
