@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(256)
     const int E1 = L.n[1] + L.lo[1] + L.hi[1];
     const int E2 = L.n[2] + L.lo[2] + L.hi[2];
     const int plane = E0 * E1;
-    const int bl = blockIdx.x, z0 = blockIdx.y * pz;
+    const int bl = blockIdx.y, z0 = blockIdx.x * pz; // block-major, as lab_fill_rows_kernel
     const int nz = min(pz, E2 - z0);
     const int block = block_begin + bl;
     const int bx = block % L.nb[0];
@@ -246,7 +246,9 @@ __global__ void __launch_bounds__(256, kRowsCtas)
     const int E1 = n1 + L.lo[1] + L.hi[1];
     const int E2 = L.n[2] + L.lo[2] + L.hi[2];
     // one CTA per (slab, block): x the slab, so that a block's slabs run
-    // together (CTAs start in the order of their linear index)
+    // together (CTAs start in the order of their linear index) and the ghost
+    // planes read from a block's z neighbours are read close in time to the
+    // neighbours' own CTAs, while they are in L2
     const int bl = blockIdx.y, z0 = blockIdx.x * pz;
     const int block = block_begin + bl;
     const int bx = block % L.nb[0];
@@ -398,7 +400,7 @@ __global__ void __launch_bounds__(256, 4)
     const int E0 = n0 + L.lo[0] + L.hi[0];
     const int E1 = n1 + L.lo[1] + L.hi[1];
     const int E2 = n2 + L.lo[2] + L.hi[2];
-    const int bl = blockIdx.x, z0 = blockIdx.y * pz;
+    const int bl = blockIdx.y, z0 = blockIdx.x * pz; // block-major, as lab_fill_rows_kernel
     const int z1 = min(z0 + pz, E2);
     const int block = block_begin + bl;
     const int bx = block % L.nb[0];
@@ -584,36 +586,36 @@ static cn_status launch_fill(cn_grid *g, int comp, const cn_stencil *s, int b0, 
     }
     const int64_t slabs = (E2 + pz - 1) / pz;
     if (slabs > 65535) return fail(CN_ERR_UNSUPPORTED, "cn_lab_fill: more than 65535 lab slabs per block");
-    const dim3 grid((unsigned)cnt, (unsigned)slabs);
     const int threads = plane * pz >= 1024 ? 256 : 128;
-    T *out = reinterpret_cast<T *>(d_labs);
-    if (grow) {
-        lab_fill_grow_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, FastDiv((uint32_t)E0),
-                                                          FastDiv((uint32_t)plane), apply_bc, out);
-    } else {
-        LabDivs dv;
-        dv.n0 = FastDiv((uint32_t)L.n[0]);
-        dv.n1 = FastDiv((uint32_t)L.n[1]);
-        dv.gx = FastDiv((uint32_t)(L.lo[0] + L.hi[0]));
-        dv.wrow = FastDiv((uint32_t)(L.tensorial ? E0 : L.n[0]));
-        dv.gy = FastDiv((uint32_t)(L.lo[1] + L.hi[1]));
-        dv.wpl = FastDiv((uint32_t)(L.tensorial ? E1 : L.n[1]));
-        if (rows_form) {
-            // dynamic shared memory for the bulk copy of a slab's block planes
-            const int64_t bulk = (int64_t)pz * L.n[0] * L.n[1] * (int64_t)sizeof(T);
-            const int nbulk = bulk <= kBulkBytes ? (int)bulk : 0;
-            static DeviceOnce once;
-            cn_status r = smem_opt_in(once, lab_fill_rows_kernel<T>, (size_t)kBulkBytes);
-            if (r != CN_OK) return r;
-            // blocks along y, at most 65535 per launch
-            for (int c0 = 0; c0 < cnt; c0 += 65535) {
-                const dim3 grid_bm((unsigned)slabs, (unsigned)std::min(65535, cnt - c0));
-                lab_fill_rows_kernel<T><<<grid_bm, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0 + c0, pz, dv,
-                                                                         apply_bc, nbulk, g->d_err,
-                                                                         out + (int64_t)c0 * plane * E2);
-            }
+    LabDivs dv;
+    dv.n0 = FastDiv((uint32_t)L.n[0]);
+    dv.n1 = FastDiv((uint32_t)L.n[1]);
+    dv.gx = FastDiv((uint32_t)(L.lo[0] + L.hi[0]));
+    dv.wrow = FastDiv((uint32_t)(L.tensorial ? E0 : L.n[0]));
+    dv.gy = FastDiv((uint32_t)(L.lo[1] + L.hi[1]));
+    dv.wpl = FastDiv((uint32_t)(L.tensorial ? E1 : L.n[1]));
+    // dynamic shared memory for the bulk copy of a slab's block planes
+    const int64_t bulk = (int64_t)pz * L.n[0] * L.n[1] * (int64_t)sizeof(T);
+    const int nbulk = rows_form && bulk <= kBulkBytes ? (int)bulk : 0;
+    if (rows_form) {
+        static DeviceOnce once;
+        cn_status r = smem_opt_in(once, lab_fill_rows_kernel<T>, (size_t)kBulkBytes);
+        if (r != CN_OK) return r;
+    }
+    // CTAs in block-major order: the slab along x, the block along y (a
+    // block's slabs run together), at most 65535 blocks per launch
+    for (int c0 = 0; c0 < cnt; c0 += 65535) {
+        const dim3 grid((unsigned)slabs, (unsigned)std::min(65535, cnt - c0));
+        T *out = reinterpret_cast<T *>(d_labs) + (int64_t)c0 * plane * E2;
+        if (grow) {
+            lab_fill_grow_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0 + c0, pz,
+                                                              FastDiv((uint32_t)E0), FastDiv((uint32_t)plane),
+                                                              apply_bc, out);
+        } else if (rows_form) {
+            lab_fill_rows_kernel<T><<<grid, threads, nbulk, st>>>(src, L, bc_view(g, comp), b0 + c0, pz, dv,
+                                                                  apply_bc, nbulk, g->d_err, out);
         } else {
-            lab_fill_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0, pz, dv, apply_bc, out);
+            lab_fill_kernel<T><<<grid, threads, 0, st>>>(src, L, bc_view(g, comp), b0 + c0, pz, dv, apply_bc, out);
         }
     }
     CN_CUDA_TRY(cudaGetLastError());
